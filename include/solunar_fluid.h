@@ -1,0 +1,198 @@
+/*
+ * solunar_fluid.h -- C ABI of the B200 particle-fluid library.
+ *
+ * This is the drop-in boundary for solunar's particle fluid (`FluidWorld`, src/fluid in
+ * SkuldNorniern/solunar).  The reference has no FFI of its own: its interface is the Rust
+ * public API re-exported at src/lib.rs:53-57.  Every entry point below names the Rust
+ * item it replaces (file:line, relative to the reference project).
+ *
+ * Conventions
+ *  - Every call returns an int32_t status: SLF_OK or one of the SLF_ERR_* codes.  Codes 1..5
+ *    are the PhysicsError variants the fluid uses (src/error.rs:5-22).
+ *  - Handles are opaque.  The library owns all device memory; callers own host buffers.
+ *  - Calls on one handle must not overlap (the Rust methods take `&mut self`).  Each handle
+ *    issues its work on one CUDA stream of its own and returns when that work is done.
+ *  - Vectors are passed as `float[3]` (x, y, z); arrays of vectors are packed xyz triples.
+ *  - On error the particles are left as the last finished substep put them
+ *    (src/fluid/step.rs:55-57).
+ *  - There is no host job dispatcher: the `&dyn JobDispatch` argument of the Rust methods
+ *    (src/dispatch.rs:1-7) has no counterpart, the GPU is the dispatcher.
+ */
+#ifndef SOLUNAR_FLUID_H
+#define SOLUNAR_FLUID_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+enum {
+    SLF_OK = 0,
+    SLF_ERR_INVALID_SETTINGS = 1,    /* PhysicsError::InvalidSettings (src/error.rs:11) */
+    SLF_ERR_NON_FINITE = 2,          /* PhysicsError::NonFinite(_) (src/error.rs:9) */
+    SLF_ERR_OUT_OF_RANGE = 3,        /* PhysicsError::OutOfRange (src/error.rs:14) */
+    SLF_ERR_FLUID_FULL = 4,          /* PhysicsError::FluidFull (src/error.rs:21) */
+    SLF_ERR_DISPATCH_INCOMPLETE = 5, /* PhysicsError::DispatchIncomplete (src/error.rs:15) */
+    SLF_ERR_UNSUPPORTED = 6,         /* a feature off the fluid step (movers, terrain) */
+    SLF_ERR_CUDA = 7,                /* a CUDA call failed; see slf_last_error() */
+    SLF_ERR_TIMEOUT = 8,             /* a bounded device loop gave up */
+    SLF_ERR_INVALID_ARGUMENT = 9     /* null pointer or wrong buffer size */
+};
+
+/* FluidSolver (src/fluid/mod.rs:43-53). */
+enum { SLF_SOLVER_WCSPH = 0, SLF_SOLVER_DFSPH = 1 };
+
+/* How particle positions are held on the device.  ABSOLUTE follows the reference's f32
+ * arithmetic; CELL_RELATIVE keeps each position as an offset from the origin of its grid
+ * cell, so neighbour offsets do not lose bits to the magnitude of the coordinates. */
+enum { SLF_POSITIONS_ABSOLUTE = 0, SLF_POSITIONS_CELL_RELATIVE = 1 };
+
+/* EXACT rounds every operation as the reference's scalar f32 code does (no fused
+ * multiply-add, IEEE division and square root), so results match the CPU restatement bit
+ * for bit.  FAST lets the compiler fuse and uses reciprocal forms inside the pair loops. */
+enum { SLF_ARITHMETIC_EXACT = 0, SLF_ARITHMETIC_FAST = 1 };
+
+/* FluidSettings (src/fluid/mod.rs:55-78) followed by this library's own fields.  Defaults
+ * come from slf_settings_default() and equal FluidSettings::default (mod.rs:80-95) and the
+ * DFSPH constants (src/fluid/dfsph.rs:8-16). */
+typedef struct slf_settings {
+    int32_t solver;          /* SLF_SOLVER_* */
+    float spacing;           /* m between particles at rest */
+    float rest_density;      /* kg/m^3 */
+    float support;           /* kernel reach as a multiple of spacing, 1.5..4.0 */
+    uint64_t max_particles;
+    float sound_speed;       /* m/s */
+    float viscosity;
+    float gravity[3];        /* m/s^2 */
+    float courant;           /* share of the kernel radius a particle may move a substep */
+    uint32_t max_substeps;
+    /* library fields (the reference hard-codes these) */
+    int32_t positions;             /* SLF_POSITIONS_*, default ABSOLUTE */
+    int32_t arithmetic;            /* SLF_ARITHMETIC_*, default EXACT */
+    int32_t warm_start;            /* DFSPH solves start from last substep's stiffness; 0 */
+    float divergence_tolerance;    /* dfsph.rs:11, 1e-3 */
+    float density_tolerance;       /* dfsph.rs:9, 5e-4 */
+    uint32_t min_iterations;       /* dfsph.rs:12, 2 */
+    uint32_t max_iterations;       /* dfsph.rs:13, 100 */
+} slf_settings;
+
+/* FluidReport (src/fluid/step.rs:27-49). */
+typedef struct slf_report {
+    uint32_t substeps;
+    int32_t capped;
+    float max_compression;
+    float max_speed;
+    uint32_t held_back;
+    uint32_t iterations;
+    uint32_t emitted;
+    uint32_t drained;
+    uint32_t lost;
+    float sound_speed;
+} slf_report;
+
+typedef struct slf_world slf_world;
+
+/* ---- settings and lifetime --------------------------------------------------------- */
+
+/* FluidSettings::default (src/fluid/mod.rs:80-95). */
+int32_t slf_settings_default(slf_settings* out);
+
+/* FluidWorld::new (src/fluid/mod.rs:344); FluidSettings::validate (mod.rs:98-117).  Fails
+ * with SLF_ERR_INVALID_SETTINGS on settings out of range, SLF_ERR_CUDA without a device. */
+int32_t slf_create(const slf_settings* settings, slf_world** out);
+
+/* Drop of FluidWorld.  Null is ignored. */
+void slf_destroy(slf_world* world);
+
+/* FluidWorld::settings (mod.rs:372). */
+int32_t slf_get_settings(const slf_world* world, slf_settings* out);
+
+/* FluidWorld::particle_mass (mod.rs:380). */
+int32_t slf_particle_mass(const slf_world* world, float* out);
+
+/* FluidWorld::kernel (mod.rs:376): the Wendland C2 kernel's radius and scale (mod.rs:125-138). */
+int32_t slf_kernel(const slf_world* world, float* radius, float* scale);
+
+/* FluidWorld::len (mod.rs:384). */
+int32_t slf_len(const slf_world* world, uint64_t* out);
+
+/* ---- particles, walls, domain ------------------------------------------------------ */
+
+/* FluidWorld::add_particle (mod.rs:412-426). */
+int32_t slf_add_particle(slf_world* world, const float position[3], const float velocity[3],
+                         uint32_t* id_out);
+
+/* n calls of FluidWorld::add_particle, all or none: every value is checked first.  ids_out
+ * may be null. */
+int32_t slf_add_particles(slf_world* world, uint64_t n, const float* positions,
+                          const float* velocities, uint32_t* ids_out);
+
+/* FluidWorld::fill_box (mod.rs:493-524). */
+int32_t slf_fill_box(slf_world* world, const float low[3], const float high[3],
+                     uint64_t* count_out);
+
+/* FluidWorld::set_domain (mod.rs:433-444).  low == high == NULL clears the domain. */
+int32_t slf_set_domain(slf_world* world, const float* low, const float* high);
+
+/* FluidWorld::add_box_container (src/fluid/boundary.rs:41-68). */
+int32_t slf_add_box_container(slf_world* world, const float low[3], const float high[3],
+                              uint32_t* boundary_out);
+
+/* FluidWorld::add_wall (boundary.rs:74-91). */
+int32_t slf_add_wall(slf_world* world, const float low[3], const float high[3],
+                     uint32_t* boundary_out);
+
+/* FluidWorld::remove_boundary (boundary.rs:94-115).  *removed = 0 for an unknown id. */
+int32_t slf_remove_boundary(slf_world* world, uint32_t boundary, int32_t* removed);
+
+/* FluidWorld::wall_positions (boundary.rs:118-120): count, then xyz triples in wall order. */
+int32_t slf_wall_count(const slf_world* world, uint64_t* out);
+int32_t slf_read_wall_positions(const slf_world* world, float* out, uint64_t n);
+
+/* ---- the step ------------------------------------------------------------------------ */
+
+/* FluidWorld::step (src/fluid/step.rs:58-90): as many WCSPH substeps as the flow needs
+ * (step.rs:102-224) or DFSPH substeps (src/fluid/dfsph.rs:46-103). */
+int32_t slf_step(slf_world* world, float dt, slf_report* out);
+
+/* FluidWorld::update_neighbors (mod.rs:540-608): sorts particles by cell then id. */
+int32_t slf_update_neighbors(slf_world* world);
+
+/* FluidWorld::compute_densities (mod.rs:621-675).  SLF_ERR_OUT_OF_RANGE when particles were
+ * added since the last slf_update_neighbors. */
+int32_t slf_compute_densities(slf_world* world);
+
+/* ---- read-outs (arrays in the current particle order) ------------------------------ */
+
+/* FluidWorld::ids (mod.rs:393), positions (:397), velocities (:401), densities (:406).
+ * n must equal slf_len(). */
+int32_t slf_read_ids(const slf_world* world, uint32_t* out, uint64_t n);
+int32_t slf_read_positions(const slf_world* world, float* out, uint64_t n);
+int32_t slf_read_velocities(const slf_world* world, float* out, uint64_t n);
+int32_t slf_read_densities(const slf_world* world, float* out, uint64_t n);
+
+/* FluidWorld::neighbors_of (mod.rs:612-614) for every particle at once, as the lists the
+ * last slf_update_neighbors would build (mod.rs:279-308): start[n+1] and items.  Call with
+ * items == NULL to learn *items_len.  start may be NULL. */
+int32_t slf_neighbor_lists(slf_world* world, uint32_t* start, uint64_t start_len,
+                           uint32_t* items, uint64_t items_capacity, uint64_t* items_len);
+
+/* The wall lists of the same pass (`wall_neighbors`, mod.rs:327), indexes into the wall
+ * order of slf_read_wall_positions. */
+int32_t slf_wall_neighbor_lists(slf_world* world, uint32_t* start, uint64_t start_len,
+                                uint32_t* items, uint64_t items_capacity, uint64_t* items_len);
+
+/* FluidWorld::state_hash (mod.rs:677-691), FNV-1a (src/snapshot/bytes.rs:6-13). */
+int32_t slf_state_hash(const slf_world* world, uint64_t* out);
+
+/* Message of the last failed call on any handle of this thread ("" if none). */
+const char* slf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOLUNAR_FLUID_H */

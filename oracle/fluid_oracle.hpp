@@ -1,0 +1,1125 @@
+// fluid_oracle.hpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of solunar's particle-fluid step, the checker for the CUDA library.  Only
+// tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it; the library never
+// links or calls it.  Templated on the arithmetic type: `float` is the parity oracle and the
+// timed CPU baseline, `double` is the precision oracle.
+//
+// It follows, function by function (paths relative to the reference project):
+//   src/fluid/mod.rs      Kernel :125-165, Grid :169-262, near :264-277, Lists :279-308,
+//                         add_particle :412, set_domain :433, keep_in_domain :451,
+//                         fill_box :493-524, cell_of :526-533, update_neighbors :540-608,
+//                         compute_densities :621-675, state_hash :677-691, rest_mass :694-709
+//   src/fluid/step.rs     step :58-90, fastest :92-96, wcsph :102-116, wcsph_steps :118-142,
+//                         wcsph_substep :144-224, viscous :229-251, viscosity :254-259,
+//                         wall_viscous :262-301, advance :305-339
+//   src/fluid/dfsph.rs    dfsph :46-77, dfsph_substep :79-103, gradients :108-136,
+//                         factors :138-163, density_rate :166-181, push_apart :184-216,
+//                         solve :222-275
+//   src/fluid/boundary.rs add_box_container :41-68, add_wall :74-91, remove_boundary :94-115,
+//                         cells_in :123-126, check_room :128-137, settle_walls :155-178,
+//                         check_box :230-238, union :240-247
+//   src/snapshot/bytes.rs fnv1a :6-13
+//
+// Arithmetic follows the reference's scalar code: left-to-right evaluation, no fused
+// multiply-add (build with -ffp-contract=off), IEEE division and square root, `powi` as binary
+// exponentiation, `Iterator::sum` as a sequential fold.  The reference's vector type comes from
+// the un-vendored `algebrix` crate (git rev 1bf888b98936f382f1def04ce06b15fbbfcdd46d); its
+// operations are assumed to be componentwise IEEE f32 with dot = x*x' + y*y' + z*z' summed left
+// to right, length = sqrt(dot), v / s divided per component, normalize_or dividing by the
+// length.  Parity with the Rust binary itself is therefore unpinned at the bit level; the
+// reference's own tests (property tests, no stored vectors) pin this restatement instead.
+//
+// Movers (rigid coupling), terrain, emitters and drains are not on the path: they are absent
+// from this restatement, as they are empty in every configuration it is run on.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <tuple>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace oracle {
+
+enum Status : int32_t {
+    OK = 0,
+    INVALID_SETTINGS = 1,
+    NON_FINITE = 2,
+    OUT_OF_RANGE = 3,
+    FLUID_FULL = 4,
+    DISPATCH_INCOMPLETE = 5,
+    UNSUPPORTED = 6,
+    INVALID_ARGUMENT = 9,
+};
+
+// ---- scalar helpers ---------------------------------------------------------------------
+
+// Rust f32::min / f32::max: a NaN operand yields the other one.
+template <class R> inline R rmin(R a, R b) {
+    if (std::isnan(a)) return b;
+    if (std::isnan(b)) return a;
+    return b < a ? b : a;
+}
+template <class R> inline R rmax(R a, R b) {
+    if (std::isnan(a)) return b;
+    if (std::isnan(b)) return a;
+    return b > a ? b : a;
+}
+// `powi` lowered to binary exponentiation (mod.rs:136,145,154; step.rs:149,156).
+template <class R> inline R pow2(R x) { return x * x; }
+template <class R> inline R pow3(R x) { return x * (x * x); }
+template <class R> inline R pow4(R x) { R s = x * x; return s * s; }
+template <class R> inline R pow7(R x) { R s = x * x; R q = s * s; return (x * s) * q; }
+
+// Rust `as i32` from a float: saturating, NaN to zero (mod.rs:529-531).
+template <class R> inline int32_t sat_i32(R v) {
+    if (std::isnan(v)) return 0;
+    if (v >= R(2147483647.0)) return std::numeric_limits<int32_t>::max();
+    if (v <= R(-2147483648.0)) return std::numeric_limits<int32_t>::min();
+    return static_cast<int32_t>(v);
+}
+
+template <class R> inline uint64_t bits_of(R v) {
+    if constexpr (std::is_same_v<R, float>) {
+        uint32_t b;
+        std::memcpy(&b, &v, 4);
+        return b;
+    } else {
+        uint64_t b;
+        std::memcpy(&b, &v, 8);
+        return b;
+    }
+}
+
+// ---- vectors ------------------------------------------------------------------------------
+
+template <class R> struct V3 {
+    R x{0}, y{0}, z{0};
+    V3() = default;
+    V3(R a, R b, R c) : x(a), y(b), z(c) {}
+    static V3 splat(R v) { return V3(v, v, v); }
+    bool operator==(const V3& o) const { return x == o.x && y == o.y && z == o.z; }
+    bool operator!=(const V3& o) const { return !(*this == o); }
+};
+template <class R> inline V3<R> operator+(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class R> inline V3<R> operator-(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class R> inline V3<R> operator-(V3<R> a) { return {-a.x, -a.y, -a.z}; }
+template <class R> inline V3<R> operator*(V3<R> a, R s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class R> inline V3<R> operator/(V3<R> a, R s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class R> inline R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R> inline R length_squared(V3<R> a) { return dot(a, a); }
+template <class R> inline R length(V3<R> a) { return std::sqrt(length_squared(a)); }
+template <class R> inline bool is_finite(V3<R> a) {
+    return std::isfinite(a.x) && std::isfinite(a.y) && std::isfinite(a.z);
+}
+template <class R> inline V3<R> vmin(V3<R> a, V3<R> b) { return {rmin(a.x, b.x), rmin(a.y, b.y), rmin(a.z, b.z)}; }
+template <class R> inline V3<R> vmax(V3<R> a, V3<R> b) { return {rmax(a.x, b.x), rmax(a.y, b.y), rmax(a.z, b.z)}; }
+template <class R> inline V3<R> clamp(V3<R> v, V3<R> lo, V3<R> hi) { return vmin(vmax(v, lo), hi); }
+template <class R> inline V3<R> normalize_or(V3<R> v, V3<R> fallback) {
+    R len = length(v);
+    if (std::isfinite(len) && len > R(0)) return v / len;
+    return fallback;
+}
+
+// ---- settings -------------------------------------------------------------------------------
+
+struct Settings {
+    int32_t solver = 0;  // 0 WCSPH, 1 DFSPH
+    float spacing = 0.05f;
+    float rest_density = 1000.0f;
+    float support = 2.0f;
+    uint64_t max_particles = uint64_t(1) << 22;
+    float sound_speed = 20.0f;
+    float viscosity = 0.15f;
+    float gravity[3] = {0.0f, -9.81f, 0.0f};
+    float courant = 0.4f;
+    uint32_t max_substeps = 2000;
+    float divergence_tolerance = 1e-3f;
+    float density_tolerance = 5e-4f;
+    uint32_t min_iterations = 2;
+    uint32_t max_iterations = 100;
+    // 0: the reference's sequential sum of the solver error in the working precision
+    //    (dfsph.rs:266-267); 1: a compensated sum in double, as the CUDA library takes it.
+    int32_t residual_sum = 0;
+
+    // mod.rs:98-117
+    bool valid() const {
+        auto positive = [](float v) { return std::isfinite(v) && v > 0.0f; };
+        bool support_ok = support >= 1.5f && support <= 4.0f;
+        return positive(spacing) && positive(rest_density) && support_ok && max_particles > 0 &&
+               positive(sound_speed) && std::isfinite(viscosity) && viscosity >= 0.0f &&
+               std::isfinite(gravity[0]) && std::isfinite(gravity[1]) && std::isfinite(gravity[2]) &&
+               courant > 0.0f && courant <= 1.0f && max_substeps > 0;
+    }
+};
+
+struct Report {
+    uint32_t substeps = 0;
+    int32_t capped = 0;
+    float max_compression = 0;
+    float max_speed = 0;
+    uint32_t held_back = 0;
+    uint32_t iterations = 0;
+    uint32_t emitted = 0, drained = 0, lost = 0;
+    float sound_speed = 0;
+};
+
+// ---- kernel (mod.rs:125-165) ------------------------------------------------------------
+
+template <class R> struct Kernel {
+    R radius{0}, scale{0};
+    Kernel() = default;
+    explicit Kernel(R r) : radius(r), scale(R(21) / (R(2) * R(3.14159265358979323846) * pow3(r))) {}
+    R value(R distance) const {
+        R q = distance / radius;
+        if (q >= R(1)) return R(0);
+        return scale * pow4(R(1) - q) * (R(1) + R(4) * q);
+    }
+    R slope(R distance) const {
+        R q = distance / radius;
+        if (q >= R(1)) return R(0);
+        return scale * R(-20) * q * pow3(R(1) - q) / radius;
+    }
+    V3<R> gradient(V3<R> offset) const {
+        R distance = length(offset);
+        if (distance <= R(0)) return V3<R>();
+        return offset * (slope(distance) / distance);
+    }
+};
+
+// ---- grid (mod.rs:167-262) -----------------------------------------------------------------
+
+struct Key {
+    int32_t x, y, z;
+    bool operator==(const Key& o) const { return x == o.x && y == o.y && z == o.z; }
+    bool operator!=(const Key& o) const { return !(*this == o); }
+    bool operator<(const Key& o) const { return std::tie(x, y, z) < std::tie(o.x, o.y, o.z); }
+};
+
+struct Range {
+    uint32_t begin, end;
+    bool operator==(const Range& o) const { return begin == o.begin && end == o.end; }
+};
+
+struct Grid {
+    std::vector<std::pair<Key, Range>> cells;
+    std::vector<uint32_t> dense;
+    Key low{0, 0, 0};
+    int64_t span[3] = {0, 0, 0};
+
+    // `keys` already sorted (mod.rs:182-197).
+    static Grid build(const std::vector<Key>& keys) {
+        Grid g;
+        for (size_t i = 0; i < keys.size(); ++i) {
+            uint32_t index = uint32_t(i);
+            if (!g.cells.empty() && g.cells.back().first == keys[i]) {
+                g.cells.back().second.end = index + 1;
+            } else {
+                g.cells.push_back({keys[i], Range{index, index + 1}});
+            }
+        }
+        g.index();
+        return g;
+    }
+
+    // mod.rs:199-227: a dense table while its box is at most 64 cells per occupied one + 4096.
+    void index() {
+        if (cells.empty()) return;
+        Key lo = cells[0].first, hi = cells[0].first;
+        for (auto& c : cells) {
+            lo = Key{std::min(lo.x, c.first.x), std::min(lo.y, c.first.y), std::min(lo.z, c.first.z)};
+            hi = Key{std::max(hi.x, c.first.x), std::max(hi.y, c.first.y), std::max(hi.z, c.first.z)};
+        }
+        int64_t sx = int64_t(hi.x) - lo.x + 1, sy = int64_t(hi.y) - lo.y + 1, sz = int64_t(hi.z) - lo.z + 1;
+        // saturating products, as i64::saturating_mul
+        auto sat_mul = [](int64_t a, int64_t b) -> int64_t {
+            __int128 p = (__int128)a * b;
+            if (p > std::numeric_limits<int64_t>::max()) return std::numeric_limits<int64_t>::max();
+            return (int64_t)p;
+        };
+        int64_t volume = sat_mul(sat_mul(sx, sy), sz);
+        if (volume > 64 * int64_t(cells.size()) + 4096) return;
+        dense.assign(size_t(volume), UINT32_MAX);
+        for (size_t slot = 0; slot < cells.size(); ++slot) {
+            const Key& c = cells[slot].first;
+            int64_t at = (int64_t(c.x - lo.x) * sy + int64_t(c.y - lo.y)) * sz + int64_t(c.z - lo.z);
+            dense[size_t(at)] = uint32_t(slot);
+        }
+        low = lo;
+        span[0] = sx;
+        span[1] = sy;
+        span[2] = sz;
+    }
+
+    bool range(Key key, Range& out) const {
+        size_t slot;
+        if (dense.empty()) {
+            auto it = std::lower_bound(cells.begin(), cells.end(), key,
+                                       [](const std::pair<Key, Range>& c, const Key& k) { return c.first < k; });
+            if (it == cells.end() || it->first != key) return false;
+            slot = size_t(it - cells.begin());
+        } else {
+            int64_t x = int64_t(key.x) - low.x, y = int64_t(key.y) - low.y, z = int64_t(key.z) - low.z;
+            if (x < 0 || x >= span[0] || y < 0 || y >= span[1] || z < 0 || z >= span[2]) return false;
+            uint32_t s = dense[size_t((x * span[1] + y) * span[2] + z)];
+            if (s == UINT32_MAX) return false;
+            slot = s;
+        }
+        out = cells[slot].second;
+        return true;
+    }
+
+    // The 27 cells around, dz outer, then dy, dx inner (mod.rs:250-261).  Neighbour keys are
+    // formed in 64-bit; one past the i32 range holds nothing.
+    void around(Key c, std::vector<Range>& out) const {
+        out.clear();
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int64_t x = int64_t(c.x) + dx, y = int64_t(c.y) + dy, z = int64_t(c.z) + dz;
+                    if (x > INT32_MAX || x < INT32_MIN || y > INT32_MAX || y < INT32_MIN || z > INT32_MAX ||
+                        z < INT32_MIN)
+                        continue;
+                    Range r;
+                    if (range(Key{int32_t(x), int32_t(y), int32_t(z)}, r)) out.push_back(r);
+                }
+    }
+};
+
+// CSR neighbour lists (mod.rs:279-308).
+struct Lists {
+    std::vector<uint32_t> start;
+    std::vector<uint32_t> items;
+    size_t count(size_t i) const {
+        if (i + 1 >= start.size()) return 0;
+        return start[i + 1] - start[i];
+    }
+};
+
+inline uint64_t fnv1a(const uint8_t* data, size_t n) {
+    uint64_t hash = 0xcbf29ce484222325ull;
+    for (size_t i = 0; i < n; ++i) {
+        hash ^= uint64_t(data[i]);
+        hash *= 0x00000100000001b3ull;
+    }
+    return hash;
+}
+
+// Compensated sum in double (Neumaier), the CUDA library's residual reduction.
+struct CompensatedSum {
+    double sum = 0.0, carry = 0.0;
+    void add(double v) {
+        double t = sum + v;
+        if (std::fabs(sum) >= std::fabs(v)) carry += (sum - t) + v;
+        else carry += (v - t) + sum;
+        sum = t;
+    }
+    double value() const { return sum + carry; }
+};
+
+// ---- walls (boundary.rs:20-33) ------------------------------------------------------------
+
+template <class R> struct Container {
+    uint32_t id;
+    V3<R> low, high;
+};
+
+template <class R> struct Walls {
+    std::vector<V3<R>> positions;
+    std::vector<uint32_t> owners;
+    Grid grid;
+    uint32_t next = 0;
+    bool has_bounds = false;
+    V3<R> bounds_low, bounds_high;
+    std::vector<Container<R>> containers;
+};
+
+// ---- the world --------------------------------------------------------------------------------
+
+template <class R> class World {
+  public:
+    using Vec = V3<R>;
+
+    Settings settings;
+    Kernel<R> kernel;
+    R mass{0};
+    std::vector<uint32_t> ids;
+    std::vector<Vec> positions, velocities;
+    std::vector<R> densities;
+    uint32_t next_id = 0;
+    Grid grid;
+    Lists neighbors, wall_neighbors;
+    Walls<R> walls;
+    bool has_domain = false;
+    Vec domain_low, domain_high;
+    // per-pair gradient caches of the last DFSPH substep (dfsph.rs:24-41)
+    std::vector<Vec> grad_fluid, grad_walls;
+    // solver iteration counts of the last DFSPH substep: divergence, density
+    uint32_t last_iterations[2] = {0, 0};
+    int threads = 0;  // 0: OpenMP default
+
+    static Status create(const Settings& s, World& out) {
+        if (!s.valid()) return INVALID_SETTINGS;
+        out = World();
+        out.settings = s;
+        out.kernel = Kernel<R>(radius_of(s));
+        out.mass = rest_mass(s);
+        return OK;
+    }
+
+    static R radius_of(const Settings& s) { return R(s.spacing) * R(s.support); }
+    R radius() const { return radius_of(settings); }
+    size_t len() const { return ids.size(); }
+    Vec gravity() const { return Vec(R(settings.gravity[0]), R(settings.gravity[1]), R(settings.gravity[2])); }
+
+    // mod.rs:694-709
+    static R rest_mass(const Settings& s) {
+        Kernel<R> k(radius_of(s));
+        int reach = int(std::ceil(s.support));
+        R sum = R(0);
+        for (int z = -reach; z <= reach; ++z)
+            for (int y = -reach; y <= reach; ++y)
+                for (int x = -reach; x <= reach; ++x) {
+                    Vec offset = Vec(R(x), R(y), R(z)) * R(s.spacing);
+                    sum += k.value(length(offset));
+                }
+        return R(s.rest_density) / sum;
+    }
+
+    // mod.rs:412-426
+    Status add_particle(Vec position, Vec velocity, uint32_t* id_out) {
+        if (!is_finite(position) || !is_finite(velocity)) return NON_FINITE;
+        if (len() >= settings.max_particles || next_id == UINT32_MAX) return FLUID_FULL;
+        uint32_t id = next_id++;
+        ids.push_back(id);
+        positions.push_back(position);
+        velocities.push_back(velocity);
+        densities.push_back(R(0));
+        if (id_out) *id_out = id;
+        return OK;
+    }
+
+    // mod.rs:433-444
+    Status set_domain(const Vec* low, const Vec* high) {
+        if (low && high) {
+            if (!is_finite(*low) || !is_finite(*high)) return NON_FINITE;
+            if (high->x <= low->x || high->y <= low->y || high->z <= low->z) return OUT_OF_RANGE;
+            has_domain = true;
+            domain_low = *low;
+            domain_high = *high;
+        } else {
+            has_domain = false;
+        }
+        return OK;
+    }
+
+    // mod.rs:451-486
+    uint32_t keep_in_domain() {
+        if (!has_domain) return 0;
+        size_t kept = 0;
+        uint32_t lost = 0;
+        for (size_t i = 0; i < len(); ++i) {
+            if (clamp(positions[i], domain_low, domain_high) == positions[i]) {
+                ids[kept] = ids[i];
+                positions[kept] = positions[i];
+                velocities[kept] = velocities[i];
+                densities[kept] = densities[i];
+                ++kept;
+            } else {
+                ++lost;
+            }
+        }
+        ids.resize(kept);
+        positions.resize(kept);
+        velocities.resize(kept);
+        densities.resize(kept);
+        return lost;
+    }
+
+    // mod.rs:493-524
+    Status fill_box(Vec low, Vec high, uint64_t* count_out) {
+        if (!is_finite(low) || !is_finite(high)) return NON_FINITE;
+        if (high.x < low.x || high.y < low.y || high.z < low.z) return OUT_OF_RANGE;
+        R spacing = R(settings.spacing);
+        auto count = [&](R extent) -> uint64_t {
+            R c = rmin(std::floor(extent / spacing), R(4294967295.0));
+            if (std::isnan(c) || c <= R(0)) return 0;
+            return uint64_t(c);
+        };
+        Vec size = high - low;
+        uint64_t nx = count(size.x), ny = count(size.y), nz = count(size.z);
+        auto sat_mul = [](uint64_t a, uint64_t b) -> uint64_t {
+            unsigned __int128 p = (unsigned __int128)a * b;
+            return p > UINT64_MAX ? UINT64_MAX : uint64_t(p);
+        };
+        uint64_t total = sat_mul(sat_mul(nx, ny), nz);
+        uint64_t room = settings.max_particles > len() ? settings.max_particles - len() : 0;
+        uint64_t ids_left = uint64_t(UINT32_MAX - next_id);
+        if (total > room || total > ids_left) return FLUID_FULL;
+        Vec start = low + Vec::splat(spacing * R(0.5));
+        for (uint64_t y = 0; y < ny; ++y)
+            for (uint64_t z = 0; z < nz; ++z)
+                for (uint64_t x = 0; x < nx; ++x) {
+                    Vec at = start + Vec(R(x), R(y), R(z)) * spacing;
+                    Status st = add_particle(at, Vec(), nullptr);
+                    if (st != OK) return st;
+                }
+        if (count_out) *count_out = total;
+        return OK;
+    }
+
+    // boundary.rs:230-238
+    static Status check_box(Vec low, Vec high) {
+        if (!is_finite(low) || !is_finite(high)) return NON_FINITE;
+        if (high.x <= low.x || high.y <= low.y || high.z <= low.z) return OUT_OF_RANGE;
+        return OK;
+    }
+
+    // boundary.rs:123-126 (f32::round rounds half away from zero)
+    void cells_in(Vec extent, int64_t out[3]) const {
+        auto count = [&](R length) -> int64_t {
+            R c = rmin(std::round(length / R(settings.spacing)), R(1e9));
+            return int64_t(c);
+        };
+        out[0] = count(extent.x);
+        out[1] = count(extent.y);
+        out[2] = count(extent.z);
+    }
+
+    // boundary.rs:128-137
+    Status check_room(int64_t count) const {
+        uint64_t room = settings.max_particles > walls.positions.size()
+                            ? settings.max_particles - walls.positions.size()
+                            : 0;
+        if (count < 0 || uint64_t(count) > room || walls.next == UINT32_MAX) return FLUID_FULL;
+        return OK;
+    }
+
+    // boundary.rs:41-68
+    Status add_box_container(Vec low, Vec high, uint32_t* id_out) {
+        Status st = check_box(low, high);
+        if (st != OK) return st;
+        int64_t cells[3];
+        cells_in(high - low, cells);
+        int64_t layers = int64_t(std::ceil(settings.support));
+        int64_t shell = (cells[0] + 2 * layers) * (cells[1] + 2 * layers) * (cells[2] + 2 * layers) -
+                        cells[0] * cells[1] * cells[2];
+        st = check_room(shell);
+        if (st != OK) return st;
+        R spacing = R(settings.spacing);
+        std::vector<Vec> points;
+        points.reserve(size_t(shell));
+        for (int64_t y = -layers; y < cells[1] + layers; ++y)
+            for (int64_t z = -layers; z < cells[2] + layers; ++z)
+                for (int64_t x = -layers; x < cells[0] + layers; ++x) {
+                    bool inside = x >= 0 && x < cells[0] && y >= 0 && y < cells[1] && z >= 0 && z < cells[2];
+                    if (!inside) {
+                        Vec at(R(float(x)) + R(0.5), R(float(y)) + R(0.5), R(float(z)) + R(0.5));
+                        points.push_back(low + at * spacing);
+                    }
+                }
+        uint32_t id = add_wall_points(points);
+        walls.containers.push_back(Container<R>{id, low, high});
+        update_bounds();
+        if (id_out) *id_out = id;
+        return OK;
+    }
+
+    // boundary.rs:74-91
+    Status add_wall(Vec low, Vec high, uint32_t* id_out) {
+        Status st = check_box(low, high);
+        if (st != OK) return st;
+        int64_t cells[3];
+        cells_in(high - low, cells);
+        for (auto& c : cells) c = std::max<int64_t>(c, 1);
+        int64_t count = cells[0] * cells[1] * cells[2];
+        st = check_room(count);
+        if (st != OK) return st;
+        R spacing = R(settings.spacing);
+        std::vector<Vec> points;
+        points.reserve(size_t(count));
+        for (int64_t y = 0; y < cells[1]; ++y)
+            for (int64_t z = 0; z < cells[2]; ++z)
+                for (int64_t x = 0; x < cells[0]; ++x) {
+                    Vec at(R(float(x)) + R(0.5), R(float(y)) + R(0.5), R(float(z)) + R(0.5));
+                    points.push_back(low + at * spacing);
+                }
+        uint32_t id = add_wall_points(points);
+        if (id_out) *id_out = id;
+        return OK;
+    }
+
+    // boundary.rs:94-115
+    bool remove_boundary(uint32_t id) {
+        size_t before = walls.positions.size();
+        size_t kept = 0;
+        for (size_t i = 0; i < walls.positions.size(); ++i) {
+            if (walls.owners[i] != id) {
+                walls.positions[kept] = walls.positions[i];
+                walls.owners[kept] = walls.owners[i];
+                ++kept;
+            }
+        }
+        walls.positions.resize(kept);
+        walls.owners.resize(kept);
+        bool had_container = false;
+        std::vector<Container<R>> rest;
+        for (auto& c : walls.containers) {
+            if (c.id == id) had_container = true;
+            else rest.push_back(c);
+        }
+        walls.containers = rest;
+        update_bounds();
+        bool gone = walls.positions.size() != before || had_container;
+        if (gone) settle_walls();
+        return gone;
+    }
+
+    // boundary.rs:240-247
+    void update_bounds() {
+        walls.has_bounds = false;
+        for (auto& c : walls.containers) {
+            if (!walls.has_bounds) {
+                walls.bounds_low = c.low;
+                walls.bounds_high = c.high;
+                walls.has_bounds = true;
+            } else {
+                walls.bounds_low = vmin(walls.bounds_low, c.low);
+                walls.bounds_high = vmax(walls.bounds_high, c.high);
+            }
+        }
+    }
+
+    uint32_t add_wall_points(const std::vector<Vec>& points) {
+        uint32_t id = walls.next++;
+        for (auto& p : points) {
+            walls.positions.push_back(p);
+            walls.owners.push_back(id);
+        }
+        settle_walls();
+        return id;
+    }
+
+    Key cell_of(Vec p) const {
+        Vec c = p / radius();
+        return Key{sat_i32(std::floor(c.x)), sat_i32(std::floor(c.y)), sat_i32(std::floor(c.z))};
+    }
+
+    // boundary.rs:155-178: by cell, owner, position bits, then index.
+    void settle_walls() {
+        size_t n = walls.positions.size();
+        struct WK {
+            Key cell;
+            uint32_t owner;
+            uint64_t bx, by, bz;
+            size_t index;
+        };
+        std::vector<WK> order(n);
+        for (size_t i = 0; i < n; ++i) {
+            Vec p = walls.positions[i];
+            order[i] = WK{cell_of(p), walls.owners[i], bits_of(p.x), bits_of(p.y), bits_of(p.z), i};
+        }
+        std::sort(order.begin(), order.end(), [](const WK& a, const WK& b) {
+            return std::tie(a.cell.x, a.cell.y, a.cell.z, a.owner, a.bx, a.by, a.bz, a.index) <
+                   std::tie(b.cell.x, b.cell.y, b.cell.z, b.owner, b.bx, b.by, b.bz, b.index);
+        });
+        std::vector<Vec> pos(n);
+        std::vector<uint32_t> own(n);
+        std::vector<Key> keys(n);
+        for (size_t i = 0; i < n; ++i) {
+            pos[i] = walls.positions[order[i].index];
+            own[i] = order[i].owner;
+            keys[i] = order[i].cell;
+        }
+        walls.positions = std::move(pos);
+        walls.owners = std::move(own);
+        walls.grid = Grid::build(keys);
+    }
+
+    // mod.rs:264-277: indexes within `reach` of `at`, in range order.
+    static void near(const std::vector<Vec>& pts, const std::vector<Range>& ranges, Vec at, R reach,
+                     std::vector<uint32_t>& out) {
+        for (const Range& r : ranges)
+            for (uint32_t other = r.begin; other < r.end; ++other)
+                if (length_squared(pts[other] - at) < reach) out.push_back(other);
+    }
+
+    // mod.rs:540-608
+    void update_neighbors() {
+        size_t n = len();
+        struct OK_ {
+            Key cell;
+            uint32_t id, index;
+        };
+        std::vector<OK_> order(n);
+        for (size_t i = 0; i < n; ++i) order[i] = OK_{cell_of(positions[i]), ids[i], uint32_t(i)};
+        std::sort(order.begin(), order.end(), [](const OK_& a, const OK_& b) {
+            return std::tie(a.cell.x, a.cell.y, a.cell.z, a.id, a.index) <
+                   std::tie(b.cell.x, b.cell.y, b.cell.z, b.id, b.index);
+        });
+        std::vector<uint32_t> nid(n);
+        std::vector<Vec> np(n), nv(n);
+        std::vector<R> nd(n);
+        std::vector<Key> keys(n);
+        for (size_t i = 0; i < n; ++i) {
+            uint32_t k = order[i].index;
+            nid[i] = ids[k];
+            np[i] = positions[k];
+            nv[i] = velocities[k];
+            nd[i] = densities[k];
+            keys[i] = order[i].cell;
+        }
+        ids = std::move(nid);
+        positions = std::move(np);
+        velocities = std::move(nv);
+        densities = std::move(nd);
+        grid = Grid::build(keys);
+
+        R reach = pow2(radius());
+        std::vector<uint32_t> fcount(n), wcount(n);
+        // lists are formed per particle; joining them in particle order is the chunked join of
+        // mod.rs:294-307 without the chunk boundaries, which do not change the result
+        std::vector<std::vector<uint32_t>> fparts, wparts;
+        const size_t chunk = 512;
+        size_t jobs = (n + chunk - 1) / chunk;
+        fparts.resize(jobs);
+        wparts.resize(jobs);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads())
+        for (long long job = 0; job < (long long)jobs; ++job) {
+            std::vector<Range> af, aw;
+            bool have = false;
+            Key last{0, 0, 0};
+            size_t b = size_t(job) * chunk, e = std::min(n, b + chunk);
+            for (size_t i = b; i < e; ++i) {
+                Vec at = positions[i];
+                Key c = cell_of(at);
+                if (!have || c != last) {
+                    have = true;
+                    last = c;
+                    grid.around(c, af);
+                    walls.grid.around(c, aw);
+                }
+                size_t bf = fparts[job].size(), bw = wparts[job].size();
+                near(positions, af, at, reach, fparts[job]);
+                near(walls.positions, aw, at, reach, wparts[job]);
+                fcount[i] = uint32_t(fparts[job].size() - bf);
+                wcount[i] = uint32_t(wparts[job].size() - bw);
+            }
+        }
+        join(fcount, fparts, neighbors);
+        join(wcount, wparts, wall_neighbors);
+    }
+
+    static void join(const std::vector<uint32_t>& counts, std::vector<std::vector<uint32_t>>& parts, Lists& out) {
+        out.start.assign(counts.size() + 1, 0);
+        for (size_t i = 0; i < counts.size(); ++i) out.start[i + 1] = out.start[i] + counts[i];
+        out.items.clear();
+        out.items.reserve(out.start.back());
+        for (auto& p : parts) out.items.insert(out.items.end(), p.begin(), p.end());
+    }
+
+    int nthreads() const {
+#ifdef _OPENMP
+        return threads > 0 ? threads : omp_get_max_threads();
+#else
+        return 1;
+#endif
+    }
+
+    // mod.rs:621-675
+    Status compute_densities() {
+        if (neighbors.start.size() != len() + 1) return OUT_OF_RANGE;
+        size_t n = len();
+        std::vector<R> out(n);
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            size_t i = size_t(ii);
+            Vec at = positions[i];
+            R sum = R(0);
+            for (uint32_t k = neighbors.start[i]; k < neighbors.start[i + 1]; ++k)
+                sum += kernel.value(length(positions[neighbors.items[k]] - at));
+            R wsum = R(0);
+            for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
+                wsum += kernel.value(length(walls.positions[wall_neighbors.items[k]] - at));
+            out[i] = mass * (sum + wsum);
+        }
+        densities = std::move(out);
+        return OK;
+    }
+
+    // mod.rs:677-691
+    uint64_t state_hash() const {
+        std::vector<size_t> order(len());
+        std::iota(order.begin(), order.end(), size_t(0));
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return ids[a] < ids[b]; });
+        std::vector<uint8_t> bytes;
+        bytes.reserve(len() * 28);
+        auto put32 = [&](uint32_t v) {
+            for (int s = 0; s < 4; ++s) bytes.push_back(uint8_t(v >> (8 * s)));
+        };
+        for (size_t i : order) {
+            put32(ids[i]);
+            for (const Vec& v : {positions[i], velocities[i]}) {
+                // the hash is of f32 bits; the double oracle hashes its values rounded to f32
+                put32(uint32_t(bits_of(float(v.x))));
+                put32(uint32_t(bits_of(float(v.y))));
+                put32(uint32_t(bits_of(float(v.z))));
+            }
+        }
+        return fnv1a(bytes.data(), bytes.size());
+    }
+
+    // step.rs:92-96
+    R fastest() const {
+        R most = R(0);
+        for (auto& v : velocities) most = rmax(most, length(v));
+        return most;
+    }
+
+    // step.rs:58-90
+    Status step(R dt, Report& report) {
+        report = Report();
+        if (!std::isfinite(dt) || dt < R(0)) return NON_FINITE;
+        if (dt == R(0)) return OK;
+        if (len() > 0) {
+            Status st = settings.solver == 0 ? wcsph(dt, report) : dfsph(dt, report);
+            if (st != OK) return st;
+        }
+        report.lost = keep_in_domain();
+        report.max_speed = float(fastest());
+        R rest = R(settings.rest_density);
+        R most = R(0);
+        for (auto d : densities) most = rmax(most, d / rest - R(1));
+        report.max_compression = float(most);
+        return OK;
+    }
+
+    // step.rs:102-116 (no coupled bodies: the sound speed stays the configured one)
+    Status wcsph(R dt, Report& report) {
+        report.sound_speed = settings.sound_speed;
+        return wcsph_steps(dt, report);
+    }
+
+    // step.rs:118-142
+    Status wcsph_steps(R dt, Report& report) {
+        R fast = fastest();
+        R largest = R(settings.courant) * radius() / (R(settings.sound_speed) + fast);
+        R wanted = rmax(std::ceil(dt / largest), R(1));
+        R cap = R(float(settings.max_substeps));
+        uint32_t substeps = uint32_t(rmin(wanted, cap));
+        report.capped = wanted > cap;
+        R small = dt / R(float(substeps));
+        for (uint32_t i = 0; i < substeps; ++i) {
+            uint32_t held = 0;
+            Status st = wcsph_substep(small, held);
+            if (st != OK) return st;
+            report.held_back += held;
+        }
+        report.substeps = substeps;
+        return OK;
+    }
+
+    // step.rs:254-259
+    R viscosity(R dt) const {
+        R r = radius();
+        return rmin(R(settings.viscosity) * R(settings.sound_speed) * r, R(0.05f) * r * r / dt);
+    }
+
+    // step.rs:262-301 (no terrains)
+    Vec wall_viscous(size_t index, R dt) const {
+        R r = radius();
+        R soften = R(0.01f) * r * r;
+        R stable = r * r / dt;
+        Vec at = positions[index];
+        Vec velocity = velocities[index];
+        R density = densities[index];
+        Vec push;
+        Vec away;
+        for (uint32_t k = wall_neighbors.start[index]; k < wall_neighbors.start[index + 1]; ++k)
+            away = away + (-kernel.gradient(at - walls.positions[wall_neighbors.items[k]]));
+        Vec normal = normalize_or(away, Vec());
+        Vec into = normal * rmin(dot(velocity, normal), R(0));
+        R wall_visc = rmin(R(1) * R(settings.sound_speed) * r, R(0.25f) * stable);
+        for (uint32_t k = wall_neighbors.start[index]; k < wall_neighbors.start[index + 1]; ++k) {
+            Vec offset = at - walls.positions[wall_neighbors.items[k]];
+            R toward = dot(into, offset);
+            if (toward < R(0)) {
+                R squeeze = toward / (length_squared(offset) + soften);
+                R damp = -wall_visc * squeeze / density;
+                push = push - kernel.gradient(offset) * (mass * damp);
+            }
+        }
+        return push;
+    }
+
+    // step.rs:229-251
+    Vec viscous(size_t index, R dt) const {
+        R r = radius();
+        R soften = R(0.01f) * r * r;
+        R visc = viscosity(dt);
+        Vec at = positions[index];
+        Vec velocity = velocities[index];
+        R density = densities[index];
+        Vec push;
+        for (uint32_t k = neighbors.start[index]; k < neighbors.start[index + 1]; ++k) {
+            uint32_t other = neighbors.items[k];
+            if (other == index) continue;
+            Vec offset = at - positions[other];
+            R toward = dot(velocity - velocities[other], offset);
+            if (toward < R(0)) {
+                R squeeze = toward / (length_squared(offset) + soften);
+                R damp = -visc * squeeze * R(2) / (density + densities[other]);
+                push = push - kernel.gradient(offset) * (mass * damp);
+            }
+        }
+        return push + wall_viscous(index, dt);
+    }
+
+    // step.rs:144-224
+    Status wcsph_substep(R dt, uint32_t& held) {
+        update_neighbors();
+        Status st = compute_densities();
+        if (st != OK) return st;
+        size_t n = len();
+        R rest = R(settings.rest_density);
+        R stiffness = rest * pow2(R(settings.sound_speed)) / R(7);
+        std::vector<R> pressures(n), scaled(n);
+        for (size_t i = 0; i < n; ++i) {
+            R ratio = rmin(densities[i] / rest, R(1.1f));
+            pressures[i] = rmax(stiffness * (pow7(ratio) - R(1)), R(0));
+        }
+        for (size_t i = 0; i < n; ++i) scaled[i] = pressures[i] / (densities[i] * densities[i]);
+        R r = radius();
+        R soften = R(0.01f) * r * r;
+        R visc = viscosity(dt);
+        Vec g = gravity();
+        std::vector<Vec> pushes(n);
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            size_t i = size_t(ii);
+            Vec at = positions[i];
+            Vec velocity = velocities[i];
+            R density = densities[i];
+            R own = scaled[i];
+            Vec push;
+            for (uint32_t k = neighbors.start[i]; k < neighbors.start[i + 1]; ++k) {
+                uint32_t other = neighbors.items[k];
+                Vec offset = at - positions[other];
+                R squared = length_squared(offset);
+                if (squared <= R(0)) continue;
+                R distance = std::sqrt(squared);
+                Vec gradient = offset * (kernel.slope(distance) / distance);
+                R toward = rmin(dot(velocity - velocities[other], offset), R(0));
+                R damp = -visc * toward / (squared + soften) * R(2) / (density + densities[other]);
+                push = push - gradient * (mass * (own + scaled[other] + damp));
+            }
+            R mirrored = own + pressures[i] / (rest * rest);
+            for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k) {
+                Vec offset = at - walls.positions[wall_neighbors.items[k]];
+                push = push - kernel.gradient(offset) * (mass * mirrored);
+            }
+            pushes[i] = push + wall_viscous(i, dt) + g;
+        }
+        for (size_t i = 0; i < n; ++i) velocities[i] = velocities[i] + pushes[i] * dt;
+        return advance(dt, held);
+    }
+
+    // step.rs:305-339 (no terrains).  A non-finite particle stops the pass there, as in the
+    // reference; earlier particles have moved.
+    Status advance(R dt, uint32_t& held) {
+        held = 0;
+        Vec rest = Vec::splat(R(settings.spacing) / R(2));
+        for (size_t i = 0; i < len(); ++i) {
+            Vec& at = positions[i];
+            Vec& velocity = velocities[i];
+            Vec next = at + velocity * dt;
+            if (walls.has_bounds) {
+                Vec low = walls.bounds_low, high = walls.bounds_high;
+                Vec inside = clamp(next, low + rest, high - rest);
+                if (inside != next) {
+                    if (clamp(next, low, high) != next) held += 1;
+                    if (inside.x != next.x) velocity.x = R(0);
+                    if (inside.y != next.y) velocity.y = R(0);
+                    if (inside.z != next.z) velocity.z = R(0);
+                    next = inside;
+                }
+            }
+            if (!is_finite(next) || !is_finite(velocity)) return NON_FINITE;
+            at = next;
+        }
+        return OK;
+    }
+
+    // ---- DFSPH (dfsph.rs) ----------------------------------------------------------------
+
+    // dfsph.rs:46-77
+    Status dfsph(R dt, Report& report) {
+        R spacing = R(settings.spacing);
+        R courant = R(settings.courant);
+        R pull = length(gravity());
+        R left = dt;
+        while (left > R(0)) {
+            R small = courant * spacing / rmax(fastest(), R(1e-6f));
+            if (pull > R(0)) small = rmin(small, std::sqrt(R(2) * courant * spacing / pull));
+            if (report.substeps + 1 >= settings.max_substeps && small < left) {
+                report.capped = 1;
+                small = left;
+            }
+            small = rmin(small, left);
+            uint32_t held = 0, iterations = 0;
+            Status st = dfsph_substep(small, held, iterations);
+            if (st != OK) return st;
+            report.iterations += iterations;
+            report.held_back += held;
+            report.substeps += 1;
+            left -= small;
+        }
+        return OK;
+    }
+
+    // dfsph.rs:108-136
+    void gradients() {
+        grad_fluid.resize(neighbors.items.size());
+        grad_walls.resize(wall_neighbors.items.size());
+        size_t n = len();
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            size_t i = size_t(ii);
+            Vec at = positions[i];
+            for (uint32_t k = neighbors.start[i]; k < neighbors.start[i + 1]; ++k)
+                grad_fluid[k] = kernel.gradient(at - positions[neighbors.items[k]]);
+            for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
+                grad_walls[k] = kernel.gradient(at - walls.positions[wall_neighbors.items[k]]);
+        }
+    }
+
+    // dfsph.rs:138-163
+    std::vector<R> factors() const {
+        size_t n = len();
+        std::vector<R> out(n);
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            size_t i = size_t(ii);
+            Vec sum;
+            R squares = R(0);
+            for (uint32_t k = neighbors.start[i]; k < neighbors.start[i + 1]; ++k) {
+                Vec part = grad_fluid[k] * mass;
+                sum = sum + part;
+                squares += length_squared(part);
+            }
+            for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
+                sum = sum + grad_walls[k] * mass;
+            R total = length_squared(sum) + squares;
+            out[i] = total > R(0) ? R(1) / total : R(0);
+        }
+        return out;
+    }
+
+    // dfsph.rs:166-181
+    R density_rate(size_t i) const {
+        Vec velocity = velocities[i];
+        R rate = R(0);
+        for (uint32_t k = neighbors.start[i]; k < neighbors.start[i + 1]; ++k)
+            rate += dot(velocity - velocities[neighbors.items[k]], grad_fluid[k]);
+        for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
+            rate += dot(velocity, grad_walls[k]);
+        return rate * mass;
+    }
+
+    // dfsph.rs:184-216
+    void push_apart(const std::vector<R>& stiffness, R dt) {
+        size_t n = len();
+        std::vector<Vec> changes(n);
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            size_t i = size_t(ii);
+            R own = stiffness[i];
+            Vec change;
+            for (uint32_t k = neighbors.start[i]; k < neighbors.start[i + 1]; ++k)
+                change = change - grad_fluid[k] * (mass * (own + stiffness[neighbors.items[k]]));
+            for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
+                change = change - grad_walls[k] * (mass * own);
+            changes[i] = change * dt;
+        }
+        for (size_t i = 0; i < n; ++i) velocities[i] = velocities[i] + changes[i];
+    }
+
+    // dfsph.rs:222-275; solve 0 = divergence, 1 = density
+    uint32_t solve(int which, R dt, const std::vector<R>& alpha) {
+        R rest = R(settings.rest_density);
+        size_t n = len();
+        R tolerance = which == 0 ? R(settings.divergence_tolerance) : R(settings.density_tolerance);
+        uint32_t iterations = 0;
+        std::vector<R> stiffness(n), errors(n);
+        for (;;) {
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+            for (long long ii = 0; ii < (long long)n; ++ii) {
+                size_t i = size_t(ii);
+                R rate = density_rate(i);
+                R target, error;
+                if (which == 1) {
+                    R over = rmax(densities[i] + dt * rate - rest, R(0));
+                    target = over / (dt * dt);
+                    error = over / rest;
+                } else {
+                    size_t crowd = neighbors.count(i) + wall_neighbors.count(i);
+                    R r = crowd < 20 ? R(0) : rmax(rate, R(0));
+                    target = r / dt;
+                    error = dt * r / rest;
+                }
+                stiffness[i] = target * alpha[i];
+                errors[i] = error;
+            }
+            size_t loaded = 0;
+            for (auto e : errors) loaded += e > R(0) ? 1 : 0;
+            if (loaded == 0) loaded = 1;
+            bool settled;
+            if (settings.residual_sum == 0) {
+                R sum = R(0);
+                for (auto e : errors) sum += e;
+                R average = sum / R(float(loaded));
+                settled = iterations >= settings.min_iterations && average <= tolerance;
+            } else {
+                CompensatedSum acc;
+                for (auto e : errors) acc.add(double(e));
+                double average = acc.value() / double(loaded);
+                settled = iterations >= settings.min_iterations && average <= double(tolerance);
+            }
+            if (settled || iterations >= settings.max_iterations) return iterations;
+            push_apart(stiffness, dt);
+            iterations += 1;
+        }
+    }
+
+    // dfsph.rs:79-103
+    Status dfsph_substep(R dt, uint32_t& held, uint32_t& iterations) {
+        update_neighbors();
+        Status st = compute_densities();
+        if (st != OK) return st;
+        gradients();
+        std::vector<R> alpha = factors();
+        last_iterations[0] = solve(0, dt, alpha);
+        iterations = last_iterations[0];
+        size_t n = len();
+        Vec g = gravity();
+        std::vector<Vec> pushes(n);
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) pushes[size_t(ii)] = viscous(size_t(ii), dt) + g;
+        for (size_t i = 0; i < n; ++i) velocities[i] = velocities[i] + pushes[i] * dt;
+        last_iterations[1] = solve(1, dt, alpha);
+        iterations += last_iterations[1];
+        return advance(dt, held);
+    }
+};
+
+}  // namespace oracle

@@ -1,0 +1,339 @@
+// oracle_capi.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// C entry points over the CPU restatement in fluid_oracle.hpp, loaded with ctypes by the tests
+// and by bench.py's CPU baseline.  The names mirror include/solunar_fluid.h with an `orc_`
+// prefix; a handle holds either the float (parity) or the double (precision) restatement.
+// Vectors come in as f32 (the library's input type) and go out as f64, which holds either
+// precision exactly.
+#include <cstdint>
+#include <cstring>
+#include <memory>
+
+#include "../include/solunar_fluid.h"
+#include "fluid_oracle.hpp"
+
+using namespace oracle;
+
+namespace {
+
+struct Handle {
+    int precision = 32;
+    World<float> f;
+    World<double> d;
+};
+
+Settings from_c(const slf_settings* s, int residual_sum) {
+    Settings o;
+    o.solver = s->solver;
+    o.spacing = s->spacing;
+    o.rest_density = s->rest_density;
+    o.support = s->support;
+    o.max_particles = s->max_particles;
+    o.sound_speed = s->sound_speed;
+    o.viscosity = s->viscosity;
+    o.gravity[0] = s->gravity[0];
+    o.gravity[1] = s->gravity[1];
+    o.gravity[2] = s->gravity[2];
+    o.courant = s->courant;
+    o.max_substeps = s->max_substeps;
+    o.divergence_tolerance = s->divergence_tolerance;
+    o.density_tolerance = s->density_tolerance;
+    o.min_iterations = s->min_iterations;
+    o.max_iterations = s->max_iterations;
+    o.residual_sum = residual_sum;
+    return o;
+}
+
+template <class R> V3<R> v3(const float* p) { return V3<R>(R(p[0]), R(p[1]), R(p[2])); }
+
+void to_report(const Report& r, slf_report* out) {
+    if (!out) return;
+    out->substeps = r.substeps;
+    out->capped = r.capped;
+    out->max_compression = r.max_compression;
+    out->max_speed = r.max_speed;
+    out->held_back = r.held_back;
+    out->iterations = r.iterations;
+    out->emitted = r.emitted;
+    out->drained = r.drained;
+    out->lost = r.lost;
+    out->sound_speed = r.sound_speed;
+}
+
+template <class R> int32_t read_lists(const Lists& l, uint32_t* start, uint64_t start_len, uint32_t* items,
+                                      uint64_t cap, uint64_t* len) {
+    if (len) *len = l.items.size();
+    if (start) {
+        if (start_len != l.start.size()) return INVALID_ARGUMENT;
+        std::memcpy(start, l.start.data(), l.start.size() * 4);
+    }
+    if (items) {
+        if (cap < l.items.size()) return INVALID_ARGUMENT;
+        std::memcpy(items, l.items.data(), l.items.size() * 4);
+    }
+    return OK;
+}
+
+}  // namespace
+
+#define ORC_DISPATCH(h, ...)                \
+    do {                                    \
+        if ((h)->precision == 32) {         \
+            auto& w = (h)->f;               \
+            using R = float;                \
+            (void)sizeof(R);                \
+            __VA_ARGS__;                    \
+        } else {                            \
+            auto& w = (h)->d;               \
+            using R = double;               \
+            (void)sizeof(R);                \
+            __VA_ARGS__;                    \
+        }                                   \
+    } while (0)
+
+extern "C" {
+
+int32_t orc_create(const slf_settings* s, int32_t precision, int32_t residual_sum, void** out) {
+    if (!s || !out) return INVALID_ARGUMENT;
+    auto h = std::make_unique<Handle>();
+    h->precision = precision == 64 ? 64 : 32;
+    Settings o = from_c(s, residual_sum);
+    Status st = h->precision == 32 ? World<float>::create(o, h->f) : World<double>::create(o, h->d);
+    if (st != OK) return st;
+    *out = h.release();
+    return OK;
+}
+
+void orc_destroy(void* p) { delete static_cast<Handle*>(p); }
+
+int32_t orc_set_threads(void* p, int32_t threads) {
+    auto* h = static_cast<Handle*>(p);
+    h->f.threads = threads;
+    h->d.threads = threads;
+    return OK;
+}
+
+int32_t orc_len(void* p, uint64_t* out) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, *out = w.len());
+    return OK;
+}
+
+int32_t orc_particle_mass(void* p, double* out) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, *out = double(w.mass));
+    return OK;
+}
+
+int32_t orc_kernel(void* p, double* radius, double* scale) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, (*radius = double(w.kernel.radius), *scale = double(w.kernel.scale)));
+    return OK;
+}
+
+int32_t orc_add_particles(void* p, uint64_t n, const float* pos, const float* vel, uint32_t* ids) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, {
+        for (uint64_t i = 0; i < n && st == OK; ++i)
+            st = w.add_particle(v3<R>(pos + 3 * i), v3<R>(vel + 3 * i), ids ? ids + i : nullptr);
+    });
+    return st;
+}
+
+int32_t orc_fill_box(void* p, const float* low, const float* high, uint64_t* count) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.fill_box(v3<R>(low), v3<R>(high), count));
+    return st;
+}
+
+int32_t orc_set_domain(void* p, const float* low, const float* high) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, {
+        if (low && high) {
+            auto a = v3<R>(low), b = v3<R>(high);
+            st = w.set_domain(&a, &b);
+        } else {
+            st = w.set_domain(nullptr, nullptr);
+        }
+    });
+    return st;
+}
+
+int32_t orc_add_box_container(void* p, const float* low, const float* high, uint32_t* id) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.add_box_container(v3<R>(low), v3<R>(high), id));
+    return st;
+}
+
+int32_t orc_add_wall(void* p, const float* low, const float* high, uint32_t* id) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.add_wall(v3<R>(low), v3<R>(high), id));
+    return st;
+}
+
+int32_t orc_remove_boundary(void* p, uint32_t id, int32_t* removed) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, *removed = w.remove_boundary(id) ? 1 : 0);
+    return OK;
+}
+
+int32_t orc_wall_count(void* p, uint64_t* out) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, *out = w.walls.positions.size());
+    return OK;
+}
+
+int32_t orc_read_wall_positions(void* p, double* out, uint64_t n) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, {
+        if (n != w.walls.positions.size()) {
+            st = INVALID_ARGUMENT;
+        } else {
+            for (uint64_t i = 0; i < n; ++i) {
+                out[3 * i] = double(w.walls.positions[i].x);
+                out[3 * i + 1] = double(w.walls.positions[i].y);
+                out[3 * i + 2] = double(w.walls.positions[i].z);
+            }
+        }
+    });
+    return st;
+}
+
+int32_t orc_step(void* p, float dt, slf_report* out) {
+    auto* h = static_cast<Handle*>(p);
+    Report r;
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.step(R(dt), r));
+    to_report(r, out);
+    return st;
+}
+
+int32_t orc_update_neighbors(void* p) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, w.update_neighbors());
+    return OK;
+}
+
+int32_t orc_compute_densities(void* p) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.compute_densities());
+    return st;
+}
+
+int32_t orc_read_ids(void* p, uint32_t* out, uint64_t n) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, {
+        if (n != w.len()) st = INVALID_ARGUMENT;
+        else std::memcpy(out, w.ids.data(), n * 4);
+    });
+    return st;
+}
+
+static int32_t read_vecs(Handle* h, int which, double* out, uint64_t n) {
+    int32_t st = OK;
+    ORC_DISPATCH(h, {
+        const auto& src = which == 0 ? w.positions : w.velocities;
+        if (n != src.size()) {
+            st = INVALID_ARGUMENT;
+        } else {
+            for (uint64_t i = 0; i < n; ++i) {
+                out[3 * i] = double(src[i].x);
+                out[3 * i + 1] = double(src[i].y);
+                out[3 * i + 2] = double(src[i].z);
+            }
+        }
+    });
+    return st;
+}
+
+int32_t orc_read_positions(void* p, double* out, uint64_t n) { return read_vecs(static_cast<Handle*>(p), 0, out, n); }
+int32_t orc_read_velocities(void* p, double* out, uint64_t n) { return read_vecs(static_cast<Handle*>(p), 1, out, n); }
+
+int32_t orc_read_densities(void* p, double* out, uint64_t n) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, {
+        if (n != w.len()) st = INVALID_ARGUMENT;
+        else
+            for (uint64_t i = 0; i < n; ++i) out[i] = double(w.densities[i]);
+    });
+    return st;
+}
+
+int32_t orc_neighbor_lists(void* p, uint32_t* start, uint64_t start_len, uint32_t* items, uint64_t cap,
+                           uint64_t* len) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = read_lists<R>(w.neighbors, start, start_len, items, cap, len));
+    return st;
+}
+
+int32_t orc_wall_neighbor_lists(void* p, uint32_t* start, uint64_t start_len, uint32_t* items, uint64_t cap,
+                                uint64_t* len) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = read_lists<R>(w.wall_neighbors, start, start_len, items, cap, len));
+    return st;
+}
+
+int32_t orc_state_hash(void* p, uint64_t* out) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, *out = w.state_hash());
+    return OK;
+}
+
+int32_t orc_last_iterations(void* p, uint32_t* out) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, (out[0] = w.last_iterations[0], out[1] = w.last_iterations[1]));
+    return OK;
+}
+
+// Kernel::value / slope / gradient of a kernel with this radius (mod.rs:125-165), float.
+int32_t orc_kernel_eval_f32(float radius, uint64_t n, const float* offsets, float* value, float* slope,
+                            float* gradient) {
+    Kernel<float> k(radius);
+    for (uint64_t i = 0; i < n; ++i) {
+        V3<float> o(offsets[3 * i], offsets[3 * i + 1], offsets[3 * i + 2]);
+        float d = length(o);
+        value[i] = k.value(d);
+        slope[i] = k.slope(d);
+        V3<float> g = k.gradient(o);
+        gradient[3 * i] = g.x;
+        gradient[3 * i + 1] = g.y;
+        gradient[3 * i + 2] = g.z;
+    }
+    return OK;
+}
+
+// Grid::build over sorted keys, then Grid::range for each query (mod.rs:169-247).
+// out[2*i], out[2*i+1] = range, or UINT32_MAX twice when the cell is absent.  force_search
+// drops the dense table.  *dense_out tells whether a dense table was built.
+int32_t orc_grid_ranges(const int32_t* keys, uint64_t n, const int32_t* queries, uint64_t nq, int32_t force_search,
+                        uint32_t* out, int32_t* dense_out) {
+    std::vector<Key> k(n);
+    for (uint64_t i = 0; i < n; ++i) k[i] = Key{keys[3 * i], keys[3 * i + 1], keys[3 * i + 2]};
+    Grid g = Grid::build(k);
+    if (dense_out) *dense_out = g.dense.empty() ? 0 : 1;
+    if (force_search) g.dense.clear();
+    for (uint64_t i = 0; i < nq; ++i) {
+        Range r;
+        if (g.range(Key{queries[3 * i], queries[3 * i + 1], queries[3 * i + 2]}, r)) {
+            out[2 * i] = r.begin;
+            out[2 * i + 1] = r.end;
+        } else {
+            out[2 * i] = UINT32_MAX;
+            out[2 * i + 1] = UINT32_MAX;
+        }
+    }
+    return OK;
+}
+
+}  // extern "C"

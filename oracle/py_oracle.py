@@ -1,0 +1,268 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes wrapper of the CPU restatement (oracle/liboracle_fluid.so).
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU baseline as the checker; the
+library never imports it.  `OracleWorld` has the method names of solunar_b200.FluidWorld so a
+parity test can drive both the same way.  `precision=32` is the float restatement of the
+reference (parity oracle), `precision=64` the double one (precision oracle).
+`residual_sum=0` sums the DFSPH solver error as the reference does (sequential, working
+precision, src/fluid/dfsph.rs:266-267); `residual_sum=1` takes a compensated sum in double, as
+the CUDA library does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from solunar_b200.abi import CReport, CSettings, FluidReport, FluidSettings, PhysicsError, vec3
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_fluid.so")
+
+_lib = None
+
+
+def build() -> str:
+    """Compiles the restatement with its Makefile (gcc, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        f3 = ctypes.POINTER(ctypes.c_float)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        dp = ctypes.POINTER(ctypes.c_double)
+        sig = {
+            "orc_create": [ctypes.POINTER(CSettings), ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(vp)],
+            "orc_set_threads": [vp, ctypes.c_int32],
+            "orc_len": [vp, u64p],
+            "orc_particle_mass": [vp, dp],
+            "orc_kernel": [vp, dp, dp],
+            "orc_add_particles": [vp, ctypes.c_uint64, f3, f3, u32p],
+            "orc_fill_box": [vp, f3, f3, u64p],
+            "orc_set_domain": [vp, f3, f3],
+            "orc_add_box_container": [vp, f3, f3, u32p],
+            "orc_add_wall": [vp, f3, f3, u32p],
+            "orc_remove_boundary": [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32)],
+            "orc_wall_count": [vp, u64p],
+            "orc_read_wall_positions": [vp, dp, ctypes.c_uint64],
+            "orc_step": [vp, ctypes.c_float, ctypes.POINTER(CReport)],
+            "orc_update_neighbors": [vp],
+            "orc_compute_densities": [vp],
+            "orc_read_ids": [vp, u32p, ctypes.c_uint64],
+            "orc_read_positions": [vp, dp, ctypes.c_uint64],
+            "orc_read_velocities": [vp, dp, ctypes.c_uint64],
+            "orc_read_densities": [vp, dp, ctypes.c_uint64],
+            "orc_neighbor_lists": [vp, u32p, ctypes.c_uint64, u32p, ctypes.c_uint64, u64p],
+            "orc_wall_neighbor_lists": [vp, u32p, ctypes.c_uint64, u32p, ctypes.c_uint64, u64p],
+            "orc_state_hash": [vp, u64p],
+            "orc_last_iterations": [vp, u32p],
+            "orc_kernel_eval_f32": [ctypes.c_float, ctypes.c_uint64, f3, f3, f3, f3],
+            "orc_grid_ranges": [ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32),
+                                ctypes.c_uint64, ctypes.c_int32, u32p, ctypes.POINTER(ctypes.c_int32)],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int32
+        L.orc_destroy.argtypes = [vp]
+        L.orc_destroy.restype = None
+        _lib = L
+    return _lib
+
+
+def _check(code: int):
+    if code != 0:
+        raise PhysicsError(code)
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+class OracleWorld:
+    """FluidWorld (src/fluid/mod.rs:310-339) restated on the CPU."""
+
+    def __init__(self, settings: FluidSettings | None = None, precision: int = 32, residual_sum: int = 0,
+                 threads: int = 0):
+        self._settings = settings or FluidSettings()
+        self.precision = precision
+        c = self._settings.to_c()
+        h = ctypes.c_void_p()
+        _check(lib().orc_create(ctypes.byref(c), precision, residual_sum, ctypes.byref(h)))
+        self._h = h
+        if threads:
+            lib().orc_set_threads(self._h, threads)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.orc_destroy(h)
+            self._h = None
+
+    # -- settings --
+    def settings(self) -> FluidSettings:
+        return self._settings
+
+    def set_threads(self, threads: int):
+        lib().orc_set_threads(self._h, threads)
+
+    def particle_mass(self) -> float:
+        v = ctypes.c_double()
+        lib().orc_particle_mass(self._h, ctypes.byref(v))
+        return v.value
+
+    def kernel(self):
+        r, s = ctypes.c_double(), ctypes.c_double()
+        lib().orc_kernel(self._h, ctypes.byref(r), ctypes.byref(s))
+        return r.value, s.value
+
+    def len(self) -> int:
+        v = ctypes.c_uint64()
+        lib().orc_len(self._h, ctypes.byref(v))
+        return v.value
+
+    __len__ = len
+
+    # -- particles and walls --
+    def add_particle(self, position, velocity) -> int:
+        return int(self.add_particles(np.asarray([position]), np.asarray([velocity]))[0])
+
+    def add_particles(self, positions, velocities=None) -> np.ndarray:
+        p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+        v = np.zeros_like(p) if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32).reshape(-1, 3)
+        ids = np.zeros(len(p), dtype=np.uint32)
+        _check(lib().orc_add_particles(self._h, len(p), _ptr(p, ctypes.c_float), _ptr(v, ctypes.c_float),
+                                       _ptr(ids, ctypes.c_uint32)))
+        return ids
+
+    def fill_box(self, low, high) -> int:
+        n = ctypes.c_uint64()
+        _check(lib().orc_fill_box(self._h, vec3(low), vec3(high), ctypes.byref(n)))
+        return n.value
+
+    def set_domain(self, domain):
+        if domain is None:
+            _check(lib().orc_set_domain(self._h, None, None))
+        else:
+            _check(lib().orc_set_domain(self._h, vec3(domain[0]), vec3(domain[1])))
+
+    def add_box_container(self, low, high) -> int:
+        i = ctypes.c_uint32()
+        _check(lib().orc_add_box_container(self._h, vec3(low), vec3(high), ctypes.byref(i)))
+        return i.value
+
+    def add_wall(self, low, high) -> int:
+        i = ctypes.c_uint32()
+        _check(lib().orc_add_wall(self._h, vec3(low), vec3(high), ctypes.byref(i)))
+        return i.value
+
+    def remove_boundary(self, boundary: int) -> bool:
+        r = ctypes.c_int32()
+        _check(lib().orc_remove_boundary(self._h, boundary, ctypes.byref(r)))
+        return bool(r.value)
+
+    def wall_positions(self) -> np.ndarray:
+        n = ctypes.c_uint64()
+        lib().orc_wall_count(self._h, ctypes.byref(n))
+        out = np.zeros((n.value, 3), dtype=np.float64)
+        _check(lib().orc_read_wall_positions(self._h, _ptr(out, ctypes.c_double), n.value))
+        return out
+
+    # -- stepping --
+    def step(self, dt: float) -> FluidReport:
+        r = CReport()
+        _check(lib().orc_step(self._h, dt, ctypes.byref(r)))
+        return FluidReport.from_c(r)
+
+    def update_neighbors(self):
+        _check(lib().orc_update_neighbors(self._h))
+
+    def compute_densities(self):
+        _check(lib().orc_compute_densities(self._h))
+
+    def last_iterations(self):
+        out = (ctypes.c_uint32 * 2)()
+        lib().orc_last_iterations(self._h, out)
+        return int(out[0]), int(out[1])
+
+    # -- read-outs --
+    def ids(self) -> np.ndarray:
+        n = self.len()
+        out = np.zeros(n, dtype=np.uint32)
+        _check(lib().orc_read_ids(self._h, _ptr(out, ctypes.c_uint32), n))
+        return out
+
+    def _vecs(self, fn) -> np.ndarray:
+        n = self.len()
+        out = np.zeros((n, 3), dtype=np.float64)
+        _check(fn(self._h, _ptr(out, ctypes.c_double), n))
+        return out
+
+    def positions(self) -> np.ndarray:
+        return self._vecs(lib().orc_read_positions)
+
+    def velocities(self) -> np.ndarray:
+        return self._vecs(lib().orc_read_velocities)
+
+    def densities(self) -> np.ndarray:
+        n = self.len()
+        out = np.zeros(n, dtype=np.float64)
+        _check(lib().orc_read_densities(self._h, _ptr(out, ctypes.c_double), n))
+        return out
+
+    def _lists(self, fn):
+        n = ctypes.c_uint64()
+        _check(fn(self._h, None, 0, None, 0, ctypes.byref(n)))
+        start = np.zeros(self.len() + 1, dtype=np.uint32)
+        items = np.zeros(max(n.value, 1), dtype=np.uint32)
+        _check(fn(self._h, _ptr(start, ctypes.c_uint32), len(start), _ptr(items, ctypes.c_uint32), n.value,
+                  ctypes.byref(n)))
+        return start, items[: n.value]
+
+    def neighbor_lists(self):
+        return self._lists(lib().orc_neighbor_lists)
+
+    def wall_neighbor_lists(self):
+        return self._lists(lib().orc_wall_neighbor_lists)
+
+    def neighbors_of(self, index: int) -> np.ndarray:
+        start, items = self.neighbor_lists()
+        return items[start[index]:start[index + 1]]
+
+    def state_hash(self) -> int:
+        v = ctypes.c_uint64()
+        lib().orc_state_hash(self._h, ctypes.byref(v))
+        return v.value
+
+
+def kernel_eval(radius: float, offsets) -> tuple:
+    """Kernel::value, slope and gradient (src/fluid/mod.rs:140-164) in f32 at these offsets."""
+    o = np.ascontiguousarray(offsets, dtype=np.float32).reshape(-1, 3)
+    n = len(o)
+    value = np.zeros(n, dtype=np.float32)
+    slope = np.zeros(n, dtype=np.float32)
+    grad = np.zeros((n, 3), dtype=np.float32)
+    lib().orc_kernel_eval_f32(radius, n, _ptr(o, ctypes.c_float), _ptr(value, ctypes.c_float),
+                              _ptr(slope, ctypes.c_float), _ptr(grad, ctypes.c_float))
+    return value, slope, grad
+
+
+def grid_ranges(sorted_keys, queries, force_search: bool):
+    """Grid::build then Grid::range (src/fluid/mod.rs:180-247).  Returns (ranges, had_dense)."""
+    k = np.ascontiguousarray(sorted_keys, dtype=np.int32).reshape(-1, 3)
+    q = np.ascontiguousarray(queries, dtype=np.int32).reshape(-1, 3)
+    out = np.zeros((len(q), 2), dtype=np.uint32)
+    dense = ctypes.c_int32()
+    lib().orc_grid_ranges(_ptr(k, ctypes.c_int32), len(k), _ptr(q, ctypes.c_int32), len(q),
+                          1 if force_search else 0, _ptr(out, ctypes.c_uint32), ctypes.byref(dense))
+    return out, bool(dense.value)

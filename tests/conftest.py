@@ -1,0 +1,35 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+REFERENCE = "/root/reference"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+    config.addinivalue_line("markers", "slow: takes more than a few seconds on the CPU")
+
+
+@pytest.fixture(scope="session")
+def oracle_lib():
+    from oracle import py_oracle
+
+    py_oracle.build()
+    return py_oracle
+
+
+@pytest.fixture(scope="session")
+def gpu_lib():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from solunar_b200 import fluid
+
+    fluid.load_library()
+    return fluid
