@@ -191,6 +191,17 @@ int32_t slf_state_hash(const slf_world* world, uint64_t* out);
 /* Message of the last failed call on any handle of this thread ("" if none). */
 const char* slf_last_error(void);
 
+/* ---- diagnostics and testing ------------------------------------------------------------ */
+
+/* DFSPH solver iterations of the last substep: divergence and density (the per-solve split of
+ * FluidReport::iterations, src/fluid/dfsph.rs:89,100). */
+int32_t slf_last_iterations(const slf_world* world, uint32_t* divergence, uint32_t* density);
+
+/* Fault injection, the counterpart of the reference's `SkipsJobs` test dispatcher
+ * (src/dispatch.rs:50-65): the next sort leaves the 512-particle job `job` undone, which the
+ * completeness check reports as SLF_ERR_DISPATCH_INCOMPLETE with the particles untouched. */
+int32_t slf_debug_skip_job(slf_world* world, int64_t job);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,183 @@
+// fluid_device.cuh -- device-side types and the per-pair arithmetic of the fluid step.
+//
+// Kernels in this library are compiled with -fmad=false and IEEE division and square root, so
+// that `a * b + c` rounds twice and every expression below rounds exactly as the reference's
+// scalar f32 code (src/fluid/mod.rs, step.rs, dfsph.rs) does.  The formulas keep the
+// reference's evaluation order; each cites the line it follows.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace slf {
+
+constexpr int kBlock = 256;           // threads per block of the per-particle kernels
+constexpr uint32_t kNoCell = 0xFFFFFFFFu;
+
+// ---- world constants, derived once from the settings on the host (in f32, reference order) --
+struct Params {
+    float spacing;
+    float radius;        // spacing * support (mod.rs:120-122)
+    float reach;         // radius.powi(2) (mod.rs:568)
+    float scale;         // 21 / (2 pi r^3) (mod.rs:136)
+    float mass;          // rest_mass (mod.rs:694-709)
+    float rest;          // rest_density
+    float rest_sq;       // rest * rest (step.rs:198)
+    float stiffness;     // rest * c^2 / 7 (step.rs:149)
+    float soften;        // 0.01 * r * r (step.rs:165)
+    float3 gravity;
+    int has_bounds;      // a container exists (boundary.rs:240-247)
+    float3 low, high;    // union of the containers
+    float3 low_in, high_in;  // low + spacing/2, high - spacing/2 (step.rs:308-312)
+    uint32_t n;          // particles
+    int solver;          // 0 WCSPH, 1 DFSPH
+    float div_tol, den_tol;
+    uint32_t min_iter, max_iter;
+};
+
+// Per-substep constants, in device memory so a captured substep reads the current ones.
+struct StepConsts {
+    float dt;
+    float viscosity;       // viscosity(dt) (step.rs:254-259)
+    float wall_viscosity;  // min(c r, 0.25 r^2 / dt) (step.rs:282-283)
+    float dt_sq;           // dt * dt (dfsph.rs:246)
+};
+
+// Written by the kernels, read back by the host after each substep.
+struct Status {
+    uint32_t nonfinite;    // advance found a non finite particle (step.rs:333-335)
+    uint32_t held;         // held_back of the substep (step.rs:314-316)
+    uint32_t vmax_bits;    // max |v| of the advanced state, f32 bits (non-negative)
+    uint32_t maxcomp_bits; // max(0, rho / rest - 1), f32 bits
+    int32_t cell_lo[3];    // bounding box of the advanced particles' cells
+    int32_t cell_hi[3];
+    uint32_t settled;      // the last solver check stopped the loop
+    uint32_t loaded;       // particles with error > 0 in the last check (dfsph.rs:266)
+    double average;        // last average error (dfsph.rs:267)
+    uint32_t processed;    // particles a neighbour pass visited (dispatch completeness)
+    uint32_t ticket;       // block counter of the last-block reduction
+    uint32_t pad[2];
+};
+
+// ---- cell tables ----------------------------------------------------------------------------
+// Dense: a start offset for every cell of a box, x-major like the reference's dense table
+// (mod.rs:218-223): range of cell c = [start[c], start[c + 1]).  Sorted: the occupied cells'
+// keys in key order with their starts, searched like the reference's fallback (mod.rs:231).
+struct GridDev {
+    int mode;              // 0 empty, 1 dense, 2 sorted
+    int lx, ly, lz;        // dense: lowest key
+    int sx, sy, sz;        // dense: cells per axis
+    uint32_t cells;        // sorted: occupied cells
+    const uint32_t* start; // dense: volume + 1; sorted: cells + 1
+    const int4* keys;      // sorted: key of each occupied cell
+
+#ifdef __CUDACC__
+    __device__ __forceinline__ bool range(long long cx, long long cy, long long cz, uint32_t& b,
+                                          uint32_t& e) const {
+        if (mode == 1) {
+            long long x = cx - lx, y = cy - ly, z = cz - lz;
+            if (x < 0 || x >= sx || y < 0 || y >= sy || z < 0 || z >= sz) return false;
+            long long c = (x * sy + y) * sz + z;
+            b = start[c];
+            e = start[c + 1];
+            return e > b;
+        }
+        if (mode == 2) {
+            if (cx > 2147483647LL || cx < -2147483648LL || cy > 2147483647LL || cy < -2147483648LL ||
+                cz > 2147483647LL || cz < -2147483648LL)
+                return false;
+            uint32_t lo = 0, hi = cells;
+            while (lo < hi) {
+                uint32_t mid = (lo + hi) >> 1;
+                int4 k = keys[mid];
+                bool less = k.x < cx || (k.x == cx && (k.y < cy || (k.y == cy && k.z < cz)));
+                if (less) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo == cells) return false;
+            int4 k = keys[lo];
+            if (k.x != cx || k.y != cy || k.z != cz) return false;
+            b = start[lo];
+            e = start[lo + 1];
+            return true;
+        }
+        return false;
+    }
+#endif
+};
+
+#ifdef __CUDACC__
+
+// ---- reference arithmetic (mod.rs:125-165, 526-533) ------------------------------------------
+
+__device__ __forceinline__ float pow3(float x) { return x * (x * x); }
+__device__ __forceinline__ float pow4(float x) { float s = x * x; return s * s; }
+__device__ __forceinline__ float pow7(float x) { float s = x * x; float q = s * s; return (x * s) * q; }
+
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return ax * bx + ay * by + az * bz;
+}
+
+// Kernel::value (mod.rs:140-146)
+__device__ __forceinline__ float kernel_value(const Params& p, float distance) {
+    float q = distance / p.radius;
+    if (q >= 1.0f) return 0.0f;
+    return p.scale * pow4(1.0f - q) * (1.0f + 4.0f * q);
+}
+
+// Kernel::slope (mod.rs:149-155)
+__device__ __forceinline__ float kernel_slope(const Params& p, float distance) {
+    float q = distance / p.radius;
+    if (q >= 1.0f) return 0.0f;
+    return p.scale * -20.0f * q * pow3(1.0f - q) / p.radius;
+}
+
+// Kernel::gradient (mod.rs:158-164): the factor g with gradient = offset * g.
+__device__ __forceinline__ float kernel_gradient_factor(const Params& p, float ox, float oy, float oz) {
+    float distance = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
+    if (distance <= 0.0f) return 0.0f;
+    return kernel_slope(p, distance) / distance;
+}
+
+// cell_of (mod.rs:526-533): floor(p / r) per axis, `as i32` (PTX float-to-int conversions
+// saturate and map NaN to zero, as Rust's does).
+__device__ __forceinline__ int3 cell_of(const Params& p, float x, float y, float z) {
+    return make_int3(__float2int_rz(floorf(x / p.radius)), __float2int_rz(floorf(y / p.radius)),
+                     __float2int_rz(floorf(z / p.radius)));
+}
+
+// Visit the points of `g` within reach of `at` in the reference's list order: the 27 cells
+// dz outer, dy, dx inner (mod.rs:250-261), each cell's points in array order, kept when
+// |p - at|^2 < reach strictly (mod.rs:264-277).
+template <class F>
+__device__ __forceinline__ void each_near(const Params& p, const GridDev& g, const float4* __restrict__ pts,
+                                          int3 cell, float ax, float ay, float az, F&& f) {
+    if (g.mode == 0) return;
+#pragma unroll 1
+    for (int dz = -1; dz <= 1; ++dz) {
+#pragma unroll 1
+        for (int dy = -1; dy <= 1; ++dy) {
+#pragma unroll 1
+            for (int dx = -1; dx <= 1; ++dx) {
+                uint32_t b, e;
+                if (!g.range((long long)cell.x + dx, (long long)cell.y + dy, (long long)cell.z + dz, b, e))
+                    continue;
+#pragma unroll 1
+                for (uint32_t j = b; j < e; ++j) {
+                    float4 q = __ldg(&pts[j]);
+                    float ox = q.x - ax, oy = q.y - ay, oz = q.z - az;
+                    if (dot3(ox, oy, oz, ox, oy, oz) < p.reach) f(j, q);
+                }
+            }
+        }
+    }
+}
+
+// f32 bits for atomicMax on non-negative floats.
+__device__ __forceinline__ void atomic_max_nonneg(uint32_t* addr, float v) {
+    if (v > 0.0f) atomicMax(addr, __float_as_uint(v));
+}
+
+#endif  // __CUDACC__
+
+}  // namespace slf

@@ -1,0 +1,816 @@
+// kernels.cu -- the fluid substep on the device.
+//
+// One thread per particle throughout.  Particles live in SoA float4 arrays (x, y, z, unused)
+// sorted by (cell, id) like the reference's arrays (src/fluid/mod.rs:540-566); every pass reads
+// neighbours through the cell tables in the reference's list order, so each particle's sums are
+// the reference's sequential sums, bit for bit.  Grid-wide reductions (bounding box, fastest
+// particle, solver residual) are block trees feeding one atomic or one last-block finish per
+// launch; the residual is summed in double-double (compensated), deterministically.
+#include <cfloat>
+#include <climits>
+
+#include "fluid_device.cuh"
+#include "launch.h"
+
+namespace slf {
+
+// ---- block reductions ---------------------------------------------------------------------
+
+template <class T, class Op>
+__device__ __forceinline__ T warp_reduce(T v, Op op) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Reduces one value per thread over the block; the result is valid in thread 0.
+template <class T, class Op>
+__device__ __forceinline__ T block_reduce(T v, Op op, T identity) {
+    __shared__ T warp_vals[kBlock / 32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_reduce(v, op);
+    __syncthreads();
+    if (lane == 0) warp_vals[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? warp_vals[lane] : identity;
+        v = warp_reduce(v, op);
+    }
+    return v;
+}
+
+struct MinI { __device__ int operator()(int a, int b) const { return a < b ? a : b; } };
+struct MaxI { __device__ int operator()(int a, int b) const { return a > b ? a : b; } };
+struct MaxU { __device__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; } };
+struct SumU { __device__ uint32_t operator()(uint32_t a, uint32_t b) const { return a + b; } };
+
+// Bounding box of cells, fastest speed, held-back count and non-finite flag of a block's
+// particles, folded into the status with one atomic each.
+__device__ __forceinline__ void fold_advance_stats(Status* st, bool valid, int3 c, float speed, uint32_t held,
+                                                   uint32_t bad) {
+    int lox = valid ? c.x : INT_MAX, loy = valid ? c.y : INT_MAX, loz = valid ? c.z : INT_MAX;
+    int hix = valid ? c.x : INT_MIN, hiy = valid ? c.y : INT_MIN, hiz = valid ? c.z : INT_MIN;
+    uint32_t sb = (valid && speed > 0.0f) ? __float_as_uint(speed) : 0u;
+    lox = block_reduce(lox, MinI(), INT_MAX);
+    loy = block_reduce(loy, MinI(), INT_MAX);
+    loz = block_reduce(loz, MinI(), INT_MAX);
+    hix = block_reduce(hix, MaxI(), INT_MIN);
+    hiy = block_reduce(hiy, MaxI(), INT_MIN);
+    hiz = block_reduce(hiz, MaxI(), INT_MIN);
+    sb = block_reduce(sb, MaxU(), 0u);
+    held = block_reduce(held, SumU(), 0u);
+    bad = block_reduce(bad, MaxU(), 0u);
+    if (threadIdx.x == 0) {
+        if (lox != INT_MAX) {
+            atomicMin(&st->cell_lo[0], lox);
+            atomicMin(&st->cell_lo[1], loy);
+            atomicMin(&st->cell_lo[2], loz);
+            atomicMax(&st->cell_hi[0], hix);
+            atomicMax(&st->cell_hi[1], hiy);
+            atomicMax(&st->cell_hi[2], hiz);
+        }
+        if (sb) atomicMax(&st->vmax_bits, sb);
+        if (held) atomicAdd(&st->held, held);
+        if (bad) atomicMax(&st->nonfinite, 1u);
+    }
+}
+
+// ---- bounding box and fastest speed of the current state ---------------------------------
+
+__global__ void k_state_stats(Params p, const float4* __restrict__ pos, const float4* __restrict__ vel,
+                              Status* st) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < p.n;
+    int3 c = make_int3(0, 0, 0);
+    float speed = 0.0f;
+    if (valid) {
+        float4 a = pos[i];
+        float4 v = vel[i];
+        c = cell_of(p, a.x, a.y, a.z);
+        // Vec3::length (step.rs:92-96)
+        speed = sqrtf(dot3(v.x, v.y, v.z, v.x, v.y, v.z));
+        if (!(speed == speed)) speed = 0.0f;  // f32::max ignores NaN
+    }
+    fold_advance_stats(st, valid, c, speed, 0u, 0u);
+}
+
+// max(0, rho / rest - 1) over the particles (step.rs:84-88)
+__global__ void k_max_compression(Params p, const float* __restrict__ rho, Status* st) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t b = 0;
+    if (i < p.n) {
+        float c = rho[i] / p.rest - 1.0f;
+        if (c > 0.0f) b = __float_as_uint(c);
+    }
+    b = block_reduce(b, MaxU(), 0u);
+    if (threadIdx.x == 0 && b) atomicMax(&st->maxcomp_bits, b);
+}
+
+// ---- spatial hash: counting sort by dense cell index, then id within each cell ------------
+
+__global__ void k_count_cells(Params p, const float4* __restrict__ pos, int3 low, int3 span, uint32_t* count,
+                              uint32_t* lin, uint32_t* slot) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float4 a = pos[i];
+    int3 c = cell_of(p, a.x, a.y, a.z);
+    long long x = (long long)c.x - low.x, y = (long long)c.y - low.y, z = (long long)c.z - low.z;
+    // the box was taken over these very positions; stay in bounds regardless
+    x = x < 0 ? 0 : (x >= span.x ? span.x - 1 : x);
+    y = y < 0 ? 0 : (y >= span.y ? span.y - 1 : y);
+    z = z < 0 ? 0 : (z >= span.z ? span.z - 1 : z);
+    uint32_t l = (uint32_t)((x * span.y + y) * span.z + z);
+    lin[i] = l;
+    slot[i] = atomicAdd(&count[l], 1u);
+}
+
+__global__ void k_scatter_members(uint32_t n, const uint32_t* __restrict__ lin, const uint32_t* __restrict__ slot,
+                                  const uint32_t* __restrict__ start, const uint32_t* __restrict__ ids,
+                                  uint32_t* members) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    members[start[lin[i]] + slot[i]] = ids[i];
+}
+
+// Final place = cell start + number of the cell's ids below this one's: the (cell, id) order
+// of mod.rs:550, whatever order the atomics handed out the slots in.
+__global__ void k_rank_reorder(uint32_t n, const uint32_t* __restrict__ lin, const uint32_t* __restrict__ start,
+                               const uint32_t* __restrict__ members, const uint32_t* __restrict__ ids_in,
+                               const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
+                               const float* __restrict__ rho_in, const float* __restrict__ kap_in,
+                               uint32_t* __restrict__ ids_out, float4* __restrict__ pos_out,
+                               float4* __restrict__ vel_out, float* __restrict__ rho_out,
+                               float* __restrict__ kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // a job left undone (the fault injection of the dispatcher tests) places nothing; the count
+    // of placed particles tells the host whether every particle was placed
+    bool work = i < n && !(i >= skip_begin && i < skip_end);
+    uint32_t placed = block_reduce(work ? 1u : 0u, SumU(), 0u);
+    if (threadIdx.x == 0 && placed) atomicAdd(&st->processed, placed);
+    if (!work) return;
+    uint32_t l = lin[i];
+    uint32_t b = start[l], e = start[l + 1];
+    uint32_t id = ids_in[i];
+    uint32_t rank = 0;
+    for (uint32_t k = b; k < e; ++k) rank += members[k] < id ? 1u : 0u;
+    uint32_t f = b + rank;
+    ids_out[f] = id;
+    pos_out[f] = pos_in[i];
+    vel_out[f] = vel_in[i];
+    rho_out[f] = rho_in[i];
+    if (kap_in) kap_out[f] = kap_in[i];
+}
+
+// ---- exclusive scan of u32 in place, total written at data[m] ------------------------------
+
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kBlock * kScanItems;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t warp_sums[kBlock / 32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = lane < kBlock / 32 ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < kBlock / 32) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    uint32_t warp_prefix = warp > 0 ? warp_sums[warp - 1] : 0u;
+    if (total) *total = warp_sums[kBlock / 32 - 1];
+    return warp_prefix + x - v;
+}
+
+__global__ void k_scan_tiles(uint32_t* data, uint32_t m, uint32_t* tile_sums) {
+    uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < m ? data[base + k] : 0u;
+        sum += v[k];
+    }
+    uint32_t total;
+    uint32_t prefix = block_exclusive_scan(sum, &total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < m) data[base + k] = prefix;
+        prefix += v[k];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// One block scans the tile sums (any count) in place.
+__global__ void k_scan_sums(uint32_t* sums, uint32_t tiles) {
+    __shared__ uint32_t carry_s;
+    if (threadIdx.x == 0) carry_s = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < tiles; base += kBlock) {
+        uint32_t i = base + threadIdx.x;
+        uint32_t v = i < tiles ? sums[i] : 0u;
+        uint32_t total;
+        uint32_t x = block_exclusive_scan(v, &total);
+        uint32_t carry = carry_s;
+        if (i < tiles) sums[i] = x + carry;
+        __syncthreads();
+        if (threadIdx.x == 0) carry_s = carry + total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[tiles] = carry_s;  // grand total
+}
+
+__global__ void k_scan_add(uint32_t* data, uint32_t m, const uint32_t* __restrict__ tile_sums) {
+    uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t add = tile_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < m) data[base + k] += add;
+    if (blockIdx.x == 0 && threadIdx.x == 0) data[m] = tile_sums[gridDim.x];
+}
+
+// ---- densities (mod.rs:621-675), with WCSPH pressure (step.rs:147-172) or DFSPH factors ----
+
+template <int SOLVER>
+__global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDev wg, const float4* __restrict__ pos,
+                                                    const float4* __restrict__ walls, float* __restrict__ rho,
+                                                    float* __restrict__ press, float* __restrict__ scaled,
+                                                    float* __restrict__ alpha, uint32_t* __restrict__ crowd,
+                                                    Status* st) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < p.n;
+    uint32_t compressed = 0;
+    if (valid) {
+        float4 a = pos[i];
+        int3 cell = cell_of(p, a.x, a.y, a.z);
+        float sum = 0.0f, wsum = 0.0f;
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f, squares = 0.0f;
+        uint32_t nf = 0, nw = 0;
+        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+            float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
+            float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
+            sum += kernel_value(p, d);
+            if (SOLVER == 1) {
+                // dfsph.rs:118 gradient(at - other), then factors (dfsph.rs:149-153)
+                float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+                float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
+                float px = (rx * g) * p.mass, py = (ry * g) * p.mass, pz = (rz * g) * p.mass;
+                sx = sx + px;
+                sy = sy + py;
+                sz = sz + pz;
+                squares += dot3(px, py, pz, px, py, pz);
+                ++nf;
+            }
+        });
+        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+            float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
+            float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
+            wsum += kernel_value(p, d);
+            if (SOLVER == 1) {
+                float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+                float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
+                sx = sx + (rx * g) * p.mass;
+                sy = sy + (ry * g) * p.mass;
+                sz = sz + (rz * g) * p.mass;
+                ++nw;
+            }
+        });
+        float density = p.mass * (sum + wsum);
+        rho[i] = density;
+        if (SOLVER == 0) {
+            float ratio = fminf(density / p.rest, 1.1f);
+            float pressure = fmaxf(p.stiffness * (pow7(ratio) - 1.0f), 0.0f);
+            press[i] = pressure;
+            scaled[i] = pressure / (density * density);
+        } else {
+            float total = dot3(sx, sy, sz, sx, sy, sz) + squares;
+            alpha[i] = total > 0.0f ? 1.0f / total : 0.0f;
+            crowd[i] = nf + nw;
+        }
+        float c = density / p.rest - 1.0f;
+        if (c > 0.0f) compressed = __float_as_uint(c);
+    }
+    compressed = block_reduce(compressed, MaxU(), 0u);
+    if (threadIdx.x == 0 && compressed) atomicMax(&st->maxcomp_bits, compressed);
+}
+
+// ---- wall viscosity (step.rs:262-301, no terrains) ---------------------------------------
+
+__device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc, const GridDev& wg,
+                                               const float4* __restrict__ walls, int3 cell, float4 a, float4 v,
+                                               float density) {
+    float awx = 0.0f, awy = 0.0f, awz = 0.0f;
+    each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        float g = kernel_gradient_factor(p, rx, ry, rz);
+        awx = awx + -(rx * g);
+        awy = awy + -(ry * g);
+        awz = awz + -(rz * g);
+    });
+    // normalize_or(ZERO) dividing by the length
+    float len = sqrtf(dot3(awx, awy, awz, awx, awy, awz));
+    float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+    if (isfinite(len) && len > 0.0f) {
+        nx = awx / len;
+        ny = awy / len;
+        nz = awz / len;
+    }
+    float k = fminf(dot3(v.x, v.y, v.z, nx, ny, nz), 0.0f);
+    float ix = nx * k, iy = ny * k, iz = nz * k;
+    float px = 0.0f, py = 0.0f, pz = 0.0f;
+    each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        float toward = dot3(ix, iy, iz, rx, ry, rz);
+        if (toward < 0.0f) {
+            float squeeze = toward / (dot3(rx, ry, rz, rx, ry, rz) + p.soften);
+            float damp = -wall_visc * squeeze / density;
+            float g = kernel_gradient_factor(p, rx, ry, rz);
+            float s = p.mass * damp;
+            px = px - (rx * g) * s;
+            py = py - (ry * g) * s;
+            pz = pz - (rz * g) * s;
+        }
+    });
+    return make_float3(px, py, pz);
+}
+
+// ---- advance (step.rs:305-339, no terrains) -------------------------------------------------
+
+__device__ __forceinline__ void advance_one(const Params& p, float dt, float4& a, float4& v, uint32_t& held,
+                                            uint32_t& bad) {
+    float nx = a.x + v.x * dt, ny = a.y + v.y * dt, nz = a.z + v.z * dt;
+    if (p.has_bounds) {
+        float ix = fminf(fmaxf(nx, p.low_in.x), p.high_in.x);
+        float iy = fminf(fmaxf(ny, p.low_in.y), p.high_in.y);
+        float iz = fminf(fmaxf(nz, p.low_in.z), p.high_in.z);
+        if (ix != nx || iy != ny || iz != nz) {
+            float cx = fminf(fmaxf(nx, p.low.x), p.high.x);
+            float cy = fminf(fmaxf(ny, p.low.y), p.high.y);
+            float cz = fminf(fmaxf(nz, p.low.z), p.high.z);
+            if (cx != nx || cy != ny || cz != nz) held += 1;
+            if (ix != nx) v.x = 0.0f;
+            if (iy != ny) v.y = 0.0f;
+            if (iz != nz) v.z = 0.0f;
+            nx = ix;
+            ny = iy;
+            nz = iz;
+        }
+    }
+    if (!(isfinite(nx) && isfinite(ny) && isfinite(nz) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) bad = 1;
+    a.x = nx;
+    a.y = ny;
+    a.z = nz;
+}
+
+// ---- WCSPH: forces, velocity update and advance in one pass (step.rs:159-223, 305-339) -----
+
+__global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepConsts* __restrict__ sc, GridDev fg,
+                                                        GridDev wg, const float4* __restrict__ pos,
+                                                        const float4* __restrict__ vel, const float* __restrict__ rho,
+                                                        const float* __restrict__ press,
+                                                        const float* __restrict__ scaled,
+                                                        const float4* __restrict__ walls, float4* __restrict__ pos_out,
+                                                        float4* __restrict__ vel_out, Status* st) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < p.n;
+    int3 nc = make_int3(0, 0, 0);
+    float speed = 0.0f;
+    uint32_t held = 0, bad = 0;
+    if (valid) {
+        const float dt = sc->dt;
+        const float visc = sc->viscosity;
+        float4 a = pos[i];
+        float4 v = vel[i];
+        float density = rho[i];
+        float own = scaled[i];
+        int3 cell = cell_of(p, a.x, a.y, a.z);
+        float px = 0.0f, py = 0.0f, pz = 0.0f;
+        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+            float squared = dot3(rx, ry, rz, rx, ry, rz);
+            if (squared <= 0.0f) return;
+            float distance = sqrtf(squared);
+            float g = kernel_slope(p, distance) / distance;
+            float gx = rx * g, gy = ry * g, gz = rz * g;
+            float4 w = __ldg(&vel[j]);
+            float toward = fminf(dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx, ry, rz), 0.0f);
+            float damp = -visc * toward / (squared + p.soften) * 2.0f / (density + __ldg(&rho[j]));
+            float s = p.mass * (own + __ldg(&scaled[j]) + damp);
+            px = px - gx * s;
+            py = py - gy * s;
+            pz = pz - gz * s;
+        });
+        float mirrored = own + press[i] / p.rest_sq;
+        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+            float g = kernel_gradient_factor(p, rx, ry, rz);
+            float s = p.mass * mirrored;
+            px = px - (rx * g) * s;
+            py = py - (ry * g) * s;
+            pz = pz - (rz * g) * s;
+        });
+        float3 wv = wall_viscous(p, sc->wall_viscosity, wg, walls, cell, a, v, density);
+        float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
+        v.x = v.x + ax * dt;
+        v.y = v.y + ay * dt;
+        v.z = v.z + az * dt;
+        advance_one(p, dt, a, v, held, bad);
+        pos_out[i] = a;
+        vel_out[i] = v;
+        nc = cell_of(p, a.x, a.y, a.z);
+        speed = sqrtf(dot3(v.x, v.y, v.z, v.x, v.y, v.z));
+        if (!(speed == speed)) speed = 0.0f;
+    }
+    fold_advance_stats(st, valid, nc, speed, held, bad);
+}
+
+// ---- DFSPH ----------------------------------------------------------------------------------
+
+// double-double accumulation (TwoSum), for the solver residual
+struct DD {
+    double hi, lo;
+};
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+    double s = a.hi + b.hi;
+    double bb = s - a.hi;
+    double err = (a.hi - (s - bb)) + (b.hi - bb);
+    double lo = a.lo + b.lo + err;
+    double h = s + lo;
+    return DD{h, lo - (h - s)};
+}
+
+// density_rate (dfsph.rs:166-181), then the solve's stiffness and error (dfsph.rs:241-259), and
+// the average error of the particles under load (dfsph.rs:263-268) in a last-block finish.
+template <int WHICH>
+__global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __restrict__ sc, GridDev fg,
+                                                 GridDev wg, const float4* __restrict__ pos,
+                                                 const float4* __restrict__ vel, const float* __restrict__ rho,
+                                                 const float* __restrict__ alpha, const uint32_t* __restrict__ crowd,
+                                                 const float4* __restrict__ walls, float* __restrict__ kappa,
+                                                 DD* __restrict__ partial, uint32_t* __restrict__ partial_loaded,
+                                                 Status* st, uint32_t iterations) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double err = 0.0;
+    uint32_t loaded = 0;
+    if (i < p.n) {
+        const float dt = sc->dt;
+        float4 a = pos[i];
+        float4 v = vel[i];
+        int3 cell = cell_of(p, a.x, a.y, a.z);
+        float rate = 0.0f;
+        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+            float g = kernel_gradient_factor(p, rx, ry, rz);
+            float4 w = __ldg(&vel[j]);
+            rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx * g, ry * g, rz * g);
+        });
+        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+            float g = kernel_gradient_factor(p, rx, ry, rz);
+            rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
+        });
+        rate = rate * p.mass;
+        float target, error;
+        if (WHICH == 1) {
+            float over = fmaxf(rho[i] + dt * rate - p.rest, 0.0f);
+            target = over / sc->dt_sq;
+            error = over / p.rest;
+        } else {
+            float r = crowd[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
+            target = r / dt;
+            error = dt * r / p.rest;
+        }
+        kappa[i] = target * alpha[i];
+        err = (double)error;
+        loaded = error > 0.0f ? 1u : 0u;
+    }
+    // block sum: a fixed shuffle tree in double-double
+    DD acc{err, 0.0};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        DD other{__shfl_xor_sync(0xffffffffu, acc.hi, o), __shfl_xor_sync(0xffffffffu, acc.lo, o)};
+        acc = dd_add(acc, other);
+    }
+    __shared__ DD warp_acc[kBlock / 32];
+    __shared__ bool last_block;
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) warp_acc[warp] = acc;
+    loaded = block_reduce(loaded, SumU(), 0u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD b = warp_acc[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) b = dd_add(b, warp_acc[k]);
+        partial[blockIdx.x] = b;
+        partial_loaded[blockIdx.x] = loaded;
+        __threadfence();
+        uint32_t ticket = atomicAdd(&st->ticket, 1u);
+        last_block = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last_block) return;
+    // the last block to finish sums the block partials in block order
+    __threadfence();
+    DD t{0.0, 0.0};
+    uint32_t cnt = 0;
+    for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+        // other blocks wrote these: read through L2, never a stale L1 line
+        const double* part = reinterpret_cast<const double*>(partial);
+        DD v{__ldcg(part + 2 * k), __ldcg(part + 2 * k + 1)};
+        t = dd_add(t, v);
+        cnt += __ldcg(partial_loaded + k);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        DD other{__shfl_xor_sync(0xffffffffu, t.hi, o), __shfl_xor_sync(0xffffffffu, t.lo, o)};
+        t = dd_add(t, other);
+    }
+    cnt = block_reduce(cnt, SumU(), 0u);
+    __syncthreads();
+    if (lane == 0) warp_acc[warp] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD b = warp_acc[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) b = dd_add(b, warp_acc[k]);
+        uint32_t load = cnt > 0 ? cnt : 1u;
+        double average = (b.hi + b.lo) / (double)load;
+        double tol = WHICH == 1 ? (double)p.den_tol : (double)p.div_tol;
+        bool settled = iterations >= p.min_iter && average <= tol;
+        st->average = average;
+        st->loaded = cnt;
+        st->settled = (settled || iterations >= p.max_iter) ? 1u : 0u;
+        st->ticket = 0;
+    }
+}
+
+// push_apart (dfsph.rs:184-216): the velocity change from each particle's stiffness.
+__global__ void __launch_bounds__(kBlock) k_push(Params p, const StepConsts* __restrict__ sc, GridDev fg, GridDev wg,
+                                                 const float4* __restrict__ pos, float4* __restrict__ vel,
+                                                 const float* __restrict__ kappa, const float4* __restrict__ walls) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const float dt = sc->dt;
+    float4 a = pos[i];
+    int3 cell = cell_of(p, a.x, a.y, a.z);
+    float own = kappa[i];
+    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        float g = kernel_gradient_factor(p, rx, ry, rz);
+        float s = p.mass * (own + __ldg(&kappa[j]));
+        cx = cx - (rx * g) * s;
+        cy = cy - (ry * g) * s;
+        cz = cz - (rz * g) * s;
+    });
+    each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        float g = kernel_gradient_factor(p, rx, ry, rz);
+        float s = p.mass * own;
+        cx = cx - (rx * g) * s;
+        cy = cy - (ry * g) * s;
+        cz = cz - (rz * g) * s;
+    });
+    float4 v = vel[i];
+    v.x = v.x + cx * dt;
+    v.y = v.y + cy * dt;
+    v.z = v.z + cz * dt;
+    vel[i] = v;
+}
+
+// viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
+// because neighbours read the old velocities.
+__global__ void __launch_bounds__(kBlock) k_viscous(Params p, const StepConsts* __restrict__ sc, GridDev fg, GridDev wg,
+                                                    const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                    const float* __restrict__ rho, const float4* __restrict__ walls,
+                                                    float4* __restrict__ vel_out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const float dt = sc->dt;
+    const float visc = sc->viscosity;
+    float4 a = pos[i];
+    float4 v = vel[i];
+    float density = rho[i];
+    int3 cell = cell_of(p, a.x, a.y, a.z);
+    float px = 0.0f, py = 0.0f, pz = 0.0f;
+    each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+        if (j == i) return;
+        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        float4 w = __ldg(&vel[j]);
+        float toward = dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx, ry, rz);
+        if (toward < 0.0f) {
+            float squeeze = toward / (dot3(rx, ry, rz, rx, ry, rz) + p.soften);
+            float damp = -visc * squeeze * 2.0f / (density + __ldg(&rho[j]));
+            float g = kernel_gradient_factor(p, rx, ry, rz);
+            float s = p.mass * damp;
+            px = px - (rx * g) * s;
+            py = py - (ry * g) * s;
+            pz = pz - (rz * g) * s;
+        }
+    });
+    float3 wv = wall_viscous(p, sc->wall_viscosity, wg, walls, cell, a, v, density);
+    float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
+    v.x = v.x + ax * dt;
+    v.y = v.y + ay * dt;
+    v.z = v.z + az * dt;
+    vel_out[i] = v;
+}
+
+__global__ void k_advance(Params p, const StepConsts* __restrict__ sc, const float4* __restrict__ pos_in,
+                          float4* __restrict__ pos_out, float4* __restrict__ vel, Status* st) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < p.n;
+    int3 nc = make_int3(0, 0, 0);
+    float speed = 0.0f;
+    uint32_t held = 0, bad = 0;
+    if (valid) {
+        float4 a = pos_in[i];
+        float4 v = vel[i];
+        advance_one(p, sc->dt, a, v, held, bad);
+        pos_out[i] = a;
+        vel[i] = v;
+        nc = cell_of(p, a.x, a.y, a.z);
+        speed = sqrtf(dot3(v.x, v.y, v.z, v.x, v.y, v.z));
+        if (!(speed == speed)) speed = 0.0f;
+    }
+    fold_advance_stats(st, valid, nc, speed, held, bad);
+}
+
+// ---- neighbour lists on demand (mod.rs:570-606) --------------------------------------------
+
+__global__ void k_list_count(Params p, GridDev g, const float4* __restrict__ pos, const float4* __restrict__ pts,
+                             uint32_t* counts) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float4 a = pos[i];
+    int3 cell = cell_of(p, a.x, a.y, a.z);
+    uint32_t c = 0;
+    each_near(p, g, pts, cell, a.x, a.y, a.z, [&](uint32_t, float4) { ++c; });
+    counts[i] = c;
+}
+
+__global__ void k_list_fill(Params p, GridDev g, const float4* __restrict__ pos, const float4* __restrict__ pts,
+                            const uint32_t* __restrict__ start, uint32_t* items) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float4 a = pos[i];
+    int3 cell = cell_of(p, a.x, a.y, a.z);
+    uint32_t k = start[i];
+    each_near(p, g, pts, cell, a.x, a.y, a.z, [&](uint32_t j, float4) { items[k++] = j; });
+}
+
+// ---- domain (mod.rs:451-486): keep flags, then a stable compaction -------------------------
+
+__global__ void k_domain_flags(Params p, const float4* __restrict__ pos, float3 low, float3 high, uint32_t* keep) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float4 a = pos[i];
+    float cx = fminf(fmaxf(a.x, low.x), high.x), cy = fminf(fmaxf(a.y, low.y), high.y),
+          cz = fminf(fmaxf(a.z, low.z), high.z);
+    keep[i] = (cx == a.x && cy == a.y && cz == a.z) ? 1u : 0u;
+}
+
+__global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ dest,
+                          const uint32_t* __restrict__ ids_in, const float4* __restrict__ pos_in,
+                          const float4* __restrict__ vel_in, const float* __restrict__ rho_in,
+                          uint32_t* __restrict__ ids_out, float4* __restrict__ pos_out,
+                          float4* __restrict__ vel_out, float* __restrict__ rho_out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !keep[i]) return;
+    uint32_t f = dest[i];
+    ids_out[f] = ids_in[i];
+    pos_out[f] = pos_in[i];
+    vel_out[f] = vel_in[i];
+    rho_out[f] = rho_in[i];
+}
+
+__global__ void k_set_consts(StepConsts c, StepConsts* out) { *out = c; }
+
+// ---- launchers ------------------------------------------------------------------------------
+
+static inline uint32_t blocks_for(uint32_t n) { return (n + kBlock - 1) / kBlock; }
+
+void launch_state_stats(const Params& p, const float4* pos, const float4* vel, Status* st, cudaStream_t s) {
+    if (p.n) k_state_stats<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, vel, st);
+}
+
+void launch_max_compression(const Params& p, const float* rho, Status* st, cudaStream_t s) {
+    if (p.n) k_max_compression<<<blocks_for(p.n), kBlock, 0, s>>>(p, rho, st);
+}
+
+void launch_count_cells(const Params& p, const float4* pos, int3 low, int3 span, uint32_t* count, uint32_t* lin,
+                        uint32_t* slot, cudaStream_t s) {
+    if (p.n) k_count_cells<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, low, span, count, lin, slot);
+}
+
+size_t scan_tiles(uint32_t m) { return (m + kScanTile - 1) / kScanTile; }
+
+void launch_exclusive_scan(uint32_t* data, uint32_t m, uint32_t* tile_sums, cudaStream_t s) {
+    if (m == 0) return;
+    uint32_t tiles = (uint32_t)scan_tiles(m);
+    k_scan_tiles<<<tiles, kBlock, 0, s>>>(data, m, tile_sums);
+    k_scan_sums<<<1, kBlock, 0, s>>>(tile_sums, tiles);
+    k_scan_add<<<tiles, kBlock, 0, s>>>(data, m, tile_sums);
+}
+
+void launch_scatter_members(uint32_t n, const uint32_t* lin, const uint32_t* slot, const uint32_t* start,
+                            const uint32_t* ids, uint32_t* members, cudaStream_t s) {
+    if (n) k_scatter_members<<<blocks_for(n), kBlock, 0, s>>>(n, lin, slot, start, ids, members);
+}
+
+void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start, const uint32_t* members,
+                         const uint32_t* ids_in, const float4* pos_in, const float4* vel_in, const float* rho_in,
+                         const float* kap_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
+                         float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, cudaStream_t s) {
+    if (n)
+        k_rank_reorder<<<blocks_for(n), kBlock, 0, s>>>(n, lin, start, members, ids_in, pos_in, vel_in, rho_in,
+                                                        kap_in, ids_out, pos_out, vel_out, rho_out, kap_out,
+                                                        skip_begin, skip_end, st);
+}
+
+void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
+                    float* rho, float* press, float* scaled, float* alpha, uint32_t* crowd, Status* st,
+                    cudaStream_t s) {
+    if (!p.n) return;
+    if (p.solver == 0)
+        k_density<0><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, rho, press, scaled, alpha, crowd, st);
+    else
+        k_density<1><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, rho, press, scaled, alpha, crowd, st);
+}
+
+void launch_wcsph_force(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg,
+                        const float4* pos, const float4* vel, const float* rho, const float* press,
+                        const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
+                        cudaStream_t s) {
+    if (p.n)
+        k_wcsph_force<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, rho, press, scaled, walls, pos_out,
+                                                         vel_out, st);
+}
+
+size_t rate_partial_bytes(uint32_t n) { return blocks_for(n) * (sizeof(DD) + sizeof(uint32_t)) + 64; }
+
+void launch_rate(int which, const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg,
+                 const float4* pos, const float4* vel, const float* rho, const float* alpha, const uint32_t* crowd,
+                 const float4* walls, float* kappa, void* partials, Status* st, uint32_t iterations,
+                 cudaStream_t s) {
+    if (!p.n) return;
+    uint32_t nb = blocks_for(p.n);
+    DD* part = static_cast<DD*>(partials);
+    uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
+    if (which == 0)
+        k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, rho, alpha, crowd, walls, kappa, part, loaded, st,
+                                        iterations);
+    else
+        k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, rho, alpha, crowd, walls, kappa, part, loaded, st,
+                                        iterations);
+}
+
+void launch_push(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg, const float4* pos,
+                 float4* vel, const float* kappa, const float4* walls, cudaStream_t s) {
+    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, kappa, walls);
+}
+
+void launch_viscous(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg, const float4* pos,
+                    const float4* vel, const float* rho, const float4* walls, float4* vel_out, cudaStream_t s) {
+    if (p.n) k_viscous<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, rho, walls, vel_out);
+}
+
+void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,
+                    Status* st, cudaStream_t s) {
+    if (p.n) k_advance<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, pos_in, pos_out, vel, st);
+}
+
+void launch_list_count(const Params& p, const GridDev& g, const float4* pos, const float4* pts, uint32_t* counts,
+                       cudaStream_t s) {
+    if (p.n) k_list_count<<<blocks_for(p.n), kBlock, 0, s>>>(p, g, pos, pts, counts);
+}
+
+void launch_list_fill(const Params& p, const GridDev& g, const float4* pos, const float4* pts, const uint32_t* start,
+                      uint32_t* items, cudaStream_t s) {
+    if (p.n) k_list_fill<<<blocks_for(p.n), kBlock, 0, s>>>(p, g, pos, pts, start, items);
+}
+
+void launch_domain_flags(const Params& p, const float4* pos, float3 low, float3 high, uint32_t* keep, cudaStream_t s) {
+    if (p.n) k_domain_flags<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, low, high, keep);
+}
+
+void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, const uint32_t* ids_in,
+                    const float4* pos_in, const float4* vel_in, const float* rho_in, uint32_t* ids_out,
+                    float4* pos_out, float4* vel_out, float* rho_out, cudaStream_t s) {
+    if (n)
+        k_compact<<<blocks_for(n), kBlock, 0, s>>>(n, keep, dest, ids_in, pos_in, vel_in, rho_in, ids_out, pos_out,
+                                                   vel_out, rho_out);
+}
+
+void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s) { k_set_consts<<<1, 1, 0, s>>>(c, out); }
+
+}  // namespace slf

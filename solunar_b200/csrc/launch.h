@@ -1,0 +1,64 @@
+// launch.h -- host-side launchers of the fluid kernels (kernels.cu).  All launches go on the
+// stream given; none synchronises.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fluid_device.cuh"
+
+namespace slf {
+
+void launch_state_stats(const Params& p, const float4* pos, const float4* vel, Status* st, cudaStream_t s);
+void launch_max_compression(const Params& p, const float* rho, Status* st, cudaStream_t s);
+
+// counting sort by dense cell index
+void launch_count_cells(const Params& p, const float4* pos, int3 low, int3 span, uint32_t* count, uint32_t* lin,
+                        uint32_t* slot, cudaStream_t s);
+size_t scan_tiles(uint32_t m);
+// exclusive scan of data[0, m) in place; data[m] receives the total.  tile_sums holds
+// scan_tiles(m) + 1 entries.
+void launch_exclusive_scan(uint32_t* data, uint32_t m, uint32_t* tile_sums, cudaStream_t s);
+void launch_scatter_members(uint32_t n, const uint32_t* lin, const uint32_t* slot, const uint32_t* start,
+                            const uint32_t* ids, uint32_t* members, cudaStream_t s);
+void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start, const uint32_t* members,
+                         const uint32_t* ids_in, const float4* pos_in, const float4* vel_in, const float* rho_in,
+                         const float* kap_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
+                         float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, cudaStream_t s);
+
+// pair passes
+void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
+                    float* rho, float* press, float* scaled, float* alpha, uint32_t* crowd, Status* st,
+                    cudaStream_t s);
+void launch_wcsph_force(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg,
+                        const float4* pos, const float4* vel, const float* rho, const float* press,
+                        const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
+                        cudaStream_t s);
+size_t rate_partial_bytes(uint32_t n);
+void launch_rate(int which, const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg,
+                 const float4* pos, const float4* vel, const float* rho, const float* alpha, const uint32_t* crowd,
+                 const float4* walls, float* kappa, void* partials, Status* st, uint32_t iterations,
+                 cudaStream_t s);
+void launch_push(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg, const float4* pos,
+                 float4* vel, const float* kappa, const float4* walls, cudaStream_t s);
+void launch_viscous(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg, const float4* pos,
+                    const float4* vel, const float* rho, const float4* walls, float4* vel_out, cudaStream_t s);
+void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,
+                    Status* st, cudaStream_t s);
+
+// neighbour lists on demand
+void launch_list_count(const Params& p, const GridDev& g, const float4* pos, const float4* pts, uint32_t* counts,
+                       cudaStream_t s);
+void launch_list_fill(const Params& p, const GridDev& g, const float4* pos, const float4* pts, const uint32_t* start,
+                      uint32_t* items, cudaStream_t s);
+
+// domain
+void launch_domain_flags(const Params& p, const float4* pos, float3 low, float3 high, uint32_t* keep, cudaStream_t s);
+void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, const uint32_t* ids_in,
+                    const float4* pos_in, const float4* vel_in, const float* rho_in, uint32_t* ids_out,
+                    float4* pos_out, float4* vel_out, float* rho_out, cudaStream_t s);
+
+void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s);
+
+}  // namespace slf

@@ -1,0 +1,1236 @@
+// world.cpp -- the host side of the library: FluidWorld's state owner and the C ABI.
+//
+// The world holds settings and walls on the host (walls are static and built once, as the
+// reference builds them, src/fluid/boundary.rs) and every particle array on the device.  A step
+// launches the substep kernels on the world's stream and reads back one small status block per
+// substep, which carries what the host decides on: the bounding box of cells for the next sort,
+// the fastest particle (substep length), the solver's stop flag, non-finite and held-back counts.
+//
+// Buffer discipline: the committed particle state is never written by a substep.  The sort
+// copies it into a second slot, the substep works there and in a third, and only a substep that
+// finished clean is committed by switching slot indexes.  A failed substep therefore leaves the
+// particles as the last finished substep put them (src/fluid/step.rs:55-57).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/solunar_fluid.h"
+#include "launch.h"
+
+namespace slf {
+namespace {
+
+thread_local std::string g_error;
+
+int32_t fail(int32_t code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+#define SLF_CUDA(expr)                                                                            \
+    do {                                                                                          \
+        cudaError_t e_ = (expr);                                                                  \
+        if (e_ != cudaSuccess) return fail(SLF_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define SLF_TRY(expr)                 \
+    do {                              \
+        int32_t st_ = (expr);         \
+        if (st_ != SLF_OK) return st_; \
+    } while (0)
+
+// Device array that grows geometrically.
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    int32_t ensure(size_t n, size_t keep, cudaStream_t s) {
+        if (n <= cap) return SLF_OK;
+        size_t want = std::max<size_t>(n, cap + cap / 2);
+        want = std::max<size_t>(want, 256);
+        T* q = nullptr;
+        SLF_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&q), want * sizeof(T), s));
+        if (p && keep) SLF_CUDA(cudaMemcpyAsync(q, p, std::min(keep, cap) * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        if (p) SLF_CUDA(cudaFreeAsync(p, s));
+        p = q;
+        cap = want;
+        return SLF_OK;
+    }
+    void release(cudaStream_t s) {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// ---- host arithmetic in the reference's f32 order ------------------------------------------
+
+inline float pow3f(float x) { return x * (x * x); }
+inline float pow4f(float x) { float s = x * x; return s * s; }
+
+struct HostKernel {
+    float radius, scale;
+    explicit HostKernel(float r) : radius(r), scale(21.0f / (2.0f * 3.14159265358979323846f * pow3f(r))) {}
+    float value(float d) const {
+        float q = d / radius;
+        if (q >= 1.0f) return 0.0f;
+        return scale * pow4f(1.0f - q) * (1.0f + 4.0f * q);
+    }
+};
+
+inline float rmin(float a, float b) {
+    if (std::isnan(a)) return b;
+    if (std::isnan(b)) return a;
+    return b < a ? b : a;
+}
+inline float rmax(float a, float b) {
+    if (std::isnan(a)) return b;
+    if (std::isnan(b)) return a;
+    return b > a ? b : a;
+}
+
+inline int32_t sat_i32(float v) {
+    if (std::isnan(v)) return 0;
+    if (v >= 2147483647.0f) return INT32_MAX;
+    if (v <= -2147483648.0f) return INT32_MIN;
+    return static_cast<int32_t>(v);
+}
+
+struct F3 {
+    float x, y, z;
+};
+inline bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+struct Key3 {
+    int32_t x, y, z;
+    bool operator==(const Key3& o) const { return x == o.x && y == o.y && z == o.z; }
+    bool operator<(const Key3& o) const { return std::tie(x, y, z) < std::tie(o.x, o.y, o.z); }
+};
+
+struct ContainerBox {
+    uint32_t id;
+    F3 low, high;
+};
+
+}  // namespace
+
+struct World {
+    slf_settings s{};
+    float radius = 0, mass = 0, scale = 0;
+    cudaStream_t stream = nullptr;
+
+    // particles
+    uint64_t n = 0;
+    uint32_t next_id = 0;
+    std::vector<float4> pend_pos, pend_vel;
+    std::vector<uint32_t> pend_ids;
+    int cpos = 0, cid = 0;  // committed slots of pos/vel (of 3) and ids/rho (of 2)
+    DevBuf<float4> pos[3], vel[3];
+    DevBuf<uint32_t> ids[2];
+    DevBuf<float> rho[2];
+    DevBuf<float> press, scaled, alpha, kappa;
+    DevBuf<uint32_t> crowd, lin, cslot, members, count, tiles, keep;
+    DevBuf<uint8_t> partials;
+    bool stats_fresh = false;  // status holds bbox and speed of the committed state
+
+    // fluid cell table of the last sort
+    GridDev fgrid{};
+    int lists_pos = -1;  // slot of the positions the last sort produced
+    uint64_t lists_n = 0;
+    bool lists_valid = false;
+
+    // walls
+    std::vector<F3> wpos;
+    std::vector<uint32_t> wown;
+    uint32_t wall_next = 0;
+    std::vector<ContainerBox> containers;
+    bool has_bounds = false;
+    F3 blow{}, bhigh{};
+    DevBuf<float4> dwalls;
+    DevBuf<uint32_t> dwstart;
+    DevBuf<int4> dwkeys;
+    GridDev wgrid{};
+    bool walls_dirty = true;
+
+    bool has_domain = false;
+    F3 dlow{}, dhigh{};
+
+    Status* d_status = nullptr;
+    Status* h_status = nullptr;
+    StepConsts* d_consts = nullptr;
+
+    int64_t skip_job = -1;  // testing: next sort leaves this 512-particle job undone
+
+    ~World() {
+        if (stream) {
+            for (auto* b : {&pos[0], &pos[1], &pos[2], &vel[0], &vel[1], &vel[2]}) b->release(stream);
+            for (auto* b : {&ids[0], &ids[1], &crowd, &lin, &cslot, &members, &count, &tiles, &keep, &dwstart})
+                b->release(stream);
+            for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha, &kappa}) b->release(stream);
+            partials.release(stream);
+            dwalls.release(stream);
+            dwkeys.release(stream);
+            cudaStreamSynchronize(stream);
+            if (d_status) cudaFree(d_status);
+            if (d_consts) cudaFree(d_consts);
+            if (h_status) cudaFreeHost(h_status);
+            cudaStreamDestroy(stream);
+        }
+    }
+
+    // ---- settings ----------------------------------------------------------------------------
+
+    static bool valid(const slf_settings& s) {
+        auto positive = [](float v) { return std::isfinite(v) && v > 0.0f; };
+        bool support = s.support >= 1.5f && s.support <= 4.0f;
+        return (s.solver == SLF_SOLVER_WCSPH || s.solver == SLF_SOLVER_DFSPH) && positive(s.spacing) &&
+               positive(s.rest_density) && support && s.max_particles > 0 && positive(s.sound_speed) &&
+               std::isfinite(s.viscosity) && s.viscosity >= 0.0f && finite3(s.gravity) && s.courant > 0.0f &&
+               s.courant <= 1.0f && s.max_substeps > 0 && s.min_iterations <= s.max_iterations &&
+               std::isfinite(s.divergence_tolerance) && std::isfinite(s.density_tolerance);
+    }
+
+    // rest_mass (src/fluid/mod.rs:694-709)
+    float rest_mass() const {
+        HostKernel k(radius);
+        int reach = int(std::ceil(s.support));
+        float sum = 0.0f;
+        for (int z = -reach; z <= reach; ++z)
+            for (int y = -reach; y <= reach; ++y)
+                for (int x = -reach; x <= reach; ++x) {
+                    float ox = float(x) * s.spacing, oy = float(y) * s.spacing, oz = float(z) * s.spacing;
+                    sum += k.value(std::sqrt(ox * ox + oy * oy + oz * oz));
+                }
+        return s.rest_density / sum;
+    }
+
+    int32_t init(const slf_settings& settings) {
+        s = settings;
+        radius = s.spacing * s.support;
+        HostKernel k(radius);
+        scale = k.scale;
+        mass = rest_mass();
+        SLF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        SLF_CUDA(cudaMalloc(&d_status, sizeof(Status)));
+        SLF_CUDA(cudaMalloc(&d_consts, sizeof(StepConsts)));
+        SLF_CUDA(cudaMallocHost(&h_status, sizeof(Status)));
+        std::memset(h_status, 0, sizeof(Status));
+        SLF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(Status), stream));
+        return SLF_OK;
+    }
+
+    Params params() const {
+        Params p{};
+        p.spacing = s.spacing;
+        p.radius = radius;
+        p.reach = radius * radius;
+        p.scale = scale;
+        p.mass = mass;
+        p.rest = s.rest_density;
+        p.rest_sq = s.rest_density * s.rest_density;
+        p.stiffness = s.rest_density * (s.sound_speed * s.sound_speed) / 7.0f;
+        p.soften = 0.01f * radius * radius;
+        p.gravity = make_float3(s.gravity[0], s.gravity[1], s.gravity[2]);
+        p.has_bounds = has_bounds ? 1 : 0;
+        float half = s.spacing / 2.0f;
+        p.low = make_float3(blow.x, blow.y, blow.z);
+        p.high = make_float3(bhigh.x, bhigh.y, bhigh.z);
+        p.low_in = make_float3(blow.x + half, blow.y + half, blow.z + half);
+        p.high_in = make_float3(bhigh.x - half, bhigh.y - half, bhigh.z - half);
+        p.n = uint32_t(n);
+        p.solver = s.solver;
+        p.div_tol = s.divergence_tolerance;
+        p.den_tol = s.density_tolerance;
+        p.min_iter = s.min_iterations;
+        p.max_iter = s.max_iterations;
+        return p;
+    }
+
+    // viscosity(dt) (step.rs:254-259) and the wall damping (step.rs:282-283)
+    StepConsts consts(float dt) const {
+        StepConsts c{};
+        c.dt = dt;
+        c.viscosity = rmin(s.viscosity * s.sound_speed * radius, 0.05f * radius * radius / dt);
+        float stable = radius * radius / dt;
+        c.wall_viscosity = rmin(1.0f * s.sound_speed * radius, 0.25f * stable);
+        c.dt_sq = dt * dt;
+        return c;
+    }
+
+    Key3 cell_of(F3 p) const {
+        return Key3{sat_i32(std::floor(p.x / radius)), sat_i32(std::floor(p.y / radius)),
+                    sat_i32(std::floor(p.z / radius))};
+    }
+
+    // ---- particles ---------------------------------------------------------------------------
+
+    uint64_t total() const { return n + pend_ids.size(); }
+
+    int32_t add(uint64_t k, const float* p, const float* v, uint32_t* ids_out) {
+        for (uint64_t i = 0; i < k; ++i)
+            if (!finite3(p + 3 * i) || !finite3(v + 3 * i)) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        if (total() + k > s.max_particles || uint64_t(next_id) + k > uint64_t(UINT32_MAX))
+            return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
+        for (uint64_t i = 0; i < k; ++i) {
+            pend_pos.push_back(make_float4(p[3 * i], p[3 * i + 1], p[3 * i + 2], 0.0f));
+            pend_vel.push_back(make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0f));
+            if (ids_out) ids_out[i] = next_id;
+            pend_ids.push_back(next_id++);
+        }
+        return SLF_OK;
+    }
+
+    // fill_box (src/fluid/mod.rs:493-524)
+    int32_t fill_box(const float* low, const float* high, uint64_t* count_out) {
+        if (!finite3(low) || !finite3(high)) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid box");
+        if (high[0] < low[0] || high[1] < low[1] || high[2] < low[2])
+            return fail(SLF_ERR_OUT_OF_RANGE, "inside out fluid box");
+        float spacing = s.spacing;
+        auto count = [&](float extent) -> uint64_t {
+            float c = rmin(std::floor(extent / spacing), 4294967295.0f);
+            if (std::isnan(c) || c <= 0.0f) return 0;
+            return uint64_t(c);
+        };
+        float sx = high[0] - low[0], sy = high[1] - low[1], sz = high[2] - low[2];
+        uint64_t nx = count(sx), ny = count(sy), nz = count(sz);
+        auto sat_mul = [](uint64_t a, uint64_t b) -> uint64_t {
+            unsigned __int128 q = (unsigned __int128)a * b;
+            return q > UINT64_MAX ? UINT64_MAX : uint64_t(q);
+        };
+        uint64_t tot = sat_mul(sat_mul(nx, ny), nz);
+        uint64_t room = s.max_particles > total() ? s.max_particles - total() : 0;
+        uint64_t ids_left = uint64_t(UINT32_MAX - next_id);
+        if (tot > room || tot > ids_left) return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
+        float half = spacing * 0.5f;
+        float st[3] = {low[0] + half, low[1] + half, low[2] + half};
+        std::vector<float> pts;
+        pts.reserve(size_t(tot) * 3);
+        for (uint64_t y = 0; y < ny; ++y)
+            for (uint64_t z = 0; z < nz; ++z)
+                for (uint64_t x = 0; x < nx; ++x) {
+                    pts.push_back(st[0] + float(x) * spacing);
+                    pts.push_back(st[1] + float(y) * spacing);
+                    pts.push_back(st[2] + float(z) * spacing);
+                }
+        std::vector<float> zeros(pts.size(), 0.0f);
+        SLF_TRY(add(tot, pts.data(), zeros.data(), nullptr));
+        if (count_out) *count_out = tot;
+        return SLF_OK;
+    }
+
+    // Moves staged particles onto the device, after the committed ones.
+    int32_t flush() {
+        if (pend_ids.empty()) return SLF_OK;
+        uint64_t k = pend_ids.size();
+        uint64_t m = n + k;
+        for (int i = 0; i < 3; ++i) {
+            SLF_TRY(pos[i].ensure(m, i == cpos ? n : 0, stream));
+            SLF_TRY(vel[i].ensure(m, i == cpos ? n : 0, stream));
+        }
+        for (int i = 0; i < 2; ++i) {
+            SLF_TRY(ids[i].ensure(m, i == cid ? n : 0, stream));
+            SLF_TRY(rho[i].ensure(m, i == cid ? n : 0, stream));
+        }
+        SLF_CUDA(cudaMemcpyAsync(pos[cpos].p + n, pend_pos.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(vel[cpos].p + n, pend_vel.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(ids[cid].p + n, pend_ids.data(), k * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaMemsetAsync(rho[cid].p + n, 0, k * sizeof(float), stream));
+        SLF_CUDA(cudaStreamSynchronize(stream));  // the staging vectors are pageable and freed next
+        pend_pos.clear();
+        pend_vel.clear();
+        pend_ids.clear();
+        n = m;
+        lists_valid = false;
+        stats_fresh = false;
+        return SLF_OK;
+    }
+
+    int32_t ensure_work_buffers() {
+        SLF_TRY(press.ensure(n, 0, stream));
+        SLF_TRY(scaled.ensure(n, 0, stream));
+        SLF_TRY(alpha.ensure(n, 0, stream));
+        SLF_TRY(kappa.ensure(n, 0, stream));
+        SLF_TRY(crowd.ensure(n, 0, stream));
+        SLF_TRY(lin.ensure(n, 0, stream));
+        SLF_TRY(cslot.ensure(n, 0, stream));
+        SLF_TRY(members.ensure(n, 0, stream));
+        SLF_TRY(partials.ensure(rate_partial_bytes(uint32_t(n)), 0, stream));
+        return SLF_OK;
+    }
+
+    // ---- walls (src/fluid/boundary.rs) -------------------------------------------------------
+
+    static int32_t check_box(const float* low, const float* high) {
+        if (!finite3(low) || !finite3(high)) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid box");
+        if (high[0] <= low[0] || high[1] <= low[1] || high[2] <= low[2])
+            return fail(SLF_ERR_OUT_OF_RANGE, "inside out fluid box");
+        return SLF_OK;
+    }
+
+    void cells_in(const float* low, const float* high, int64_t out[3]) const {
+        for (int a = 0; a < 3; ++a) {
+            float c = rmin(std::round((high[a] - low[a]) / s.spacing), 1e9f);
+            out[a] = int64_t(c);
+        }
+    }
+
+    int32_t check_room(int64_t count) const {
+        uint64_t room = s.max_particles > wpos.size() ? s.max_particles - wpos.size() : 0;
+        if (count < 0 || uint64_t(count) > room || wall_next == UINT32_MAX)
+            return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
+        return SLF_OK;
+    }
+
+    uint32_t add_wall_points(const std::vector<F3>& pts) {
+        uint32_t id = wall_next++;
+        for (auto& p : pts) {
+            wpos.push_back(p);
+            wown.push_back(id);
+        }
+        settle_walls();
+        return id;
+    }
+
+    int32_t add_box_container(const float* low, const float* high, uint32_t* out) {
+        SLF_TRY(check_box(low, high));
+        int64_t c[3];
+        cells_in(low, high, c);
+        int64_t layers = int64_t(std::ceil(s.support));
+        int64_t shell = (c[0] + 2 * layers) * (c[1] + 2 * layers) * (c[2] + 2 * layers) - c[0] * c[1] * c[2];
+        SLF_TRY(check_room(shell));
+        std::vector<F3> pts;
+        pts.reserve(size_t(shell));
+        for (int64_t y = -layers; y < c[1] + layers; ++y)
+            for (int64_t z = -layers; z < c[2] + layers; ++z)
+                for (int64_t x = -layers; x < c[0] + layers; ++x) {
+                    bool inside = x >= 0 && x < c[0] && y >= 0 && y < c[1] && z >= 0 && z < c[2];
+                    if (inside) continue;
+                    pts.push_back(F3{low[0] + (float(x) + 0.5f) * s.spacing, low[1] + (float(y) + 0.5f) * s.spacing,
+                                     low[2] + (float(z) + 0.5f) * s.spacing});
+                }
+        uint32_t id = add_wall_points(pts);
+        containers.push_back(ContainerBox{id, F3{low[0], low[1], low[2]}, F3{high[0], high[1], high[2]}});
+        update_bounds();
+        if (out) *out = id;
+        return SLF_OK;
+    }
+
+    int32_t add_wall(const float* low, const float* high, uint32_t* out) {
+        SLF_TRY(check_box(low, high));
+        int64_t c[3];
+        cells_in(low, high, c);
+        for (auto& v : c) v = std::max<int64_t>(v, 1);
+        int64_t count = c[0] * c[1] * c[2];
+        SLF_TRY(check_room(count));
+        std::vector<F3> pts;
+        pts.reserve(size_t(count));
+        for (int64_t y = 0; y < c[1]; ++y)
+            for (int64_t z = 0; z < c[2]; ++z)
+                for (int64_t x = 0; x < c[0]; ++x)
+                    pts.push_back(F3{low[0] + (float(x) + 0.5f) * s.spacing, low[1] + (float(y) + 0.5f) * s.spacing,
+                                     low[2] + (float(z) + 0.5f) * s.spacing});
+        uint32_t id = add_wall_points(pts);
+        if (out) *out = id;
+        return SLF_OK;
+    }
+
+    bool remove_boundary(uint32_t id) {
+        size_t before = wpos.size();
+        size_t kept = 0;
+        for (size_t i = 0; i < wpos.size(); ++i)
+            if (wown[i] != id) {
+                wpos[kept] = wpos[i];
+                wown[kept] = wown[i];
+                ++kept;
+            }
+        wpos.resize(kept);
+        wown.resize(kept);
+        bool had = false;
+        std::vector<ContainerBox> rest;
+        for (auto& c : containers) {
+            if (c.id == id) had = true;
+            else rest.push_back(c);
+        }
+        containers = rest;
+        update_bounds();
+        bool gone = wpos.size() != before || had;
+        if (gone) settle_walls();
+        return gone;
+    }
+
+    void update_bounds() {
+        has_bounds = false;
+        for (auto& c : containers) {
+            if (!has_bounds) {
+                blow = c.low;
+                bhigh = c.high;
+                has_bounds = true;
+            } else {
+                blow = F3{rmin(blow.x, c.low.x), rmin(blow.y, c.low.y), rmin(blow.z, c.low.z)};
+                bhigh = F3{rmax(bhigh.x, c.high.x), rmax(bhigh.y, c.high.y), rmax(bhigh.z, c.high.z)};
+            }
+        }
+    }
+
+    static uint32_t fbits(float v) {
+        uint32_t b;
+        std::memcpy(&b, &v, 4);
+        return b;
+    }
+
+    // settle_walls (boundary.rs:155-178): sort by cell, owner, position bits, index.
+    void settle_walls() {
+        size_t m = wpos.size();
+        struct WK {
+            Key3 cell;
+            uint32_t owner, bx, by, bz;
+            size_t index;
+        };
+        std::vector<WK> order(m);
+        for (size_t i = 0; i < m; ++i)
+            order[i] = WK{cell_of(wpos[i]), wown[i], fbits(wpos[i].x), fbits(wpos[i].y), fbits(wpos[i].z), i};
+        std::sort(order.begin(), order.end(), [](const WK& a, const WK& b) {
+            return std::tie(a.cell.x, a.cell.y, a.cell.z, a.owner, a.bx, a.by, a.bz, a.index) <
+                   std::tie(b.cell.x, b.cell.y, b.cell.z, b.owner, b.bx, b.by, b.bz, b.index);
+        });
+        std::vector<F3> np(m);
+        std::vector<uint32_t> no(m);
+        for (size_t i = 0; i < m; ++i) {
+            np[i] = wpos[order[i].index];
+            no[i] = order[i].owner;
+        }
+        wpos = std::move(np);
+        wown = std::move(no);
+        walls_dirty = true;
+    }
+
+    // Uploads the walls and their cell table: dense over the walls' box while it holds at most 64
+    // cells per occupied one plus 4096 (mod.rs:214-216), else the occupied cells for search.
+    int32_t upload_walls() {
+        if (!walls_dirty) return SLF_OK;
+        size_t m = wpos.size();
+        wgrid = GridDev{};
+        if (m == 0) {
+            walls_dirty = false;
+            return SLF_OK;
+        }
+        std::vector<float4> w(m);
+        std::vector<Key3> keys(m);
+        for (size_t i = 0; i < m; ++i) {
+            w[i] = make_float4(wpos[i].x, wpos[i].y, wpos[i].z, 0.0f);
+            keys[i] = cell_of(wpos[i]);
+        }
+        std::vector<Key3> cells;
+        std::vector<uint32_t> starts;
+        for (size_t i = 0; i < m; ++i)
+            if (i == 0 || !(keys[i] == keys[i - 1])) {
+                cells.push_back(keys[i]);
+                starts.push_back(uint32_t(i));
+            }
+        starts.push_back(uint32_t(m));
+        Key3 lo = cells[0], hi = cells[0];
+        for (auto& c : cells) {
+            lo = Key3{std::min(lo.x, c.x), std::min(lo.y, c.y), std::min(lo.z, c.z)};
+            hi = Key3{std::max(hi.x, c.x), std::max(hi.y, c.y), std::max(hi.z, c.z)};
+        }
+        int64_t sx = int64_t(hi.x) - lo.x + 1, sy = int64_t(hi.y) - lo.y + 1, sz = int64_t(hi.z) - lo.z + 1;
+        __int128 vol = (__int128)sx * sy * sz;
+        SLF_TRY(dwalls.ensure(m, 0, stream));
+        SLF_CUDA(cudaMemcpyAsync(dwalls.p, w.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        if (vol <= (__int128)64 * (__int128)cells.size() + 4096 && vol < (__int128)(1u << 30)) {
+            size_t volume = size_t(vol);
+            std::vector<uint32_t> start(volume + 1, 0);
+            // cells are in key order, which is the dense table's x-major order
+            size_t c = 0;
+            for (size_t at = 0; at < volume; ++at) {
+                start[at] = c < cells.size() ? starts[c] : uint32_t(m);
+                if (c < cells.size()) {
+                    const Key3& k = cells[c];
+                    size_t lin = size_t(((int64_t(k.x) - lo.x) * sy + (int64_t(k.y) - lo.y)) * sz + (int64_t(k.z) - lo.z));
+                    if (lin == at) ++c;
+                }
+            }
+            start[volume] = uint32_t(m);
+            SLF_TRY(dwstart.ensure(volume + 1, 0, stream));
+            SLF_CUDA(cudaMemcpyAsync(dwstart.p, start.data(), (volume + 1) * 4, cudaMemcpyHostToDevice, stream));
+            wgrid.mode = 1;
+            wgrid.lx = lo.x;
+            wgrid.ly = lo.y;
+            wgrid.lz = lo.z;
+            wgrid.sx = int(sx);
+            wgrid.sy = int(sy);
+            wgrid.sz = int(sz);
+            wgrid.start = dwstart.p;
+            SLF_CUDA(cudaStreamSynchronize(stream));
+        } else {
+            std::vector<int4> k4(cells.size());
+            for (size_t i = 0; i < cells.size(); ++i) k4[i] = make_int4(cells[i].x, cells[i].y, cells[i].z, 0);
+            SLF_TRY(dwkeys.ensure(cells.size(), 0, stream));
+            SLF_TRY(dwstart.ensure(starts.size(), 0, stream));
+            SLF_CUDA(cudaMemcpyAsync(dwkeys.p, k4.data(), k4.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
+            SLF_CUDA(cudaMemcpyAsync(dwstart.p, starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, stream));
+            SLF_CUDA(cudaStreamSynchronize(stream));
+            wgrid.mode = 2;
+            wgrid.cells = uint32_t(cells.size());
+            wgrid.keys = dwkeys.p;
+            wgrid.start = dwstart.p;
+        }
+        walls_dirty = false;
+        return SLF_OK;
+    }
+
+    // ---- status --------------------------------------------------------------------------
+
+    int32_t read_status() {
+        SLF_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(Status), cudaMemcpyDeviceToHost, stream));
+        SLF_CUDA(cudaStreamSynchronize(stream));
+        return SLF_OK;
+    }
+
+    // Clears the per-substep fields; the box starts empty.
+    int32_t reset_status() {
+        Status z{};
+        z.cell_lo[0] = z.cell_lo[1] = z.cell_lo[2] = INT32_MAX;
+        z.cell_hi[0] = z.cell_hi[1] = z.cell_hi[2] = INT32_MIN;
+        *h_status = z;
+        SLF_CUDA(cudaMemcpyAsync(d_status, h_status, sizeof(Status), cudaMemcpyHostToDevice, stream));
+        return SLF_OK;
+    }
+
+    // Box of cells and fastest speed of the committed state.
+    int32_t refresh_stats() {
+        if (stats_fresh) return SLF_OK;
+        SLF_TRY(reset_status());
+        Params p = params();
+        launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream);
+        SLF_TRY(read_status());
+        stats_fresh = true;
+        return SLF_OK;
+    }
+
+    float fastest() const { float v; uint32_t b = h_status->vmax_bits; std::memcpy(&v, &b, 4); return v; }
+
+    // ---- the spatial hash (update_neighbors, src/fluid/mod.rs:540-566) ------------------------
+
+    // Sorts the committed state into slot `to` (pos/vel) and the other id slot, by (cell, id).
+    // Needs the committed state's box in the status.  Commits nothing.
+    int32_t sort_into(int to) {
+        Params p = params();
+        if (n == 0) return SLF_OK;
+        int64_t lo[3], span[3];
+        __int128 vol = 1;
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = h_status->cell_lo[a];
+            span[a] = int64_t(h_status->cell_hi[a]) - lo[a] + 1;
+            if (span[a] <= 0) return fail(SLF_ERR_CUDA, "empty cell box before a sort");
+            vol *= span[a];
+        }
+        // a dense count table over the box; a scene spread too thin for it is not supported yet
+        if (vol > (__int128)64 * (__int128)n + (1 << 22) || vol >= (__int128)(1u << 31))
+            return fail(SLF_ERR_UNSUPPORTED, "particles spread over too many cells for the dense cell table");
+        uint32_t volume = uint32_t(vol);
+        SLF_TRY(ensure_work_buffers());
+        SLF_TRY(count.ensure(size_t(volume) + 1, 0, stream));
+        SLF_TRY(tiles.ensure(scan_tiles(volume) + 1, 0, stream));
+        SLF_CUDA(cudaMemsetAsync(count.p, 0, (size_t(volume) + 1) * 4, stream));
+        int3 lo3 = make_int3(int(lo[0]), int(lo[1]), int(lo[2]));
+        int3 sp3 = make_int3(int(span[0]), int(span[1]), int(span[2]));
+        launch_count_cells(p, pos[cpos].p, lo3, sp3, count.p, lin.p, cslot.p, stream);
+        launch_exclusive_scan(count.p, volume, tiles.p, stream);
+        launch_scatter_members(uint32_t(n), lin.p, cslot.p, count.p, ids[cid].p, members.p, stream);
+        uint32_t job_lo = 0, job_hi = 0;
+        if (skip_job >= 0) {
+            job_lo = uint32_t(skip_job) * 512u;
+            job_hi = job_lo + 512u;
+            skip_job = -1;
+        }
+        launch_rank_reorder(uint32_t(n), lin.p, count.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p,
+                            rho[cid].p, nullptr, ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, nullptr,
+                            job_lo, job_hi, d_status, stream);
+        fgrid = GridDev{};
+        fgrid.mode = 1;
+        fgrid.lx = lo3.x;
+        fgrid.ly = lo3.y;
+        fgrid.lz = lo3.z;
+        fgrid.sx = sp3.x;
+        fgrid.sy = sp3.y;
+        fgrid.sz = sp3.z;
+        fgrid.start = count.p;
+        return SLF_OK;
+    }
+
+    int32_t update_neighbors() {
+        SLF_TRY(flush());
+        SLF_TRY(upload_walls());
+        if (n == 0) {
+            lists_valid = true;
+            lists_n = 0;
+            return SLF_OK;
+        }
+        SLF_TRY(refresh_stats());
+        int to = (cpos + 1) % 3;
+        h_status->processed = 0;
+        SLF_CUDA(cudaMemsetAsync(&d_status->processed, 0, 4, stream));
+        SLF_TRY(sort_into(to));
+        SLF_TRY(read_status());
+        if (h_status->processed != n) {
+            lists_valid = false;
+            return fail(SLF_ERR_DISPATCH_INCOMPLETE, "dispatcher did not run every job");
+        }
+        cpos = to;
+        cid = 1 - cid;
+        lists_pos = to;
+        lists_n = n;
+        lists_valid = true;
+        stats_fresh = false;
+        return SLF_OK;
+    }
+
+    int32_t compute_densities() {
+        SLF_TRY(flush());
+        if (!lists_valid || lists_n != n) return fail(SLF_ERR_OUT_OF_RANGE, "neighbour lists are stale");
+        if (n == 0) return SLF_OK;
+        SLF_TRY(ensure_work_buffers());
+        SLF_TRY(upload_walls());
+        Params p = params();
+        launch_density(p, fgrid, wgrid, pos[cpos].p, dwalls.p, rho[cid].p, press.p, scaled.p, alpha.p, crowd.p,
+                       d_status, stream);
+        SLF_CUDA(cudaStreamSynchronize(stream));
+        return SLF_OK;
+    }
+
+    // ---- substeps ----------------------------------------------------------------------------
+
+    // one WCSPH substep (step.rs:144-224) from the committed state; commits on success
+    int32_t wcsph_substep(float dt, uint32_t& held) {
+        Params p = params();
+        int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
+        SLF_TRY(sort_into(a));
+        int nid = 1 - cid;
+        launch_set_consts(consts(dt), d_consts, stream);
+        launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, rho[nid].p, press.p, scaled.p, alpha.p, crowd.p,
+                       d_status, stream);
+        SLF_TRY(reset_status());
+        launch_wcsph_force(p, d_consts, fgrid, wgrid, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
+                           pos[b].p, vel[b].p, d_status, stream);
+        SLF_TRY(read_status());
+        if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        held = h_status->held;
+        cpos = b;
+        cid = nid;
+        lists_pos = a;
+        lists_n = n;
+        lists_valid = true;
+        stats_fresh = true;  // the force pass folded the new state's box and speed
+        return SLF_OK;
+    }
+
+    // solve (dfsph.rs:222-275): Jacobi iterations until the average error is under tolerance.
+    int32_t solve(int which, const Params& p, int a, float4* v, int nid, uint32_t& iterations) {
+        iterations = 0;
+        for (;;) {
+            launch_rate(which, p, d_consts, fgrid, wgrid, pos[a].p, v, rho[nid].p, alpha.p, crowd.p, dwalls.p,
+                        kappa.p, partials.p, d_status, iterations, stream);
+            SLF_CUDA(cudaMemcpyAsync(&h_status->settled, &d_status->settled, 4, cudaMemcpyDeviceToHost, stream));
+            SLF_CUDA(cudaStreamSynchronize(stream));
+            if (h_status->settled) return SLF_OK;
+            // the device stops the loop at max_iterations; past that its flag was not written
+            if (iterations > s.max_iterations) return fail(SLF_ERR_TIMEOUT, "solver stop flag never set");
+            launch_push(p, d_consts, fgrid, wgrid, pos[a].p, v, kappa.p, dwalls.p, stream);
+            iterations += 1;
+        }
+    }
+
+    // one DFSPH substep (dfsph.rs:79-103) from the committed state; commits on success
+    int32_t dfsph_substep(float dt, uint32_t& held, uint32_t& iterations) {
+        Params p = params();
+        int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
+        SLF_TRY(sort_into(a));
+        int nid = 1 - cid;
+        launch_set_consts(consts(dt), d_consts, stream);
+        launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, rho[nid].p, press.p, scaled.p, alpha.p, crowd.p,
+                       d_status, stream);
+        uint32_t div_it = 0, den_it = 0;
+        SLF_TRY(solve(0, p, a, vel[a].p, nid, div_it));
+        launch_viscous(p, d_consts, fgrid, wgrid, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
+        SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it));
+        SLF_TRY(reset_status());
+        launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, stream);
+        SLF_TRY(read_status());
+        if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        held = h_status->held;
+        iterations = div_it + den_it;
+        last_iterations[0] = div_it;
+        last_iterations[1] = den_it;
+        cpos = b;
+        cid = nid;
+        lists_pos = a;
+        lists_n = n;
+        lists_valid = true;
+        stats_fresh = true;
+        return SLF_OK;
+    }
+    uint32_t last_iterations[2] = {0, 0};
+
+    // step (step.rs:58-90)
+    int32_t step(float dt, slf_report* out) {
+        slf_report r{};
+        if (out) *out = r;
+        if (!std::isfinite(dt) || dt < 0.0f) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid step");
+        if (dt == 0.0f) return SLF_OK;
+        SLF_TRY(flush());
+        SLF_TRY(upload_walls());
+        if (n > 0) {
+            SLF_TRY(ensure_work_buffers());
+            SLF_TRY(refresh_stats());
+            if (s.solver == SLF_SOLVER_WCSPH) {
+                // wcsph (step.rs:102-142), no coupled bodies
+                r.sound_speed = s.sound_speed;
+                float fast = fastest();
+                float largest = s.courant * radius / (s.sound_speed + fast);
+                float wanted = rmax(std::ceil(dt / largest), 1.0f);
+                float cap = float(s.max_substeps);
+                uint32_t substeps = uint32_t(rmin(wanted, cap));
+                r.capped = wanted > cap;
+                float small = dt / float(substeps);
+                for (uint32_t i = 0; i < substeps; ++i) {
+                    uint32_t held = 0;
+                    SLF_TRY(wcsph_substep(small, held));
+                    r.held_back += held;
+                }
+                r.substeps = substeps;
+            } else {
+                // dfsph (dfsph.rs:46-77)
+                float spacing = s.spacing, courant = s.courant;
+                float pull = std::sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] +
+                                       s.gravity[2] * s.gravity[2]);
+                float left = dt;
+                while (left > 0.0f) {
+                    float small = courant * spacing / rmax(fastest(), 1e-6f);
+                    if (pull > 0.0f) small = rmin(small, std::sqrt(2.0f * courant * spacing / pull));
+                    if (r.substeps + 1 >= s.max_substeps && small < left) {
+                        r.capped = 1;
+                        small = left;
+                    }
+                    small = rmin(small, left);
+                    uint32_t held = 0, its = 0;
+                    SLF_TRY(dfsph_substep(small, held, its));
+                    r.iterations += its;
+                    r.held_back += held;
+                    r.substeps += 1;
+                    left -= small;
+                }
+            }
+        }
+        // keep_in_domain (mod.rs:451-486)
+        SLF_TRY(keep_in_domain(r.lost));
+        // max_speed and max_compression of what is left (step.rs:83-88)
+        if (n > 0) {
+            SLF_TRY(reset_status());
+            Params p = params();
+            launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream);
+            launch_max_compression(p, rho[cid].p, d_status, stream);
+            SLF_TRY(read_status());
+            stats_fresh = true;
+            std::memcpy(&r.max_speed, &h_status->vmax_bits, 4);
+            std::memcpy(&r.max_compression, &h_status->maxcomp_bits, 4);
+        }
+        if (out) *out = r;
+        return SLF_OK;
+    }
+
+    int32_t keep_in_domain(uint32_t& lost) {
+        lost = 0;
+        if (!has_domain || n == 0) return SLF_OK;
+        Params p = params();
+        SLF_TRY(keep.ensure(n + 1, 0, stream));
+        SLF_TRY(members.ensure(n + 1, 0, stream));
+        SLF_TRY(tiles.ensure(scan_tiles(uint32_t(n)) + 1, 0, stream));
+        launch_domain_flags(p, pos[cpos].p, make_float3(dlow.x, dlow.y, dlow.z), make_float3(dhigh.x, dhigh.y, dhigh.z),
+                            keep.p, stream);
+        SLF_CUDA(cudaMemcpyAsync(members.p, keep.p, n * 4, cudaMemcpyDeviceToDevice, stream));
+        launch_exclusive_scan(members.p, uint32_t(n), tiles.p, stream);
+        uint32_t kept = 0;
+        SLF_CUDA(cudaMemcpyAsync(&kept, members.p + n, 4, cudaMemcpyDeviceToHost, stream));
+        SLF_CUDA(cudaStreamSynchronize(stream));
+        if (kept == n) return SLF_OK;
+        int to = (cpos + 1) % 3;
+        if (to == lists_pos) to = (cpos + 2) % 3;
+        launch_compact(uint32_t(n), keep.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p, rho[cid].p,
+                       ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, stream);
+        SLF_CUDA(cudaStreamSynchronize(stream));
+        lost = uint32_t(n - kept);
+        n = kept;
+        cpos = to;
+        cid = 1 - cid;
+        lists_valid = false;
+        stats_fresh = false;
+        return SLF_OK;
+    }
+
+    // ---- read-outs -------------------------------------------------------------------------
+
+    int32_t read_vec(const DevBuf<float4>& b, float* out, uint64_t k) {
+        std::vector<float4> tmp(k);
+        if (k) {
+            SLF_CUDA(cudaMemcpyAsync(tmp.data(), b.p, k * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+            SLF_CUDA(cudaStreamSynchronize(stream));
+        }
+        for (uint64_t i = 0; i < k; ++i) {
+            out[3 * i] = tmp[i].x;
+            out[3 * i + 1] = tmp[i].y;
+            out[3 * i + 2] = tmp[i].z;
+        }
+        return SLF_OK;
+    }
+
+    template <class T> int32_t read_plain(const DevBuf<T>& b, T* out, uint64_t k) {
+        if (k) {
+            SLF_CUDA(cudaMemcpyAsync(out, b.p, k * sizeof(T), cudaMemcpyDeviceToHost, stream));
+            SLF_CUDA(cudaStreamSynchronize(stream));
+        }
+        return SLF_OK;
+    }
+
+    int32_t lists(bool walls, uint32_t* start, uint64_t start_len, uint32_t* items, uint64_t cap, uint64_t* len) {
+        SLF_TRY(flush());
+        if (!lists_valid || lists_n != n) return fail(SLF_ERR_OUT_OF_RANGE, "neighbour lists are stale");
+        if (start && start_len != n + 1) return fail(SLF_ERR_INVALID_ARGUMENT, "start must hold len + 1 entries");
+        SLF_TRY(upload_walls());
+        if (n == 0) {
+            if (start) start[0] = 0;
+            if (len) *len = 0;
+            return SLF_OK;
+        }
+        Params p = params();
+        DevBuf<uint32_t> cnt, tl, it;
+        SLF_TRY(cnt.ensure(n + 1, 0, stream));
+        SLF_TRY(tl.ensure(scan_tiles(uint32_t(n)) + 1, 0, stream));
+        const GridDev& g = walls ? wgrid : fgrid;
+        const float4* pts = walls ? dwalls.p : pos[lists_pos].p;
+        launch_list_count(p, g, pos[lists_pos].p, pts, cnt.p, stream);
+        launch_exclusive_scan(cnt.p, uint32_t(n), tl.p, stream);
+        uint32_t total_items = 0;
+        SLF_CUDA(cudaMemcpyAsync(&total_items, cnt.p + n, 4, cudaMemcpyDeviceToHost, stream));
+        SLF_CUDA(cudaStreamSynchronize(stream));
+        if (len) *len = total_items;
+        int32_t st = SLF_OK;
+        if (start) st = read_plain(cnt, start, n + 1);
+        if (st == SLF_OK && items) {
+            if (cap < total_items) {
+                st = fail(SLF_ERR_INVALID_ARGUMENT, "items buffer too small");
+            } else if (total_items) {
+                st = it.ensure(total_items, 0, stream);
+                if (st == SLF_OK) {
+                    launch_list_fill(p, g, pos[lists_pos].p, pts, cnt.p, it.p, stream);
+                    st = read_plain(it, items, total_items);
+                }
+            }
+        }
+        cnt.release(stream);
+        tl.release(stream);
+        it.release(stream);
+        cudaStreamSynchronize(stream);
+        return st;
+    }
+
+    uint64_t state_hash_host(const std::vector<uint32_t>& id, const std::vector<float>& p,
+                             const std::vector<float>& v) const {
+        std::vector<size_t> order(id.size());
+        std::iota(order.begin(), order.end(), size_t(0));
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return id[a] < id[b]; });
+        uint64_t h = 0xcbf29ce484222325ull;
+        auto put = [&](uint32_t w) {
+            for (int k = 0; k < 4; ++k) {
+                h ^= uint64_t((w >> (8 * k)) & 0xffu);
+                h *= 0x00000100000001b3ull;
+            }
+        };
+        for (size_t i : order) {
+            put(id[i]);
+            for (int k = 0; k < 3; ++k) put(fbits(p[3 * i + k]));
+            for (int k = 0; k < 3; ++k) put(fbits(v[3 * i + k]));
+        }
+        return h;
+    }
+};
+
+}  // namespace slf
+
+// ---- C ABI ---------------------------------------------------------------------------------
+
+using slf::World;
+using slf::fail;
+
+struct slf_world {
+    World w;
+};
+
+#define SLF_NEED(ptr)                                                                \
+    do {                                                                             \
+        if (!(ptr)) return fail(SLF_ERR_INVALID_ARGUMENT, "null argument: " #ptr);  \
+    } while (0)
+
+extern "C" {
+
+int32_t slf_settings_default(slf_settings* out) {
+    SLF_NEED(out);
+    slf_settings s{};
+    s.solver = SLF_SOLVER_WCSPH;
+    s.spacing = 0.05f;
+    s.rest_density = 1000.0f;
+    s.support = 2.0f;
+    s.max_particles = uint64_t(1) << 22;
+    s.sound_speed = 20.0f;
+    s.viscosity = 0.15f;
+    s.gravity[0] = 0.0f;
+    s.gravity[1] = -9.81f;
+    s.gravity[2] = 0.0f;
+    s.courant = 0.4f;
+    s.max_substeps = 2000;
+    s.positions = SLF_POSITIONS_ABSOLUTE;
+    s.arithmetic = SLF_ARITHMETIC_EXACT;
+    s.warm_start = 0;
+    s.divergence_tolerance = 1e-3f;
+    s.density_tolerance = 5e-4f;
+    s.min_iterations = 2;
+    s.max_iterations = 100;
+    *out = s;
+    return SLF_OK;
+}
+
+int32_t slf_create(const slf_settings* settings, slf_world** out) {
+    SLF_NEED(settings);
+    SLF_NEED(out);
+    *out = nullptr;
+    if (!World::valid(*settings)) return fail(SLF_ERR_INVALID_SETTINGS, "invalid settings");
+    if (settings->positions != SLF_POSITIONS_ABSOLUTE || settings->arithmetic != SLF_ARITHMETIC_EXACT ||
+        settings->warm_start)
+        return fail(SLF_ERR_UNSUPPORTED, "only absolute positions, exact arithmetic and cold starts are built");
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+        return fail(SLF_ERR_CUDA, "no CUDA device");
+    auto h = std::make_unique<slf_world>();
+    int32_t st = h->w.init(*settings);
+    if (st != SLF_OK) return st;
+    *out = h.release();
+    return SLF_OK;
+}
+
+void slf_destroy(slf_world* world) { delete world; }
+
+int32_t slf_get_settings(const slf_world* world, slf_settings* out) {
+    SLF_NEED(world);
+    SLF_NEED(out);
+    *out = world->w.s;
+    return SLF_OK;
+}
+
+int32_t slf_particle_mass(const slf_world* world, float* out) {
+    SLF_NEED(world);
+    SLF_NEED(out);
+    *out = world->w.mass;
+    return SLF_OK;
+}
+
+int32_t slf_kernel(const slf_world* world, float* radius, float* scale) {
+    SLF_NEED(world);
+    if (radius) *radius = world->w.radius;
+    if (scale) *scale = world->w.scale;
+    return SLF_OK;
+}
+
+int32_t slf_len(const slf_world* world, uint64_t* out) {
+    SLF_NEED(world);
+    SLF_NEED(out);
+    *out = world->w.total();
+    return SLF_OK;
+}
+
+int32_t slf_add_particle(slf_world* world, const float position[3], const float velocity[3], uint32_t* id_out) {
+    SLF_NEED(world);
+    SLF_NEED(position);
+    SLF_NEED(velocity);
+    return world->w.add(1, position, velocity, id_out);
+}
+
+int32_t slf_add_particles(slf_world* world, uint64_t n, const float* positions, const float* velocities,
+                          uint32_t* ids_out) {
+    SLF_NEED(world);
+    if (n == 0) return SLF_OK;
+    SLF_NEED(positions);
+    SLF_NEED(velocities);
+    return world->w.add(n, positions, velocities, ids_out);
+}
+
+int32_t slf_fill_box(slf_world* world, const float low[3], const float high[3], uint64_t* count_out) {
+    SLF_NEED(world);
+    SLF_NEED(low);
+    SLF_NEED(high);
+    return world->w.fill_box(low, high, count_out);
+}
+
+int32_t slf_set_domain(slf_world* world, const float* low, const float* high) {
+    SLF_NEED(world);
+    World& w = world->w;
+    if (!low && !high) {
+        w.has_domain = false;
+        return SLF_OK;
+    }
+    SLF_NEED(low);
+    SLF_NEED(high);
+    if (!slf::finite3(low) || !slf::finite3(high)) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid domain");
+    if (high[0] <= low[0] || high[1] <= low[1] || high[2] <= low[2])
+        return fail(SLF_ERR_OUT_OF_RANGE, "inside out fluid domain");
+    w.has_domain = true;
+    w.dlow = slf::F3{low[0], low[1], low[2]};
+    w.dhigh = slf::F3{high[0], high[1], high[2]};
+    return SLF_OK;
+}
+
+int32_t slf_add_box_container(slf_world* world, const float low[3], const float high[3], uint32_t* boundary_out) {
+    SLF_NEED(world);
+    SLF_NEED(low);
+    SLF_NEED(high);
+    return world->w.add_box_container(low, high, boundary_out);
+}
+
+int32_t slf_add_wall(slf_world* world, const float low[3], const float high[3], uint32_t* boundary_out) {
+    SLF_NEED(world);
+    SLF_NEED(low);
+    SLF_NEED(high);
+    return world->w.add_wall(low, high, boundary_out);
+}
+
+int32_t slf_remove_boundary(slf_world* world, uint32_t boundary, int32_t* removed) {
+    SLF_NEED(world);
+    bool gone = world->w.remove_boundary(boundary);
+    if (removed) *removed = gone ? 1 : 0;
+    return SLF_OK;
+}
+
+int32_t slf_wall_count(const slf_world* world, uint64_t* out) {
+    SLF_NEED(world);
+    SLF_NEED(out);
+    *out = world->w.wpos.size();
+    return SLF_OK;
+}
+
+int32_t slf_read_wall_positions(const slf_world* world, float* out, uint64_t n) {
+    SLF_NEED(world);
+    const World& w = world->w;
+    if (n != w.wpos.size()) return fail(SLF_ERR_INVALID_ARGUMENT, "n must equal the wall count");
+    if (n) SLF_NEED(out);
+    for (uint64_t i = 0; i < n; ++i) {
+        out[3 * i] = w.wpos[i].x;
+        out[3 * i + 1] = w.wpos[i].y;
+        out[3 * i + 2] = w.wpos[i].z;
+    }
+    return SLF_OK;
+}
+
+int32_t slf_step(slf_world* world, float dt, slf_report* out) {
+    SLF_NEED(world);
+    return world->w.step(dt, out);
+}
+
+int32_t slf_update_neighbors(slf_world* world) {
+    SLF_NEED(world);
+    return world->w.update_neighbors();
+}
+
+int32_t slf_compute_densities(slf_world* world) {
+    SLF_NEED(world);
+    return world->w.compute_densities();
+}
+
+static int32_t prep_read(const slf_world* world, uint64_t n) {
+    World& w = const_cast<World&>(world->w);
+    int32_t st = w.flush();
+    if (st != SLF_OK) return st;
+    if (n != w.n) return fail(SLF_ERR_INVALID_ARGUMENT, "n must equal slf_len()");
+    return SLF_OK;
+}
+
+int32_t slf_read_ids(const slf_world* world, uint32_t* out, uint64_t n) {
+    SLF_NEED(world);
+    SLF_TRY(prep_read(world, n));
+    if (n) SLF_NEED(out);
+    World& w = const_cast<World&>(world->w);
+    return w.read_plain(w.ids[w.cid], out, n);
+}
+
+int32_t slf_read_positions(const slf_world* world, float* out, uint64_t n) {
+    SLF_NEED(world);
+    SLF_TRY(prep_read(world, n));
+    if (n) SLF_NEED(out);
+    World& w = const_cast<World&>(world->w);
+    return w.read_vec(w.pos[w.cpos], out, n);
+}
+
+int32_t slf_read_velocities(const slf_world* world, float* out, uint64_t n) {
+    SLF_NEED(world);
+    SLF_TRY(prep_read(world, n));
+    if (n) SLF_NEED(out);
+    World& w = const_cast<World&>(world->w);
+    return w.read_vec(w.vel[w.cpos], out, n);
+}
+
+int32_t slf_read_densities(const slf_world* world, float* out, uint64_t n) {
+    SLF_NEED(world);
+    SLF_TRY(prep_read(world, n));
+    if (n) SLF_NEED(out);
+    World& w = const_cast<World&>(world->w);
+    return w.read_plain(w.rho[w.cid], out, n);
+}
+
+int32_t slf_neighbor_lists(slf_world* world, uint32_t* start, uint64_t start_len, uint32_t* items,
+                           uint64_t items_capacity, uint64_t* items_len) {
+    SLF_NEED(world);
+    return world->w.lists(false, start, start_len, items, items_capacity, items_len);
+}
+
+int32_t slf_wall_neighbor_lists(slf_world* world, uint32_t* start, uint64_t start_len, uint32_t* items,
+                                uint64_t items_capacity, uint64_t* items_len) {
+    SLF_NEED(world);
+    return world->w.lists(true, start, start_len, items, items_capacity, items_len);
+}
+
+int32_t slf_state_hash(const slf_world* world, uint64_t* out) {
+    SLF_NEED(world);
+    SLF_NEED(out);
+    World& w = const_cast<World&>(world->w);
+    SLF_TRY(w.flush());
+    uint64_t n = w.n;
+    std::vector<uint32_t> id(n);
+    std::vector<float> p(3 * n), v(3 * n);
+    SLF_TRY(w.read_plain(w.ids[w.cid], id.data(), n));
+    SLF_TRY(w.read_vec(w.pos[w.cpos], p.data(), n));
+    SLF_TRY(w.read_vec(w.vel[w.cpos], v.data(), n));
+    *out = w.state_hash_host(id, p, v);
+    return SLF_OK;
+}
+
+const char* slf_last_error(void) { return slf::g_error.c_str(); }
+
+int32_t slf_debug_skip_job(slf_world* world, int64_t job) {
+    SLF_NEED(world);
+    world->w.skip_job = job;
+    return SLF_OK;
+}
+
+int32_t slf_last_iterations(const slf_world* world, uint32_t* divergence, uint32_t* density) {
+    SLF_NEED(world);
+    if (divergence) *divergence = world->w.last_iterations[0];
+    if (density) *density = world->w.last_iterations[1];
+    return SLF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,271 @@
+"""FluidWorld: solunar's particle-fluid API (src/fluid/mod.rs:310-739, step.rs, dfsph.rs,
+boundary.rs) over the CUDA library's C ABI (include/solunar_fluid.h).
+
+Method names, argument meaning and errors follow the Rust `FluidWorld`; errors raise
+`PhysicsError` whose `.kind` names the PhysicsError variant.  The `&dyn JobDispatch` argument of
+the Rust methods has no counterpart: the GPU runs every job.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .abi import CReport, CSettings, FluidReport, FluidSettings, PhysicsError, vec3
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_NAME = "libsolunar_fluid.so"
+
+_lib = None
+
+
+def library_path() -> str:
+    return os.path.join(HERE, LIB_NAME)
+
+
+def load_library():
+    """Loads the in-tree CUDA library.  Raises if it was not built: there is no CPU path."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m solunar_b200.build` "
+                           "(the fluid step has no CPU fallback)")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    fp = ctypes.POINTER(ctypes.c_float)
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    sig = {
+        "slf_settings_default": [ctypes.POINTER(CSettings)],
+        "slf_create": [ctypes.POINTER(CSettings), ctypes.POINTER(vp)],
+        "slf_get_settings": [vp, ctypes.POINTER(CSettings)],
+        "slf_particle_mass": [vp, fp],
+        "slf_kernel": [vp, fp, fp],
+        "slf_len": [vp, u64p],
+        "slf_add_particle": [vp, fp, fp, u32p],
+        "slf_add_particles": [vp, ctypes.c_uint64, fp, fp, u32p],
+        "slf_fill_box": [vp, fp, fp, u64p],
+        "slf_set_domain": [vp, fp, fp],
+        "slf_add_box_container": [vp, fp, fp, u32p],
+        "slf_add_wall": [vp, fp, fp, u32p],
+        "slf_remove_boundary": [vp, ctypes.c_uint32, i32p],
+        "slf_wall_count": [vp, u64p],
+        "slf_read_wall_positions": [vp, fp, ctypes.c_uint64],
+        "slf_step": [vp, ctypes.c_float, ctypes.POINTER(CReport)],
+        "slf_update_neighbors": [vp],
+        "slf_compute_densities": [vp],
+        "slf_read_ids": [vp, u32p, ctypes.c_uint64],
+        "slf_read_positions": [vp, fp, ctypes.c_uint64],
+        "slf_read_velocities": [vp, fp, ctypes.c_uint64],
+        "slf_read_densities": [vp, fp, ctypes.c_uint64],
+        "slf_neighbor_lists": [vp, u32p, ctypes.c_uint64, u32p, ctypes.c_uint64, u64p],
+        "slf_wall_neighbor_lists": [vp, u32p, ctypes.c_uint64, u32p, ctypes.c_uint64, u64p],
+        "slf_state_hash": [vp, u64p],
+        "slf_last_iterations": [vp, u32p, u32p],
+        "slf_debug_skip_job": [vp, ctypes.c_int64],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int32
+    L.slf_destroy.argtypes = [vp]
+    L.slf_destroy.restype = None
+    L.slf_last_error.argtypes = []
+    L.slf_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _check(code: int):
+    if code != 0:
+        msg = _lib.slf_last_error().decode(errors="replace") if _lib is not None else ""
+        raise PhysicsError(code, msg)
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def default_settings() -> FluidSettings:
+    c = CSettings()
+    _check(load_library().slf_settings_default(ctypes.byref(c)))
+    return FluidSettings.from_c(c)
+
+
+class FluidWorld:
+    """FluidWorld (src/fluid/mod.rs:310-339) with its particles on the GPU."""
+
+    def __init__(self, settings: FluidSettings | None = None):
+        # FluidWorld::new (mod.rs:344-370)
+        L = load_library()
+        self._settings = settings or FluidSettings()
+        c = self._settings.to_c()
+        h = ctypes.c_void_p()
+        _check(L.slf_create(ctypes.byref(c), ctypes.byref(h)))
+        self._h = h
+
+    new = classmethod(lambda cls, settings=None: cls(settings))
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.slf_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    # ---- settings and sizes (mod.rs:372-390) ----
+    def settings(self) -> FluidSettings:
+        c = CSettings()
+        _check(_lib.slf_get_settings(self._h, ctypes.byref(c)))
+        return FluidSettings.from_c(c)
+
+    def kernel(self):
+        r, s = ctypes.c_float(), ctypes.c_float()
+        _check(_lib.slf_kernel(self._h, ctypes.byref(r), ctypes.byref(s)))
+        return r.value, s.value
+
+    def particle_mass(self) -> float:
+        m = ctypes.c_float()
+        _check(_lib.slf_particle_mass(self._h, ctypes.byref(m)))
+        return m.value
+
+    def len(self) -> int:
+        n = ctypes.c_uint64()
+        _check(_lib.slf_len(self._h, ctypes.byref(n)))
+        return n.value
+
+    __len__ = len
+
+    def is_empty(self) -> bool:
+        return self.len() == 0
+
+    # ---- particles (mod.rs:412-524) ----
+    def add_particle(self, position, velocity) -> int:
+        i = ctypes.c_uint32()
+        _check(_lib.slf_add_particle(self._h, vec3(position), vec3(velocity), ctypes.byref(i)))
+        return i.value
+
+    def add_particles(self, positions, velocities=None) -> np.ndarray:
+        p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+        v = (np.zeros_like(p) if velocities is None
+             else np.ascontiguousarray(velocities, dtype=np.float32).reshape(-1, 3))
+        ids = np.zeros(len(p), dtype=np.uint32)
+        _check(_lib.slf_add_particles(self._h, len(p), _ptr(p, ctypes.c_float), _ptr(v, ctypes.c_float),
+                                      _ptr(ids, ctypes.c_uint32)))
+        return ids
+
+    def fill_box(self, low, high) -> int:
+        n = ctypes.c_uint64()
+        _check(_lib.slf_fill_box(self._h, vec3(low), vec3(high), ctypes.byref(n)))
+        return n.value
+
+    def set_domain(self, domain):
+        if domain is None:
+            _check(_lib.slf_set_domain(self._h, None, None))
+        else:
+            _check(_lib.slf_set_domain(self._h, vec3(domain[0]), vec3(domain[1])))
+
+    # ---- walls (boundary.rs:41-120) ----
+    def add_box_container(self, low, high) -> int:
+        i = ctypes.c_uint32()
+        _check(_lib.slf_add_box_container(self._h, vec3(low), vec3(high), ctypes.byref(i)))
+        return i.value
+
+    def add_wall(self, low, high) -> int:
+        i = ctypes.c_uint32()
+        _check(_lib.slf_add_wall(self._h, vec3(low), vec3(high), ctypes.byref(i)))
+        return i.value
+
+    def remove_boundary(self, boundary: int) -> bool:
+        r = ctypes.c_int32()
+        _check(_lib.slf_remove_boundary(self._h, boundary, ctypes.byref(r)))
+        return bool(r.value)
+
+    def wall_positions(self) -> np.ndarray:
+        n = ctypes.c_uint64()
+        _check(_lib.slf_wall_count(self._h, ctypes.byref(n)))
+        out = np.zeros((n.value, 3), dtype=np.float32)
+        _check(_lib.slf_read_wall_positions(self._h, _ptr(out, ctypes.c_float), n.value))
+        return out
+
+    # ---- the step (step.rs:58-90) ----
+    def step(self, dt: float) -> FluidReport:
+        r = CReport()
+        _check(_lib.slf_step(self._h, dt, ctypes.byref(r)))
+        return FluidReport.from_c(r)
+
+    def update_neighbors(self):
+        _check(_lib.slf_update_neighbors(self._h))
+
+    def compute_densities(self):
+        _check(_lib.slf_compute_densities(self._h))
+
+    def last_iterations(self):
+        a, b = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(_lib.slf_last_iterations(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def debug_skip_job(self, job: int):
+        _check(_lib.slf_debug_skip_job(self._h, job))
+
+    # ---- read-outs (mod.rs:393-408, 612, 678) ----
+    def ids(self) -> np.ndarray:
+        n = self.len()
+        out = np.zeros(n, dtype=np.uint32)
+        _check(_lib.slf_read_ids(self._h, _ptr(out, ctypes.c_uint32), n))
+        return out
+
+    def _vecs(self, fn) -> np.ndarray:
+        n = self.len()
+        out = np.zeros((n, 3), dtype=np.float32)
+        _check(fn(self._h, _ptr(out, ctypes.c_float), n))
+        return out
+
+    def positions(self) -> np.ndarray:
+        return self._vecs(_lib.slf_read_positions)
+
+    def velocities(self) -> np.ndarray:
+        return self._vecs(_lib.slf_read_velocities)
+
+    def densities(self) -> np.ndarray:
+        n = self.len()
+        out = np.zeros(n, dtype=np.float32)
+        _check(_lib.slf_read_densities(self._h, _ptr(out, ctypes.c_float), n))
+        return out
+
+    def _lists(self, fn):
+        total = ctypes.c_uint64()
+        _check(fn(self._h, None, 0, None, 0, ctypes.byref(total)))
+        start = np.zeros(self.len() + 1, dtype=np.uint32)
+        items = np.zeros(max(total.value, 1), dtype=np.uint32)
+        _check(fn(self._h, _ptr(start, ctypes.c_uint32), len(start), _ptr(items, ctypes.c_uint32), total.value,
+                  ctypes.byref(total)))
+        return start, items[: total.value]
+
+    def neighbor_lists(self):
+        """(start, items): every particle's neighbours, itself included (mod.rs:279-308)."""
+        return self._lists(_lib.slf_neighbor_lists)
+
+    def wall_neighbor_lists(self):
+        return self._lists(_lib.slf_wall_neighbor_lists)
+
+    def neighbors_of(self, index: int) -> np.ndarray:
+        start, items = self.neighbor_lists()
+        if index + 1 >= len(start):
+            return items[:0]
+        return items[start[index]:start[index + 1]]
+
+    def state_hash(self) -> int:
+        v = ctypes.c_uint64()
+        _check(_lib.slf_state_hash(self._h, ctypes.byref(v)))
+        return v.value

@@ -1,8 +1,10 @@
-"""Pins the CPU restatement (oracle/) with the reference's own fluid tests.
+"""The reference's own fluid tests, restated against both implementations.
 
 The reference stores no golden vectors for this path; its tests are properties.  Each test
-here restates one of them (src/fluid/mod.rs:742-973, src/fluid/step.rs:342-584) against the
-float restatement, with the reference's thresholds.
+here restates one of them (src/fluid/mod.rs:742-973, src/fluid/step.rs:342-584) with the
+reference's thresholds.  Tests that take `backend` run against the CPU restatement (pinning the
+oracle) and, marked `gpu`, against the CUDA library; the rest probe parts only the restatement
+exposes (kernel samples, the cell table, thread counts).
 """
 import math
 import os
@@ -27,6 +29,18 @@ def shaken_world(oracle_lib, count, **kw):
     w = world(oracle_lib, **kw)
     w.add_particles(scenes.shaken(count))
     return w
+
+
+@pytest.fixture(params=["oracle", pytest.param("gpu", marks=pytest.mark.gpu)])
+def backend(request):
+    """A factory of worlds: the CPU restatement, or the CUDA library."""
+    if request.param == "oracle":
+        from oracle import py_oracle
+
+        py_oracle.build()
+        return lambda **kw: py_oracle.OracleWorld(FluidSettings(**kw))
+    gpu = request.getfixturevalue("gpu_lib")
+    return lambda **kw: gpu.FluidWorld(FluidSettings(**kw))
 
 
 def test_kernel_holds_unit_mass_and_its_slope_matches(oracle_lib):
@@ -79,9 +93,10 @@ def brute_force_sets(pos32: np.ndarray, reach: np.float32):
     return out
 
 
-def test_neighbors_are_exactly_the_brute_force_ones(oracle_lib):
+def test_neighbors_are_exactly_the_brute_force_ones(backend):
     # src/fluid/mod.rs:830-845
-    w = shaken_world(oracle_lib, 900)
+    w = backend()
+    w.add_particles(scenes.shaken(900))
     w.update_neighbors()
     pos = w.positions().astype(np.float32)
     r = np.float32(w.settings().radius())
@@ -107,9 +122,9 @@ def test_any_thread_count_gives_the_same_lists_densities_and_hash(oracle_lib):
     assert run(7) == one
 
 
-def test_a_lattice_inside_is_at_rest_density(oracle_lib):
+def test_a_lattice_inside_is_at_rest_density(backend):
     # src/fluid/mod.rs:866-895
-    w = world(oracle_lib)
+    w = backend()
     assert w.fill_box((0, 0, 0), (0.6, 0.6, 0.6)) == 12 ** 3
     w.update_neighbors()
     w.compute_densities()
@@ -127,9 +142,10 @@ def test_a_lattice_inside_is_at_rest_density(oracle_lib):
     assert abs(w.particle_mass() / cell - 1.0) < 0.1
 
 
-def test_ids_follow_particles_through_the_sort(oracle_lib):
+def test_ids_follow_particles_through_the_sort(backend):
     # src/fluid/mod.rs:897-913
-    w = shaken_world(oracle_lib, 700)
+    w = backend()
+    w.add_particles(scenes.shaken(700))
     before = dict(zip(w.ids().tolist(), w.positions().tolist()))
     h = w.state_hash()
     w.update_neighbors()
@@ -138,14 +154,14 @@ def test_ids_follow_particles_through_the_sort(oracle_lib):
     assert w.state_hash() == h
 
 
-def test_bad_input_is_refused_and_changes_nothing(oracle_lib):
+def test_bad_input_is_refused_and_changes_nothing(backend):
     # src/fluid/mod.rs:915-972 (the dispatcher case has no CPU-restatement counterpart; the
     # CUDA library's fault-injection test covers DispatchIncomplete)
     for kw in [dict(spacing=0.0), dict(rest_density=float("nan")), dict(support=9.0), dict(max_particles=0)]:
         with pytest.raises(PhysicsError) as e:
-            world(oracle_lib, **kw)
+            backend(**kw)
         assert e.value.kind == "InvalidSettings"
-    w = world(oracle_lib, max_particles=100)
+    w = backend(max_particles=100)
     nan = (float("nan"), 0.0, 0.0)
     with pytest.raises(PhysicsError):
         w.add_particle(nan, (0, 0, 0))
@@ -170,8 +186,8 @@ def test_bad_input_is_refused_and_changes_nothing(oracle_lib):
 
 # ---- step.rs tests ---------------------------------------------------------------------------
 
-def tank(oracle_lib, water, size, solver=FluidSolver.WCSPH, **kw):
-    w = world(oracle_lib, solver=solver, **kw)
+def tank(make, water, size, solver=FluidSolver.WCSPH, **kw):
+    w = make(solver=solver, **kw)
     w.add_box_container((0, 0, 0), size)
     w.fill_box((0, 0, 0), water)
     return w
@@ -182,11 +198,11 @@ def inside(w, size):
     return bool(np.all(p >= 0) and np.all(p <= np.asarray(size)))
 
 
-def test_still_water_stays_still_and_presses_by_its_depth(oracle_lib):
+def test_still_water_stays_still_and_presses_by_its_depth(backend):
     # src/fluid/step.rs:377-411
     size = (0.5, 0.6, 0.5)
     depth = 0.4
-    w = tank(oracle_lib, (0.5, depth, 0.5), size)
+    w = tank(backend, (0.5, depth, 0.5), size)
     count = w.len()
     held = 0
     last = None
@@ -207,11 +223,11 @@ def test_still_water_stays_still_and_presses_by_its_depth(oracle_lib):
     assert abs(top - (depth - 0.025)) < 0.05
 
 
-def test_a_column_collapses_but_never_outruns_the_ideal_front(oracle_lib):
+def test_a_column_collapses_but_never_outruns_the_ideal_front(backend):
     # src/fluid/step.rs:413-445
     size = (1.6, 0.6, 0.2)
     height = 0.4
-    w = tank(oracle_lib, (0.4, height, 0.2), size)
+    w = tank(backend, (0.4, height, 0.2), size)
     start = float(np.max(w.positions()[:, 0]))
     ideal = 2.0 * math.sqrt(9.81 * height)
     held = 0
@@ -243,14 +259,14 @@ def martin_moyce_table():
 
 
 @pytest.mark.slow
-def test_the_dam_break_front_follows_martin_and_moyce(oracle_lib):
+def test_the_dam_break_front_follows_martin_and_moyce(backend):
     # src/fluid/step.rs:462-507
     table = martin_moyce_table()
     if not table:
         pytest.skip("reference sources not present")
     width = 0.3
     spacing = np.float32(0.3) / np.float32(18.0)
-    w = world(oracle_lib, spacing=float(spacing))
+    w = backend(spacing=float(spacing))
     size = (3.2, 0.8, 0.1)
     w.add_box_container((0, 0, 0), size)
     w.fill_box((0, 0, 0), (width, 2 * width, 0.1))
@@ -275,9 +291,9 @@ def test_the_dam_break_front_follows_martin_and_moyce(oracle_lib):
     assert inside(w, size)
 
 
-def test_a_gate_holds_until_it_is_taken_away(oracle_lib):
+def test_a_gate_holds_until_it_is_taken_away(backend):
     # src/fluid/step.rs:509-532
-    w = tank(oracle_lib, (0.4, 0.4, 0.2), (1.2, 0.6, 0.2))
+    w = tank(backend, (0.4, 0.4, 0.2), (1.2, 0.6, 0.2))
     gate = w.add_wall((0.4, 0.0, 0.0), (0.5, 0.6, 0.2))
     for _ in range(30):
         w.step(TICK)
@@ -293,7 +309,7 @@ def test_a_gate_holds_until_it_is_taken_away(oracle_lib):
 def test_any_thread_count_ends_on_the_same_state(oracle_lib, solver):
     # src/fluid/step.rs:534-550
     def run(threads):
-        w = tank(oracle_lib, (0.3, 0.3, 0.2), (0.9, 0.5, 0.2), solver=solver)
+        w = tank(lambda **kw: world(oracle_lib, **kw), (0.3, 0.3, 0.2), (0.9, 0.5, 0.2), solver=solver)
         w.set_threads(threads)
         for _ in range(12):
             w.step(TICK)
@@ -305,21 +321,21 @@ def test_any_thread_count_ends_on_the_same_state(oracle_lib, solver):
     assert run(1) == one
 
 
-def test_bad_steps_are_refused_and_a_cap_is_reported(oracle_lib):
+def test_bad_steps_are_refused_and_a_cap_is_reported(backend):
     # src/fluid/step.rs:552-583
-    w = tank(oracle_lib, (0.2, 0.2, 0.2), (0.3, 0.3, 0.3))
+    w = tank(backend, (0.2, 0.2, 0.2), (0.3, 0.3, 0.3))
     with pytest.raises(PhysicsError):
         w.step(-1.0)
     with pytest.raises(PhysicsError):
         w.step(float("nan"))
     assert w.step(0.0).substeps == 0
-    tight = world(oracle_lib, max_substeps=2)
+    tight = backend(max_substeps=2)
     tight.fill_box((0, 0, 0), (0.1, 0.1, 0.1))
     r = tight.step(TICK)
     assert r.capped and r.substeps == 2
     for kw in [dict(sound_speed=0.0), dict(courant=1.5), dict(viscosity=-1.0)]:
         with pytest.raises(PhysicsError):
-            world(oracle_lib, **kw)
+            backend(**kw)
 
 
 def test_the_double_restatement_agrees_with_the_float_one_on_a_short_dam(oracle_lib):
