@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Throughput of solunar's particle-fluid substep on B200: one JSON line.
+
+Workload: the one-million-particle DFSPH dam break (100^3 particles at 0.01 m, support 2, in a
+2 x 1 x 1 m tank of boundary particles, jitter +-1e-5 m), advanced by FluidWorld::step(1e-3 s),
+which takes as many DFSPH substeps as the flow needs.  A timed step is one such call; `value`
+is substeps per second over all ranks, device-timed with CUDA events on the world's stream,
+with the particle state resident in HBM and L2 flushed (a 256 MiB write) before each step.
+`e2e` is the same metric through the C ABI with host-owned state: each step uploads positions
+and velocities from pinned host memory, steps, and reads them back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one independent replica per GPU under torchrun ("replicas only": the fluid step has
+no exchange between GPUs), value = all ranks' substeps / the slowest rank's time.
+`--impl reference` times the CPU restatement of the reference (the Rust reference cannot be
+built here) on the host cores, on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1M-particle DFSPH substeps/s: plain vs fwd+adjoint, 0.1% density err, 1 B200"
+UNIT = "substeps/s"
+FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scene", default="dfsph_dam_1m")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed CPU work in the baseline")
+    return ap.parse_args()
+
+
+def scene_of(name):
+    from solunar_b200 import scenes
+
+    return getattr(scenes, name)()
+
+
+def workload(sc) -> dict:
+    return {
+        "workload": f"{sc.name}: {sc.particles} particles ({'x'.join(map(str, sc.block_counts))} at "
+                    f"{sc.settings.spacing} m, support {sc.settings.support}) in a "
+                    f"{'x'.join(map(str, sc.tank))} m tank, {sc.settings.solver.name}, step({sc.dt}) per timed step",
+        "particles": sc.particles,
+        "solver": sc.settings.solver.name,
+        "arithmetic": sc.settings.arithmetic.name,
+        "positions": sc.settings.positions.name,
+        "l2": "flushed (256 MiB write) before every timed step",
+    }
+
+
+def peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def traffic_for(kernel: str, scene: str):
+    """DRAM bytes per launch of `kernel` at this workload, from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    entry = d.get(scene, {}).get(kernel)
+    return None if entry is None else float(entry["dram_bytes_per_launch"])
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_baseline(sc, budget_s: float, threads: int = 0) -> dict:
+    """The CPU restatement (OpenMP over all host cores) on a bounded sample of the workload."""
+    from oracle import py_oracle
+
+    py_oracle.build()
+    cores = threads or os.cpu_count()
+    w = py_oracle.OracleWorld(sc.settings, residual_sum=0, threads=cores)
+    sc.build(w)
+    w.update_neighbors()
+    substeps = 0
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        r = w.step(sc.dt)
+        substeps += r.substeps
+        steps += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": substeps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} steps ({substeps} substeps) of the {sc.particles}-particle scene from rest, "
+                      f"{dt:.1f} s on {cores} threads (C++ float restatement, OpenMP)"}
+
+
+def run_reference(args, rank: int, world_size: int):
+    if rank != 0:
+        return
+    sc = scene_of(args.scene)
+    from oracle import py_oracle
+
+    py_oracle.build()
+    cores = os.cpu_count()
+    w = py_oracle.OracleWorld(sc.settings, residual_sum=0, threads=cores)
+    sc.build(w)
+    w.update_neighbors()
+    budget = 150.0
+    t_start = time.perf_counter()
+    for _ in range(args.warmup):
+        w.step(sc.dt)
+        if time.perf_counter() - t_start > budget / 3:
+            break
+    substeps = 0
+    steps = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        substeps += w.step(sc.dt).substeps
+        steps += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - t0
+    value = substeps / dt
+    sample = (f"{steps} of {args.steps} timed steps ({substeps} substeps) of the {sc.particles}-particle scene, "
+              f"{dt:.1f} s on {cores} threads (C++ float restatement of the reference, OpenMP; the Rust "
+              f"reference has no toolchain here)")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world_size,
+           "steps": steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(steps, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "config": workload(sc),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world_size)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world_size > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world_size > 1:
+            dist.barrier(device_ids=[local_rank])
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world_size == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from solunar_b200 import fluid
+
+    sc = scene_of(args.scene)
+    sc.settings.device = local_rank
+    world = fluid.FluidWorld(sc.settings)
+    sc.build(world)
+    world.update_neighbors()
+    stream = torch.cuda.ExternalStream(world.stream(), device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    for _ in range(max(args.warmup, 3)):
+        world.step(sc.dt)
+
+    clocks = Clocks(local_rank)
+    clocks.start()
+    world.profile(True)
+    world.profile_reset()
+    launches0 = fluid.kernel_launches()
+    barrier()
+    times_ms = []
+    substeps = iterations = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = world.step(sc.dt)
+        e1.record(stream)
+        e1.synchronize()
+        times_ms.append(e0.elapsed_time(e1))
+        substeps += r.substeps
+        iterations += r.iterations
+    barrier()
+    launches = fluid.kernel_launches() - launches0
+    clock_info = clocks.stop()
+    prof = world.profile_read()
+    world.profile(False)
+
+    total_ms = max_over_ranks(sum(times_ms))
+    all_substeps = substeps * world_size
+    value = all_substeps / (total_ms / 1e3)
+
+    # roofline of the kernel with the largest share of device time
+    pk = peaks()
+    dominant = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (count, ms, abytes) = dominant
+    avg_ms = ms / max(count, 1)
+    per_launch = abytes / max(count, 1)
+    achieved = per_launch / (avg_ms / 1e3) / 1e9
+    traffic = traffic_for(name, sc.name)
+    kernel_ms = sum(v[1] for v in prof.values())
+    all_bytes = sum(v[2] for v in prof.values())
+    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"], "traffic": traffic,
+                "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": avg_ms,
+                "share_of_kernel_time": ms / kernel_ms if kernel_ms else None,
+                "substep_algorithmic_gbs": all_bytes / (sum(times_ms) / 1e3) / 1e9,
+                "kernels": {k: {"launches": v[0], "ms": v[1], "gbs": (v[2] / v[0]) / (v[1] / v[0] / 1e3) / 1e9
+                                if v[0] and v[1] else None} for k, v in prof.items()}}
+
+    # end to end through the C ABI with host-owned state in pinned memory
+    n = world.len()
+    host_pos = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    host_vel = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    world.read_positions_ptr(host_pos.data_ptr(), n)
+    world.read_velocities_ptr(host_vel.data_ptr(), n)
+    barrier()
+    e2e_ms = 0.0
+    e2e_substeps = 0
+    for _ in range(args.e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        world.write_state_ptr(host_pos.data_ptr(), host_vel.data_ptr(), n)
+        r = world.step(sc.dt)
+        world.read_positions_ptr(host_pos.data_ptr(), n)
+        world.read_velocities_ptr(host_vel.data_ptr(), n)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        e2e_substeps += r.substeps
+    barrier()
+    e2e_ms = max_over_ranks(e2e_ms)
+    e2e = {"value": e2e_substeps * world_size / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+           "d2h_bytes_per_step": 24 * n}
+
+    base = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        world.close()
+        base = cpu_baseline(sc, args.cpu_budget)
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+               "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": dict(workload(sc), parallelism=f"replicas x{world_size}",
+                              substeps=substeps, solver_iterations_per_substep=iterations / max(substeps, 1),
+                              particle_substeps_per_s=value * sc.particles),
+               "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "clocks": clock_info,
+               "gpu_launches": launches}
+        print(json.dumps(out), flush=True)
+    if world_size > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -77,6 +77,7 @@ typedef struct slf_settings {
     float density_tolerance;       /* dfsph.rs:9, 5e-4 */
     uint32_t min_iterations;       /* dfsph.rs:12, 2 */
     uint32_t max_iterations;       /* dfsph.rs:13, 100 */
+    int32_t device;                /* CUDA device ordinal of the world, 0 */
 } slf_settings;
 
 /* FluidReport (src/fluid/step.rs:27-49). */
@@ -188,10 +189,39 @@ int32_t slf_wall_neighbor_lists(slf_world* world, uint32_t* start, uint64_t star
 /* FluidWorld::state_hash (mod.rs:677-691), FNV-1a (src/snapshot/bytes.rs:6-13). */
 int32_t slf_state_hash(const slf_world* world, uint64_t* out);
 
+/* Overwrites the positions and velocities of the current particles, in the current order (the
+ * arrays FluidWorld::positions / velocities expose, mod.rs:397-403).  n must equal slf_len().
+ * A host that owns the particle arrays uploads them with this before a step. */
+int32_t slf_write_state(slf_world* world, const float* positions, const float* velocities,
+                        uint64_t n);
+
+/* The CUDA stream (a cudaStream_t) the world issues its work on, for callers that order their
+ * own work or events after a step. */
+int32_t slf_get_stream(const slf_world* world, void** stream);
+
 /* Message of the last failed call on any handle of this thread ("" if none). */
 const char* slf_last_error(void);
 
 /* ---- diagnostics and testing ------------------------------------------------------------ */
+
+/* Per-kernel device time.  While profiling is on, every launch of the world is bracketed by
+ * CUDA events on its stream; entries accumulate launches, milliseconds and the algorithmic
+ * bytes each launch must move (one read or write of each particle field it touches). */
+typedef struct slf_profile_entry {
+    char name[32];
+    uint64_t launches;
+    double milliseconds;
+    double algorithmic_bytes;
+} slf_profile_entry;
+
+int32_t slf_profile_enable(slf_world* world, int32_t on);
+/* Copies up to `capacity` entries; *count receives how many exist.  Resets nothing. */
+int32_t slf_profile_read(slf_world* world, slf_profile_entry* out, uint32_t capacity,
+                         uint32_t* count);
+int32_t slf_profile_reset(slf_world* world);
+
+/* Kernel launches this process has issued through the library so far. */
+int32_t slf_kernel_launches(uint64_t* out);
 
 /* DFSPH solver iterations of the last substep: divergence and density (the per-solve split of
  * FluidReport::iterations, src/fluid/dfsph.rs:89,100). */

@@ -68,6 +68,7 @@ class CSettings(ctypes.Structure):
         ("density_tolerance", ctypes.c_float),
         ("min_iterations", ctypes.c_uint32),
         ("max_iterations", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
     ]
 
 
@@ -107,6 +108,7 @@ class FluidSettings:
     density_tolerance: float = 5e-4
     min_iterations: int = 2
     max_iterations: int = 100
+    device: int = 0
 
     def radius(self) -> float:
         """FluidSettings::radius (mod.rs:120-122), in f32."""
@@ -132,6 +134,7 @@ class FluidSettings:
         c.density_tolerance = self.density_tolerance
         c.min_iterations = int(self.min_iterations)
         c.max_iterations = int(self.max_iterations)
+        c.device = int(self.device)
         return c
 
     @classmethod
@@ -154,6 +157,7 @@ class FluidSettings:
             density_tolerance=c.density_tolerance,
             min_iterations=c.min_iterations,
             max_iterations=c.max_iterations,
+            device=c.device,
         )
 
 
@@ -186,6 +190,15 @@ class FluidReport:
             lost=r.lost,
             sound_speed=r.sound_speed,
         )
+
+
+class CProfileEntry(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char * 32),
+        ("launches", ctypes.c_uint64),
+        ("milliseconds", ctypes.c_double),
+        ("algorithmic_bytes", ctypes.c_double),
+    ]
 
 
 def vec3(v) -> "ctypes.Array[ctypes.c_float]":

@@ -56,7 +56,23 @@ struct Status {
     double average;        // last average error (dfsph.rs:267)
     uint32_t processed;    // particles a neighbour pass visited (dispatch completeness)
     uint32_t ticket;       // block counter of the last-block reduction
-    uint32_t pad[2];
+    uint32_t list_max;     // longest neighbour list the last density pass found
+    uint32_t pad;
+};
+
+// Neighbour lists of one substep, built by the density pass in the reference's list order
+// (mod.rs:570-606) and read by every later pass of the substep.  Slot-major: entry k of
+// particle i sits at [k * stride + i], so a warp reading slot k of 32 particles reads one
+// contiguous run.  With each neighbour its kernel gradient factor g = slope(d) / d (0 at d = 0)
+// is kept: positions do not move within a substep (the reference keeps the whole gradient per
+// pair for the same reason, dfsph.rs:24-41), and gradient = offset * g rounds as
+// Kernel::gradient does (mod.rs:158-164).
+struct PairLists {
+    uint32_t cap;          // slots per particle
+    uint32_t stride;       // particles per slot row
+    uint32_t* idx;         // [cap][stride] neighbour indexes
+    float* g;              // [cap][stride] gradient factors
+    uint32_t* count;       // [stride] neighbours found; above cap the lists are incomplete
 };
 
 // ---- cell tables ----------------------------------------------------------------------------

@@ -6,6 +6,7 @@
 // the reference's sequential sums, bit for bit.  Grid-wide reductions (bounding box, fastest
 // particle, solver residual) are block trees feeding one atomic or one last-block finish per
 // launch; the residual is summed in double-double (compensated), deterministically.
+#include <atomic>
 #include <cfloat>
 #include <climits>
 
@@ -240,52 +241,63 @@ __global__ void k_scan_add(uint32_t* data, uint32_t m, const uint32_t* __restric
     if (blockIdx.x == 0 && threadIdx.x == 0) data[m] = tile_sums[gridDim.x];
 }
 
-// ---- densities (mod.rs:621-675), with WCSPH pressure (step.rs:147-172) or DFSPH factors ----
+// ---- densities (mod.rs:621-675) and the substep's neighbour lists, with WCSPH pressure
+// (step.rs:147-172) or the DFSPH factors (dfsph.rs:108-163) --------------------------------
 
 template <int SOLVER>
 __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDev wg, const float4* __restrict__ pos,
-                                                    const float4* __restrict__ walls, float* __restrict__ rho,
-                                                    float* __restrict__ press, float* __restrict__ scaled,
-                                                    float* __restrict__ alpha, uint32_t* __restrict__ crowd,
-                                                    Status* st) {
+                                                    const float4* __restrict__ walls, PairLists fl, PairLists wl,
+                                                    float* __restrict__ rho, float* __restrict__ press,
+                                                    float* __restrict__ scaled, float* __restrict__ alpha, Status* st) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < p.n;
-    uint32_t compressed = 0;
+    uint32_t compressed = 0, longest = 0;
     if (valid) {
         float4 a = pos[i];
         int3 cell = cell_of(p, a.x, a.y, a.z);
         float sum = 0.0f, wsum = 0.0f;
         float sx = 0.0f, sy = 0.0f, sz = 0.0f, squares = 0.0f;
         uint32_t nf = 0, nw = 0;
-        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
             float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             sum += kernel_value(p, d);
+            float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
+            if (nf < fl.cap) {
+                fl.idx[(size_t)nf * fl.stride + i] = j;
+                fl.g[(size_t)nf * fl.stride + i] = g;
+            }
+            ++nf;
             if (SOLVER == 1) {
-                // dfsph.rs:118 gradient(at - other), then factors (dfsph.rs:149-153)
+                // gradient(at - other) (dfsph.rs:118), then factors (dfsph.rs:149-153)
                 float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-                float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
                 float px = (rx * g) * p.mass, py = (ry * g) * p.mass, pz = (rz * g) * p.mass;
                 sx = sx + px;
                 sy = sy + py;
                 sz = sz + pz;
                 squares += dot3(px, py, pz, px, py, pz);
-                ++nf;
             }
         });
-        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
             float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             wsum += kernel_value(p, d);
+            float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
+            if (nw < wl.cap) {
+                wl.idx[(size_t)nw * wl.stride + i] = j;
+                wl.g[(size_t)nw * wl.stride + i] = g;
+            }
+            ++nw;
             if (SOLVER == 1) {
                 float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-                float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
                 sx = sx + (rx * g) * p.mass;
                 sy = sy + (ry * g) * p.mass;
                 sz = sz + (rz * g) * p.mass;
-                ++nw;
             }
         });
+        fl.count[i] = nf;
+        wl.count[i] = nw;
+        longest = nf > nw ? nf : nw;
         float density = p.mass * (sum + wsum);
         rho[i] = density;
         if (SOLVER == 0) {
@@ -296,24 +308,40 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
         } else {
             float total = dot3(sx, sy, sz, sx, sy, sz) + squares;
             alpha[i] = total > 0.0f ? 1.0f / total : 0.0f;
-            crowd[i] = nf + nw;
         }
         float c = density / p.rest - 1.0f;
         if (c > 0.0f) compressed = __float_as_uint(c);
     }
     compressed = block_reduce(compressed, MaxU(), 0u);
-    if (threadIdx.x == 0 && compressed) atomicMax(&st->maxcomp_bits, compressed);
+    longest = block_reduce(longest, MaxU(), 0u);
+    if (threadIdx.x == 0) {
+        if (compressed) atomicMax(&st->maxcomp_bits, compressed);
+        if (longest) atomicMax(&st->list_max, longest);
+    }
+}
+
+// Walks particle i's list: f(j, g) for each neighbour in list order.
+template <class F>
+__device__ __forceinline__ void each_listed(const PairLists& l, uint32_t i, F&& f) {
+    uint32_t n = l.count[i];
+    if (n > l.cap) n = l.cap;
+    const uint32_t* __restrict__ idx = l.idx + i;
+    const float* __restrict__ gg = l.g + i;
+    const size_t s = l.stride;
+#pragma unroll 2
+    for (uint32_t k = 0; k < n; ++k) f(__ldg(idx + k * s), __ldg(gg + k * s));
 }
 
 // ---- wall viscosity (step.rs:262-301, no terrains) ---------------------------------------
 
-__device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc, const GridDev& wg,
-                                               const float4* __restrict__ walls, int3 cell, float4 a, float4 v,
+__device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc, const PairLists& wl,
+                                               const float4* __restrict__ walls, uint32_t i, float4 a, float4 v,
                                                float density) {
+    if (wl.count[i] == 0) return make_float3(0.0f, 0.0f, 0.0f);
     float awx = 0.0f, awy = 0.0f, awz = 0.0f;
-    each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+    each_listed(wl, i, [&](uint32_t j, float g) {
+        float4 q = __ldg(&walls[j]);
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float g = kernel_gradient_factor(p, rx, ry, rz);
         awx = awx + -(rx * g);
         awy = awy + -(ry * g);
         awz = awz + -(rz * g);
@@ -329,13 +357,13 @@ __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc,
     float k = fminf(dot3(v.x, v.y, v.z, nx, ny, nz), 0.0f);
     float ix = nx * k, iy = ny * k, iz = nz * k;
     float px = 0.0f, py = 0.0f, pz = 0.0f;
-    each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+    each_listed(wl, i, [&](uint32_t j, float g) {
+        float4 q = __ldg(&walls[j]);
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float toward = dot3(ix, iy, iz, rx, ry, rz);
         if (toward < 0.0f) {
             float squeeze = toward / (dot3(rx, ry, rz, rx, ry, rz) + p.soften);
             float damp = -wall_visc * squeeze / density;
-            float g = kernel_gradient_factor(p, rx, ry, rz);
             float s = p.mass * damp;
             px = px - (rx * g) * s;
             py = py - (ry * g) * s;
@@ -375,8 +403,8 @@ __device__ __forceinline__ void advance_one(const Params& p, float dt, float4& a
 
 // ---- WCSPH: forces, velocity update and advance in one pass (step.rs:159-223, 305-339) -----
 
-__global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepConsts* __restrict__ sc, GridDev fg,
-                                                        GridDev wg, const float4* __restrict__ pos,
+__global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                        PairLists wl, const float4* __restrict__ pos,
                                                         const float4* __restrict__ vel, const float* __restrict__ rho,
                                                         const float* __restrict__ press,
                                                         const float* __restrict__ scaled,
@@ -394,14 +422,13 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepCons
         float4 v = vel[i];
         float density = rho[i];
         float own = scaled[i];
-        int3 cell = cell_of(p, a.x, a.y, a.z);
         float px = 0.0f, py = 0.0f, pz = 0.0f;
-        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+        each_listed(fl, i, [&](uint32_t j, float g) {
+            float4 q = __ldg(&pos[j]);
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
             float squared = dot3(rx, ry, rz, rx, ry, rz);
             if (squared <= 0.0f) return;
-            float distance = sqrtf(squared);
-            float g = kernel_slope(p, distance) / distance;
+            // g = slope(distance) / distance with distance = sqrt(squared) > 0
             float gx = rx * g, gy = ry * g, gz = rz * g;
             float4 w = __ldg(&vel[j]);
             float toward = fminf(dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx, ry, rz), 0.0f);
@@ -412,15 +439,15 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepCons
             pz = pz - gz * s;
         });
         float mirrored = own + press[i] / p.rest_sq;
-        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+        each_listed(wl, i, [&](uint32_t j, float g) {
+            float4 q = __ldg(&walls[j]);
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            float g = kernel_gradient_factor(p, rx, ry, rz);
             float s = p.mass * mirrored;
             px = px - (rx * g) * s;
             py = py - (ry * g) * s;
             pz = pz - (rz * g) * s;
         });
-        float3 wv = wall_viscous(p, sc->wall_viscosity, wg, walls, cell, a, v, density);
+        float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, i, a, v, density);
         float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
         v.x = v.x + ax * dt;
         v.y = v.y + ay * dt;
@@ -453,13 +480,13 @@ __device__ __forceinline__ DD dd_add(DD a, DD b) {
 // density_rate (dfsph.rs:166-181), then the solve's stiffness and error (dfsph.rs:241-259), and
 // the average error of the particles under load (dfsph.rs:263-268) in a last-block finish.
 template <int WHICH>
-__global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __restrict__ sc, GridDev fg,
-                                                 GridDev wg, const float4* __restrict__ pos,
+__global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                 PairLists wl, const float4* __restrict__ pos,
                                                  const float4* __restrict__ vel, const float* __restrict__ rho,
-                                                 const float* __restrict__ alpha, const uint32_t* __restrict__ crowd,
-                                                 const float4* __restrict__ walls, float* __restrict__ kappa,
-                                                 DD* __restrict__ partial, uint32_t* __restrict__ partial_loaded,
-                                                 Status* st, uint32_t iterations) {
+                                                 const float* __restrict__ alpha, const float4* __restrict__ walls,
+                                                 float* __restrict__ kappa, DD* __restrict__ partial,
+                                                 uint32_t* __restrict__ partial_loaded, Status* st,
+                                                 uint32_t iterations) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double err = 0.0;
     uint32_t loaded = 0;
@@ -467,17 +494,16 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
         const float dt = sc->dt;
         float4 a = pos[i];
         float4 v = vel[i];
-        int3 cell = cell_of(p, a.x, a.y, a.z);
         float rate = 0.0f;
-        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            float g = kernel_gradient_factor(p, rx, ry, rz);
+        each_listed(fl, i, [&](uint32_t j, float g) {
+            float4 q = __ldg(&pos[j]);
             float4 w = __ldg(&vel[j]);
+            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
             rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx * g, ry * g, rz * g);
         });
-        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+        each_listed(wl, i, [&](uint32_t j, float g) {
+            float4 q = __ldg(&walls[j]);
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            float g = kernel_gradient_factor(p, rx, ry, rz);
             rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
         });
         rate = rate * p.mass;
@@ -487,7 +513,7 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
             target = over / sc->dt_sq;
             error = over / p.rest;
         } else {
-            float r = crowd[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
+            float r = fl.count[i] + wl.count[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
             target = r / dt;
             error = dt * r / p.rest;
         }
@@ -554,27 +580,27 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
 }
 
 // push_apart (dfsph.rs:184-216): the velocity change from each particle's stiffness.
-__global__ void __launch_bounds__(kBlock) k_push(Params p, const StepConsts* __restrict__ sc, GridDev fg, GridDev wg,
-                                                 const float4* __restrict__ pos, float4* __restrict__ vel,
-                                                 const float* __restrict__ kappa, const float4* __restrict__ walls) {
+__global__ void __launch_bounds__(kBlock) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                 PairLists wl, const float4* __restrict__ pos,
+                                                 float4* __restrict__ vel, const float* __restrict__ kappa,
+                                                 const float4* __restrict__ walls) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const float dt = sc->dt;
     float4 a = pos[i];
-    int3 cell = cell_of(p, a.x, a.y, a.z);
     float own = kappa[i];
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+    each_listed(fl, i, [&](uint32_t j, float g) {
+        float4 q = __ldg(&pos[j]);
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float g = kernel_gradient_factor(p, rx, ry, rz);
         float s = p.mass * (own + __ldg(&kappa[j]));
         cx = cx - (rx * g) * s;
         cy = cy - (ry * g) * s;
         cz = cz - (rz * g) * s;
     });
-    each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+    each_listed(wl, i, [&](uint32_t j, float g) {
+        float4 q = __ldg(&walls[j]);
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float g = kernel_gradient_factor(p, rx, ry, rz);
         float s = p.mass * own;
         cx = cx - (rx * g) * s;
         cy = cy - (ry * g) * s;
@@ -589,10 +615,10 @@ __global__ void __launch_bounds__(kBlock) k_push(Params p, const StepConsts* __r
 
 // viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
 // because neighbours read the old velocities.
-__global__ void __launch_bounds__(kBlock) k_viscous(Params p, const StepConsts* __restrict__ sc, GridDev fg, GridDev wg,
-                                                    const float4* __restrict__ pos, const float4* __restrict__ vel,
-                                                    const float* __restrict__ rho, const float4* __restrict__ walls,
-                                                    float4* __restrict__ vel_out) {
+__global__ void __launch_bounds__(kBlock) k_viscous(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                    PairLists wl, const float4* __restrict__ pos,
+                                                    const float4* __restrict__ vel, const float* __restrict__ rho,
+                                                    const float4* __restrict__ walls, float4* __restrict__ vel_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const float dt = sc->dt;
@@ -600,24 +626,23 @@ __global__ void __launch_bounds__(kBlock) k_viscous(Params p, const StepConsts* 
     float4 a = pos[i];
     float4 v = vel[i];
     float density = rho[i];
-    int3 cell = cell_of(p, a.x, a.y, a.z);
     float px = 0.0f, py = 0.0f, pz = 0.0f;
-    each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+    each_listed(fl, i, [&](uint32_t j, float g) {
         if (j == i) return;
+        float4 q = __ldg(&pos[j]);
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float4 w = __ldg(&vel[j]);
         float toward = dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx, ry, rz);
         if (toward < 0.0f) {
             float squeeze = toward / (dot3(rx, ry, rz, rx, ry, rz) + p.soften);
             float damp = -visc * squeeze * 2.0f / (density + __ldg(&rho[j]));
-            float g = kernel_gradient_factor(p, rx, ry, rz);
             float s = p.mass * damp;
             px = px - (rx * g) * s;
             py = py - (ry * g) * s;
             pz = pz - (rz * g) * s;
         }
     });
-    float3 wv = wall_viscous(p, sc->wall_viscosity, wg, walls, cell, a, v, density);
+    float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, i, a, v, density);
     float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
     v.x = v.x + ax * dt;
     v.y = v.y + ay * dt;
@@ -695,9 +720,39 @@ __global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const u
 
 __global__ void k_set_consts(StepConsts c, StepConsts* out) { *out = c; }
 
+// xyz triples <-> float4, so host copies move 12 bytes a particle
+__global__ void k_pack3(uint32_t n, const float4* __restrict__ in, float* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = in[i];
+    out[3 * i] = v.x;
+    out[3 * i + 1] = v.y;
+    out[3 * i + 2] = v.z;
+}
+
+__global__ void k_unpack3(uint32_t n, const float* __restrict__ in, float4* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0f);
+}
+
 // ---- launchers ------------------------------------------------------------------------------
 
-static inline uint32_t blocks_for(uint32_t n) { return (n + kBlock - 1) / kBlock; }
+static std::atomic<uint64_t> g_launches{0};
+uint64_t kernel_launches() { return g_launches.load(); }
+
+static inline uint32_t blocks_for(uint32_t n) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return (n + kBlock - 1) / kBlock;
+}
+
+void launch_pack3(uint32_t n, const float4* in, float* out, cudaStream_t s) {
+    if (n) k_pack3<<<blocks_for(n), kBlock, 0, s>>>(n, in, out);
+}
+
+void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s) {
+    if (n) k_unpack3<<<blocks_for(n), kBlock, 0, s>>>(n, in, out);
+}
 
 void launch_state_stats(const Params& p, const float4* pos, const float4* vel, Status* st, cudaStream_t s) {
     if (p.n) k_state_stats<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, vel, st);
@@ -717,6 +772,7 @@ size_t scan_tiles(uint32_t m) { return (m + kScanTile - 1) / kScanTile; }
 void launch_exclusive_scan(uint32_t* data, uint32_t m, uint32_t* tile_sums, cudaStream_t s) {
     if (m == 0) return;
     uint32_t tiles = (uint32_t)scan_tiles(m);
+    g_launches.fetch_add(3, std::memory_order_relaxed);
     k_scan_tiles<<<tiles, kBlock, 0, s>>>(data, m, tile_sums);
     k_scan_sums<<<1, kBlock, 0, s>>>(tile_sums, tiles);
     k_scan_add<<<tiles, kBlock, 0, s>>>(data, m, tile_sums);
@@ -738,50 +794,49 @@ void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start,
 }
 
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
-                    float* rho, float* press, float* scaled, float* alpha, uint32_t* crowd, Status* st,
-                    cudaStream_t s) {
+                    const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
+                    Status* st, cudaStream_t s) {
     if (!p.n) return;
     if (p.solver == 0)
-        k_density<0><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, rho, press, scaled, alpha, crowd, st);
+        k_density<0><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st);
     else
-        k_density<1><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, rho, press, scaled, alpha, crowd, st);
+        k_density<1><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st);
 }
 
-void launch_wcsph_force(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg,
+void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                         const float4* pos, const float4* vel, const float* rho, const float* press,
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
                         cudaStream_t s) {
     if (p.n)
-        k_wcsph_force<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, rho, press, scaled, walls, pos_out,
+        k_wcsph_force<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled, walls, pos_out,
                                                          vel_out, st);
 }
 
-size_t rate_partial_bytes(uint32_t n) { return blocks_for(n) * (sizeof(DD) + sizeof(uint32_t)) + 64; }
+size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (sizeof(DD) + sizeof(uint32_t)) + 64; }
 
-void launch_rate(int which, const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg,
-                 const float4* pos, const float4* vel, const float* rho, const float* alpha, const uint32_t* crowd,
-                 const float4* walls, float* kappa, void* partials, Status* st, uint32_t iterations,
-                 cudaStream_t s) {
+void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                 const float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
+                 float* kappa, void* partials, Status* st, uint32_t iterations, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = blocks_for(p.n);
     DD* part = static_cast<DD*>(partials);
     uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
     if (which == 0)
-        k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, rho, alpha, crowd, walls, kappa, part, loaded, st,
+        k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kappa, part, loaded, st,
                                         iterations);
     else
-        k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, rho, alpha, crowd, walls, kappa, part, loaded, st,
+        k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kappa, part, loaded, st,
                                         iterations);
 }
 
-void launch_push(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg, const float4* pos,
+void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                  float4* vel, const float* kappa, const float4* walls, cudaStream_t s) {
-    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, kappa, walls);
+    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, kappa, walls);
 }
 
-void launch_viscous(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg, const float4* pos,
+void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                     const float4* vel, const float* rho, const float4* walls, float4* vel_out, cudaStream_t s) {
-    if (p.n) k_viscous<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fg, wg, pos, vel, rho, walls, vel_out);
+    if (p.n) k_viscous<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, walls, vel_out);
 }
 
 void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,
@@ -811,6 +866,9 @@ void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, cons
                                                    vel_out, rho_out);
 }
 
-void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s) { k_set_consts<<<1, 1, 0, s>>>(c, out); }
+void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k_set_consts<<<1, 1, 0, s>>>(c, out);
+}
 
 }  // namespace slf

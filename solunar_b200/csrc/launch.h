@@ -27,22 +27,21 @@ void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start,
                          const float* kap_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
                          float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, cudaStream_t s);
 
-// pair passes
+// pair passes: the density pass builds the substep's neighbour lists, the others walk them
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
-                    float* rho, float* press, float* scaled, float* alpha, uint32_t* crowd, Status* st,
-                    cudaStream_t s);
-void launch_wcsph_force(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg,
+                    const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
+                    Status* st, cudaStream_t s);
+void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                         const float4* pos, const float4* vel, const float* rho, const float* press,
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
                         cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
-void launch_rate(int which, const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg,
-                 const float4* pos, const float4* vel, const float* rho, const float* alpha, const uint32_t* crowd,
-                 const float4* walls, float* kappa, void* partials, Status* st, uint32_t iterations,
-                 cudaStream_t s);
-void launch_push(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg, const float4* pos,
+void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                 const float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
+                 float* kappa, void* partials, Status* st, uint32_t iterations, cudaStream_t s);
+void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                  float4* vel, const float* kappa, const float4* walls, cudaStream_t s);
-void launch_viscous(const Params& p, const StepConsts* sc, const GridDev& fg, const GridDev& wg, const float4* pos,
+void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                     const float4* vel, const float* rho, const float4* walls, float4* vel_out, cudaStream_t s);
 void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,
                     Status* st, cudaStream_t s);
@@ -60,5 +59,12 @@ void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, cons
                     float4* pos_out, float4* vel_out, float* rho_out, cudaStream_t s);
 
 void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s);
+
+// xyz triples <-> float4
+void launch_pack3(uint32_t n, const float4* in, float* out, cudaStream_t s);
+void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s);
+
+// kernels launched through this library by the process so far
+uint64_t kernel_launches();
 
 }  // namespace slf

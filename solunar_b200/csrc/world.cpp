@@ -119,6 +119,80 @@ struct ContainerBox {
     F3 low, high;
 };
 
+// Per-kernel device time from CUDA events bracketing each launch (while enabled).
+struct Profiler {
+    bool on = false;
+    std::vector<std::string> names;
+    std::vector<uint64_t> launches;
+    std::vector<double> ms, bytes;
+    struct Pending {
+        int kind;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+
+    int kind(const char* name) {
+        for (size_t i = 0; i < names.size(); ++i)
+            if (names[i] == name) return int(i);
+        names.emplace_back(name);
+        launches.push_back(0);
+        ms.push_back(0.0);
+        bytes.push_back(0.0);
+        return int(names.size() - 1);
+    }
+    cudaEvent_t take() {
+        if (pool.empty()) {
+            cudaEvent_t e = nullptr;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    // after a synchronisation of the stream: every pending pair has completed
+    void collect() {
+        for (auto& p : pending) {
+            float t = 0.0f;
+            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) {
+                ms[p.kind] += t;
+                launches[p.kind] += 1;
+                bytes[p.kind] += p.bytes;
+            }
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void reset() {
+        for (size_t i = 0; i < names.size(); ++i) {
+            launches[i] = 0;
+            ms[i] = 0.0;
+            bytes[i] = 0.0;
+        }
+    }
+    ~Profiler() {
+        for (auto& p : pending) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+// Algorithmic bytes a particle costs in each kernel: one read or write of every particle field
+// the pass must touch, neighbour gathers served on chip not counted (f32 fields, 12-byte
+// vectors).  The spatial hash's 72 bytes (read position, velocity, id; write them sorted; write
+// and read the cell key) are split over its kernels.
+namespace bytes_per_particle {
+constexpr double count_cells = 20, scan = 2, scatter = 8, reorder = 44;
+constexpr double density_wcsph = 16, density_dfsph = 20, wcsph_force = 52;
+constexpr double rate_divergence = 32, rate_density = 36, push = 40, viscosity = 40, advance = 48;
+constexpr double stats = 24;
+}  // namespace bytes_per_particle
+
 }  // namespace
 
 struct World {
@@ -136,7 +210,11 @@ struct World {
     DevBuf<uint32_t> ids[2];
     DevBuf<float> rho[2];
     DevBuf<float> press, scaled, alpha, kappa;
-    DevBuf<uint32_t> crowd, lin, cslot, members, count, tiles, keep;
+    DevBuf<uint32_t> lin, cslot, members, count, tiles, keep;
+    // neighbour lists of the current substep (fluid and walls)
+    DevBuf<uint32_t> fidx, widx, fcnt, wcnt;
+    DevBuf<float> fgv, wgv;
+    uint32_t list_cap = 0;
     DevBuf<uint8_t> partials;
     bool stats_fresh = false;  // status holds bbox and speed of the committed state
 
@@ -167,14 +245,36 @@ struct World {
     StepConsts* d_consts = nullptr;
 
     int64_t skip_job = -1;  // testing: next sort leaves this 512-particle job undone
+    Profiler prof;
+    DevBuf<float> stage;  // xyz triples for host copies
+
+    template <class F> void timed(const char* name, double per_particle, F&& f) {
+        if (!prof.on) {
+            f();
+            return;
+        }
+        Profiler::Pending pd{prof.kind(name), prof.take(), prof.take(), per_particle * double(n)};
+        cudaEventRecord(pd.a, stream);
+        f();
+        cudaEventRecord(pd.b, stream);
+        prof.pending.push_back(pd);
+    }
+
+    int32_t sync() {
+        SLF_CUDA(cudaStreamSynchronize(stream));
+        prof.collect();
+        return SLF_OK;
+    }
 
     ~World() {
         if (stream) {
             for (auto* b : {&pos[0], &pos[1], &pos[2], &vel[0], &vel[1], &vel[2]}) b->release(stream);
-            for (auto* b : {&ids[0], &ids[1], &crowd, &lin, &cslot, &members, &count, &tiles, &keep, &dwstart})
+            for (auto* b : {&ids[0], &ids[1], &lin, &cslot, &members, &count, &tiles, &keep, &dwstart, &fidx, &widx,
+                            &fcnt, &wcnt})
                 b->release(stream);
-            for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha, &kappa}) b->release(stream);
+            for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha, &kappa, &fgv, &wgv}) b->release(stream);
             partials.release(stream);
+            stage.release(stream);
             dwalls.release(stream);
             dwkeys.release(stream);
             cudaStreamSynchronize(stream);
@@ -217,6 +317,11 @@ struct World {
         HostKernel k(radius);
         scale = k.scale;
         mass = rest_mass();
+        // lists hold half again the neighbours of a rest lattice, plus slack; a longer one makes
+        // the substep run again with more room
+        double expected = 4.0 / 3.0 * 3.14159265358979 * double(s.support) * s.support * s.support;
+        list_cap = (uint32_t(expected * 1.5 + 16.0) + 7u) & ~7u;
+        SLF_CUDA(cudaSetDevice(s.device));
         SLF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         SLF_CUDA(cudaMalloc(&d_status, sizeof(Status)));
         SLF_CUDA(cudaMalloc(&d_consts, sizeof(StepConsts)));
@@ -357,12 +462,30 @@ struct World {
         SLF_TRY(scaled.ensure(n, 0, stream));
         SLF_TRY(alpha.ensure(n, 0, stream));
         SLF_TRY(kappa.ensure(n, 0, stream));
-        SLF_TRY(crowd.ensure(n, 0, stream));
+        size_t slots = size_t(list_cap) * n;
+        SLF_TRY(fidx.ensure(slots, 0, stream));
+        SLF_TRY(fgv.ensure(slots, 0, stream));
+        SLF_TRY(widx.ensure(slots, 0, stream));
+        SLF_TRY(wgv.ensure(slots, 0, stream));
+        SLF_TRY(fcnt.ensure(n, 0, stream));
+        SLF_TRY(wcnt.ensure(n, 0, stream));
         SLF_TRY(lin.ensure(n, 0, stream));
         SLF_TRY(cslot.ensure(n, 0, stream));
         SLF_TRY(members.ensure(n, 0, stream));
         SLF_TRY(partials.ensure(rate_partial_bytes(uint32_t(n)), 0, stream));
         return SLF_OK;
+    }
+
+    PairLists fluid_lists() const { return PairLists{list_cap, uint32_t(n), fidx.p, fgv.p, fcnt.p}; }
+    PairLists wall_lists() const { return PairLists{list_cap, uint32_t(n), widx.p, wgv.p, wcnt.p}; }
+
+    // After a density pass: a list longer than its room leaves the substep to be run again.
+    static constexpr int32_t kRetry = -1;
+    int32_t lists_fit() {
+        if (h_status->list_max <= list_cap) return SLF_OK;
+        list_cap = (uint32_t(h_status->list_max) + h_status->list_max / 4 + 15u) & ~7u;
+        SLF_TRY(ensure_work_buffers());
+        return kRetry;
     }
 
     // ---- walls (src/fluid/boundary.rs) -------------------------------------------------------
@@ -590,8 +713,7 @@ struct World {
 
     int32_t read_status() {
         SLF_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(Status), cudaMemcpyDeviceToHost, stream));
-        SLF_CUDA(cudaStreamSynchronize(stream));
-        return SLF_OK;
+        return sync();
     }
 
     // Clears the per-substep fields; the box starts empty.
@@ -609,7 +731,7 @@ struct World {
         if (stats_fresh) return SLF_OK;
         SLF_TRY(reset_status());
         Params p = params();
-        launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream);
+        timed("stats", bytes_per_particle::stats, [&] { launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream); });
         SLF_TRY(read_status());
         stats_fresh = true;
         return SLF_OK;
@@ -642,18 +764,23 @@ struct World {
         SLF_CUDA(cudaMemsetAsync(count.p, 0, (size_t(volume) + 1) * 4, stream));
         int3 lo3 = make_int3(int(lo[0]), int(lo[1]), int(lo[2]));
         int3 sp3 = make_int3(int(span[0]), int(span[1]), int(span[2]));
-        launch_count_cells(p, pos[cpos].p, lo3, sp3, count.p, lin.p, cslot.p, stream);
-        launch_exclusive_scan(count.p, volume, tiles.p, stream);
-        launch_scatter_members(uint32_t(n), lin.p, cslot.p, count.p, ids[cid].p, members.p, stream);
+        timed("hash_count", bytes_per_particle::count_cells,
+              [&] { launch_count_cells(p, pos[cpos].p, lo3, sp3, count.p, lin.p, cslot.p, stream); });
+        timed("hash_scan", bytes_per_particle::scan, [&] { launch_exclusive_scan(count.p, volume, tiles.p, stream); });
+        timed("hash_scatter", bytes_per_particle::scatter, [&] {
+            launch_scatter_members(uint32_t(n), lin.p, cslot.p, count.p, ids[cid].p, members.p, stream);
+        });
         uint32_t job_lo = 0, job_hi = 0;
         if (skip_job >= 0) {
             job_lo = uint32_t(skip_job) * 512u;
             job_hi = job_lo + 512u;
             skip_job = -1;
         }
-        launch_rank_reorder(uint32_t(n), lin.p, count.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p,
-                            rho[cid].p, nullptr, ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, nullptr,
-                            job_lo, job_hi, d_status, stream);
+        timed("hash_reorder", bytes_per_particle::reorder, [&] {
+            launch_rank_reorder(uint32_t(n), lin.p, count.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p,
+                                rho[cid].p, nullptr, ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, nullptr,
+                                job_lo, job_hi, d_status, stream);
+        });
         fgrid = GridDev{};
         fgrid.mode = 1;
         fgrid.lx = lo3.x;
@@ -700,10 +827,15 @@ struct World {
         SLF_TRY(ensure_work_buffers());
         SLF_TRY(upload_walls());
         Params p = params();
-        launch_density(p, fgrid, wgrid, pos[cpos].p, dwalls.p, rho[cid].p, press.p, scaled.p, alpha.p, crowd.p,
-                       d_status, stream);
-        SLF_CUDA(cudaStreamSynchronize(stream));
-        return SLF_OK;
+        for (;;) {
+            SLF_TRY(reset_status());
+            launch_density(p, fgrid, wgrid, pos[cpos].p, dwalls.p, fluid_lists(), wall_lists(), rho[cid].p, press.p,
+                           scaled.p, alpha.p, d_status, stream);
+            SLF_TRY(read_status());
+            int32_t st = lists_fit();
+            if (st == SLF_OK) return SLF_OK;
+            if (st != kRetry) return st;
+        }
     }
 
     // ---- substeps ----------------------------------------------------------------------------
@@ -714,13 +846,19 @@ struct World {
         int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
         SLF_TRY(sort_into(a));
         int nid = 1 - cid;
-        launch_set_consts(consts(dt), d_consts, stream);
-        launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, rho[nid].p, press.p, scaled.p, alpha.p, crowd.p,
-                       d_status, stream);
         SLF_TRY(reset_status());
-        launch_wcsph_force(p, d_consts, fgrid, wgrid, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
-                           pos[b].p, vel[b].p, d_status, stream);
+        launch_set_consts(consts(dt), d_consts, stream);
+        PairLists fl = fluid_lists(), wl = wall_lists();
+        timed("density", bytes_per_particle::density_wcsph, [&] {
+            launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rho[nid].p, press.p, scaled.p, alpha.p,
+                           d_status, stream);
+        });
+        timed("wcsph_force_advance", bytes_per_particle::wcsph_force, [&] {
+            launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
+                               pos[b].p, vel[b].p, d_status, stream);
+        });
         SLF_TRY(read_status());
+        SLF_TRY(lists_fit());
         if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
         held = h_status->held;
         cpos = b;
@@ -735,15 +873,20 @@ struct World {
     // solve (dfsph.rs:222-275): Jacobi iterations until the average error is under tolerance.
     int32_t solve(int which, const Params& p, int a, float4* v, int nid, uint32_t& iterations) {
         iterations = 0;
+        PairLists fl = fluid_lists(), wl = wall_lists();
         for (;;) {
-            launch_rate(which, p, d_consts, fgrid, wgrid, pos[a].p, v, rho[nid].p, alpha.p, crowd.p, dwalls.p,
-                        kappa.p, partials.p, d_status, iterations, stream);
-            SLF_CUDA(cudaMemcpyAsync(&h_status->settled, &d_status->settled, 4, cudaMemcpyDeviceToHost, stream));
-            SLF_CUDA(cudaStreamSynchronize(stream));
+            timed(which == 0 ? "rate_divergence" : "rate_density",
+                  which == 0 ? bytes_per_particle::rate_divergence : bytes_per_particle::rate_density, [&] {
+                      launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, kappa.p,
+                                  partials.p, d_status, iterations, stream);
+                  });
+            SLF_TRY(read_status());
+            SLF_TRY(lists_fit());
             if (h_status->settled) return SLF_OK;
             // the device stops the loop at max_iterations; past that its flag was not written
             if (iterations > s.max_iterations) return fail(SLF_ERR_TIMEOUT, "solver stop flag never set");
-            launch_push(p, d_consts, fgrid, wgrid, pos[a].p, v, kappa.p, dwalls.p, stream);
+            timed(which == 0 ? "push_divergence" : "push_density", bytes_per_particle::push,
+                  [&] { launch_push(p, d_consts, fl, wl, pos[a].p, v, kappa.p, dwalls.p, stream); });
             iterations += 1;
         }
     }
@@ -754,15 +897,21 @@ struct World {
         int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
         SLF_TRY(sort_into(a));
         int nid = 1 - cid;
+        SLF_TRY(reset_status());
         launch_set_consts(consts(dt), d_consts, stream);
-        launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, rho[nid].p, press.p, scaled.p, alpha.p, crowd.p,
-                       d_status, stream);
+        PairLists fl = fluid_lists(), wl = wall_lists();
+        timed("density_alpha", bytes_per_particle::density_dfsph, [&] {
+            launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rho[nid].p, press.p, scaled.p, alpha.p,
+                           d_status, stream);
+        });
         uint32_t div_it = 0, den_it = 0;
         SLF_TRY(solve(0, p, a, vel[a].p, nid, div_it));
-        launch_viscous(p, d_consts, fgrid, wgrid, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
+        timed("viscosity", bytes_per_particle::viscosity, [&] {
+            launch_viscous(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
+        });
         SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it));
-        SLF_TRY(reset_status());
-        launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, stream);
+        timed("advance", bytes_per_particle::advance,
+              [&] { launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, stream); });
         SLF_TRY(read_status());
         if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
         held = h_status->held;
@@ -802,7 +951,10 @@ struct World {
                 float small = dt / float(substeps);
                 for (uint32_t i = 0; i < substeps; ++i) {
                     uint32_t held = 0;
-                    SLF_TRY(wcsph_substep(small, held));
+                    int32_t st = wcsph_substep(small, held);
+                    if (st == kRetry) st = wcsph_substep(small, held);
+                    if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
+                    SLF_TRY(st);
                     r.held_back += held;
                 }
                 r.substeps = substeps;
@@ -821,7 +973,10 @@ struct World {
                     }
                     small = rmin(small, left);
                     uint32_t held = 0, its = 0;
-                    SLF_TRY(dfsph_substep(small, held, its));
+                    int32_t st = dfsph_substep(small, held, its);
+                    if (st == kRetry) st = dfsph_substep(small, held, its);
+                    if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
+                    SLF_TRY(st);
                     r.iterations += its;
                     r.held_back += held;
                     r.substeps += 1;
@@ -835,8 +990,10 @@ struct World {
         if (n > 0) {
             SLF_TRY(reset_status());
             Params p = params();
-            launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream);
-            launch_max_compression(p, rho[cid].p, d_status, stream);
+            timed("stats", bytes_per_particle::stats, [&] {
+                launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream);
+                launch_max_compression(p, rho[cid].p, d_status, stream);
+            });
             SLF_TRY(read_status());
             stats_fresh = true;
             std::memcpy(&r.max_speed, &h_status->vmax_bits, 4);
@@ -877,17 +1034,34 @@ struct World {
 
     // ---- read-outs -------------------------------------------------------------------------
 
+    // packs xyz on the device and copies 12 bytes a particle straight into the caller's buffer
     int32_t read_vec(const DevBuf<float4>& b, float* out, uint64_t k) {
-        std::vector<float4> tmp(k);
-        if (k) {
-            SLF_CUDA(cudaMemcpyAsync(tmp.data(), b.p, k * sizeof(float4), cudaMemcpyDeviceToHost, stream));
-            SLF_CUDA(cudaStreamSynchronize(stream));
-        }
-        for (uint64_t i = 0; i < k; ++i) {
-            out[3 * i] = tmp[i].x;
-            out[3 * i + 1] = tmp[i].y;
-            out[3 * i + 2] = tmp[i].z;
-        }
+        if (!k) return SLF_OK;
+        SLF_TRY(stage.ensure(3 * k, 0, stream));
+        launch_pack3(uint32_t(k), b.p, stage.p, stream);
+        SLF_CUDA(cudaMemcpyAsync(out, stage.p, k * 12, cudaMemcpyDeviceToHost, stream));
+        return sync();
+    }
+
+    int32_t write_vec(DevBuf<float4>& b, const float* in, uint64_t k) {
+        if (!k) return SLF_OK;
+        SLF_TRY(stage.ensure(3 * k, 0, stream));
+        SLF_CUDA(cudaMemcpyAsync(stage.p, in, k * 12, cudaMemcpyHostToDevice, stream));
+        launch_unpack3(uint32_t(k), stage.p, b.p, stream);
+        return SLF_OK;
+    }
+
+    int32_t write_state(const float* p, const float* v, uint64_t k) {
+        SLF_TRY(flush());
+        if (k != n) return fail(SLF_ERR_INVALID_ARGUMENT, "n must equal slf_len()");
+        for (uint64_t i = 0; i < k; ++i)
+            if (!finite3(p + 3 * i) || !finite3(v + 3 * i))
+                return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        SLF_TRY(write_vec(pos[cpos], p, k));
+        SLF_TRY(write_vec(vel[cpos], v, k));
+        SLF_TRY(sync());
+        lists_valid = false;
+        stats_fresh = false;
         return SLF_OK;
     }
 
@@ -978,6 +1152,14 @@ struct slf_world {
         if (!(ptr)) return fail(SLF_ERR_INVALID_ARGUMENT, "null argument: " #ptr);  \
     } while (0)
 
+// Every call on a world runs on that world's device.
+#define SLF_WORLD(world)                                                                          \
+    do {                                                                                          \
+        SLF_NEED(world);                                                                          \
+        cudaError_t e_ = cudaSetDevice((world)->w.s.device);                                      \
+        if (e_ != cudaSuccess) return fail(SLF_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
 extern "C" {
 
 int32_t slf_settings_default(slf_settings* out) {
@@ -1002,6 +1184,7 @@ int32_t slf_settings_default(slf_settings* out) {
     s.density_tolerance = 5e-4f;
     s.min_iterations = 2;
     s.max_iterations = 100;
+    s.device = 0;
     *out = s;
     return SLF_OK;
 }
@@ -1017,6 +1200,8 @@ int32_t slf_create(const slf_settings* settings, slf_world** out) {
     int devices = 0;
     if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
         return fail(SLF_ERR_CUDA, "no CUDA device");
+    if (settings->device < 0 || settings->device >= devices)
+        return fail(SLF_ERR_INVALID_SETTINGS, "no such CUDA device");
     auto h = std::make_unique<slf_world>();
     int32_t st = h->w.init(*settings);
     if (st != SLF_OK) return st;
@@ -1024,38 +1209,42 @@ int32_t slf_create(const slf_settings* settings, slf_world** out) {
     return SLF_OK;
 }
 
-void slf_destroy(slf_world* world) { delete world; }
+void slf_destroy(slf_world* world) {
+    if (!world) return;
+    cudaSetDevice(world->w.s.device);
+    delete world;
+}
 
 int32_t slf_get_settings(const slf_world* world, slf_settings* out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(out);
     *out = world->w.s;
     return SLF_OK;
 }
 
 int32_t slf_particle_mass(const slf_world* world, float* out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(out);
     *out = world->w.mass;
     return SLF_OK;
 }
 
 int32_t slf_kernel(const slf_world* world, float* radius, float* scale) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     if (radius) *radius = world->w.radius;
     if (scale) *scale = world->w.scale;
     return SLF_OK;
 }
 
 int32_t slf_len(const slf_world* world, uint64_t* out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(out);
     *out = world->w.total();
     return SLF_OK;
 }
 
 int32_t slf_add_particle(slf_world* world, const float position[3], const float velocity[3], uint32_t* id_out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(position);
     SLF_NEED(velocity);
     return world->w.add(1, position, velocity, id_out);
@@ -1063,7 +1252,7 @@ int32_t slf_add_particle(slf_world* world, const float position[3], const float 
 
 int32_t slf_add_particles(slf_world* world, uint64_t n, const float* positions, const float* velocities,
                           uint32_t* ids_out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     if (n == 0) return SLF_OK;
     SLF_NEED(positions);
     SLF_NEED(velocities);
@@ -1071,14 +1260,14 @@ int32_t slf_add_particles(slf_world* world, uint64_t n, const float* positions, 
 }
 
 int32_t slf_fill_box(slf_world* world, const float low[3], const float high[3], uint64_t* count_out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(low);
     SLF_NEED(high);
     return world->w.fill_box(low, high, count_out);
 }
 
 int32_t slf_set_domain(slf_world* world, const float* low, const float* high) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     World& w = world->w;
     if (!low && !high) {
         w.has_domain = false;
@@ -1096,35 +1285,35 @@ int32_t slf_set_domain(slf_world* world, const float* low, const float* high) {
 }
 
 int32_t slf_add_box_container(slf_world* world, const float low[3], const float high[3], uint32_t* boundary_out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(low);
     SLF_NEED(high);
     return world->w.add_box_container(low, high, boundary_out);
 }
 
 int32_t slf_add_wall(slf_world* world, const float low[3], const float high[3], uint32_t* boundary_out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(low);
     SLF_NEED(high);
     return world->w.add_wall(low, high, boundary_out);
 }
 
 int32_t slf_remove_boundary(slf_world* world, uint32_t boundary, int32_t* removed) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     bool gone = world->w.remove_boundary(boundary);
     if (removed) *removed = gone ? 1 : 0;
     return SLF_OK;
 }
 
 int32_t slf_wall_count(const slf_world* world, uint64_t* out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(out);
     *out = world->w.wpos.size();
     return SLF_OK;
 }
 
 int32_t slf_read_wall_positions(const slf_world* world, float* out, uint64_t n) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     const World& w = world->w;
     if (n != w.wpos.size()) return fail(SLF_ERR_INVALID_ARGUMENT, "n must equal the wall count");
     if (n) SLF_NEED(out);
@@ -1137,17 +1326,17 @@ int32_t slf_read_wall_positions(const slf_world* world, float* out, uint64_t n) 
 }
 
 int32_t slf_step(slf_world* world, float dt, slf_report* out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     return world->w.step(dt, out);
 }
 
 int32_t slf_update_neighbors(slf_world* world) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     return world->w.update_neighbors();
 }
 
 int32_t slf_compute_densities(slf_world* world) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     return world->w.compute_densities();
 }
 
@@ -1160,7 +1349,7 @@ static int32_t prep_read(const slf_world* world, uint64_t n) {
 }
 
 int32_t slf_read_ids(const slf_world* world, uint32_t* out, uint64_t n) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_TRY(prep_read(world, n));
     if (n) SLF_NEED(out);
     World& w = const_cast<World&>(world->w);
@@ -1168,7 +1357,7 @@ int32_t slf_read_ids(const slf_world* world, uint32_t* out, uint64_t n) {
 }
 
 int32_t slf_read_positions(const slf_world* world, float* out, uint64_t n) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_TRY(prep_read(world, n));
     if (n) SLF_NEED(out);
     World& w = const_cast<World&>(world->w);
@@ -1176,7 +1365,7 @@ int32_t slf_read_positions(const slf_world* world, float* out, uint64_t n) {
 }
 
 int32_t slf_read_velocities(const slf_world* world, float* out, uint64_t n) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_TRY(prep_read(world, n));
     if (n) SLF_NEED(out);
     World& w = const_cast<World&>(world->w);
@@ -1184,7 +1373,7 @@ int32_t slf_read_velocities(const slf_world* world, float* out, uint64_t n) {
 }
 
 int32_t slf_read_densities(const slf_world* world, float* out, uint64_t n) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_TRY(prep_read(world, n));
     if (n) SLF_NEED(out);
     World& w = const_cast<World&>(world->w);
@@ -1193,18 +1382,18 @@ int32_t slf_read_densities(const slf_world* world, float* out, uint64_t n) {
 
 int32_t slf_neighbor_lists(slf_world* world, uint32_t* start, uint64_t start_len, uint32_t* items,
                            uint64_t items_capacity, uint64_t* items_len) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     return world->w.lists(false, start, start_len, items, items_capacity, items_len);
 }
 
 int32_t slf_wall_neighbor_lists(slf_world* world, uint32_t* start, uint64_t start_len, uint32_t* items,
                                 uint64_t items_capacity, uint64_t* items_len) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     return world->w.lists(true, start, start_len, items, items_capacity, items_len);
 }
 
 int32_t slf_state_hash(const slf_world* world, uint64_t* out) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     SLF_NEED(out);
     World& w = const_cast<World&>(world->w);
     SLF_TRY(w.flush());
@@ -1220,14 +1409,71 @@ int32_t slf_state_hash(const slf_world* world, uint64_t* out) {
 
 const char* slf_last_error(void) { return slf::g_error.c_str(); }
 
+int32_t slf_write_state(slf_world* world, const float* positions, const float* velocities, uint64_t n) {
+    SLF_WORLD(world);
+    if (n) {
+        SLF_NEED(positions);
+        SLF_NEED(velocities);
+    }
+    return world->w.write_state(positions, velocities, n);
+}
+
+int32_t slf_get_stream(const slf_world* world, void** stream) {
+    SLF_WORLD(world);
+    SLF_NEED(stream);
+    *stream = world->w.stream;
+    return SLF_OK;
+}
+
+int32_t slf_profile_enable(slf_world* world, int32_t on) {
+    SLF_WORLD(world);
+    World& w = world->w;
+    SLF_CUDA(cudaStreamSynchronize(w.stream));
+    w.prof.collect();
+    w.prof.on = on != 0;
+    return SLF_OK;
+}
+
+int32_t slf_profile_read(slf_world* world, slf_profile_entry* out, uint32_t capacity, uint32_t* count) {
+    SLF_WORLD(world);
+    World& w = world->w;
+    SLF_CUDA(cudaStreamSynchronize(w.stream));
+    w.prof.collect();
+    if (count) *count = uint32_t(w.prof.names.size());
+    for (uint32_t i = 0; i < capacity && i < w.prof.names.size(); ++i) {
+        slf_profile_entry e{};
+        std::snprintf(e.name, sizeof(e.name), "%s", w.prof.names[i].c_str());
+        e.launches = w.prof.launches[i];
+        e.milliseconds = w.prof.ms[i];
+        e.algorithmic_bytes = w.prof.bytes[i];
+        out[i] = e;
+    }
+    return SLF_OK;
+}
+
+int32_t slf_profile_reset(slf_world* world) {
+    SLF_WORLD(world);
+    World& w = world->w;
+    SLF_CUDA(cudaStreamSynchronize(w.stream));
+    w.prof.collect();
+    w.prof.reset();
+    return SLF_OK;
+}
+
+int32_t slf_kernel_launches(uint64_t* out) {
+    SLF_NEED(out);
+    *out = slf::kernel_launches();
+    return SLF_OK;
+}
+
 int32_t slf_debug_skip_job(slf_world* world, int64_t job) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     world->w.skip_job = job;
     return SLF_OK;
 }
 
 int32_t slf_last_iterations(const slf_world* world, uint32_t* divergence, uint32_t* density) {
-    SLF_NEED(world);
+    SLF_WORLD(world);
     if (divergence) *divergence = world->w.last_iterations[0];
     if (density) *density = world->w.last_iterations[1];
     return SLF_OK;

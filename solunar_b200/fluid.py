@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from .abi import CReport, CSettings, FluidReport, FluidSettings, PhysicsError, vec3
+from .abi import CProfileEntry, CReport, CSettings, FluidReport, FluidSettings, PhysicsError, vec3
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_NAME = "libsolunar_fluid.so"
@@ -67,6 +67,12 @@ def load_library():
         "slf_state_hash": [vp, u64p],
         "slf_last_iterations": [vp, u32p, u32p],
         "slf_debug_skip_job": [vp, ctypes.c_int64],
+        "slf_write_state": [vp, fp, fp, ctypes.c_uint64],
+        "slf_get_stream": [vp, ctypes.POINTER(vp)],
+        "slf_profile_enable": [vp, ctypes.c_int32],
+        "slf_profile_read": [vp, ctypes.POINTER(CProfileEntry), ctypes.c_uint32, u32p],
+        "slf_profile_reset": [vp],
+        "slf_kernel_launches": [u64p],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -269,3 +275,48 @@ class FluidWorld:
         v = ctypes.c_uint64()
         _check(_lib.slf_state_hash(self._h, ctypes.byref(v)))
         return v.value
+
+    # ---- host-owned state, streams, profiling ----
+    def write_state(self, positions, velocities):
+        """Overwrites positions and velocities of the current particles (current order)."""
+        p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+        v = np.ascontiguousarray(velocities, dtype=np.float32).reshape(-1, 3)
+        _check(_lib.slf_write_state(self._h, _ptr(p, ctypes.c_float), _ptr(v, ctypes.c_float), len(p)))
+
+    def write_state_ptr(self, positions_ptr: int, velocities_ptr: int, n: int):
+        """write_state from raw host pointers (pinned buffers)."""
+        fp = ctypes.POINTER(ctypes.c_float)
+        _check(_lib.slf_write_state(self._h, ctypes.cast(positions_ptr, fp), ctypes.cast(velocities_ptr, fp), n))
+
+    def read_positions_ptr(self, ptr: int, n: int):
+        _check(_lib.slf_read_positions(self._h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)), n))
+
+    def read_velocities_ptr(self, ptr: int, n: int):
+        _check(_lib.slf_read_velocities(self._h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)), n))
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(_lib.slf_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def profile(self, on: bool = True):
+        _check(_lib.slf_profile_enable(self._h, 1 if on else 0))
+
+    def profile_reset(self):
+        _check(_lib.slf_profile_reset(self._h))
+
+    def profile_read(self) -> dict:
+        """{kernel: (launches, milliseconds, algorithmic bytes)} accumulated while profiling."""
+        count = ctypes.c_uint32()
+        _check(_lib.slf_profile_read(self._h, None, 0, ctypes.byref(count)))
+        arr = (CProfileEntry * max(count.value, 1))()
+        _check(_lib.slf_profile_read(self._h, arr, count.value, ctypes.byref(count)))
+        return {arr[i].name.decode(): (arr[i].launches, arr[i].milliseconds, arr[i].algorithmic_bytes)
+                for i in range(count.value)}
+
+
+def kernel_launches() -> int:
+    """Kernels launched through the library by this process so far."""
+    v = ctypes.c_uint64()
+    _check(load_library().slf_kernel_launches(ctypes.byref(v)))
+    return v.value

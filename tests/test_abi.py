@@ -58,7 +58,7 @@ def test_the_settings_struct_matches_the_header(lib_path):
         assert getattr(d, field) == pytest.approx(getattr(ref, field)), field
     assert d.gravity == pytest.approx((0.0, -9.81, 0.0))
     assert d.divergence_tolerance == pytest.approx(1e-3) and d.density_tolerance == pytest.approx(5e-4)
-    assert ctypes.sizeof(CSettings) == 80  # sizeof(slf_settings) as gcc lays it out
+    assert ctypes.sizeof(CSettings) == 88  # sizeof(slf_settings) as gcc lays it out
     assert ctypes.sizeof(CReport) == 40
 
 
