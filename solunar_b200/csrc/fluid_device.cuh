@@ -61,18 +61,24 @@ struct Status {
 };
 
 // Neighbour lists of one substep, built by the density pass in the reference's list order
-// (mod.rs:570-606) and read by every later pass of the substep.  Slot-major: entry k of
-// particle i sits at [k * stride + i], so a warp reading slot k of 32 particles reads one
-// contiguous run.  With each neighbour its kernel gradient factor g = slope(d) / d (0 at d = 0)
-// is kept: positions do not move within a substep (the reference keeps the whole gradient per
-// pair for the same reason, dfsph.rs:24-41), and gradient = offset * g rounds as
-// Kernel::gradient does (mod.rs:158-164).
+// (mod.rs:570-606) and read by every later pass of the substep.  An entry is 8 bytes: the
+// neighbour's index and its kernel gradient factor g = slope(d) / d (0 at d = 0), kept because
+// positions do not move within a substep (the reference keeps the whole gradient per pair for
+// the same reason, dfsph.rs:24-41); gradient = offset * g rounds as Kernel::gradient does
+// (mod.rs:158-164).  Layout: warp tiles, entry k of particle i at
+// ((i / 32) * cap + k) * 32 + i % 32, so a warp reading slot k of its 32 particles reads 256
+// contiguous bytes and each warp's lists are one contiguous block.
 struct PairLists {
     uint32_t cap;          // slots per particle
-    uint32_t stride;       // particles per slot row
-    uint32_t* idx;         // [cap][stride] neighbour indexes
-    float* g;              // [cap][stride] gradient factors
-    uint32_t* count;       // [stride] neighbours found; above cap the lists are incomplete
+    uint2* e;              // entries {index, g bits}
+    uint32_t* count;       // neighbours found per particle; above cap the lists are incomplete
+
+    __host__ __device__ static size_t slots_for(uint32_t n, uint32_t cap) {
+        return size_t((n + 31u) / 32u) * cap * 32u;
+    }
+    __host__ __device__ size_t at(uint32_t i, uint32_t k) const {
+        return (size_t(i >> 5) * cap + k) * 32u + (i & 31u);
+    }
 };
 
 // ---- cell tables ----------------------------------------------------------------------------

@@ -263,10 +263,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             sum += kernel_value(p, d);
             float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
-            if (nf < fl.cap) {
-                fl.idx[(size_t)nf * fl.stride + i] = j;
-                fl.g[(size_t)nf * fl.stride + i] = g;
-            }
+            if (nf < fl.cap) fl.e[fl.at(i, nf)] = make_uint2(j, __float_as_uint(g));
             ++nf;
             if (SOLVER == 1) {
                 // gradient(at - other) (dfsph.rs:118), then factors (dfsph.rs:149-153)
@@ -283,10 +280,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             wsum += kernel_value(p, d);
             float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
-            if (nw < wl.cap) {
-                wl.idx[(size_t)nw * wl.stride + i] = j;
-                wl.g[(size_t)nw * wl.stride + i] = g;
-            }
+            if (nw < wl.cap) wl.e[wl.at(i, nw)] = make_uint2(j, __float_as_uint(g));
             ++nw;
             if (SOLVER == 1) {
                 float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
@@ -320,16 +314,57 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
     }
 }
 
-// Walks particle i's list: f(j, g) for each neighbour in list order.
+// Walks particle i's list: f(j, g, q) for each neighbour in list order, q = pts[j].  Entries are
+// taken four at a time and their gathers issued before any is used; past the end of the list
+// the last entry is loaded again (a valid address) but not used, so the sums see exactly the
+// list's terms in its order.
 template <class F>
-__device__ __forceinline__ void each_listed(const PairLists& l, uint32_t i, F&& f) {
+__device__ __forceinline__ void each_listed(const PairLists& l, uint32_t i, const float4* __restrict__ pts, F&& f) {
     uint32_t n = l.count[i];
     if (n > l.cap) n = l.cap;
-    const uint32_t* __restrict__ idx = l.idx + i;
-    const float* __restrict__ gg = l.g + i;
-    const size_t s = l.stride;
-#pragma unroll 2
-    for (uint32_t k = 0; k < n; ++k) f(__ldg(idx + k * s), __ldg(gg + k * s));
+    if (n == 0) return;
+    const uint2* __restrict__ base = l.e + l.at(i, 0);
+    for (uint32_t k = 0; k < n; k += 4) {
+        uint2 e[4];
+        float4 q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            uint32_t kk = k + u < n ? k + u : n - 1;
+            e[u] = __ldg(base + size_t(kk) * 32u);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) q[u] = __ldg(&pts[e[u].x]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u < n) f(e[u].x, __uint_as_float(e[u].y), q[u]);
+    }
+}
+
+// The same walk with a second array gathered alongside (velocities).
+template <class F>
+__device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, const float4* __restrict__ pts,
+                                             const float4* __restrict__ more, F&& f) {
+    uint32_t n = l.count[i];
+    if (n > l.cap) n = l.cap;
+    if (n == 0) return;
+    const uint2* __restrict__ base = l.e + l.at(i, 0);
+    for (uint32_t k = 0; k < n; k += 4) {
+        uint2 e[4];
+        float4 q[4], w[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            uint32_t kk = k + u < n ? k + u : n - 1;
+            e[u] = __ldg(base + size_t(kk) * 32u);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            q[u] = __ldg(&pts[e[u].x]);
+            w[u] = __ldg(&more[e[u].x]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u < n) f(e[u].x, __uint_as_float(e[u].y), q[u], w[u]);
+    }
 }
 
 // ---- wall viscosity (step.rs:262-301, no terrains) ---------------------------------------
@@ -339,8 +374,7 @@ __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc,
                                                float density) {
     if (wl.count[i] == 0) return make_float3(0.0f, 0.0f, 0.0f);
     float awx = 0.0f, awy = 0.0f, awz = 0.0f;
-    each_listed(wl, i, [&](uint32_t j, float g) {
-        float4 q = __ldg(&walls[j]);
+    each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         awx = awx + -(rx * g);
         awy = awy + -(ry * g);
@@ -357,8 +391,7 @@ __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc,
     float k = fminf(dot3(v.x, v.y, v.z, nx, ny, nz), 0.0f);
     float ix = nx * k, iy = ny * k, iz = nz * k;
     float px = 0.0f, py = 0.0f, pz = 0.0f;
-    each_listed(wl, i, [&](uint32_t j, float g) {
-        float4 q = __ldg(&walls[j]);
+    each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float toward = dot3(ix, iy, iz, rx, ry, rz);
         if (toward < 0.0f) {
@@ -423,14 +456,12 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepCons
         float density = rho[i];
         float own = scaled[i];
         float px = 0.0f, py = 0.0f, pz = 0.0f;
-        each_listed(fl, i, [&](uint32_t j, float g) {
-            float4 q = __ldg(&pos[j]);
+        each_listed2(fl, i, pos, vel, [&](uint32_t j, float g, float4 q, float4 w) {
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
             float squared = dot3(rx, ry, rz, rx, ry, rz);
             if (squared <= 0.0f) return;
             // g = slope(distance) / distance with distance = sqrt(squared) > 0
             float gx = rx * g, gy = ry * g, gz = rz * g;
-            float4 w = __ldg(&vel[j]);
             float toward = fminf(dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx, ry, rz), 0.0f);
             float damp = -visc * toward / (squared + p.soften) * 2.0f / (density + __ldg(&rho[j]));
             float s = p.mass * (own + __ldg(&scaled[j]) + damp);
@@ -439,8 +470,7 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepCons
             pz = pz - gz * s;
         });
         float mirrored = own + press[i] / p.rest_sq;
-        each_listed(wl, i, [&](uint32_t j, float g) {
-            float4 q = __ldg(&walls[j]);
+        each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
             float s = p.mass * mirrored;
             px = px - (rx * g) * s;
@@ -484,7 +514,7 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
                                                  PairLists wl, const float4* __restrict__ pos,
                                                  const float4* __restrict__ vel, const float* __restrict__ rho,
                                                  const float* __restrict__ alpha, const float4* __restrict__ walls,
-                                                 float* __restrict__ kappa, DD* __restrict__ partial,
+                                                 float* __restrict__ kappa_w, DD* __restrict__ partial,
                                                  uint32_t* __restrict__ partial_loaded, Status* st,
                                                  uint32_t iterations) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -495,14 +525,11 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
         float4 a = pos[i];
         float4 v = vel[i];
         float rate = 0.0f;
-        each_listed(fl, i, [&](uint32_t j, float g) {
-            float4 q = __ldg(&pos[j]);
-            float4 w = __ldg(&vel[j]);
+        each_listed2(fl, i, pos, vel, [&](uint32_t, float g, float4 q, float4 w) {
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
             rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx * g, ry * g, rz * g);
         });
-        each_listed(wl, i, [&](uint32_t j, float g) {
-            float4 q = __ldg(&walls[j]);
+        each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
             rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
         });
@@ -517,7 +544,8 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
             target = r / dt;
             error = dt * r / p.rest;
         }
-        kappa[i] = target * alpha[i];
+        // the stiffness rides in the spare lane of the position, where push_apart gathers it
+        kappa_w[4 * (size_t)i + 3] = target * alpha[i];
         err = (double)error;
         loaded = error > 0.0f ? 1u : 0u;
     }
@@ -579,27 +607,25 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
     }
 }
 
-// push_apart (dfsph.rs:184-216): the velocity change from each particle's stiffness.
+// push_apart (dfsph.rs:184-216): the velocity change from each particle's stiffness, which the
+// rate pass left in the w lane of each position.
 __global__ void __launch_bounds__(kBlock) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
-                                                 float4* __restrict__ vel, const float* __restrict__ kappa,
-                                                 const float4* __restrict__ walls) {
+                                                 float4* __restrict__ vel, const float4* __restrict__ walls) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const float dt = sc->dt;
     float4 a = pos[i];
-    float own = kappa[i];
+    float own = a.w;
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    each_listed(fl, i, [&](uint32_t j, float g) {
-        float4 q = __ldg(&pos[j]);
+    each_listed(fl, i, pos, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float s = p.mass * (own + __ldg(&kappa[j]));
+        float s = p.mass * (own + q.w);
         cx = cx - (rx * g) * s;
         cy = cy - (ry * g) * s;
         cz = cz - (rz * g) * s;
     });
-    each_listed(wl, i, [&](uint32_t j, float g) {
-        float4 q = __ldg(&walls[j]);
+    each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float s = p.mass * own;
         cx = cx - (rx * g) * s;
@@ -627,11 +653,9 @@ __global__ void __launch_bounds__(kBlock) k_viscous(Params p, const StepConsts* 
     float4 v = vel[i];
     float density = rho[i];
     float px = 0.0f, py = 0.0f, pz = 0.0f;
-    each_listed(fl, i, [&](uint32_t j, float g) {
+    each_listed2(fl, i, pos, vel, [&](uint32_t j, float g, float4 q, float4 w) {
         if (j == i) return;
-        float4 q = __ldg(&pos[j]);
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float4 w = __ldg(&vel[j]);
         float toward = dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx, ry, rz);
         if (toward < 0.0f) {
             float squeeze = toward / (dot3(rx, ry, rz, rx, ry, rz) + p.soften);
@@ -815,23 +839,23 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
 size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (sizeof(DD) + sizeof(uint32_t)) + 64; }
 
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                 const float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 float* kappa, void* partials, Status* st, uint32_t iterations, cudaStream_t s) {
+                 float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
+                 void* partials, Status* st, uint32_t iterations, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = blocks_for(p.n);
     DD* part = static_cast<DD*>(partials);
     uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
     if (which == 0)
-        k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kappa, part, loaded, st,
-                                        iterations);
+        k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
+                                        part, loaded, st, iterations);
     else
-        k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kappa, part, loaded, st,
-                                        iterations);
+        k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
+                                        part, loaded, st, iterations);
 }
 
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
-                 float4* vel, const float* kappa, const float4* walls, cudaStream_t s) {
-    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, kappa, walls);
+                 float4* vel, const float4* walls, cudaStream_t s) {
+    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls);
 }
 
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,

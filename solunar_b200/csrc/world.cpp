@@ -209,11 +209,11 @@ struct World {
     DevBuf<float4> pos[3], vel[3];
     DevBuf<uint32_t> ids[2];
     DevBuf<float> rho[2];
-    DevBuf<float> press, scaled, alpha, kappa;
+    DevBuf<float> press, scaled, alpha;
     DevBuf<uint32_t> lin, cslot, members, count, tiles, keep;
     // neighbour lists of the current substep (fluid and walls)
-    DevBuf<uint32_t> fidx, widx, fcnt, wcnt;
-    DevBuf<float> fgv, wgv;
+    DevBuf<uint2> fent, went;
+    DevBuf<uint32_t> fcnt, wcnt;
     uint32_t list_cap = 0;
     DevBuf<uint8_t> partials;
     bool stats_fresh = false;  // status holds bbox and speed of the committed state
@@ -269,10 +269,11 @@ struct World {
     ~World() {
         if (stream) {
             for (auto* b : {&pos[0], &pos[1], &pos[2], &vel[0], &vel[1], &vel[2]}) b->release(stream);
-            for (auto* b : {&ids[0], &ids[1], &lin, &cslot, &members, &count, &tiles, &keep, &dwstart, &fidx, &widx,
-                            &fcnt, &wcnt})
+            for (auto* b : {&ids[0], &ids[1], &lin, &cslot, &members, &count, &tiles, &keep, &dwstart, &fcnt, &wcnt})
                 b->release(stream);
-            for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha, &kappa, &fgv, &wgv}) b->release(stream);
+            for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha}) b->release(stream);
+            fent.release(stream);
+            went.release(stream);
             partials.release(stream);
             stage.release(stream);
             dwalls.release(stream);
@@ -461,12 +462,9 @@ struct World {
         SLF_TRY(press.ensure(n, 0, stream));
         SLF_TRY(scaled.ensure(n, 0, stream));
         SLF_TRY(alpha.ensure(n, 0, stream));
-        SLF_TRY(kappa.ensure(n, 0, stream));
-        size_t slots = size_t(list_cap) * n;
-        SLF_TRY(fidx.ensure(slots, 0, stream));
-        SLF_TRY(fgv.ensure(slots, 0, stream));
-        SLF_TRY(widx.ensure(slots, 0, stream));
-        SLF_TRY(wgv.ensure(slots, 0, stream));
+        size_t slots = PairLists::slots_for(uint32_t(n), list_cap);
+        SLF_TRY(fent.ensure(slots, 0, stream));
+        SLF_TRY(went.ensure(slots, 0, stream));
         SLF_TRY(fcnt.ensure(n, 0, stream));
         SLF_TRY(wcnt.ensure(n, 0, stream));
         SLF_TRY(lin.ensure(n, 0, stream));
@@ -476,8 +474,8 @@ struct World {
         return SLF_OK;
     }
 
-    PairLists fluid_lists() const { return PairLists{list_cap, uint32_t(n), fidx.p, fgv.p, fcnt.p}; }
-    PairLists wall_lists() const { return PairLists{list_cap, uint32_t(n), widx.p, wgv.p, wcnt.p}; }
+    PairLists fluid_lists() const { return PairLists{list_cap, fent.p, fcnt.p}; }
+    PairLists wall_lists() const { return PairLists{list_cap, went.p, wcnt.p}; }
 
     // After a density pass: a list longer than its room leaves the substep to be run again.
     static constexpr int32_t kRetry = -1;
@@ -877,7 +875,7 @@ struct World {
         for (;;) {
             timed(which == 0 ? "rate_divergence" : "rate_density",
                   which == 0 ? bytes_per_particle::rate_divergence : bytes_per_particle::rate_density, [&] {
-                      launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, kappa.p,
+                      launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p,
                                   partials.p, d_status, iterations, stream);
                   });
             SLF_TRY(read_status());
@@ -886,7 +884,7 @@ struct World {
             // the device stops the loop at max_iterations; past that its flag was not written
             if (iterations > s.max_iterations) return fail(SLF_ERR_TIMEOUT, "solver stop flag never set");
             timed(which == 0 ? "push_divergence" : "push_density", bytes_per_particle::push,
-                  [&] { launch_push(p, d_consts, fl, wl, pos[a].p, v, kappa.p, dwalls.p, stream); });
+                  [&] { launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, stream); });
             iterations += 1;
         }
     }
