@@ -57,7 +57,7 @@ struct Status {
     uint32_t processed;    // particles a neighbour pass visited (dispatch completeness)
     uint32_t ticket;       // block counter of the last-block reduction
     uint32_t list_max;     // longest neighbour list the last density pass found
-    uint32_t pad;
+    uint32_t iterations;   // pushes of the running solve so far (dfsph.rs:236, 273)
 };
 
 // Neighbour lists of one substep, built by the density pass in the reference's list order

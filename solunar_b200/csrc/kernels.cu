@@ -515,8 +515,9 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
                                                  const float4* __restrict__ vel, const float* __restrict__ rho,
                                                  const float* __restrict__ alpha, const float4* __restrict__ walls,
                                                  float* __restrict__ kappa_w, DD* __restrict__ partial,
-                                                 uint32_t* __restrict__ partial_loaded, Status* st,
-                                                 uint32_t iterations) {
+                                                 uint32_t* __restrict__ partial_loaded, Status* st) {
+    // a solve that already stopped leaves the rest of its batch of launches idle
+    if (__ldcg(&st->settled)) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double err = 0.0;
     uint32_t loaded = 0;
@@ -599,10 +600,12 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
         uint32_t load = cnt > 0 ? cnt : 1u;
         double average = (b.hi + b.lo) / (double)load;
         double tol = WHICH == 1 ? (double)p.den_tol : (double)p.div_tol;
+        uint32_t iterations = st->iterations;
         bool settled = iterations >= p.min_iter && average <= tol;
         st->average = average;
         st->loaded = cnt;
-        st->settled = (settled || iterations >= p.max_iter) ? 1u : 0u;
+        if (settled || iterations >= p.max_iter) st->settled = 1u;
+        else st->iterations = iterations + 1u;  // a push follows
         st->ticket = 0;
     }
 }
@@ -611,7 +614,9 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
 // rate pass left in the w lane of each position.
 __global__ void __launch_bounds__(kBlock) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
-                                                 float4* __restrict__ vel, const float4* __restrict__ walls) {
+                                                 float4* __restrict__ vel, const float4* __restrict__ walls,
+                                                 const Status* st) {
+    if (__ldcg(&st->settled)) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const float dt = sc->dt;
@@ -840,22 +845,22 @@ size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (size
 
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 void* partials, Status* st, uint32_t iterations, cudaStream_t s) {
+                 void* partials, Status* st, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = blocks_for(p.n);
     DD* part = static_cast<DD*>(partials);
     uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
     if (which == 0)
         k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
-                                        part, loaded, st, iterations);
+                                        part, loaded, st);
     else
         k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
-                                        part, loaded, st, iterations);
+                                        part, loaded, st);
 }
 
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
-                 float4* vel, const float4* walls, cudaStream_t s) {
-    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls);
+                 float4* vel, const float4* walls, const Status* st, cudaStream_t s) {
+    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st);
 }
 
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,

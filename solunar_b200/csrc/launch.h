@@ -36,12 +36,14 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
                         cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
-// writes each particle's stiffness into the w lane of its position
+// One solver check: writes each particle's stiffness into the w lane of its position, and either
+// sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve
+// has settled, so a batch of iterations can be queued ahead of the check that ends it.
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 void* partials, Status* st, uint32_t iterations, cudaStream_t s);
+                 void* partials, Status* st, cudaStream_t s);
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
-                 float4* vel, const float4* walls, cudaStream_t s);
+                 float4* vel, const float4* walls, const Status* st, cudaStream_t s);
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                     const float4* vel, const float* rho, const float4* walls, float4* vel_out, cudaStream_t s);
 void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,

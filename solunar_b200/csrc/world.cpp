@@ -869,23 +869,69 @@ struct World {
     }
 
     // solve (dfsph.rs:222-275): Jacobi iterations until the average error is under tolerance.
+    // Iterations are queued in batches; the device counts them and turns the launches after
+    // the stopping check into no-ops, so the host waits once a batch instead of once an
+    // iteration.  A batch is as long as the last solve of the same kind took.
+    uint32_t expected_iterations[2] = {2, 2};
     int32_t solve(int which, const Params& p, int a, float4* v, int nid, uint32_t& iterations) {
         iterations = 0;
         PairLists fl = fluid_lists(), wl = wall_lists();
+        SLF_CUDA(cudaMemsetAsync(&d_status->settled, 0, 4, stream));
+        SLF_CUDA(cudaMemsetAsync(&d_status->iterations, 0, 4, stream));
+        const char* rate_name = which == 0 ? "rate_divergence" : "rate_density";
+        const char* push_name = which == 0 ? "push_divergence" : "push_density";
+        double rate_bytes = which == 0 ? bytes_per_particle::rate_divergence : bytes_per_particle::rate_density;
+        size_t first = prof.pending.size();
+        std::vector<int> kinds;  // 0 rate, 1 push, in launch order, for the profile
+        uint32_t batch = std::max<uint32_t>(expected_iterations[which], 1u);
+        uint32_t queued = 0;
+        auto rate = [&] {
+            timed(rate_name, rate_bytes, [&] {
+                launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p,
+                            d_status, stream);
+            });
+            kinds.push_back(0);
+        };
+        // check, then (push, check) pairs: the order of the reference's loop
+        rate();
         for (;;) {
-            timed(which == 0 ? "rate_divergence" : "rate_density",
-                  which == 0 ? bytes_per_particle::rate_divergence : bytes_per_particle::rate_density, [&] {
-                      launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p,
-                                  partials.p, d_status, iterations, stream);
-                  });
-            SLF_TRY(read_status());
+            for (uint32_t b = 0; b < batch; ++b) {
+                timed(push_name, bytes_per_particle::push,
+                      [&] { launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream); });
+                kinds.push_back(1);
+                rate();
+            }
+            queued += batch;
+            // profile entries of launches that turned out idle are kept apart
+            size_t mark = prof.pending.size();
+            SLF_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(Status), cudaMemcpyDeviceToHost, stream));
+            SLF_CUDA(cudaStreamSynchronize(stream));
+            if (h_status->settled) {
+                iterations = h_status->iterations;
+                if (prof.on && mark == prof.pending.size()) relabel_idle(first, kinds, iterations);
+                SLF_TRY(sync());
+                SLF_TRY(lists_fit());
+                expected_iterations[which] = std::max<uint32_t>(iterations, 1u);
+                return SLF_OK;
+            }
             SLF_TRY(lists_fit());
-            if (h_status->settled) return SLF_OK;
-            // the device stops the loop at max_iterations; past that its flag was not written
-            if (iterations > s.max_iterations) return fail(SLF_ERR_TIMEOUT, "solver stop flag never set");
-            timed(which == 0 ? "push_divergence" : "push_density", bytes_per_particle::push,
-                  [&] { launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, stream); });
-            iterations += 1;
+            // the device stops at max_iterations; past that its flag was not written
+            if (queued > s.max_iterations + 1) return fail(SLF_ERR_TIMEOUT, "solver stop flag never set");
+            batch = std::max<uint32_t>(4u, batch / 2);
+        }
+    }
+
+    // The launches of a solve after its stopping check did nothing; their profile entries
+    // go under "solver_idle" so the kernels' averages hold only launches that worked.
+    void relabel_idle(size_t first, const std::vector<int>& kinds, uint32_t iterations) {
+        uint32_t rates = 0, pushes = 0;
+        int idle = prof.kind("solver_idle");
+        for (size_t k = 0; k < kinds.size() && first + k < prof.pending.size(); ++k) {
+            bool used = kinds[k] == 0 ? rates++ <= iterations : pushes++ < iterations;
+            if (!used) {
+                prof.pending[first + k].kind = idle;
+                prof.pending[first + k].bytes = 0.0;
+            }
         }
     }
 
