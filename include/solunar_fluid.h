@@ -202,6 +202,27 @@ int32_t slf_get_stream(const slf_world* world, void** stream);
 /* Message of the last failed call on any handle of this thread ("" if none). */
 const char* slf_last_error(void);
 
+/* ---- sorting without allocation ---------------------------------------------------------- */
+
+/* No counterpart in the reference: the cell sort of slf_update_neighbors for callers that
+ * cannot allocate device memory (an engine that hands out all GPU memory from its own pool, a
+ * plugin that only receives buffers from its host).  It allocates nothing: its scratch is one
+ * fixed array in device memory, about 7.4 MB, that every GPU which loads this library holds
+ * until the process exits.
+ *
+ * positions: n packed xyz float triples and ids: n ids, both in device memory; radius: the
+ * cell size (the kernel radius, spacing * support).  order (device, n entries) receives, for
+ * each place k of the (cell, id) order of update_neighbors (src/fluid/mod.rs:541-550), the
+ * input index of the particle found there.  At most 262,144 particles whose bounding box spans
+ * at most 1,048,576 cells: larger calls fail with SLF_ERR_OUT_OF_RANGE.  The call runs on
+ * `stream` (a cudaStream_t; NULL for the default stream) and waits for it before returning.
+ * The first call on a device looks up the scratch array's address there, so make that first
+ * call before any stream capture.  All calls share the one array and it keeps the last call's
+ * contents (the call clears what must start at zero); calls whose work overlaps on the GPU
+ * race on it. */
+int32_t slf_sort_by_cell_noalloc(const float* positions, const uint32_t* ids, uint64_t n, float radius,
+                                 uint32_t* order, void* stream);
+
 /* ---- diagnostics and testing ------------------------------------------------------------ */
 
 /* Per-kernel device time.  While profiling is on, every launch of the world is bracketed by

@@ -21,7 +21,7 @@ LIB = os.path.join(HERE, "libsolunar_fluid.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["kernels.cu"]
+CUDA_SOURCES = ["kernels.cu", "noalloc.cu"]
 HOST_SOURCES = ["world.cpp"]
 
 

@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "fluid_device.cuh"
@@ -69,5 +70,8 @@ void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s);
 
 // kernels launched through this library by the process so far
 uint64_t kernel_launches();
+
+// message slf_last_error() returns on this thread
+void set_last_error(const std::string& message);
 
 }  // namespace slf

@@ -1180,6 +1180,8 @@ struct World {
     }
 };
 
+void set_last_error(const std::string& message) { g_error = message; }
+
 }  // namespace slf
 
 // ---- C ABI ---------------------------------------------------------------------------------

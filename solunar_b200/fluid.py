@@ -73,6 +73,7 @@ def load_library():
         "slf_profile_read": [vp, ctypes.POINTER(CProfileEntry), ctypes.c_uint32, u32p],
         "slf_profile_reset": [vp],
         "slf_kernel_launches": [u64p],
+        "slf_sort_by_cell_noalloc": [vp, vp, ctypes.c_uint64, ctypes.c_float, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -320,3 +321,13 @@ def kernel_launches() -> int:
     v = ctypes.c_uint64()
     _check(load_library().slf_kernel_launches(ctypes.byref(v)))
     return v.value
+
+
+def sort_by_cell_noalloc(positions_ptr: int, ids_ptr: int, n: int, radius: float, order_ptr: int,
+                         stream: int = 0):
+    """slf_sort_by_cell_noalloc on device pointers: order[k] = input index of the k-th particle
+    in (cell, id) order.  For hosts that cannot allocate device memory: the library keeps this
+    sort's scratch in a fixed device array and allocates nothing."""
+    L = load_library()
+    _check(L.slf_sort_by_cell_noalloc(ctypes.c_void_p(positions_ptr), ctypes.c_void_p(ids_ptr), n, radius,
+                                      ctypes.c_void_p(order_ptr), ctypes.c_void_p(stream)))
