@@ -351,3 +351,20 @@ def test_the_double_restatement_agrees_with_the_float_one_on_a_short_dam(oracle_
     assert np.array_equal(a.ids(), b.ids())
     assert np.max(np.abs(a.positions() - b.positions())) < 1e-4
     assert np.max(np.abs(a.densities() - b.densities()) / 1000.0) < 1e-3
+
+
+@pytest.mark.parametrize("counts", [(10, 12, 6), (14, 10, 8)])
+def test_the_compensated_residual_stops_the_solves_where_the_reference_sum_does(oracle_lib, counts):
+    # The CUDA library sums the DFSPH solver error in compensated FP64; the reference sums it in
+    # f32, sequentially (src/fluid/dfsph.rs:266-267).  On these dams both stop every solve at
+    # the same iteration, so the two runs stay bit-identical.
+    sc = scenes.small_dam(FluidSolver.DFSPH, counts=counts)
+    ref = oracle_lib.OracleWorld(sc.settings, residual_sum=0)
+    comp = oracle_lib.OracleWorld(sc.settings, residual_sum=1)
+    sc.build(ref)
+    sc.build(comp)
+    for _ in range(6):
+        a, b = ref.step(sc.dt), comp.step(sc.dt)
+        assert a.iterations == b.iterations
+        assert ref.last_iterations() == comp.last_iterations()
+    assert ref.state_hash() == comp.state_hash()
