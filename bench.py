@@ -42,16 +42,22 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scene", default="dfsph_dam_1m")
+    ap.add_argument("--arithmetic", choices=["exact", "fast"], default="exact",
+                    help="exact: the reference's rounding, bit-identical to the CPU restatement; "
+                         "fast: fused arithmetic, within FP32 tolerance")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed CPU work in the baseline")
     return ap.parse_args()
 
 
-def scene_of(name):
+def scene_of(name, arithmetic="exact"):
     from solunar_b200 import scenes
+    from solunar_b200.abi import Arithmetic
 
-    return getattr(scenes, name)()
+    sc = getattr(scenes, name)()
+    sc.settings.arithmetic = Arithmetic.FAST if arithmetic == "fast" else Arithmetic.EXACT
+    return sc
 
 
 def workload(sc) -> dict:
@@ -229,7 +235,7 @@ def main():
 
     from solunar_b200 import fluid
 
-    sc = scene_of(args.scene)
+    sc = scene_of(args.scene, args.arithmetic)
     sc.settings.device = local_rank
     world = fluid.FluidWorld(sc.settings)
     sc.build(world)

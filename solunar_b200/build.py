@@ -21,7 +21,10 @@ LIB = os.path.join(HERE, "libsolunar_fluid.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# kernels whose rounding follows the reference: no contraction, IEEE division and square root
 CUDA_SOURCES = ["kernels.cu", "noalloc.cu"]
+# the FAST arithmetic variants: contraction on
+CUDA_FAST_SOURCES = ["kernels_fast.cu"]
 HOST_SOURCES = ["world.cpp"]
 
 
@@ -54,14 +57,15 @@ def build(verbose: bool = False, force: bool = False) -> str:
     headers.append(os.path.join(INCLUDE, "solunar_fluid.h"))
     objects = []
     nvcc = _nvcc()
-    for src in CUDA_SOURCES:
+    for src in CUDA_SOURCES + CUDA_FAST_SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
         objects.append(obj)
         if force or _stale(obj, [path] + headers):
-            cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-fmad=false", "-prec-div=true",
-                   "-prec-sqrt=true", "-ftz=false", "--extended-lambda", "-Xcompiler", "-fPIC",
-                   "-I", CSRC, "-c", path, "-o", obj]
+            rounding = (["-fmad=true"] if src in CUDA_FAST_SOURCES else
+                        ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"])
+            cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", *rounding, "--extended-lambda", "-Xcompiler",
+                   "-fPIC", "-I", CSRC, "-c", path, "-o", obj]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
             subprocess.run(cmd, check=True)

@@ -33,6 +33,11 @@ struct Params {
     int solver;          // 0 WCSPH, 1 DFSPH
     float div_tol, den_tol;
     uint32_t min_iter, max_iter;
+    // reciprocal constants of the FAST arithmetic
+    float inv_radius;      // 1 / r
+    float grad_scale;      // scale * (-20) / r^2: slope(d) / d = grad_scale * (1 - d / r)^3
+    float inv_rest;        // 1 / rest_density
+    float inv_rest_sq;     // 1 / rest_density^2
 };
 
 // Per-substep constants, in device memory so a captured substep reads the current ones.
@@ -136,8 +141,10 @@ __device__ __forceinline__ float pow3(float x) { return x * (x * x); }
 __device__ __forceinline__ float pow4(float x) { float s = x * x; return s * s; }
 __device__ __forceinline__ float pow7(float x) { float s = x * x; float q = s * s; return (x * s) * q; }
 
+// x*x' + y*y' + z*z', left to right, each operation rounded on its own whatever the compiler's
+// contraction setting: the neighbour test and the cell keys depend on these bits.
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
-    return ax * bx + ay * by + az * bz;
+    return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), __fmul_rn(az, bz));
 }
 
 // Kernel::value (mod.rs:140-146)
@@ -164,8 +171,8 @@ __device__ __forceinline__ float kernel_gradient_factor(const Params& p, float o
 // cell_of (mod.rs:526-533): floor(p / r) per axis, `as i32` (PTX float-to-int conversions
 // saturate and map NaN to zero, as Rust's does).
 __device__ __forceinline__ int3 cell_of(const Params& p, float x, float y, float z) {
-    return make_int3(__float2int_rz(floorf(x / p.radius)), __float2int_rz(floorf(y / p.radius)),
-                     __float2int_rz(floorf(z / p.radius)));
+    return make_int3(__float2int_rz(floorf(__fdiv_rn(x, p.radius))), __float2int_rz(floorf(__fdiv_rn(y, p.radius))),
+                     __float2int_rz(floorf(__fdiv_rn(z, p.radius))));
 }
 
 // Visit the points of `g` within reach of `at` in the reference's list order: the 27 cells
@@ -174,6 +181,7 @@ __device__ __forceinline__ int3 cell_of(const Params& p, float x, float y, float
 template <class F>
 __device__ __forceinline__ void each_near(const Params& p, const GridDev& g, const float4* __restrict__ pts,
                                           int3 cell, float ax, float ay, float az, F&& f) {
+    // the offsets below are single subtractions and the test uses dot3: exact under any flags
     if (g.mode == 0) return;
 #pragma unroll 1
     for (int dz = -1; dz <= 1; ++dz) {

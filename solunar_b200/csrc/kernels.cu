@@ -12,38 +12,9 @@
 
 #include "fluid_device.cuh"
 #include "launch.h"
+#include "reduce.cuh"
 
 namespace slf {
-
-// ---- block reductions ---------------------------------------------------------------------
-
-template <class T, class Op>
-__device__ __forceinline__ T warp_reduce(T v, Op op) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-// Reduces one value per thread over the block; the result is valid in thread 0.
-template <class T, class Op>
-__device__ __forceinline__ T block_reduce(T v, Op op, T identity) {
-    __shared__ T warp_vals[kBlock / 32];
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = warp_reduce(v, op);
-    __syncthreads();
-    if (lane == 0) warp_vals[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        v = lane < (int)(blockDim.x >> 5) ? warp_vals[lane] : identity;
-        v = warp_reduce(v, op);
-    }
-    return v;
-}
-
-struct MinI { __device__ int operator()(int a, int b) const { return a < b ? a : b; } };
-struct MaxI { __device__ int operator()(int a, int b) const { return a > b ? a : b; } };
-struct MaxU { __device__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; } };
-struct SumU { __device__ uint32_t operator()(uint32_t a, uint32_t b) const { return a + b; } };
 
 // Bounding box of cells, fastest speed, held-back count and non-finite flag of a block's
 // particles, folded into the status with one atomic each.
@@ -315,28 +286,43 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
 }
 
 // Walks particle i's list: f(j, g, q) for each neighbour in list order, q = pts[j].  Entries are
-// taken four at a time and their gathers issued before any is used; past the end of the list
-// the last entry is loaded again (a valid address) but not used, so the sums see exactly the
-// list's terms in its order.
+// taken kListUnroll at a time, their gathers issued before any is used, and the next group's
+// entries are requested before this group is used; past the end of the list the last entry is
+// loaded again (a valid address) but not used, so the sums see exactly the list's terms in its
+// order.
+#ifndef SLF_LIST_UNROLL
+#define SLF_LIST_UNROLL 4
+#endif
+constexpr int kListUnroll = SLF_LIST_UNROLL;
+// resident blocks per SM the list-walking kernels are compiled for (caps their registers)
+#ifndef SLF_PAIR_MIN_BLOCKS
+#define SLF_PAIR_MIN_BLOCKS 1
+#endif
+
 template <class F>
 __device__ __forceinline__ void each_listed(const PairLists& l, uint32_t i, const float4* __restrict__ pts, F&& f) {
     uint32_t n = l.count[i];
     if (n > l.cap) n = l.cap;
     if (n == 0) return;
     const uint2* __restrict__ base = l.e + l.at(i, 0);
-    for (uint32_t k = 0; k < n; k += 4) {
-        uint2 e[4];
-        float4 q[4];
+    uint2 e[kListUnroll];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            uint32_t kk = k + u < n ? k + u : n - 1;
-            e[u] = __ldg(base + size_t(kk) * 32u);
+    for (int u = 0; u < kListUnroll; ++u) e[u] = __ldg(base + size_t(u < (int)n ? u : n - 1) * 32u);
+    for (uint32_t k = 0; k < n; k += kListUnroll) {
+        float4 q[kListUnroll];
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u) q[u] = __ldg(&pts[e[u].x]);
+        uint2 next[kListUnroll];
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u) {
+            uint32_t kk = k + kListUnroll + u;
+            next[u] = __ldg(base + size_t(kk < n ? kk : n - 1) * 32u);
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) q[u] = __ldg(&pts[e[u].x]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < kListUnroll; ++u)
             if (k + u < n) f(e[u].x, __uint_as_float(e[u].y), q[u]);
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u) e[u] = next[u];
     }
 }
 
@@ -348,22 +334,27 @@ __device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, con
     if (n > l.cap) n = l.cap;
     if (n == 0) return;
     const uint2* __restrict__ base = l.e + l.at(i, 0);
-    for (uint32_t k = 0; k < n; k += 4) {
-        uint2 e[4];
-        float4 q[4], w[4];
+    uint2 e[kListUnroll];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            uint32_t kk = k + u < n ? k + u : n - 1;
-            e[u] = __ldg(base + size_t(kk) * 32u);
-        }
+    for (int u = 0; u < kListUnroll; ++u) e[u] = __ldg(base + size_t(u < (int)n ? u : n - 1) * 32u);
+    for (uint32_t k = 0; k < n; k += kListUnroll) {
+        float4 q[kListUnroll], w[kListUnroll];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < kListUnroll; ++u) {
             q[u] = __ldg(&pts[e[u].x]);
             w[u] = __ldg(&more[e[u].x]);
         }
+        uint2 next[kListUnroll];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < kListUnroll; ++u) {
+            uint32_t kk = k + kListUnroll + u;
+            next[u] = __ldg(base + size_t(kk < n ? kk : n - 1) * 32u);
+        }
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u)
             if (k + u < n) f(e[u].x, __uint_as_float(e[u].y), q[u], w[u]);
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u) e[u] = next[u];
     }
 }
 
@@ -436,7 +427,7 @@ __device__ __forceinline__ void advance_one(const Params& p, float dt, float4& a
 
 // ---- WCSPH: forces, velocity update and advance in one pass (step.rs:159-223, 305-339) -----
 
-__global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                         PairLists wl, const float4* __restrict__ pos,
                                                         const float4* __restrict__ vel, const float* __restrict__ rho,
                                                         const float* __restrict__ press,
@@ -494,23 +485,10 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force(Params p, const StepCons
 
 // ---- DFSPH ----------------------------------------------------------------------------------
 
-// double-double accumulation (TwoSum), for the solver residual
-struct DD {
-    double hi, lo;
-};
-__device__ __forceinline__ DD dd_add(DD a, DD b) {
-    double s = a.hi + b.hi;
-    double bb = s - a.hi;
-    double err = (a.hi - (s - bb)) + (b.hi - bb);
-    double lo = a.lo + b.lo + err;
-    double h = s + lo;
-    return DD{h, lo - (h - s)};
-}
-
 // density_rate (dfsph.rs:166-181), then the solve's stiffness and error (dfsph.rs:241-259), and
 // the average error of the particles under load (dfsph.rs:263-268) in a last-block finish.
 template <int WHICH>
-__global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
                                                  const float4* __restrict__ vel, const float* __restrict__ rho,
                                                  const float* __restrict__ alpha, const float4* __restrict__ walls,
@@ -550,69 +528,12 @@ __global__ void __launch_bounds__(kBlock) k_rate(Params p, const StepConsts* __r
         err = (double)error;
         loaded = error > 0.0f ? 1u : 0u;
     }
-    // block sum: a fixed shuffle tree in double-double
-    DD acc{err, 0.0};
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        DD other{__shfl_xor_sync(0xffffffffu, acc.hi, o), __shfl_xor_sync(0xffffffffu, acc.lo, o)};
-        acc = dd_add(acc, other);
-    }
-    __shared__ DD warp_acc[kBlock / 32];
-    __shared__ bool last_block;
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) warp_acc[warp] = acc;
-    loaded = block_reduce(loaded, SumU(), 0u);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        DD b = warp_acc[0];
-        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) b = dd_add(b, warp_acc[k]);
-        partial[blockIdx.x] = b;
-        partial_loaded[blockIdx.x] = loaded;
-        __threadfence();
-        uint32_t ticket = atomicAdd(&st->ticket, 1u);
-        last_block = ticket == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last_block) return;
-    // the last block to finish sums the block partials in block order
-    __threadfence();
-    DD t{0.0, 0.0};
-    uint32_t cnt = 0;
-    for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
-        // other blocks wrote these: read through L2, never a stale L1 line
-        const double* part = reinterpret_cast<const double*>(partial);
-        DD v{__ldcg(part + 2 * k), __ldcg(part + 2 * k + 1)};
-        t = dd_add(t, v);
-        cnt += __ldcg(partial_loaded + k);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        DD other{__shfl_xor_sync(0xffffffffu, t.hi, o), __shfl_xor_sync(0xffffffffu, t.lo, o)};
-        t = dd_add(t, other);
-    }
-    cnt = block_reduce(cnt, SumU(), 0u);
-    __syncthreads();
-    if (lane == 0) warp_acc[warp] = t;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        DD b = warp_acc[0];
-        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) b = dd_add(b, warp_acc[k]);
-        uint32_t load = cnt > 0 ? cnt : 1u;
-        double average = (b.hi + b.lo) / (double)load;
-        double tol = WHICH == 1 ? (double)p.den_tol : (double)p.div_tol;
-        uint32_t iterations = st->iterations;
-        bool settled = iterations >= p.min_iter && average <= tol;
-        st->average = average;
-        st->loaded = cnt;
-        if (settled || iterations >= p.max_iter) st->settled = 1u;
-        else st->iterations = iterations + 1u;  // a push follows
-        st->ticket = 0;
-    }
+    residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
 }
 
 // push_apart (dfsph.rs:184-216): the velocity change from each particle's stiffness, which the
 // rate pass left in the w lane of each position.
-__global__ void __launch_bounds__(kBlock) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
                                                  float4* __restrict__ vel, const float4* __restrict__ walls,
                                                  const Status* st) {
@@ -646,7 +567,7 @@ __global__ void __launch_bounds__(kBlock) k_push(Params p, const StepConsts* __r
 
 // viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
 // because neighbours read the old velocities.
-__global__ void __launch_bounds__(kBlock) k_viscous(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                     PairLists wl, const float4* __restrict__ pos,
                                                     const float4* __restrict__ vel, const float* __restrict__ rho,
                                                     const float4* __restrict__ walls, float4* __restrict__ vel_out) {
@@ -769,6 +690,7 @@ __global__ void k_unpack3(uint32_t n, const float* __restrict__ in, float4* __re
 
 static std::atomic<uint64_t> g_launches{0};
 uint64_t kernel_launches() { return g_launches.load(); }
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 static inline uint32_t blocks_for(uint32_t n) {
     g_launches.fetch_add(1, std::memory_order_relaxed);

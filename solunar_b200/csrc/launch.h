@@ -68,8 +68,27 @@ void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s);
 void launch_pack3(uint32_t n, const float4* in, float* out, cudaStream_t s);
 void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s);
 
+// FAST arithmetic variants (kernels_fast.cu): same lists, order and sums, fused rounding; the
+// lists hold indexes only and each pass recomputes the kernel gradient from the positions
+void launch_density_fast(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos,
+                         const float4* walls, const PairLists& fl, const PairLists& wl, float* rho, float* press,
+                         float* scaled, float* alpha, Status* st, cudaStream_t s);
+void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                             const float4* pos, const float4* vel, const float* rho, const float* press,
+                             const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
+                             cudaStream_t s);
+void launch_rate_fast(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                      float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
+                      void* partials, Status* st, cudaStream_t s);
+void launch_push_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                      const float4* pos, float4* vel, const float4* walls, const Status* st, cudaStream_t s);
+void launch_viscous_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                         const float4* pos, const float4* vel, const float* rho, const float4* walls,
+                         float4* vel_out, cudaStream_t s);
+
 // kernels launched through this library by the process so far
 uint64_t kernel_launches();
+void note_launch();
 
 // message slf_last_error() returns on this thread
 void set_last_error(const std::string& message);

@@ -356,6 +356,10 @@ struct World {
         p.den_tol = s.density_tolerance;
         p.min_iter = s.min_iterations;
         p.max_iter = s.max_iterations;
+        p.inv_radius = 1.0f / radius;
+        p.grad_scale = scale * -20.0f / (radius * radius);
+        p.inv_rest = 1.0f / s.rest_density;
+        p.inv_rest_sq = 1.0f / (s.rest_density * s.rest_density);
         return p;
     }
 
@@ -472,6 +476,43 @@ struct World {
         SLF_TRY(members.ensure(n, 0, stream));
         SLF_TRY(partials.ensure(rate_partial_bytes(uint32_t(n)), 0, stream));
         return SLF_OK;
+    }
+
+    bool fast() const { return s.arithmetic == SLF_ARITHMETIC_FAST; }
+
+    // the pair passes of the settings' arithmetic
+    void density_pass(const Params& p, const float4* ps, const PairLists& fl, const PairLists& wl, float* rh) {
+        if (fast())
+            launch_density_fast(p, fgrid, wgrid, ps, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status,
+                                stream);
+        else
+            launch_density(p, fgrid, wgrid, ps, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status, stream);
+    }
+    void force_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
+        if (fast())
+            launch_wcsph_force_fast(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
+                                    pos[b].p, vel[b].p, d_status, stream);
+        else
+            launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
+                               pos[b].p, vel[b].p, d_status, stream);
+    }
+    void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid) {
+        if (fast())
+            launch_rate_fast(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p,
+                             d_status, stream);
+        else
+            launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p, d_status,
+                        stream);
+    }
+    void push_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v) {
+        if (fast()) launch_push_fast(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
+        else launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
+    }
+    void viscous_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
+        if (fast())
+            launch_viscous_fast(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
+        else
+            launch_viscous(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
     }
 
     PairLists fluid_lists() const { return PairLists{list_cap, fent.p, fcnt.p}; }
@@ -827,8 +868,7 @@ struct World {
         Params p = params();
         for (;;) {
             SLF_TRY(reset_status());
-            launch_density(p, fgrid, wgrid, pos[cpos].p, dwalls.p, fluid_lists(), wall_lists(), rho[cid].p, press.p,
-                           scaled.p, alpha.p, d_status, stream);
+            density_pass(p, pos[cpos].p, fluid_lists(), wall_lists(), rho[cid].p);
             SLF_TRY(read_status());
             int32_t st = lists_fit();
             if (st == SLF_OK) return SLF_OK;
@@ -847,14 +887,9 @@ struct World {
         SLF_TRY(reset_status());
         launch_set_consts(consts(dt), d_consts, stream);
         PairLists fl = fluid_lists(), wl = wall_lists();
-        timed("density", bytes_per_particle::density_wcsph, [&] {
-            launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rho[nid].p, press.p, scaled.p, alpha.p,
-                           d_status, stream);
-        });
-        timed("wcsph_force_advance", bytes_per_particle::wcsph_force, [&] {
-            launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
-                               pos[b].p, vel[b].p, d_status, stream);
-        });
+        timed("density", bytes_per_particle::density_wcsph,
+              [&] { density_pass(p, pos[a].p, fl, wl, rho[nid].p); });
+        timed("wcsph_force_advance", bytes_per_particle::wcsph_force, [&] { force_pass(p, fl, wl, a, b, nid); });
         SLF_TRY(read_status());
         SLF_TRY(lists_fit());
         if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
@@ -886,18 +921,14 @@ struct World {
         uint32_t batch = std::max<uint32_t>(expected_iterations[which], 1u);
         uint32_t queued = 0;
         auto rate = [&] {
-            timed(rate_name, rate_bytes, [&] {
-                launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p,
-                            d_status, stream);
-            });
+            timed(rate_name, rate_bytes, [&] { rate_pass(which, p, fl, wl, a, v, nid); });
             kinds.push_back(0);
         };
         // check, then (push, check) pairs: the order of the reference's loop
         rate();
         for (;;) {
             for (uint32_t b = 0; b < batch; ++b) {
-                timed(push_name, bytes_per_particle::push,
-                      [&] { launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream); });
+                timed(push_name, bytes_per_particle::push, [&] { push_pass(p, fl, wl, a, v); });
                 kinds.push_back(1);
                 rate();
             }
@@ -944,15 +975,11 @@ struct World {
         SLF_TRY(reset_status());
         launch_set_consts(consts(dt), d_consts, stream);
         PairLists fl = fluid_lists(), wl = wall_lists();
-        timed("density_alpha", bytes_per_particle::density_dfsph, [&] {
-            launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rho[nid].p, press.p, scaled.p, alpha.p,
-                           d_status, stream);
-        });
+        timed("density_alpha", bytes_per_particle::density_dfsph,
+              [&] { density_pass(p, pos[a].p, fl, wl, rho[nid].p); });
         uint32_t div_it = 0, den_it = 0;
         SLF_TRY(solve(0, p, a, vel[a].p, nid, div_it));
-        timed("viscosity", bytes_per_particle::viscosity, [&] {
-            launch_viscous(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
-        });
+        timed("viscosity", bytes_per_particle::viscosity, [&] { viscous_pass(p, fl, wl, a, b, nid); });
         SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it));
         timed("advance", bytes_per_particle::advance,
               [&] { launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, stream); });
@@ -1240,9 +1267,10 @@ int32_t slf_create(const slf_settings* settings, slf_world** out) {
     SLF_NEED(out);
     *out = nullptr;
     if (!World::valid(*settings)) return fail(SLF_ERR_INVALID_SETTINGS, "invalid settings");
-    if (settings->positions != SLF_POSITIONS_ABSOLUTE || settings->arithmetic != SLF_ARITHMETIC_EXACT ||
-        settings->warm_start)
-        return fail(SLF_ERR_UNSUPPORTED, "only absolute positions, exact arithmetic and cold starts are built");
+    if (settings->positions != SLF_POSITIONS_ABSOLUTE || settings->warm_start)
+        return fail(SLF_ERR_UNSUPPORTED, "only absolute positions and cold starts are built");
+    if (settings->arithmetic != SLF_ARITHMETIC_EXACT && settings->arithmetic != SLF_ARITHMETIC_FAST)
+        return fail(SLF_ERR_INVALID_SETTINGS, "unknown arithmetic");
     int devices = 0;
     if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
         return fail(SLF_ERR_CUDA, "no CUDA device");
