@@ -202,6 +202,30 @@ int32_t slf_get_stream(const slf_world* world, void** stream);
 /* Message of the last failed call on any handle of this thread ("" if none). */
 const char* slf_last_error(void);
 
+/* ---- the adjoint (no counterpart in the reference, which has no gradients) -------------- */
+
+/* Gradients of a loss with respect to the settings, accumulated over the taped steps. */
+typedef struct slf_param_grads {
+    double viscosity;    /* dL / d settings.viscosity */
+    double sound_speed;  /* dL / d settings.sound_speed: Tait stiffness and both viscosities */
+    double gravity[3];   /* dL / d settings.gravity */
+} slf_param_grads;
+
+/* Starts recording the steps that follow for slf_step_backward: the current state is the first
+ * checkpoint, and the state after every `checkpoint_every`-th step is kept too (segment
+ * checkpointing: the backward pass recomputes each segment from its checkpoint).  The number of
+ * particles must not change while recording.  WCSPH only. */
+int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
+/* Stops recording and frees the tape. */
+int32_t slf_tape_end(slf_world* world);
+/* Reverse pass over every step recorded since slf_tape_begin.  dpositions, dvelocities: dL/d of
+ * the current positions and velocities (xyz triples, current order, n = slf_len()).  Writes
+ * dL/d of the positions and velocities at slf_tape_begin, in the order they had then, and the
+ * parameter gradients.  Neighbour lists are the forward's, fixed within each substep; substep
+ * counts are those the forward took.  The world's state is left as it was. */
+int32_t slf_step_backward(slf_world* world, const float* dpositions, const float* dvelocities, uint64_t n,
+                          float* dpositions0, float* dvelocities0, slf_param_grads* out);
+
 /* ---- sorting without allocation ---------------------------------------------------------- */
 
 /* No counterpart in the reference: the cell sort of slf_update_neighbors for callers that

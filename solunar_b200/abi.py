@@ -201,5 +201,13 @@ class CProfileEntry(ctypes.Structure):
     ]
 
 
+class CParamGrads(ctypes.Structure):
+    _fields_ = [
+        ("viscosity", ctypes.c_double),
+        ("sound_speed", ctypes.c_double),
+        ("gravity", ctypes.c_double * 3),
+    ]
+
+
 def vec3(v) -> "ctypes.Array[ctypes.c_float]":
     return (ctypes.c_float * 3)(float(v[0]), float(v[1]), float(v[2]))

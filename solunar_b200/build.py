@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # kernels whose rounding follows the reference: no contraction, IEEE division and square root
 CUDA_SOURCES = ["kernels.cu", "noalloc.cu"]
 # the FAST arithmetic variants: contraction on
-CUDA_FAST_SOURCES = ["kernels_fast.cu"]
+CUDA_FAST_SOURCES = ["kernels_fast.cu", "adjoint.cu"]
 HOST_SOURCES = ["world.cpp"]
 
 

@@ -1,0 +1,301 @@
+// adjoint.cu -- the hand-written adjoint of the WCSPH substep (step_backward).
+//
+// The substep (src/fluid/step.rs:144-224, 229-339) maps the sorted state (x, v) to
+// x' = clamp(x + v' dt), v' = v + a dt (zeroed where clamped), with
+//   a_i = sum_j T(r_ij, u_ij, s_i + s_j, rho_i + rho_j) + walls_i + wall_viscous_i + g,
+//   T(r, u, S, R) = -grad W(r) m (S + Pi),  Pi = -nu min(0, u.r) 2 / ((|r|^2 + eps) R),
+//   rho_i = m (sum_j W(|r_ij|) + sum_w W(|r_iw|)),  s = p / rho^2,  p = max(0, B (min(rho/rho0, 1.1)^7 - 1)).
+// T is odd in (r, u), so the pair's part of the loss, a_i-bar . T_ij + a_j-bar . T_ji, equals
+// (a_i-bar - a_j-bar) . T_ij: each particle gathers its own adjoint over its own (symmetric) list,
+// with no atomics and no second list.  Neighbour lists are the forward's, fixed for the substep;
+// non-smooth points take the branch the forward took.  Particle-level adjoints are FP32; the
+// parameter gradients are summed in FP64.
+#include <cmath>
+
+#include "fluid_device.cuh"
+#include "launch.h"
+#include "reduce.cuh"
+
+namespace slf {
+
+// Neighbour j in slot k: EXACT lists hold {index, g} pairs, FAST lists indexes only.
+__device__ __forceinline__ uint32_t listed(const PairLists& l, bool packed, uint32_t i, uint32_t k) {
+    size_t at = (size_t(i >> 5) * l.cap + k) * 32u + (i & 31u);
+    return packed ? l.e[at].x : reinterpret_cast<const uint32_t*>(l.e)[at];
+}
+
+__device__ __forceinline__ uint32_t listed_count(const PairLists& l, uint32_t i) {
+    uint32_t n = l.count[i];
+    return n < l.cap ? n : l.cap;
+}
+
+// gradient factor g(d) = slope(d) / d = grad_scale (1 - d/r)^3 and its derivative in d
+__device__ __forceinline__ void grad_factor(const Params& p, float d, float& g, float& gp) {
+    float om = 1.0f - d * p.inv_radius;
+    if (om <= 0.0f) {
+        g = gp = 0.0f;
+        return;
+    }
+    g = p.grad_scale * om * om * om;
+    gp = -3.0f * p.grad_scale * om * om * p.inv_radius;
+}
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float dotf(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+
+// ---- advance and velocity update (step.rs:212-222, 305-339) ---------------------------------
+// y = x + v' dt is clamped per component; a clamped component passes no adjoint to y and zeroes
+// v'.  v' = v + a dt.  Gravity's gradient is the sum of a-bar.
+__global__ void k_adj_advance(Params p, const StepConsts* __restrict__ sc, const float4* __restrict__ vel_pre,
+                              const float4* __restrict__ xo, const float4* __restrict__ vo,
+                              float4* __restrict__ ab, float4* __restrict__ xb, float4* __restrict__ vb,
+                              double* __restrict__ grads) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    if (i < p.n) {
+        const float dt = sc->dt;
+        uint32_t flags = __float_as_uint(vel_pre[i].w);
+        float4 x = xo[i], v = vo[i];
+        float yx = flags & 1u ? 0.0f : x.x, yy = flags & 2u ? 0.0f : x.y, yz = flags & 4u ? 0.0f : x.z;
+        float wx = (flags & 1u ? 0.0f : v.x) + yx * dt;
+        float wy = (flags & 2u ? 0.0f : v.y) + yy * dt;
+        float wz = (flags & 4u ? 0.0f : v.z) + yz * dt;
+        ab[i] = make_float4(wx * dt, wy * dt, wz * dt, 0.0f);
+        xb[i] = make_float4(yx, yy, yz, 0.0f);
+        vb[i] = make_float4(wx, wy, wz, 0.0f);
+        gx = wx * dt;
+        gy = wy * dt;
+        gz = wz * dt;
+    }
+    // gravity: a_i gets g, so g-bar = sum of a-bar
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gx += __shfl_xor_sync(0xffffffffu, gx, o);
+        gy += __shfl_xor_sync(0xffffffffu, gy, o);
+        gz += __shfl_xor_sync(0xffffffffu, gz, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&grads[kGradGravity], gx);
+        atomicAdd(&grads[kGradGravity + 1], gy);
+        atomicAdd(&grads[kGradGravity + 2], gz);
+    }
+}
+
+// ---- forces (step.rs:173-211), wall viscosity (step.rs:262-301), Tait pressure (step.rs:147-172)
+__global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                      PairLists wl, int packed, const float4* __restrict__ pos,
+                                                      const float4* __restrict__ vel, const float* __restrict__ rho,
+                                                      const float* __restrict__ press,
+                                                      const float* __restrict__ scaled,
+                                                      const float4* __restrict__ walls,
+                                                      const float4* __restrict__ ab, float4* __restrict__ xb,
+                                                      float4* __restrict__ vb, float* __restrict__ rb,
+                                                      double* __restrict__ grads) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double nu_bar = 0.0, nuw_bar = 0.0, b_bar = 0.0;
+    if (i < p.n) {
+        const float nu = sc->viscosity, nuw = sc->wall_viscosity, m = p.mass;
+        float3 xi = f3(pos[i]), vi = f3(vel[i]), ai = f3(ab[i]);
+        float rho_i = rho[i], p_i = press[i], s_i = scaled[i];
+        float3 xbar = make_float3(0, 0, 0), vbar = make_float3(0, 0, 0);
+        float sbar = 0.0f, pbar = 0.0f, rbar = 0.0f;
+
+        // fluid pairs: L = (a_i-bar - a_j-bar) . T(r, u, S, R)
+        uint32_t nf = listed_count(fl, i);
+        for (uint32_t k = 0; k < nf; ++k) {
+            uint32_t j = listed(fl, packed != 0, i, k);
+            float3 r = xi - f3(__ldg(&pos[j]));
+            float d2 = dotf(r, r);
+            if (d2 <= 0.0f) continue;
+            float d = sqrtf(d2);
+            float g, gp;
+            grad_factor(p, d, g, gp);
+            float3 u = vi - f3(__ldg(&vel[j]));
+            float3 w = ai - f3(__ldg(&ab[j]));
+            float R = rho_i + __ldg(&rho[j]);
+            float S = s_i + __ldg(&scaled[j]);
+            float ur = dotf(u, r);
+            bool act = ur < 0.0f;
+            float t = act ? ur : 0.0f;
+            float den = (d2 + p.soften) * R;
+            float Pi = -nu * t * 2.0f / den;
+            float G = dotf(w, r);
+            float P = -m * g * G;  // dL/dPi and dL/dS
+            float dPi_dt = -2.0f * nu / den;
+            float dPi_dd2 = -Pi / (d2 + p.soften);
+            float c1 = -m * (S + Pi);
+            float3 dr = w * (c1 * g) + r * (c1 * G * gp / d + P * dPi_dd2 * 2.0f);
+            if (act) dr = dr + u * (P * dPi_dt);
+            xbar = xbar + dr;
+            if (act) vbar = vbar + r * (P * dPi_dt);
+            rbar += P * (-Pi / R);
+            sbar += P;
+            // viscosity enters a_i's own term: a_i-bar . dT/dnu
+            nu_bar += (double)(2.0f * m * g * t * dotf(ai, r) / den);
+        }
+
+        // walls: pressure mirrored onto the wall (step.rs:197-202)
+        uint32_t nw = listed_count(wl, i);
+        float M = s_i + p_i * p.inv_rest_sq;
+        float3 A = make_float3(0, 0, 0);  // sum of -grad W over walls, for the wall normal
+        for (uint32_t k = 0; k < nw; ++k) {
+            uint32_t j = listed(wl, packed != 0, i, k);
+            float3 r = xi - f3(__ldg(&walls[j]));
+            float d = sqrtf(dotf(r, r));
+            if (d <= 0.0f) continue;
+            float g, gp;
+            grad_factor(p, d, g, gp);
+            float ar = dotf(ai, r);
+            float mb = -m * g * ar;
+            sbar += mb;
+            pbar += mb * p.inv_rest_sq;
+            xbar = xbar + (ai * g + r * (ar * gp / d)) * (-m * M);
+            A = A - r * g;
+        }
+
+        // wall viscosity (step.rs:262-301): n = A / |A|, I = n min(v.n, 0), and per wall with
+        // tau = I.r < 0: D = -nu_w tau / ((|r|^2 + eps) rho), push -= r g m D
+        float alen = sqrtf(dotf(A, A));
+        if (nw > 0 && alen > 0.0f && isfinite(alen)) {
+            float3 nrm = A * (1.0f / alen);
+            float vn = dotf(vi, nrm);
+            float kk = fminf(vn, 0.0f);
+            float3 I = nrm * kk;
+            float3 Ibar = make_float3(0, 0, 0);
+            for (uint32_t k = 0; k < nw; ++k) {
+                uint32_t j = listed(wl, packed != 0, i, k);
+                float3 r = xi - f3(__ldg(&walls[j]));
+                float tau = dotf(I, r);
+                if (!(tau < 0.0f)) continue;
+                float d2 = dotf(r, r);
+                float d = sqrtf(d2);
+                float g, gp;
+                grad_factor(p, d, g, gp);
+                float e2 = d2 + p.soften;
+                float D = -nuw * tau / (e2 * rho_i);
+                float ar = dotf(ai, r);
+                float h = -m * g * ar;  // L = sum D h
+                float tb = h * (-nuw / (e2 * rho_i));
+                rbar += -D * h / rho_i;
+                nuw_bar += (double)(-tau / (e2 * rho_i) * h);
+                // through h(r), through |r|^2 in D, through tau = I.r
+                float3 dh = (ai * g + r * (ar * gp / d)) * (-m);
+                xbar = xbar + dh * D + r * (h * (-D / e2) * 2.0f) + I * tb;
+                Ibar = Ibar + r * tb;
+            }
+            // I = n k, k = min(v.n, 0)
+            float3 nbar = Ibar * kk;
+            if (vn < 0.0f) {
+                float kbar = dotf(Ibar, nrm);
+                vbar = vbar + nrm * kbar;
+                nbar = nbar + vi * kbar;
+            }
+            // n = A / |A|
+            float3 Abar = (nbar - nrm * dotf(nrm, nbar)) * (1.0f / alen);
+            // A = sum -r g
+            for (uint32_t k = 0; k < nw; ++k) {
+                uint32_t j = listed(wl, packed != 0, i, k);
+                float3 r = xi - f3(__ldg(&walls[j]));
+                float d = sqrtf(dotf(r, r));
+                if (d <= 0.0f) continue;
+                float g, gp;
+                grad_factor(p, d, g, gp);
+                xbar = xbar - (Abar * g + r * (dotf(Abar, r) * gp / d));
+            }
+        }
+
+        // s = p / rho^2 and the Tait equation of state
+        float ptot = pbar + sbar / (rho_i * rho_i);
+        rbar += sbar * (-2.0f * p_i / (rho_i * rho_i * rho_i));
+        float raw = rho_i * p.inv_rest;
+        float ratio = fminf(raw, 1.1f);
+        float r2 = ratio * ratio, r3 = r2 * ratio, r6 = r3 * r3;
+        if (p_i > 0.0f) {
+            b_bar = (double)(ptot * (r6 * ratio - 1.0f));
+            if (raw < 1.1f) rbar += ptot * p.stiffness * 7.0f * r6 * p.inv_rest;
+        }
+        float4 x0 = xb[i], v0 = vb[i];
+        xb[i] = make_float4(x0.x + xbar.x, x0.y + xbar.y, x0.z + xbar.z, 0.0f);
+        vb[i] = make_float4(v0.x + vbar.x, v0.y + vbar.y, v0.z + vbar.z, 0.0f);
+        rb[i] = rbar;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nu_bar += __shfl_xor_sync(0xffffffffu, nu_bar, o);
+        nuw_bar += __shfl_xor_sync(0xffffffffu, nuw_bar, o);
+        b_bar += __shfl_xor_sync(0xffffffffu, b_bar, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&grads[kGradViscosity], nu_bar);
+        atomicAdd(&grads[kGradWallViscosity], nuw_bar);
+        atomicAdd(&grads[kGradStiffness], b_bar);
+    }
+}
+
+// ---- densities (mod.rs:621-675): rho_i = m (sum_j W(r_ij) + sum_w W(r_iw)) ---------------------
+__global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, PairLists wl, int packed,
+                                                        const float4* __restrict__ pos,
+                                                        const float4* __restrict__ walls,
+                                                        const float* __restrict__ rb, float4* __restrict__ xb) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float3 xi = f3(pos[i]);
+    float rbi = rb[i];
+    float3 xbar = make_float3(0, 0, 0);
+    uint32_t nf = listed_count(fl, i);
+    for (uint32_t k = 0; k < nf; ++k) {
+        uint32_t j = listed(fl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&pos[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        xbar = xbar + r * (g * p.mass * (rbi + __ldg(&rb[j])));
+    }
+    uint32_t nw = listed_count(wl, i);
+    for (uint32_t k = 0; k < nw; ++k) {
+        uint32_t j = listed(wl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&walls[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        xbar = xbar + r * (g * p.mass * rbi);
+    }
+    float4 x0 = xb[i];
+    xb[i] = make_float4(x0.x + xbar.x, x0.y + xbar.y, x0.z + xbar.z, 0.0f);
+}
+
+// ---- the sort (mod.rs:541-566): back to the order before it ------------------------------------
+__global__ void k_adj_unsort(uint32_t n, const uint32_t* __restrict__ dest, const float4* __restrict__ xb,
+                             const float4* __restrict__ vb, float4* __restrict__ xp, float4* __restrict__ vp) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t f = dest[i];
+    xp[i] = xb[f];
+    vp[i] = vb[f];
+}
+
+static inline uint32_t adj_blocks(uint32_t n) {
+    note_launch();
+    return (n + kBlock - 1) / kBlock;
+}
+
+void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                          bool packed, const float4* pos, const float4* vel, const float* rho, const float* press,
+                          const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
+                          const float4* xo, const float4* vo, float4* ab, float4* xb, float4* vb, float* rb,
+                          float4* xp, float4* vp, double* grads, cudaStream_t s) {
+    if (!p.n) return;
+    uint32_t nb = adj_blocks(p.n);
+    k_adj_advance<<<nb, kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, ab, xb, vb, grads);
+    k_adj_force<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, press, scaled, walls,
+                                                   ab, xb, vb, rb, grads);
+    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, rb, xb);
+    k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp);
+}
+
+}  // namespace slf

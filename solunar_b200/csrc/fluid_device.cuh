@@ -86,6 +86,9 @@ struct PairLists {
     }
 };
 
+// Slots of the adjoint's FP64 parameter-gradient accumulators.
+enum GradSlot { kGradViscosity = 0, kGradWallViscosity = 1, kGradStiffness = 2, kGradGravity = 3, kGradSlots = 6 };
+
 // ---- cell tables ----------------------------------------------------------------------------
 // Dense: a start offset for every cell of a box, x-major like the reference's dense table
 // (mod.rs:218-223): range of cell c = [start[c], start[c + 1]).  Sorted: the occupied cells'

@@ -112,7 +112,8 @@ __global__ void k_rank_reorder(uint32_t n, const uint32_t* __restrict__ lin, con
                                const float* __restrict__ rho_in, const float* __restrict__ kap_in,
                                uint32_t* __restrict__ ids_out, float4* __restrict__ pos_out,
                                float4* __restrict__ vel_out, float* __restrict__ rho_out,
-                               float* __restrict__ kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st) {
+                               float* __restrict__ kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st,
+                               uint32_t* __restrict__ dest) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     // a job left undone (the fault injection of the dispatcher tests) places nothing; the count
     // of placed particles tells the host whether every particle was placed
@@ -126,6 +127,7 @@ __global__ void k_rank_reorder(uint32_t n, const uint32_t* __restrict__ lin, con
     uint32_t rank = 0;
     for (uint32_t k = b; k < e; ++k) rank += members[k] < id ? 1u : 0u;
     uint32_t f = b + rank;
+    if (dest) dest[i] = f;  // where each particle went, for the adjoint's way back
     ids_out[f] = id;
     pos_out[f] = pos_in[i];
     vel_out[f] = vel_in[i];
@@ -433,7 +435,8 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
                                                         const float* __restrict__ press,
                                                         const float* __restrict__ scaled,
                                                         const float4* __restrict__ walls, float4* __restrict__ pos_out,
-                                                        float4* __restrict__ vel_out, Status* st) {
+                                                        float4* __restrict__ vel_out, Status* st,
+                                                        float4* __restrict__ vel_pre) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < p.n;
     int3 nc = make_int3(0, 0, 0);
@@ -473,7 +476,14 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
         v.x = v.x + ax * dt;
         v.y = v.y + ay * dt;
         v.z = v.z + az * dt;
+        float4 pre = v;
         advance_one(p, dt, a, v, held, bad);
+        if (vel_pre) {
+            // the velocity before the wall zeroed any component, and which ones it zeroed
+            uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
+            pre.w = __uint_as_float(flags);
+            vel_pre[i] = pre;
+        }
         pos_out[i] = a;
         vel_out[i] = v;
         nc = cell_of(p, a.x, a.y, a.z);
@@ -737,11 +747,12 @@ void launch_scatter_members(uint32_t n, const uint32_t* lin, const uint32_t* slo
 void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start, const uint32_t* members,
                          const uint32_t* ids_in, const float4* pos_in, const float4* vel_in, const float* rho_in,
                          const float* kap_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
-                         float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, cudaStream_t s) {
+                         float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
+                         cudaStream_t s) {
     if (n)
         k_rank_reorder<<<blocks_for(n), kBlock, 0, s>>>(n, lin, start, members, ids_in, pos_in, vel_in, rho_in,
                                                         kap_in, ids_out, pos_out, vel_out, rho_out, kap_out,
-                                                        skip_begin, skip_end, st);
+                                                        skip_begin, skip_end, st, dest);
 }
 
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
@@ -757,10 +768,10 @@ void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const
 void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                         const float4* pos, const float4* vel, const float* rho, const float* press,
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                        cudaStream_t s) {
+                        float4* vel_pre, cudaStream_t s) {
     if (p.n)
         k_wcsph_force<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled, walls, pos_out,
-                                                         vel_out, st);
+                                                         vel_out, st, vel_pre);
 }
 
 size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (sizeof(DD) + sizeof(uint32_t)) + 64; }

@@ -269,7 +269,8 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_fast(Params p, const Ste
                                                              const float* __restrict__ scaled,
                                                              const float4* __restrict__ walls,
                                                              float4* __restrict__ pos_out,
-                                                             float4* __restrict__ vel_out, Status* st) {
+                                                             float4* __restrict__ vel_out, Status* st,
+                                                             float4* __restrict__ vel_pre) {
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < p.n;
@@ -308,7 +309,13 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_fast(Params p, const Ste
         v.x = fmaf(px + wv.x + p.gravity.x, dt, v.x);
         v.y = fmaf(py + wv.y + p.gravity.y, dt, v.y);
         v.z = fmaf(pz + wv.z + p.gravity.z, dt, v.z);
+        float4 pre = v;
         advance_fast(p, dt, a, v, held, bad);
+        if (vel_pre) {
+            uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
+            pre.w = __uint_as_float(flags);
+            vel_pre[i] = pre;
+        }
         pos_out[i] = a;
         vel_out[i] = v;
         nc = cell_of(p, a.x, a.y, a.z);
@@ -456,10 +463,10 @@ void launch_density_fast(const Params& p, const GridDev& fg, const GridDev& wg, 
 void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                              const float4* pos, const float4* vel, const float* rho, const float* press,
                              const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                             cudaStream_t s) {
+                             float4* vel_pre, cudaStream_t s) {
     if (p.n)
         k_wcsph_force_fast<<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled, walls,
-                                                               pos_out, vel_out, st);
+                                                               pos_out, vel_out, st, vel_pre);
 }
 
 void launch_rate_fast(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,

@@ -26,16 +26,19 @@ void launch_scatter_members(uint32_t n, const uint32_t* lin, const uint32_t* slo
 void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start, const uint32_t* members,
                          const uint32_t* ids_in, const float4* pos_in, const float4* vel_in, const float* rho_in,
                          const float* kap_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
-                         float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, cudaStream_t s);
+                         float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
+                         cudaStream_t s);
 
 // pair passes: the density pass builds the substep's neighbour lists, the others walk them
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
                     Status* st, cudaStream_t s);
+// vel_pre (optional): the velocity before the wall clamp, its w lane the bits of the components
+// the clamp zeroed (1 x, 2 y, 4 z), for the adjoint
 void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                         const float4* pos, const float4* vel, const float* rho, const float* press,
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                        cudaStream_t s);
+                        float4* vel_pre, cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
 // sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve
@@ -76,7 +79,7 @@ void launch_density_fast(const Params& p, const GridDev& fg, const GridDev& wg, 
 void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                              const float4* pos, const float4* vel, const float* rho, const float* press,
                              const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                             cudaStream_t s);
+                             float4* vel_pre, cudaStream_t s);
 void launch_rate_fast(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                       float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
                       void* partials, Status* st, cudaStream_t s);
@@ -85,6 +88,17 @@ void launch_push_fast(const Params& p, const StepConsts* sc, const PairLists& fl
 void launch_viscous_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                          const float4* pos, const float4* vel, const float* rho, const float4* walls,
                          float4* vel_out, cudaStream_t s);
+
+// The adjoint of one WCSPH substep (adjoint.cu).  Inputs are the recomputed forward of the
+// substep (sorted positions and velocities, lists, densities, pressures, the pre-clamp velocity,
+// the sort's destinations) and the adjoint of its output state xo, vo (sorted order); outputs
+// the adjoint of its input state xp, vp in the order before the sort, and adds the parameter
+// gradients (viscosity, wall viscosity, stiffness, gravity) to grads[kGradSlots].
+void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                          bool packed, const float4* pos, const float4* vel, const float* rho, const float* press,
+                          const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
+                          const float4* xo, const float4* vo, float4* ab, float4* xb, float4* vb, float* rb,
+                          float4* xp, float4* vp, double* grads, cudaStream_t s);
 
 // kernels launched through this library by the process so far
 uint64_t kernel_launches();

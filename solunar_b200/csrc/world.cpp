@@ -245,6 +245,21 @@ struct World {
     StepConsts* d_consts = nullptr;
 
     int64_t skip_job = -1;  // testing: next sort leaves this 512-particle job undone
+    // set while the adjoint recomputes a substep: the sort's destinations, the pre-clamp velocity
+    uint32_t* sort_dest = nullptr;
+    float4* vel_pre = nullptr;
+
+    // ---- the tape of slf_tape_begin: checkpoints and the substep lengths of each step ----
+    struct Tape {
+        bool on = false;
+        uint32_t every = 1;
+        uint64_t n = 0;
+        std::vector<std::vector<float>> steps;  // substep lengths of each recorded step
+        std::vector<size_t> ckpt_step;          // checkpoint c = the state before step ckpt_step[c]
+        DevBuf<float4> cpos, cvel;              // [c][n]
+        DevBuf<uint32_t> cids;
+    } tape;
+    std::vector<float>* tape_step = nullptr;  // the step being recorded
     Profiler prof;
     DevBuf<float> stage;  // xyz triples for host copies
 
@@ -276,6 +291,9 @@ struct World {
             went.release(stream);
             partials.release(stream);
             stage.release(stream);
+            tape.cpos.release(stream);
+            tape.cvel.release(stream);
+            tape.cids.release(stream);
             dwalls.release(stream);
             dwkeys.release(stream);
             cudaStreamSynchronize(stream);
@@ -491,10 +509,10 @@ struct World {
     void force_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
         if (fast())
             launch_wcsph_force_fast(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
-                                    pos[b].p, vel[b].p, d_status, stream);
+                                    pos[b].p, vel[b].p, d_status, vel_pre, stream);
         else
             launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
-                               pos[b].p, vel[b].p, d_status, stream);
+                               pos[b].p, vel[b].p, d_status, vel_pre, stream);
     }
     void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid) {
         if (fast())
@@ -818,7 +836,7 @@ struct World {
         timed("hash_reorder", bytes_per_particle::reorder, [&] {
             launch_rank_reorder(uint32_t(n), lin.p, count.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p,
                                 rho[cid].p, nullptr, ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, nullptr,
-                                job_lo, job_hi, d_status, stream);
+                                job_lo, job_hi, d_status, sort_dest, stream);
         });
         fgrid = GridDev{};
         fgrid.mode = 1;
@@ -999,8 +1017,211 @@ struct World {
     }
     uint32_t last_iterations[2] = {0, 0};
 
-    // step (step.rs:58-90)
+    // step (step.rs:58-90), recorded when a tape is on
     int32_t step(float dt, slf_report* out) {
+        if (!tape.on) return step_untaped(dt, out);
+        SLF_TRY(flush());
+        if (n != tape.n || has_domain)
+            return fail(SLF_ERR_UNSUPPORTED, "the particles changed while a tape was recording");
+        tape.steps.emplace_back();
+        tape_step = &tape.steps.back();
+        int32_t st = step_untaped(dt, out);
+        tape_step = nullptr;
+        if (st != SLF_OK) {
+            tape.steps.pop_back();
+            return st;
+        }
+        if (tape.steps.size() % tape.every == 0) SLF_TRY(checkpoint());
+        return SLF_OK;
+    }
+
+    // ---- the adjoint ---------------------------------------------------------------------------
+
+    int32_t tape_begin(uint32_t every) {
+        SLF_TRY(flush());
+        tape.on = true;
+        tape.every = std::max<uint32_t>(every, 1u);
+        tape.n = n;
+        tape.steps.clear();
+        tape.ckpt_step.clear();
+        return checkpoint();
+    }
+
+    int32_t tape_end() {
+        tape.on = false;
+        tape.steps.clear();
+        tape.ckpt_step.clear();
+        tape.cpos.release(stream);
+        tape.cvel.release(stream);
+        tape.cids.release(stream);
+        return sync();
+    }
+
+    // the committed state becomes checkpoint number ckpt_step.size()
+    int32_t checkpoint() {
+        size_t c = tape.ckpt_step.size(), m = n;
+        SLF_TRY(tape.cpos.ensure((c + 1) * m, c * m, stream));
+        SLF_TRY(tape.cvel.ensure((c + 1) * m, c * m, stream));
+        SLF_TRY(tape.cids.ensure((c + 1) * m, c * m, stream));
+        SLF_TRY(save_state(tape.cpos.p + c * m, tape.cvel.p + c * m, tape.cids.p + c * m));
+        tape.ckpt_step.push_back(tape.steps.size());
+        return SLF_OK;
+    }
+
+    int32_t save_state(float4* p, float4* v, uint32_t* id) {
+        if (!n) return SLF_OK;
+        SLF_CUDA(cudaMemcpyAsync(p, pos[cpos].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(v, vel[cpos].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(id, ids[cid].p, n * 4, cudaMemcpyDeviceToDevice, stream));
+        return SLF_OK;
+    }
+
+    int32_t load_state(const float4* p, const float4* v, const uint32_t* id) {
+        if (n) {
+            SLF_CUDA(cudaMemcpyAsync(pos[cpos].p, p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+            SLF_CUDA(cudaMemcpyAsync(vel[cpos].p, v, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+            SLF_CUDA(cudaMemcpyAsync(ids[cid].p, id, n * 4, cudaMemcpyDeviceToDevice, stream));
+        }
+        stats_fresh = false;
+        lists_valid = false;
+        return refresh_stats();
+    }
+
+    int32_t substep_retrying(float dt) {
+        uint32_t held = 0;
+        int32_t st = wcsph_substep(dt, held);
+        if (st == kRetry) st = wcsph_substep(dt, held);
+        if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
+        return st;
+    }
+
+    // step_backward: reverse over the taped steps, one checkpoint segment at a time.
+    int32_t step_backward(const float* dpos, const float* dvel, uint64_t k, float* dpos0, float* dvel0,
+                          slf_param_grads* out) {
+        if (!tape.on || tape.steps.empty()) return fail(SLF_ERR_OUT_OF_RANGE, "no steps recorded");
+        if (s.solver != SLF_SOLVER_WCSPH) return fail(SLF_ERR_UNSUPPORTED, "the adjoint covers WCSPH steps");
+        SLF_TRY(flush());
+        if (k != n || n != tape.n) return fail(SLF_ERR_INVALID_ARGUMENT, "n must equal slf_len()");
+        slf_param_grads pg{};
+        if (n == 0) {
+            if (out) *out = pg;
+            return SLF_OK;
+        }
+        // the committed state, to put back at the end
+        DevBuf<float4> spos, svel, xo, vo, xp, vp, ab, xb, vb, pre;
+        DevBuf<uint32_t> sids, dest;
+        DevBuf<float> srho, rb;
+        DevBuf<double> grads;
+        int32_t st = SLF_OK;
+        auto release = [&] {
+            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre}) b->release(stream);
+            sids.release(stream);
+            dest.release(stream);
+            srho.release(stream);
+            rb.release(stream);
+            grads.release(stream);
+        };
+        auto run = [&]() -> int32_t {
+            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre}) SLF_TRY(b->ensure(n, 0, stream));
+            SLF_TRY(sids.ensure(n, 0, stream));
+            SLF_TRY(dest.ensure(n, 0, stream));
+            SLF_TRY(srho.ensure(n, 0, stream));
+            SLF_TRY(rb.ensure(n, 0, stream));
+            SLF_TRY(grads.ensure(kGradSlots, 0, stream));
+            SLF_TRY(save_state(spos.p, svel.p, sids.p));
+            SLF_CUDA(cudaMemcpyAsync(srho.p, rho[cid].p, n * 4, cudaMemcpyDeviceToDevice, stream));
+            SLF_TRY(write_vec(xo, dpos, n));
+            SLF_TRY(write_vec(vo, dvel, n));
+            // states before each substep of a segment
+            size_t most = 0;
+            for (size_t c = 0; c < tape.ckpt_step.size(); ++c) {
+                size_t b = tape.ckpt_step[c], e = c + 1 < tape.ckpt_step.size() ? tape.ckpt_step[c + 1] : tape.steps.size();
+                size_t subs = 0;
+                for (size_t t = b; t < e; ++t) subs += tape.steps[t].size();
+                most = std::max(most, subs);
+            }
+            DevBuf<float4> gpos, gvel;
+            DevBuf<uint32_t> gids;
+            auto rel2 = [&] {
+                gpos.release(stream);
+                gvel.release(stream);
+                gids.release(stream);
+            };
+            auto segs = [&]() -> int32_t {
+                SLF_TRY(gpos.ensure(std::max<size_t>(most, 1) * n, 0, stream));
+                SLF_TRY(gvel.ensure(std::max<size_t>(most, 1) * n, 0, stream));
+                SLF_TRY(gids.ensure(std::max<size_t>(most, 1) * n, 0, stream));
+                Params p = params();
+                for (size_t c = tape.ckpt_step.size(); c-- > 0;) {
+                    size_t b = tape.ckpt_step[c];
+                    size_t e = c + 1 < tape.ckpt_step.size() ? tape.ckpt_step[c + 1] : tape.steps.size();
+                    if (b >= e) continue;
+                    std::vector<float> dts;
+                    for (size_t t = b; t < e; ++t) dts.insert(dts.end(), tape.steps[t].begin(), tape.steps[t].end());
+                    // forward through the segment, keeping the state before each substep
+                    SLF_TRY(load_state(tape.cpos.p + c * n, tape.cvel.p + c * n, tape.cids.p + c * n));
+                    for (size_t q = 0; q < dts.size(); ++q) {
+                        SLF_TRY(save_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
+                        SLF_TRY(substep_retrying(dts[q]));
+                    }
+                    // backward through it
+                    for (size_t q = dts.size(); q-- > 0;) {
+                        SLF_TRY(load_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
+                        sort_dest = dest.p;
+                        vel_pre = pre.p;
+                        int32_t rs = substep_retrying(dts[q]);
+                        sort_dest = nullptr;
+                        vel_pre = nullptr;
+                        SLF_TRY(rs);
+                        int a = (cpos + 2) % 3;
+                        SLF_CUDA(cudaMemsetAsync(grads.p, 0, kGradSlots * sizeof(double), stream));
+                        launch_adjoint_wcsph(p, d_consts, fluid_lists(), wall_lists(), !fast(), pos[a].p, vel[a].p,
+                                             rho[cid].p, press.p, scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p,
+                                             xb.p, vb.p, rb.p, xp.p, vp.p, grads.p, stream);
+                        double g[kGradSlots];
+                        SLF_CUDA(cudaMemcpyAsync(g, grads.p, sizeof(g), cudaMemcpyDeviceToHost, stream));
+                        SLF_TRY(sync());
+                        accumulate_param_grads(dts[q], g, pg);
+                        std::swap(xo, xp);
+                        std::swap(vo, vp);
+                    }
+                }
+                return SLF_OK;
+            };
+            int32_t r = segs();
+            rel2();
+            SLF_TRY(r);
+            if (dpos0) SLF_TRY(read_vec(xo, dpos0, n));
+            if (dvel0) SLF_TRY(read_vec(vo, dvel0, n));
+            // the state as it was
+            SLF_TRY(load_state(spos.p, svel.p, sids.p));
+            SLF_CUDA(cudaMemcpyAsync(rho[cid].p, srho.p, n * 4, cudaMemcpyDeviceToDevice, stream));
+            return sync();
+        };
+        st = run();
+        release();
+        sync();
+        if (st == SLF_OK && out) *out = pg;
+        return st;
+    }
+
+    // The substep's sensitivities to its derived constants, taken back to the settings:
+    // nu = min(viscosity c r, 0.05 r^2 / dt) (step.rs:254-259), nu_w = min(c r, 0.25 r^2 / dt)
+    // (step.rs:282-283), B = rest c^2 / 7 (step.rs:149); the branch the substep took decides.
+    void accumulate_param_grads(float dt, const double* g, slf_param_grads& pg) const {
+        double r = radius, c = s.sound_speed, visc = s.viscosity;
+        bool nu_free = double(s.viscosity) * c * r < 0.05 * r * r / dt;
+        bool nuw_free = c * r < 0.25 * r * r / dt;
+        if (nu_free) {
+            pg.viscosity += g[kGradViscosity] * c * r;
+            pg.sound_speed += g[kGradViscosity] * visc * r;
+        }
+        if (nuw_free) pg.sound_speed += g[kGradWallViscosity] * r;
+        pg.sound_speed += g[kGradStiffness] * 2.0 * double(s.rest_density) * c / 7.0;
+        for (int a = 0; a < 3; ++a) pg.gravity[a] += g[kGradGravity + a];
+    }
+
+    int32_t step_untaped(float dt, slf_report* out) {
         slf_report r{};
         if (out) *out = r;
         if (!std::isfinite(dt) || dt < 0.0f) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid step");
@@ -1022,6 +1243,7 @@ struct World {
                 float small = dt / float(substeps);
                 for (uint32_t i = 0; i < substeps; ++i) {
                     uint32_t held = 0;
+                    if (tape_step) tape_step->push_back(small);
                     int32_t st = wcsph_substep(small, held);
                     if (st == kRetry) st = wcsph_substep(small, held);
                     if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
@@ -1044,6 +1266,7 @@ struct World {
                     }
                     small = rmin(small, left);
                     uint32_t held = 0, its = 0;
+                    if (tape_step) tape_step->push_back(small);
                     int32_t st = dfsph_substep(small, held, its);
                     if (st == kRetry) st = dfsph_substep(small, held, its);
                     if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
@@ -1497,6 +1720,26 @@ int32_t slf_get_stream(const slf_world* world, void** stream) {
     SLF_NEED(stream);
     *stream = world->w.stream;
     return SLF_OK;
+}
+
+int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every) {
+    SLF_WORLD(world);
+    return world->w.tape_begin(checkpoint_every);
+}
+
+int32_t slf_tape_end(slf_world* world) {
+    SLF_WORLD(world);
+    return world->w.tape_end();
+}
+
+int32_t slf_step_backward(slf_world* world, const float* dpositions, const float* dvelocities, uint64_t n,
+                          float* dpositions0, float* dvelocities0, slf_param_grads* out) {
+    SLF_WORLD(world);
+    if (n) {
+        SLF_NEED(dpositions);
+        SLF_NEED(dvelocities);
+    }
+    return world->w.step_backward(dpositions, dvelocities, n, dpositions0, dvelocities0, out);
 }
 
 int32_t slf_profile_enable(slf_world* world, int32_t on) {

@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from .abi import CProfileEntry, CReport, CSettings, FluidReport, FluidSettings, PhysicsError, vec3
+from .abi import CParamGrads, CProfileEntry, CReport, CSettings, FluidReport, FluidSettings, PhysicsError, vec3
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_NAME = "libsolunar_fluid.so"
@@ -74,6 +74,9 @@ def load_library():
         "slf_profile_reset": [vp],
         "slf_kernel_launches": [u64p],
         "slf_sort_by_cell_noalloc": [vp, vp, ctypes.c_uint64, ctypes.c_float, vp, vp],
+        "slf_tape_begin": [vp, ctypes.c_uint32],
+        "slf_tape_end": [vp],
+        "slf_step_backward": [vp, fp, fp, ctypes.c_uint64, fp, fp, ctypes.POINTER(CParamGrads)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -276,6 +279,28 @@ class FluidWorld:
         v = ctypes.c_uint64()
         _check(_lib.slf_state_hash(self._h, ctypes.byref(v)))
         return v.value
+
+    # ---- the adjoint ----
+    def tape_begin(self, checkpoint_every: int = 1):
+        """Records the steps that follow for step_backward, checkpointing every k-th state."""
+        _check(_lib.slf_tape_begin(self._h, checkpoint_every))
+
+    def tape_end(self):
+        _check(_lib.slf_tape_end(self._h))
+
+    def step_backward(self, dpositions, dvelocities):
+        """dL/d(positions, velocities at tape_begin, in their order then) and dL/d settings, from
+        dL/d of the current positions and velocities (current order)."""
+        n = self.len()
+        dp = np.ascontiguousarray(dpositions, dtype=np.float32).reshape(n, 3)
+        dv = np.ascontiguousarray(dvelocities, dtype=np.float32).reshape(n, 3)
+        out_p = np.zeros((n, 3), dtype=np.float32)
+        out_v = np.zeros((n, 3), dtype=np.float32)
+        g = CParamGrads()
+        _check(_lib.slf_step_backward(self._h, _ptr(dp, ctypes.c_float), _ptr(dv, ctypes.c_float), n,
+                                      _ptr(out_p, ctypes.c_float), _ptr(out_v, ctypes.c_float), ctypes.byref(g)))
+        params = {"viscosity": g.viscosity, "sound_speed": g.sound_speed, "gravity": tuple(g.gravity)}
+        return out_p, out_v, params
 
     # ---- host-owned state, streams, profiling ----
     def write_state(self, positions, velocities):

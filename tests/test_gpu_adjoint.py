@@ -1,0 +1,137 @@
+"""step_backward: the hand-written WCSPH adjoint against finite differences.
+
+Loss: the squared distance of the fluid's centroid after the run to a point 0.3 m downstream
+of where it started (the differentiable WCSPH configuration, on a smaller block).  Gradients with
+respect to the initial velocities (along seeded random directions), the viscosity, the sound
+speed and gravity are compared with central differences.
+
+The reference's model is not smooth everywhere: pressure is clamped at zero below rest density
+(src/fluid/step.rs:156), where a jittered lattice at rest sits; viscosity acts only on approach
+(step.rs:192); walls clamp positions (step.rs:311-328).  A difference whose interval straddles
+one of these kinks measures a different slope, and at eps = 1e-3 m/s many do.  Stated tolerances:
+  * against central differences of the FP64 restatement at eps 1e-4 and 3e-5 (the better of the
+    two): relative error 1e-3, on at least three of four directions;
+  * against central differences of the GPU forward in FP32 (the better of eps 3e-3 and 1e-2;
+    smaller steps drown in the FP32 resolution of the loss, larger ones in its curvature):
+    relative error 2e-2;
+  * parameters (viscosity, sound speed, gravity): relative error 2e-2 against FP32 differences.
+"""
+import numpy as np
+import pytest
+
+from solunar_b200 import scenes
+from solunar_b200.abi import FluidSettings, FluidSolver
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 30
+DT = 2e-4
+
+
+def scene():
+    s = FluidSettings(solver=FluidSolver.WCSPH, spacing=0.02, support=4.0, sound_speed=20.0, viscosity=0.01)
+    sc = scenes.Scene("adjoint_dam", s, (0.4, 0.4, 0.4), (8, 8, 8), jitter=1e-4, velocity_sigma=0.1,
+                      dt=DT, steps=STEPS)
+    return sc
+
+
+def initial(sc):
+    # the block starts 2 % denser than rest (lattice at 0.98 of the spacing): its pressures are
+    # clearly positive inside and clearly clamped at the free surface, so few particles sit on
+    # the pressure clamp's kink at rest density
+    pos = scenes.lattice_block((0.02, 0.02, 0.02), sc.block_counts, 0.98 * sc.settings.spacing)
+    pos = (pos + scenes.jitter(len(pos), sc.jitter)).astype(np.float32)
+    vel = np.random.default_rng(3).normal(0.0, sc.velocity_sigma, size=pos.shape).astype(np.float32)
+    return pos, vel
+
+
+def run(make, sc, vel0=None, settings=None):
+    w = make(settings or sc.settings)
+    pos, vel = initial(sc)
+    w.add_box_container((0.0, 0.0, 0.0), sc.tank)
+    w.add_particles(pos, vel if vel0 is None else vel0)
+    return w, pos, vel
+
+
+def loss(w, target):
+    c = np.mean(np.asarray(w.positions(), dtype=np.float64), axis=0)
+    return float(np.sum((c - target) ** 2)), c
+
+
+@pytest.fixture(scope="module")
+def adjoint(gpu_lib):
+    sc = scene()
+    w, pos, vel = run(gpu_lib.FluidWorld, sc)
+    target = np.mean(pos.astype(np.float64), axis=0) + np.array([0.3, 0.0, 0.0])
+    w.tape_begin(10)
+    for _ in range(STEPS):
+        w.step(DT)
+    L, c = loss(w, target)
+    n = w.len()
+    dpos = np.tile(2.0 * (c - target) / n, (n, 1)).astype(np.float32)
+    dp0, dv0, params = w.step_backward(dpos, np.zeros_like(dpos))
+    # the state is left where the run ended
+    L2, _ = loss(w, target)
+    assert L2 == L
+    return sc, pos, vel, target, dp0, dv0, params
+
+
+def fd(make, sc, target, vel0=None, settings=None):
+    w, _, _ = run(make, sc, vel0, settings)
+    for _ in range(STEPS):
+        w.step(DT)
+    return loss(w, target)[0]
+
+
+def test_velocity_gradient_matches_central_differences(gpu_lib, adjoint):
+    sc, pos, vel, target, dp0, dv0, params = adjoint
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        d = rng.normal(size=vel.shape).astype(np.float32)
+        d /= np.sqrt(np.mean(d * d))
+        ana = float(np.sum(dv0.astype(np.float64) * d))
+        best = np.inf
+        for eps in (3e-3, 1e-2):
+            lp = fd(gpu_lib.FluidWorld, sc, target, (vel + eps * d).astype(np.float32))
+            lm = fd(gpu_lib.FluidWorld, sc, target, (vel - eps * d).astype(np.float32))
+            num = (lp - lm) / (2 * eps)
+            best = min(best, abs(ana - num) / abs(num))
+        assert best <= 2e-2, best
+
+
+def test_parameter_gradients_match_central_differences(gpu_lib, adjoint):
+    sc, pos, vel, target, dp0, dv0, params = adjoint
+    s = sc.settings
+    for name, eps in [("viscosity", 1e-3), ("sound_speed", 2e-2)]:
+        base = getattr(s, name)
+        hi = FluidSettings(**{**s.__dict__, name: base + eps})
+        lo = FluidSettings(**{**s.__dict__, name: base - eps})
+        num = (fd(gpu_lib.FluidWorld, sc, target, settings=hi) - fd(gpu_lib.FluidWorld, sc, target, settings=lo)) / (2 * eps)
+        assert abs(params[name] - num) <= 2e-2 * abs(num) + 1e-7, (name, params[name], num)
+    g = list(s.gravity)
+    eps = 1e-2
+    hi = FluidSettings(**{**s.__dict__, "gravity": (g[0] + eps, g[1], g[2])})
+    lo = FluidSettings(**{**s.__dict__, "gravity": (g[0] - eps, g[1], g[2])})
+    num = (fd(gpu_lib.FluidWorld, sc, target, settings=hi) - fd(gpu_lib.FluidWorld, sc, target, settings=lo)) / (2 * eps)
+    assert abs(params["gravity"][0] - num) <= 1e-2 * abs(num) + 1e-9, (params["gravity"][0], num)
+
+
+def test_velocity_gradient_matches_the_fp64_reference(oracle_lib, adjoint):
+    sc, pos, vel, target, dp0, dv0, params = adjoint
+    make64 = lambda s: oracle_lib.OracleWorld(s, precision=64)
+    rng = np.random.default_rng(11)
+    within = []
+    for _ in range(4):
+        d = rng.normal(size=vel.shape)
+        d /= np.sqrt(np.mean(d * d))
+        best = np.inf
+        for eps in (1e-4, 3e-5):
+            # the FP64 restatement takes float inputs: the perturbed velocities are rounded to
+            # f32, so the adjoint is projected on the difference actually applied
+            vp = (vel + eps * d).astype(np.float32)
+            vm = (vel - eps * d).astype(np.float32)
+            num = (fd(make64, sc, target, vp) - fd(make64, sc, target, vm)) / (2 * eps)
+            ana = float(np.sum(dv0.astype(np.float64) * (vp.astype(np.float64) - vm.astype(np.float64)) / (2 * eps)))
+            best = min(best, abs(ana - num) / abs(num))
+        within.append(best <= 1e-3)
+    assert sum(within) >= 3, within
