@@ -214,7 +214,7 @@ typedef struct slf_param_grads {
 /* Starts recording the steps that follow for slf_step_backward: the current state is the first
  * checkpoint, and the state after every `checkpoint_every`-th step is kept too (segment
  * checkpointing: the backward pass recomputes each segment from its checkpoint).  The number of
- * particles must not change while recording.  WCSPH only. */
+ * particles must not change while recording.  WCSPH and DFSPH steps. */
 int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
 /* Stops recording and frees the tape. */
 int32_t slf_tape_end(slf_world* world);
@@ -222,7 +222,8 @@ int32_t slf_tape_end(slf_world* world);
  * the current positions and velocities (xyz triples, current order, n = slf_len()).  Writes
  * dL/d of the positions and velocities at slf_tape_begin, in the order they had then, and the
  * parameter gradients.  Neighbour lists are the forward's, fixed within each substep; substep
- * counts are those the forward took.  The world's state is left as it was. */
+ * lengths and DFSPH solver iteration counts are those the forward took.  The world's state is
+ * left as it was. */
 int32_t slf_step_backward(slf_world* world, const float* dpositions, const float* dvelocities, uint64_t n,
                           float* dpositions0, float* dvelocities0, slf_param_grads* out);
 

@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
                                                       const float4* __restrict__ walls,
                                                       const float4* __restrict__ ab, float4* __restrict__ xb,
                                                       float4* __restrict__ vb, float* __restrict__ rb,
-                                                      double* __restrict__ grads) {
+                                                      double* __restrict__ grads, int add_rho) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double nu_bar = 0.0, nuw_bar = 0.0, b_bar = 0.0;
     if (i < p.n) {
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         float4 x0 = xb[i], v0 = vb[i];
         xb[i] = make_float4(x0.x + xbar.x, x0.y + xbar.y, x0.z + xbar.z, 0.0f);
         vb[i] = make_float4(v0.x + vbar.x, v0.y + vbar.y, v0.z + vbar.z, 0.0f);
-        rb[i] = rbar;
+        rb[i] = add_rho ? rb[i] + rbar : rbar;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -279,6 +279,230 @@ __global__ void k_adj_unsort(uint32_t n, const uint32_t* __restrict__ dest, cons
     vp[i] = vb[f];
 }
 
+// ---- DFSPH (dfsph.rs:79-275) --------------------------------------------------------------------
+// Within a substep the solves are linear in the velocities apart from the clamps of the stiffness:
+// push_apart (dfsph.rs:184-216) is the transpose of density_rate (dfsph.rs:166-181) up to -dt, so
+// the adjoint of a push is a rate pass on the velocity adjoint, and the adjoint of a rate pass is
+// a push pass on the rate adjoint.
+
+// advance (step.rs:305-339): the clamp passes nothing through clamped components
+__global__ void k_adj_advance_dfsph(Params p, const StepConsts* __restrict__ sc, const float4* __restrict__ vel_pre,
+                                    const float4* __restrict__ xo, const float4* __restrict__ vo,
+                                    float4* __restrict__ xb, float4* __restrict__ w) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const float dt = sc->dt;
+    uint32_t flags = __float_as_uint(vel_pre[i].w);
+    float4 x = xo[i], v = vo[i];
+    float yx = flags & 1u ? 0.0f : x.x, yy = flags & 2u ? 0.0f : x.y, yz = flags & 4u ? 0.0f : x.z;
+    xb[i] = make_float4(yx, yy, yz, 0.0f);
+    w[i] = make_float4((flags & 1u ? 0.0f : v.x) + yx * dt, (flags & 2u ? 0.0f : v.y) + yy * dt,
+                       (flags & 4u ? 0.0f : v.z) + yz * dt, 0.0f);
+}
+
+// One iteration's stiffness, back from the velocity adjoint w after its push: kappa-bar = -dt
+// rate(w); then through kappa = phi(rate) alpha (dfsph.rs:241-259).
+template <int WHICH>
+__global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                      PairLists wl, int packed, const float4* __restrict__ pos,
+                                                      const float4* __restrict__ walls,
+                                                      const float4* __restrict__ w, const float* __restrict__ rate,
+                                                      const float* __restrict__ alpha, const float* __restrict__ rho,
+                                                      float* __restrict__ ratebar, float* __restrict__ kappa,
+                                                      float* __restrict__ abar, float* __restrict__ rb) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const float dt = sc->dt, m = p.mass;
+    float3 xi = f3(pos[i]), wi = f3(w[i]);
+    float acc = 0.0f;
+    uint32_t nf = listed_count(fl, i);
+    for (uint32_t k = 0; k < nf; ++k) {
+        uint32_t j = listed(fl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&pos[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        acc += dotf(wi - f3(__ldg(&w[j])), r) * g;
+    }
+    uint32_t nw = listed_count(wl, i);
+    for (uint32_t k = 0; k < nw; ++k) {
+        uint32_t j = listed(wl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&walls[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        acc += dotf(wi, r) * g;
+    }
+    float kbar = -dt * m * acc;
+    float ri = rate[i], ai = alpha[i];
+    float phi, dphi, dphi_rho = 0.0f;
+    if (WHICH == 1) {
+        float over = rho[i] + dt * ri - p.rest;
+        bool on = over > 0.0f;
+        phi = on ? over / sc->dt_sq : 0.0f;
+        dphi = on ? 1.0f / dt : 0.0f;
+        dphi_rho = on ? 1.0f / sc->dt_sq : 0.0f;
+    } else {
+        bool on = fl.count[i] + wl.count[i] >= 20u && ri > 0.0f;
+        phi = on ? ri / dt : 0.0f;
+        dphi = on ? 1.0f / dt : 0.0f;
+    }
+    kappa[i] = phi * ai;
+    ratebar[i] = kbar * ai * dphi;
+    abar[i] += kbar * phi;
+    if (WHICH == 1) rb[i] += kbar * ai * dphi_rho;
+}
+
+// The velocity adjoint before the iteration: w plus the rate pass's transpose (a push on the
+// rate adjoint); and the positions' share of both passes, through grad W.
+__global__ void __launch_bounds__(kBlock) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                     PairLists wl, int packed, const float4* __restrict__ pos,
+                                                     const float4* __restrict__ walls, const float4* __restrict__ w,
+                                                     const float* __restrict__ kappa,
+                                                     const float* __restrict__ ratebar,
+                                                     const float4* __restrict__ vel, float4* __restrict__ wout,
+                                                     float4* __restrict__ xb) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const float dt = sc->dt, m = p.mass;
+    float3 xi = f3(pos[i]), wi = f3(w[i]), vi = f3(vel[i]);
+    float ki = kappa[i], rbi = ratebar[i];
+    float3 vacc = make_float3(0, 0, 0), xacc = make_float3(0, 0, 0);
+    uint32_t nf = listed_count(fl, i);
+    for (uint32_t k = 0; k < nf; ++k) {
+        uint32_t j = listed(fl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&pos[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        float rbj = __ldg(&ratebar[j]);
+        vacc = vacc + r * (g * m * (rbi + rbj));
+        // c . grad W(r) with c = -dt m (k_i + k_j)(w_i - w_j) + m (rb_i + rb_j)(v_i - v_j)
+        float3 c = (wi - f3(__ldg(&w[j]))) * (-dt * m * (ki + __ldg(&kappa[j]))) +
+                   (vi - f3(__ldg(&vel[j]))) * (m * (rbi + rbj));
+        xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
+    }
+    uint32_t nw = listed_count(wl, i);
+    for (uint32_t k = 0; k < nw; ++k) {
+        uint32_t j = listed(wl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&walls[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        vacc = vacc + r * (g * m * rbi);
+        float3 c = wi * (-dt * m * ki) + vi * (m * rbi);
+        xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
+    }
+    wout[i] = make_float4(wi.x + vacc.x, wi.y + vacc.y, wi.z + vacc.z, 0.0f);
+    float4 x0 = xb[i];
+    xb[i] = make_float4(x0.x + xacc.x, x0.y + xacc.y, x0.z + xacc.z, 0.0f);
+}
+
+// viscosity + gravity (dfsph.rs:90-99): a-bar = dt w, gravity-bar = sum a-bar
+__global__ void k_adj_scale(Params p, const StepConsts* __restrict__ sc, const float4* __restrict__ w,
+                            float4* __restrict__ ab, double* __restrict__ grads) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    if (i < p.n) {
+        float4 v = w[i];
+        float dt = sc->dt;
+        ab[i] = make_float4(v.x * dt, v.y * dt, v.z * dt, 0.0f);
+        gx = v.x * dt;
+        gy = v.y * dt;
+        gz = v.z * dt;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gx += __shfl_xor_sync(0xffffffffu, gx, o);
+        gy += __shfl_xor_sync(0xffffffffu, gy, o);
+        gz += __shfl_xor_sync(0xffffffffu, gz, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&grads[kGradGravity], gx);
+        atomicAdd(&grads[kGradGravity + 1], gy);
+        atomicAdd(&grads[kGradGravity + 2], gz);
+    }
+}
+
+// factors (dfsph.rs:138-163): alpha = 1 / T, T = |G|^2 + sum_j |m grad W_ij|^2,
+// G = sum_j m grad W_ij + sum_w m grad W_iw.  First G and T-bar = -alpha-bar alpha^2 per particle.
+__global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists fl, PairLists wl, int packed,
+                                                           const float4* __restrict__ pos,
+                                                           const float4* __restrict__ walls,
+                                                           const float* __restrict__ alpha,
+                                                           const float* __restrict__ abar, float4* __restrict__ gt) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float3 xi = f3(pos[i]);
+    float3 G = make_float3(0, 0, 0);
+    uint32_t nf = listed_count(fl, i);
+    for (uint32_t k = 0; k < nf; ++k) {
+        uint32_t j = listed(fl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&pos[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        G = G + r * (g * p.mass);
+    }
+    uint32_t nw = listed_count(wl, i);
+    for (uint32_t k = 0; k < nw; ++k) {
+        uint32_t j = listed(wl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&walls[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        G = G + r * (g * p.mass);
+    }
+    float a = alpha[i];
+    gt[i] = make_float4(G.x, G.y, G.z, -abar[i] * a * a);
+}
+
+__global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, PairLists wl, int packed,
+                                                      const float4* __restrict__ pos,
+                                                      const float4* __restrict__ walls,
+                                                      const float4* __restrict__ gt, float4* __restrict__ xb) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const float m = p.mass;
+    float3 xi = f3(pos[i]);
+    float4 own = gt[i];
+    float3 Gi = f3(own);
+    float tbi = own.w;
+    float3 xacc = make_float3(0, 0, 0);
+    uint32_t nf = listed_count(fl, i);
+    for (uint32_t k = 0; k < nf; ++k) {
+        uint32_t j = listed(fl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&pos[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        float3 gw = r * (g * m);
+        float4 oj = __ldg(&gt[j]);
+        float3 c = (Gi + gw) * (2.0f * m * tbi) - (f3(oj) - gw) * (2.0f * m * oj.w);
+        xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
+    }
+    uint32_t nw = listed_count(wl, i);
+    for (uint32_t k = 0; k < nw; ++k) {
+        uint32_t j = listed(wl, packed != 0, i, k);
+        float3 r = xi - f3(__ldg(&walls[j]));
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        float3 c = Gi * (2.0f * m * tbi);
+        xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
+    }
+    float4 x0 = xb[i];
+    xb[i] = make_float4(x0.x + xacc.x, x0.y + xacc.y, x0.z + xacc.z, 0.0f);
+}
+
 static inline uint32_t adj_blocks(uint32_t n) {
     note_launch();
     return (n + kBlock - 1) / kBlock;
@@ -293,9 +517,55 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
     uint32_t nb = adj_blocks(p.n);
     k_adj_advance<<<nb, kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, ab, xb, vb, grads);
     k_adj_force<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, press, scaled, walls,
-                                                   ab, xb, vb, rb, grads);
+                                                   ab, xb, vb, rb, grads, 0);
     k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, rb, xb);
     k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp);
+}
+
+
+
+void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float4* vel_pre, const float4* xo,
+                              const float4* vo, float4* xb, float4* w, cudaStream_t s) {
+    if (p.n) k_adj_advance_dfsph<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, xb, w);
+}
+
+void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                          bool packed, const float4* pos, const float4* walls, const float4* w, const float* rate,
+                          const float* alpha, const float* rho, const float4* vel, float* ratebar, float* kappa,
+                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s) {
+    if (!p.n) return;
+    if (which == 1)
+        k_adj_kappa<1><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
+                                                          rho, ratebar, kappa, abar, rb);
+    else
+        k_adj_kappa<0><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
+                                                          rho, ratebar, kappa, abar, rb);
+    k_adj_push<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, kappa, ratebar, vel,
+                                                  wout, xb);
+}
+
+void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,
+                          const float4* pos, const float4* vel, const float* rho, const float* zeros,
+                          const float4* walls, float4* w, float4* ab, float4* xb, float* rb, double* grads,
+                          cudaStream_t s) {
+    if (!p.n) return;
+    k_adj_scale<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, w, ab, grads);
+    k_adj_force<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, zeros, zeros, walls,
+                                                   ab, xb, w, rb, grads, 1);
+}
+
+void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, bool packed,
+                                const float4* pos, const float4* walls, const float* alpha, const float* abar,
+                                float4* gt, const float* rb, float4* xb, cudaStream_t s) {
+    if (!p.n) return;
+    k_adj_alpha_prep<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, alpha, abar, gt);
+    k_adj_alpha<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, gt, xb);
+    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, rb, xb);
+}
+
+void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const float4* vb, float4* xp, float4* vp,
+                       cudaStream_t s) {
+    if (n) k_adj_unsort<<<adj_blocks(n), kBlock, 0, s>>>(n, dest, xb, vb, xp, vp);
 }
 
 }  // namespace slf

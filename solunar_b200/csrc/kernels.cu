@@ -503,7 +503,8 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, 
                                                  const float4* __restrict__ vel, const float* __restrict__ rho,
                                                  const float* __restrict__ alpha, const float4* __restrict__ walls,
                                                  float* __restrict__ kappa_w, DD* __restrict__ partial,
-                                                 uint32_t* __restrict__ partial_loaded, Status* st) {
+                                                 uint32_t* __restrict__ partial_loaded, Status* st,
+                                                 float* __restrict__ rate_out) {
     // a solve that already stopped leaves the rest of its batch of launches idle
     if (__ldcg(&st->settled)) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -523,6 +524,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, 
             rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
         });
         rate = rate * p.mass;
+        if (rate_out) rate_out[i] = rate;  // recorded for the adjoint
         float target, error;
         if (WHICH == 1) {
             float over = fmaxf(rho[i] + dt * rate - p.rest, 0.0f);
@@ -611,7 +613,8 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params 
 }
 
 __global__ void k_advance(Params p, const StepConsts* __restrict__ sc, const float4* __restrict__ pos_in,
-                          float4* __restrict__ pos_out, float4* __restrict__ vel, Status* st) {
+                          float4* __restrict__ pos_out, float4* __restrict__ vel, Status* st,
+                          float4* __restrict__ vel_pre) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < p.n;
     int3 nc = make_int3(0, 0, 0);
@@ -620,7 +623,13 @@ __global__ void k_advance(Params p, const StepConsts* __restrict__ sc, const flo
     if (valid) {
         float4 a = pos_in[i];
         float4 v = vel[i];
+        float4 pre = v;
         advance_one(p, sc->dt, a, v, held, bad);
+        if (vel_pre) {
+            uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
+            pre.w = __uint_as_float(flags);
+            vel_pre[i] = pre;
+        }
         pos_out[i] = a;
         vel[i] = v;
         nc = cell_of(p, a.x, a.y, a.z);
@@ -778,17 +787,17 @@ size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (size
 
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 void* partials, Status* st, cudaStream_t s) {
+                 void* partials, Status* st, float* rate_out, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = blocks_for(p.n);
     DD* part = static_cast<DD*>(partials);
     uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
     if (which == 0)
         k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
-                                        part, loaded, st);
+                                        part, loaded, st, rate_out);
     else
         k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
-                                        part, loaded, st);
+                                        part, loaded, st, rate_out);
 }
 
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
@@ -802,8 +811,8 @@ void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, 
 }
 
 void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,
-                    Status* st, cudaStream_t s) {
-    if (p.n) k_advance<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, pos_in, pos_out, vel, st);
+                    Status* st, float4* vel_pre, cudaStream_t s) {
+    if (p.n) k_advance<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, pos_in, pos_out, vel, st, vel_pre);
 }
 
 void launch_list_count(const Params& p, const GridDev& g, const float4* pos, const float4* pts, uint32_t* counts,

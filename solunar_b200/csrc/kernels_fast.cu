@@ -334,7 +334,8 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
                                                       const float* __restrict__ alpha,
                                                       const float4* __restrict__ walls, float* __restrict__ kappa_w,
                                                       DD* __restrict__ partial,
-                                                      uint32_t* __restrict__ partial_loaded, Status* st) {
+                                                      uint32_t* __restrict__ partial_loaded, Status* st,
+                                                      float* __restrict__ rate_out) {
     if (__ldcg(&st->settled)) return;
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -356,6 +357,7 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
             rate = fmaf(g, fmaf(v.x, rx, fmaf(v.y, ry, v.z * rz)), rate);
         });
         rate = rate * p.mass;
+        if (rate_out) rate_out[i] = rate;
         float target, error;
         if (WHICH == 1) {
             float over = fmaxf(fmaf(dt, rate, rho[i]) - p.rest, 0.0f);
@@ -471,17 +473,17 @@ void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLi
 
 void launch_rate_fast(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                       float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                      void* partials, Status* st, cudaStream_t s) {
+                      void* partials, Status* st, float* rate_out, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = fast_blocks(p.n);
     DD* part = static_cast<DD*>(partials);
     uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
     if (which == 0)
         k_rate_fast<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls,
-                                             reinterpret_cast<float*>(pos), part, loaded, st);
+                                             reinterpret_cast<float*>(pos), part, loaded, st, rate_out);
     else
         k_rate_fast<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls,
-                                             reinterpret_cast<float*>(pos), part, loaded, st);
+                                             reinterpret_cast<float*>(pos), part, loaded, st, rate_out);
 }
 
 void launch_push_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,

@@ -43,15 +43,16 @@ size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
 // sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve
 // has settled, so a batch of iterations can be queued ahead of the check that ends it.
+// rate_out (optional): each particle's density rate, recorded for the adjoint
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 void* partials, Status* st, cudaStream_t s);
+                 void* partials, Status* st, float* rate_out, cudaStream_t s);
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                  float4* vel, const float4* walls, const Status* st, cudaStream_t s);
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                     const float4* vel, const float* rho, const float4* walls, float4* vel_out, cudaStream_t s);
 void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,
-                    Status* st, cudaStream_t s);
+                    Status* st, float4* vel_pre, cudaStream_t s);
 
 // neighbour lists on demand
 void launch_list_count(const Params& p, const GridDev& g, const float4* pos, const float4* pts, uint32_t* counts,
@@ -82,7 +83,7 @@ void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLi
                              float4* vel_pre, cudaStream_t s);
 void launch_rate_fast(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                       float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                      void* partials, Status* st, cudaStream_t s);
+                      void* partials, Status* st, float* rate_out, cudaStream_t s);
 void launch_push_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                       const float4* pos, float4* vel, const float4* walls, const Status* st, cudaStream_t s);
 void launch_viscous_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
@@ -99,6 +100,25 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
                           const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
                           const float4* xo, const float4* vo, float4* ab, float4* xb, float4* vb, float* rb,
                           float4* xp, float4* vp, double* grads, cudaStream_t s);
+
+// The adjoint of a DFSPH substep, in pieces the host strings together (adjoint.cu): the advance;
+// one solver iteration (kappa, then the velocity adjoint before its push); the viscosity; the
+// factors and the densities; and the way back through the sort.
+void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float4* vel_pre, const float4* xo,
+                              const float4* vo, float4* xb, float4* w, cudaStream_t s);
+void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                          bool packed, const float4* pos, const float4* walls, const float4* w, const float* rate,
+                          const float* alpha, const float* rho, const float4* vel, float* ratebar, float* kappa,
+                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s);
+void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,
+                          const float4* pos, const float4* vel, const float* rho, const float* zeros,
+                          const float4* walls, float4* w, float4* ab, float4* xb, float* rb, double* grads,
+                          cudaStream_t s);
+void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, bool packed,
+                                const float4* pos, const float4* walls, const float* alpha, const float* abar,
+                                float4* gt, const float* rb, float4* xb, cudaStream_t s);
+void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const float4* vb, float4* xp, float4* vp,
+                       cudaStream_t s);
 
 // kernels launched through this library by the process so far
 uint64_t kernel_launches();

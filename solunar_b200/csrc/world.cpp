@@ -514,13 +514,14 @@ struct World {
             launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
                                pos[b].p, vel[b].p, d_status, vel_pre, stream);
     }
-    void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid) {
+    void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid,
+                   float* rate_out = nullptr) {
         if (fast())
             launch_rate_fast(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p,
-                             d_status, stream);
+                             d_status, rate_out, stream);
         else
             launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p, d_status,
-                        stream);
+                        rate_out, stream);
     }
     void push_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v) {
         if (fast()) launch_push_fast(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
@@ -1000,7 +1001,7 @@ struct World {
         timed("viscosity", bytes_per_particle::viscosity, [&] { viscous_pass(p, fl, wl, a, b, nid); });
         SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it));
         timed("advance", bytes_per_particle::advance,
-              [&] { launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, stream); });
+              [&] { launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, vel_pre, stream); });
         SLF_TRY(read_status());
         if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
         held = h_status->held;
@@ -1088,18 +1089,82 @@ struct World {
     }
 
     int32_t substep_retrying(float dt) {
-        uint32_t held = 0;
-        int32_t st = wcsph_substep(dt, held);
-        if (st == kRetry) st = wcsph_substep(dt, held);
+        uint32_t held = 0, its = 0;
+        auto once = [&] { return s.solver == SLF_SOLVER_WCSPH ? wcsph_substep(dt, held) : dfsph_substep(dt, held, its); };
+        int32_t st = once();
+        if (st == kRetry) st = once();
         if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
         return st;
+    }
+
+    // A DFSPH substep run again for its adjoint, keeping what the backward pass needs: each
+    // solver iteration's velocities and density rates, the velocities the viscosity read and the
+    // advance's clamp flags.  Iterations run one at a time (the forward's batches only save host
+    // waits); the counts equal the forward's because the recompute is bit-identical.
+    struct DfsphRecord {
+        DevBuf<float4> div_vel, den_vel, va, pre;
+        DevBuf<float> div_rate, den_rate;
+        uint32_t div_n = 0, den_n = 0;
+        void release(cudaStream_t st) {
+            for (auto* b : {&div_vel, &den_vel, &va, &pre}) b->release(st);
+            div_rate.release(st);
+            den_rate.release(st);
+        }
+    };
+
+    int32_t solve_record(int which, const Params& p, int a, float4* v, int nid, DevBuf<float4>& vels,
+                         DevBuf<float>& rates, uint32_t& count) {
+        count = 0;
+        PairLists fl = fluid_lists(), wl = wall_lists();
+        SLF_CUDA(cudaMemsetAsync(&d_status->settled, 0, 4, stream));
+        SLF_CUDA(cudaMemsetAsync(&d_status->iterations, 0, 4, stream));
+        for (;;) {
+            SLF_TRY(rates.ensure((size_t(count) + 1) * n, size_t(count) * n, stream));
+            SLF_TRY(vels.ensure((size_t(count) + 1) * n, size_t(count) * n, stream));
+            rate_pass(which, p, fl, wl, a, v, nid, rates.p + size_t(count) * n);
+            SLF_TRY(read_status());
+            SLF_TRY(lists_fit());
+            if (h_status->settled) return SLF_OK;
+            if (count > s.max_iterations) return fail(SLF_ERR_TIMEOUT, "solver stop flag never set");
+            SLF_CUDA(cudaMemcpyAsync(vels.p + size_t(count) * n, v, n * sizeof(float4), cudaMemcpyDeviceToDevice,
+                                     stream));
+            push_pass(p, fl, wl, a, v);
+            count += 1;
+        }
+    }
+
+    int32_t dfsph_substep_record(float dt, DfsphRecord& rec) {
+        Params p = params();
+        int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
+        SLF_TRY(sort_into(a));
+        int nid = 1 - cid;
+        SLF_TRY(reset_status());
+        launch_set_consts(consts(dt), d_consts, stream);
+        PairLists fl = fluid_lists(), wl = wall_lists();
+        density_pass(p, pos[a].p, fl, wl, rho[nid].p);
+        SLF_TRY(solve_record(0, p, a, vel[a].p, nid, rec.div_vel, rec.div_rate, rec.div_n));
+        SLF_TRY(rec.va.ensure(n, 0, stream));
+        SLF_CUDA(cudaMemcpyAsync(rec.va.p, vel[a].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        viscous_pass(p, fl, wl, a, b, nid);
+        SLF_TRY(solve_record(1, p, a, vel[b].p, nid, rec.den_vel, rec.den_rate, rec.den_n));
+        SLF_TRY(rec.pre.ensure(n, 0, stream));
+        SLF_TRY(reset_status());
+        launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, rec.pre.p, stream);
+        SLF_TRY(read_status());
+        if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        cpos = b;
+        cid = nid;
+        lists_pos = a;
+        lists_n = n;
+        lists_valid = true;
+        stats_fresh = true;
+        return SLF_OK;
     }
 
     // step_backward: reverse over the taped steps, one checkpoint segment at a time.
     int32_t step_backward(const float* dpos, const float* dvel, uint64_t k, float* dpos0, float* dvel0,
                           slf_param_grads* out) {
         if (!tape.on || tape.steps.empty()) return fail(SLF_ERR_OUT_OF_RANGE, "no steps recorded");
-        if (s.solver != SLF_SOLVER_WCSPH) return fail(SLF_ERR_UNSUPPORTED, "the adjoint covers WCSPH steps");
         SLF_TRY(flush());
         if (k != n || n != tape.n) return fail(SLF_ERR_INVALID_ARGUMENT, "n must equal slf_len()");
         slf_param_grads pg{};
@@ -1108,25 +1173,27 @@ struct World {
             return SLF_OK;
         }
         // the committed state, to put back at the end
-        DevBuf<float4> spos, svel, xo, vo, xp, vp, ab, xb, vb, pre;
+        DevBuf<float4> spos, svel, xo, vo, xp, vp, ab, xb, vb, pre, gt;
         DevBuf<uint32_t> sids, dest;
-        DevBuf<float> srho, rb;
+        DevBuf<float> srho, rb, abar, ratebar, kap, zeros;
         DevBuf<double> grads;
+        DfsphRecord rec;
         int32_t st = SLF_OK;
         auto release = [&] {
-            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre}) b->release(stream);
+            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt}) b->release(stream);
+            for (auto* b : {&srho, &rb, &abar, &ratebar, &kap, &zeros}) b->release(stream);
             sids.release(stream);
             dest.release(stream);
-            srho.release(stream);
-            rb.release(stream);
             grads.release(stream);
+            rec.release(stream);
         };
         auto run = [&]() -> int32_t {
-            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre}) SLF_TRY(b->ensure(n, 0, stream));
+            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt})
+                SLF_TRY(b->ensure(n, 0, stream));
+            for (auto* b : {&srho, &rb, &abar, &ratebar, &kap, &zeros}) SLF_TRY(b->ensure(n, 0, stream));
+            SLF_CUDA(cudaMemsetAsync(zeros.p, 0, n * 4, stream));
             SLF_TRY(sids.ensure(n, 0, stream));
             SLF_TRY(dest.ensure(n, 0, stream));
-            SLF_TRY(srho.ensure(n, 0, stream));
-            SLF_TRY(rb.ensure(n, 0, stream));
             SLF_TRY(grads.ensure(kGradSlots, 0, stream));
             SLF_TRY(save_state(spos.p, svel.p, sids.p));
             SLF_CUDA(cudaMemcpyAsync(srho.p, rho[cid].p, n * 4, cudaMemcpyDeviceToDevice, stream));
@@ -1169,15 +1236,54 @@ struct World {
                         SLF_TRY(load_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
                         sort_dest = dest.p;
                         vel_pre = pre.p;
-                        int32_t rs = substep_retrying(dts[q]);
+                        int32_t rs;
+                        if (s.solver == SLF_SOLVER_WCSPH) {
+                            rs = substep_retrying(dts[q]);
+                        } else {
+                            rs = dfsph_substep_record(dts[q], rec);
+                            if (rs == kRetry) {
+                                SLF_TRY(load_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
+                                rs = dfsph_substep_record(dts[q], rec);
+                            }
+                            if (rs == kRetry) rs = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
+                        }
                         sort_dest = nullptr;
                         vel_pre = nullptr;
                         SLF_TRY(rs);
                         int a = (cpos + 2) % 3;
                         SLF_CUDA(cudaMemsetAsync(grads.p, 0, kGradSlots * sizeof(double), stream));
-                        launch_adjoint_wcsph(p, d_consts, fluid_lists(), wall_lists(), !fast(), pos[a].p, vel[a].p,
-                                             rho[cid].p, press.p, scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p,
-                                             xb.p, vb.p, rb.p, xp.p, vp.p, grads.p, stream);
+                        PairLists fl = fluid_lists(), wl = wall_lists();
+                        bool packed = !fast();
+                        if (s.solver == SLF_SOLVER_WCSPH) {
+                            launch_adjoint_wcsph(p, d_consts, fl, wl, packed, pos[a].p, vel[a].p, rho[cid].p, press.p,
+                                                 scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p, xb.p, vb.p, rb.p,
+                                                 xp.p, vp.p, grads.p, stream);
+                        } else {
+                            // advance, density solve, viscosity, divergence solve, factors,
+                            // densities, sort: the substep's steps backwards
+                            launch_adj_advance_dfsph(p, d_consts, rec.pre.p, xo.p, vo.p, xb.p, vb.p, stream);
+                            SLF_CUDA(cudaMemsetAsync(rb.p, 0, n * 4, stream));
+                            SLF_CUDA(cudaMemsetAsync(abar.p, 0, n * 4, stream));
+                            for (uint32_t it = rec.den_n; it-- > 0;) {
+                                launch_adj_iteration(1, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
+                                                     rec.den_rate.p + size_t(it) * n, alpha.p, rho[cid].p,
+                                                     rec.den_vel.p + size_t(it) * n, ratebar.p, kap.p, abar.p, rb.p,
+                                                     vp.p, xb.p, stream);
+                                std::swap(vb, vp);
+                            }
+                            launch_adj_viscosity(p, d_consts, fl, wl, packed, pos[a].p, rec.va.p, rho[cid].p, zeros.p,
+                                                 dwalls.p, vb.p, ab.p, xb.p, rb.p, grads.p, stream);
+                            for (uint32_t it = rec.div_n; it-- > 0;) {
+                                launch_adj_iteration(0, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
+                                                     rec.div_rate.p + size_t(it) * n, alpha.p, rho[cid].p,
+                                                     rec.div_vel.p + size_t(it) * n, ratebar.p, kap.p, abar.p, rb.p,
+                                                     vp.p, xb.p, stream);
+                                std::swap(vb, vp);
+                            }
+                            launch_adj_factors_density(p, fl, wl, packed, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p,
+                                                       rb.p, xb.p, stream);
+                            launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream);
+                        }
                         double g[kGradSlots];
                         SLF_CUDA(cudaMemcpyAsync(g, grads.p, sizeof(g), cudaMemcpyDeviceToHost, stream));
                         SLF_TRY(sync());

@@ -135,3 +135,78 @@ def test_velocity_gradient_matches_the_fp64_reference(oracle_lib, adjoint):
             best = min(best, abs(ana - num) / abs(num))
         within.append(best <= 1e-3)
     assert sum(within) >= 3, within
+
+
+# ---- DFSPH: the same loss through 5 substeps (25 solver iterations), tape checkpoint every 2 ----
+
+DFSPH_STEPS = 5
+DFSPH_DT = 1e-3
+
+
+def dfsph_settings(**kw):
+    # viscosity 0.01: viscosity(dt) = min(0.01 c r, 0.05 r^2 / dt) is on its free branch here
+    return FluidSettings(**{**dict(solver=FluidSolver.DFSPH, spacing=0.02, support=2.0, viscosity=0.01), **kw})
+
+
+def dfsph_run(make, vel0=None, settings=None):
+    w = make(settings or dfsph_settings())
+    pos = scenes.lattice_block((0.02, 0.02, 0.02), (10, 10, 10), 0.98 * 0.02)
+    pos = (pos + scenes.jitter(len(pos), 1e-4)).astype(np.float32)
+    vel = np.random.default_rng(3).normal(0.0, 0.1, size=pos.shape).astype(np.float32)
+    w.add_box_container((0.0, 0.0, 0.0), (0.5, 0.5, 0.5))
+    w.add_particles(pos, vel if vel0 is None else vel0)
+    return w, pos, vel
+
+
+def dfsph_fd(make, target, vel0=None, settings=None):
+    w, _, _ = dfsph_run(make, vel0, settings)
+    for _ in range(DFSPH_STEPS):
+        w.step(DFSPH_DT)
+    return loss(w, target)[0]
+
+
+@pytest.fixture(scope="module")
+def dfsph_adjoint(gpu_lib):
+    w, pos, vel = dfsph_run(gpu_lib.FluidWorld)
+    target = np.mean(pos.astype(np.float64), axis=0) + np.array([0.3, 0.0, 0.0])
+    w.tape_begin(2)
+    for _ in range(DFSPH_STEPS):
+        w.step(DFSPH_DT)
+    L, c = loss(w, target)
+    n = w.len()
+    dpos = np.tile(2.0 * (c - target) / n, (n, 1)).astype(np.float32)
+    dp0, dv0, params = w.step_backward(dpos, np.zeros_like(dpos))
+    return pos, vel, target, dp0, dv0, params
+
+
+def test_dfsph_velocity_gradient_matches_the_fp64_reference(oracle_lib, dfsph_adjoint):
+    # the solves' iteration counts are the forward's; at these small steps they do not change
+    pos, vel, target, dp0, dv0, params = dfsph_adjoint
+    make64 = lambda s: oracle_lib.OracleWorld(s, precision=64, residual_sum=1)
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        d = rng.normal(size=vel.shape)
+        d /= np.sqrt(np.mean(d * d))
+        eps = 3e-5
+        vp = (vel + eps * d).astype(np.float32)
+        vm = (vel - eps * d).astype(np.float32)
+        num = (dfsph_fd(make64, target, vp) - dfsph_fd(make64, target, vm)) / (2 * eps)
+        ana = float(np.sum(dv0.astype(np.float64) * (vp.astype(np.float64) - vm.astype(np.float64)) / (2 * eps)))
+        assert abs(ana - num) <= 1e-3 * abs(num), (ana, num)
+
+
+def test_dfsph_parameter_gradients_match_the_fp64_reference(oracle_lib, dfsph_adjoint):
+    # the loss moves by about 1e-10 for a 1e-3 change of the viscosity: below what FP32 positions
+    # resolve, so the differences are taken on the FP64 restatement
+    pos, vel, target, dp0, dv0, params = dfsph_adjoint
+    make64 = lambda s: oracle_lib.OracleWorld(s, precision=64, residual_sum=1)
+    s = dfsph_settings()
+    eps = 1e-4
+    num = (dfsph_fd(make64, target, settings=dfsph_settings(viscosity=s.viscosity + eps)) -
+           dfsph_fd(make64, target, settings=dfsph_settings(viscosity=s.viscosity - eps))) / (2 * eps)
+    assert abs(params["viscosity"] - num) <= 1e-2 * abs(num), (params["viscosity"], num)
+    g = list(s.gravity)
+    eps = 1e-3
+    num = (dfsph_fd(make64, target, settings=dfsph_settings(gravity=(g[0] + eps, g[1], g[2]))) -
+           dfsph_fd(make64, target, settings=dfsph_settings(gravity=(g[0] - eps, g[1], g[2])))) / (2 * eps)
+    assert abs(params["gravity"][0] - num) <= 1e-3 * abs(num), (params["gravity"][0], num)
