@@ -46,6 +46,8 @@ def parse():
                     help="exact: the reference's rounding, bit-identical to the CPU restatement; "
                          "fast: fused arithmetic, within FP32 tolerance")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--adjoint-steps", type=int, default=8,
+                    help="steps of the forward+adjoint measurement (0 skips it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed CPU work in the baseline")
     return ap.parse_args()
@@ -139,14 +141,22 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def cpu_baseline(sc, budget_s: float, threads: int = 0) -> dict:
-    """The CPU restatement (OpenMP over all host cores) on a bounded sample of the workload."""
+def cpu_baseline(sc, budget_s: float, state=None, threads: int = 0) -> dict:
+    """The CPU restatement (OpenMP over all host cores) on a bounded sample of the workload,
+    continuing from `state` = (positions, velocities) in their sorted order when given: added in
+    that order, the particles keep the same (cell, id) order and the same physics."""
     from oracle import py_oracle
 
     py_oracle.build()
     cores = threads or os.cpu_count()
     w = py_oracle.OracleWorld(sc.settings, residual_sum=0, threads=cores)
-    sc.build(w)
+    if state is None:
+        sc.build(w)
+        where = "from rest"
+    else:
+        w.add_box_container((0.0, 0.0, 0.0), sc.tank)
+        w.add_particles(state[0], state[1])
+        where = "from the state the GPU's timed steps ended on"
     w.update_neighbors()
     substeps = 0
     t0 = time.perf_counter()
@@ -159,7 +169,7 @@ def cpu_baseline(sc, budget_s: float, threads: int = 0) -> dict:
             break
     dt = time.perf_counter() - t0
     return {"value": substeps / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{steps} steps ({substeps} substeps) of the {sc.particles}-particle scene from rest, "
+            "sample": f"{steps} steps ({substeps} substeps) of the {sc.particles}-particle scene {where}, "
                       f"{dt:.1f} s on {cores} threads (C++ float restatement, OpenMP)"}
 
 
@@ -322,10 +332,56 @@ def main():
     e2e = {"value": e2e_substeps * world_size / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 24 * n,
            "d2h_bytes_per_step": 24 * n}
 
+    # forward + adjoint (step_backward) on the same world: a taped forward of K steps with a
+    # checkpoint every ~sqrt(K), then the reverse pass, for a loss of the kinetic energy of the
+    # water beyond x = 1 m (gradients with respect to every initial velocity and the settings)
+    adjoint = None
+    if args.adjoint_steps > 0:
+        import math
+
+        import numpy as np
+
+        k = args.adjoint_steps
+        every = max(1, int(round(math.sqrt(k))))
+        barrier()
+        world.tape_begin(every)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        adj_substeps = 0
+        for _ in range(k):
+            adj_substeps += world.step(sc.dt).substeps
+        e1.record(stream)
+        e1.synchronize()
+        fwd_ms = e0.elapsed_time(e1)
+        pos_now = world.positions()
+        vel_now = world.velocities()
+        m = world.particle_mass()
+        dv = np.where((pos_now[:, 0] > 1.0)[:, None], m * vel_now, 0.0).astype(np.float32)
+        torch.cuda.synchronize()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        dp0, dv0, grads = world.step_backward(np.zeros_like(dv), dv)
+        e3.record(stream)
+        e3.synchronize()
+        bwd_ms = e2.elapsed_time(e3)
+        world.tape_end()
+        fwd_ms = max_over_ranks(fwd_ms)
+        bwd_ms = max_over_ranks(bwd_ms)
+        adjoint = {"value": adj_substeps * world_size / ((fwd_ms + bwd_ms) / 1e3), "unit": UNIT,
+                   "steps": k, "substeps": adj_substeps, "checkpoint_every": every,
+                   "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                   "ratio_to_forward": (fwd_ms + bwd_ms) / fwd_ms,
+                   "loss": "kinetic energy of the water beyond x = 1 m after the steps",
+                   "grad_viscosity": grads["viscosity"], "grad_gravity": list(grads["gravity"]),
+                   "grad_uniform_inflow": [float(x) for x in dv0.astype(np.float64).sum(axis=0)]}
+
     base = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        state = (world.positions(), world.velocities())
         world.close()
-        base = cpu_baseline(sc, args.cpu_budget)
+        base = cpu_baseline(sc, args.cpu_budget, state)
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
@@ -334,8 +390,8 @@ def main():
                "config": dict(workload(sc), parallelism=f"replicas x{world_size}",
                               substeps=substeps, solver_iterations_per_substep=iterations / max(substeps, 1),
                               particle_substeps_per_s=value * sc.particles),
-               "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "clocks": clock_info,
-               "gpu_launches": launches}
+               "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "forward_adjoint": adjoint,
+               "clocks": clock_info, "gpu_launches": launches}
         print(json.dumps(out), flush=True)
     if world_size > 1:
         dist.destroy_process_group()
