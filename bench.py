@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--arithmetic", choices=["exact", "fast"], default="exact",
                     help="exact: the reference's rounding, bit-identical to the CPU restatement; "
                          "fast: fused arithmetic, within FP32 tolerance")
+    ap.add_argument("--positions", choices=["absolute", "cell_relative"], default="absolute",
+                    help="cell_relative: offsets from each particle's cell (FAST arithmetic, no adjoint)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--adjoint-steps", type=int, default=8,
                     help="steps of the forward+adjoint measurement (0 skips it)")
@@ -53,12 +55,15 @@ def parse():
     return ap.parse_args()
 
 
-def scene_of(name, arithmetic="exact"):
+def scene_of(name, arithmetic="exact", positions="absolute"):
     from solunar_b200 import scenes
-    from solunar_b200.abi import Arithmetic
+    from solunar_b200.abi import Arithmetic, Positions
 
     sc = getattr(scenes, name)()
     sc.settings.arithmetic = Arithmetic.FAST if arithmetic == "fast" else Arithmetic.EXACT
+    if positions == "cell_relative":
+        sc.settings.positions = Positions.CELL_RELATIVE
+        sc.settings.arithmetic = Arithmetic.FAST
     return sc
 
 
@@ -245,7 +250,7 @@ def main():
 
     from solunar_b200 import fluid
 
-    sc = scene_of(args.scene, args.arithmetic)
+    sc = scene_of(args.scene, args.arithmetic, args.positions)
     sc.settings.device = local_rank
     world = fluid.FluidWorld(sc.settings)
     sc.build(world)
@@ -336,7 +341,7 @@ def main():
     # checkpoint every ~sqrt(K), then the reverse pass, for a loss of the kinetic energy of the
     # water beyond x = 1 m (gradients with respect to every initial velocity and the settings)
     adjoint = None
-    if args.adjoint_steps > 0:
+    if args.adjoint_steps > 0 and args.positions == "absolute":
         import math
 
         import numpy as np

@@ -21,7 +21,8 @@ namespace slf {
 // Neighbour j in slot k: EXACT lists hold {index, g} pairs, FAST lists indexes only.
 __device__ __forceinline__ uint32_t listed(const PairLists& l, bool packed, uint32_t i, uint32_t k) {
     size_t at = (size_t(i >> 5) * l.cap + k) * 32u + (i & 31u);
-    return packed ? l.e[at].x : reinterpret_cast<const uint32_t*>(l.e)[at];
+    // FAST entries carry the cell step in their top six bits (zero steps: absolute positions)
+    return packed ? l.e[at].x : (reinterpret_cast<const uint32_t*>(l.e)[at] & ((1u << 26) - 1u));
 }
 
 __device__ __forceinline__ uint32_t listed_count(const PairLists& l, uint32_t i) {

@@ -80,12 +80,19 @@ __global__ void k_max_compression(Params p, const float* __restrict__ rho, Statu
 
 // ---- spatial hash: counting sort by dense cell index, then id within each cell ------------
 
-__global__ void k_count_cells(Params p, const float4* __restrict__ pos, int3 low, int3 span, uint32_t* count,
-                              uint32_t* lin, uint32_t* slot) {
+// cells (cell-relative positions) non-null: the cell is stored, not computed
+__global__ void k_count_cells(Params p, const float4* __restrict__ pos, const int4* __restrict__ cells, int3 low,
+                              int3 span, uint32_t* count, uint32_t* lin, uint32_t* slot) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
-    float4 a = pos[i];
-    int3 c = cell_of(p, a.x, a.y, a.z);
+    int3 c;
+    if (cells) {
+        int4 c4 = cells[i];
+        c = make_int3(c4.x, c4.y, c4.z);
+    } else {
+        float4 a = pos[i];
+        c = cell_of(p, a.x, a.y, a.z);
+    }
     long long x = (long long)c.x - low.x, y = (long long)c.y - low.y, z = (long long)c.z - low.z;
     // the box was taken over these very positions; stay in bounds regardless
     x = x < 0 ? 0 : (x >= span.x ? span.x - 1 : x);
@@ -109,10 +116,10 @@ __global__ void k_scatter_members(uint32_t n, const uint32_t* __restrict__ lin, 
 __global__ void k_rank_reorder(uint32_t n, const uint32_t* __restrict__ lin, const uint32_t* __restrict__ start,
                                const uint32_t* __restrict__ members, const uint32_t* __restrict__ ids_in,
                                const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
-                               const float* __restrict__ rho_in, const float* __restrict__ kap_in,
+                               const float* __restrict__ rho_in, const int4* __restrict__ cells_in,
                                uint32_t* __restrict__ ids_out, float4* __restrict__ pos_out,
                                float4* __restrict__ vel_out, float* __restrict__ rho_out,
-                               float* __restrict__ kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st,
+                               int4* __restrict__ cells_out, uint32_t skip_begin, uint32_t skip_end, Status* st,
                                uint32_t* __restrict__ dest) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     // a job left undone (the fault injection of the dispatcher tests) places nothing; the count
@@ -132,7 +139,7 @@ __global__ void k_rank_reorder(uint32_t n, const uint32_t* __restrict__ lin, con
     pos_out[f] = pos_in[i];
     vel_out[f] = vel_in[i];
     rho_out[f] = rho_in[i];
-    if (kap_in) kap_out[f] = kap_in[i];
+    if (cells_in) cells_out[f] = cells_in[i];
 }
 
 // ---- exclusive scan of u32 in place, total written at data[m] ------------------------------
@@ -301,8 +308,19 @@ constexpr int kListUnroll = SLF_LIST_UNROLL;
 #define SLF_PAIR_MIN_BLOCKS 1
 #endif
 
-template <class F>
-__device__ __forceinline__ void each_listed(const PairLists& l, uint32_t i, const float4* __restrict__ pts, F&& f) {
+// Where a walk finds its neighbours (the global arrays, read through the L1).
+struct FromGlobal {
+    const float4* __restrict__ p;
+    const float4* __restrict__ v;
+    __device__ __forceinline__ void get(uint32_t j, float4& q) const { q = __ldg(&p[j]); }
+    __device__ __forceinline__ void get(uint32_t j, float4& q, float4& w) const {
+        q = __ldg(&p[j]);
+        w = __ldg(&v[j]);
+    }
+};
+
+template <class Src, class F>
+__device__ __forceinline__ void each_listed_from(const PairLists& l, uint32_t i, const Src& src, F&& f) {
     uint32_t n = l.count[i];
     if (n > l.cap) n = l.cap;
     if (n == 0) return;
@@ -313,7 +331,7 @@ __device__ __forceinline__ void each_listed(const PairLists& l, uint32_t i, cons
     for (uint32_t k = 0; k < n; k += kListUnroll) {
         float4 q[kListUnroll];
 #pragma unroll
-        for (int u = 0; u < kListUnroll; ++u) q[u] = __ldg(&pts[e[u].x]);
+        for (int u = 0; u < kListUnroll; ++u) src.get(e[u].x, q[u]);
         uint2 next[kListUnroll];
 #pragma unroll
         for (int u = 0; u < kListUnroll; ++u) {
@@ -328,10 +346,14 @@ __device__ __forceinline__ void each_listed(const PairLists& l, uint32_t i, cons
     }
 }
 
-// The same walk with a second array gathered alongside (velocities).
 template <class F>
-__device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, const float4* __restrict__ pts,
-                                             const float4* __restrict__ more, F&& f) {
+__device__ __forceinline__ void each_listed(const PairLists& l, uint32_t i, const float4* __restrict__ pts, F&& f) {
+    each_listed_from(l, i, FromGlobal{pts, nullptr}, f);
+}
+
+// The same walk with a second array gathered alongside (velocities).
+template <class Src, class F>
+__device__ __forceinline__ void each_listed2_from(const PairLists& l, uint32_t i, const Src& src, F&& f) {
     uint32_t n = l.count[i];
     if (n > l.cap) n = l.cap;
     if (n == 0) return;
@@ -342,10 +364,7 @@ __device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, con
     for (uint32_t k = 0; k < n; k += kListUnroll) {
         float4 q[kListUnroll], w[kListUnroll];
 #pragma unroll
-        for (int u = 0; u < kListUnroll; ++u) {
-            q[u] = __ldg(&pts[e[u].x]);
-            w[u] = __ldg(&more[e[u].x]);
-        }
+        for (int u = 0; u < kListUnroll; ++u) src.get(e[u].x, q[u], w[u]);
         uint2 next[kListUnroll];
 #pragma unroll
         for (int u = 0; u < kListUnroll; ++u) {
@@ -358,6 +377,12 @@ __device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, con
 #pragma unroll
         for (int u = 0; u < kListUnroll; ++u) e[u] = next[u];
     }
+}
+
+template <class F>
+__device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, const float4* __restrict__ pts,
+                                             const float4* __restrict__ more, F&& f) {
+    each_listed2_from(l, i, FromGlobal{pts, more}, f);
 }
 
 // ---- wall viscosity (step.rs:262-301, no terrains) ---------------------------------------
@@ -495,8 +520,47 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
 
 // ---- DFSPH ----------------------------------------------------------------------------------
 
-// density_rate (dfsph.rs:166-181), then the solve's stiffness and error (dfsph.rs:241-259), and
-// the average error of the particles under load (dfsph.rs:263-268) in a last-block finish.
+// density_rate (dfsph.rs:166-181), then the solve's stiffness and error (dfsph.rs:241-259) of
+// particle i, its neighbours taken from src.
+template <int WHICH, class Src>
+__device__ __forceinline__ void rate_particle(const Params& p, const StepConsts* __restrict__ sc,
+                                              const PairLists& fl, const PairLists& wl, uint32_t i, const Src& src,
+                                              const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                              const float* __restrict__ rho, const float* __restrict__ alpha,
+                                              const float4* __restrict__ walls, float* __restrict__ kappa_w,
+                                              float* __restrict__ rate_out, double& err, uint32_t& loaded) {
+    const float dt = sc->dt;
+    float4 a = pos[i];
+    float4 v = vel[i];
+    float rate = 0.0f;
+    each_listed2_from(fl, i, src, [&](uint32_t, float g, float4 q, float4 w) {
+        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx * g, ry * g, rz * g);
+    });
+    each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
+        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
+    });
+    rate = rate * p.mass;
+    if (rate_out) rate_out[i] = rate;  // recorded for the adjoint
+    float target, error;
+    if (WHICH == 1) {
+        float over = fmaxf(rho[i] + dt * rate - p.rest, 0.0f);
+        target = over / sc->dt_sq;
+        error = over / p.rest;
+    } else {
+        float r = fl.count[i] + wl.count[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
+        target = r / dt;
+        error = dt * r / p.rest;
+    }
+    // the stiffness rides in the spare lane of the position, where push_apart gathers it
+    kappa_w[4 * (size_t)i + 3] = target * alpha[i];
+    err = (double)error;
+    loaded = error > 0.0f ? 1u : 0u;
+}
+
+// One check of the solve, a particle a thread, and the average error of the particles under
+// load (dfsph.rs:263-268) in a last-block finish.
 template <int WHICH>
 __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
@@ -510,53 +574,24 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, 
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double err = 0.0;
     uint32_t loaded = 0;
-    if (i < p.n) {
-        const float dt = sc->dt;
-        float4 a = pos[i];
-        float4 v = vel[i];
-        float rate = 0.0f;
-        each_listed2(fl, i, pos, vel, [&](uint32_t, float g, float4 q, float4 w) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx * g, ry * g, rz * g);
-        });
-        each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
-        });
-        rate = rate * p.mass;
-        if (rate_out) rate_out[i] = rate;  // recorded for the adjoint
-        float target, error;
-        if (WHICH == 1) {
-            float over = fmaxf(rho[i] + dt * rate - p.rest, 0.0f);
-            target = over / sc->dt_sq;
-            error = over / p.rest;
-        } else {
-            float r = fl.count[i] + wl.count[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
-            target = r / dt;
-            error = dt * r / p.rest;
-        }
-        // the stiffness rides in the spare lane of the position, where push_apart gathers it
-        kappa_w[4 * (size_t)i + 3] = target * alpha[i];
-        err = (double)error;
-        loaded = error > 0.0f ? 1u : 0u;
-    }
+    if (i < p.n)
+        rate_particle<WHICH>(p, sc, fl, wl, i, FromGlobal{pos, vel}, pos, vel, rho, alpha, walls, kappa_w, rate_out,
+                             err, loaded);
     residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
 }
 
-// push_apart (dfsph.rs:184-216): the velocity change from each particle's stiffness, which the
-// rate pass left in the w lane of each position.
-__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
-                                                 PairLists wl, const float4* __restrict__ pos,
-                                                 float4* __restrict__ vel, const float4* __restrict__ walls,
-                                                 const Status* st) {
-    if (__ldcg(&st->settled)) return;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
+// push_apart (dfsph.rs:184-216) of particle i: the velocity change from each particle's
+// stiffness, which the rate pass left in the w lane of each position.
+template <class Src>
+__device__ __forceinline__ void push_particle(const Params& p, const StepConsts* __restrict__ sc, const PairLists& fl,
+                                              const PairLists& wl, uint32_t i, const Src& src,
+                                              const float4* __restrict__ pos, float4* __restrict__ vel,
+                                              const float4* __restrict__ walls) {
     const float dt = sc->dt;
     float4 a = pos[i];
     float own = a.w;
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    each_listed(fl, i, pos, [&](uint32_t, float g, float4 q) {
+    each_listed_from(fl, i, src, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float s = p.mass * (own + q.w);
         cx = cx - (rx * g) * s;
@@ -575,6 +610,16 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_push(Params p, 
     v.y = v.y + cy * dt;
     v.z = v.z + cz * dt;
     vel[i] = v;
+}
+
+__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                 PairLists wl, const float4* __restrict__ pos,
+                                                 float4* __restrict__ vel, const float4* __restrict__ walls,
+                                                 const Status* st) {
+    if (__ldcg(&st->settled)) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    push_particle(p, sc, fl, wl, i, FromGlobal{pos, nullptr}, pos, vel, walls);
 }
 
 // viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
@@ -664,10 +709,18 @@ __global__ void k_list_fill(Params p, GridDev g, const float4* __restrict__ pos,
 
 // ---- domain (mod.rs:451-486): keep flags, then a stable compaction -------------------------
 
-__global__ void k_domain_flags(Params p, const float4* __restrict__ pos, float3 low, float3 high, uint32_t* keep) {
+__global__ void k_domain_flags(Params p, const float4* __restrict__ pos, const int4* __restrict__ cells, float3 low,
+                               float3 high, uint32_t* keep) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     float4 a = pos[i];
+    if (cells) {  // cell-relative: the position rebuilt in double
+        int4 c = cells[i];
+        const double r = p.radius;
+        double x = double(c.x) * r + a.x, y = double(c.y) * r + a.y, z = double(c.z) * r + a.z;
+        keep[i] = (x >= low.x && x <= high.x && y >= low.y && y <= high.y && z >= low.z && z <= high.z) ? 1u : 0u;
+        return;
+    }
     float cx = fminf(fmaxf(a.x, low.x), high.x), cy = fminf(fmaxf(a.y, low.y), high.y),
           cz = fminf(fmaxf(a.z, low.z), high.z);
     keep[i] = (cx == a.x && cy == a.y && cz == a.z) ? 1u : 0u;
@@ -676,8 +729,9 @@ __global__ void k_domain_flags(Params p, const float4* __restrict__ pos, float3 
 __global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ dest,
                           const uint32_t* __restrict__ ids_in, const float4* __restrict__ pos_in,
                           const float4* __restrict__ vel_in, const float* __restrict__ rho_in,
-                          uint32_t* __restrict__ ids_out, float4* __restrict__ pos_out,
-                          float4* __restrict__ vel_out, float* __restrict__ rho_out) {
+                          const int4* __restrict__ cells_in, uint32_t* __restrict__ ids_out,
+                          float4* __restrict__ pos_out, float4* __restrict__ vel_out, float* __restrict__ rho_out,
+                          int4* __restrict__ cells_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !keep[i]) return;
     uint32_t f = dest[i];
@@ -685,6 +739,7 @@ __global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const u
     pos_out[f] = pos_in[i];
     vel_out[f] = vel_in[i];
     rho_out[f] = rho_in[i];
+    if (cells_in) cells_out[f] = cells_in[i];
 }
 
 __global__ void k_set_consts(StepConsts c, StepConsts* out) { *out = c; }
@@ -732,9 +787,9 @@ void launch_max_compression(const Params& p, const float* rho, Status* st, cudaS
     if (p.n) k_max_compression<<<blocks_for(p.n), kBlock, 0, s>>>(p, rho, st);
 }
 
-void launch_count_cells(const Params& p, const float4* pos, int3 low, int3 span, uint32_t* count, uint32_t* lin,
-                        uint32_t* slot, cudaStream_t s) {
-    if (p.n) k_count_cells<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, low, span, count, lin, slot);
+void launch_count_cells(const Params& p, const float4* pos, const int4* cells, int3 low, int3 span, uint32_t* count,
+                        uint32_t* lin, uint32_t* slot, cudaStream_t s) {
+    if (p.n) k_count_cells<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, cells, low, span, count, lin, slot);
 }
 
 size_t scan_tiles(uint32_t m) { return (m + kScanTile - 1) / kScanTile; }
@@ -755,12 +810,12 @@ void launch_scatter_members(uint32_t n, const uint32_t* lin, const uint32_t* slo
 
 void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start, const uint32_t* members,
                          const uint32_t* ids_in, const float4* pos_in, const float4* vel_in, const float* rho_in,
-                         const float* kap_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
-                         float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
+                         const int4* cells_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
+                         int4* cells_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
                          cudaStream_t s) {
     if (n)
         k_rank_reorder<<<blocks_for(n), kBlock, 0, s>>>(n, lin, start, members, ids_in, pos_in, vel_in, rho_in,
-                                                        kap_in, ids_out, pos_out, vel_out, rho_out, kap_out,
+                                                        cells_in, ids_out, pos_out, vel_out, rho_out, cells_out,
                                                         skip_begin, skip_end, st, dest);
 }
 
@@ -825,16 +880,18 @@ void launch_list_fill(const Params& p, const GridDev& g, const float4* pos, cons
     if (p.n) k_list_fill<<<blocks_for(p.n), kBlock, 0, s>>>(p, g, pos, pts, start, items);
 }
 
-void launch_domain_flags(const Params& p, const float4* pos, float3 low, float3 high, uint32_t* keep, cudaStream_t s) {
-    if (p.n) k_domain_flags<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, low, high, keep);
+void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, float3 low, float3 high,
+                         uint32_t* keep, cudaStream_t s) {
+    if (p.n) k_domain_flags<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, cells, low, high, keep);
 }
 
 void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, const uint32_t* ids_in,
-                    const float4* pos_in, const float4* vel_in, const float* rho_in, uint32_t* ids_out,
-                    float4* pos_out, float4* vel_out, float* rho_out, cudaStream_t s) {
+                    const float4* pos_in, const float4* vel_in, const float* rho_in, const int4* cells_in,
+                    uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out, int4* cells_out,
+                    cudaStream_t s) {
     if (n)
-        k_compact<<<blocks_for(n), kBlock, 0, s>>>(n, keep, dest, ids_in, pos_in, vel_in, rho_in, ids_out, pos_out,
-                                                   vel_out, rho_out);
+        k_compact<<<blocks_for(n), kBlock, 0, s>>>(n, keep, dest, ids_in, pos_in, vel_in, rho_in, cells_in, ids_out,
+                                                   pos_out, vel_out, rho_out, cells_out);
 }
 
 void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s) {

@@ -8,6 +8,12 @@
 // neighbour lists hold indexes only (4 bytes an entry): each pass recomputes the factor from the
 // positions, which do not move within a substep.  Cell keys and the neighbour test stay exact
 // (fluid_device.cuh), so cell order and neighbour sets still match the reference bit for bit.
+//
+// Cell-relative positions (SLF_POSITIONS_CELL_RELATIVE, template flag REL): a particle's position
+// is an f32 offset in [0, r) from the corner of its cell, its cell an integer triple beside it, and
+// walls are stored the same way.  A pair's offset x_i - x_j = (o_i - o_j) - (c_j - c_i) r is then
+// formed from small numbers; the cell step c_j - c_i (each -1, 0 or 1) rides in the top six bits
+// of the list entry, so no pass gathers cells.
 #include <cfloat>
 #include <climits>
 
@@ -16,6 +22,23 @@
 #include "reduce.cuh"
 
 namespace slf {
+
+// List entries: the neighbour's index in the low 26 bits, the cell step to it (dx, dy, dz, each
+// stored + 1) in the top 6.
+constexpr uint32_t kIndexMask = (1u << 26) - 1u;
+__device__ __forceinline__ uint32_t encode_entry(uint32_t j, int dx, int dy, int dz) {
+    return j | (uint32_t((dx + 1) | ((dy + 1) << 2) | ((dz + 1) << 4)) << 26);
+}
+
+// x_i - x_j from particle i's stored position a and neighbour q's, given the entry e
+template <bool REL>
+__device__ __forceinline__ float3 pair_offset(const Params& p, float4 a, float4 q, uint32_t e) {
+    if (!REL) return make_float3(a.x - q.x, a.y - q.y, a.z - q.z);
+    float dx = float(int((e >> 26) & 3u) - 1), dy = float(int((e >> 28) & 3u) - 1),
+          dz = float(int((e >> 30) & 3u) - 1);
+    return make_float3(fmaf(-dx, p.radius, a.x - q.x), fmaf(-dy, p.radius, a.y - q.y),
+                       fmaf(-dz, p.radius, a.z - q.z));
+}
 
 // Index-only lists in the warp-tiled layout of PairLists, 4 bytes an entry.
 struct IndexLists {
@@ -48,54 +71,101 @@ __device__ __forceinline__ float fast_value(const Params& p, float l2) {
 
 __device__ __forceinline__ float fl2(float x, float y, float z) { return fmaf(x, x, fmaf(y, y, z * z)); }
 
-// f(j, q) for each listed neighbour, four entries and their gathers ahead.
-template <class F>
-__device__ __forceinline__ void each_index(const IndexLists& l, uint32_t i, const float4* __restrict__ pts, F&& f) {
+// Where a walk finds its neighbours (the global arrays, read through the L1).
+struct FromGlobalF {
+    const float4* __restrict__ p;
+    const float4* __restrict__ v;
+    __device__ __forceinline__ void get(uint32_t e, float4& q) const { q = __ldg(&p[e & kIndexMask]); }
+    __device__ __forceinline__ void get(uint32_t e, float4& q, float4& w) const {
+        q = __ldg(&p[e & kIndexMask]);
+        w = __ldg(&v[e & kIndexMask]);
+    }
+};
+
+// f(entry, q) for each listed neighbour, q its stored position; four entries and their
+// gathers ahead
+template <class Src, class F>
+__device__ __forceinline__ void each_index_from(const IndexLists& l, uint32_t i, const Src& src, F&& f) {
     uint32_t n = l.count[i];
     if (n > l.cap) n = l.cap;
     if (n == 0) return;
     const uint32_t* __restrict__ base = l.idx + l.at(i, 0);
     for (uint32_t k = 0; k < n; k += 4) {
-        uint32_t j[4];
+        uint32_t e[4];
         float4 q[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) j[u] = __ldg(base + size_t(k + u < n ? k + u : n - 1) * 32u);
+        for (int u = 0; u < 4; ++u) e[u] = __ldg(base + size_t(k + u < n ? k + u : n - 1) * 32u);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) q[u] = __ldg(&pts[j[u]]);
+        for (int u = 0; u < 4; ++u) src.get(e[u], q[u]);
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            if (k + u < n) f(j[u], q[u]);
+            if (k + u < n) f(e[u], q[u]);
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void each_index(const IndexLists& l, uint32_t i, const float4* __restrict__ pts, F&& f) {
+    each_index_from(l, i, FromGlobalF{pts, nullptr}, f);
+}
+
+template <class Src, class F>
+__device__ __forceinline__ void each_index2_from(const IndexLists& l, uint32_t i, const Src& src, F&& f) {
+    uint32_t n = l.count[i];
+    if (n > l.cap) n = l.cap;
+    if (n == 0) return;
+    const uint32_t* __restrict__ base = l.idx + l.at(i, 0);
+    for (uint32_t k = 0; k < n; k += 4) {
+        uint32_t e[4];
+        float4 q[4], w[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) e[u] = __ldg(base + size_t(k + u < n ? k + u : n - 1) * 32u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) src.get(e[u], q[u], w[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u < n) f(e[u], q[u], w[u]);
     }
 }
 
 template <class F>
 __device__ __forceinline__ void each_index2(const IndexLists& l, uint32_t i, const float4* __restrict__ pts,
                                             const float4* __restrict__ more, F&& f) {
-    uint32_t n = l.count[i];
-    if (n > l.cap) n = l.cap;
-    if (n == 0) return;
-    const uint32_t* __restrict__ base = l.idx + l.at(i, 0);
-    for (uint32_t k = 0; k < n; k += 4) {
-        uint32_t j[4];
-        float4 q[4], w[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) j[u] = __ldg(base + size_t(k + u < n ? k + u : n - 1) * 32u);
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            q[u] = __ldg(&pts[j[u]]);
-            w[u] = __ldg(&more[j[u]]);
+    each_index2_from(l, i, FromGlobalF{pts, more}, f);
+}
+
+// The candidates of each_near (fluid_device.cuh) in cell-relative form: the 27 cells around
+// `cell` in the same order, a candidate kept when |x_j - x_i|^2 < reach, x_j - x_i formed from
+// the offsets and the cell step.  f(j, q, dx, dy, dz, rx, ry, rz) with r = x_i - x_j.
+template <class F>
+__device__ __forceinline__ void each_near_rel(const Params& p, const GridDev& g, const float4* __restrict__ pts,
+                                              int3 cell, float4 a, F&& f) {
+    if (g.mode == 0) return;
+#pragma unroll 1
+    for (int dz = -1; dz <= 1; ++dz) {
+#pragma unroll 1
+        for (int dy = -1; dy <= 1; ++dy) {
+#pragma unroll 1
+            for (int dx = -1; dx <= 1; ++dx) {
+                uint32_t b, e;
+                if (!g.range((long long)cell.x + dx, (long long)cell.y + dy, (long long)cell.z + dz, b, e)) continue;
+                float sx = float(dx) * p.radius, sy = float(dy) * p.radius, sz = float(dz) * p.radius;
+#pragma unroll 1
+                for (uint32_t j = b; j < e; ++j) {
+                    float4 q = __ldg(&pts[j]);
+                    float rx = (a.x - q.x) - sx, ry = (a.y - q.y) - sy, rz = (a.z - q.z) - sz;
+                    if (dot3(rx, ry, rz, rx, ry, rz) < p.reach) f(j, q, dx, dy, dz, rx, ry, rz);
+                }
+            }
         }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (k + u < n) f(j[u], q[u], w[u]);
     }
 }
 
 // ---- densities and lists (mod.rs:621-675; step.rs:147-172; dfsph.rs:108-163) ---------------
 
-template <int SOLVER>
+template <int SOLVER, bool REL>
 __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, GridDev wg,
                                                          const float4* __restrict__ pos,
+                                                         const int4* __restrict__ cells,
                                                          const float4* __restrict__ walls, PairLists fpl,
                                                          PairLists wpl, float* __restrict__ rho,
                                                          float* __restrict__ press, float* __restrict__ scaled,
@@ -106,15 +176,20 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
     uint32_t compressed = 0, longest = 0;
     if (valid) {
         float4 a = pos[i];
-        int3 cell = cell_of(p, a.x, a.y, a.z);
+        int3 cell;
+        if (REL) {
+            int4 c4 = cells[i];
+            cell = make_int3(c4.x, c4.y, c4.z);
+        } else {
+            cell = cell_of(p, a.x, a.y, a.z);
+        }
         float sum = 0.0f, wsum = 0.0f;
         float sx = 0.0f, sy = 0.0f, sz = 0.0f, squares = 0.0f;
         uint32_t nf = 0, nw = 0;
-        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        auto fluid = [&](uint32_t j, int dx, int dy, int dz, float rx, float ry, float rz) {
             float l2 = fl2(rx, ry, rz);
             sum += fast_value(p, l2);
-            if (nf < fl.cap) fl.idx[fl.at(i, nf)] = j;
+            if (nf < fl.cap) fl.idx[fl.at(i, nf)] = encode_entry(j, dx, dy, dz);
             ++nf;
             if (SOLVER == 1) {
                 float g = fast_factor(p, l2) * p.mass;
@@ -124,12 +199,11 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
                 sz += pz;
                 squares = fmaf(px, px, fmaf(py, py, fmaf(pz, pz, squares)));
             }
-        });
-        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+        };
+        auto wall = [&](uint32_t j, int dx, int dy, int dz, float rx, float ry, float rz) {
             float l2 = fl2(rx, ry, rz);
             wsum += fast_value(p, l2);
-            if (nw < wl.cap) wl.idx[wl.at(i, nw)] = j;
+            if (nw < wl.cap) wl.idx[wl.at(i, nw)] = encode_entry(j, dx, dy, dz);
             ++nw;
             if (SOLVER == 1) {
                 float g = fast_factor(p, l2) * p.mass;
@@ -137,7 +211,18 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
                 sy = fmaf(ry, g, sy);
                 sz = fmaf(rz, g, sz);
             }
-        });
+        };
+        if (REL) {
+            each_near_rel(p, fg, pos, cell, a, [&](uint32_t j, float4, int dx, int dy, int dz, float rx, float ry,
+                                                   float rz) { fluid(j, dx, dy, dz, rx, ry, rz); });
+            each_near_rel(p, wg, walls, cell, a, [&](uint32_t j, float4, int dx, int dy, int dz, float rx, float ry,
+                                                     float rz) { wall(j, dx, dy, dz, rx, ry, rz); });
+        } else {
+            each_near(p, fg, pos, cell, a.x, a.y, a.z,
+                      [&](uint32_t j, float4 q) { fluid(j, 0, 0, 0, a.x - q.x, a.y - q.y, a.z - q.z); });
+            each_near(p, wg, walls, cell, a.x, a.y, a.z,
+                      [&](uint32_t j, float4 q) { wall(j, 0, 0, 0, a.x - q.x, a.y - q.y, a.z - q.z); });
+        }
         fl.count[i] = nf;
         wl.count[i] = nw;
         longest = nf > nw ? nf : nw;
@@ -166,17 +251,18 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
 
 // ---- wall viscosity (step.rs:262-301) --------------------------------------------------------
 
+template <bool REL>
 __device__ __forceinline__ float3 wall_viscous_fast(const Params& p, float wall_visc, const IndexLists& wl,
                                                     const float4* __restrict__ walls, uint32_t i, float4 a,
                                                     float4 v, float density) {
     if (wl.count[i] == 0) return make_float3(0.0f, 0.0f, 0.0f);
     float awx = 0.0f, awy = 0.0f, awz = 0.0f;
-    each_index(wl, i, walls, [&](uint32_t, float4 q) {
-        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float g = fast_factor(p, fl2(rx, ry, rz));
-        awx = fmaf(-rx, g, awx);
-        awy = fmaf(-ry, g, awy);
-        awz = fmaf(-rz, g, awz);
+    each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+        float3 r = pair_offset<REL>(p, a, q, e);
+        float g = fast_factor(p, fl2(r.x, r.y, r.z));
+        awx = fmaf(-r.x, g, awx);
+        awy = fmaf(-r.y, g, awy);
+        awz = fmaf(-r.z, g, awz);
     });
     float l2 = fl2(awx, awy, awz);
     float nx = 0.0f, ny = 0.0f, nz = 0.0f;
@@ -190,46 +276,108 @@ __device__ __forceinline__ float3 wall_viscous_fast(const Params& p, float wall_
     float ix = nx * k, iy = ny * k, iz = nz * k;
     float px = 0.0f, py = 0.0f, pz = 0.0f;
     float c = -wall_visc * p.mass / density;
-    each_index(wl, i, walls, [&](uint32_t, float4 q) {
-        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float toward = fmaf(ix, rx, fmaf(iy, ry, iz * rz));
+    each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+        float3 r = pair_offset<REL>(p, a, q, e);
+        float toward = fmaf(ix, r.x, fmaf(iy, r.y, iz * r.z));
         if (toward < 0.0f) {
-            float l2r = fl2(rx, ry, rz);
+            float l2r = fl2(r.x, r.y, r.z);
             float s = c * toward / (l2r + p.soften) * fast_factor(p, l2r);
-            px = fmaf(-rx, s, px);
-            py = fmaf(-ry, s, py);
-            pz = fmaf(-rz, s, pz);
+            px = fmaf(-r.x, s, px);
+            py = fmaf(-r.y, s, py);
+            pz = fmaf(-r.z, s, pz);
         }
     });
     return make_float3(px, py, pz);
 }
 
-// ---- WCSPH forces, velocity update, advance (step.rs:159-223, 305-339) ---------------------
+// ---- advance (step.rs:305-339) ----------------------------------------------------------------
+
+__device__ __forceinline__ void clamp_into(const Params& p, float& nx, float& ny, float& nz, float4& v,
+                                           uint32_t& held) {
+    if (!p.has_bounds) return;
+    float ix = fminf(fmaxf(nx, p.low_in.x), p.high_in.x);
+    float iy = fminf(fmaxf(ny, p.low_in.y), p.high_in.y);
+    float iz = fminf(fmaxf(nz, p.low_in.z), p.high_in.z);
+    if (ix != nx || iy != ny || iz != nz) {
+        float cx = fminf(fmaxf(nx, p.low.x), p.high.x);
+        float cy = fminf(fmaxf(ny, p.low.y), p.high.y);
+        float cz = fminf(fmaxf(nz, p.low.z), p.high.z);
+        if (cx != nx || cy != ny || cz != nz) held += 1;
+        if (ix != nx) v.x = 0.0f;
+        if (iy != ny) v.y = 0.0f;
+        if (iz != nz) v.z = 0.0f;
+        nx = ix;
+        ny = iy;
+        nz = iz;
+    }
+}
 
 __device__ __forceinline__ void advance_fast(const Params& p, float dt, float4& a, float4& v, uint32_t& held,
                                              uint32_t& bad) {
     float nx = fmaf(v.x, dt, a.x), ny = fmaf(v.y, dt, a.y), nz = fmaf(v.z, dt, a.z);
-    if (p.has_bounds) {
-        float ix = fminf(fmaxf(nx, p.low_in.x), p.high_in.x);
-        float iy = fminf(fmaxf(ny, p.low_in.y), p.high_in.y);
-        float iz = fminf(fmaxf(nz, p.low_in.z), p.high_in.z);
-        if (ix != nx || iy != ny || iz != nz) {
-            float cx = fminf(fmaxf(nx, p.low.x), p.high.x);
-            float cy = fminf(fmaxf(ny, p.low.y), p.high.y);
-            float cz = fminf(fmaxf(nz, p.low.z), p.high.z);
-            if (cx != nx || cy != ny || cz != nz) held += 1;
-            if (ix != nx) v.x = 0.0f;
-            if (iy != ny) v.y = 0.0f;
-            if (iz != nz) v.z = 0.0f;
-            nx = ix;
-            ny = iy;
-            nz = iz;
-        }
-    }
+    clamp_into(p, nx, ny, nz, v, held);
     if (!(isfinite(nx) && isfinite(ny) && isfinite(nz) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) bad = 1;
     a.x = nx;
     a.y = ny;
     a.z = nz;
+}
+
+// One axis of a cell-relative position moved by d: the offset stays in [0, r), the cell follows.
+__device__ __forceinline__ void renormalise(float r, float& o, int& c) {
+    if (o >= 0.0f && o < r) return;
+    float k = floorf(o / r);
+    c += int(k);
+    o = fmaf(-k, r, o);
+    if (o < 0.0f) {  // rounding at the edge
+        o += r;
+        c -= 1;
+    }
+    if (o >= r) {
+        o -= r;
+        c += 1;
+    }
+}
+
+// The advance in cell-relative form: offsets move by v dt; the container clamp compares the
+// position rebuilt in double with the bounds (f32 absolute coordinates lose the offsets' bits).
+__device__ __forceinline__ void advance_rel(const Params& p, float dt, float4& a, int4& c, float4& v, uint32_t& held,
+                                            uint32_t& bad) {
+    float ox = fmaf(v.x, dt, a.x), oy = fmaf(v.y, dt, a.y), oz = fmaf(v.z, dt, a.z);
+    if (p.has_bounds) {
+        const double r = p.radius;
+        double x = double(c.x) * r + ox, y = double(c.y) * r + oy, z = double(c.z) * r + oz;
+        double ix = fmin(fmax(x, (double)p.low_in.x), (double)p.high_in.x);
+        double iy = fmin(fmax(y, (double)p.low_in.y), (double)p.high_in.y);
+        double iz = fmin(fmax(z, (double)p.low_in.z), (double)p.high_in.z);
+        if (ix != x || iy != y || iz != z) {
+            double cx = fmin(fmax(x, (double)p.low.x), (double)p.high.x);
+            double cy = fmin(fmax(y, (double)p.low.y), (double)p.high.y);
+            double cz = fmin(fmax(z, (double)p.low.z), (double)p.high.z);
+            if (cx != x || cy != y || cz != z) held += 1;
+            if (ix != x) {
+                v.x = 0.0f;
+                ox = float(ix - double(c.x) * r);
+            }
+            if (iy != y) {
+                v.y = 0.0f;
+                oy = float(iy - double(c.y) * r);
+            }
+            if (iz != z) {
+                v.z = 0.0f;
+                oz = float(iz - double(c.z) * r);
+            }
+        }
+    }
+    if (!(isfinite(ox) && isfinite(oy) && isfinite(oz) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) {
+        bad = 1;
+    } else {
+        renormalise(p.radius, ox, c.x);
+        renormalise(p.radius, oy, c.y);
+        renormalise(p.radius, oz, c.z);
+    }
+    a.x = ox;
+    a.y = oy;
+    a.z = oz;
 }
 
 __device__ __forceinline__ void fold_stats(Status* st, bool valid, int3 c, float speed, uint32_t held, uint32_t bad) {
@@ -260,15 +408,26 @@ __device__ __forceinline__ void fold_stats(Status* st, bool valid, int3 c, float
     }
 }
 
+__device__ __forceinline__ void record_clamp(float4* vel_pre, uint32_t i, float4 pre, float4 v) {
+    if (!vel_pre) return;
+    uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
+    pre.w = __uint_as_float(flags);
+    vel_pre[i] = pre;
+}
+
+// ---- WCSPH forces, velocity update, advance (step.rs:159-223, 305-339) ---------------------
+
+template <bool REL>
 __global__ void __launch_bounds__(kBlock) k_wcsph_force_fast(Params p, const StepConsts* __restrict__ sc,
                                                              PairLists fpl, PairLists wpl,
                                                              const float4* __restrict__ pos,
+                                                             const int4* __restrict__ cells,
                                                              const float4* __restrict__ vel,
                                                              const float* __restrict__ rho,
                                                              const float* __restrict__ press,
                                                              const float* __restrict__ scaled,
                                                              const float4* __restrict__ walls,
-                                                             float4* __restrict__ pos_out,
+                                                             float4* __restrict__ pos_out, int4* __restrict__ cells_out,
                                                              float4* __restrict__ vel_out, Status* st,
                                                              float4* __restrict__ vel_pre) {
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
@@ -285,54 +444,97 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_fast(Params p, const Ste
         float density = rho[i];
         float own = scaled[i];
         float px = 0.0f, py = 0.0f, pz = 0.0f;
-        each_index2(fl, i, pos, vel, [&](uint32_t j, float4 q, float4 w) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            float squared = fl2(rx, ry, rz);
+        each_index2(fl, i, pos, vel, [&](uint32_t e, float4 q, float4 w) {
+            float3 r = pair_offset<REL>(p, a, q, e);
+            float squared = fl2(r.x, r.y, r.z);
             if (squared <= 0.0f) return;
             float g = fast_factor(p, squared);
-            float toward = fminf(fmaf(v.x - w.x, rx, fmaf(v.y - w.y, ry, (v.z - w.z) * rz)), 0.0f);
-            float damp = visc2 * toward / ((squared + p.soften) * (density + __ldg(&rho[j])));
-            float s = g * p.mass * (own + __ldg(&scaled[j]) + damp);
-            px = fmaf(-rx, s, px);
-            py = fmaf(-ry, s, py);
-            pz = fmaf(-rz, s, pz);
+            float toward = fminf(fmaf(v.x - w.x, r.x, fmaf(v.y - w.y, r.y, (v.z - w.z) * r.z)), 0.0f);
+            float damp = visc2 * toward / ((squared + p.soften) * (density + __ldg(&rho[e & kIndexMask])));
+            float s = g * p.mass * (own + __ldg(&scaled[e & kIndexMask]) + damp);
+            px = fmaf(-r.x, s, px);
+            py = fmaf(-r.y, s, py);
+            pz = fmaf(-r.z, s, pz);
         });
         float mirrored = p.mass * (own + press[i] * p.inv_rest_sq);
-        each_index(wl, i, walls, [&](uint32_t, float4 q) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            float s = fast_factor(p, fl2(rx, ry, rz)) * mirrored;
-            px = fmaf(-rx, s, px);
-            py = fmaf(-ry, s, py);
-            pz = fmaf(-rz, s, pz);
+        each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+            float3 r = pair_offset<REL>(p, a, q, e);
+            float s = fast_factor(p, fl2(r.x, r.y, r.z)) * mirrored;
+            px = fmaf(-r.x, s, px);
+            py = fmaf(-r.y, s, py);
+            pz = fmaf(-r.z, s, pz);
         });
-        float3 wv = wall_viscous_fast(p, sc->wall_viscosity, wl, walls, i, a, v, density);
+        float3 wv = wall_viscous_fast<REL>(p, sc->wall_viscosity, wl, walls, i, a, v, density);
         v.x = fmaf(px + wv.x + p.gravity.x, dt, v.x);
         v.y = fmaf(py + wv.y + p.gravity.y, dt, v.y);
         v.z = fmaf(pz + wv.z + p.gravity.z, dt, v.z);
         float4 pre = v;
-        advance_fast(p, dt, a, v, held, bad);
-        if (vel_pre) {
-            uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
-            pre.w = __uint_as_float(flags);
-            vel_pre[i] = pre;
+        if (REL) {
+            int4 c = cells[i];
+            advance_rel(p, dt, a, c, v, held, bad);
+            cells_out[i] = c;
+            nc = make_int3(c.x, c.y, c.z);
+        } else {
+            advance_fast(p, dt, a, v, held, bad);
+            nc = cell_of(p, a.x, a.y, a.z);
         }
+        record_clamp(vel_pre, i, pre, v);
         pos_out[i] = a;
         vel_out[i] = v;
-        nc = cell_of(p, a.x, a.y, a.z);
         speed = sqrtf(dot3(v.x, v.y, v.z, v.x, v.y, v.z));
         if (!(speed == speed)) speed = 0.0f;
     }
     fold_stats(st, valid, nc, speed, held, bad);
 }
 
-// ---- DFSPH: density rate and stiffness, push_apart, viscosity --------------------------------
+// ---- DFSPH: density rate and stiffness, push_apart, viscosity, advance ------------------------
 
-template <int WHICH>
+template <int WHICH, bool REL, class Src>
+__device__ __forceinline__ void rate_particle_fast(const Params& p, const StepConsts* __restrict__ sc,
+                                                   const IndexLists& fl, const IndexLists& wl, uint32_t i,
+                                                   const Src& src, const float4* __restrict__ pos,
+                                                   const float4* __restrict__ vel, const float* __restrict__ rho,
+                                                   const float* __restrict__ alpha,
+                                                   const float4* __restrict__ walls, float* __restrict__ kappa,
+                                                   float* __restrict__ rate_out, double& err, uint32_t& loaded) {
+    const float dt = sc->dt;
+    float4 a = pos[i];
+    float4 v = vel[i];
+    float rate = 0.0f;
+    each_index2_from(fl, i, src, [&](uint32_t e, float4 q, float4 w) {
+        float3 r = pair_offset<REL>(p, a, q, e);
+        float g = fast_factor(p, fl2(r.x, r.y, r.z));
+        rate = fmaf(g, fmaf(v.x - w.x, r.x, fmaf(v.y - w.y, r.y, (v.z - w.z) * r.z)), rate);
+    });
+    each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+        float3 r = pair_offset<REL>(p, a, q, e);
+        float g = fast_factor(p, fl2(r.x, r.y, r.z));
+        rate = fmaf(g, fmaf(v.x, r.x, fmaf(v.y, r.y, v.z * r.z)), rate);
+    });
+    rate = rate * p.mass;
+    if (rate_out) rate_out[i] = rate;
+    float target, error;
+    if (WHICH == 1) {
+        float over = fmaxf(fmaf(dt, rate, rho[i]) - p.rest, 0.0f);
+        target = over / sc->dt_sq;
+        error = over * p.inv_rest;
+    } else {
+        float r = fl.count[i] + wl.count[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
+        target = r / dt;
+        error = dt * r * p.inv_rest;
+    }
+    // the stiffness goes into the position's spare lane
+    kappa[4 * (size_t)i + 3] = target * alpha[i];
+    err = (double)error;
+    loaded = error > 0.0f ? 1u : 0u;
+}
+
+template <int WHICH, bool REL>
 __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts* __restrict__ sc, PairLists fpl,
                                                       PairLists wpl, const float4* __restrict__ pos,
                                                       const float4* __restrict__ vel, const float* __restrict__ rho,
                                                       const float* __restrict__ alpha,
-                                                      const float4* __restrict__ walls, float* __restrict__ kappa_w,
+                                                      const float4* __restrict__ walls, float* __restrict__ kappa,
                                                       DD* __restrict__ partial,
                                                       uint32_t* __restrict__ partial_loaded, Status* st,
                                                       float* __restrict__ rate_out) {
@@ -341,65 +543,34 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double err = 0.0;
     uint32_t loaded = 0;
-    if (i < p.n) {
-        const float dt = sc->dt;
-        float4 a = pos[i];
-        float4 v = vel[i];
-        float rate = 0.0f;
-        each_index2(fl, i, pos, vel, [&](uint32_t, float4 q, float4 w) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            float g = fast_factor(p, fl2(rx, ry, rz));
-            rate = fmaf(g, fmaf(v.x - w.x, rx, fmaf(v.y - w.y, ry, (v.z - w.z) * rz)), rate);
-        });
-        each_index(wl, i, walls, [&](uint32_t, float4 q) {
-            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-            float g = fast_factor(p, fl2(rx, ry, rz));
-            rate = fmaf(g, fmaf(v.x, rx, fmaf(v.y, ry, v.z * rz)), rate);
-        });
-        rate = rate * p.mass;
-        if (rate_out) rate_out[i] = rate;
-        float target, error;
-        if (WHICH == 1) {
-            float over = fmaxf(fmaf(dt, rate, rho[i]) - p.rest, 0.0f);
-            target = over / sc->dt_sq;
-            error = over * p.inv_rest;
-        } else {
-            float r = fl.count[i] + wl.count[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
-            target = r / dt;
-            error = dt * r * p.inv_rest;
-        }
-        kappa_w[4 * (size_t)i + 3] = target * alpha[i];
-        err = (double)error;
-        loaded = error > 0.0f ? 1u : 0u;
-    }
+    if (i < p.n)
+        rate_particle_fast<WHICH, REL>(p, sc, fl, wl, i, FromGlobalF{pos, vel}, pos, vel, rho, alpha, walls, kappa,
+                                       rate_out, err, loaded);
     residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
 }
 
-__global__ void __launch_bounds__(kBlock) k_push_fast(Params p, const StepConsts* __restrict__ sc, PairLists fpl,
-                                                      PairLists wpl, const float4* __restrict__ pos,
-                                                      float4* __restrict__ vel, const float4* __restrict__ walls,
-                                                      const Status* st) {
-    if (__ldcg(&st->settled)) return;
-    IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
+template <bool REL, class Src>
+__device__ __forceinline__ void push_particle_fast(const Params& p, const StepConsts* __restrict__ sc,
+                                                   const IndexLists& fl, const IndexLists& wl, uint32_t i,
+                                                   const Src& src, const float4* __restrict__ pos,
+                                                   float4* __restrict__ vel, const float4* __restrict__ walls) {
     const float mdt = p.mass * sc->dt;
     float4 a = pos[i];
     float own = a.w;
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    each_index(fl, i, pos, [&](uint32_t, float4 q) {
-        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float s = fast_factor(p, fl2(rx, ry, rz)) * (own + q.w);
-        cx = fmaf(-rx, s, cx);
-        cy = fmaf(-ry, s, cy);
-        cz = fmaf(-rz, s, cz);
+    each_index_from(fl, i, src, [&](uint32_t e, float4 q) {
+        float3 r = pair_offset<REL>(p, a, q, e);
+        float s = fast_factor(p, fl2(r.x, r.y, r.z)) * (own + q.w);
+        cx = fmaf(-r.x, s, cx);
+        cy = fmaf(-r.y, s, cy);
+        cz = fmaf(-r.z, s, cz);
     });
-    each_index(wl, i, walls, [&](uint32_t, float4 q) {
-        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float s = fast_factor(p, fl2(rx, ry, rz)) * own;
-        cx = fmaf(-rx, s, cx);
-        cy = fmaf(-ry, s, cy);
-        cz = fmaf(-rz, s, cz);
+    each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+        float3 r = pair_offset<REL>(p, a, q, e);
+        float s = fast_factor(p, fl2(r.x, r.y, r.z)) * own;
+        cx = fmaf(-r.x, s, cx);
+        cy = fmaf(-r.y, s, cy);
+        cz = fmaf(-r.z, s, cz);
     });
     float4 v = vel[i];
     v.x = fmaf(cx, mdt, v.x);
@@ -408,6 +579,19 @@ __global__ void __launch_bounds__(kBlock) k_push_fast(Params p, const StepConsts
     vel[i] = v;
 }
 
+template <bool REL>
+__global__ void __launch_bounds__(kBlock) k_push_fast(Params p, const StepConsts* __restrict__ sc, PairLists fpl,
+                                                      PairLists wpl, const float4* __restrict__ pos,
+                                                      float4* __restrict__ vel, const float4* __restrict__ walls,
+                                                      const Status* st) {
+    if (__ldcg(&st->settled)) return;
+    IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    push_particle_fast<REL>(p, sc, fl, wl, i, FromGlobalF{pos, nullptr}, pos, vel, walls);
+}
+
+template <bool REL>
 __global__ void __launch_bounds__(kBlock) k_viscous_fast(Params p, const StepConsts* __restrict__ sc,
                                                          PairLists fpl, PairLists wpl,
                                                          const float4* __restrict__ pos,
@@ -424,23 +608,126 @@ __global__ void __launch_bounds__(kBlock) k_viscous_fast(Params p, const StepCon
     float4 v = vel[i];
     float density = rho[i];
     float px = 0.0f, py = 0.0f, pz = 0.0f;
-    each_index2(fl, i, pos, vel, [&](uint32_t j, float4 q, float4 w) {
+    each_index2(fl, i, pos, vel, [&](uint32_t e, float4 q, float4 w) {
+        uint32_t j = e & kIndexMask;
         if (j == i) return;
-        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        float toward = fmaf(v.x - w.x, rx, fmaf(v.y - w.y, ry, (v.z - w.z) * rz));
+        float3 r = pair_offset<REL>(p, a, q, e);
+        float toward = fmaf(v.x - w.x, r.x, fmaf(v.y - w.y, r.y, (v.z - w.z) * r.z));
         if (toward < 0.0f) {
-            float l2 = fl2(rx, ry, rz);
+            float l2 = fl2(r.x, r.y, r.z);
             float s = visc2 * toward / ((l2 + p.soften) * (density + __ldg(&rho[j]))) * fast_factor(p, l2);
-            px = fmaf(-rx, s, px);
-            py = fmaf(-ry, s, py);
-            pz = fmaf(-rz, s, pz);
+            px = fmaf(-r.x, s, px);
+            py = fmaf(-r.y, s, py);
+            pz = fmaf(-r.z, s, pz);
         }
     });
-    float3 wv = wall_viscous_fast(p, sc->wall_viscosity, wl, walls, i, a, v, density);
+    float3 wv = wall_viscous_fast<REL>(p, sc->wall_viscosity, wl, walls, i, a, v, density);
     v.x = fmaf(px + wv.x + p.gravity.x, dt, v.x);
     v.y = fmaf(py + wv.y + p.gravity.y, dt, v.y);
     v.z = fmaf(pz + wv.z + p.gravity.z, dt, v.z);
     vel_out[i] = v;
+}
+
+// DFSPH advance of cell-relative positions (the absolute one is k_advance in kernels.cu)
+__global__ void k_advance_rel(Params p, const StepConsts* __restrict__ sc, const float4* __restrict__ pos_in,
+                              const int4* __restrict__ cells_in, float4* __restrict__ pos_out,
+                              int4* __restrict__ cells_out, float4* __restrict__ vel, Status* st,
+                              float4* __restrict__ vel_pre) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < p.n;
+    int3 nc = make_int3(0, 0, 0);
+    float speed = 0.0f;
+    uint32_t held = 0, bad = 0;
+    if (valid) {
+        float4 a = pos_in[i];
+        int4 c = cells_in[i];
+        float4 v = vel[i];
+        float4 pre = v;
+        advance_rel(p, sc->dt, a, c, v, held, bad);
+        record_clamp(vel_pre, i, pre, v);
+        pos_out[i] = a;
+        cells_out[i] = c;
+        vel[i] = v;
+        nc = make_int3(c.x, c.y, c.z);
+        speed = sqrtf(dot3(v.x, v.y, v.z, v.x, v.y, v.z));
+        if (!(speed == speed)) speed = 0.0f;
+    }
+    fold_stats(st, valid, nc, speed, held, bad);
+}
+
+// ---- cell-relative positions in and out -----------------------------------------------------
+
+// absolute f32 positions -> offset in [0, r) and cell, cell = floor(x / r) as cell_of has it
+__global__ void k_to_relative(Params p, uint32_t n, const float* __restrict__ xyz, const float4* __restrict__ abs4,
+                              float4* __restrict__ pos, int4* __restrict__ cells) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float x, y, z;
+    if (xyz) {
+        x = xyz[3 * i];
+        y = xyz[3 * i + 1];
+        z = xyz[3 * i + 2];
+    } else {
+        float4 q = abs4[i];
+        x = q.x;
+        y = q.y;
+        z = q.z;
+    }
+    int3 c = cell_of(p, x, y, z);
+    const double r = p.radius;
+    float ox = float(double(x) - double(c.x) * r), oy = float(double(y) - double(c.y) * r),
+          oz = float(double(z) - double(c.z) * r);
+    renormalise(p.radius, ox, c.x);
+    renormalise(p.radius, oy, c.y);
+    renormalise(p.radius, oz, c.z);
+    pos[i] = make_float4(ox, oy, oz, 0.0f);
+    cells[i] = make_int4(c.x, c.y, c.z, 0);
+}
+
+// offset and cell -> absolute f32 positions, xyz triples
+__global__ void k_from_relative(Params p, uint32_t n, const float4* __restrict__ pos, const int4* __restrict__ cells,
+                                float* __restrict__ xyz) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 a = pos[i];
+    int4 c = cells[i];
+    const double r = p.radius;
+    xyz[3 * i] = float(double(c.x) * r + a.x);
+    xyz[3 * i + 1] = float(double(c.y) * r + a.y);
+    xyz[3 * i + 2] = float(double(c.z) * r + a.z);
+}
+
+// bounding box of cells and fastest speed of a cell-relative state
+__global__ void k_state_stats_rel(Params p, const int4* __restrict__ cells, const float4* __restrict__ vel,
+                                  Status* st) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < p.n;
+    int3 c = make_int3(0, 0, 0);
+    float speed = 0.0f;
+    if (valid) {
+        int4 c4 = cells[i];
+        c = make_int3(c4.x, c4.y, c4.z);
+        float4 v = vel[i];
+        speed = sqrtf(dot3(v.x, v.y, v.z, v.x, v.y, v.z));
+        if (!(speed == speed)) speed = 0.0f;
+    }
+    fold_stats(st, valid, c, speed, 0u, 0u);
+}
+
+// neighbour lists on demand, cell-relative (k_list_count / k_list_fill in kernels.cu)
+__global__ void k_list_rel(Params p, GridDev g, const float4* __restrict__ pos, const int4* __restrict__ cells,
+                           const float4* __restrict__ pts, const uint32_t* __restrict__ start, uint32_t* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float4 a = pos[i];
+    int4 c4 = cells[i];
+    uint32_t k = start ? start[i] : 0u, c = 0;
+    each_near_rel(p, g, pts, make_int3(c4.x, c4.y, c4.z), a,
+                  [&](uint32_t j, float4, int, int, int, float, float, float) {
+                      if (start) out[k++] = j;
+                      else ++c;
+                  });
+    if (!start) out[i] = c;
 }
 
 // ---- launchers ------------------------------------------------------------------------------
@@ -450,51 +737,105 @@ static inline uint32_t fast_blocks(uint32_t n) {
     return (n + kBlock - 1) / kBlock;
 }
 
-void launch_density_fast(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos,
+void launch_density_fast(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const int4* cells,
                          const float4* walls, const PairLists& fl, const PairLists& wl, float* rho, float* press,
                          float* scaled, float* alpha, Status* st, cudaStream_t s) {
     if (!p.n) return;
-    if (p.solver == 0)
-        k_density_fast<0><<<fast_blocks(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled,
-                                                               alpha, st);
-    else
-        k_density_fast<1><<<fast_blocks(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled,
-                                                               alpha, st);
+    uint32_t nb = fast_blocks(p.n);
+    if (cells) {
+        if (p.solver == 0)
+            k_density_fast<0, true><<<nb, kBlock, 0, s>>>(p, fg, wg, pos, cells, walls, fl, wl, rho, press, scaled,
+                                                           alpha, st);
+        else
+            k_density_fast<1, true><<<nb, kBlock, 0, s>>>(p, fg, wg, pos, cells, walls, fl, wl, rho, press, scaled,
+                                                           alpha, st);
+    } else {
+        if (p.solver == 0)
+            k_density_fast<0, false><<<nb, kBlock, 0, s>>>(p, fg, wg, pos, cells, walls, fl, wl, rho, press, scaled,
+                                                            alpha, st);
+        else
+            k_density_fast<1, false><<<nb, kBlock, 0, s>>>(p, fg, wg, pos, cells, walls, fl, wl, rho, press, scaled,
+                                                            alpha, st);
+    }
 }
 
 void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                             const float4* pos, const float4* vel, const float* rho, const float* press,
-                             const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                             float4* vel_pre, cudaStream_t s) {
-    if (p.n)
-        k_wcsph_force_fast<<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled, walls,
-                                                               pos_out, vel_out, st, vel_pre);
+                             const float4* pos, const int4* cells, const float4* vel, const float* rho,
+                             const float* press, const float* scaled, const float4* walls, float4* pos_out,
+                             int4* cells_out, float4* vel_out, Status* st, float4* vel_pre, cudaStream_t s) {
+    if (!p.n) return;
+    uint32_t nb = fast_blocks(p.n);
+    if (cells)
+        k_wcsph_force_fast<true><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, cells, vel, rho, press, scaled, walls,
+                                                       pos_out, cells_out, vel_out, st, vel_pre);
+    else
+        k_wcsph_force_fast<false><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, cells, vel, rho, press, scaled, walls,
+                                                        pos_out, cells_out, vel_out, st, vel_pre);
 }
 
-void launch_rate_fast(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                      float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                      void* partials, Status* st, float* rate_out, cudaStream_t s) {
+void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc, const PairLists& fl,
+                      const PairLists& wl, float4* pos, const float4* vel, const float* rho, const float* alpha,
+                      const float4* walls, void* partials, Status* st, float* rate_out, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = fast_blocks(p.n);
     DD* part = static_cast<DD*>(partials);
     uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
-    if (which == 0)
-        k_rate_fast<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls,
-                                             reinterpret_cast<float*>(pos), part, loaded, st, rate_out);
+    float* kw = reinterpret_cast<float*>(pos);
+    if (which == 0 && rel)
+        k_rate_fast<0, true><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
+                                                   rate_out);
+    else if (which == 0)
+        k_rate_fast<0, false><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
+                                                    rate_out);
+    else if (rel)
+        k_rate_fast<1, true><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
+                                                   rate_out);
     else
-        k_rate_fast<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls,
-                                             reinterpret_cast<float*>(pos), part, loaded, st, rate_out);
+        k_rate_fast<1, false><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
+                                                    rate_out);
 }
 
-void launch_push_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+void launch_push_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                       const float4* pos, float4* vel, const float4* walls, const Status* st, cudaStream_t s) {
-    if (p.n) k_push_fast<<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st);
+    if (!p.n) return;
+    if (rel) k_push_fast<true><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st);
+    else k_push_fast<false><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st);
 }
 
-void launch_viscous_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+void launch_viscous_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                          const float4* pos, const float4* vel, const float* rho, const float4* walls,
                          float4* vel_out, cudaStream_t s) {
-    if (p.n) k_viscous_fast<<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, walls, vel_out);
+    if (!p.n) return;
+    if (rel)
+        k_viscous_fast<true><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, walls, vel_out);
+    else
+        k_viscous_fast<false><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, walls, vel_out);
+}
+
+void launch_advance_rel(const Params& p, const StepConsts* sc, const float4* pos_in, const int4* cells_in,
+                        float4* pos_out, int4* cells_out, float4* vel, Status* st, float4* vel_pre, cudaStream_t s) {
+    if (p.n)
+        k_advance_rel<<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, pos_in, cells_in, pos_out, cells_out, vel, st,
+                                                          vel_pre);
+}
+
+void launch_to_relative(const Params& p, uint32_t n, const float* xyz, const float4* abs4, float4* pos, int4* cells,
+                        cudaStream_t s) {
+    if (n) k_to_relative<<<fast_blocks(n), kBlock, 0, s>>>(p, n, xyz, abs4, pos, cells);
+}
+
+void launch_from_relative(const Params& p, uint32_t n, const float4* pos, const int4* cells, float* xyz,
+                          cudaStream_t s) {
+    if (n) k_from_relative<<<fast_blocks(n), kBlock, 0, s>>>(p, n, pos, cells, xyz);
+}
+
+void launch_state_stats_rel(const Params& p, const int4* cells, const float4* vel, Status* st, cudaStream_t s) {
+    if (p.n) k_state_stats_rel<<<fast_blocks(p.n), kBlock, 0, s>>>(p, cells, vel, st);
+}
+
+void launch_list_rel(const Params& p, const GridDev& g, const float4* pos, const int4* cells, const float4* pts,
+                     const uint32_t* start, uint32_t* out, cudaStream_t s) {
+    if (p.n) k_list_rel<<<fast_blocks(p.n), kBlock, 0, s>>>(p, g, pos, cells, pts, start, out);
 }
 
 }  // namespace slf

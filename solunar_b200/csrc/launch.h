@@ -14,9 +14,9 @@ namespace slf {
 void launch_state_stats(const Params& p, const float4* pos, const float4* vel, Status* st, cudaStream_t s);
 void launch_max_compression(const Params& p, const float* rho, Status* st, cudaStream_t s);
 
-// counting sort by dense cell index
-void launch_count_cells(const Params& p, const float4* pos, int3 low, int3 span, uint32_t* count, uint32_t* lin,
-                        uint32_t* slot, cudaStream_t s);
+// counting sort by dense cell index; cells (cell-relative positions) optional
+void launch_count_cells(const Params& p, const float4* pos, const int4* cells, int3 low, int3 span, uint32_t* count,
+                        uint32_t* lin, uint32_t* slot, cudaStream_t s);
 size_t scan_tiles(uint32_t m);
 // exclusive scan of data[0, m) in place; data[m] receives the total.  tile_sums holds
 // scan_tiles(m) + 1 entries.
@@ -25,8 +25,8 @@ void launch_scatter_members(uint32_t n, const uint32_t* lin, const uint32_t* slo
                             const uint32_t* ids, uint32_t* members, cudaStream_t s);
 void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start, const uint32_t* members,
                          const uint32_t* ids_in, const float4* pos_in, const float4* vel_in, const float* rho_in,
-                         const float* kap_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
-                         float* kap_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
+                         const int4* cells_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
+                         int4* cells_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
                          cudaStream_t s);
 
 // pair passes: the density pass builds the substep's neighbour lists, the others walk them
@@ -61,10 +61,12 @@ void launch_list_fill(const Params& p, const GridDev& g, const float4* pos, cons
                       uint32_t* items, cudaStream_t s);
 
 // domain
-void launch_domain_flags(const Params& p, const float4* pos, float3 low, float3 high, uint32_t* keep, cudaStream_t s);
+void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, float3 low, float3 high,
+                         uint32_t* keep, cudaStream_t s);
 void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, const uint32_t* ids_in,
-                    const float4* pos_in, const float4* vel_in, const float* rho_in, uint32_t* ids_out,
-                    float4* pos_out, float4* vel_out, float* rho_out, cudaStream_t s);
+                    const float4* pos_in, const float4* vel_in, const float* rho_in, const int4* cells_in,
+                    uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out, int4* cells_out,
+                    cudaStream_t s);
 
 void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s);
 
@@ -73,22 +75,36 @@ void launch_pack3(uint32_t n, const float4* in, float* out, cudaStream_t s);
 void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s);
 
 // FAST arithmetic variants (kernels_fast.cu): same lists, order and sums, fused rounding; the
-// lists hold indexes only and each pass recomputes the kernel gradient from the positions
-void launch_density_fast(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos,
+// lists hold indexes only (with the cell step in their top bits) and each pass recomputes the
+// kernel gradient from the positions.  `cells` non-null (or `rel`) selects cell-relative
+// positions: pos holds offsets in [0, r) from the cell corner, cells the integer cells.
+void launch_density_fast(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const int4* cells,
                          const float4* walls, const PairLists& fl, const PairLists& wl, float* rho, float* press,
                          float* scaled, float* alpha, Status* st, cudaStream_t s);
 void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                             const float4* pos, const float4* vel, const float* rho, const float* press,
-                             const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                             float4* vel_pre, cudaStream_t s);
-void launch_rate_fast(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                      float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                      void* partials, Status* st, float* rate_out, cudaStream_t s);
-void launch_push_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                             const float4* pos, const int4* cells, const float4* vel, const float* rho,
+                             const float* press, const float* scaled, const float4* walls, float4* pos_out,
+                             int4* cells_out, float4* vel_out, Status* st, float4* vel_pre, cudaStream_t s);
+// the stiffness goes into pos.w, as in launch_rate
+void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc, const PairLists& fl,
+                      const PairLists& wl, float4* pos, const float4* vel, const float* rho, const float* alpha,
+                      const float4* walls, void* partials, Status* st, float* rate_out, cudaStream_t s);
+void launch_push_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                       const float4* pos, float4* vel, const float4* walls, const Status* st, cudaStream_t s);
-void launch_viscous_fast(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+void launch_viscous_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                          const float4* pos, const float4* vel, const float* rho, const float4* walls,
                          float4* vel_out, cudaStream_t s);
+void launch_advance_rel(const Params& p, const StepConsts* sc, const float4* pos_in, const int4* cells_in,
+                        float4* pos_out, int4* cells_out, float4* vel, Status* st, float4* vel_pre, cudaStream_t s);
+// absolute positions (xyz triples, or float4 when xyz is null) -> offsets and cells; and back
+void launch_to_relative(const Params& p, uint32_t n, const float* xyz, const float4* abs4, float4* pos, int4* cells,
+                        cudaStream_t s);
+void launch_from_relative(const Params& p, uint32_t n, const float4* pos, const int4* cells, float* xyz,
+                          cudaStream_t s);
+void launch_state_stats_rel(const Params& p, const int4* cells, const float4* vel, Status* st, cudaStream_t s);
+// start null: counts into out[i]; else fills lists at start[i]
+void launch_list_rel(const Params& p, const GridDev& g, const float4* pos, const int4* cells, const float4* pts,
+                     const uint32_t* start, uint32_t* out, cudaStream_t s);
 
 // The adjoint of one WCSPH substep (adjoint.cu).  Inputs are the recomputed forward of the
 // substep (sorted positions and velocities, lists, densities, pressures, the pre-clamp velocity,

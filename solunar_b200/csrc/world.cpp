@@ -207,6 +207,7 @@ struct World {
     std::vector<uint32_t> pend_ids;
     int cpos = 0, cid = 0;  // committed slots of pos/vel (of 3) and ids/rho (of 2)
     DevBuf<float4> pos[3], vel[3];
+    DevBuf<int4> cell[3];  // cell-relative positions: the cell of each pos slot's offsets
     DevBuf<uint32_t> ids[2];
     DevBuf<float> rho[2];
     DevBuf<float> press, scaled, alpha;
@@ -287,6 +288,7 @@ struct World {
             for (auto* b : {&ids[0], &ids[1], &lin, &cslot, &members, &count, &tiles, &keep, &dwstart, &fcnt, &wcnt})
                 b->release(stream);
             for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha}) b->release(stream);
+            for (auto* b : {&cell[0], &cell[1], &cell[2]}) b->release(stream);
             fent.release(stream);
             went.release(stream);
             partials.release(stream);
@@ -400,11 +402,14 @@ struct World {
     // ---- particles ---------------------------------------------------------------------------
 
     uint64_t total() const { return n + pend_ids.size(); }
+    // FAST list entries keep the index in 26 bits
+    uint64_t index_limit() const { return fast() ? (uint64_t(1) << 26) : UINT64_MAX; }
 
     int32_t add(uint64_t k, const float* p, const float* v, uint32_t* ids_out) {
         for (uint64_t i = 0; i < k; ++i)
             if (!finite3(p + 3 * i) || !finite3(v + 3 * i)) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
-        if (total() + k > s.max_particles || uint64_t(next_id) + k > uint64_t(UINT32_MAX))
+        if (total() + k > s.max_particles || uint64_t(next_id) + k > uint64_t(UINT32_MAX) ||
+            total() + k > index_limit())
             return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
         for (uint64_t i = 0; i < k; ++i) {
             pend_pos.push_back(make_float4(p[3 * i], p[3 * i + 1], p[3 * i + 2], 0.0f));
@@ -435,6 +440,8 @@ struct World {
         uint64_t tot = sat_mul(sat_mul(nx, ny), nz);
         uint64_t room = s.max_particles > total() ? s.max_particles - total() : 0;
         uint64_t ids_left = uint64_t(UINT32_MAX - next_id);
+        if (index_limit() > total()) room = std::min<uint64_t>(room, index_limit() - total());
+        else room = 0;
         if (tot > room || tot > ids_left) return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
         float half = spacing * 0.5f;
         float st[3] = {low[0] + half, low[1] + half, low[2] + half};
@@ -461,12 +468,21 @@ struct World {
         for (int i = 0; i < 3; ++i) {
             SLF_TRY(pos[i].ensure(m, i == cpos ? n : 0, stream));
             SLF_TRY(vel[i].ensure(m, i == cpos ? n : 0, stream));
+            if (rel()) SLF_TRY(cell[i].ensure(m, i == cpos ? n : 0, stream));
         }
         for (int i = 0; i < 2; ++i) {
             SLF_TRY(ids[i].ensure(m, i == cid ? n : 0, stream));
             SLF_TRY(rho[i].ensure(m, i == cid ? n : 0, stream));
         }
-        SLF_CUDA(cudaMemcpyAsync(pos[cpos].p + n, pend_pos.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        if (rel()) {
+            // absolute positions land in a free slot, then become offsets and cells
+            float4* tmp = pos[(cpos + 1) % 3].p;
+            SLF_CUDA(cudaMemcpyAsync(tmp, pend_pos.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
+            launch_to_relative(params(), uint32_t(k), nullptr, tmp, pos[cpos].p + n, cell[cpos].p + n, stream);
+        } else {
+            SLF_CUDA(cudaMemcpyAsync(pos[cpos].p + n, pend_pos.data(), k * sizeof(float4), cudaMemcpyHostToDevice,
+                                     stream));
+        }
         SLF_CUDA(cudaMemcpyAsync(vel[cpos].p + n, pend_vel.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
         SLF_CUDA(cudaMemcpyAsync(ids[cid].p + n, pend_ids.data(), k * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         SLF_CUDA(cudaMemsetAsync(rho[cid].p + n, 0, k * sizeof(float), stream));
@@ -497,19 +513,23 @@ struct World {
     }
 
     bool fast() const { return s.arithmetic == SLF_ARITHMETIC_FAST; }
+    // cell-relative positions (always with FAST arithmetic)
+    bool rel() const { return s.positions == SLF_POSITIONS_CELL_RELATIVE; }
+    int4* cells_of(int slot) const { return rel() ? cell[slot].p : nullptr; }
 
-    // the pair passes of the settings' arithmetic
-    void density_pass(const Params& p, const float4* ps, const PairLists& fl, const PairLists& wl, float* rh) {
+    // the pair passes of the settings' arithmetic, over the positions of slot a
+    void density_pass(const Params& p, int a, const PairLists& fl, const PairLists& wl, float* rh) {
         if (fast())
-            launch_density_fast(p, fgrid, wgrid, ps, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status,
-                                stream);
+            launch_density_fast(p, fgrid, wgrid, pos[a].p, cells_of(a), dwalls.p, fl, wl, rh, press.p, scaled.p,
+                                alpha.p, d_status, stream);
         else
-            launch_density(p, fgrid, wgrid, ps, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status, stream);
+            launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status,
+                           stream);
     }
     void force_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
         if (fast())
-            launch_wcsph_force_fast(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
-                                    pos[b].p, vel[b].p, d_status, vel_pre, stream);
+            launch_wcsph_force_fast(p, d_consts, fl, wl, pos[a].p, cells_of(a), vel[a].p, rho[nid].p, press.p,
+                                    scaled.p, dwalls.p, pos[b].p, cells_of(b), vel[b].p, d_status, vel_pre, stream);
         else
             launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
                                pos[b].p, vel[b].p, d_status, vel_pre, stream);
@@ -517,19 +537,29 @@ struct World {
     void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid,
                    float* rate_out = nullptr) {
         if (fast())
-            launch_rate_fast(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p,
-                             d_status, rate_out, stream);
+            launch_rate_fast(which, rel(), p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p,
+                             partials.p, d_status, rate_out, stream);
         else
             launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p, d_status,
                         rate_out, stream);
     }
     void push_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v) {
-        if (fast()) launch_push_fast(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
+        if (fast()) launch_push_fast(rel(), p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
         else launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
+    }
+    void advance_pass(const Params& p, int a, int b, float4* pre) {
+        if (rel()) launch_advance_rel(p, d_consts, pos[a].p, cell[a].p, pos[b].p, cell[b].p, vel[b].p, d_status, pre,
+                                      stream);
+        else launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, pre, stream);
+    }
+    void stats_pass(const Params& p) {
+        if (rel()) launch_state_stats_rel(p, cell[cpos].p, vel[cpos].p, d_status, stream);
+        else launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream);
     }
     void viscous_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
         if (fast())
-            launch_viscous_fast(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
+            launch_viscous_fast(rel(), p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p,
+                                stream);
         else
             launch_viscous(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
     }
@@ -564,6 +594,7 @@ struct World {
 
     int32_t check_room(int64_t count) const {
         uint64_t room = s.max_particles > wpos.size() ? s.max_particles - wpos.size() : 0;
+        if (index_limit() < UINT64_MAX) room = std::min<uint64_t>(room, index_limit() > wpos.size() ? index_limit() - wpos.size() : 0);
         if (count < 0 || uint64_t(count) > room || wall_next == UINT32_MAX)
             return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
         return SLF_OK;
@@ -705,8 +736,15 @@ struct World {
         std::vector<float4> w(m);
         std::vector<Key3> keys(m);
         for (size_t i = 0; i < m; ++i) {
-            w[i] = make_float4(wpos[i].x, wpos[i].y, wpos[i].z, 0.0f);
             keys[i] = cell_of(wpos[i]);
+            if (rel()) {  // offset from the corner of the wall point's cell
+                const double r = radius;
+                w[i] = make_float4(float(double(wpos[i].x) - double(keys[i].x) * r),
+                                   float(double(wpos[i].y) - double(keys[i].y) * r),
+                                   float(double(wpos[i].z) - double(keys[i].z) * r), 0.0f);
+            } else {
+                w[i] = make_float4(wpos[i].x, wpos[i].y, wpos[i].z, 0.0f);
+            }
         }
         std::vector<Key3> cells;
         std::vector<uint32_t> starts;
@@ -769,6 +807,12 @@ struct World {
 
     // ---- status --------------------------------------------------------------------------
 
+    // non-finite values in the last passes
+    int32_t check_state() const {
+        if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        return SLF_OK;
+    }
+
     int32_t read_status() {
         SLF_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(Status), cudaMemcpyDeviceToHost, stream));
         return sync();
@@ -789,7 +833,7 @@ struct World {
         if (stats_fresh) return SLF_OK;
         SLF_TRY(reset_status());
         Params p = params();
-        timed("stats", bytes_per_particle::stats, [&] { launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream); });
+        timed("stats", bytes_per_particle::stats, [&] { stats_pass(p); });
         SLF_TRY(read_status());
         stats_fresh = true;
         return SLF_OK;
@@ -823,7 +867,7 @@ struct World {
         int3 lo3 = make_int3(int(lo[0]), int(lo[1]), int(lo[2]));
         int3 sp3 = make_int3(int(span[0]), int(span[1]), int(span[2]));
         timed("hash_count", bytes_per_particle::count_cells,
-              [&] { launch_count_cells(p, pos[cpos].p, lo3, sp3, count.p, lin.p, cslot.p, stream); });
+              [&] { launch_count_cells(p, pos[cpos].p, cells_of(cpos), lo3, sp3, count.p, lin.p, cslot.p, stream); });
         timed("hash_scan", bytes_per_particle::scan, [&] { launch_exclusive_scan(count.p, volume, tiles.p, stream); });
         timed("hash_scatter", bytes_per_particle::scatter, [&] {
             launch_scatter_members(uint32_t(n), lin.p, cslot.p, count.p, ids[cid].p, members.p, stream);
@@ -836,7 +880,8 @@ struct World {
         }
         timed("hash_reorder", bytes_per_particle::reorder, [&] {
             launch_rank_reorder(uint32_t(n), lin.p, count.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p,
-                                rho[cid].p, nullptr, ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, nullptr,
+                                rho[cid].p, cells_of(cpos), ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p,
+                                cells_of(to),
                                 job_lo, job_hi, d_status, sort_dest, stream);
         });
         fgrid = GridDev{};
@@ -887,7 +932,7 @@ struct World {
         Params p = params();
         for (;;) {
             SLF_TRY(reset_status());
-            density_pass(p, pos[cpos].p, fluid_lists(), wall_lists(), rho[cid].p);
+            density_pass(p, cpos, fluid_lists(), wall_lists(), rho[cid].p);
             SLF_TRY(read_status());
             int32_t st = lists_fit();
             if (st == SLF_OK) return SLF_OK;
@@ -907,11 +952,11 @@ struct World {
         launch_set_consts(consts(dt), d_consts, stream);
         PairLists fl = fluid_lists(), wl = wall_lists();
         timed("density", bytes_per_particle::density_wcsph,
-              [&] { density_pass(p, pos[a].p, fl, wl, rho[nid].p); });
+              [&] { density_pass(p, a, fl, wl, rho[nid].p); });
         timed("wcsph_force_advance", bytes_per_particle::wcsph_force, [&] { force_pass(p, fl, wl, a, b, nid); });
         SLF_TRY(read_status());
         SLF_TRY(lists_fit());
-        if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        SLF_TRY(check_state());
         held = h_status->held;
         cpos = b;
         cid = nid;
@@ -995,15 +1040,15 @@ struct World {
         launch_set_consts(consts(dt), d_consts, stream);
         PairLists fl = fluid_lists(), wl = wall_lists();
         timed("density_alpha", bytes_per_particle::density_dfsph,
-              [&] { density_pass(p, pos[a].p, fl, wl, rho[nid].p); });
+              [&] { density_pass(p, a, fl, wl, rho[nid].p); });
         uint32_t div_it = 0, den_it = 0;
         SLF_TRY(solve(0, p, a, vel[a].p, nid, div_it));
         timed("viscosity", bytes_per_particle::viscosity, [&] { viscous_pass(p, fl, wl, a, b, nid); });
         SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it));
         timed("advance", bytes_per_particle::advance,
-              [&] { launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, vel_pre, stream); });
+              [&] { advance_pass(p, a, b, vel_pre); });
         SLF_TRY(read_status());
-        if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        SLF_TRY(check_state());
         held = h_status->held;
         iterations = div_it + den_it;
         last_iterations[0] = div_it;
@@ -1039,6 +1084,7 @@ struct World {
     // ---- the adjoint ---------------------------------------------------------------------------
 
     int32_t tape_begin(uint32_t every) {
+        if (rel()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on absolute positions only");
         SLF_TRY(flush());
         tape.on = true;
         tape.every = std::max<uint32_t>(every, 1u);
@@ -1141,7 +1187,7 @@ struct World {
         SLF_TRY(reset_status());
         launch_set_consts(consts(dt), d_consts, stream);
         PairLists fl = fluid_lists(), wl = wall_lists();
-        density_pass(p, pos[a].p, fl, wl, rho[nid].p);
+        density_pass(p, a, fl, wl, rho[nid].p);
         SLF_TRY(solve_record(0, p, a, vel[a].p, nid, rec.div_vel, rec.div_rate, rec.div_n));
         SLF_TRY(rec.va.ensure(n, 0, stream));
         SLF_CUDA(cudaMemcpyAsync(rec.va.p, vel[a].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
@@ -1149,9 +1195,9 @@ struct World {
         SLF_TRY(solve_record(1, p, a, vel[b].p, nid, rec.den_vel, rec.den_rate, rec.den_n));
         SLF_TRY(rec.pre.ensure(n, 0, stream));
         SLF_TRY(reset_status());
-        launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, rec.pre.p, stream);
+        advance_pass(p, a, b, rec.pre.p);
         SLF_TRY(read_status());
-        if (h_status->nonfinite) return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        SLF_TRY(check_state());
         cpos = b;
         cid = nid;
         lists_pos = a;
@@ -1391,7 +1437,7 @@ struct World {
             SLF_TRY(reset_status());
             Params p = params();
             timed("stats", bytes_per_particle::stats, [&] {
-                launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream);
+                stats_pass(p);
                 launch_max_compression(p, rho[cid].p, d_status, stream);
             });
             SLF_TRY(read_status());
@@ -1410,8 +1456,8 @@ struct World {
         SLF_TRY(keep.ensure(n + 1, 0, stream));
         SLF_TRY(members.ensure(n + 1, 0, stream));
         SLF_TRY(tiles.ensure(scan_tiles(uint32_t(n)) + 1, 0, stream));
-        launch_domain_flags(p, pos[cpos].p, make_float3(dlow.x, dlow.y, dlow.z), make_float3(dhigh.x, dhigh.y, dhigh.z),
-                            keep.p, stream);
+        launch_domain_flags(p, pos[cpos].p, cells_of(cpos), make_float3(dlow.x, dlow.y, dlow.z),
+                            make_float3(dhigh.x, dhigh.y, dhigh.z), keep.p, stream);
         SLF_CUDA(cudaMemcpyAsync(members.p, keep.p, n * 4, cudaMemcpyDeviceToDevice, stream));
         launch_exclusive_scan(members.p, uint32_t(n), tiles.p, stream);
         uint32_t kept = 0;
@@ -1421,7 +1467,7 @@ struct World {
         int to = (cpos + 1) % 3;
         if (to == lists_pos) to = (cpos + 2) % 3;
         launch_compact(uint32_t(n), keep.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p, rho[cid].p,
-                       ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, stream);
+                       cells_of(cpos), ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, cells_of(to), stream);
         SLF_CUDA(cudaStreamSynchronize(stream));
         lost = uint32_t(n - kept);
         n = kept;
@@ -1443,6 +1489,16 @@ struct World {
         return sync();
     }
 
+    // the committed positions as xyz triples (cell-relative ones rebuilt in double, rounded once)
+    int32_t read_positions(float* out, uint64_t k) {
+        if (!rel()) return read_vec(pos[cpos], out, k);
+        if (!k) return SLF_OK;
+        SLF_TRY(stage.ensure(3 * k, 0, stream));
+        launch_from_relative(params(), uint32_t(k), pos[cpos].p, cell[cpos].p, stage.p, stream);
+        SLF_CUDA(cudaMemcpyAsync(out, stage.p, k * 12, cudaMemcpyDeviceToHost, stream));
+        return sync();
+    }
+
     int32_t write_vec(DevBuf<float4>& b, const float* in, uint64_t k) {
         if (!k) return SLF_OK;
         SLF_TRY(stage.ensure(3 * k, 0, stream));
@@ -1457,7 +1513,14 @@ struct World {
         for (uint64_t i = 0; i < k; ++i)
             if (!finite3(p + 3 * i) || !finite3(v + 3 * i))
                 return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
-        SLF_TRY(write_vec(pos[cpos], p, k));
+        if (rel()) {
+            SLF_TRY(stage.ensure(3 * k, 0, stream));
+            SLF_CUDA(cudaMemcpyAsync(stage.p, p, k * 12, cudaMemcpyHostToDevice, stream));
+            launch_to_relative(params(), uint32_t(k), stage.p, nullptr, pos[cpos].p, cell[cpos].p, stream);
+            SLF_TRY(sync());
+        } else {
+            SLF_TRY(write_vec(pos[cpos], p, k));
+        }
         SLF_TRY(write_vec(vel[cpos], v, k));
         SLF_TRY(sync());
         lists_valid = false;
@@ -1489,7 +1552,8 @@ struct World {
         SLF_TRY(tl.ensure(scan_tiles(uint32_t(n)) + 1, 0, stream));
         const GridDev& g = walls ? wgrid : fgrid;
         const float4* pts = walls ? dwalls.p : pos[lists_pos].p;
-        launch_list_count(p, g, pos[lists_pos].p, pts, cnt.p, stream);
+        if (rel()) launch_list_rel(p, g, pos[lists_pos].p, cell[lists_pos].p, pts, nullptr, cnt.p, stream);
+        else launch_list_count(p, g, pos[lists_pos].p, pts, cnt.p, stream);
         launch_exclusive_scan(cnt.p, uint32_t(n), tl.p, stream);
         uint32_t total_items = 0;
         SLF_CUDA(cudaMemcpyAsync(&total_items, cnt.p + n, 4, cudaMemcpyDeviceToHost, stream));
@@ -1503,7 +1567,10 @@ struct World {
             } else if (total_items) {
                 st = it.ensure(total_items, 0, stream);
                 if (st == SLF_OK) {
-                    launch_list_fill(p, g, pos[lists_pos].p, pts, cnt.p, it.p, stream);
+                    if (rel())
+                        launch_list_rel(p, g, pos[lists_pos].p, cell[lists_pos].p, pts, cnt.p, it.p, stream);
+                    else
+                        launch_list_fill(p, g, pos[lists_pos].p, pts, cnt.p, it.p, stream);
                     st = read_plain(it, items, total_items);
                 }
             }
@@ -1596,10 +1663,13 @@ int32_t slf_create(const slf_settings* settings, slf_world** out) {
     SLF_NEED(out);
     *out = nullptr;
     if (!World::valid(*settings)) return fail(SLF_ERR_INVALID_SETTINGS, "invalid settings");
-    if (settings->positions != SLF_POSITIONS_ABSOLUTE || settings->warm_start)
-        return fail(SLF_ERR_UNSUPPORTED, "only absolute positions and cold starts are built");
+    if (settings->warm_start) return fail(SLF_ERR_UNSUPPORTED, "only cold starts are built");
     if (settings->arithmetic != SLF_ARITHMETIC_EXACT && settings->arithmetic != SLF_ARITHMETIC_FAST)
         return fail(SLF_ERR_INVALID_SETTINGS, "unknown arithmetic");
+    if (settings->positions != SLF_POSITIONS_ABSOLUTE && settings->positions != SLF_POSITIONS_CELL_RELATIVE)
+        return fail(SLF_ERR_INVALID_SETTINGS, "unknown positions");
+    if (settings->positions == SLF_POSITIONS_CELL_RELATIVE && settings->arithmetic != SLF_ARITHMETIC_FAST)
+        return fail(SLF_ERR_UNSUPPORTED, "cell-relative positions run with FAST arithmetic only");
     int devices = 0;
     if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
         return fail(SLF_ERR_CUDA, "no CUDA device");
@@ -1764,7 +1834,7 @@ int32_t slf_read_positions(const slf_world* world, float* out, uint64_t n) {
     SLF_TRY(prep_read(world, n));
     if (n) SLF_NEED(out);
     World& w = const_cast<World&>(world->w);
-    return w.read_vec(w.pos[w.cpos], out, n);
+    return w.read_positions(out, n);
 }
 
 int32_t slf_read_velocities(const slf_world* world, float* out, uint64_t n) {
@@ -1804,7 +1874,7 @@ int32_t slf_state_hash(const slf_world* world, uint64_t* out) {
     std::vector<uint32_t> id(n);
     std::vector<float> p(3 * n), v(3 * n);
     SLF_TRY(w.read_plain(w.ids[w.cid], id.data(), n));
-    SLF_TRY(w.read_vec(w.pos[w.cpos], p.data(), n));
+    SLF_TRY(w.read_positions(p.data(), n));
     SLF_TRY(w.read_vec(w.vel[w.cpos], v.data(), n));
     *out = w.state_hash_host(id, p, v);
     return SLF_OK;

@@ -93,13 +93,16 @@ class Scene:
     dt: float = 1e-3
     steps: int = 1
     seed: int = SEED
+    origin: tuple = (0.0, 0.0, 0.0)  # the whole scene moved by this much
+    container: bool = True
 
     @property
     def particles(self) -> int:
         return int(np.prod(self.block_counts))
 
     def initial_state(self):
-        pos = lattice_block(self.block_low, self.block_counts, self.settings.spacing)
+        low = tuple(float(b) + float(o) for b, o in zip(self.block_low, self.origin))
+        pos = lattice_block(low, self.block_counts, self.settings.spacing)
         if self.jitter:
             pos = (pos + jitter(len(pos), self.jitter, self.seed)).astype(np.float32)
         vel = np.zeros_like(pos)
@@ -110,7 +113,8 @@ class Scene:
 
     def build(self, world):
         """Adds the container and the particles to `world`; returns (positions, velocities)."""
-        world.add_box_container((0.0, 0.0, 0.0), self.tank)
+        if self.container:
+            world.add_box_container(self.origin, tuple(float(o) + float(t) for o, t in zip(self.origin, self.tank)))
         pos, vel = self.initial_state()
         world.add_particles(pos, vel)
         return pos, vel
@@ -137,6 +141,14 @@ def dfsph_precision_1m() -> Scene:
     s = FluidSettings(solver=FluidSolver.DFSPH, spacing=0.01, support=2.0)
     return Scene("dfsph_precision_1m", s, (4.0, 2.0, 2.0), (100, 100, 100), jitter=1e-5, velocity_sigma=0.05,
                  dt=1e-3, steps=300)
+
+
+def dfsph_precision_far(counts=(100, 100, 100), origin=(1024.0, 1024.0, 1024.0)) -> Scene:
+    """The precision study's block moved far from the origin, where an f32 coordinate keeps only
+    about 1/160 of the spacing: no container, no gravity, velocities N(0, 0.05 m/s)."""
+    s = FluidSettings(solver=FluidSolver.DFSPH, spacing=0.01, support=2.0, gravity=(0.0, 0.0, 0.0))
+    return Scene("dfsph_precision_far", s, (4.0, 2.0, 2.0), counts, jitter=1e-5, velocity_sigma=0.05, dt=1e-3,
+                 steps=300, origin=origin, container=False)
 
 
 def dfsph_dam_1m() -> Scene:
