@@ -211,10 +211,14 @@ typedef struct slf_param_grads {
     double gravity[3];   /* dL / d settings.gravity */
 } slf_param_grads;
 
-/* Starts recording the steps that follow for slf_step_backward: the current state is the first
- * checkpoint, and the state after every `checkpoint_every`-th step is kept too (segment
- * checkpointing: the backward pass recomputes each segment from its checkpoint).  The number of
- * particles must not change while recording.  WCSPH and DFSPH steps. */
+/* Starts recording the steps that follow for slf_step_backward.  checkpoint_every = k > 0: the
+ * current state is the first checkpoint and the state after every k-th step is kept too (segment
+ * checkpointing: the backward pass runs each segment forward again from its checkpoint, about
+ * twice the forward's work, for 36 bytes per particle per checkpoint).  checkpoint_every = 0:
+ * every substep keeps the state before it and its solver record (the rates and velocities of each
+ * DFSPH iteration), about 68 + 20 x iterations bytes per particle per substep; the backward pass
+ * then redoes only each substep's sort and densities.  The number of particles must not change
+ * while recording.  WCSPH and DFSPH steps. */
 int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
 /* Stops recording and frees the tape. */
 int32_t slf_tape_end(slf_world* world);

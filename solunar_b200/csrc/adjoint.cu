@@ -41,6 +41,51 @@ __device__ __forceinline__ void grad_factor(const Params& p, float d, float& g, 
     gp = -3.0f * p.grad_scale * om * om * p.inv_radius;
 }
 
+// Walks i's list four entries at a time: gather(j) for all four first, so their loads are in
+// flight together, then body(j, gathered) for each in list order (the sums keep their order).
+template <class G, class Gather, class Body>
+__device__ __forceinline__ void walk4(const PairLists& l, bool packed, uint32_t i, Gather&& gather, Body&& body) {
+    uint32_t n = listed_count(l, i);
+    for (uint32_t k = 0; k < n; k += 4) {
+        uint32_t j[4];
+        G g[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) j[u] = listed(l, packed, i, k + u < n ? k + u : n - 1);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) g[u] = gather(j[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u < n) body(j[u], g[u]);
+    }
+}
+
+struct Two {
+    float4 a, b;
+};
+struct Three {
+    float4 a, b, c;
+};
+struct FiveF {
+    float4 a, b, c;
+    float d, e;
+};
+
+// Adds three per-thread values into parameter-gradient slots: a block sum first, then one FP64
+// atomic per slot and block (every thread of the block calls it).
+struct SumD {
+    __device__ double operator()(double a, double b) const { return a + b; }
+};
+__device__ __forceinline__ void add_grads3(double* grads, int s0, int s1, int s2, double a, double b, double c) {
+    a = block_reduce(a, SumD(), 0.0);
+    b = block_reduce(b, SumD(), 0.0);
+    c = block_reduce(c, SumD(), 0.0);
+    if (threadIdx.x == 0) {
+        atomicAdd(&grads[s0], a);
+        atomicAdd(&grads[s1], b);
+        atomicAdd(&grads[s2], c);
+    }
+}
+
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
 __device__ __forceinline__ float dotf(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -72,17 +117,7 @@ __global__ void k_adj_advance(Params p, const StepConsts* __restrict__ sc, const
         gz = wz * dt;
     }
     // gravity: a_i gets g, so g-bar = sum of a-bar
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gx += __shfl_xor_sync(0xffffffffu, gx, o);
-        gy += __shfl_xor_sync(0xffffffffu, gy, o);
-        gz += __shfl_xor_sync(0xffffffffu, gz, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&grads[kGradGravity], gx);
-        atomicAdd(&grads[kGradGravity + 1], gy);
-        atomicAdd(&grads[kGradGravity + 2], gz);
-    }
+    add_grads3(grads, kGradGravity, kGradGravity + 1, kGradGravity + 2, gx, gy, gz);
 }
 
 // ---- forces (step.rs:173-211), wall viscosity (step.rs:262-301), Tait pressure (step.rs:147-172)
@@ -105,19 +140,21 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         float sbar = 0.0f, pbar = 0.0f, rbar = 0.0f;
 
         // fluid pairs: L = (a_i-bar - a_j-bar) . T(r, u, S, R)
-        uint32_t nf = listed_count(fl, i);
-        for (uint32_t k = 0; k < nf; ++k) {
-            uint32_t j = listed(fl, packed != 0, i, k);
-            float3 r = xi - f3(__ldg(&pos[j]));
+        walk4<FiveF>(fl, packed != 0, i,
+                     [&](uint32_t j) {
+                         return FiveF{__ldg(&pos[j]), __ldg(&vel[j]), __ldg(&ab[j]), __ldg(&rho[j]), __ldg(&scaled[j])};
+                     },
+                     [&](uint32_t, const FiveF& q) {
+            float3 r = xi - f3(q.a);
             float d2 = dotf(r, r);
-            if (d2 <= 0.0f) continue;
+            if (d2 <= 0.0f) return;
             float d = sqrtf(d2);
             float g, gp;
             grad_factor(p, d, g, gp);
-            float3 u = vi - f3(__ldg(&vel[j]));
-            float3 w = ai - f3(__ldg(&ab[j]));
-            float R = rho_i + __ldg(&rho[j]);
-            float S = s_i + __ldg(&scaled[j]);
+            float3 u = vi - f3(q.b);
+            float3 w = ai - f3(q.c);
+            float R = rho_i + q.d;
+            float S = s_i + q.e;
             float ur = dotf(u, r);
             bool act = ur < 0.0f;
             float t = act ? ur : 0.0f;
@@ -136,7 +173,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
             sbar += P;
             // viscosity enters a_i's own term: a_i-bar . dT/dnu
             nu_bar += (double)(2.0f * m * g * t * dotf(ai, r) / den);
-        }
+        });
 
         // walls: pressure mirrored onto the wall (step.rs:197-202)
         uint32_t nw = listed_count(wl, i);
@@ -223,17 +260,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         vb[i] = make_float4(v0.x + vbar.x, v0.y + vbar.y, v0.z + vbar.z, 0.0f);
         rb[i] = add_rho ? rb[i] + rbar : rbar;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        nu_bar += __shfl_xor_sync(0xffffffffu, nu_bar, o);
-        nuw_bar += __shfl_xor_sync(0xffffffffu, nuw_bar, o);
-        b_bar += __shfl_xor_sync(0xffffffffu, b_bar, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&grads[kGradViscosity], nu_bar);
-        atomicAdd(&grads[kGradWallViscosity], nuw_bar);
-        atomicAdd(&grads[kGradStiffness], b_bar);
-    }
+    add_grads3(grads, kGradViscosity, kGradWallViscosity, kGradStiffness, nu_bar, nuw_bar, b_bar);
 }
 
 // ---- densities (mod.rs:621-675): rho_i = m (sum_j W(r_ij) + sum_w W(r_iw)) ---------------------
@@ -246,16 +273,20 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
     float3 xi = f3(pos[i]);
     float rbi = rb[i];
     float3 xbar = make_float3(0, 0, 0);
-    uint32_t nf = listed_count(fl, i);
-    for (uint32_t k = 0; k < nf; ++k) {
-        uint32_t j = listed(fl, packed != 0, i, k);
-        float3 r = xi - f3(__ldg(&pos[j]));
-        float d = sqrtf(dotf(r, r));
-        if (d <= 0.0f) continue;
-        float g, gp;
-        grad_factor(p, d, g, gp);
-        xbar = xbar + r * (g * p.mass * (rbi + __ldg(&rb[j])));
-    }
+    walk4<float4>(fl, packed != 0, i,
+                  [&](uint32_t j) {
+                      float4 q = __ldg(&pos[j]);
+                      q.w = __ldg(&rb[j]);
+                      return q;
+                  },
+                  [&](uint32_t, float4 q) {
+                      float3 r = xi - f3(q);
+                      float d = sqrtf(dotf(r, r));
+                      if (d <= 0.0f) return;
+                      float g, gp;
+                      grad_factor(p, d, g, gp);
+                      xbar = xbar + r * (g * p.mass * (rbi + q.w));
+                  });
     uint32_t nw = listed_count(wl, i);
     for (uint32_t k = 0; k < nw; ++k) {
         uint32_t j = listed(wl, packed != 0, i, k);
@@ -303,29 +334,31 @@ __global__ void k_adj_advance_dfsph(Params p, const StepConsts* __restrict__ sc,
 
 // One iteration's stiffness, back from the velocity adjoint w after its push: kappa-bar = -dt
 // rate(w); then through kappa = phi(rate) alpha (dfsph.rs:241-259).
+// Writes kw = (w, kappa) and vr = (v, rate-bar) per particle: the three records k_adj_push
+// gathers per neighbour (with the position).
 template <int WHICH>
 __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                       PairLists wl, int packed, const float4* __restrict__ pos,
                                                       const float4* __restrict__ walls,
                                                       const float4* __restrict__ w, const float* __restrict__ rate,
                                                       const float* __restrict__ alpha, const float* __restrict__ rho,
-                                                      float* __restrict__ ratebar, float* __restrict__ kappa,
-                                                      float* __restrict__ abar, float* __restrict__ rb) {
+                                                      const float4* __restrict__ vel, float4* __restrict__ kw,
+                                                      float4* __restrict__ vr, float* __restrict__ abar,
+                                                      float* __restrict__ rb) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const float dt = sc->dt, m = p.mass;
     float3 xi = f3(pos[i]), wi = f3(w[i]);
     float acc = 0.0f;
-    uint32_t nf = listed_count(fl, i);
-    for (uint32_t k = 0; k < nf; ++k) {
-        uint32_t j = listed(fl, packed != 0, i, k);
-        float3 r = xi - f3(__ldg(&pos[j]));
-        float d = sqrtf(dotf(r, r));
-        if (d <= 0.0f) continue;
-        float g, gp;
-        grad_factor(p, d, g, gp);
-        acc += dotf(wi - f3(__ldg(&w[j])), r) * g;
-    }
+    walk4<Two>(fl, packed != 0, i, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&w[j])}; },
+               [&](uint32_t, const Two& q) {
+                   float3 r = xi - f3(q.a);
+                   float d = sqrtf(dotf(r, r));
+                   if (d <= 0.0f) return;
+                   float g, gp;
+                   grad_factor(p, d, g, gp);
+                   acc += dotf(wi - f3(q.b), r) * g;
+               });
     uint32_t nw = listed_count(wl, i);
     for (uint32_t k = 0; k < nw; ++k) {
         uint32_t j = listed(wl, packed != 0, i, k);
@@ -350,8 +383,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
         phi = on ? ri / dt : 0.0f;
         dphi = on ? 1.0f / dt : 0.0f;
     }
-    kappa[i] = phi * ai;
-    ratebar[i] = kbar * ai * dphi;
+    float4 v = vel[i];
+    kw[i] = make_float4(wi.x, wi.y, wi.z, phi * ai);
+    vr[i] = make_float4(v.x, v.y, v.z, kbar * ai * dphi);
     abar[i] += kbar * phi;
     if (WHICH == 1) rb[i] += kbar * ai * dphi_rho;
 }
@@ -360,32 +394,30 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
 // rate adjoint); and the positions' share of both passes, through grad W.
 __global__ void __launch_bounds__(kBlock) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                      PairLists wl, int packed, const float4* __restrict__ pos,
-                                                     const float4* __restrict__ walls, const float4* __restrict__ w,
-                                                     const float* __restrict__ kappa,
-                                                     const float* __restrict__ ratebar,
-                                                     const float4* __restrict__ vel, float4* __restrict__ wout,
+                                                     const float4* __restrict__ walls, const float4* __restrict__ kw,
+                                                     const float4* __restrict__ vr, float4* __restrict__ wout,
                                                      float4* __restrict__ xb) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const float dt = sc->dt, m = p.mass;
-    float3 xi = f3(pos[i]), wi = f3(w[i]), vi = f3(vel[i]);
-    float ki = kappa[i], rbi = ratebar[i];
+    float4 own_w = kw[i], own_v = vr[i];
+    float3 xi = f3(pos[i]), wi = f3(own_w), vi = f3(own_v);
+    float ki = own_w.w, rbi = own_v.w;
     float3 vacc = make_float3(0, 0, 0), xacc = make_float3(0, 0, 0);
-    uint32_t nf = listed_count(fl, i);
-    for (uint32_t k = 0; k < nf; ++k) {
-        uint32_t j = listed(fl, packed != 0, i, k);
-        float3 r = xi - f3(__ldg(&pos[j]));
-        float d = sqrtf(dotf(r, r));
-        if (d <= 0.0f) continue;
-        float g, gp;
-        grad_factor(p, d, g, gp);
-        float rbj = __ldg(&ratebar[j]);
-        vacc = vacc + r * (g * m * (rbi + rbj));
-        // c . grad W(r) with c = -dt m (k_i + k_j)(w_i - w_j) + m (rb_i + rb_j)(v_i - v_j)
-        float3 c = (wi - f3(__ldg(&w[j]))) * (-dt * m * (ki + __ldg(&kappa[j]))) +
-                   (vi - f3(__ldg(&vel[j]))) * (m * (rbi + rbj));
-        xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
-    }
+    walk4<Three>(fl, packed != 0, i,
+                 [&](uint32_t j) { return Three{__ldg(&pos[j]), __ldg(&kw[j]), __ldg(&vr[j])}; },
+                 [&](uint32_t, const Three& q) {
+                     float3 r = xi - f3(q.a);
+                     float d = sqrtf(dotf(r, r));
+                     if (d <= 0.0f) return;
+                     float g, gp;
+                     grad_factor(p, d, g, gp);
+                     float rbj = q.c.w;
+                     vacc = vacc + r * (g * m * (rbi + rbj));
+                     // c . grad W(r) with c = -dt m (k_i + k_j)(w_i - w_j) + m (rb_i + rb_j)(v_i - v_j)
+                     float3 c = (wi - f3(q.b)) * (-dt * m * (ki + q.b.w)) + (vi - f3(q.c)) * (m * (rbi + rbj));
+                     xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
+                 });
     uint32_t nw = listed_count(wl, i);
     for (uint32_t k = 0; k < nw; ++k) {
         uint32_t j = listed(wl, packed != 0, i, k);
@@ -416,17 +448,7 @@ __global__ void k_adj_scale(Params p, const StepConsts* __restrict__ sc, const f
         gy = v.y * dt;
         gz = v.z * dt;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gx += __shfl_xor_sync(0xffffffffu, gx, o);
-        gy += __shfl_xor_sync(0xffffffffu, gy, o);
-        gz += __shfl_xor_sync(0xffffffffu, gz, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&grads[kGradGravity], gx);
-        atomicAdd(&grads[kGradGravity + 1], gy);
-        atomicAdd(&grads[kGradGravity + 2], gz);
-    }
+    add_grads3(grads, kGradGravity, kGradGravity + 1, kGradGravity + 2, gx, gy, gz);
 }
 
 // factors (dfsph.rs:138-163): alpha = 1 / T, T = |G|^2 + sum_j |m grad W_ij|^2,
@@ -440,16 +462,14 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists f
     if (i >= p.n) return;
     float3 xi = f3(pos[i]);
     float3 G = make_float3(0, 0, 0);
-    uint32_t nf = listed_count(fl, i);
-    for (uint32_t k = 0; k < nf; ++k) {
-        uint32_t j = listed(fl, packed != 0, i, k);
-        float3 r = xi - f3(__ldg(&pos[j]));
+    walk4<float4>(fl, packed != 0, i, [&](uint32_t j) { return __ldg(&pos[j]); }, [&](uint32_t, float4 q) {
+        float3 r = xi - f3(q);
         float d = sqrtf(dotf(r, r));
-        if (d <= 0.0f) continue;
+        if (d <= 0.0f) return;
         float g, gp;
         grad_factor(p, d, g, gp);
         G = G + r * (g * p.mass);
-    }
+    });
     uint32_t nw = listed_count(wl, i);
     for (uint32_t k = 0; k < nw; ++k) {
         uint32_t j = listed(wl, packed != 0, i, k);
@@ -476,19 +496,18 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, Pa
     float3 Gi = f3(own);
     float tbi = own.w;
     float3 xacc = make_float3(0, 0, 0);
-    uint32_t nf = listed_count(fl, i);
-    for (uint32_t k = 0; k < nf; ++k) {
-        uint32_t j = listed(fl, packed != 0, i, k);
-        float3 r = xi - f3(__ldg(&pos[j]));
-        float d = sqrtf(dotf(r, r));
-        if (d <= 0.0f) continue;
-        float g, gp;
-        grad_factor(p, d, g, gp);
-        float3 gw = r * (g * m);
-        float4 oj = __ldg(&gt[j]);
-        float3 c = (Gi + gw) * (2.0f * m * tbi) - (f3(oj) - gw) * (2.0f * m * oj.w);
-        xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
-    }
+    walk4<Two>(fl, packed != 0, i, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&gt[j])}; },
+               [&](uint32_t, const Two& q) {
+                   float3 r = xi - f3(q.a);
+                   float d = sqrtf(dotf(r, r));
+                   if (d <= 0.0f) return;
+                   float g, gp;
+                   grad_factor(p, d, g, gp);
+                   float3 gw = r * (g * m);
+                   float4 oj = q.b;
+                   float3 c = (Gi + gw) * (2.0f * m * tbi) - (f3(oj) - gw) * (2.0f * m * oj.w);
+                   xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
+               });
     uint32_t nw = listed_count(wl, i);
     for (uint32_t k = 0; k < nw; ++k) {
         uint32_t j = listed(wl, packed != 0, i, k);
@@ -532,17 +551,16 @@ void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float
 
 void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                           bool packed, const float4* pos, const float4* walls, const float4* w, const float* rate,
-                          const float* alpha, const float* rho, const float4* vel, float* ratebar, float* kappa,
+                          const float* alpha, const float* rho, const float4* vel, float4* kw, float4* vr,
                           float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s) {
     if (!p.n) return;
     if (which == 1)
         k_adj_kappa<1><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
-                                                          rho, ratebar, kappa, abar, rb);
+                                                          rho, vel, kw, vr, abar, rb);
     else
         k_adj_kappa<0><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
-                                                          rho, ratebar, kappa, abar, rb);
-    k_adj_push<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, kappa, ratebar, vel,
-                                                  wout, xb);
+                                                          rho, vel, kw, vr, abar, rb);
+    k_adj_push<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, kw, vr, wout, xb);
 }
 
 void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,

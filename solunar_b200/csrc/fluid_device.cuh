@@ -65,6 +65,15 @@ struct Status {
     uint32_t iterations;   // pushes of the running solve so far (dfsph.rs:236, 273)
 };
 
+// What a solver check records for the adjoint (both null: nothing): at slot it = the solve's
+// iteration count when the check runs, rate[it * n + i] = the density rate of particle i and
+// vel[it * n + i] = the velocity it read.  The device stops a solve at max_iterations, so
+// max_iterations + 1 slots always suffice.
+struct SolveRec {
+    float* rate;
+    float4* vel;
+};
+
 // Neighbour lists of one substep, built by the density pass in the reference's list order
 // (mod.rs:570-606) and read by every later pass of the substep.  An entry is 8 bytes: the
 // neighbour's index and its kernel gradient factor g = slope(d) / d (0 at d = 0), kept because

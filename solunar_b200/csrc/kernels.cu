@@ -528,7 +528,7 @@ __device__ __forceinline__ void rate_particle(const Params& p, const StepConsts*
                                               const float4* __restrict__ pos, const float4* __restrict__ vel,
                                               const float* __restrict__ rho, const float* __restrict__ alpha,
                                               const float4* __restrict__ walls, float* __restrict__ kappa_w,
-                                              float* __restrict__ rate_out, double& err, uint32_t& loaded) {
+                                              SolveRec rec, uint32_t slot, double& err, uint32_t& loaded) {
     const float dt = sc->dt;
     float4 a = pos[i];
     float4 v = vel[i];
@@ -542,7 +542,11 @@ __device__ __forceinline__ void rate_particle(const Params& p, const StepConsts*
         rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
     });
     rate = rate * p.mass;
-    if (rate_out) rate_out[i] = rate;  // recorded for the adjoint
+    if (rec.rate) {  // recorded for the adjoint
+        size_t at = size_t(slot) * p.n + i;
+        rec.rate[at] = rate;
+        rec.vel[at] = v;
+    }
     float target, error;
     if (WHICH == 1) {
         float over = fmaxf(rho[i] + dt * rate - p.rest, 0.0f);
@@ -568,14 +572,16 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, 
                                                  const float* __restrict__ alpha, const float4* __restrict__ walls,
                                                  float* __restrict__ kappa_w, DD* __restrict__ partial,
                                                  uint32_t* __restrict__ partial_loaded, Status* st,
-                                                 float* __restrict__ rate_out) {
+                                                 SolveRec rec) {
     // a solve that already stopped leaves the rest of its batch of launches idle
     if (__ldcg(&st->settled)) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double err = 0.0;
     uint32_t loaded = 0;
+    // every block reads the count before the last block advances it
+    const uint32_t slot = rec.rate ? __ldcg(&st->iterations) : 0u;
     if (i < p.n)
-        rate_particle<WHICH>(p, sc, fl, wl, i, FromGlobal{pos, vel}, pos, vel, rho, alpha, walls, kappa_w, rate_out,
+        rate_particle<WHICH>(p, sc, fl, wl, i, FromGlobal{pos, vel}, pos, vel, rho, alpha, walls, kappa_w, rec, slot,
                              err, loaded);
     residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
 }
@@ -842,17 +848,17 @@ size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (size
 
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 void* partials, Status* st, float* rate_out, cudaStream_t s) {
+                 void* partials, Status* st, SolveRec rec, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = blocks_for(p.n);
     DD* part = static_cast<DD*>(partials);
     uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
     if (which == 0)
         k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
-                                        part, loaded, st, rate_out);
+                                        part, loaded, st, rec);
     else
         k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
-                                        part, loaded, st, rate_out);
+                                        part, loaded, st, rec);
 }
 
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,

@@ -496,7 +496,7 @@ __device__ __forceinline__ void rate_particle_fast(const Params& p, const StepCo
                                                    const float4* __restrict__ vel, const float* __restrict__ rho,
                                                    const float* __restrict__ alpha,
                                                    const float4* __restrict__ walls, float* __restrict__ kappa,
-                                                   float* __restrict__ rate_out, double& err, uint32_t& loaded) {
+                                                   SolveRec rec, uint32_t slot, double& err, uint32_t& loaded) {
     const float dt = sc->dt;
     float4 a = pos[i];
     float4 v = vel[i];
@@ -512,7 +512,11 @@ __device__ __forceinline__ void rate_particle_fast(const Params& p, const StepCo
         rate = fmaf(g, fmaf(v.x, r.x, fmaf(v.y, r.y, v.z * r.z)), rate);
     });
     rate = rate * p.mass;
-    if (rate_out) rate_out[i] = rate;
+    if (rec.rate) {
+        size_t at = size_t(slot) * p.n + i;
+        rec.rate[at] = rate;
+        rec.vel[at] = v;
+    }
     float target, error;
     if (WHICH == 1) {
         float over = fmaxf(fmaf(dt, rate, rho[i]) - p.rest, 0.0f);
@@ -537,15 +541,16 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
                                                       const float4* __restrict__ walls, float* __restrict__ kappa,
                                                       DD* __restrict__ partial,
                                                       uint32_t* __restrict__ partial_loaded, Status* st,
-                                                      float* __restrict__ rate_out) {
+                                                      SolveRec rec) {
     if (__ldcg(&st->settled)) return;
+    const uint32_t slot = rec.rate ? __ldcg(&st->iterations) : 0u;
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double err = 0.0;
     uint32_t loaded = 0;
     if (i < p.n)
         rate_particle_fast<WHICH, REL>(p, sc, fl, wl, i, FromGlobalF{pos, vel}, pos, vel, rho, alpha, walls, kappa,
-                                       rate_out, err, loaded);
+                                       rec, slot, err, loaded);
     residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
 }
 
@@ -775,7 +780,7 @@ void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLi
 
 void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc, const PairLists& fl,
                       const PairLists& wl, float4* pos, const float4* vel, const float* rho, const float* alpha,
-                      const float4* walls, void* partials, Status* st, float* rate_out, cudaStream_t s) {
+                      const float4* walls, void* partials, Status* st, SolveRec rec, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = fast_blocks(p.n);
     DD* part = static_cast<DD*>(partials);
@@ -783,16 +788,16 @@ void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc
     float* kw = reinterpret_cast<float*>(pos);
     if (which == 0 && rel)
         k_rate_fast<0, true><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
-                                                   rate_out);
+                                                   rec);
     else if (which == 0)
         k_rate_fast<0, false><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
-                                                    rate_out);
+                                                    rec);
     else if (rel)
         k_rate_fast<1, true><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
-                                                   rate_out);
+                                                   rec);
     else
         k_rate_fast<1, false><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
-                                                    rate_out);
+                                                    rec);
 }
 
 void launch_push_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,

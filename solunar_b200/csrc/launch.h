@@ -43,10 +43,10 @@ size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
 // sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve
 // has settled, so a batch of iterations can be queued ahead of the check that ends it.
-// rate_out (optional): each particle's density rate, recorded for the adjoint
+// rec (optional): the check's rates and the velocities it read, recorded for the adjoint
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 void* partials, Status* st, float* rate_out, cudaStream_t s);
+                 void* partials, Status* st, SolveRec rec, cudaStream_t s);
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                  float4* vel, const float4* walls, const Status* st, cudaStream_t s);
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
@@ -88,7 +88,7 @@ void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLi
 // the stiffness goes into pos.w, as in launch_rate
 void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc, const PairLists& fl,
                       const PairLists& wl, float4* pos, const float4* vel, const float* rho, const float* alpha,
-                      const float4* walls, void* partials, Status* st, float* rate_out, cudaStream_t s);
+                      const float4* walls, void* partials, Status* st, SolveRec rec, cudaStream_t s);
 void launch_push_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                       const float4* pos, float4* vel, const float4* walls, const Status* st, cudaStream_t s);
 void launch_viscous_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
@@ -124,7 +124,7 @@ void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float
                               const float4* vo, float4* xb, float4* w, cudaStream_t s);
 void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                           bool packed, const float4* pos, const float4* walls, const float4* w, const float* rate,
-                          const float* alpha, const float* rho, const float4* vel, float* ratebar, float* kappa,
+                          const float* alpha, const float* rho, const float4* vel, float4* kw, float4* vr,
                           float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s);
 void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,
                           const float4* pos, const float4* vel, const float* rho, const float* zeros,

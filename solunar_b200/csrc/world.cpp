@@ -250,6 +250,34 @@ struct World {
     uint32_t* sort_dest = nullptr;
     float4* vel_pre = nullptr;
 
+    // What the adjoint of a DFSPH substep needs beyond the substep's sort and densities: each
+    // solver iteration's density rates and the velocities its check read, the velocities the
+    // viscosity read and the advance's clamp flags.
+    struct DfsphRecord {
+        DevBuf<float4> div_vel, den_vel, va, pre;
+        DevBuf<float> div_rate, den_rate;
+        uint32_t div_n = 0, den_n = 0;
+        void release(cudaStream_t st) {
+            for (auto* b : {&div_vel, &den_vel, &va, &pre}) b->release(st);
+            div_rate.release(st);
+            den_rate.release(st);
+        }
+    };
+    // A substep recorded as it ran (tapes that checkpoint every substep's record): the state
+    // before it and its solver record.
+    struct SubRecord {
+        float dt = 0.0f;
+        DevBuf<float4> pos, vel;
+        DevBuf<uint32_t> ids;
+        DfsphRecord rec;
+        void release(cudaStream_t st) {
+            pos.release(st);
+            vel.release(st);
+            ids.release(st);
+            rec.release(st);
+        }
+    };
+
     // ---- the tape of slf_tape_begin: checkpoints and the substep lengths of each step ----
     struct Tape {
         bool on = false;
@@ -259,6 +287,7 @@ struct World {
         std::vector<size_t> ckpt_step;          // checkpoint c = the state before step ckpt_step[c]
         DevBuf<float4> cpos, cvel;              // [c][n]
         DevBuf<uint32_t> cids;
+        std::vector<std::unique_ptr<SubRecord>> subs;  // every == 0: each substep's record
     } tape;
     std::vector<float>* tape_step = nullptr;  // the step being recorded
     Profiler prof;
@@ -343,6 +372,13 @@ struct World {
         double expected = 4.0 / 3.0 * 3.14159265358979 * double(s.support) * s.support * s.support;
         list_cap = (uint32_t(expected * 1.5 + 16.0) + 7u) & ~7u;
         SLF_CUDA(cudaSetDevice(s.device));
+        // device memory freed on the world's stream stays in this process's default pool for the
+        // next allocation (tapes, list growth) instead of going back at every synchronisation
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, s.device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
         SLF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         SLF_CUDA(cudaMalloc(&d_status, sizeof(Status)));
         SLF_CUDA(cudaMalloc(&d_consts, sizeof(StepConsts)));
@@ -535,13 +571,13 @@ struct World {
                                pos[b].p, vel[b].p, d_status, vel_pre, stream);
     }
     void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid,
-                   float* rate_out = nullptr) {
+                   SolveRec rec = SolveRec{nullptr, nullptr}) {
         if (fast())
             launch_rate_fast(which, rel(), p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p,
-                             partials.p, d_status, rate_out, stream);
+                             partials.p, d_status, rec, stream);
         else
             launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p, d_status,
-                        rate_out, stream);
+                        rec, stream);
     }
     void push_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v) {
         if (fast()) launch_push_fast(rel(), p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
@@ -972,7 +1008,8 @@ struct World {
     // the stopping check into no-ops, so the host waits once a batch instead of once an
     // iteration.  A batch is as long as the last solve of the same kind took.
     uint32_t expected_iterations[2] = {2, 2};
-    int32_t solve(int which, const Params& p, int a, float4* v, int nid, uint32_t& iterations) {
+    int32_t solve(int which, const Params& p, int a, float4* v, int nid, uint32_t& iterations,
+                  SolveRec rec = SolveRec{nullptr, nullptr}) {
         iterations = 0;
         PairLists fl = fluid_lists(), wl = wall_lists();
         SLF_CUDA(cudaMemsetAsync(&d_status->settled, 0, 4, stream));
@@ -985,7 +1022,7 @@ struct World {
         uint32_t batch = std::max<uint32_t>(expected_iterations[which], 1u);
         uint32_t queued = 0;
         auto rate = [&] {
-            timed(rate_name, rate_bytes, [&] { rate_pass(which, p, fl, wl, a, v, nid); });
+            timed(rate_name, rate_bytes, [&] { rate_pass(which, p, fl, wl, a, v, nid, rec); });
             kinds.push_back(0);
         };
         // check, then (push, check) pairs: the order of the reference's loop
@@ -1030,8 +1067,25 @@ struct World {
         }
     }
 
-    // one DFSPH substep (dfsph.rs:79-103) from the committed state; commits on success
-    int32_t dfsph_substep(float dt, uint32_t& held, uint32_t& iterations) {
+    // a solve's records land here, max_iterations + 1 slots, before they are kept
+    DevBuf<float> rec_rate;
+    DevBuf<float4> rec_vel;
+
+    int32_t keep_record(uint32_t its, DevBuf<float>& rates, DevBuf<float4>& vels) {
+        size_t m = size_t(its) * n;
+        SLF_TRY(rates.ensure(std::max<size_t>(m, 1), 0, stream));
+        SLF_TRY(vels.ensure(std::max<size_t>(m, 1), 0, stream));
+        if (m) {
+            SLF_CUDA(cudaMemcpyAsync(rates.p, rec_rate.p, m * 4, cudaMemcpyDeviceToDevice, stream));
+            SLF_CUDA(cudaMemcpyAsync(vels.p, rec_vel.p, m * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        }
+        return SLF_OK;
+    }
+
+    // one DFSPH substep (dfsph.rs:79-103) from the committed state; commits on success.  With
+    // `rec`, the solves are recorded for the adjoint (the same batched launches, the slot of
+    // each check taken from the device's iteration count).
+    int32_t dfsph_substep(float dt, uint32_t& held, uint32_t& iterations, DfsphRecord* rec = nullptr) {
         Params p = params();
         int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
         SLF_TRY(sort_into(a));
@@ -1042,11 +1096,30 @@ struct World {
         timed("density_alpha", bytes_per_particle::density_dfsph,
               [&] { density_pass(p, a, fl, wl, rho[nid].p); });
         uint32_t div_it = 0, den_it = 0;
-        SLF_TRY(solve(0, p, a, vel[a].p, nid, div_it));
+        SolveRec sr{nullptr, nullptr};
+        if (rec) {
+            size_t slots = (size_t(s.max_iterations) + 1) * n;
+            SLF_TRY(rec_rate.ensure(slots, 0, stream));
+            SLF_TRY(rec_vel.ensure(slots, 0, stream));
+            sr = SolveRec{rec_rate.p, rec_vel.p};
+        }
+        SLF_TRY(solve(0, p, a, vel[a].p, nid, div_it, sr));
+        if (rec) {
+            SLF_TRY(keep_record(div_it, rec->div_rate, rec->div_vel));
+            rec->div_n = div_it;
+            SLF_TRY(rec->va.ensure(n, 0, stream));
+            SLF_CUDA(cudaMemcpyAsync(rec->va.p, vel[a].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        }
         timed("viscosity", bytes_per_particle::viscosity, [&] { viscous_pass(p, fl, wl, a, b, nid); });
-        SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it));
-        timed("advance", bytes_per_particle::advance,
-              [&] { advance_pass(p, a, b, vel_pre); });
+        SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it, sr));
+        float4* pre = vel_pre;
+        if (rec) {
+            SLF_TRY(keep_record(den_it, rec->den_rate, rec->den_vel));
+            rec->den_n = den_it;
+            SLF_TRY(rec->pre.ensure(n, 0, stream));
+            pre = rec->pre.p;
+        }
+        timed("advance", bytes_per_particle::advance, [&] { advance_pass(p, a, b, pre); });
         SLF_TRY(read_status());
         SLF_TRY(check_state());
         held = h_status->held;
@@ -1071,13 +1144,15 @@ struct World {
             return fail(SLF_ERR_UNSUPPORTED, "the particles changed while a tape was recording");
         tape.steps.emplace_back();
         tape_step = &tape.steps.back();
+        size_t recorded = tape.subs.size();
         int32_t st = step_untaped(dt, out);
         tape_step = nullptr;
         if (st != SLF_OK) {
             tape.steps.pop_back();
+            drop_records(recorded);
             return st;
         }
-        if (tape.steps.size() % tape.every == 0) SLF_TRY(checkpoint());
+        if (tape.every && tape.steps.size() % tape.every == 0) SLF_TRY(checkpoint());
         return SLF_OK;
     }
 
@@ -1087,17 +1162,41 @@ struct World {
         if (rel()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on absolute positions only");
         SLF_TRY(flush());
         tape.on = true;
-        tape.every = std::max<uint32_t>(every, 1u);
+        tape.every = every;
         tape.n = n;
         tape.steps.clear();
         tape.ckpt_step.clear();
-        return checkpoint();
+        drop_records(0);
+        return every ? checkpoint() : SLF_OK;
+    }
+
+    // releases the recorded substeps from the keep-th on
+    void drop_records(size_t keep) {
+        while (tape.subs.size() > keep) {
+            tape.subs.back()->release(stream);
+            tape.subs.pop_back();
+        }
+    }
+
+    // a new substep record holding the committed state, for a tape with every == 0
+    int32_t record_begin(float dt) {
+        auto sub = std::make_unique<SubRecord>();
+        sub->dt = dt;
+        SLF_TRY(sub->pos.ensure(n, 0, stream));
+        SLF_TRY(sub->vel.ensure(n, 0, stream));
+        SLF_TRY(sub->ids.ensure(n, 0, stream));
+        SLF_TRY(save_state(sub->pos.p, sub->vel.p, sub->ids.p));
+        tape.subs.push_back(std::move(sub));
+        return SLF_OK;
     }
 
     int32_t tape_end() {
         tape.on = false;
         tape.steps.clear();
         tape.ckpt_step.clear();
+        drop_records(0);
+        rec_rate.release(stream);
+        rec_vel.release(stream);
         tape.cpos.release(stream);
         tape.cvel.release(stream);
         tape.cids.release(stream);
@@ -1143,68 +1242,27 @@ struct World {
         return st;
     }
 
-    // A DFSPH substep run again for its adjoint, keeping what the backward pass needs: each
-    // solver iteration's velocities and density rates, the velocities the viscosity read and the
-    // advance's clamp flags.  Iterations run one at a time (the forward's batches only save host
-    // waits); the counts equal the forward's because the recompute is bit-identical.
-    struct DfsphRecord {
-        DevBuf<float4> div_vel, den_vel, va, pre;
-        DevBuf<float> div_rate, den_rate;
-        uint32_t div_n = 0, den_n = 0;
-        void release(cudaStream_t st) {
-            for (auto* b : {&div_vel, &den_vel, &va, &pre}) b->release(st);
-            div_rate.release(st);
-            den_rate.release(st);
-        }
-    };
-
-    int32_t solve_record(int which, const Params& p, int a, float4* v, int nid, DevBuf<float4>& vels,
-                         DevBuf<float>& rates, uint32_t& count) {
-        count = 0;
-        PairLists fl = fluid_lists(), wl = wall_lists();
-        SLF_CUDA(cudaMemsetAsync(&d_status->settled, 0, 4, stream));
-        SLF_CUDA(cudaMemsetAsync(&d_status->iterations, 0, 4, stream));
-        for (;;) {
-            SLF_TRY(rates.ensure((size_t(count) + 1) * n, size_t(count) * n, stream));
-            SLF_TRY(vels.ensure((size_t(count) + 1) * n, size_t(count) * n, stream));
-            rate_pass(which, p, fl, wl, a, v, nid, rates.p + size_t(count) * n);
-            SLF_TRY(read_status());
-            SLF_TRY(lists_fit());
-            if (h_status->settled) return SLF_OK;
-            if (count > s.max_iterations) return fail(SLF_ERR_TIMEOUT, "solver stop flag never set");
-            SLF_CUDA(cudaMemcpyAsync(vels.p + size_t(count) * n, v, n * sizeof(float4), cudaMemcpyDeviceToDevice,
-                                     stream));
-            push_pass(p, fl, wl, a, v);
-            count += 1;
-        }
-    }
-
-    int32_t dfsph_substep_record(float dt, DfsphRecord& rec) {
+    // The sort and density pass of a DFSPH substep from the committed state, without the
+    // solves: the lists, factors and densities the adjoint of a recorded substep reads.  The
+    // sort's destinations go to sort_dest.  Commits nothing; returns the slots used.
+    int32_t dfsph_replay(float dt, int& a, int& nid) {
         Params p = params();
-        int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
-        SLF_TRY(sort_into(a));
-        int nid = 1 - cid;
-        SLF_TRY(reset_status());
-        launch_set_consts(consts(dt), d_consts, stream);
-        PairLists fl = fluid_lists(), wl = wall_lists();
-        density_pass(p, a, fl, wl, rho[nid].p);
-        SLF_TRY(solve_record(0, p, a, vel[a].p, nid, rec.div_vel, rec.div_rate, rec.div_n));
-        SLF_TRY(rec.va.ensure(n, 0, stream));
-        SLF_CUDA(cudaMemcpyAsync(rec.va.p, vel[a].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
-        viscous_pass(p, fl, wl, a, b, nid);
-        SLF_TRY(solve_record(1, p, a, vel[b].p, nid, rec.den_vel, rec.den_rate, rec.den_n));
-        SLF_TRY(rec.pre.ensure(n, 0, stream));
-        SLF_TRY(reset_status());
-        advance_pass(p, a, b, rec.pre.p);
-        SLF_TRY(read_status());
-        SLF_TRY(check_state());
-        cpos = b;
-        cid = nid;
-        lists_pos = a;
-        lists_n = n;
-        lists_valid = true;
-        stats_fresh = true;
-        return SLF_OK;
+        a = (cpos + 1) % 3;
+        nid = 1 - cid;
+        for (int attempt = 0;; ++attempt) {
+            if (attempt > 0) {  // the committed state's box again
+                stats_fresh = false;
+                SLF_TRY(refresh_stats());
+            }
+            SLF_TRY(sort_into(a));
+            SLF_TRY(reset_status());
+            launch_set_consts(consts(dt), d_consts, stream);
+            density_pass(p, a, fluid_lists(), wall_lists(), rho[nid].p);
+            SLF_TRY(read_status());
+            int32_t st = lists_fit();
+            if (st == SLF_OK) return SLF_OK;
+            if (st != kRetry || attempt > 0) return st == kRetry ? fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice") : st;
+        }
     }
 
     // step_backward: reverse over the taped steps, one checkpoint segment at a time.
@@ -1219,24 +1277,24 @@ struct World {
             return SLF_OK;
         }
         // the committed state, to put back at the end
-        DevBuf<float4> spos, svel, xo, vo, xp, vp, ab, xb, vb, pre, gt;
+        DevBuf<float4> spos, svel, xo, vo, xp, vp, ab, xb, vb, pre, gt, kw, vr;
         DevBuf<uint32_t> sids, dest;
-        DevBuf<float> srho, rb, abar, ratebar, kap, zeros;
+        DevBuf<float> srho, rb, abar, zeros;
         DevBuf<double> grads;
         DfsphRecord rec;
         int32_t st = SLF_OK;
         auto release = [&] {
-            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt}) b->release(stream);
-            for (auto* b : {&srho, &rb, &abar, &ratebar, &kap, &zeros}) b->release(stream);
+            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt, &kw, &vr}) b->release(stream);
+            for (auto* b : {&srho, &rb, &abar, &zeros}) b->release(stream);
             sids.release(stream);
             dest.release(stream);
             grads.release(stream);
             rec.release(stream);
         };
         auto run = [&]() -> int32_t {
-            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt})
+            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt, &kw, &vr})
                 SLF_TRY(b->ensure(n, 0, stream));
-            for (auto* b : {&srho, &rb, &abar, &ratebar, &kap, &zeros}) SLF_TRY(b->ensure(n, 0, stream));
+            for (auto* b : {&srho, &rb, &abar, &zeros}) SLF_TRY(b->ensure(n, 0, stream));
             SLF_CUDA(cudaMemsetAsync(zeros.p, 0, n * 4, stream));
             SLF_TRY(sids.ensure(n, 0, stream));
             SLF_TRY(dest.ensure(n, 0, stream));
@@ -1245,7 +1303,93 @@ struct World {
             SLF_CUDA(cudaMemcpyAsync(srho.p, rho[cid].p, n * 4, cudaMemcpyDeviceToDevice, stream));
             SLF_TRY(write_vec(xo, dpos, n));
             SLF_TRY(write_vec(vo, dvel, n));
-            // states before each substep of a segment
+            // the adjoint of the substep whose forward state sits in slots a (sorted positions)
+            // and nid (densities), its constants in d_consts: (xo, vo) after it -> (xp, vp) before
+            auto adjoint_substep = [&](float dt, int a, int nid, const DfsphRecord& rec) -> int32_t {
+                Params p = params();
+                SLF_CUDA(cudaMemsetAsync(grads.p, 0, kGradSlots * sizeof(double), stream));
+                PairLists fl = fluid_lists(), wl = wall_lists();
+                bool packed = !fast();
+                if (s.solver == SLF_SOLVER_WCSPH) {
+                    launch_adjoint_wcsph(p, d_consts, fl, wl, packed, pos[a].p, vel[a].p, rho[nid].p, press.p,
+                                         scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p, xb.p, vb.p, rb.p, xp.p,
+                                         vp.p, grads.p, stream);
+                } else {
+                    // advance, density solve, viscosity, divergence solve, factors, densities,
+                    // sort: the substep's steps backwards
+                    launch_adj_advance_dfsph(p, d_consts, rec.pre.p, xo.p, vo.p, xb.p, vb.p, stream);
+                    SLF_CUDA(cudaMemsetAsync(rb.p, 0, n * 4, stream));
+                    SLF_CUDA(cudaMemsetAsync(abar.p, 0, n * 4, stream));
+                    for (uint32_t it = rec.den_n; it-- > 0;) {
+                        launch_adj_iteration(1, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
+                                             rec.den_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
+                                             rec.den_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p, vp.p, xb.p,
+                                             stream);
+                        std::swap(vb, vp);
+                    }
+                    launch_adj_viscosity(p, d_consts, fl, wl, packed, pos[a].p, rec.va.p, rho[nid].p, zeros.p,
+                                         dwalls.p, vb.p, ab.p, xb.p, rb.p, grads.p, stream);
+                    for (uint32_t it = rec.div_n; it-- > 0;) {
+                        launch_adj_iteration(0, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
+                                             rec.div_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
+                                             rec.div_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p, vp.p, xb.p,
+                                             stream);
+                        std::swap(vb, vp);
+                    }
+                    launch_adj_factors_density(p, fl, wl, packed, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p, rb.p,
+                                               xb.p, stream);
+                    launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream);
+                }
+                double g[kGradSlots];
+                SLF_CUDA(cudaMemcpyAsync(g, grads.p, sizeof(g), cudaMemcpyDeviceToHost, stream));
+                SLF_TRY(sync());
+                accumulate_param_grads(dt, g, pg);
+                std::swap(xo, xp);
+                std::swap(vo, vp);
+                return SLF_OK;
+            };
+            // substep q again from its state, recording what its adjoint reads; the state's slots
+            // come back in a and nid
+            auto recompute = [&](float dt, DfsphRecord& rec, int& a, int& nid) -> int32_t {
+                sort_dest = dest.p;
+                vel_pre = pre.p;
+                int32_t rs;
+                uint32_t held = 0, its = 0;
+                if (s.solver == SLF_SOLVER_WCSPH) {
+                    rs = wcsph_substep(dt, held);
+                    if (rs == kRetry) rs = wcsph_substep(dt, held);
+                } else {
+                    rs = dfsph_substep(dt, held, its, &rec);
+                    if (rs == kRetry) rs = dfsph_substep(dt, held, its, &rec);
+                }
+                if (rs == kRetry) rs = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
+                sort_dest = nullptr;
+                vel_pre = nullptr;
+                a = (cpos + 2) % 3;  // the committed substep's sorted positions
+                nid = cid;
+                return rs;
+            };
+
+            // every substep was recorded as it ran: only its sort and densities are redone
+            auto recorded = [&]() -> int32_t {
+                for (size_t q = tape.subs.size(); q-- > 0;) {
+                    SubRecord& sub = *tape.subs[q];
+                    SLF_TRY(load_state(sub.pos.p, sub.vel.p, sub.ids.p));
+                    int a = 0, nid = 0;
+                    if (s.solver == SLF_SOLVER_WCSPH) {
+                        SLF_TRY(recompute(sub.dt, sub.rec, a, nid));
+                    } else {
+                        sort_dest = dest.p;
+                        int32_t rs = dfsph_replay(sub.dt, a, nid);
+                        sort_dest = nullptr;
+                        SLF_TRY(rs);
+                    }
+                    SLF_TRY(adjoint_substep(sub.dt, a, nid, sub.rec));
+                }
+                return SLF_OK;
+            };
+
+            // checkpoints: states before each substep of a segment
             size_t most = 0;
             for (size_t c = 0; c < tape.ckpt_step.size(); ++c) {
                 size_t b = tape.ckpt_step[c], e = c + 1 < tape.ckpt_step.size() ? tape.ckpt_step[c + 1] : tape.steps.size();
@@ -1264,83 +1408,30 @@ struct World {
                 SLF_TRY(gpos.ensure(std::max<size_t>(most, 1) * n, 0, stream));
                 SLF_TRY(gvel.ensure(std::max<size_t>(most, 1) * n, 0, stream));
                 SLF_TRY(gids.ensure(std::max<size_t>(most, 1) * n, 0, stream));
-                Params p = params();
                 for (size_t c = tape.ckpt_step.size(); c-- > 0;) {
                     size_t b = tape.ckpt_step[c];
                     size_t e = c + 1 < tape.ckpt_step.size() ? tape.ckpt_step[c + 1] : tape.steps.size();
                     if (b >= e) continue;
                     std::vector<float> dts;
                     for (size_t t = b; t < e; ++t) dts.insert(dts.end(), tape.steps[t].begin(), tape.steps[t].end());
-                    // forward through the segment, keeping the state before each substep
+                    // forward through the segment, keeping the state before each substep (the
+                    // last substep runs once, recorded, below)
                     SLF_TRY(load_state(tape.cpos.p + c * n, tape.cvel.p + c * n, tape.cids.p + c * n));
                     for (size_t q = 0; q < dts.size(); ++q) {
                         SLF_TRY(save_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
-                        SLF_TRY(substep_retrying(dts[q]));
+                        if (q + 1 < dts.size()) SLF_TRY(substep_retrying(dts[q]));
                     }
                     // backward through it
                     for (size_t q = dts.size(); q-- > 0;) {
-                        SLF_TRY(load_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
-                        sort_dest = dest.p;
-                        vel_pre = pre.p;
-                        int32_t rs;
-                        if (s.solver == SLF_SOLVER_WCSPH) {
-                            rs = substep_retrying(dts[q]);
-                        } else {
-                            rs = dfsph_substep_record(dts[q], rec);
-                            if (rs == kRetry) {
-                                SLF_TRY(load_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
-                                rs = dfsph_substep_record(dts[q], rec);
-                            }
-                            if (rs == kRetry) rs = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
-                        }
-                        sort_dest = nullptr;
-                        vel_pre = nullptr;
-                        SLF_TRY(rs);
-                        int a = (cpos + 2) % 3;
-                        SLF_CUDA(cudaMemsetAsync(grads.p, 0, kGradSlots * sizeof(double), stream));
-                        PairLists fl = fluid_lists(), wl = wall_lists();
-                        bool packed = !fast();
-                        if (s.solver == SLF_SOLVER_WCSPH) {
-                            launch_adjoint_wcsph(p, d_consts, fl, wl, packed, pos[a].p, vel[a].p, rho[cid].p, press.p,
-                                                 scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p, xb.p, vb.p, rb.p,
-                                                 xp.p, vp.p, grads.p, stream);
-                        } else {
-                            // advance, density solve, viscosity, divergence solve, factors,
-                            // densities, sort: the substep's steps backwards
-                            launch_adj_advance_dfsph(p, d_consts, rec.pre.p, xo.p, vo.p, xb.p, vb.p, stream);
-                            SLF_CUDA(cudaMemsetAsync(rb.p, 0, n * 4, stream));
-                            SLF_CUDA(cudaMemsetAsync(abar.p, 0, n * 4, stream));
-                            for (uint32_t it = rec.den_n; it-- > 0;) {
-                                launch_adj_iteration(1, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
-                                                     rec.den_rate.p + size_t(it) * n, alpha.p, rho[cid].p,
-                                                     rec.den_vel.p + size_t(it) * n, ratebar.p, kap.p, abar.p, rb.p,
-                                                     vp.p, xb.p, stream);
-                                std::swap(vb, vp);
-                            }
-                            launch_adj_viscosity(p, d_consts, fl, wl, packed, pos[a].p, rec.va.p, rho[cid].p, zeros.p,
-                                                 dwalls.p, vb.p, ab.p, xb.p, rb.p, grads.p, stream);
-                            for (uint32_t it = rec.div_n; it-- > 0;) {
-                                launch_adj_iteration(0, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
-                                                     rec.div_rate.p + size_t(it) * n, alpha.p, rho[cid].p,
-                                                     rec.div_vel.p + size_t(it) * n, ratebar.p, kap.p, abar.p, rb.p,
-                                                     vp.p, xb.p, stream);
-                                std::swap(vb, vp);
-                            }
-                            launch_adj_factors_density(p, fl, wl, packed, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p,
-                                                       rb.p, xb.p, stream);
-                            launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream);
-                        }
-                        double g[kGradSlots];
-                        SLF_CUDA(cudaMemcpyAsync(g, grads.p, sizeof(g), cudaMemcpyDeviceToHost, stream));
-                        SLF_TRY(sync());
-                        accumulate_param_grads(dts[q], g, pg);
-                        std::swap(xo, xp);
-                        std::swap(vo, vp);
+                        if (q + 1 < dts.size()) SLF_TRY(load_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
+                        int a = 0, nid = 0;
+                        SLF_TRY(recompute(dts[q], rec, a, nid));
+                        SLF_TRY(adjoint_substep(dts[q], a, nid, rec));
                     }
                 }
                 return SLF_OK;
             };
-            int32_t r = segs();
+            int32_t r = tape.every == 0 ? recorded() : segs();
             rel2();
             SLF_TRY(r);
             if (dpos0) SLF_TRY(read_vec(xo, dpos0, n));
@@ -1396,6 +1487,7 @@ struct World {
                 for (uint32_t i = 0; i < substeps; ++i) {
                     uint32_t held = 0;
                     if (tape_step) tape_step->push_back(small);
+                    if (tape_step && tape.every == 0) SLF_TRY(record_begin(small));
                     int32_t st = wcsph_substep(small, held);
                     if (st == kRetry) st = wcsph_substep(small, held);
                     if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
@@ -1419,8 +1511,13 @@ struct World {
                     small = rmin(small, left);
                     uint32_t held = 0, its = 0;
                     if (tape_step) tape_step->push_back(small);
-                    int32_t st = dfsph_substep(small, held, its);
-                    if (st == kRetry) st = dfsph_substep(small, held, its);
+                    DfsphRecord* rec = nullptr;
+                    if (tape_step && tape.every == 0) {
+                        SLF_TRY(record_begin(small));
+                        rec = &tape.subs.back()->rec;
+                    }
+                    int32_t st = dfsph_substep(small, held, its, rec);
+                    if (st == kRetry) st = dfsph_substep(small, held, its, rec);
                     if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
                     SLF_TRY(st);
                     r.iterations += its;

@@ -210,3 +210,41 @@ def test_dfsph_parameter_gradients_match_the_fp64_reference(oracle_lib, dfsph_ad
     num = (dfsph_fd(make64, target, settings=dfsph_settings(gravity=(g[0] + eps, g[1], g[2]))) -
            dfsph_fd(make64, target, settings=dfsph_settings(gravity=(g[0] - eps, g[1], g[2])))) / (2 * eps)
     assert abs(params["gravity"][0] - num) <= 1e-3 * abs(num), (params["gravity"][0], num)
+
+
+# ---- tape modes: keeping every substep's record, or checkpoints at any spacing, feed the
+# backward pass the same forward values (recomputation is bit-identical), so the particle
+# gradients agree bit for bit; the parameter gradients are FP64 sums taken with atomics, whose
+# order varies, so they agree to 1e-9 ----
+
+def same_params(a, b):
+    flat = lambda d: np.array([d["viscosity"], d["sound_speed"], *d["gravity"]])
+    np.testing.assert_allclose(flat(a), flat(b), rtol=1e-9, atol=1e-300)
+
+def taped_gradients(w, steps, dt, every, target):
+    w.tape_begin(every)
+    for _ in range(steps):
+        w.step(dt)
+    L, c = loss(w, target)
+    n = w.len()
+    dpos = np.tile(2.0 * (c - target) / n, (n, 1)).astype(np.float32)
+    out = w.step_backward(dpos, np.zeros_like(dpos))
+    w.tape_end()
+    return out
+
+
+@pytest.mark.parametrize("every", [0, 1, 3])
+def test_dfsph_tape_modes_give_identical_gradients(gpu_lib, dfsph_adjoint, every):
+    pos, vel, target, dp0, dv0, params = dfsph_adjoint
+    w, _, _ = dfsph_run(gpu_lib.FluidWorld)
+    dp, dv, pr = taped_gradients(w, DFSPH_STEPS, DFSPH_DT, every, target)
+    assert np.array_equal(dp, dp0) and np.array_equal(dv, dv0)
+    same_params(pr, params)
+
+
+def test_wcsph_recorded_tape_gives_identical_gradients(gpu_lib, adjoint):
+    sc, pos, vel, target, dp0, dv0, params = adjoint
+    w, _, _ = run(gpu_lib.FluidWorld, sc)
+    dp, dv, pr = taped_gradients(w, STEPS, DT, 0, target)
+    assert np.array_equal(dp, dp0) and np.array_equal(dv, dv0)
+    same_params(pr, params)
