@@ -48,9 +48,9 @@ def parse():
     ap.add_argument("--positions", choices=["absolute", "cell_relative"], default="absolute",
                     help="cell_relative: offsets from each particle's cell (FAST arithmetic, no adjoint)")
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--adjoint-every", type=int, default=0,
+    ap.add_argument("--adjoint-every", type=int, default=8,
                     help="tape checkpoint spacing of the forward+adjoint leg; 0 records every substep")
-    ap.add_argument("--adjoint-steps", type=int, default=8,
+    ap.add_argument("--adjoint-steps", type=int, default=32,
                     help="steps of the forward+adjoint measurement (0 skips it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed CPU work in the baseline")
@@ -355,10 +355,10 @@ def main():
             m = world.particle_mass()
             return np.where((pos_now[:, 0] > 1.0)[:, None], m * vel_now, 0.0).astype(np.float32)
 
-        # one untimed round first, as the rounds of an optimisation loop follow one another (the
-        # tape's memory is then in the allocator's pool)
+        # one untimed round first (one segment long), as the rounds of an optimisation loop follow
+        # one another: the tape's memory is then in the allocator's pool
         world.tape_begin(every)
-        for _ in range(k):
+        for _ in range(k if every == 0 else min(k, every)):
             world.step(sc.dt)
         dv = loss_grad()
         world.step_backward(np.zeros_like(dv), dv)
@@ -386,7 +386,9 @@ def main():
         world.tape_end()
         fwd_ms = max_over_ranks(fwd_ms)
         bwd_ms = max_over_ranks(bwd_ms)
+        finite = bool(np.isfinite(dv0).all() and np.isfinite(dp0).all())
         adjoint = {"value": adj_substeps * world_size / ((fwd_ms + bwd_ms) / 1e3), "unit": UNIT,
+                   "gradients_finite": finite,
                    "steps": k, "substeps": adj_substeps, "checkpoint_every": every,
                    "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                    "ratio_to_forward": (fwd_ms + bwd_ms) / fwd_ms,

@@ -213,8 +213,9 @@ typedef struct slf_param_grads {
 
 /* Starts recording the steps that follow for slf_step_backward.  checkpoint_every = k > 0: the
  * current state is the first checkpoint and the state after every k-th step is kept too (segment
- * checkpointing: the backward pass runs each segment forward again from its checkpoint, about
- * twice the forward's work, for 36 bytes per particle per checkpoint).  checkpoint_every = 0:
+ * checkpointing, 36 bytes per particle per checkpoint: the backward pass runs each segment
+ * forward again from its checkpoint, recording its substeps, which holds one segment's records
+ * at a time).  checkpoint_every = 0:
  * every substep keeps the state before it and its solver record (the rates and velocities of each
  * DFSPH iteration), about 68 + 20 x iterations bytes per particle per substep; the backward pass
  * then redoes only each substep's sort and densities.  The number of particles must not change

@@ -1370,10 +1370,11 @@ struct World {
                 return rs;
             };
 
-            // every substep was recorded as it ran: only its sort and densities are redone
-            auto recorded = [&]() -> int32_t {
-                for (size_t q = tape.subs.size(); q-- > 0;) {
-                    SubRecord& sub = *tape.subs[q];
+            // backward through recorded substeps subs[0, count): each one's sort and densities
+            // again (WCSPH: the whole substep, one pass), then its adjoint
+            auto backward_through = [&](std::vector<std::unique_ptr<SubRecord>>& subs, size_t count) -> int32_t {
+                for (size_t q = count; q-- > 0;) {
+                    SubRecord& sub = *subs[q];
                     SLF_TRY(load_state(sub.pos.p, sub.vel.p, sub.ids.p));
                     int a = 0, nid = 0;
                     if (s.solver == SLF_SOLVER_WCSPH) {
@@ -1389,45 +1390,45 @@ struct World {
                 return SLF_OK;
             };
 
-            // checkpoints: states before each substep of a segment
-            size_t most = 0;
-            for (size_t c = 0; c < tape.ckpt_step.size(); ++c) {
-                size_t b = tape.ckpt_step[c], e = c + 1 < tape.ckpt_step.size() ? tape.ckpt_step[c + 1] : tape.steps.size();
-                size_t subs = 0;
-                for (size_t t = b; t < e; ++t) subs += tape.steps[t].size();
-                most = std::max(most, subs);
-            }
-            DevBuf<float4> gpos, gvel;
-            DevBuf<uint32_t> gids;
+            // every substep was recorded as it ran
+            auto recorded = [&]() -> int32_t { return backward_through(tape.subs, tape.subs.size()); };
+
+            // checkpoints: each segment runs forward again from its checkpoint, recording its
+            // substeps (states and solver records), then backward through them
+            std::vector<std::unique_ptr<SubRecord>> segsubs;
             auto rel2 = [&] {
-                gpos.release(stream);
-                gvel.release(stream);
-                gids.release(stream);
+                for (auto& r : segsubs) r->release(stream);
+                segsubs.clear();
             };
             auto segs = [&]() -> int32_t {
-                SLF_TRY(gpos.ensure(std::max<size_t>(most, 1) * n, 0, stream));
-                SLF_TRY(gvel.ensure(std::max<size_t>(most, 1) * n, 0, stream));
-                SLF_TRY(gids.ensure(std::max<size_t>(most, 1) * n, 0, stream));
                 for (size_t c = tape.ckpt_step.size(); c-- > 0;) {
                     size_t b = tape.ckpt_step[c];
                     size_t e = c + 1 < tape.ckpt_step.size() ? tape.ckpt_step[c + 1] : tape.steps.size();
                     if (b >= e) continue;
                     std::vector<float> dts;
                     for (size_t t = b; t < e; ++t) dts.insert(dts.end(), tape.steps[t].begin(), tape.steps[t].end());
-                    // forward through the segment, keeping the state before each substep (the
-                    // last substep runs once, recorded, below)
+                    while (segsubs.size() < dts.size()) segsubs.push_back(std::make_unique<SubRecord>());
                     SLF_TRY(load_state(tape.cpos.p + c * n, tape.cvel.p + c * n, tape.cids.p + c * n));
                     for (size_t q = 0; q < dts.size(); ++q) {
-                        SLF_TRY(save_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
-                        if (q + 1 < dts.size()) SLF_TRY(substep_retrying(dts[q]));
+                        SubRecord& sub = *segsubs[q];
+                        sub.dt = dts[q];
+                        SLF_TRY(sub.pos.ensure(n, 0, stream));
+                        SLF_TRY(sub.vel.ensure(n, 0, stream));
+                        SLF_TRY(sub.ids.ensure(n, 0, stream));
+                        SLF_TRY(save_state(sub.pos.p, sub.vel.p, sub.ids.p));
+                        uint32_t held = 0, its = 0;
+                        int32_t rs;
+                        if (s.solver == SLF_SOLVER_WCSPH) {
+                            rs = wcsph_substep(dts[q], held);
+                            if (rs == kRetry) rs = wcsph_substep(dts[q], held);
+                        } else {
+                            rs = dfsph_substep(dts[q], held, its, &sub.rec);
+                            if (rs == kRetry) rs = dfsph_substep(dts[q], held, its, &sub.rec);
+                        }
+                        if (rs == kRetry) rs = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
+                        SLF_TRY(rs);
                     }
-                    // backward through it
-                    for (size_t q = dts.size(); q-- > 0;) {
-                        if (q + 1 < dts.size()) SLF_TRY(load_state(gpos.p + q * n, gvel.p + q * n, gids.p + q * n));
-                        int a = 0, nid = 0;
-                        SLF_TRY(recompute(dts[q], rec, a, nid));
-                        SLF_TRY(adjoint_substep(dts[q], a, nid, rec));
-                    }
+                    SLF_TRY(backward_through(segsubs, dts.size()));
                 }
                 return SLF_OK;
             };
