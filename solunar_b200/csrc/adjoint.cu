@@ -130,7 +130,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
                                                       const float4* __restrict__ ab, float4* __restrict__ xb,
                                                       float4* __restrict__ vb, float* __restrict__ rb,
                                                       double* __restrict__ grads, int add_rho) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     double nu_bar = 0.0, nuw_bar = 0.0, b_bar = 0.0;
     if (i < p.n) {
         const float nu = sc->viscosity, nuw = sc->wall_viscosity, m = p.mass;
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         float sbar = 0.0f, pbar = 0.0f, rbar = 0.0f;
 
         // fluid pairs: L = (a_i-bar - a_j-bar) . T(r, u, S, R)
-        walk4<FiveF>(fl, packed != 0, i,
+        walk4<FiveF>(fl, packed != 0, row,
                      [&](uint32_t j) {
                          return FiveF{__ldg(&pos[j]), __ldg(&vel[j]), __ldg(&ab[j]), __ldg(&rho[j]), __ldg(&scaled[j])};
                      },
@@ -176,11 +177,11 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         });
 
         // walls: pressure mirrored onto the wall (step.rs:197-202)
-        uint32_t nw = listed_count(wl, i);
+        uint32_t nw = listed_count(wl, row);
         float M = s_i + p_i * p.inv_rest_sq;
         float3 A = make_float3(0, 0, 0);  // sum of -grad W over walls, for the wall normal
         for (uint32_t k = 0; k < nw; ++k) {
-            uint32_t j = listed(wl, packed != 0, i, k);
+            uint32_t j = listed(wl, packed != 0, row, k);
             float3 r = xi - f3(__ldg(&walls[j]));
             float d = sqrtf(dotf(r, r));
             if (d <= 0.0f) continue;
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
             float3 I = nrm * kk;
             float3 Ibar = make_float3(0, 0, 0);
             for (uint32_t k = 0; k < nw; ++k) {
-                uint32_t j = listed(wl, packed != 0, i, k);
+                uint32_t j = listed(wl, packed != 0, row, k);
                 float3 r = xi - f3(__ldg(&walls[j]));
                 float tau = dotf(I, r);
                 if (!(tau < 0.0f)) continue;
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
             float3 Abar = (nbar - nrm * dotf(nrm, nbar)) * (1.0f / alen);
             // A = sum -r g
             for (uint32_t k = 0; k < nw; ++k) {
-                uint32_t j = listed(wl, packed != 0, i, k);
+                uint32_t j = listed(wl, packed != 0, row, k);
                 float3 r = xi - f3(__ldg(&walls[j]));
                 float d = sqrtf(dotf(r, r));
                 if (d <= 0.0f) continue;
@@ -268,12 +269,13 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
                                                         const float4* __restrict__ pos,
                                                         const float4* __restrict__ walls,
                                                         const float* __restrict__ rb, float4* __restrict__ xb) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
     float3 xi = f3(pos[i]);
     float rbi = rb[i];
     float3 xbar = make_float3(0, 0, 0);
-    walk4<float4>(fl, packed != 0, i,
+    walk4<float4>(fl, packed != 0, row,
                   [&](uint32_t j) {
                       float4 q = __ldg(&pos[j]);
                       q.w = __ldg(&rb[j]);
@@ -287,9 +289,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
                       grad_factor(p, d, g, gp);
                       xbar = xbar + r * (g * p.mass * (rbi + q.w));
                   });
-    uint32_t nw = listed_count(wl, i);
+    uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, i, k);
+        uint32_t j = listed(wl, packed != 0, row, k);
         float3 r = xi - f3(__ldg(&walls[j]));
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) continue;
@@ -345,12 +347,13 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
                                                       const float4* __restrict__ vel, float4* __restrict__ kw,
                                                       float4* __restrict__ vr, float* __restrict__ abar,
                                                       float* __restrict__ rb) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
     const float dt = sc->dt, m = p.mass;
     float3 xi = f3(pos[i]), wi = f3(w[i]);
     float acc = 0.0f;
-    walk4<Two>(fl, packed != 0, i, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&w[j])}; },
+    walk4<Two>(fl, packed != 0, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&w[j])}; },
                [&](uint32_t, const Two& q) {
                    float3 r = xi - f3(q.a);
                    float d = sqrtf(dotf(r, r));
@@ -359,9 +362,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
                    grad_factor(p, d, g, gp);
                    acc += dotf(wi - f3(q.b), r) * g;
                });
-    uint32_t nw = listed_count(wl, i);
+    uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, i, k);
+        uint32_t j = listed(wl, packed != 0, row, k);
         float3 r = xi - f3(__ldg(&walls[j]));
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) continue;
@@ -379,7 +382,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
         dphi = on ? 1.0f / dt : 0.0f;
         dphi_rho = on ? 1.0f / sc->dt_sq : 0.0f;
     } else {
-        bool on = fl.count[i] + wl.count[i] >= 20u && ri > 0.0f;
+        bool on = fl.count[row] + wl.count[row] >= 20u && ri > 0.0f;
         phi = on ? ri / dt : 0.0f;
         dphi = on ? 1.0f / dt : 0.0f;
     }
@@ -397,14 +400,15 @@ __global__ void __launch_bounds__(kBlock) k_adj_push(Params p, const StepConsts*
                                                      const float4* __restrict__ walls, const float4* __restrict__ kw,
                                                      const float4* __restrict__ vr, float4* __restrict__ wout,
                                                      float4* __restrict__ xb) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
     const float dt = sc->dt, m = p.mass;
     float4 own_w = kw[i], own_v = vr[i];
     float3 xi = f3(pos[i]), wi = f3(own_w), vi = f3(own_v);
     float ki = own_w.w, rbi = own_v.w;
     float3 vacc = make_float3(0, 0, 0), xacc = make_float3(0, 0, 0);
-    walk4<Three>(fl, packed != 0, i,
+    walk4<Three>(fl, packed != 0, row,
                  [&](uint32_t j) { return Three{__ldg(&pos[j]), __ldg(&kw[j]), __ldg(&vr[j])}; },
                  [&](uint32_t, const Three& q) {
                      float3 r = xi - f3(q.a);
@@ -418,9 +422,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_push(Params p, const StepConsts*
                      float3 c = (wi - f3(q.b)) * (-dt * m * (ki + q.b.w)) + (vi - f3(q.c)) * (m * (rbi + rbj));
                      xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
                  });
-    uint32_t nw = listed_count(wl, i);
+    uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, i, k);
+        uint32_t j = listed(wl, packed != 0, row, k);
         float3 r = xi - f3(__ldg(&walls[j]));
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) continue;
@@ -458,11 +462,12 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists f
                                                            const float4* __restrict__ walls,
                                                            const float* __restrict__ alpha,
                                                            const float* __restrict__ abar, float4* __restrict__ gt) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
     float3 xi = f3(pos[i]);
     float3 G = make_float3(0, 0, 0);
-    walk4<float4>(fl, packed != 0, i, [&](uint32_t j) { return __ldg(&pos[j]); }, [&](uint32_t, float4 q) {
+    walk4<float4>(fl, packed != 0, row, [&](uint32_t j) { return __ldg(&pos[j]); }, [&](uint32_t, float4 q) {
         float3 r = xi - f3(q);
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) return;
@@ -470,9 +475,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists f
         grad_factor(p, d, g, gp);
         G = G + r * (g * p.mass);
     });
-    uint32_t nw = listed_count(wl, i);
+    uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, i, k);
+        uint32_t j = listed(wl, packed != 0, row, k);
         float3 r = xi - f3(__ldg(&walls[j]));
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) continue;
@@ -488,7 +493,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, Pa
                                                       const float4* __restrict__ pos,
                                                       const float4* __restrict__ walls,
                                                       const float4* __restrict__ gt, float4* __restrict__ xb) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
     const float m = p.mass;
     float3 xi = f3(pos[i]);
@@ -496,7 +502,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, Pa
     float3 Gi = f3(own);
     float tbi = own.w;
     float3 xacc = make_float3(0, 0, 0);
-    walk4<Two>(fl, packed != 0, i, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&gt[j])}; },
+    walk4<Two>(fl, packed != 0, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&gt[j])}; },
                [&](uint32_t, const Two& q) {
                    float3 r = xi - f3(q.a);
                    float d = sqrtf(dotf(r, r));
@@ -508,9 +514,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, Pa
                    float3 c = (Gi + gw) * (2.0f * m * tbi) - (f3(oj) - gw) * (2.0f * m * oj.w);
                    xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
                });
-    uint32_t nw = listed_count(wl, i);
+    uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, i, k);
+        uint32_t j = listed(wl, packed != 0, row, k);
         float3 r = xi - f3(__ldg(&walls[j]));
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) continue;

@@ -79,20 +79,27 @@ struct SolveRec {
 // neighbour's index and its kernel gradient factor g = slope(d) / d (0 at d = 0), kept because
 // positions do not move within a substep (the reference keeps the whole gradient per pair for
 // the same reason, dfsph.rs:24-41); gradient = offset * g rounds as Kernel::gradient does
-// (mod.rs:158-164).  Layout: warp tiles, entry k of particle i at
-// ((i / 32) * cap + k) * 32 + i % 32, so a warp reading slot k of its 32 particles reads 256
-// contiguous bytes and each warp's lists are one contiguous block.
+// (mod.rs:158-164).  Layout: warp tiles, entry k of row s at ((s / 32) * cap + k) * 32 + s % 32,
+// so a warp reading slot k of its 32 rows reads 256 contiguous bytes and each warp's lists are
+// one contiguous block.  Rows follow the walk order: thread s of a list pass walks particle
+// order[s] (identity when order is null) and its list is row s.  The order visits the cells in 2 x 2-column bricks
+// (world.cpp builds it after each sort), so a block's 256 particles span about 2 x 2 x 8 cells and
+// their neighbourhoods overlap in the L1; particle arrays stay in the reference's sorted order.
 struct PairLists {
-    uint32_t cap;          // slots per particle
+    uint32_t cap;          // slots per row
     uint2* e;              // entries {index, g bits}
-    uint32_t* count;       // neighbours found per particle; above cap the lists are incomplete
+    uint32_t* count;       // neighbours found per row; above cap the lists are incomplete
+    const uint32_t* order; // particle of each row (null: row = particle)
 
     __host__ __device__ static size_t slots_for(uint32_t n, uint32_t cap) {
         return size_t((n + 31u) / 32u) * cap * 32u;
     }
-    __host__ __device__ size_t at(uint32_t i, uint32_t k) const {
-        return (size_t(i >> 5) * cap + k) * 32u + (i & 31u);
+    __host__ __device__ size_t at(uint32_t row, uint32_t k) const {
+        return (size_t(row >> 5) * cap + k) * 32u + (row & 31u);
     }
+#ifdef __CUDACC__
+    __device__ __forceinline__ uint32_t particle(uint32_t row) const { return order ? __ldg(&order[row]) : row; }
+#endif
 };
 
 // Slots of the adjoint's FP64 parameter-gradient accumulators.

@@ -229,7 +229,8 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
                                                     const float4* __restrict__ walls, PairLists fl, PairLists wl,
                                                     float* __restrict__ rho, float* __restrict__ press,
                                                     float* __restrict__ scaled, float* __restrict__ alpha, Status* st) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     bool valid = i < p.n;
     uint32_t compressed = 0, longest = 0;
     if (valid) {
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             sum += kernel_value(p, d);
             float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
-            if (nf < fl.cap) fl.e[fl.at(i, nf)] = make_uint2(j, __float_as_uint(g));
+            if (nf < fl.cap) fl.e[fl.at(row, nf)] = make_uint2(j, __float_as_uint(g));
             ++nf;
             if (SOLVER == 1) {
                 // gradient(at - other) (dfsph.rs:118), then factors (dfsph.rs:149-153)
@@ -260,7 +261,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             wsum += kernel_value(p, d);
             float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
-            if (nw < wl.cap) wl.e[wl.at(i, nw)] = make_uint2(j, __float_as_uint(g));
+            if (nw < wl.cap) wl.e[wl.at(row, nw)] = make_uint2(j, __float_as_uint(g));
             ++nw;
             if (SOLVER == 1) {
                 float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
@@ -269,8 +270,8 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
                 sz = sz + (rz * g) * p.mass;
             }
         });
-        fl.count[i] = nf;
-        wl.count[i] = nw;
+        fl.count[row] = nf;
+        wl.count[row] = nw;
         longest = nf > nw ? nf : nw;
         float density = p.mass * (sum + wsum);
         rho[i] = density;
@@ -388,11 +389,11 @@ __device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, con
 // ---- wall viscosity (step.rs:262-301, no terrains) ---------------------------------------
 
 __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc, const PairLists& wl,
-                                               const float4* __restrict__ walls, uint32_t i, float4 a, float4 v,
+                                               const float4* __restrict__ walls, uint32_t row, float4 a, float4 v,
                                                float density) {
-    if (wl.count[i] == 0) return make_float3(0.0f, 0.0f, 0.0f);
+    if (wl.count[row] == 0) return make_float3(0.0f, 0.0f, 0.0f);
     float awx = 0.0f, awy = 0.0f, awz = 0.0f;
-    each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
+    each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         awx = awx + -(rx * g);
         awy = awy + -(ry * g);
@@ -409,7 +410,7 @@ __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc,
     float k = fminf(dot3(v.x, v.y, v.z, nx, ny, nz), 0.0f);
     float ix = nx * k, iy = ny * k, iz = nz * k;
     float px = 0.0f, py = 0.0f, pz = 0.0f;
-    each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
+    each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float toward = dot3(ix, iy, iz, rx, ry, rz);
         if (toward < 0.0f) {
@@ -462,7 +463,8 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
                                                         const float4* __restrict__ walls, float4* __restrict__ pos_out,
                                                         float4* __restrict__ vel_out, Status* st,
                                                         float4* __restrict__ vel_pre) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     bool valid = i < p.n;
     int3 nc = make_int3(0, 0, 0);
     float speed = 0.0f;
@@ -475,7 +477,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
         float density = rho[i];
         float own = scaled[i];
         float px = 0.0f, py = 0.0f, pz = 0.0f;
-        each_listed2(fl, i, pos, vel, [&](uint32_t j, float g, float4 q, float4 w) {
+        each_listed2(fl, row, pos, vel, [&](uint32_t j, float g, float4 q, float4 w) {
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
             float squared = dot3(rx, ry, rz, rx, ry, rz);
             if (squared <= 0.0f) return;
@@ -489,14 +491,14 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
             pz = pz - gz * s;
         });
         float mirrored = own + press[i] / p.rest_sq;
-        each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
+        each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
             float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
             float s = p.mass * mirrored;
             px = px - (rx * g) * s;
             py = py - (ry * g) * s;
             pz = pz - (rz * g) * s;
         });
-        float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, i, a, v, density);
+        float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, row, a, v, density);
         float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
         v.x = v.x + ax * dt;
         v.y = v.y + ay * dt;
@@ -524,7 +526,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
 // particle i, its neighbours taken from src.
 template <int WHICH, class Src>
 __device__ __forceinline__ void rate_particle(const Params& p, const StepConsts* __restrict__ sc,
-                                              const PairLists& fl, const PairLists& wl, uint32_t i, const Src& src,
+                                              const PairLists& fl, const PairLists& wl, uint32_t i, uint32_t row, const Src& src,
                                               const float4* __restrict__ pos, const float4* __restrict__ vel,
                                               const float* __restrict__ rho, const float* __restrict__ alpha,
                                               const float4* __restrict__ walls, float* __restrict__ kappa_w,
@@ -533,11 +535,11 @@ __device__ __forceinline__ void rate_particle(const Params& p, const StepConsts*
     float4 a = pos[i];
     float4 v = vel[i];
     float rate = 0.0f;
-    each_listed2_from(fl, i, src, [&](uint32_t, float g, float4 q, float4 w) {
+    each_listed2_from(fl, row, src, [&](uint32_t, float g, float4 q, float4 w) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx * g, ry * g, rz * g);
     });
-    each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
+    each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
     });
@@ -553,7 +555,7 @@ __device__ __forceinline__ void rate_particle(const Params& p, const StepConsts*
         target = over / sc->dt_sq;
         error = over / p.rest;
     } else {
-        float r = fl.count[i] + wl.count[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
+        float r = fl.count[row] + wl.count[row] < 20u ? 0.0f : fmaxf(rate, 0.0f);
         target = r / dt;
         error = dt * r / p.rest;
     }
@@ -575,13 +577,14 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, 
                                                  SolveRec rec) {
     // a solve that already stopped leaves the rest of its batch of launches idle
     if (__ldcg(&st->settled)) return;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     double err = 0.0;
     uint32_t loaded = 0;
     // every block reads the count before the last block advances it
     const uint32_t slot = rec.rate ? __ldcg(&st->iterations) : 0u;
     if (i < p.n)
-        rate_particle<WHICH>(p, sc, fl, wl, i, FromGlobal{pos, vel}, pos, vel, rho, alpha, walls, kappa_w, rec, slot,
+        rate_particle<WHICH>(p, sc, fl, wl, i, row, FromGlobal{pos, vel}, pos, vel, rho, alpha, walls, kappa_w, rec, slot,
                              err, loaded);
     residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
 }
@@ -590,21 +593,21 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, 
 // stiffness, which the rate pass left in the w lane of each position.
 template <class Src>
 __device__ __forceinline__ void push_particle(const Params& p, const StepConsts* __restrict__ sc, const PairLists& fl,
-                                              const PairLists& wl, uint32_t i, const Src& src,
+                                              const PairLists& wl, uint32_t i, uint32_t row, const Src& src,
                                               const float4* __restrict__ pos, float4* __restrict__ vel,
                                               const float4* __restrict__ walls) {
     const float dt = sc->dt;
     float4 a = pos[i];
     float own = a.w;
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    each_listed_from(fl, i, src, [&](uint32_t, float g, float4 q) {
+    each_listed_from(fl, row, src, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float s = p.mass * (own + q.w);
         cx = cx - (rx * g) * s;
         cy = cy - (ry * g) * s;
         cz = cz - (rz * g) * s;
     });
-    each_listed(wl, i, walls, [&](uint32_t, float g, float4 q) {
+    each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float s = p.mass * own;
         cx = cx - (rx * g) * s;
@@ -623,9 +626,10 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_push(Params p, 
                                                  float4* __restrict__ vel, const float4* __restrict__ walls,
                                                  const Status* st) {
     if (__ldcg(&st->settled)) return;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
-    push_particle(p, sc, fl, wl, i, FromGlobal{pos, nullptr}, pos, vel, walls);
+    push_particle(p, sc, fl, wl, i, row, FromGlobal{pos, nullptr}, pos, vel, walls);
 }
 
 // viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
@@ -634,7 +638,8 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params 
                                                     PairLists wl, const float4* __restrict__ pos,
                                                     const float4* __restrict__ vel, const float* __restrict__ rho,
                                                     const float4* __restrict__ walls, float4* __restrict__ vel_out) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
     const float dt = sc->dt;
     const float visc = sc->viscosity;
@@ -642,7 +647,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params 
     float4 v = vel[i];
     float density = rho[i];
     float px = 0.0f, py = 0.0f, pz = 0.0f;
-    each_listed2(fl, i, pos, vel, [&](uint32_t j, float g, float4 q, float4 w) {
+    each_listed2(fl, row, pos, vel, [&](uint32_t j, float g, float4 q, float4 w) {
         if (j == i) return;
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float toward = dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx, ry, rz);
@@ -655,7 +660,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params 
             pz = pz - (rz * g) * s;
         }
     });
-    float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, i, a, v, density);
+    float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, row, a, v, density);
     float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
     v.x = v.x + ax * dt;
     v.y = v.y + ay * dt;
@@ -711,6 +716,34 @@ __global__ void k_list_fill(Params p, GridDev g, const float4* __restrict__ pos,
     int3 cell = cell_of(p, a.x, a.y, a.z);
     uint32_t k = start[i];
     each_near(p, g, pts, cell, a.x, a.y, a.z, [&](uint32_t j, float4) { items[k++] = j; });
+}
+
+// ---- the walk order of the list passes (PairLists::order) -------------------------------------
+// Cells taken in 2 x 2-column bricks: key = ((x / 2, y / 2), z, x % 2, y % 2) over the dense box,
+// so 256 consecutive rows cover about 2 x 2 x 8 cells instead of a 1 x 1 x 32 column.
+
+__device__ __forceinline__ uint32_t brick_key(uint32_t lin, int3 span) {
+    uint32_t z = lin % (uint32_t)span.z, xy = lin / (uint32_t)span.z;
+    uint32_t y = xy % (uint32_t)span.y, x = xy / (uint32_t)span.y;
+    uint32_t by = ((uint32_t)span.y + 1u) / 2u;
+    return (((x >> 1) * by + (y >> 1)) * (uint32_t)span.z + z) * 4u + (x & 1u) * 2u + (y & 1u);
+}
+
+// bcount[key(cell)] = members of the cell (bcount cleared beforehand: keys of the padding stay 0)
+__global__ void k_brick_count(uint32_t volume, int3 span, const uint32_t* __restrict__ start,
+                              uint32_t* __restrict__ bcount) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= volume) return;
+    bcount[brick_key(c, span)] = start[c + 1] - start[c];
+}
+
+// each cell's members, contiguous in the sorted arrays, go to the rows its key's scan names
+__global__ void k_brick_fill(uint32_t volume, int3 span, const uint32_t* __restrict__ start,
+                             const uint32_t* __restrict__ bstart, uint32_t* __restrict__ order) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= volume) return;
+    uint32_t b = start[c], e = start[c + 1], r = bstart[brick_key(c, span)];
+    for (uint32_t m = b; m < e; ++m) order[r + (m - b)] = m;
 }
 
 // ---- domain (mod.rs:451-486): keep flags, then a stable compaction -------------------------
@@ -864,6 +897,20 @@ void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLis
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                  float4* vel, const float4* walls, const Status* st, cudaStream_t s) {
     if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st);
+}
+
+size_t walk_order_keys(int3 span) {
+    return size_t((span.x + 1) / 2) * size_t((span.y + 1) / 2) * size_t(span.z) * 4u;
+}
+
+void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32_t* bcount, uint32_t* tile_sums,
+                       uint32_t* order, cudaStream_t s) {
+    if (!volume) return;
+    size_t keys = walk_order_keys(span);
+    cudaMemsetAsync(bcount, 0, (keys + 1) * sizeof(uint32_t), s);
+    k_brick_count<<<blocks_for(volume), kBlock, 0, s>>>(volume, span, start, bcount);
+    launch_exclusive_scan(bcount, uint32_t(keys), tile_sums, s);
+    k_brick_fill<<<blocks_for(volume), kBlock, 0, s>>>(volume, span, start, bcount, order);
 }
 
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,

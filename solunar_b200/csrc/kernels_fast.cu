@@ -171,7 +171,8 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
                                                          float* __restrict__ press, float* __restrict__ scaled,
                                                          float* __restrict__ alpha, Status* st) {
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fpl.particle(row) : row;  // row of the walk order, its particle
     bool valid = i < p.n;
     uint32_t compressed = 0, longest = 0;
     if (valid) {
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
         auto fluid = [&](uint32_t j, int dx, int dy, int dz, float rx, float ry, float rz) {
             float l2 = fl2(rx, ry, rz);
             sum += fast_value(p, l2);
-            if (nf < fl.cap) fl.idx[fl.at(i, nf)] = encode_entry(j, dx, dy, dz);
+            if (nf < fl.cap) fl.idx[fl.at(row, nf)] = encode_entry(j, dx, dy, dz);
             ++nf;
             if (SOLVER == 1) {
                 float g = fast_factor(p, l2) * p.mass;
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
         auto wall = [&](uint32_t j, int dx, int dy, int dz, float rx, float ry, float rz) {
             float l2 = fl2(rx, ry, rz);
             wsum += fast_value(p, l2);
-            if (nw < wl.cap) wl.idx[wl.at(i, nw)] = encode_entry(j, dx, dy, dz);
+            if (nw < wl.cap) wl.idx[wl.at(row, nw)] = encode_entry(j, dx, dy, dz);
             ++nw;
             if (SOLVER == 1) {
                 float g = fast_factor(p, l2) * p.mass;
@@ -223,8 +224,8 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
             each_near(p, wg, walls, cell, a.x, a.y, a.z,
                       [&](uint32_t j, float4 q) { wall(j, 0, 0, 0, a.x - q.x, a.y - q.y, a.z - q.z); });
         }
-        fl.count[i] = nf;
-        wl.count[i] = nw;
+        fl.count[row] = nf;
+        wl.count[row] = nw;
         longest = nf > nw ? nf : nw;
         float density = p.mass * (sum + wsum);
         rho[i] = density;
@@ -253,11 +254,11 @@ __global__ void __launch_bounds__(kBlock) k_density_fast(Params p, GridDev fg, G
 
 template <bool REL>
 __device__ __forceinline__ float3 wall_viscous_fast(const Params& p, float wall_visc, const IndexLists& wl,
-                                                    const float4* __restrict__ walls, uint32_t i, float4 a,
+                                                    const float4* __restrict__ walls, uint32_t row, float4 a,
                                                     float4 v, float density) {
-    if (wl.count[i] == 0) return make_float3(0.0f, 0.0f, 0.0f);
+    if (wl.count[row] == 0) return make_float3(0.0f, 0.0f, 0.0f);
     float awx = 0.0f, awy = 0.0f, awz = 0.0f;
-    each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+    each_index(wl, row, walls, [&](uint32_t e, float4 q) {
         float3 r = pair_offset<REL>(p, a, q, e);
         float g = fast_factor(p, fl2(r.x, r.y, r.z));
         awx = fmaf(-r.x, g, awx);
@@ -276,7 +277,7 @@ __device__ __forceinline__ float3 wall_viscous_fast(const Params& p, float wall_
     float ix = nx * k, iy = ny * k, iz = nz * k;
     float px = 0.0f, py = 0.0f, pz = 0.0f;
     float c = -wall_visc * p.mass / density;
-    each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+    each_index(wl, row, walls, [&](uint32_t e, float4 q) {
         float3 r = pair_offset<REL>(p, a, q, e);
         float toward = fmaf(ix, r.x, fmaf(iy, r.y, iz * r.z));
         if (toward < 0.0f) {
@@ -431,7 +432,8 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_fast(Params p, const Ste
                                                              float4* __restrict__ vel_out, Status* st,
                                                              float4* __restrict__ vel_pre) {
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fpl.particle(row) : row;  // row of the walk order, its particle
     bool valid = i < p.n;
     int3 nc = make_int3(0, 0, 0);
     float speed = 0.0f;
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_fast(Params p, const Ste
         float density = rho[i];
         float own = scaled[i];
         float px = 0.0f, py = 0.0f, pz = 0.0f;
-        each_index2(fl, i, pos, vel, [&](uint32_t e, float4 q, float4 w) {
+        each_index2(fl, row, pos, vel, [&](uint32_t e, float4 q, float4 w) {
             float3 r = pair_offset<REL>(p, a, q, e);
             float squared = fl2(r.x, r.y, r.z);
             if (squared <= 0.0f) return;
@@ -457,14 +459,14 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_fast(Params p, const Ste
             pz = fmaf(-r.z, s, pz);
         });
         float mirrored = p.mass * (own + press[i] * p.inv_rest_sq);
-        each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+        each_index(wl, row, walls, [&](uint32_t e, float4 q) {
             float3 r = pair_offset<REL>(p, a, q, e);
             float s = fast_factor(p, fl2(r.x, r.y, r.z)) * mirrored;
             px = fmaf(-r.x, s, px);
             py = fmaf(-r.y, s, py);
             pz = fmaf(-r.z, s, pz);
         });
-        float3 wv = wall_viscous_fast<REL>(p, sc->wall_viscosity, wl, walls, i, a, v, density);
+        float3 wv = wall_viscous_fast<REL>(p, sc->wall_viscosity, wl, walls, row, a, v, density);
         v.x = fmaf(px + wv.x + p.gravity.x, dt, v.x);
         v.y = fmaf(py + wv.y + p.gravity.y, dt, v.y);
         v.z = fmaf(pz + wv.z + p.gravity.z, dt, v.z);
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_fast(Params p, const Ste
 
 template <int WHICH, bool REL, class Src>
 __device__ __forceinline__ void rate_particle_fast(const Params& p, const StepConsts* __restrict__ sc,
-                                                   const IndexLists& fl, const IndexLists& wl, uint32_t i,
+                                                   const IndexLists& fl, const IndexLists& wl, uint32_t i, uint32_t row,
                                                    const Src& src, const float4* __restrict__ pos,
                                                    const float4* __restrict__ vel, const float* __restrict__ rho,
                                                    const float* __restrict__ alpha,
@@ -501,12 +503,12 @@ __device__ __forceinline__ void rate_particle_fast(const Params& p, const StepCo
     float4 a = pos[i];
     float4 v = vel[i];
     float rate = 0.0f;
-    each_index2_from(fl, i, src, [&](uint32_t e, float4 q, float4 w) {
+    each_index2_from(fl, row, src, [&](uint32_t e, float4 q, float4 w) {
         float3 r = pair_offset<REL>(p, a, q, e);
         float g = fast_factor(p, fl2(r.x, r.y, r.z));
         rate = fmaf(g, fmaf(v.x - w.x, r.x, fmaf(v.y - w.y, r.y, (v.z - w.z) * r.z)), rate);
     });
-    each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+    each_index(wl, row, walls, [&](uint32_t e, float4 q) {
         float3 r = pair_offset<REL>(p, a, q, e);
         float g = fast_factor(p, fl2(r.x, r.y, r.z));
         rate = fmaf(g, fmaf(v.x, r.x, fmaf(v.y, r.y, v.z * r.z)), rate);
@@ -523,7 +525,7 @@ __device__ __forceinline__ void rate_particle_fast(const Params& p, const StepCo
         target = over / sc->dt_sq;
         error = over * p.inv_rest;
     } else {
-        float r = fl.count[i] + wl.count[i] < 20u ? 0.0f : fmaxf(rate, 0.0f);
+        float r = fl.count[row] + wl.count[row] < 20u ? 0.0f : fmaxf(rate, 0.0f);
         target = r / dt;
         error = dt * r * p.inv_rest;
     }
@@ -545,32 +547,33 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
     if (__ldcg(&st->settled)) return;
     const uint32_t slot = rec.rate ? __ldcg(&st->iterations) : 0u;
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fpl.particle(row) : row;  // row of the walk order, its particle
     double err = 0.0;
     uint32_t loaded = 0;
     if (i < p.n)
-        rate_particle_fast<WHICH, REL>(p, sc, fl, wl, i, FromGlobalF{pos, vel}, pos, vel, rho, alpha, walls, kappa,
+        rate_particle_fast<WHICH, REL>(p, sc, fl, wl, i, row, FromGlobalF{pos, vel}, pos, vel, rho, alpha, walls, kappa,
                                        rec, slot, err, loaded);
     residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
 }
 
 template <bool REL, class Src>
 __device__ __forceinline__ void push_particle_fast(const Params& p, const StepConsts* __restrict__ sc,
-                                                   const IndexLists& fl, const IndexLists& wl, uint32_t i,
+                                                   const IndexLists& fl, const IndexLists& wl, uint32_t i, uint32_t row,
                                                    const Src& src, const float4* __restrict__ pos,
                                                    float4* __restrict__ vel, const float4* __restrict__ walls) {
     const float mdt = p.mass * sc->dt;
     float4 a = pos[i];
     float own = a.w;
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    each_index_from(fl, i, src, [&](uint32_t e, float4 q) {
+    each_index_from(fl, row, src, [&](uint32_t e, float4 q) {
         float3 r = pair_offset<REL>(p, a, q, e);
         float s = fast_factor(p, fl2(r.x, r.y, r.z)) * (own + q.w);
         cx = fmaf(-r.x, s, cx);
         cy = fmaf(-r.y, s, cy);
         cz = fmaf(-r.z, s, cz);
     });
-    each_index(wl, i, walls, [&](uint32_t e, float4 q) {
+    each_index(wl, row, walls, [&](uint32_t e, float4 q) {
         float3 r = pair_offset<REL>(p, a, q, e);
         float s = fast_factor(p, fl2(r.x, r.y, r.z)) * own;
         cx = fmaf(-r.x, s, cx);
@@ -591,9 +594,10 @@ __global__ void __launch_bounds__(kBlock) k_push_fast(Params p, const StepConsts
                                                       const Status* st) {
     if (__ldcg(&st->settled)) return;
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fpl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
-    push_particle_fast<REL>(p, sc, fl, wl, i, FromGlobalF{pos, nullptr}, pos, vel, walls);
+    push_particle_fast<REL>(p, sc, fl, wl, i, row, FromGlobalF{pos, nullptr}, pos, vel, walls);
 }
 
 template <bool REL>
@@ -605,7 +609,8 @@ __global__ void __launch_bounds__(kBlock) k_viscous_fast(Params p, const StepCon
                                                          const float4* __restrict__ walls,
                                                          float4* __restrict__ vel_out) {
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = row < p.n ? fpl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
     const float dt = sc->dt;
     const float visc2 = -2.0f * sc->viscosity * p.mass;
@@ -613,7 +618,7 @@ __global__ void __launch_bounds__(kBlock) k_viscous_fast(Params p, const StepCon
     float4 v = vel[i];
     float density = rho[i];
     float px = 0.0f, py = 0.0f, pz = 0.0f;
-    each_index2(fl, i, pos, vel, [&](uint32_t e, float4 q, float4 w) {
+    each_index2(fl, row, pos, vel, [&](uint32_t e, float4 q, float4 w) {
         uint32_t j = e & kIndexMask;
         if (j == i) return;
         float3 r = pair_offset<REL>(p, a, q, e);
@@ -626,7 +631,7 @@ __global__ void __launch_bounds__(kBlock) k_viscous_fast(Params p, const StepCon
             pz = fmaf(-r.z, s, pz);
         }
     });
-    float3 wv = wall_viscous_fast<REL>(p, sc->wall_viscosity, wl, walls, i, a, v, density);
+    float3 wv = wall_viscous_fast<REL>(p, sc->wall_viscosity, wl, walls, row, a, v, density);
     v.x = fmaf(px + wv.x + p.gravity.x, dt, v.x);
     v.y = fmaf(py + wv.y + p.gravity.y, dt, v.y);
     v.z = fmaf(pz + wv.z + p.gravity.z, dt, v.z);

@@ -29,6 +29,13 @@ void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start,
                          int4* cells_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
                          cudaStream_t s);
 
+// The list passes' walk order (PairLists::order) over the dense cell box `span` of a sort:
+// start is the sort's cell table (volume + 1), bcount holds walk_order_keys(span) + 1 words,
+// tile_sums scan_tiles(walk_order_keys(span)) + 1, order n.
+size_t walk_order_keys(int3 span);
+void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32_t* bcount, uint32_t* tile_sums,
+                       uint32_t* order, cudaStream_t s);
+
 // pair passes: the density pass builds the substep's neighbour lists, the others walk them
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,

@@ -191,6 +191,7 @@ constexpr double count_cells = 20, scan = 2, scatter = 8, reorder = 44;
 constexpr double density_wcsph = 16, density_dfsph = 20, wcsph_force = 52;
 constexpr double rate_divergence = 32, rate_density = 36, push = 40, viscosity = 40, advance = 48;
 constexpr double stats = 24;
+constexpr double walk_order = 4;  // one row index written a particle
 }  // namespace bytes_per_particle
 
 }  // namespace
@@ -219,8 +220,10 @@ struct World {
     DevBuf<uint8_t> partials;
     bool stats_fresh = false;  // status holds bbox and speed of the committed state
 
-    // fluid cell table of the last sort
+    // fluid cell table of the last sort, and the list passes' walk order over it
     GridDev fgrid{};
+    DevBuf<uint32_t> worder, wkeys, wsums;
+    bool worder_valid = false;
     int lists_pos = -1;  // slot of the positions the last sort produced
     uint64_t lists_n = 0;
     bool lists_valid = false;
@@ -314,7 +317,8 @@ struct World {
     ~World() {
         if (stream) {
             for (auto* b : {&pos[0], &pos[1], &pos[2], &vel[0], &vel[1], &vel[2]}) b->release(stream);
-            for (auto* b : {&ids[0], &ids[1], &lin, &cslot, &members, &count, &tiles, &keep, &dwstart, &fcnt, &wcnt})
+            for (auto* b : {&ids[0], &ids[1], &lin, &cslot, &members, &count, &tiles, &keep, &dwstart, &fcnt, &wcnt,
+                            &worder, &wkeys, &wsums})
                 b->release(stream);
             for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha}) b->release(stream);
             for (auto* b : {&cell[0], &cell[1], &cell[2]}) b->release(stream);
@@ -600,8 +604,9 @@ struct World {
             launch_viscous(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
     }
 
-    PairLists fluid_lists() const { return PairLists{list_cap, fent.p, fcnt.p}; }
-    PairLists wall_lists() const { return PairLists{list_cap, went.p, wcnt.p}; }
+    const uint32_t* walk_order() const { return worder_valid ? worder.p : nullptr; }
+    PairLists fluid_lists() const { return PairLists{list_cap, fent.p, fcnt.p, walk_order()}; }
+    PairLists wall_lists() const { return PairLists{list_cap, went.p, wcnt.p, walk_order()}; }
 
     // After a density pass: a list longer than its room leaves the substep to be run again.
     static constexpr int32_t kRetry = -1;
@@ -920,6 +925,17 @@ struct World {
                                 cells_of(to),
                                 job_lo, job_hi, d_status, sort_dest, stream);
         });
+        // the walk order of this sort's lists (identity where its key space would not fit 32 bits)
+        worder_valid = false;
+        size_t keys = walk_order_keys(sp3);
+        if (keys < (size_t(1) << 31)) {
+            SLF_TRY(worder.ensure(n, 0, stream));
+            SLF_TRY(wkeys.ensure(keys + 1, 0, stream));
+            SLF_TRY(wsums.ensure(scan_tiles(uint32_t(keys)) + 1, 0, stream));
+            timed("walk_order", bytes_per_particle::walk_order,
+                  [&] { launch_walk_order(volume, sp3, count.p, wkeys.p, wsums.p, worder.p, stream); });
+            worder_valid = true;
+        }
         fgrid = GridDev{};
         fgrid.mode = 1;
         fgrid.lx = lo3.x;
