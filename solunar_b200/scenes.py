@@ -144,8 +144,8 @@ def dfsph_precision_1m() -> Scene:
 
 
 def dfsph_precision_far(counts=(100, 100, 100), origin=(1024.0, 1024.0, 1024.0)) -> Scene:
-    """The precision study's block moved far from the origin, where an f32 coordinate keeps only
-    about 1/160 of the spacing: no container, no gravity, velocities N(0, 0.05 m/s)."""
+    """The precision study's block moved far from the origin, where an f32 coordinate resolves
+    1.2e-4 m, about 1/80 of the spacing: no container, no gravity, velocities N(0, 0.05 m/s)."""
     s = FluidSettings(solver=FluidSolver.DFSPH, spacing=0.01, support=2.0, gravity=(0.0, 0.0, 0.0))
     return Scene("dfsph_precision_far", s, (4.0, 2.0, 2.0), counts, jitter=1e-5, velocity_sigma=0.05, dt=1e-3,
                  steps=300, origin=origin, container=False)
