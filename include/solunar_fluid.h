@@ -149,6 +149,16 @@ int32_t slf_add_wall(slf_world* world, const float low[3], const float high[3],
 /* FluidWorld::remove_boundary (boundary.rs:94-115).  *removed = 0 for an unknown id. */
 int32_t slf_remove_boundary(slf_world* world, uint32_t boundary, int32_t* removed);
 
+/* FluidWorld::add_emitter (flow.rs:86-99): after each step every lattice slot of the box with
+ * no water within 0.9 spacing of its centre gets a particle moving at `velocity`.  Boxes of more
+ * than 2^30 slots are refused when the step runs them (SLF_ERR_OUT_OF_RANGE). */
+int32_t slf_add_emitter(slf_world* world, const float low[3], const float high[3], const float velocity[3],
+                        uint32_t* flow_out);
+/* FluidWorld::add_drain (flow.rs:104-106): after each step the water in the box is taken out. */
+int32_t slf_add_drain(slf_world* world, const float low[3], const float high[3], uint32_t* flow_out);
+/* FluidWorld::remove_flow (flow.rs:109-113): *removed = 0 for an id that is not there. */
+int32_t slf_remove_flow(slf_world* world, uint32_t flow, int32_t* removed);
+
 /* FluidWorld::wall_positions (boundary.rs:118-120): count, then xyz triples in wall order. */
 int32_t slf_wall_count(const slf_world* world, uint64_t* out);
 int32_t slf_read_wall_positions(const slf_world* world, float* out, uint64_t n);

@@ -19,6 +19,8 @@
 //   src/fluid/boundary.rs add_box_container :41-68, add_wall :74-91, remove_boundary :94-115,
 //                         cells_in :123-126, check_room :128-137, settle_walls :155-178,
 //                         check_box :230-238, union :240-247
+//   src/fluid/flow.rs     CLEAR_SHARE :7, add_emitter :86-99, add_drain :104-106,
+//                         remove_flow :109-113, add_flow :115-139, run_flows :144-231
 //   src/snapshot/bytes.rs fnv1a :6-13
 //
 // Arithmetic follows the reference's scalar code: left-to-right evaluation, no fused
@@ -30,8 +32,8 @@
 // length.  Parity with the Rust binary itself is therefore unpinned at the bit level; the
 // reference's own tests (property tests, no stored vectors) pin this restatement instead.
 //
-// Movers (rigid coupling), terrain, emitters and drains are not on the path: they are absent
-// from this restatement, as they are empty in every configuration it is run on.
+// Movers (rigid coupling) and terrain are not on the path: they are absent from this
+// restatement, as they are empty in every configuration it is run on.
 #pragma once
 
 #include <algorithm>
@@ -362,6 +364,15 @@ template <class R> class World {
     Walls<R> walls;
     bool has_domain = false;
     Vec domain_low, domain_high;
+    // emitters and drains (flow.rs:14-33), in the order they were added
+    struct Flow {
+        uint32_t id;
+        Vec low, high;
+        bool emitter;
+        Vec velocity;
+    };
+    std::vector<Flow> flows;
+    uint32_t flow_next = 0;
     // per-pair gradient caches of the last DFSPH substep (dfsph.rs:24-41)
     std::vector<Vec> grad_fluid, grad_walls;
     // solver iteration counts of the last DFSPH substep: divergence, density
@@ -444,6 +455,126 @@ template <class R> class World {
         velocities.resize(kept);
         densities.resize(kept);
         return lost;
+    }
+
+    // flow.rs:115-139
+    Status add_flow(Vec low, Vec high, bool emitter, Vec velocity, uint32_t* id_out) {
+        if (!is_finite(low) || !is_finite(high)) return NON_FINITE;
+        if (high.x <= low.x || high.y <= low.y || high.z <= low.z) return OUT_OF_RANGE;
+        if (flow_next == UINT32_MAX) return FLUID_FULL;
+        uint32_t id = flow_next++;
+        flows.push_back(Flow{id, low, high, emitter, velocity});
+        if (id_out) *id_out = id;
+        return OK;
+    }
+
+    // flow.rs:86-99, 104-106
+    Status add_emitter(Vec low, Vec high, Vec velocity, uint32_t* id_out) {
+        if (!is_finite(velocity)) return NON_FINITE;
+        return add_flow(low, high, true, velocity, id_out);
+    }
+    Status add_drain(Vec low, Vec high, uint32_t* id_out) { return add_flow(low, high, false, Vec(), id_out); }
+
+    // flow.rs:109-113
+    bool remove_flow(uint32_t id) {
+        size_t before = flows.size();
+        flows.erase(std::remove_if(flows.begin(), flows.end(), [&](const Flow& f) { return f.id == id; }),
+                    flows.end());
+        return flows.size() != before;
+    }
+
+    // mod.rs:468-486
+    void keep_only(const std::vector<char>& keep) {
+        size_t kept = 0;
+        for (size_t i = 0; i < len(); ++i)
+            if (keep[i]) {
+                ids[kept] = ids[i];
+                positions[kept] = positions[i];
+                velocities[kept] = velocities[i];
+                densities[kept] = densities[i];
+                ++kept;
+            }
+        ids.resize(kept);
+        positions.resize(kept);
+        velocities.resize(kept);
+        densities.resize(kept);
+    }
+
+    // Rust's `f as i64`: saturating, NaN to 0
+    static int64_t as_i64(R v) {
+        if (std::isnan(v)) return 0;
+        if (v >= R(9.2233720368547758e18)) return INT64_MAX;
+        if (v <= R(-9.2233720368547758e18)) return INT64_MIN;
+        return int64_t(v);
+    }
+
+    // Largest emitter lattice restated here: the reference allocates one flag per slot
+    // (flow.rs:185) for up to 4096^3 slots; larger boxes are refused.
+    static constexpr int64_t kMaxEmitterSlots = int64_t(1) << 30;
+
+    // flow.rs:144-231: drains first, then emitters, each in the order they were added
+    Status run_flows(uint32_t& emitted, uint32_t& drained) {
+        emitted = drained = 0;
+        if (flows.empty()) return OK;
+        std::vector<Flow> list = flows;
+        for (const Flow& flow : list) {
+            if (flow.emitter) continue;
+            std::vector<char> keep(len());
+            size_t gone = 0;
+            for (size_t i = 0; i < len(); ++i) {
+                const Vec& at = positions[i];
+                bool inside = at.x >= flow.low.x && at.y >= flow.low.y && at.z >= flow.low.z &&
+                              at.x <= flow.high.x && at.y <= flow.high.y && at.z <= flow.high.z;
+                keep[i] = !inside;
+                gone += inside ? 1 : 0;
+            }
+            if (gone > 0) {
+                drained += uint32_t(gone);
+                keep_only(keep);
+            }
+        }
+        const R spacing = R(settings.spacing);
+        for (const Flow& flow : list) {
+            if (!flow.emitter) continue;
+            Vec size = flow.high - flow.low;
+            auto count = [&](R extent) -> int64_t {
+                int64_t c = as_i64(std::floor(extent / spacing));
+                return std::min<int64_t>(std::max<int64_t>(c, 0), int64_t(1) << 12);
+            };
+            int64_t cx = count(size.x), cy = count(size.y), cz = count(size.z);
+            int64_t total = cx * cy * cz;
+            if (total == 0) continue;
+            if (total > kMaxEmitterSlots) return OUT_OF_RANGE;
+            R share = R(0.9f) * spacing;
+            R clear = share * share;
+            std::vector<char> taken(size_t(total), 0);
+            for (const Vec& at : positions) {
+                Vec local = (at - flow.low) / spacing - Vec::splat(R(0.5));
+                // a slot index outside [-1, cells] reaches no slot; clamping keeps the loops finite
+                auto nearest = [](R v, int64_t cells) {
+                    int64_t c = as_i64(std::round(v));
+                    return std::min<int64_t>(std::max<int64_t>(c, -2), cells + 1);
+                };
+                int64_t nx = nearest(local.x, cx), ny = nearest(local.y, cy), nz = nearest(local.z, cz);
+                for (int64_t y = ny - 1; y <= ny + 1; ++y)
+                    for (int64_t z = nz - 1; z <= nz + 1; ++z)
+                        for (int64_t x = nx - 1; x <= nx + 1; ++x) {
+                            if (!(x >= 0 && x < cx && y >= 0 && y < cy && z >= 0 && z < cz)) continue;
+                            Vec center = flow.low + Vec(R(x) + R(0.5), R(y) + R(0.5), R(z) + R(0.5)) * spacing;
+                            if (length_squared(at - center) < clear) taken[size_t((y * cz + z) * cx + x)] = 1;
+                        }
+            }
+            for (int64_t y = 0; y < cy; ++y)
+                for (int64_t z = 0; z < cz; ++z)
+                    for (int64_t x = 0; x < cx; ++x) {
+                        if (taken[size_t((y * cz + z) * cx + x)]) continue;
+                        Vec at = flow.low + Vec(R(x) + R(0.5), R(y) + R(0.5), R(z) + R(0.5)) * spacing;
+                        Status st = add_particle(at, flow.velocity, nullptr);
+                        if (st != OK) return st;
+                        ++emitted;
+                    }
+        }
+        return OK;
     }
 
     // mod.rs:493-524
@@ -795,6 +926,8 @@ template <class R> class World {
             Status st = settings.solver == 0 ? wcsph(dt, report) : dfsph(dt, report);
             if (st != OK) return st;
         }
+        Status flowed = run_flows(report.emitted, report.drained);
+        if (flowed != OK) return flowed;
         report.lost = keep_in_domain();
         report.max_speed = float(fastest());
         R rest = R(settings.rest_density);

@@ -182,6 +182,33 @@ int32_t orc_remove_boundary(void* p, uint32_t id, int32_t* removed) {
     return OK;
 }
 
+int32_t orc_add_emitter(void* p, const float* low, const float* high, const float* velocity, uint32_t* id) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.add_emitter(v3<R>(low), v3<R>(high), v3<R>(velocity), id));
+    return st;
+}
+
+int32_t orc_add_drain(void* p, const float* low, const float* high, uint32_t* id) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.add_drain(v3<R>(low), v3<R>(high), id));
+    return st;
+}
+
+int32_t orc_remove_flow(void* p, uint32_t id, int32_t* removed) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, *removed = w.remove_flow(id) ? 1 : 0);
+    return OK;
+}
+
+int32_t orc_run_flows(void* p, uint32_t* emitted, uint32_t* drained) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.run_flows(*emitted, *drained));
+    return st;
+}
+
 int32_t orc_wall_count(void* p, uint64_t* out) {
     auto* h = static_cast<Handle*>(p);
     ORC_DISPATCH(h, *out = w.walls.positions.size());

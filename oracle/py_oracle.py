@@ -53,6 +53,10 @@ def lib():
             "orc_add_box_container": [vp, f3, f3, u32p],
             "orc_add_wall": [vp, f3, f3, u32p],
             "orc_remove_boundary": [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32)],
+            "orc_add_emitter": [vp, f3, f3, f3, u32p],
+            "orc_add_drain": [vp, f3, f3, u32p],
+            "orc_remove_flow": [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32)],
+            "orc_run_flows": [vp, u32p, u32p],
             "orc_wall_count": [vp, u64p],
             "orc_read_wall_positions": [vp, dp, ctypes.c_uint64],
             "orc_step": [vp, ctypes.c_float, ctypes.POINTER(CReport)],
@@ -170,6 +174,27 @@ class OracleWorld:
         r = ctypes.c_int32()
         _check(lib().orc_remove_boundary(self._h, boundary, ctypes.byref(r)))
         return bool(r.value)
+
+    # ---- emitters and drains (flow.rs:86-139) ----
+    def add_emitter(self, low, high, velocity) -> int:
+        i = ctypes.c_uint32()
+        _check(lib().orc_add_emitter(self._h, vec3(low), vec3(high), vec3(velocity), ctypes.byref(i)))
+        return i.value
+
+    def add_drain(self, low, high) -> int:
+        i = ctypes.c_uint32()
+        _check(lib().orc_add_drain(self._h, vec3(low), vec3(high), ctypes.byref(i)))
+        return i.value
+
+    def remove_flow(self, flow: int) -> bool:
+        r = ctypes.c_int32()
+        _check(lib().orc_remove_flow(self._h, flow, ctypes.byref(r)))
+        return bool(r.value)
+
+    def run_flows(self):
+        e, d = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().orc_run_flows(self._h, ctypes.byref(e), ctypes.byref(d)))
+        return e.value, d.value
 
     def wall_positions(self) -> np.ndarray:
         n = ctypes.c_uint64()

@@ -748,21 +748,83 @@ __global__ void k_brick_fill(uint32_t volume, int3 span, const uint32_t* __restr
 
 // ---- domain (mod.rs:451-486): keep flags, then a stable compaction -------------------------
 
-__global__ void k_domain_flags(Params p, const float4* __restrict__ pos, const int4* __restrict__ cells, float3 low,
-                               float3 high, uint32_t* keep) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
+// The f32 position the readouts give: cell-relative ones rebuilt in double and rounded once.
+__device__ __forceinline__ float4 absolute_of(const Params& p, const float4* __restrict__ pos,
+                                              const int4* __restrict__ cells, uint32_t i) {
     float4 a = pos[i];
-    if (cells) {  // cell-relative: the position rebuilt in double
+    if (cells) {
         int4 c = cells[i];
         const double r = p.radius;
-        double x = double(c.x) * r + a.x, y = double(c.y) * r + a.y, z = double(c.z) * r + a.z;
-        keep[i] = (x >= low.x && x <= high.x && y >= low.y && y <= high.y && z >= low.z && z <= high.z) ? 1u : 0u;
+        a.x = float(double(c.x) * r + a.x);
+        a.y = float(double(c.y) * r + a.y);
+        a.z = float(double(c.z) * r + a.z);
+    }
+    return a;
+}
+
+// drain = 0: keep what the domain holds, clamp(p) == p (mod.rs:451-486); drain = 1: keep what
+// lies outside the drain box, inclusive bounds (flow.rs:154-161)
+__global__ void k_domain_flags(Params p, const float4* __restrict__ pos, const int4* __restrict__ cells, float3 low,
+                               float3 high, int drain, uint32_t* keep) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float4 a = absolute_of(p, pos, cells, i);
+    if (drain) {
+        bool inside = a.x >= low.x && a.y >= low.y && a.z >= low.z && a.x <= high.x && a.y <= high.y && a.z <= high.z;
+        keep[i] = inside ? 0u : 1u;
         return;
     }
     float cx = fminf(fmaxf(a.x, low.x), high.x), cy = fminf(fmaxf(a.y, low.y), high.y),
           cz = fminf(fmaxf(a.z, low.z), high.z);
     keep[i] = (cx == a.x && cy == a.y && cz == a.z) ? 1u : 0u;
+}
+
+// ---- emitters (flow.rs:168-226) --------------------------------------------------------------
+// Lattice slots of an emitter box: cnt per axis, slot (x, y, z) at index (y cnt.z + z) cnt.x + x,
+// its centre low + ((x, y, z) + 1/2) spacing.  A slot is taken when a particle is nearer its
+// centre than 0.9 spacing; each particle tests the 3 x 3 x 3 slots around its nearest one.
+
+// Rust's `f as i64` (saturating, NaN to 0), then held to [-2, cells + 1]: further out reaches no slot
+__device__ __forceinline__ long long nearest_slot(float v, int cells) {
+    float r = roundf(v);
+    long long c = (r != r) ? 0 : (r >= 9.2233720e18f ? LLONG_MAX : (r <= -9.2233720e18f ? LLONG_MIN : (long long)r));
+    return c < -2 ? -2 : (c > cells + 1 ? cells + 1 : c);
+}
+
+__global__ void k_emitter_taken(Params p, const float4* __restrict__ pos, const int4* __restrict__ cells, float3 low,
+                                int3 cnt, float spacing, float clear, uint32_t* __restrict__ taken) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float4 a = absolute_of(p, pos, cells, i);
+    long long nx = nearest_slot((a.x - low.x) / spacing - 0.5f, cnt.x);
+    long long ny = nearest_slot((a.y - low.y) / spacing - 0.5f, cnt.y);
+    long long nz = nearest_slot((a.z - low.z) / spacing - 0.5f, cnt.z);
+    for (long long y = ny - 1; y <= ny + 1; ++y)
+        for (long long z = nz - 1; z <= nz + 1; ++z)
+            for (long long x = nx - 1; x <= nx + 1; ++x) {
+                if (x < 0 || x >= cnt.x || y < 0 || y >= cnt.y || z < 0 || z >= cnt.z) continue;
+                float ox = a.x - (low.x + (float(x) + 0.5f) * spacing);
+                float oy = a.y - (low.y + (float(y) + 0.5f) * spacing);
+                float oz = a.z - (low.z + (float(z) + 0.5f) * spacing);
+                if (dot3(ox, oy, oz, ox, oy, oz) < clear) taken[(y * cnt.z + z) * cnt.x + x] = 1u;
+            }
+}
+
+// After an exclusive scan of `taken` (total at taken_ex[total]): the free slots in slot order
+// become particles first_id, first_id + 1, ... until `room` of them are placed.
+__global__ void k_emit(uint32_t total, const uint32_t* __restrict__ taken_ex, int3 cnt, float3 low, float spacing,
+                       float3 velocity, uint32_t room, uint32_t first_id, float4* __restrict__ pos_out,
+                       float4* __restrict__ vel_out, uint32_t* __restrict__ ids_out, float* __restrict__ rho_out) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= total || taken_ex[s + 1] != taken_ex[s]) return;
+    uint32_t rank = s - taken_ex[s];
+    if (rank >= room) return;
+    uint32_t x = s % uint32_t(cnt.x), z = (s / uint32_t(cnt.x)) % uint32_t(cnt.z), y = s / (uint32_t(cnt.x) * uint32_t(cnt.z));
+    pos_out[rank] = make_float4(low.x + (float(x) + 0.5f) * spacing, low.y + (float(y) + 0.5f) * spacing,
+                                low.z + (float(z) + 0.5f) * spacing, 0.0f);
+    vel_out[rank] = make_float4(velocity.x, velocity.y, velocity.z, 0.0f);
+    ids_out[rank] = first_id + rank;
+    rho_out[rank] = 0.0f;
 }
 
 __global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ dest,
@@ -933,9 +995,22 @@ void launch_list_fill(const Params& p, const GridDev& g, const float4* pos, cons
     if (p.n) k_list_fill<<<blocks_for(p.n), kBlock, 0, s>>>(p, g, pos, pts, start, items);
 }
 
-void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, float3 low, float3 high,
+void launch_emitter_taken(const Params& p, const float4* pos, const int4* cells, float3 low, int3 cnt, float spacing,
+                          float clear, uint32_t* taken, cudaStream_t s) {
+    if (p.n) k_emitter_taken<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, cells, low, cnt, spacing, clear, taken);
+}
+
+void launch_emit(uint32_t total, const uint32_t* taken_ex, int3 cnt, float3 low, float spacing, float3 velocity,
+                 uint32_t room, uint32_t first_id, float4* pos_out, float4* vel_out, uint32_t* ids_out, float* rho_out,
+                 cudaStream_t s) {
+    if (total && room)
+        k_emit<<<blocks_for(total), kBlock, 0, s>>>(total, taken_ex, cnt, low, spacing, velocity, room, first_id, pos_out,
+                                                    vel_out, ids_out, rho_out);
+}
+
+void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, float3 low, float3 high, int drain,
                          uint32_t* keep, cudaStream_t s) {
-    if (p.n) k_domain_flags<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, cells, low, high, keep);
+    if (p.n) k_domain_flags<<<blocks_for(p.n), kBlock, 0, s>>>(p, pos, cells, low, high, drain, keep);
 }
 
 void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, const uint32_t* ids_in,

@@ -68,8 +68,16 @@ void launch_list_fill(const Params& p, const GridDev& g, const float4* pos, cons
                       uint32_t* items, cudaStream_t s);
 
 // domain
-void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, float3 low, float3 high,
+// keep flags: the domain's inside (drain = 0) or a drain box's outside (drain = 1)
+void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, float3 low, float3 high, int drain,
                          uint32_t* keep, cudaStream_t s);
+// emitters: mark the taken lattice slots (taken cleared, total + 1 words), then, after an
+// exclusive scan of taken, write up to `room` particles for the free slots in slot order
+void launch_emitter_taken(const Params& p, const float4* pos, const int4* cells, float3 low, int3 cnt, float spacing,
+                          float clear, uint32_t* taken, cudaStream_t s);
+void launch_emit(uint32_t total, const uint32_t* taken_ex, int3 cnt, float3 low, float spacing, float3 velocity,
+                 uint32_t room, uint32_t first_id, float4* pos_out, float4* vel_out, uint32_t* ids_out, float* rho_out,
+                 cudaStream_t s);
 void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, const uint32_t* ids_in,
                     const float4* pos_in, const float4* vel_in, const float* rho_in, const int4* cells_in,
                     uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out, int4* cells_out,

@@ -318,7 +318,7 @@ struct World {
         if (stream) {
             for (auto* b : {&pos[0], &pos[1], &pos[2], &vel[0], &vel[1], &vel[2]}) b->release(stream);
             for (auto* b : {&ids[0], &ids[1], &lin, &cslot, &members, &count, &tiles, &keep, &dwstart, &fcnt, &wcnt,
-                            &worder, &wkeys, &wsums})
+                            &worder, &wkeys, &wsums, &etaken, &etiles})
                 b->release(stream);
             for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha}) b->release(stream);
             for (auto* b : {&cell[0], &cell[1], &cell[2]}) b->release(stream);
@@ -326,6 +326,7 @@ struct World {
             went.release(stream);
             partials.release(stream);
             stage.release(stream);
+            estage.release(stream);
             tape.cpos.release(stream);
             tape.cvel.release(stream);
             tape.cids.release(stream);
@@ -1156,7 +1157,7 @@ struct World {
     int32_t step(float dt, slf_report* out) {
         if (!tape.on) return step_untaped(dt, out);
         SLF_TRY(flush());
-        if (n != tape.n || has_domain)
+        if (n != tape.n || has_domain || !flows.empty())
             return fail(SLF_ERR_UNSUPPORTED, "the particles changed while a tape was recording");
         tape.steps.emplace_back();
         tape_step = &tape.steps.back();
@@ -1544,7 +1545,8 @@ struct World {
                 }
             }
         }
-        // keep_in_domain (mod.rs:451-486)
+        // run_flows (step.rs:76-81), then keep_in_domain (mod.rs:451-486)
+        SLF_TRY(run_flows(r.emitted, r.drained));
         SLF_TRY(keep_in_domain(r.lost));
         // max_speed and max_compression of what is left (step.rs:83-88)
         if (n > 0) {
@@ -1563,15 +1565,17 @@ struct World {
         return SLF_OK;
     }
 
-    int32_t keep_in_domain(uint32_t& lost) {
-        lost = 0;
-        if (!has_domain || n == 0) return SLF_OK;
+    // Keeps, in order, the particles inside the box (drain = 0) or outside it (drain = 1);
+    // `removed` counts the others.
+    int32_t keep_where(F3 low, F3 high, int drain, uint32_t& removed) {
+        removed = 0;
+        if (n == 0) return SLF_OK;
         Params p = params();
         SLF_TRY(keep.ensure(n + 1, 0, stream));
         SLF_TRY(members.ensure(n + 1, 0, stream));
         SLF_TRY(tiles.ensure(scan_tiles(uint32_t(n)) + 1, 0, stream));
-        launch_domain_flags(p, pos[cpos].p, cells_of(cpos), make_float3(dlow.x, dlow.y, dlow.z),
-                            make_float3(dhigh.x, dhigh.y, dhigh.z), keep.p, stream);
+        launch_domain_flags(p, pos[cpos].p, cells_of(cpos), make_float3(low.x, low.y, low.z),
+                            make_float3(high.x, high.y, high.z), drain, keep.p, stream);
         SLF_CUDA(cudaMemcpyAsync(members.p, keep.p, n * 4, cudaMemcpyDeviceToDevice, stream));
         launch_exclusive_scan(members.p, uint32_t(n), tiles.p, stream);
         uint32_t kept = 0;
@@ -1583,12 +1587,135 @@ struct World {
         launch_compact(uint32_t(n), keep.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p, rho[cid].p,
                        cells_of(cpos), ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, cells_of(to), stream);
         SLF_CUDA(cudaStreamSynchronize(stream));
-        lost = uint32_t(n - kept);
+        removed = uint32_t(n - kept);
         n = kept;
         cpos = to;
         cid = 1 - cid;
         lists_valid = false;
         stats_fresh = false;
+        return SLF_OK;
+    }
+
+    // keep_in_domain (mod.rs:451-486)
+    int32_t keep_in_domain(uint32_t& lost) {
+        lost = 0;
+        if (!has_domain) return SLF_OK;
+        return keep_where(dlow, dhigh, 0, lost);
+    }
+
+    // ---- emitters and drains (src/fluid/flow.rs) ---------------------------------------------
+
+    struct FlowBox {
+        uint32_t id;
+        F3 low, high;
+        bool emitter;
+        F3 velocity;
+    };
+    std::vector<FlowBox> flows;
+    uint32_t flow_next = 0;
+    DevBuf<uint32_t> etaken, etiles;
+    DevBuf<float4> estage;
+
+    // add_flow (flow.rs:115-139), add_emitter (:86-99), add_drain (:104-106)
+    int32_t add_flow(const float* low, const float* high, bool emitter, const float* velocity, uint32_t* out) {
+        if (emitter && !finite3(velocity)) return fail(SLF_ERR_NON_FINITE, "non finite value in emitter velocity");
+        if (!finite3(low) || !finite3(high)) return fail(SLF_ERR_NON_FINITE, "non finite value in flow box");
+        if (high[0] <= low[0] || high[1] <= low[1] || high[2] <= low[2])
+            return fail(SLF_ERR_OUT_OF_RANGE, "inside out flow box");
+        if (flow_next == UINT32_MAX) return fail(SLF_ERR_FLUID_FULL, "no flow ids left");
+        FlowBox f{flow_next++, F3{low[0], low[1], low[2]}, F3{high[0], high[1], high[2]}, emitter, F3{0, 0, 0}};
+        if (emitter) f.velocity = F3{velocity[0], velocity[1], velocity[2]};
+        flows.push_back(f);
+        if (out) *out = f.id;
+        return SLF_OK;
+    }
+
+    // remove_flow (flow.rs:109-113)
+    bool remove_flow(uint32_t id) {
+        size_t before = flows.size();
+        flows.erase(std::remove_if(flows.begin(), flows.end(), [&](const FlowBox& f) { return f.id == id; }),
+                    flows.end());
+        return flows.size() != before;
+    }
+
+    // Rust's `f as i64`: saturating, NaN to 0
+    static int64_t as_i64(float v) {
+        if (std::isnan(v)) return 0;
+        if (v >= 9.2233720e18f) return INT64_MAX;
+        if (v <= -9.2233720e18f) return INT64_MIN;
+        return int64_t(v);
+    }
+
+    // run_flows (flow.rs:144-231): drains first, then emitters, each in the order they were
+    // added.  An emitter whose lattice would hold more than 2^30 slots is refused (the reference
+    // allocates one flag per slot, up to 4096^3).
+    int32_t run_flows(uint32_t& emitted, uint32_t& drained) {
+        emitted = drained = 0;
+        if (flows.empty()) return SLF_OK;
+        std::vector<FlowBox> list = flows;
+        for (const FlowBox& f : list) {
+            if (f.emitter) continue;
+            uint32_t gone = 0;
+            SLF_TRY(keep_where(f.low, f.high, 1, gone));
+            drained += gone;
+        }
+        const float spacing = s.spacing;
+        for (const FlowBox& f : list) {
+            if (!f.emitter) continue;
+            auto count = [&](float extent) -> int64_t {
+                return std::min<int64_t>(std::max<int64_t>(as_i64(std::floor(extent / spacing)), 0), int64_t(1) << 12);
+            };
+            int64_t cx = count(f.high.x - f.low.x), cy = count(f.high.y - f.low.y), cz = count(f.high.z - f.low.z);
+            int64_t total = cx * cy * cz;
+            if (total == 0) continue;
+            if (total > (int64_t(1) << 30)) return fail(SLF_ERR_OUT_OF_RANGE, "emitter box holds more than 2^30 slots");
+            float share = 0.9f * spacing;
+            float clear = share * share;
+            uint32_t slots = uint32_t(total);
+            SLF_TRY(etaken.ensure(size_t(slots) + 1, 0, stream));
+            SLF_TRY(etiles.ensure(scan_tiles(slots) + 1, 0, stream));
+            SLF_CUDA(cudaMemsetAsync(etaken.p, 0, (size_t(slots) + 1) * 4, stream));
+            Params p = params();
+            float3 low3 = make_float3(f.low.x, f.low.y, f.low.z);
+            int3 cnt = make_int3(int(cx), int(cy), int(cz));
+            launch_emitter_taken(p, pos[cpos].p, cells_of(cpos), low3, cnt, spacing, clear, etaken.p, stream);
+            launch_exclusive_scan(etaken.p, slots, etiles.p, stream);
+            uint32_t taken = 0;
+            SLF_CUDA(cudaMemcpyAsync(&taken, etaken.p + slots, 4, cudaMemcpyDeviceToHost, stream));
+            SLF_CUDA(cudaStreamSynchronize(stream));
+            uint64_t free_slots = uint64_t(slots) - taken;
+            // add_particle's room (mod.rs:416-418): the particle cap and the ids left
+            uint64_t room = s.max_particles > n ? s.max_particles - n : 0;
+            room = std::min<uint64_t>(room, uint64_t(UINT32_MAX - next_id));
+            room = std::min<uint64_t>(room, index_limit() > n ? index_limit() - n : 0);
+            uint64_t k = std::min<uint64_t>(free_slots, room);
+            if (k) {
+                uint64_t m = n + k;
+                for (int i = 0; i < 3; ++i) {
+                    SLF_TRY(pos[i].ensure(m, i == cpos ? n : 0, stream));
+                    SLF_TRY(vel[i].ensure(m, i == cpos ? n : 0, stream));
+                    if (rel()) SLF_TRY(cell[i].ensure(m, i == cpos ? n : 0, stream));
+                }
+                for (int i = 0; i < 2; ++i) {
+                    SLF_TRY(ids[i].ensure(m, i == cid ? n : 0, stream));
+                    SLF_TRY(rho[i].ensure(m, i == cid ? n : 0, stream));
+                }
+                float4* out = pos[cpos].p + n;
+                if (rel()) {
+                    SLF_TRY(estage.ensure(k, 0, stream));
+                    out = estage.p;
+                }
+                launch_emit(slots, etaken.p, cnt, low3, spacing, make_float3(f.velocity.x, f.velocity.y, f.velocity.z),
+                            uint32_t(k), next_id, out, vel[cpos].p + n, ids[cid].p + n, rho[cid].p + n, stream);
+                if (rel()) launch_to_relative(p, uint32_t(k), nullptr, estage.p, pos[cpos].p + n, cell[cpos].p + n, stream);
+                n = m;
+                next_id += uint32_t(k);
+                emitted += uint32_t(k);
+                lists_valid = false;
+                stats_fresh = false;
+            }
+            if (k < free_slots) return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
+        }
         return SLF_OK;
     }
 
@@ -1889,6 +2016,29 @@ int32_t slf_remove_boundary(slf_world* world, uint32_t boundary, int32_t* remove
     SLF_WORLD(world);
     bool gone = world->w.remove_boundary(boundary);
     if (removed) *removed = gone ? 1 : 0;
+    return SLF_OK;
+}
+
+int32_t slf_add_emitter(slf_world* world, const float low[3], const float high[3], const float velocity[3],
+                        uint32_t* flow_out) {
+    SLF_WORLD(world);
+    SLF_NEED(low);
+    SLF_NEED(high);
+    SLF_NEED(velocity);
+    return world->w.add_flow(low, high, true, velocity, flow_out);
+}
+
+int32_t slf_add_drain(slf_world* world, const float low[3], const float high[3], uint32_t* flow_out) {
+    SLF_WORLD(world);
+    SLF_NEED(low);
+    SLF_NEED(high);
+    return world->w.add_flow(low, high, false, nullptr, flow_out);
+}
+
+int32_t slf_remove_flow(slf_world* world, uint32_t flow, int32_t* removed) {
+    SLF_WORLD(world);
+    bool r = world->w.remove_flow(flow);
+    if (removed) *removed = r ? 1 : 0;
     return SLF_OK;
 }
 

@@ -53,6 +53,9 @@ def load_library():
         "slf_add_box_container": [vp, fp, fp, u32p],
         "slf_add_wall": [vp, fp, fp, u32p],
         "slf_remove_boundary": [vp, ctypes.c_uint32, i32p],
+        "slf_add_emitter": [vp, fp, fp, fp, u32p],
+        "slf_add_drain": [vp, fp, fp, u32p],
+        "slf_remove_flow": [vp, ctypes.c_uint32, i32p],
         "slf_wall_count": [vp, u64p],
         "slf_read_wall_positions": [vp, fp, ctypes.c_uint64],
         "slf_step": [vp, ctypes.c_float, ctypes.POINTER(CReport)],
@@ -199,6 +202,22 @@ class FluidWorld:
     def remove_boundary(self, boundary: int) -> bool:
         r = ctypes.c_int32()
         _check(_lib.slf_remove_boundary(self._h, boundary, ctypes.byref(r)))
+        return bool(r.value)
+
+    # ---- emitters and drains (flow.rs:86-139) ----
+    def add_emitter(self, low, high, velocity) -> int:
+        i = ctypes.c_uint32()
+        _check(_lib.slf_add_emitter(self._h, vec3(low), vec3(high), vec3(velocity), ctypes.byref(i)))
+        return i.value
+
+    def add_drain(self, low, high) -> int:
+        i = ctypes.c_uint32()
+        _check(_lib.slf_add_drain(self._h, vec3(low), vec3(high), ctypes.byref(i)))
+        return i.value
+
+    def remove_flow(self, flow: int) -> bool:
+        r = ctypes.c_int32()
+        _check(_lib.slf_remove_flow(self._h, flow, ctypes.byref(r)))
         return bool(r.value)
 
     def wall_positions(self) -> np.ndarray:
