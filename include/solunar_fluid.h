@@ -39,7 +39,8 @@ enum {
     SLF_ERR_UNSUPPORTED = 6,         /* a feature off the fluid step (movers, terrain) */
     SLF_ERR_CUDA = 7,                /* a CUDA call failed; see slf_last_error() */
     SLF_ERR_TIMEOUT = 8,             /* a bounded device loop gave up */
-    SLF_ERR_INVALID_ARGUMENT = 9     /* null pointer or wrong buffer size */
+    SLF_ERR_INVALID_ARGUMENT = 9,    /* null pointer or wrong buffer size */
+    SLF_ERR_SNAPSHOT = 10            /* SnapshotError (src/snapshot/mod.rs:56-63); see slf_last_error() */
 };
 
 /* FluidSolver (src/fluid/mod.rs:43-53). */
@@ -148,6 +149,16 @@ int32_t slf_add_wall(slf_world* world, const float low[3], const float high[3],
 
 /* FluidWorld::remove_boundary (boundary.rs:94-115).  *removed = 0 for an unknown id. */
 int32_t slf_remove_boundary(slf_world* world, uint32_t boundary, int32_t* removed);
+
+/* FluidWorld::save_snapshot (src/fluid/save.rs:18-73): the SLFL version 3 bytes of the world.
+ * *size receives the byte count; out = NULL asks for the size only, else capacity >= *size. */
+int32_t slf_save_snapshot(slf_world* world, uint8_t* out, uint64_t capacity, uint64_t* size);
+/* FluidWorld::load_snapshot (save.rs:79-181): a new world from untrusted snapshot bytes
+ * (versions 1-3).  The library's own settings fields (positions, arithmetic, solver limits,
+ * device) come from `library`, or the defaults when it is NULL.  Bad bytes return
+ * SLF_ERR_SNAPSHOT with the reference's message in slf_last_error(); coupled bodies or terrain
+ * in the snapshot return SLF_ERR_UNSUPPORTED. */
+int32_t slf_load_snapshot(const uint8_t* data, uint64_t size, const slf_settings* library, slf_world** out);
 
 /* FluidWorld::add_emitter (flow.rs:86-99): after each step every lattice slot of the box with
  * no water within 0.9 spacing of its centre gets a particle moving at `velocity`.  Boxes of more

@@ -21,7 +21,9 @@
 //                         check_box :230-238, union :240-247
 //   src/fluid/flow.rs     CLEAR_SHARE :7, add_emitter :86-99, add_drain :104-106,
 //                         remove_flow :109-113, add_flow :115-139, run_flows :144-231
-//   src/snapshot/bytes.rs fnv1a :6-13
+//   src/fluid/save.rs     save_snapshot :18-73, load_snapshot :79-181 (Walls::save/load
+//                         boundary.rs:182-227, Flows::save/load flow.rs:36-83)
+//   src/snapshot/bytes.rs fnv1a :6-13, Writer :15-67, Reader :89-157
 //
 // Arithmetic follows the reference's scalar code: left-to-right evaluation, no fused
 // multiply-add (build with -ffp-contract=off), IEEE division and square root, `powi` as binary
@@ -42,6 +44,7 @@
 #include <cstring>
 #include <limits>
 #include <numeric>
+#include <string>
 #include <tuple>
 #include <type_traits>
 #include <utility>
@@ -62,6 +65,7 @@ enum Status : int32_t {
     DISPATCH_INCOMPLETE = 5,
     UNSUPPORTED = 6,
     INVALID_ARGUMENT = 9,
+    SNAPSHOT = 10,  // SnapshotError (src/snapshot/mod.rs:56-63)
 };
 
 // ---- scalar helpers ---------------------------------------------------------------------
@@ -908,6 +912,231 @@ template <class R> class World {
             }
         }
         return fnv1a(bytes.data(), bytes.size());
+    }
+
+    // ---- snapshots (save.rs) -------------------------------------------------------------------
+
+    struct Out {
+        std::vector<uint8_t> b;
+        void u8(uint8_t v) { b.push_back(v); }
+        void u32(uint32_t v) { for (int k = 0; k < 4; ++k) b.push_back(uint8_t((v >> (8 * k)) & 0xffu)); }
+        void u64(uint64_t v) { for (int k = 0; k < 8; ++k) b.push_back(uint8_t((v >> (8 * k)) & 0xffu)); }
+        void f32(float v) { u32(uint32_t(bits_of(v))); }
+        void v3(const Vec& v) { f32(float(v.x)); f32(float(v.y)); f32(float(v.z)); }
+    };
+
+    // save.rs:18-73; vectors are stored as f32 (the double oracle rounds them)
+    std::vector<uint8_t> save_snapshot() const {
+        Out o;
+        for (char c : {'S', 'L', 'F', 'L'}) o.u8(uint8_t(c));
+        o.u32(3);
+        o.u8(uint8_t(settings.solver));
+        for (float v : {settings.spacing, settings.rest_density, settings.support, settings.sound_speed,
+                        settings.viscosity, settings.courant})
+            o.f32(v);
+        o.u64(settings.max_particles);
+        for (float g : settings.gravity) o.f32(g);
+        o.u32(settings.max_substeps);
+        o.u32(uint32_t(len()));
+        for (size_t i = 0; i < len(); ++i) {
+            o.u32(ids[i]);
+            o.v3(positions[i]);
+            o.v3(velocities[i]);
+        }
+        o.u32(next_id);
+        o.u32(uint32_t(walls.positions.size()));
+        for (size_t k = 0; k < walls.positions.size(); ++k) {
+            o.v3(walls.positions[k]);
+            o.u32(walls.owners[k]);
+        }
+        o.u32(walls.next);
+        o.u32(uint32_t(walls.containers.size()));
+        for (auto& c : walls.containers) {
+            o.u32(c.id);
+            o.v3(c.low);
+            o.v3(c.high);
+        }
+        o.u32(uint32_t(flows.size()));
+        for (auto& f : flows) {
+            o.u32(f.id);
+            o.v3(f.low);
+            o.v3(f.high);
+            o.u8(f.emitter ? 0 : 1);
+            if (f.emitter) o.v3(f.velocity);
+        }
+        o.u32(flow_next);
+        o.u32(0);  // coupled bodies
+        o.u32(0);  // terrain regions
+        o.u8(has_domain ? 1 : 0);
+        if (has_domain) {
+            o.v3(domain_low);
+            o.v3(domain_high);
+        }
+        o.u64(fnv1a(o.b.data(), o.b.size()));
+        return o.b;
+    }
+
+    struct In {
+        const uint8_t* d;
+        size_t n, at;
+        std::string* msg;
+        bool fail(const char* m) {
+            if (msg->empty()) *msg = m;
+            return false;
+        }
+        bool get(uint8_t* out, size_t k) {
+            if (n - at < k) return fail("snapshot truncated");
+            std::memcpy(out, d + at, k);
+            at += k;
+            return true;
+        }
+        bool u8(uint8_t& v) { return get(&v, 1); }
+        bool u32(uint32_t& v) {
+            uint8_t b[4];
+            if (!get(b, 4)) return false;
+            v = 0;
+            for (int k = 3; k >= 0; --k) v = (v << 8) | b[k];
+            return true;
+        }
+        bool u64(uint64_t& v) {
+            uint8_t b[8];
+            if (!get(b, 8)) return false;
+            v = 0;
+            for (int k = 7; k >= 0; --k) v = (v << 8) | b[k];
+            return true;
+        }
+        bool f32(float& v) {
+            uint32_t b;
+            if (!u32(b)) return false;
+            std::memcpy(&v, &b, 4);
+            return true;
+        }
+        bool v3(Vec& v) {
+            float x, y, z;
+            if (!(f32(x) && f32(y) && f32(z))) return false;
+            v = Vec(R(x), R(y), R(z));
+            return true;
+        }
+        bool count(size_t record, uint64_t max, size_t& out) {
+            uint32_t c;
+            if (!u32(c)) return false;
+            if (c > max) return fail("invalid snapshot: count over limit");
+            if (uint64_t(c) * record > uint64_t(n - at)) return fail("snapshot truncated");
+            out = c;
+            return true;
+        }
+    };
+
+    // save.rs:79-181 into `out`; `base` gives the fields the snapshot does not hold
+    static Status load_snapshot(const uint8_t* data, size_t size, const Settings& base, World& out,
+                                std::string& msg) {
+        auto bad = [&](const std::string& m) {
+            if (msg.empty()) msg = m;
+            return SNAPSHOT;
+        };
+        if (size > (size_t(1) << 30)) return bad("snapshot over limit");
+        if (size < 16) return bad("snapshot truncated");
+        if (std::memcmp(data, "SLFL", 4) != 0) return bad("not a snapshot");
+        size_t body = size - 8;
+        uint64_t stored = 0;
+        for (int k = 7; k >= 0; --k) stored = (stored << 8) | data[body + k];
+        if (stored != fnv1a(data, body)) return bad("snapshot checksum mismatch");
+        In r{data, body, 4, &msg};
+        uint32_t version;
+        if (!r.u32(version)) return SNAPSHOT;
+        if (version < 1 || version > 3) return bad("unsupported snapshot version " + std::to_string(version));
+        uint8_t solver;
+        if (!r.u8(solver)) return SNAPSHOT;
+        if (solver > 1) return bad("invalid snapshot: fluid solver");
+        Settings st = base;
+        st.solver = solver;
+        float g[3];
+        if (!(r.f32(st.spacing) && r.f32(st.rest_density) && r.f32(st.support) && r.f32(st.sound_speed) &&
+              r.f32(st.viscosity) && r.f32(st.courant) && r.u64(st.max_particles) && r.f32(g[0]) && r.f32(g[1]) &&
+              r.f32(g[2]) && r.u32(st.max_substeps)))
+            return SNAPSHOT;
+        for (int a = 0; a < 3; ++a) st.gravity[a] = g[a];
+        World w;
+        if (create(st, w) != OK) return bad("invalid snapshot: fluid settings");
+        size_t count;
+        if (!r.count(28, st.max_particles, count)) return SNAPSHOT;
+        for (size_t i = 0; i < count; ++i) {
+            uint32_t id;
+            Vec at, v;
+            if (!(r.u32(id) && r.v3(at) && r.v3(v))) return SNAPSHOT;
+            if (!is_finite(at) || !is_finite(v)) return bad("invalid snapshot: fluid particle");
+            w.ids.push_back(id);
+            w.positions.push_back(at);
+            w.velocities.push_back(v);
+        }
+        w.densities.assign(count, R(st.rest_density));
+        if (!r.u32(w.next_id)) return SNAPSHOT;
+        std::vector<uint32_t> seen = w.ids;
+        std::sort(seen.begin(), seen.end());
+        for (size_t i = 1; i < seen.size(); ++i)
+            if (seen[i] == seen[i - 1]) return bad("invalid snapshot: fluid particle id");
+        if (!seen.empty() && seen.back() >= w.next_id) return bad("invalid snapshot: fluid particle id");
+        size_t nw;
+        if (!r.count(16, st.max_particles, nw)) return SNAPSHOT;
+        for (size_t k = 0; k < nw; ++k) {
+            Vec at;
+            uint32_t owner;
+            if (!r.v3(at)) return SNAPSHOT;
+            if (!is_finite(at)) return bad("invalid snapshot: fluid wall");
+            if (!r.u32(owner)) return SNAPSHOT;
+            w.walls.positions.push_back(at);
+            w.walls.owners.push_back(owner);
+        }
+        size_t nc;
+        if (!(r.u32(w.walls.next) && r.count(28, st.max_particles, nc))) return SNAPSHOT;
+        for (size_t k = 0; k < nc; ++k) {
+            Container<R> c;
+            if (!(r.u32(c.id) && r.v3(c.low) && r.v3(c.high))) return SNAPSHOT;
+            if (check_box(c.low, c.high) != OK || c.id >= w.walls.next) return bad("invalid snapshot: fluid container");
+            w.walls.containers.push_back(c);
+        }
+        for (uint32_t o : w.walls.owners)
+            if (o >= w.walls.next) return bad("invalid snapshot: fluid wall owner");
+        w.update_bounds();
+        size_t nf;
+        if (!r.count(29, 1 << 16, nf)) return SNAPSHOT;
+        for (size_t k = 0; k < nf; ++k) {
+            Flow f{};
+            uint8_t kind;
+            if (!(r.u32(f.id) && r.v3(f.low) && r.v3(f.high) && r.u8(kind))) return SNAPSHOT;
+            if (kind == 0) {
+                f.emitter = true;
+                if (!r.v3(f.velocity)) return SNAPSHOT;
+            } else if (kind != 1) {
+                return bad("invalid snapshot: fluid flow kind");
+            }
+            bool inside_out = f.high.x <= f.low.x || f.high.y <= f.low.y || f.high.z <= f.low.z;
+            if (!(is_finite(f.low) && is_finite(f.high) && is_finite(f.velocity)) || inside_out)
+                return bad("invalid snapshot: fluid flow");
+            w.flows.push_back(f);
+        }
+        if (!r.u32(w.flow_next)) return SNAPSHOT;
+        for (auto& f : w.flows)
+            if (f.id >= w.flow_next) return bad("invalid snapshot: fluid flow id");
+        size_t coupled, terrains;
+        if (!r.count(12, 1 << 16, coupled)) return SNAPSHOT;
+        if (coupled) return UNSUPPORTED;
+        if (!r.count(32, 1 << 16, terrains)) return SNAPSHOT;
+        if (terrains) return UNSUPPORTED;
+        if (version >= 2) {
+            uint8_t flag;
+            if (!r.u8(flag)) return SNAPSHOT;
+            if (flag > 1) return bad("invalid snapshot: fluid domain flag");
+            if (flag == 1) {
+                Vec lo, hi;
+                if (!(r.v3(lo) && r.v3(hi))) return SNAPSHOT;
+                if (w.set_domain(&lo, &hi) != OK) return bad("invalid snapshot: fluid domain");
+            }
+        }
+        if (r.at != body) return bad("invalid snapshot: trailing bytes");
+        w.settle_walls();
+        out = std::move(w);
+        return OK;
     }
 
     // step.rs:92-96

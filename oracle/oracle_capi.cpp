@@ -5,6 +5,8 @@
 // prefix; a handle holds either the float (parity) or the double (precision) restatement.
 // Vectors come in as f32 (the library's input type) and go out as f64, which holds either
 // precision exactly.
+#include <vector>
+#include <string>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -208,6 +210,35 @@ int32_t orc_run_flows(void* p, uint32_t* emitted, uint32_t* drained) {
     ORC_DISPATCH(h, st = w.run_flows(*emitted, *drained));
     return st;
 }
+
+static std::string g_snapshot_message;
+
+int32_t orc_save_snapshot(void* p, uint8_t* out, uint64_t capacity, uint64_t* size) {
+    auto* h = static_cast<Handle*>(p);
+    std::vector<uint8_t> bytes;
+    ORC_DISPATCH(h, bytes = w.save_snapshot());
+    *size = bytes.size();
+    if (!out) return OK;
+    if (capacity < bytes.size()) return INVALID_ARGUMENT;
+    std::memcpy(out, bytes.data(), bytes.size());
+    return OK;
+}
+
+int32_t orc_load_snapshot(const uint8_t* data, uint64_t size, const slf_settings* s, int32_t precision,
+                          int32_t residual_sum, void** out) {
+    if (!s || !out) return INVALID_ARGUMENT;
+    auto h = std::make_unique<Handle>();
+    h->precision = precision == 64 ? 64 : 32;
+    Settings base = from_c(s, residual_sum);
+    g_snapshot_message.clear();
+    Status st = h->precision == 32 ? World<float>::load_snapshot(data, size, base, h->f, g_snapshot_message)
+                                   : World<double>::load_snapshot(data, size, base, h->d, g_snapshot_message);
+    if (st != OK) return st;
+    *out = h.release();
+    return OK;
+}
+
+const char* orc_snapshot_message() { return g_snapshot_message.c_str(); }
 
 int32_t orc_wall_count(void* p, uint64_t* out) {
     auto* h = static_cast<Handle*>(p);

@@ -57,6 +57,9 @@ def lib():
             "orc_add_drain": [vp, f3, f3, u32p],
             "orc_remove_flow": [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32)],
             "orc_run_flows": [vp, u32p, u32p],
+            "orc_save_snapshot": [vp, ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, u64p],
+            "orc_load_snapshot": [ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, ctypes.POINTER(CSettings),
+                                  ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(vp)],
             "orc_wall_count": [vp, u64p],
             "orc_read_wall_positions": [vp, dp, ctypes.c_uint64],
             "orc_step": [vp, ctypes.c_float, ctypes.POINTER(CReport)],
@@ -78,6 +81,8 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = ctypes.c_int32
+        L.orc_snapshot_message.argtypes = []
+        L.orc_snapshot_message.restype = ctypes.c_char_p
         L.orc_destroy.argtypes = [vp]
         L.orc_destroy.restype = None
         _lib = L
@@ -112,6 +117,29 @@ class OracleWorld:
         if h is not None and _lib is not None:
             _lib.orc_destroy(h)
             self._h = None
+
+    # -- snapshots (save.rs) --
+    @classmethod
+    def load_snapshot(cls, data: bytes, settings: FluidSettings | None = None, precision: int = 32,
+                      residual_sum: int = 0) -> "OracleWorld":
+        c = (settings or FluidSettings()).to_c()
+        buf = (ctypes.c_uint8 * max(len(data), 1)).from_buffer_copy(bytes(data) or b"\0")
+        h = ctypes.c_void_p()
+        st = lib().orc_load_snapshot(buf, len(data), ctypes.byref(c), precision, residual_sum, ctypes.byref(h))
+        if st != 0:
+            raise PhysicsError(st, lib().orc_snapshot_message().decode())
+        self = cls.__new__(cls)
+        self._h = h
+        self.precision = precision
+        self._settings = settings or FluidSettings()
+        return self
+
+    def save_snapshot(self) -> bytes:
+        size = ctypes.c_uint64()
+        _check(lib().orc_save_snapshot(self._h, None, 0, ctypes.byref(size)))
+        buf = (ctypes.c_uint8 * max(size.value, 1))()
+        _check(lib().orc_save_snapshot(self._h, buf, size.value, ctypes.byref(size)))
+        return bytes(buf[: size.value])
 
     # -- settings --
     def settings(self) -> FluidSettings:

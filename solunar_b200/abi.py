@@ -20,6 +20,7 @@ STATUS_NAMES = {
     7: "Cuda",
     8: "Timeout",
     9: "InvalidArgument",
+    10: "Snapshot",
 }
 
 

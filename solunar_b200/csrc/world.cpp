@@ -196,6 +196,96 @@ constexpr double walk_order = 4;  // one row index written a particle
 
 }  // namespace
 
+// ---- snapshot bytes (src/snapshot/bytes.rs): little-endian, f32 as its bits, lengths as u32 ----
+
+inline uint64_t fnv1a64(const uint8_t* data, size_t n) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= uint64_t(data[i]);
+        h *= 0x00000100000001b3ull;
+    }
+    return h;
+}
+
+struct SnapWriter {
+    std::vector<uint8_t> data;
+    void bytes(const void* p, size_t n) {
+        const uint8_t* b = static_cast<const uint8_t*>(p);
+        data.insert(data.end(), b, b + n);
+    }
+    void u8(uint8_t v) { data.push_back(v); }
+    void u32(uint32_t v) {
+        for (int k = 0; k < 4; ++k) data.push_back(uint8_t(v >> (8 * k)));
+    }
+    void u64(uint64_t v) {
+        for (int k = 0; k < 8; ++k) data.push_back(uint8_t(v >> (8 * k)));
+    }
+    void f32(float v) {
+        uint32_t b;
+        std::memcpy(&b, &v, 4);
+        u32(b);
+    }
+    void len(size_t v) { u32(uint32_t(v)); }
+    void vec3(float x, float y, float z) {
+        f32(x);
+        f32(y);
+        f32(z);
+    }
+};
+
+// Reads untrusted bytes: every read checks what is left; a failure sets `error` to the
+// reference's message (SnapshotError's Display, src/snapshot/mod.rs:65-76) and returns false.
+struct SnapReader {
+    const uint8_t* data;
+    size_t size, at;
+    std::string error;
+    bool take(void* out, size_t n) {
+        if (n > size - at) return fail_with("snapshot truncated");
+        std::memcpy(out, data + at, n);
+        at += n;
+        return true;
+    }
+    bool fail_with(const char* m) {
+        if (error.empty()) error = m;
+        return false;
+    }
+    bool u8(uint8_t& v) { return take(&v, 1); }
+    bool u32(uint32_t& v) {
+        uint8_t b[4];
+        if (!take(b, 4)) return false;
+        v = uint32_t(b[0]) | uint32_t(b[1]) << 8 | uint32_t(b[2]) << 16 | uint32_t(b[3]) << 24;
+        return true;
+    }
+    bool u64(uint64_t& v) {
+        uint32_t lo, hi;
+        if (!u32(lo) || !u32(hi)) return false;
+        v = uint64_t(lo) | uint64_t(hi) << 32;
+        return true;
+    }
+    bool f32(float& v) {
+        uint32_t b;
+        if (!u32(b)) return false;
+        std::memcpy(&v, &b, 4);
+        return true;
+    }
+    bool vec3(F3& v) { return f32(v.x) && f32(v.y) && f32(v.z); }
+    // Reader::count (bytes.rs:133-150): the count against `max` and the bytes left
+    bool count(size_t record, size_t max, size_t& out) {
+        uint32_t c;
+        if (!u32(c)) return false;
+        if (c > max) return fail_with("invalid snapshot: count over limit");
+        if ((unsigned __int128)c * record > (unsigned __int128)(size - at)) return fail_with("snapshot truncated");
+        out = c;
+        return true;
+    }
+};
+
+inline bool finite3f(const F3& v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); }
+
+constexpr uint32_t kSnapshotVersion = 3;           // FLUID_SNAPSHOT_VERSION (save.rs:9)
+constexpr size_t kMaxSnapshotBytes = size_t(1) << 30;  // MAX_FLUID_SNAPSHOT_BYTES (save.rs:12)
+constexpr size_t kMaxSnapshotParts = size_t(1) << 16;  // MAX_PARTS (save.rs:14)
+
 struct World {
     slf_settings s{};
     float radius = 0, mass = 0, scale = 0;
@@ -444,7 +534,10 @@ struct World {
 
     uint64_t total() const { return n + pend_ids.size(); }
     // FAST list entries keep the index in 26 bits
-    uint64_t index_limit() const { return fast() ? (uint64_t(1) << 26) : UINT64_MAX; }
+    static uint64_t index_limit_of(const slf_settings& st) {
+        return st.arithmetic == SLF_ARITHMETIC_FAST ? (uint64_t(1) << 26) : UINT64_MAX;
+    }
+    uint64_t index_limit() const { return index_limit_of(s); }
 
     int32_t add(uint64_t k, const float* p, const float* v, uint32_t* ids_out) {
         for (uint64_t i = 0; i < k; ++i)
@@ -1719,6 +1812,226 @@ struct World {
         return SLF_OK;
     }
 
+    // ---- snapshots (src/fluid/save.rs) ---------------------------------------------------------
+
+    // save_snapshot (save.rs:18-73): the SLFL version 3 bytes of the current state, particles in
+    // their current order; no coupled bodies or terrains exist on this path.
+    int32_t save_snapshot(std::vector<uint8_t>& out) {
+        SLF_TRY(flush());
+        std::vector<uint32_t> id(n);
+        std::vector<float> p(3 * n), v(3 * n);
+        SLF_TRY(read_plain(ids[cid], id.data(), n));
+        SLF_TRY(read_positions(p.data(), n));
+        SLF_TRY(read_vec(vel[cpos], v.data(), n));
+        SnapWriter w;
+        w.data.reserve(64 + n * 28 + wpos.size() * 16);
+        w.bytes("SLFL", 4);
+        w.u32(kSnapshotVersion);
+        w.u8(s.solver == SLF_SOLVER_DFSPH ? 1 : 0);
+        for (float x : {s.spacing, s.rest_density, s.support, s.sound_speed, s.viscosity, s.courant}) w.f32(x);
+        w.u64(s.max_particles);
+        w.vec3(s.gravity[0], s.gravity[1], s.gravity[2]);
+        w.u32(s.max_substeps);
+        w.len(n);
+        for (uint64_t i = 0; i < n; ++i) {
+            w.u32(id[i]);
+            w.vec3(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+            w.vec3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        }
+        w.u32(next_id);
+        // Walls::save (boundary.rs:182-195)
+        w.len(wpos.size());
+        for (size_t k = 0; k < wpos.size(); ++k) {
+            w.vec3(wpos[k].x, wpos[k].y, wpos[k].z);
+            w.u32(wown[k]);
+        }
+        w.u32(wall_next);
+        w.len(containers.size());
+        for (const ContainerBox& c : containers) {
+            w.u32(c.id);
+            w.vec3(c.low.x, c.low.y, c.low.z);
+            w.vec3(c.high.x, c.high.y, c.high.z);
+        }
+        // Flows::save (flow.rs:36-51)
+        w.len(flows.size());
+        for (const FlowBox& f : flows) {
+            w.u32(f.id);
+            w.vec3(f.low.x, f.low.y, f.low.z);
+            w.vec3(f.high.x, f.high.y, f.high.z);
+            if (f.emitter) {
+                w.u8(0);
+                w.vec3(f.velocity.x, f.velocity.y, f.velocity.z);
+            } else {
+                w.u8(1);
+            }
+        }
+        w.u32(flow_next);
+        w.len(0);  // coupled bodies
+        w.len(0);  // terrain regions
+        if (has_domain) {
+            w.u8(1);
+            w.vec3(dlow.x, dlow.y, dlow.z);
+            w.vec3(dhigh.x, dhigh.y, dhigh.z);
+        } else {
+            w.u8(0);
+        }
+        w.u64(fnv1a64(w.data.data(), w.data.size()));
+        out = std::move(w.data);
+        return SLF_OK;
+    }
+
+    // load_snapshot (save.rs:79-181) into a fresh world: untrusted bytes, checked in the
+    // reference's order; the library's own settings fields come from `lib`.
+    int32_t load_snapshot(const uint8_t* data, size_t size, const slf_settings& lib) {
+        auto bad = [&](const std::string& m) { return fail(SLF_ERR_SNAPSHOT, m); };
+        if (size > kMaxSnapshotBytes) return bad("snapshot over limit");
+        if (size < 4 + 4 + 8) return bad("snapshot truncated");
+        if (std::memcmp(data, "SLFL", 4) != 0) return bad("not a snapshot");
+        const size_t body = size - 8;
+        SnapReader ck{data + body, 8, 0, {}};
+        uint64_t stored = 0;
+        ck.u64(stored);
+        if (stored != fnv1a64(data, body)) return bad("snapshot checksum mismatch");
+        SnapReader r{data, body, 4, {}};
+        auto rd = [&](bool ok) { return ok ? SLF_OK : bad(r.error); };
+        uint32_t version = 0;
+        SLF_TRY(rd(r.u32(version)));
+        if (version < 1 || version > kSnapshotVersion)
+            return bad("unsupported snapshot version " + std::to_string(version));
+        uint8_t solver = 0;
+        SLF_TRY(rd(r.u8(solver)));
+        if (solver > 1) return bad("invalid snapshot: fluid solver");
+        float f[6];
+        for (float& x : f) SLF_TRY(rd(r.f32(x)));
+        uint64_t max_particles = 0;
+        SLF_TRY(rd(r.u64(max_particles)));
+        F3 grav{};
+        SLF_TRY(rd(r.vec3(grav)));
+        uint32_t max_substeps = 0;
+        SLF_TRY(rd(r.u32(max_substeps)));
+        slf_settings st = lib;
+        st.solver = solver;
+        st.spacing = f[0];
+        st.rest_density = f[1];
+        st.support = f[2];
+        st.sound_speed = f[3];
+        st.viscosity = f[4];
+        st.courant = f[5];
+        st.max_particles = max_particles;
+        st.gravity[0] = grav.x;
+        st.gravity[1] = grav.y;
+        st.gravity[2] = grav.z;
+        st.max_substeps = max_substeps;
+        if (!valid(st)) return bad("invalid snapshot: fluid settings");
+        size_t count = 0;
+        SLF_TRY(rd(r.count(28, size_t(std::min<uint64_t>(max_particles, SIZE_MAX)), count)));
+        std::vector<uint32_t> lid(count);
+        std::vector<float4> lpos(count), lvel(count);
+        for (size_t i = 0; i < count; ++i) {
+            F3 at{}, v{};
+            SLF_TRY(rd(r.u32(lid[i]) && r.vec3(at) && r.vec3(v)));
+            if (!finite3f(at) || !finite3f(v)) return bad("invalid snapshot: fluid particle");
+            lpos[i] = make_float4(at.x, at.y, at.z, 0.0f);
+            lvel[i] = make_float4(v.x, v.y, v.z, 0.0f);
+        }
+        uint32_t nid = 0;
+        SLF_TRY(rd(r.u32(nid)));
+        std::vector<uint32_t> seen = lid;
+        std::sort(seen.begin(), seen.end());
+        if (std::adjacent_find(seen.begin(), seen.end()) != seen.end() || (!seen.empty() && seen.back() >= nid))
+            return bad("invalid snapshot: fluid particle id");
+        // Walls::load (boundary.rs:202-227)
+        size_t nw = 0;
+        SLF_TRY(rd(r.count(16, size_t(std::min<uint64_t>(max_particles, SIZE_MAX)), nw)));
+        std::vector<F3> lw(nw);
+        std::vector<uint32_t> lo(nw);
+        for (size_t k = 0; k < nw; ++k) {
+            SLF_TRY(rd(r.vec3(lw[k])));
+            if (!finite3f(lw[k])) return bad("invalid snapshot: fluid wall");
+            SLF_TRY(rd(r.u32(lo[k])));
+        }
+        uint32_t wnext = 0;
+        SLF_TRY(rd(r.u32(wnext)));
+        size_t nc = 0;
+        SLF_TRY(rd(r.count(28, size_t(std::min<uint64_t>(max_particles, SIZE_MAX)), nc)));
+        std::vector<ContainerBox> lc(nc);
+        for (auto& c : lc) {
+            SLF_TRY(rd(r.u32(c.id) && r.vec3(c.low) && r.vec3(c.high)));
+            bool ok = finite3f(c.low) && finite3f(c.high) && c.high.x > c.low.x && c.high.y > c.low.y &&
+                      c.high.z > c.low.z;
+            if (!ok || c.id >= wnext) return bad("invalid snapshot: fluid container");
+        }
+        for (uint32_t o : lo)
+            if (o >= wnext) return bad("invalid snapshot: fluid wall owner");
+        // Flows::load (flow.rs:53-83)
+        size_t nf = 0;
+        SLF_TRY(rd(r.count(29, kMaxSnapshotParts, nf)));
+        std::vector<FlowBox> lf(nf);
+        for (auto& fl : lf) {
+            uint8_t kind = 0;
+            SLF_TRY(rd(r.u32(fl.id) && r.vec3(fl.low) && r.vec3(fl.high) && r.u8(kind)));
+            fl.velocity = F3{0, 0, 0};
+            if (kind == 0) {
+                fl.emitter = true;
+                SLF_TRY(rd(r.vec3(fl.velocity)));
+            } else if (kind == 1) {
+                fl.emitter = false;
+            } else {
+                return bad("invalid snapshot: fluid flow kind");
+            }
+            bool inside_out = fl.high.x <= fl.low.x || fl.high.y <= fl.low.y || fl.high.z <= fl.low.z;
+            if (!(finite3f(fl.low) && finite3f(fl.high) && finite3f(fl.velocity)) || inside_out)
+                return bad("invalid snapshot: fluid flow");
+        }
+        uint32_t fnext = 0;
+        SLF_TRY(rd(r.u32(fnext)));
+        for (auto& fl : lf)
+            if (fl.id >= fnext) return bad("invalid snapshot: fluid flow id");
+        size_t coupled = 0, terrains = 0;
+        SLF_TRY(rd(r.count(12, kMaxSnapshotParts, coupled)));
+        if (coupled) return fail(SLF_ERR_UNSUPPORTED, "coupled bodies are not on this path");
+        SLF_TRY(rd(r.count(32, kMaxSnapshotParts, terrains)));
+        if (terrains) return fail(SLF_ERR_UNSUPPORTED, "terrain regions are not on this path");
+        bool dom = false;
+        F3 dl{}, dh{};
+        if (version >= 2) {
+            uint8_t flag = 0;
+            SLF_TRY(rd(r.u8(flag)));
+            if (flag > 1) return bad("invalid snapshot: fluid domain flag");
+            if (flag == 1) {
+                SLF_TRY(rd(r.vec3(dl) && r.vec3(dh)));
+                bool ok = finite3f(dl) && finite3f(dh) && dh.x > dl.x && dh.y > dl.y && dh.z > dl.z;
+                if (!ok) return bad("invalid snapshot: fluid domain");
+                dom = true;
+            }
+        }
+        if (r.at != body) return bad("invalid snapshot: trailing bytes");
+        if (count > index_limit_of(st)) return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
+        SLF_TRY(init(st));
+        pend_pos = std::move(lpos);
+        pend_vel = std::move(lvel);
+        pend_ids = std::move(lid);
+        next_id = nid;
+        SLF_TRY(flush());
+        if (n) {  // densities of a loaded world: rest density (save.rs:144)
+            std::vector<float> rest(n, s.rest_density);
+            SLF_CUDA(cudaMemcpyAsync(rho[cid].p, rest.data(), n * 4, cudaMemcpyHostToDevice, stream));
+            SLF_TRY(sync());
+        }
+        wpos = std::move(lw);
+        wown = std::move(lo);
+        wall_next = wnext;
+        containers = std::move(lc);
+        update_bounds();
+        settle_walls();
+        flows = std::move(lf);
+        flow_next = fnext;
+        has_domain = dom;
+        dlow = dl;
+        dhigh = dh;
+        return SLF_OK;
+    }
+
     // ---- read-outs -------------------------------------------------------------------------
 
     // packs xyz on the device and copies 12 bytes a particle straight into the caller's buffer
@@ -2016,6 +2329,43 @@ int32_t slf_remove_boundary(slf_world* world, uint32_t boundary, int32_t* remove
     SLF_WORLD(world);
     bool gone = world->w.remove_boundary(boundary);
     if (removed) *removed = gone ? 1 : 0;
+    return SLF_OK;
+}
+
+int32_t slf_save_snapshot(slf_world* world, uint8_t* out, uint64_t capacity, uint64_t* size) {
+    SLF_WORLD(world);
+    SLF_NEED(size);
+    std::vector<uint8_t> bytes;
+    SLF_TRY(world->w.save_snapshot(bytes));
+    *size = bytes.size();
+    if (!out) return SLF_OK;
+    if (capacity < bytes.size()) return fail(SLF_ERR_INVALID_ARGUMENT, "snapshot buffer too small");
+    std::memcpy(out, bytes.data(), bytes.size());
+    return SLF_OK;
+}
+
+int32_t slf_load_snapshot(const uint8_t* data, uint64_t size, const slf_settings* library, slf_world** out) {
+    SLF_NEED(out);
+    *out = nullptr;
+    if (size) SLF_NEED(data);
+    slf_settings lib;
+    slf_settings_default(&lib);
+    if (library) lib = *library;
+    if (lib.warm_start) return fail(SLF_ERR_UNSUPPORTED, "only cold starts are built");
+    if (lib.arithmetic != SLF_ARITHMETIC_EXACT && lib.arithmetic != SLF_ARITHMETIC_FAST)
+        return fail(SLF_ERR_INVALID_SETTINGS, "unknown arithmetic");
+    if (lib.positions != SLF_POSITIONS_ABSOLUTE && lib.positions != SLF_POSITIONS_CELL_RELATIVE)
+        return fail(SLF_ERR_INVALID_SETTINGS, "unknown positions");
+    if (lib.positions == SLF_POSITIONS_CELL_RELATIVE && lib.arithmetic != SLF_ARITHMETIC_FAST)
+        return fail(SLF_ERR_UNSUPPORTED, "cell-relative positions run with FAST arithmetic only");
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) return fail(SLF_ERR_CUDA, "no CUDA device");
+    if (lib.device < 0 || lib.device >= devices) return fail(SLF_ERR_INVALID_SETTINGS, "no such CUDA device");
+    if (cudaSetDevice(lib.device) != cudaSuccess) return fail(SLF_ERR_CUDA, "cannot select the CUDA device");
+    auto h = std::make_unique<slf_world>();
+    int32_t st = h->w.load_snapshot(data, size_t(size), lib);
+    if (st != SLF_OK) return st;
+    *out = h.release();
     return SLF_OK;
 }
 

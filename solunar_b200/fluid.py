@@ -54,6 +54,9 @@ def load_library():
         "slf_add_wall": [vp, fp, fp, u32p],
         "slf_remove_boundary": [vp, ctypes.c_uint32, i32p],
         "slf_add_emitter": [vp, fp, fp, fp, u32p],
+        "slf_save_snapshot": [vp, ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, u64p],
+        "slf_load_snapshot": [ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, ctypes.POINTER(CSettings),
+                              ctypes.POINTER(vp)],
         "slf_add_drain": [vp, fp, fp, u32p],
         "slf_remove_flow": [vp, ctypes.c_uint32, i32p],
         "slf_wall_count": [vp, u64p],
@@ -122,6 +125,29 @@ class FluidWorld:
         self._h = h
 
     new = classmethod(lambda cls, settings=None: cls(settings))
+
+    # ---- snapshots (src/fluid/save.rs) ----
+    @classmethod
+    def load_snapshot(cls, data: bytes, settings: FluidSettings | None = None) -> "FluidWorld":
+        """FluidWorld::load_snapshot (save.rs:79-181).  `settings` supplies only the library's
+        own fields (arithmetic, positions, solver limits, device); the snapshot holds the rest."""
+        L = load_library()
+        buf = (ctypes.c_uint8 * max(len(data), 1)).from_buffer_copy(bytes(data) or b"\0")
+        c = (settings or FluidSettings()).to_c()
+        h = ctypes.c_void_p()
+        _check(L.slf_load_snapshot(buf, len(data), ctypes.byref(c), ctypes.byref(h)))
+        self = cls.__new__(cls)
+        self._h = h
+        self._settings = self.settings()
+        return self
+
+    def save_snapshot(self) -> bytes:
+        """FluidWorld::save_snapshot (save.rs:18-73): SLFL version 3 bytes."""
+        size = ctypes.c_uint64()
+        _check(_lib.slf_save_snapshot(self._h, None, 0, ctypes.byref(size)))
+        buf = (ctypes.c_uint8 * max(size.value, 1))()
+        _check(_lib.slf_save_snapshot(self._h, buf, size.value, ctypes.byref(size)))
+        return bytes(buf[: size.value])
 
     def close(self):
         h = getattr(self, "_h", None)
