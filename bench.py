@@ -243,14 +243,8 @@ def main():
             dist.barrier(device_ids=[local_rank])
         torch.cuda.synchronize()
 
-    def max_over_ranks(x: float) -> float:
-        if world_size == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     from solunar_b200 import fluid
+    from solunar_b200.replicas import reduce_timing
 
     sc = scene_of(args.scene, args.arithmetic, args.positions)
     sc.settings.device = local_rank
@@ -289,8 +283,7 @@ def main():
     prof = world.profile_read()
     world.profile(False)
 
-    total_ms = max_over_ranks(sum(times_ms))
-    all_substeps = substeps * world_size
+    all_substeps, total_ms = reduce_timing(substeps, sum(times_ms), world_size, dev)
     value = all_substeps / (total_ms / 1e3)
 
     # roofline of the kernel with the largest share of device time
@@ -335,8 +328,8 @@ def main():
         e2e_ms += e0.elapsed_time(e1)
         e2e_substeps += r.substeps
     barrier()
-    e2e_ms = max_over_ranks(e2e_ms)
-    e2e = {"value": e2e_substeps * world_size / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+    e2e_all, e2e_ms = reduce_timing(e2e_substeps, e2e_ms, world_size, dev)
+    e2e = {"value": e2e_all / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 24 * n,
            "d2h_bytes_per_step": 24 * n}
 
     # forward + adjoint (step_backward) on the same world: a taped forward of K steps (each
@@ -384,15 +377,16 @@ def main():
         e3.synchronize()
         bwd_ms = e2.elapsed_time(e3)
         world.tape_end()
-        fwd_ms = max_over_ranks(fwd_ms)
-        bwd_ms = max_over_ranks(bwd_ms)
+        adj_all, both_ms = reduce_timing(adj_substeps, fwd_ms + bwd_ms, world_size, dev)
+        _, fwd_ms = reduce_timing(adj_substeps, fwd_ms, world_size, dev)
+        bwd_ms = both_ms - fwd_ms
         finite = bool(np.isfinite(dv0).all() and np.isfinite(dp0).all())
-        adjoint = {"value": adj_substeps * world_size / ((fwd_ms + bwd_ms) / 1e3), "unit": UNIT,
+        adjoint = {"value": adj_all / (both_ms / 1e3), "unit": UNIT,
                    "gradients_finite": finite,
                    "steps": k, "substeps": adj_substeps, "checkpoint_every": every,
                    "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                    "ratio_to_forward": (fwd_ms + bwd_ms) / fwd_ms,
-                   "ratio_to_plain_substeps": value / (adj_substeps * world_size / ((fwd_ms + bwd_ms) / 1e3)),
+                   "ratio_to_plain_substeps": value / (adj_all / (both_ms / 1e3)),
                    "loss": "kinetic energy of the water beyond x = 1 m after the steps",
                    "grad_viscosity": grads["viscosity"], "grad_gravity": list(grads["gravity"]),
                    "grad_uniform_inflow": [float(x) for x in dv0.astype(np.float64).sum(axis=0)]}
