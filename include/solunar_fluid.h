@@ -160,6 +160,17 @@ int32_t slf_save_snapshot(slf_world* world, uint8_t* out, uint64_t capacity, uin
  * in the snapshot return SLF_ERR_UNSUPPORTED. */
 int32_t slf_load_snapshot(const uint8_t* data, uint64_t size, const slf_settings* library, slf_world** out);
 
+/* The node lattice of a terrain region over [low, high] (terrain.rs:275-283): nodes[a] nodes along
+ * axis a, spacing / 2 apart from `low`.  SLF_ERR_FLUID_FULL above 2^24 nodes. */
+int32_t slf_terrain_nodes(const slf_world* world, const float low[3], const float high[3], uint64_t nodes[3]);
+/* FluidWorld::add_terrain (terrain.rs:262-302): ground under a signed distance field (positive in
+ * the open) inside the box.  The reference samples an SDF volume at the nodes; here the caller
+ * passes those samples: distances[(y * nodes[2] + z) * nodes[0] + x] at low + (x, y, z) spacing/2,
+ * count = the number of nodes.  WCSPH worlds with EXACT arithmetic; a DFSPH step with terrain
+ * fails with SLF_ERR_INVALID_SETTINGS, as in the reference.  Removed by slf_remove_boundary. */
+int32_t slf_add_terrain(slf_world* world, const float low[3], const float high[3], const float* distances,
+                        uint64_t count, uint32_t* boundary_out);
+
 /* FluidWorld::add_emitter (flow.rs:86-99): after each step every lattice slot of the box with
  * no water within 0.9 spacing of its centre gets a particle moving at `velocity`.  Boxes of more
  * than 2^30 slots are refused when the step runs them (SLF_ERR_OUT_OF_RANGE). */

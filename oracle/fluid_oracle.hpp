@@ -21,6 +21,9 @@
 //                         check_box :230-238, union :240-247
 //   src/fluid/flow.rs     CLEAR_SHARE :7, add_emitter :86-99, add_drain :104-106,
 //                         remove_flow :109-113, add_flow :115-139, run_flows :144-231
+//   src/fluid/terrain.rs  TerrainField read :100-136, sample :139-142, ground :144-171,
+//                         GroundSites :176-245, solid :248-250, add_terrain :262-302 (the caller
+//                         samples the distance field), ground_near :305-310, terrain_contact :314-333
 //   src/fluid/save.rs     save_snapshot :18-73, load_snapshot :79-181 (Walls::save/load
 //                         boundary.rs:182-227, Flows::save/load flow.rs:36-83)
 //   src/snapshot/bytes.rs fnv1a :6-13, Writer :15-67, Reader :89-157
@@ -34,8 +37,8 @@
 // length.  Parity with the Rust binary itself is therefore unpinned at the bit level; the
 // reference's own tests (property tests, no stored vectors) pin this restatement instead.
 //
-// Movers (rigid coupling) and terrain are not on the path: they are absent from this
-// restatement, as they are empty in every configuration it is run on.
+// Movers (rigid coupling) are not on the path: they are absent from this restatement, as they
+// are empty in every configuration it is run on.
 #pragma once
 
 #include <algorithm>
@@ -377,6 +380,21 @@ template <class R> class World {
     };
     std::vector<Flow> flows;
     uint32_t flow_next = 0;
+    // terrain regions (terrain.rs:36-42) and what ground does to a particle (terrain.rs:176-186)
+    struct Terrain {
+        uint32_t owner;
+        Vec low;
+        size_t nx, ny, nz;
+        R step;
+        std::vector<R> distances;
+    };
+    std::vector<Terrain> terrains;
+    struct GroundSites {
+        R spacing{0}, reach{0}, low{0}, step{0};
+        std::vector<Vec> offsets;
+        std::vector<R> weights, fars, damping;
+    } sites;
+    std::vector<Vec> ground_slopes;  // mod.rs:320-322: empty without terrains
     // per-pair gradient caches of the last DFSPH substep (dfsph.rs:24-41)
     std::vector<Vec> grad_fluid, grad_walls;
     // solver iteration counts of the last DFSPH substep: divergence, density
@@ -389,6 +407,177 @@ template <class R> class World {
         out.settings = s;
         out.kernel = Kernel<R>(radius_of(s));
         out.mass = rest_mass(s);
+        out.build_ground_sites();
+        return OK;
+    }
+
+    static constexpr size_t kMaxTerrainNodes = size_t(1) << 24;  // terrain.rs:9
+    static constexpr int kMapSamples = 256;                      // terrain.rs:11
+
+    // GroundSites::new (terrain.rs:188-238)
+    void build_ground_sites() {
+        const R spacing = R(settings.spacing), r = radius();
+        GroundSites g;
+        g.spacing = spacing;
+        int reach = int(std::ceil(r / spacing));
+        for (int z = -reach; z <= reach; ++z)
+            for (int y = -reach; y <= reach; ++y)
+                for (int x = -reach; x <= reach; ++x) {
+                    Vec offset = Vec(R(x), R(y), R(z)) * spacing;
+                    R far = length(offset);
+                    if (far < r) {
+                        g.offsets.push_back(offset);
+                        g.weights.push_back(mass * kernel.value(far));
+                        g.fars.push_back(far);
+                    }
+                }
+        g.low = -spacing / R(2);
+        g.step = (r - g.low) / R(kMapSamples - 1);
+        R soften = R(0.01f) * r * r;
+        int across_reach = reach + 1;
+        for (int sample = 0; sample < kMapSamples; ++sample) {
+            R distance = g.low + g.step * R(sample);
+            R weight = R(0);
+            for (int layer = 0;; ++layer) {
+                R depth = distance + spacing * (R(layer) + R(0.5));
+                if (depth >= r) break;
+                for (int a = -across_reach; a <= across_reach; ++a)
+                    for (int b = -across_reach; b <= across_reach; ++b) {
+                        R across = R(a * a + b * b) * spacing * spacing;
+                        R squared = across + depth * depth;
+                        R far = std::sqrt(squared);
+                        if (far >= r || far <= R(0)) continue;
+                        weight += mass * depth * depth * -kernel.slope(far) / (far * (squared + soften));
+                    }
+            }
+            g.damping.push_back(weight);
+        }
+        g.reach = r + spacing / R(2);
+        sites = std::move(g);
+    }
+
+    // GroundSites::damping (terrain.rs:241-249)
+    R damping(R distance) const {
+        R at = (rmax(distance, sites.low) - sites.low) / sites.step;
+        size_t below = size_t(std::floor(at));
+        if (below + 1 >= size_t(kMapSamples)) return R(0);
+        R part = at - R(below);
+        return sites.damping[below] + (sites.damping[below + 1] - sites.damping[below]) * part;
+    }
+
+    // TerrainField::read (terrain.rs:100-136): trilinear value and its change per axis
+    bool terrain_read(const Terrain& t, Vec point, R& value, Vec& change) const {
+        Vec local = (point - t.low) / t.step;
+        auto inside = [](R v, size_t nodes) { return v >= R(0) && v <= R(nodes - 1); };
+        if (!(inside(local.x, t.nx) && inside(local.y, t.ny) && inside(local.z, t.nz))) return false;
+        auto base = [](R v, size_t nodes) { return std::min(size_t(std::floor(v)), nodes - 2); };
+        size_t x = base(local.x, t.nx), y = base(local.y, t.ny), z = base(local.z, t.nz);
+        R fx = local.x - R(x), fy = local.y - R(y), fz = local.z - R(z);
+        auto corner = [&](size_t dx, size_t dy, size_t dz) {
+            return t.distances[((y + dy) * t.nz + (z + dz)) * t.nx + (x + dx)];
+        };
+        auto lerp = [](R a, R b, R u) { return a + (b - a) * u; };
+        auto face = [&](size_t dy, size_t dz, R& v, R& g) {
+            R a = corner(0, dy, dz), b = corner(1, dy, dz);
+            v = lerp(a, b, fx);
+            g = b - a;
+        };
+        R v00, g00, v10, g10, v01, g01, v11, g11;
+        face(0, 0, v00, g00);
+        face(1, 0, v10, g10);
+        face(0, 1, v01, g01);
+        face(1, 1, v11, g11);
+        R v0 = lerp(v00, v10, fy), v1 = lerp(v01, v11, fy);
+        value = lerp(v0, v1, fz);
+        change = Vec(lerp(lerp(g00, g10, fy), lerp(g01, g11, fy), fz), lerp(v10 - v00, v11 - v01, fz), v1 - v0) / t.step;
+        return true;
+    }
+
+    // TerrainField::sample (terrain.rs:139-142)
+    bool terrain_sample(const Terrain& t, Vec point, R& distance, Vec& normal) const {
+        Vec change;
+        if (!terrain_read(t, point, distance, change)) return false;
+        normal = normalize_or(change, Vec(R(0), R(1), R(0)));
+        return true;
+    }
+
+    // solid (terrain.rs:248-250)
+    static R solid(R distance, R size) {
+        R v = R(0.5) - distance / size;
+        return v < R(0) ? R(0) : (v > R(1) ? R(1) : v);
+    }
+
+    // TerrainField::ground (terrain.rs:144-171): false outside the region
+    bool terrain_ground(const Terrain& t, Vec point, R& distance, Vec& normal, R& density, Vec& gradient) const {
+        Vec change;
+        if (!terrain_read(t, point, distance, change)) return false;
+        density = R(0);
+        gradient = Vec();
+        if (distance < sites.reach) {
+            R open = distance - sites.spacing / R(2);
+            for (size_t k = 0; k < sites.offsets.size(); ++k) {
+                if (sites.fars[k] <= open) continue;
+                R there;
+                Vec toward;
+                if (!terrain_read(t, point + sites.offsets[k], there, toward)) continue;
+                R share = solid(there, sites.spacing);
+                density += sites.weights[k] * share;
+                if (share > R(0) && share < R(1)) gradient = gradient - toward * (sites.weights[k] / sites.spacing);
+            }
+        }
+        normal = normalize_or(change, Vec(R(0), R(1), R(0)));
+        return true;
+    }
+
+    // terrain_contact (terrain.rs:314-333): true when the particle got under a surface
+    bool terrain_contact(R rest, Vec& at, Vec& velocity) const {
+        bool under = false;
+        for (const Terrain& t : terrains) {
+            R distance;
+            Vec normal;
+            if (!terrain_sample(t, at, distance, normal)) continue;
+            if (distance < rest) {
+                under = under || distance < R(0);
+                at = at + normal * (rest - distance);
+                R into = dot(velocity, normal);
+                if (into < R(0)) velocity = velocity - normal * into;
+            }
+        }
+        return under;
+    }
+
+    // add_terrain's node lattice (terrain.rs:275-283): step spacing/2, nodes per axis
+    Status terrain_nodes(Vec low, Vec high, size_t nodes[3]) const {
+        if (!is_finite(low) || !is_finite(high)) return NON_FINITE;
+        if (high.x <= low.x || high.y <= low.y || high.z <= low.z) return OUT_OF_RANGE;
+        R step = R(settings.spacing) / R(2);
+        auto count = [&](R extent) { return size_t(rmin(std::ceil(extent / step), R(1e7))) + 1; };
+        Vec size = high - low;
+        nodes[0] = count(size.x);
+        nodes[1] = count(size.y);
+        nodes[2] = count(size.z);
+        unsigned __int128 total = (unsigned __int128)nodes[0] * nodes[1] * nodes[2];
+        if (total > kMaxTerrainNodes) return FLUID_FULL;
+        return OK;
+    }
+
+    // add_terrain (terrain.rs:262-302) with the distances the caller sampled at the nodes
+    // low + (x, y, z) spacing/2, in (y, z, x) order, x fastest
+    Status add_terrain(Vec low, Vec high, const float* distances, size_t count, uint32_t* id_out) {
+        size_t nodes[3];
+        Status st = terrain_nodes(low, high, nodes);
+        if (st != OK) return st;
+        if (count != nodes[0] * nodes[1] * nodes[2]) return INVALID_ARGUMENT;
+        Terrain t;
+        t.low = low;
+        t.nx = nodes[0];
+        t.ny = nodes[1];
+        t.nz = nodes[2];
+        t.step = R(settings.spacing) / R(2);
+        t.distances.assign(distances, distances + count);
+        t.owner = add_wall_points({});
+        terrains.push_back(std::move(t));
+        if (id_out) *id_out = terrains.back().owner;
         return OK;
     }
 
@@ -715,7 +904,10 @@ template <class R> class World {
         }
         walls.containers = rest;
         update_bounds();
-        bool gone = walls.positions.size() != before || had_container;
+        size_t regions = terrains.size();
+        terrains.erase(std::remove_if(terrains.begin(), terrains.end(), [&](const Terrain& t) { return t.owner == id; }),
+                       terrains.end());
+        bool gone = walls.positions.size() != before || had_container || terrains.size() != regions;
         if (gone) settle_walls();
         return gone;
     }
@@ -876,6 +1068,7 @@ template <class R> class World {
         if (neighbors.start.size() != len() + 1) return OUT_OF_RANGE;
         size_t n = len();
         std::vector<R> out(n);
+        std::vector<Vec> slopes(terrains.empty() ? 0 : n);
 #pragma omp parallel for schedule(static) num_threads(nthreads())
         for (long long ii = 0; ii < (long long)n; ++ii) {
             size_t i = size_t(ii);
@@ -886,9 +1079,21 @@ template <class R> class World {
             R wsum = R(0);
             for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
                 wsum += kernel.value(length(walls.positions[wall_neighbors.items[k]] - at));
-            out[i] = mass * (sum + wsum);
+            // ground_near (mod.rs:657-663): each region holding the particle adds its ground
+            R ground = R(0);
+            Vec slope;
+            for (const Terrain& t : terrains) {
+                R distance, density;
+                Vec normal, gradient;
+                if (!terrain_ground(t, at, distance, normal, density, gradient)) continue;
+                ground = ground + density;
+                slope = slope + gradient;
+            }
+            out[i] = mass * (sum + wsum + R(0)) + ground;
+            if (!terrains.empty()) slopes[i] = slope;
         }
         densities = std::move(out);
+        ground_slopes = terrains.empty() ? std::vector<Vec>() : std::move(slopes);
         return OK;
     }
 
@@ -966,7 +1171,18 @@ template <class R> class World {
         }
         o.u32(flow_next);
         o.u32(0);  // coupled bodies
-        o.u32(0);  // terrain regions
+        // TerrainField::save (terrain.rs:44-55)
+        o.u32(uint32_t(terrains.size()));
+        for (auto& t : terrains) {
+            o.u32(t.owner);
+            o.v3(t.low);
+            o.u32(uint32_t(t.nx));
+            o.u32(uint32_t(t.ny));
+            o.u32(uint32_t(t.nz));
+            o.f32(float(t.step));
+            o.u32(uint32_t(t.distances.size()));
+            for (R d : t.distances) o.f32(float(d));
+        }
         o.u8(has_domain ? 1 : 0);
         if (has_domain) {
             o.v3(domain_low);
@@ -1122,7 +1338,32 @@ template <class R> class World {
         if (!r.count(12, 1 << 16, coupled)) return SNAPSHOT;
         if (coupled) return UNSUPPORTED;
         if (!r.count(32, 1 << 16, terrains)) return SNAPSHOT;
-        if (terrains) return UNSUPPORTED;
+        // TerrainField::load (terrain.rs:57-97)
+        for (size_t k = 0; k < terrains; ++k) {
+            Terrain t;
+            uint32_t nx, ny, nz;
+            float step;
+            size_t count;
+            if (!(r.u32(t.owner) && r.v3(t.low) && r.u32(nx) && r.u32(ny) && r.u32(nz) && r.f32(step) &&
+                  r.count(4, kMaxTerrainNodes, count)))
+                return SNAPSHOT;
+            unsigned __int128 total = (unsigned __int128)nx * ny * nz;
+            if (!is_finite(t.low) || !std::isfinite(step) || step <= 0.0f || nx < 2 || ny < 2 || nz < 2 ||
+                total != count)
+                return bad("invalid snapshot: fluid terrain");
+            t.nx = nx;
+            t.ny = ny;
+            t.nz = nz;
+            t.step = R(step);
+            for (size_t i = 0; i < count; ++i) {
+                float d;
+                if (!r.f32(d)) return SNAPSHOT;
+                if (!std::isfinite(d)) return bad("invalid snapshot: fluid terrain distance");
+                t.distances.push_back(R(d));
+            }
+            if (t.owner >= w.walls.next) return bad("invalid snapshot: fluid terrain owner");
+            w.terrains.push_back(std::move(t));
+        }
         if (version >= 2) {
             uint8_t flag;
             if (!r.u8(flag)) return SNAPSHOT;
@@ -1197,7 +1438,7 @@ template <class R> class World {
         return rmin(R(settings.viscosity) * R(settings.sound_speed) * r, R(0.05f) * r * r / dt);
     }
 
-    // step.rs:262-301 (no terrains)
+    // step.rs:262-301
     Vec wall_viscous(size_t index, R dt) const {
         R r = radius();
         R soften = R(0.01f) * r * r;
@@ -1212,6 +1453,16 @@ template <class R> class World {
         Vec normal = normalize_or(away, Vec());
         Vec into = normal * rmin(dot(velocity, normal), R(0));
         R wall_visc = rmin(R(1) * R(settings.sound_speed) * r, R(0.25f) * stable);
+        for (const Terrain& t : terrains) {
+            R distance;
+            Vec n;
+            if (!terrain_sample(t, at, distance, n)) continue;
+            R towards = dot(velocity, n);
+            if (towards < R(0)) {
+                R weight = damping(distance);
+                push = push - n * (wall_visc * towards * weight / density);
+            }
+        }
         for (uint32_t k = wall_neighbors.start[index]; k < wall_neighbors.start[index + 1]; ++k) {
             Vec offset = at - walls.positions[wall_neighbors.items[k]];
             R toward = dot(into, offset);
@@ -1290,14 +1541,15 @@ template <class R> class World {
                 Vec offset = at - walls.positions[wall_neighbors.items[k]];
                 push = push - kernel.gradient(offset) * (mass * mirrored);
             }
+            if (i < ground_slopes.size()) push = push - ground_slopes[i] * mirrored;
             pushes[i] = push + wall_viscous(i, dt) + g;
         }
         for (size_t i = 0; i < n; ++i) velocities[i] = velocities[i] + pushes[i] * dt;
         return advance(dt, held);
     }
 
-    // step.rs:305-339 (no terrains).  A non-finite particle stops the pass there, as in the
-    // reference; earlier particles have moved.
+    // step.rs:305-339.  A non-finite particle stops the pass there, as in the reference; earlier
+    // particles have moved.
     Status advance(R dt, uint32_t& held) {
         held = 0;
         Vec rest = Vec::splat(R(settings.spacing) / R(2));
@@ -1316,6 +1568,7 @@ template <class R> class World {
                     next = inside;
                 }
             }
+            if (terrain_contact(rest.x, next, velocity)) held += 1;
             if (!is_finite(next) || !is_finite(velocity)) return NON_FINITE;
             at = next;
         }
@@ -1326,6 +1579,8 @@ template <class R> class World {
 
     // dfsph.rs:46-77
     Status dfsph(R dt, Report& report) {
+        // dfsph.rs:52-55: ground pushes through the weakly compressible solver's pressure only
+        if (!terrains.empty()) return INVALID_SETTINGS;
         R spacing = R(settings.spacing);
         R courant = R(settings.courant);
         R pull = length(gravity());

@@ -211,6 +211,48 @@ int32_t orc_run_flows(void* p, uint32_t* emitted, uint32_t* drained) {
     return st;
 }
 
+int32_t orc_terrain_nodes(void* p, const float* low, const float* high, uint64_t* nodes) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    size_t nd[3] = {0, 0, 0};
+    ORC_DISPATCH(h, st = w.terrain_nodes(v3<R>(low), v3<R>(high), nd));
+    for (int a = 0; a < 3; ++a) nodes[a] = nd[a];
+    return st;
+}
+
+int32_t orc_add_terrain(void* p, const float* low, const float* high, const float* distances, uint64_t count,
+                        uint32_t* id) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.add_terrain(v3<R>(low), v3<R>(high), distances, size_t(count), id));
+    return st;
+}
+
+// Probes of one terrain region (the reference's unit tests read them): the field's distance and
+// way out at a point, and the ground a particle there sees.  *inside = 0 outside the region.
+int32_t orc_terrain_probe(void* p, uint32_t region, const float* point, double* distance, double* normal,
+                          double* density, double* gradient, int32_t* inside) {
+    auto* h = static_cast<Handle*>(p);
+    int32_t st = OK;
+    ORC_DISPATCH(h, {
+        if (region >= w.terrains.size()) {
+            st = INVALID_ARGUMENT;
+        } else {
+            R d, rho;
+            V3<R> n, g;
+            bool in = w.terrain_ground(w.terrains[region], v3<R>(point), d, n, rho, g);
+            *inside = in ? 1 : 0;
+            if (in) {
+                *distance = double(d);
+                normal[0] = double(n.x), normal[1] = double(n.y), normal[2] = double(n.z);
+                *density = double(rho);
+                gradient[0] = double(g.x), gradient[1] = double(g.y), gradient[2] = double(g.z);
+            }
+        }
+    });
+    return st;
+}
+
 static std::string g_snapshot_message;
 
 int32_t orc_save_snapshot(void* p, uint8_t* out, uint64_t capacity, uint64_t* size) {

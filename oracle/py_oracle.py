@@ -60,6 +60,9 @@ def lib():
             "orc_save_snapshot": [vp, ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, u64p],
             "orc_load_snapshot": [ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, ctypes.POINTER(CSettings),
                                   ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(vp)],
+            "orc_terrain_nodes": [vp, f3, f3, u64p],
+            "orc_add_terrain": [vp, f3, f3, f3, ctypes.c_uint64, u32p],
+            "orc_terrain_probe": [vp, ctypes.c_uint32, f3, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_int32)],
             "orc_wall_count": [vp, u64p],
             "orc_read_wall_positions": [vp, dp, ctypes.c_uint64],
             "orc_step": [vp, ctypes.c_float, ctypes.POINTER(CReport)],
@@ -202,6 +205,29 @@ class OracleWorld:
         r = ctypes.c_int32()
         _check(lib().orc_remove_boundary(self._h, boundary, ctypes.byref(r)))
         return bool(r.value)
+
+    # ---- terrain (terrain.rs) ----
+    def terrain_nodes(self, low, high):
+        n = (ctypes.c_uint64 * 3)()
+        _check(lib().orc_terrain_nodes(self._h, vec3(low), vec3(high), n))
+        return tuple(int(v) for v in n)
+
+    def add_terrain(self, low, high, distances) -> int:
+        d = np.ascontiguousarray(distances, dtype=np.float32).ravel()
+        i = ctypes.c_uint32()
+        _check(lib().orc_add_terrain(self._h, vec3(low), vec3(high), _ptr(d, ctypes.c_float), d.size, ctypes.byref(i)))
+        return i.value
+
+    def terrain_probe(self, region: int, point):
+        """(distance, normal, ground density, ground gradient) at `point`, or None outside."""
+        d, rho = ctypes.c_double(), ctypes.c_double()
+        nrm, grad = (ctypes.c_double * 3)(), (ctypes.c_double * 3)()
+        inside = ctypes.c_int32()
+        _check(lib().orc_terrain_probe(self._h, region, vec3(point), ctypes.byref(d), nrm, ctypes.byref(rho), grad,
+                                       ctypes.byref(inside)))
+        if not inside.value:
+            return None
+        return d.value, np.array(nrm[:]), rho.value, np.array(grad[:])
 
     # ---- emitters and drains (flow.rs:86-139) ----
     def add_emitter(self, low, high, velocity) -> int:

@@ -102,6 +102,28 @@ struct PairLists {
 #endif
 };
 
+// Terrain regions (src/fluid/terrain.rs): signed distances at nodes `step` apart from `low`, index
+// (y * nz + z) * nx + x, `offset` into the shared distance array; and the ground sites, the
+// water's lattice within the kernel around a particle with the density each site adds.
+struct TerrainRegion {
+    float lx, ly, lz;
+    float step;
+    uint32_t nx, ny, nz;
+    uint32_t pad;
+    unsigned long long offset;
+};
+struct TerrainDev {
+    uint32_t regions;              // 0: no terrain (every term below is skipped)
+    uint32_t sites;
+    const TerrainRegion* region;
+    const float* dist;
+    const float4* site;            // offset xyz, density weight
+    const float* far;              // |offset|
+    const float* damping;          // kGroundSamples weights from `low` in steps of `step`
+    float spacing, reach, low, step;
+};
+constexpr int kGroundSamples = 256;
+
 // Slots of the adjoint's FP64 parameter-gradient accumulators.
 enum GradSlot { kGradViscosity = 0, kGradWallViscosity = 1, kGradStiffness = 2, kGradGravity = 3, kGradSlots = 6 };
 

@@ -221,6 +221,99 @@ __global__ void k_scan_add(uint32_t* data, uint32_t m, const uint32_t* __restric
     if (blockIdx.x == 0 && threadIdx.x == 0) data[m] = tile_sums[gridDim.x];
 }
 
+// ---- terrain (src/fluid/terrain.rs) ------------------------------------------------------------
+
+// TerrainField::read (terrain.rs:100-136): the trilinear distance at a point and its change per
+// axis; false outside the region.
+__device__ __forceinline__ bool terrain_read(const TerrainDev& T, const TerrainRegion& t, float px, float py,
+                                             float pz, float& value, float3& change) {
+    float lx = (px - t.lx) / t.step, ly = (py - t.ly) / t.step, lz = (pz - t.lz) / t.step;
+    if (!(lx >= 0.0f && lx <= float(t.nx - 1) && ly >= 0.0f && ly <= float(t.ny - 1) && lz >= 0.0f &&
+          lz <= float(t.nz - 1)))
+        return false;
+    uint32_t x = min(uint32_t(floorf(lx)), t.nx - 2), y = min(uint32_t(floorf(ly)), t.ny - 2),
+             z = min(uint32_t(floorf(lz)), t.nz - 2);
+    float fx = lx - float(x), fy = ly - float(y), fz = lz - float(z);
+    const float* d = T.dist + t.offset;
+    auto corner = [&](uint32_t dx, uint32_t dy, uint32_t dz) {
+        return __ldg(&d[(size_t(y + dy) * t.nz + (z + dz)) * t.nx + (x + dx)]);
+    };
+    auto lerp = [](float a, float b, float u) { return a + (b - a) * u; };
+    float a00 = corner(0, 0, 0), b00 = corner(1, 0, 0), a10 = corner(0, 1, 0), b10 = corner(1, 1, 0);
+    float a01 = corner(0, 0, 1), b01 = corner(1, 0, 1), a11 = corner(0, 1, 1), b11 = corner(1, 1, 1);
+    float v00 = lerp(a00, b00, fx), g00 = b00 - a00;
+    float v10 = lerp(a10, b10, fx), g10 = b10 - a10;
+    float v01 = lerp(a01, b01, fx), g01 = b01 - a01;
+    float v11 = lerp(a11, b11, fx), g11 = b11 - a11;
+    float v0 = lerp(v00, v10, fy), v1 = lerp(v01, v11, fy);
+    value = lerp(v0, v1, fz);
+    change = make_float3(lerp(lerp(g00, g10, fy), lerp(g01, g11, fy), fz) / t.step,
+                         lerp(v10 - v00, v11 - v01, fz) / t.step, (v1 - v0) / t.step);
+    return true;
+}
+
+// normalize_or(Y) dividing by the length
+__device__ __forceinline__ float3 normalize_or_up(float3 c) {
+    float len = sqrtf(dot3(c.x, c.y, c.z, c.x, c.y, c.z));
+    if (isfinite(len) && len > 0.0f) return make_float3(c.x / len, c.y / len, c.z / len);
+    return make_float3(0.0f, 1.0f, 0.0f);
+}
+
+// TerrainField::sample (terrain.rs:139-142)
+__device__ __forceinline__ bool terrain_sample(const TerrainDev& T, const TerrainRegion& t, float px, float py,
+                                               float pz, float& distance, float3& normal) {
+    float3 change;
+    if (!terrain_read(T, t, px, py, pz, distance, change)) return false;
+    normal = normalize_or_up(change);
+    return true;
+}
+
+// ground_near (mod.rs:657-663, terrain.rs:144-171, 305-310): the density the terrain regions
+// holding the particle add, and the sum of their density gradients
+__device__ __forceinline__ float ground_near(const TerrainDev& T, float px, float py, float pz, float3& slope) {
+    float ground = 0.0f;
+    slope = make_float3(0.0f, 0.0f, 0.0f);
+    for (uint32_t r = 0; r < T.regions; ++r) {
+        const TerrainRegion& t = T.region[r];
+        float distance;
+        float3 change;
+        if (!terrain_read(T, t, px, py, pz, distance, change)) continue;
+        float density = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        if (distance < T.reach) {
+            float open = distance - T.spacing / 2.0f;
+            for (uint32_t k = 0; k < T.sites; ++k) {
+                if (__ldg(&T.far[k]) <= open) continue;  // a distance moves no faster than the point
+                float4 o = __ldg(&T.site[k]);
+                float there;
+                float3 toward;
+                if (!terrain_read(T, t, px + o.x, py + o.y, pz + o.z, there, toward)) continue;
+                float v = 0.5f - there / T.spacing;
+                float share = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);  // solid (terrain.rs:248-250)
+                density += o.w * share;
+                if (share > 0.0f && share < 1.0f) {
+                    float w = o.w / T.spacing;
+                    gx = gx - toward.x * w;
+                    gy = gy - toward.y * w;
+                    gz = gz - toward.z * w;
+                }
+            }
+        }
+        ground = ground + density;
+        slope = make_float3(slope.x + gx, slope.y + gy, slope.z + gz);
+    }
+    return ground;
+}
+
+// GroundSites::damping (terrain.rs:241-249)
+__device__ __forceinline__ float ground_damping(const TerrainDev& T, float distance) {
+    float at = (fmaxf(distance, T.low) - T.low) / T.step;
+    uint32_t below = uint32_t(floorf(at));
+    if (below + 1 >= uint32_t(kGroundSamples)) return 0.0f;
+    float part = at - float(below);
+    float d0 = __ldg(&T.damping[below]), d1 = __ldg(&T.damping[below + 1]);
+    return d0 + (d1 - d0) * part;
+}
+
 // ---- densities (mod.rs:621-675) and the substep's neighbour lists, with WCSPH pressure
 // (step.rs:147-172) or the DFSPH factors (dfsph.rs:108-163) --------------------------------
 
@@ -228,7 +321,8 @@ template <int SOLVER>
 __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDev wg, const float4* __restrict__ pos,
                                                     const float4* __restrict__ walls, PairLists fl, PairLists wl,
                                                     float* __restrict__ rho, float* __restrict__ press,
-                                                    float* __restrict__ scaled, float* __restrict__ alpha, Status* st) {
+                                                    float* __restrict__ scaled, float* __restrict__ alpha, Status* st,
+                                                    TerrainDev T, float4* __restrict__ slope) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     bool valid = i < p.n;
@@ -273,8 +367,12 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
         fl.count[row] = nf;
         wl.count[row] = nw;
         longest = nf > nw ? nf : nw;
-        float density = p.mass * (sum + wsum);
+        // mass (fluid + walls + movers, none here) + ground (mod.rs:657-663)
+        float3 gslope;
+        float ground = T.regions ? ground_near(T, a.x, a.y, a.z, gslope) : 0.0f;
+        float density = p.mass * (sum + wsum + 0.0f) + ground;
         rho[i] = density;
+        if (slope) slope[i] = make_float4(gslope.x, gslope.y, gslope.z, 0.0f);
         if (SOLVER == 0) {
             float ratio = fminf(density / p.rest, 1.1f);
             float pressure = fmaxf(p.stiffness * (pow7(ratio) - 1.0f), 0.0f);
@@ -386,12 +484,12 @@ __device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, con
     each_listed2_from(l, i, FromGlobal{pts, more}, f);
 }
 
-// ---- wall viscosity (step.rs:262-301, no terrains) ---------------------------------------
+// ---- wall viscosity (step.rs:262-301) -----------------------------------------------------
 
 __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc, const PairLists& wl,
                                                const float4* __restrict__ walls, uint32_t row, float4 a, float4 v,
-                                               float density) {
-    if (wl.count[row] == 0) return make_float3(0.0f, 0.0f, 0.0f);
+                                               float density, const TerrainDev& T) {
+    if (wl.count[row] == 0 && T.regions == 0) return make_float3(0.0f, 0.0f, 0.0f);
     float awx = 0.0f, awy = 0.0f, awz = 0.0f;
     each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
@@ -410,6 +508,20 @@ __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc,
     float k = fminf(dot3(v.x, v.y, v.z, nx, ny, nz), 0.0f);
     float ix = nx * k, iy = ny * k, iz = nz * k;
     float px = 0.0f, py = 0.0f, pz = 0.0f;
+    // the ground damps the velocity into it by the weight of frozen water at that distance
+    for (uint32_t r = 0; r < T.regions; ++r) {
+        float distance;
+        float3 gn;
+        if (!terrain_sample(T, T.region[r], a.x, a.y, a.z, distance, gn)) continue;
+        float into = dot3(v.x, v.y, v.z, gn.x, gn.y, gn.z);
+        if (into < 0.0f) {
+            float weight = ground_damping(T, distance);
+            float c = wall_visc * into * weight / density;
+            px = px - gn.x * c;
+            py = py - gn.y * c;
+            pz = pz - gn.z * c;
+        }
+    }
     each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
         float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
         float toward = dot3(ix, iy, iz, rx, ry, rz);
@@ -425,10 +537,36 @@ __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc,
     return make_float3(px, py, pz);
 }
 
-// ---- advance (step.rs:305-339, no terrains) -------------------------------------------------
+// ---- advance (step.rs:305-339) --------------------------------------------------------------
+
+// terrain_contact (terrain.rs:314-333): a particle nearer a surface than `rest` goes back there,
+// its velocity into the surface removed; true when it got under a surface.
+__device__ __forceinline__ bool terrain_contact(const TerrainDev& T, float rest, float& nx, float& ny, float& nz,
+                                                float4& v) {
+    bool under = false;
+    for (uint32_t r = 0; r < T.regions; ++r) {
+        float distance;
+        float3 gn;
+        if (!terrain_sample(T, T.region[r], nx, ny, nz, distance, gn)) continue;
+        if (distance < rest) {
+            under = under || distance < 0.0f;
+            float lift = rest - distance;
+            nx = nx + gn.x * lift;
+            ny = ny + gn.y * lift;
+            nz = nz + gn.z * lift;
+            float into = dot3(v.x, v.y, v.z, gn.x, gn.y, gn.z);
+            if (into < 0.0f) {
+                v.x = v.x - gn.x * into;
+                v.y = v.y - gn.y * into;
+                v.z = v.z - gn.z * into;
+            }
+        }
+    }
+    return under;
+}
 
 __device__ __forceinline__ void advance_one(const Params& p, float dt, float4& a, float4& v, uint32_t& held,
-                                            uint32_t& bad) {
+                                            uint32_t& bad, const TerrainDev& T) {
     float nx = a.x + v.x * dt, ny = a.y + v.y * dt, nz = a.z + v.z * dt;
     if (p.has_bounds) {
         float ix = fminf(fmaxf(nx, p.low_in.x), p.high_in.x);
@@ -447,6 +585,7 @@ __device__ __forceinline__ void advance_one(const Params& p, float dt, float4& a
             nz = iz;
         }
     }
+    if (T.regions && terrain_contact(T, p.spacing / 2.0f, nx, ny, nz, v)) held += 1;
     if (!(isfinite(nx) && isfinite(ny) && isfinite(nz) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) bad = 1;
     a.x = nx;
     a.y = ny;
@@ -462,7 +601,8 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
                                                         const float* __restrict__ scaled,
                                                         const float4* __restrict__ walls, float4* __restrict__ pos_out,
                                                         float4* __restrict__ vel_out, Status* st,
-                                                        float4* __restrict__ vel_pre) {
+                                                        float4* __restrict__ vel_pre, TerrainDev T,
+                                                        const float4* __restrict__ slope) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     bool valid = i < p.n;
@@ -498,13 +638,19 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
             py = py - (ry * g) * s;
             pz = pz - (rz * g) * s;
         });
-        float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, row, a, v, density);
+        if (slope) {  // the ground pushes back with this particle's own pressure (step.rs:203-205)
+            float4 sl = slope[i];
+            px = px - sl.x * mirrored;
+            py = py - sl.y * mirrored;
+            pz = pz - sl.z * mirrored;
+        }
+        float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, row, a, v, density, T);
         float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
         v.x = v.x + ax * dt;
         v.y = v.y + ay * dt;
         v.z = v.z + az * dt;
         float4 pre = v;
-        advance_one(p, dt, a, v, held, bad);
+        advance_one(p, dt, a, v, held, bad, T);
         if (vel_pre) {
             // the velocity before the wall zeroed any component, and which ones it zeroed
             uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
@@ -660,7 +806,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params 
             pz = pz - (rz * g) * s;
         }
     });
-    float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, row, a, v, density);
+    float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, row, a, v, density, TerrainDev{});
     float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
     v.x = v.x + ax * dt;
     v.y = v.y + ay * dt;
@@ -680,7 +826,7 @@ __global__ void k_advance(Params p, const StepConsts* __restrict__ sc, const flo
         float4 a = pos_in[i];
         float4 v = vel[i];
         float4 pre = v;
-        advance_one(p, sc->dt, a, v, held, bad);
+        advance_one(p, sc->dt, a, v, held, bad, TerrainDev{});
         if (vel_pre) {
             uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
             pre.w = __uint_as_float(flags);
@@ -922,21 +1068,23 @@ void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start,
 
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
-                    Status* st, cudaStream_t s) {
+                    Status* st, const TerrainDev& T, float4* slope, cudaStream_t s) {
     if (!p.n) return;
     if (p.solver == 0)
-        k_density<0><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st);
+        k_density<0><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
+                                                        T, slope);
     else
-        k_density<1><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st);
+        k_density<1><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
+                                                        T, slope);
 }
 
 void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                         const float4* pos, const float4* vel, const float* rho, const float* press,
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                        float4* vel_pre, cudaStream_t s) {
+                        float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s) {
     if (p.n)
         k_wcsph_force<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled, walls, pos_out,
-                                                         vel_out, st, vel_pre);
+                                                         vel_out, st, vel_pre, T, slope);
 }
 
 size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (sizeof(DD) + sizeof(uint32_t)) + 64; }

@@ -37,15 +37,16 @@ void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32
                        uint32_t* order, cudaStream_t s);
 
 // pair passes: the density pass builds the substep's neighbour lists, the others walk them
+// T: terrain regions (regions = 0: none); slope (optional): each particle's ground density gradient
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
-                    Status* st, cudaStream_t s);
+                    Status* st, const TerrainDev& T, float4* slope, cudaStream_t s);
 // vel_pre (optional): the velocity before the wall clamp, its w lane the bits of the components
 // the clamp zeroed (1 x, 2 y, 4 z), for the adjoint
 void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                         const float4* pos, const float4* vel, const float* rho, const float* press,
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                        float4* vel_pre, cudaStream_t s);
+                        float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
 // sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve

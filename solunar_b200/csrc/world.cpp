@@ -83,6 +83,12 @@ struct HostKernel {
         if (q >= 1.0f) return 0.0f;
         return scale * pow4f(1.0f - q) * (1.0f + 4.0f * q);
     }
+    // Kernel::slope (mod.rs:149-155)
+    float slope(float d) const {
+        float q = d / radius;
+        if (q >= 1.0f) return 0.0f;
+        return scale * -20.0f * q * pow3f(1.0f - q) / radius;
+    }
 };
 
 inline float rmin(float a, float b) {
@@ -334,6 +340,24 @@ struct World {
     bool has_domain = false;
     F3 dlow{}, dhigh{};
 
+    // terrain regions (terrain.rs:36-42) and the ground sites (terrain.rs:176-186)
+    struct TerrainHost {
+        uint32_t owner;
+        F3 low;
+        uint32_t nx, ny, nz;
+        float step;
+        std::vector<float> distances;
+    };
+    std::vector<TerrainHost> terrains;
+    std::vector<float4> site_host;
+    std::vector<float> far_host, damping_host;
+    float ground_reach = 0, ground_low = 0, ground_step = 0;
+    DevBuf<TerrainRegion> dregions;
+    DevBuf<float> ddist, dfar, ddamping;
+    DevBuf<float4> dsites, gslope;
+    bool terrain_dirty = true;
+    TerrainDev tdev{};
+
     Status* d_status = nullptr;
     Status* h_status = nullptr;
     StepConsts* d_consts = nullptr;
@@ -422,6 +446,10 @@ struct World {
             tape.cids.release(stream);
             dwalls.release(stream);
             dwkeys.release(stream);
+            dregions.release(stream);
+            for (auto* b : {&ddist, &dfar, &ddamping}) b->release(stream);
+            dsites.release(stream);
+            gslope.release(stream);
             cudaStreamSynchronize(stream);
             if (d_status) cudaFree(d_status);
             if (d_consts) cudaFree(d_consts);
@@ -480,8 +508,145 @@ struct World {
         SLF_CUDA(cudaMallocHost(&h_status, sizeof(Status)));
         std::memset(h_status, 0, sizeof(Status));
         SLF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(Status), stream));
+        build_ground_sites();
         return SLF_OK;
     }
+
+    // GroundSites::new (terrain.rs:188-238), in the reference's f32 order
+    void build_ground_sites() {
+        HostKernel k(radius);
+        const float spacing = s.spacing;
+        int reach = int(std::ceil(radius / spacing));
+        site_host.clear();
+        far_host.clear();
+        for (int z = -reach; z <= reach; ++z)
+            for (int y = -reach; y <= reach; ++y)
+                for (int x = -reach; x <= reach; ++x) {
+                    float ox = float(x) * spacing, oy = float(y) * spacing, oz = float(z) * spacing;
+                    float far = std::sqrt(ox * ox + oy * oy + oz * oz);
+                    if (far < radius) {
+                        site_host.push_back(make_float4(ox, oy, oz, mass * k.value(far)));
+                        far_host.push_back(far);
+                    }
+                }
+        ground_low = -spacing / 2.0f;
+        ground_step = (radius - ground_low) / float(kGroundSamples - 1);
+        float soften = 0.01f * radius * radius;
+        int across_reach = reach + 1;
+        damping_host.assign(kGroundSamples, 0.0f);
+        for (int sample = 0; sample < kGroundSamples; ++sample) {
+            float distance = ground_low + ground_step * float(sample);
+            float weight = 0.0f;
+            for (int layer = 0;; ++layer) {
+                float depth = distance + spacing * (float(layer) + 0.5f);
+                if (depth >= radius) break;
+                for (int a = -across_reach; a <= across_reach; ++a)
+                    for (int b = -across_reach; b <= across_reach; ++b) {
+                        float across = float(a * a + b * b) * spacing * spacing;
+                        float squared = across + depth * depth;
+                        float far = std::sqrt(squared);
+                        if (far >= radius || far <= 0.0f) continue;
+                        weight += mass * depth * depth * -k.slope(far) / (far * (squared + soften));
+                    }
+            }
+            damping_host[sample] = weight;
+        }
+        ground_reach = radius + spacing / 2.0f;
+    }
+
+    // the terrain regions and ground sites on the device, after a change
+    int32_t upload_terrain() {
+        if (!terrain_dirty) return SLF_OK;
+        tdev = TerrainDev{};
+        terrain_dirty = false;
+        if (terrains.empty()) return SLF_OK;
+        std::vector<TerrainRegion> regions;
+        std::vector<float> dist;
+        for (const TerrainHost& t : terrains) {
+            TerrainRegion r{};
+            r.lx = t.low.x;
+            r.ly = t.low.y;
+            r.lz = t.low.z;
+            r.step = t.step;
+            r.nx = t.nx;
+            r.ny = t.ny;
+            r.nz = t.nz;
+            r.offset = dist.size();
+            regions.push_back(r);
+            dist.insert(dist.end(), t.distances.begin(), t.distances.end());
+        }
+        SLF_TRY(dregions.ensure(regions.size(), 0, stream));
+        SLF_TRY(ddist.ensure(dist.size(), 0, stream));
+        SLF_TRY(dsites.ensure(site_host.size(), 0, stream));
+        SLF_TRY(dfar.ensure(far_host.size(), 0, stream));
+        SLF_TRY(ddamping.ensure(kGroundSamples, 0, stream));
+        SLF_CUDA(cudaMemcpyAsync(dregions.p, regions.data(), regions.size() * sizeof(TerrainRegion),
+                                 cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(ddist.p, dist.data(), dist.size() * 4, cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(dsites.p, site_host.data(), site_host.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                                 stream));
+        SLF_CUDA(cudaMemcpyAsync(dfar.p, far_host.data(), far_host.size() * 4, cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(ddamping.p, damping_host.data(), kGroundSamples * 4, cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaStreamSynchronize(stream));  // the host vectors are pageable and local
+        tdev.regions = uint32_t(regions.size());
+        tdev.sites = uint32_t(site_host.size());
+        tdev.region = dregions.p;
+        tdev.dist = ddist.p;
+        tdev.site = dsites.p;
+        tdev.far = dfar.p;
+        tdev.damping = ddamping.p;
+        tdev.spacing = s.spacing;
+        tdev.reach = ground_reach;
+        tdev.low = ground_low;
+        tdev.step = ground_step;
+        return SLF_OK;
+    }
+
+    // per-particle ground slopes of the density pass (null without terrain)
+    float4* ground_slopes() {
+        if (terrains.empty()) return nullptr;
+        if (gslope.ensure(std::max<uint64_t>(n, 1), 0, stream) != SLF_OK) return nullptr;
+        return gslope.p;
+    }
+
+    static constexpr size_t kMaxTerrainNodes = size_t(1) << 24;  // terrain.rs:9
+
+    // add_terrain's node lattice (terrain.rs:275-283)
+    int32_t terrain_nodes(const float* low, const float* high, uint64_t nodes[3]) const {
+        if (!finite3(low) || !finite3(high)) return fail(SLF_ERR_NON_FINITE, "non finite value in terrain box");
+        if (high[0] <= low[0] || high[1] <= low[1] || high[2] <= low[2])
+            return fail(SLF_ERR_OUT_OF_RANGE, "inside out terrain box");
+        float step = s.spacing / 2.0f;
+        for (int a = 0; a < 3; ++a) nodes[a] = uint64_t(rmin(std::ceil((high[a] - low[a]) / step), 1e7f)) + 1;
+        unsigned __int128 total = (unsigned __int128)nodes[0] * nodes[1] * nodes[2];
+        if (total > kMaxTerrainNodes) return fail(SLF_ERR_FLUID_FULL, "terrain region holds too many nodes");
+        return SLF_OK;
+    }
+
+    // add_terrain (terrain.rs:262-302) with distances the caller sampled at the nodes
+    int32_t add_terrain(const float* low, const float* high, const float* distances, uint64_t count, uint32_t* out) {
+        if (fast()) return fail(SLF_ERR_UNSUPPORTED, "terrain runs with EXACT arithmetic only");
+        uint64_t nodes[3];
+        SLF_TRY(terrain_nodes(low, high, nodes));
+        if (count != nodes[0] * nodes[1] * nodes[2])
+            return fail(SLF_ERR_INVALID_ARGUMENT, "distances must hold one value per terrain node");
+        for (uint64_t i = 0; i < count; ++i)
+            if (!std::isfinite(distances[i])) return fail(SLF_ERR_NON_FINITE, "non finite terrain distance");
+        TerrainHost t;
+        t.low = F3{low[0], low[1], low[2]};
+        t.nx = uint32_t(nodes[0]);
+        t.ny = uint32_t(nodes[1]);
+        t.nz = uint32_t(nodes[2]);
+        t.step = s.spacing / 2.0f;
+        t.distances.assign(distances, distances + count);
+        t.owner = add_wall_points({});
+        terrains.push_back(std::move(t));
+        terrain_dirty = true;
+        lists_valid = false;
+        if (out) *out = terrains.back().owner;
+        return SLF_OK;
+    }
+
 
     Params params() const {
         Params p{};
@@ -658,7 +823,7 @@ struct World {
                                 alpha.p, d_status, stream);
         else
             launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status,
-                           stream);
+                           tdev, ground_slopes(), stream);
     }
     void force_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
         if (fast())
@@ -666,7 +831,8 @@ struct World {
                                     scaled.p, dwalls.p, pos[b].p, cells_of(b), vel[b].p, d_status, vel_pre, stream);
         else
             launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
-                               pos[b].p, vel[b].p, d_status, vel_pre, stream);
+                               pos[b].p, vel[b].p, d_status, vel_pre, tdev, terrains.empty() ? nullptr : gslope.p,
+                               stream);
     }
     void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid,
                    SolveRec rec = SolveRec{nullptr, nullptr}) {
@@ -807,7 +973,11 @@ struct World {
         }
         containers = rest;
         update_bounds();
-        bool gone = wpos.size() != before || had;
+        size_t regions = terrains.size();
+        terrains.erase(std::remove_if(terrains.begin(), terrains.end(), [&](const TerrainHost& t) { return t.owner == id; }),
+                       terrains.end());
+        if (terrains.size() != regions) terrain_dirty = true;
+        bool gone = wpos.size() != before || had || terrains.size() != regions;
         if (gone) settle_walls();
         return gone;
     }
@@ -1045,6 +1215,7 @@ struct World {
     int32_t update_neighbors() {
         SLF_TRY(flush());
         SLF_TRY(upload_walls());
+        SLF_TRY(upload_terrain());
         if (n == 0) {
             lists_valid = true;
             lists_n = 0;
@@ -1075,6 +1246,7 @@ struct World {
         if (n == 0) return SLF_OK;
         SLF_TRY(ensure_work_buffers());
         SLF_TRY(upload_walls());
+        SLF_TRY(upload_terrain());
         Params p = params();
         for (;;) {
             SLF_TRY(reset_status());
@@ -1270,6 +1442,7 @@ struct World {
 
     int32_t tape_begin(uint32_t every) {
         if (rel()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on absolute positions only");
+        if (!terrains.empty()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint takes no terrain");
         SLF_TRY(flush());
         tape.on = true;
         tape.every = every;
@@ -1582,6 +1755,7 @@ struct World {
         if (dt == 0.0f) return SLF_OK;
         SLF_TRY(flush());
         SLF_TRY(upload_walls());
+        SLF_TRY(upload_terrain());
         if (n > 0) {
             SLF_TRY(ensure_work_buffers());
             SLF_TRY(refresh_stats());
@@ -1607,6 +1781,8 @@ struct World {
                 }
                 r.substeps = substeps;
             } else {
+                // dfsph.rs:52-55: ground pushes through the weakly compressible solver's pressure only
+                if (!terrains.empty()) return fail(SLF_ERR_INVALID_SETTINGS, "DFSPH takes no terrain");
                 // dfsph (dfsph.rs:46-77)
                 float spacing = s.spacing, courant = s.courant;
                 float pull = std::sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] +
@@ -1867,7 +2043,18 @@ struct World {
         }
         w.u32(flow_next);
         w.len(0);  // coupled bodies
-        w.len(0);  // terrain regions
+        // TerrainField::save (terrain.rs:44-55)
+        w.len(terrains.size());
+        for (const TerrainHost& t : terrains) {
+            w.u32(t.owner);
+            w.vec3(t.low.x, t.low.y, t.low.z);
+            w.len(t.nx);
+            w.len(t.ny);
+            w.len(t.nz);
+            w.f32(t.step);
+            w.len(t.distances.size());
+            for (float d : t.distances) w.f32(d);
+        }
         if (has_domain) {
             w.u8(1);
             w.vec3(dlow.x, dlow.y, dlow.z);
@@ -1987,11 +2174,27 @@ struct World {
         SLF_TRY(rd(r.u32(fnext)));
         for (auto& fl : lf)
             if (fl.id >= fnext) return bad("invalid snapshot: fluid flow id");
-        size_t coupled = 0, terrains = 0;
+        size_t coupled = 0, nterrain = 0;
         SLF_TRY(rd(r.count(12, kMaxSnapshotParts, coupled)));
         if (coupled) return fail(SLF_ERR_UNSUPPORTED, "coupled bodies are not on this path");
-        SLF_TRY(rd(r.count(32, kMaxSnapshotParts, terrains)));
-        if (terrains) return fail(SLF_ERR_UNSUPPORTED, "terrain regions are not on this path");
+        SLF_TRY(rd(r.count(32, kMaxSnapshotParts, nterrain)));
+        // TerrainField::load (terrain.rs:57-97)
+        std::vector<TerrainHost> lt(nterrain);
+        for (TerrainHost& t : lt) {
+            size_t nd = 0;
+            SLF_TRY(rd(r.u32(t.owner) && r.vec3(t.low) && r.u32(t.nx) && r.u32(t.ny) && r.u32(t.nz) && r.f32(t.step) &&
+                       r.count(4, kMaxTerrainNodes, nd)));
+            unsigned __int128 total = (unsigned __int128)t.nx * t.ny * t.nz;
+            if (!finite3f(t.low) || !std::isfinite(t.step) || t.step <= 0.0f || t.nx < 2 || t.ny < 2 || t.nz < 2 ||
+                total != nd)
+                return bad("invalid snapshot: fluid terrain");
+            t.distances.resize(nd);
+            for (float& d : t.distances) {
+                SLF_TRY(rd(r.f32(d)));
+                if (!std::isfinite(d)) return bad("invalid snapshot: fluid terrain distance");
+            }
+            if (t.owner >= wnext) return bad("invalid snapshot: fluid terrain owner");
+        }
         bool dom = false;
         F3 dl{}, dh{};
         if (version >= 2) {
@@ -2026,6 +2229,9 @@ struct World {
         settle_walls();
         flows = std::move(lf);
         flow_next = fnext;
+        if (!lt.empty() && fast()) return fail(SLF_ERR_UNSUPPORTED, "terrain runs with EXACT arithmetic only");
+        terrains = std::move(lt);
+        terrain_dirty = true;
         has_domain = dom;
         dlow = dl;
         dhigh = dh;
@@ -2095,6 +2301,7 @@ struct World {
         if (!lists_valid || lists_n != n) return fail(SLF_ERR_OUT_OF_RANGE, "neighbour lists are stale");
         if (start && start_len != n + 1) return fail(SLF_ERR_INVALID_ARGUMENT, "start must hold len + 1 entries");
         SLF_TRY(upload_walls());
+        SLF_TRY(upload_terrain());
         if (n == 0) {
             if (start) start[0] = 0;
             if (len) *len = 0;
@@ -2367,6 +2574,23 @@ int32_t slf_load_snapshot(const uint8_t* data, uint64_t size, const slf_settings
     if (st != SLF_OK) return st;
     *out = h.release();
     return SLF_OK;
+}
+
+int32_t slf_terrain_nodes(const slf_world* world, const float low[3], const float high[3], uint64_t nodes[3]) {
+    SLF_WORLD(world);
+    SLF_NEED(low);
+    SLF_NEED(high);
+    SLF_NEED(nodes);
+    return world->w.terrain_nodes(low, high, nodes);
+}
+
+int32_t slf_add_terrain(slf_world* world, const float low[3], const float high[3], const float* distances,
+                        uint64_t count, uint32_t* boundary_out) {
+    SLF_WORLD(world);
+    SLF_NEED(low);
+    SLF_NEED(high);
+    if (count) SLF_NEED(distances);
+    return world->w.add_terrain(low, high, distances, count, boundary_out);
 }
 
 int32_t slf_add_emitter(slf_world* world, const float low[3], const float high[3], const float velocity[3],

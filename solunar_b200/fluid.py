@@ -54,6 +54,8 @@ def load_library():
         "slf_add_wall": [vp, fp, fp, u32p],
         "slf_remove_boundary": [vp, ctypes.c_uint32, i32p],
         "slf_add_emitter": [vp, fp, fp, fp, u32p],
+        "slf_terrain_nodes": [vp, fp, fp, u64p],
+        "slf_add_terrain": [vp, fp, fp, fp, ctypes.c_uint64, u32p],
         "slf_save_snapshot": [vp, ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, u64p],
         "slf_load_snapshot": [ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64, ctypes.POINTER(CSettings),
                               ctypes.POINTER(vp)],
@@ -229,6 +231,20 @@ class FluidWorld:
         r = ctypes.c_int32()
         _check(_lib.slf_remove_boundary(self._h, boundary, ctypes.byref(r)))
         return bool(r.value)
+
+    # ---- terrain (terrain.rs:262-302) ----
+    def terrain_nodes(self, low, high):
+        n = (ctypes.c_uint64 * 3)()
+        _check(_lib.slf_terrain_nodes(self._h, vec3(low), vec3(high), n))
+        return tuple(int(v) for v in n)
+
+    def add_terrain(self, low, high, distances) -> int:
+        """Ground under the signed distances sampled at the region's nodes (see terrain_nodes)."""
+        d = np.ascontiguousarray(distances, dtype=np.float32).ravel()
+        i = ctypes.c_uint32()
+        _check(_lib.slf_add_terrain(self._h, vec3(low), vec3(high), _ptr(d, ctypes.c_float), d.size,
+                                    ctypes.byref(i)))
+        return i.value
 
     # ---- emitters and drains (flow.rs:86-139) ----
     def add_emitter(self, low, high, velocity) -> int:
