@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--positions", choices=["absolute", "cell_relative"], default="absolute",
                     help="cell_relative: offsets from each particle's cell (FAST arithmetic, no adjoint)")
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--adjoint-every", type=int, default=8,
+    ap.add_argument("--adjoint-every", type=int, default=0,
                     help="tape checkpoint spacing of the forward+adjoint leg; 0 records every substep")
     ap.add_argument("--adjoint-steps", type=int, default=32,
                     help="steps of the forward+adjoint measurement (0 skips it)")
@@ -103,48 +103,79 @@ def traffic_for(kernel: str, scene: str):
 
 
 class Clocks:
-    """nvidia-smi samples every 200 ms while running."""
+    """SM clocks and clock-event reasons sampled while the timed region runs: through NVML every
+    10 ms in a thread (reads only), or from `nvidia-smi -lms 200` where NVML is missing."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
-        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.rows = []
+        self.thread = None
         self.proc = None
+        self.done = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import threading
+
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+            self.done = threading.Event()
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+            def sample():
+                while not self.done.is_set():
+                    sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    active = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append((sm, tuple(bool(active & b) for b in bits)))
+                    self.done.wait(0.01)
+
+            self.thread = threading.Thread(target=sample, daemon=True)
+            self.thread.start()
+        except Exception:  # no NVML: nvidia-smi's own polling
+            self.thread = None
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            fields = ("index,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                      "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                      "clocks_event_reasons.sw_power_cap")
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={fields}",
+                                              "--format=csv,noheader,nounits", "-lms", "200"],
+                                             stdout=self.file, stderr=subprocess.DEVNULL)
+            except OSError:
+                self.proc = None
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.file.flush()
-        rows = []
-        with open(self.file.name) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.file.name)
+        if self.thread is not None:
+            self.done.set()
+            self.thread.join(timeout=5)
+            rows, mx = self.rows, self.max_mhz
+        elif self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.file.flush()
+            rows, mx = [], None
+            with open(self.file.name) as f:
+                for line in f:
+                    q = [x.strip() for x in line.split(",")]
+                    if len(q) >= 7 and q[1].replace(".", "").isdigit():
+                        rows.append((float(q[1]), tuple(v.lower() == "active" for v in q[3:7])))
+                        mx = float(q[2]) if q[2].replace(".", "").isdigit() else mx
+            os.unlink(self.file.name)
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"], "samples": 0}
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["no samples"], "samples": 0}
+        reasons = sorted({self.NAMES[k] for _, act in rows for k in range(4) if act[k]})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": mx, "reasons": reasons,
                 "samples": len(rows)}
 
 
