@@ -73,7 +73,11 @@ typedef struct slf_settings {
     /* library fields (the reference hard-codes these) */
     int32_t positions;             /* SLF_POSITIONS_*, default ABSOLUTE */
     int32_t arithmetic;            /* SLF_ARITHMETIC_*, default EXACT */
-    int32_t warm_start;            /* DFSPH solves start from last substep's stiffness; 0 */
+    int32_t warm_start;            /* 1: each DFSPH solve starts with one push at half the stiffness
+                                    * impulse (sum of kappa dt) the particle's solve of the same kind
+                                    * applied the substep before (dfsph.rs cold-starts: 0, the
+                                    * default).  Snapshots do not carry it: a loaded world starts
+                                    * cold.  Not with slf_tape_begin. */
     float divergence_tolerance;    /* dfsph.rs:11, 1e-3 */
     float density_tolerance;       /* dfsph.rs:9, 5e-4 */
     uint32_t min_iterations;       /* dfsph.rs:12, 2 */
@@ -156,8 +160,8 @@ int32_t slf_save_snapshot(slf_world* world, uint8_t* out, uint64_t capacity, uin
 /* FluidWorld::load_snapshot (save.rs:79-181): a new world from untrusted snapshot bytes
  * (versions 1-3).  The library's own settings fields (positions, arithmetic, solver limits,
  * device) come from `library`, or the defaults when it is NULL.  Bad bytes return
- * SLF_ERR_SNAPSHOT with the reference's message in slf_last_error(); coupled bodies or terrain
- * in the snapshot return SLF_ERR_UNSUPPORTED. */
+ * SLF_ERR_SNAPSHOT with the reference's message in slf_last_error(); coupled bodies in the
+ * snapshot return SLF_ERR_UNSUPPORTED. */
 int32_t slf_load_snapshot(const uint8_t* data, uint64_t size, const slf_settings* library, slf_world** out);
 
 /* The node lattice of a terrain region over [low, high] (terrain.rs:275-283): nodes[a] nodes along
@@ -251,7 +255,8 @@ typedef struct slf_param_grads {
  * every substep keeps the state before it and its solver record (the rates and velocities of each
  * DFSPH iteration), about 68 + 20 x iterations bytes per particle per substep; the backward pass
  * then redoes only each substep's sort and densities.  The number of particles must not change
- * while recording.  WCSPH and DFSPH steps. */
+ * while recording.  WCSPH and DFSPH steps; UNSUPPORTED with cell-relative positions, terrain
+ * or warm_start. */
 int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
 /* Stops recording and frees the tape. */
 int32_t slf_tape_end(slf_world* world);

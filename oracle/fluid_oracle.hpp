@@ -160,6 +160,11 @@ struct Settings {
     // 0: the reference's sequential sum of the solver error in the working precision
     //    (dfsph.rs:266-267); 1: a compensated sum in double, as the CUDA library takes it.
     int32_t residual_sum = 0;
+    // 1: each DFSPH solve starts with one push at half the stiffness impulse (sum of kappa dt)
+    //    the particle's solve of the same kind applied the substep before.  The reference
+    //    cold-starts every solve, because a half-pressure start pushed water apart and sped a
+    //    dam-break front up (dfsph.rs:217-221): 0, the default.
+    int32_t warm_start = 0;
 
     // mod.rs:98-117
     bool valid() const {
@@ -365,6 +370,9 @@ template <class R> class World {
     std::vector<uint32_t> ids;
     std::vector<Vec> positions, velocities;
     std::vector<R> densities;
+    // warm starts: per particle the stiffness impulse its last divergence (0) and density (1)
+    // solve applied, kept in particle order like the densities
+    std::vector<R> impulse[2];
     uint32_t next_id = 0;
     Grid grid;
     Lists neighbors, wall_neighbors;
@@ -609,6 +617,8 @@ template <class R> class World {
         positions.push_back(position);
         velocities.push_back(velocity);
         densities.push_back(R(0));
+        impulse[0].push_back(R(0));
+        impulse[1].push_back(R(0));
         if (id_out) *id_out = id;
         return OK;
     }
@@ -638,6 +648,8 @@ template <class R> class World {
                 positions[kept] = positions[i];
                 velocities[kept] = velocities[i];
                 densities[kept] = densities[i];
+                impulse[0][kept] = impulse[0][i];
+                impulse[1][kept] = impulse[1][i];
                 ++kept;
             } else {
                 ++lost;
@@ -647,6 +659,8 @@ template <class R> class World {
         positions.resize(kept);
         velocities.resize(kept);
         densities.resize(kept);
+        impulse[0].resize(kept);
+        impulse[1].resize(kept);
         return lost;
     }
 
@@ -685,12 +699,16 @@ template <class R> class World {
                 positions[kept] = positions[i];
                 velocities[kept] = velocities[i];
                 densities[kept] = densities[i];
+                impulse[0][kept] = impulse[0][i];
+                impulse[1][kept] = impulse[1][i];
                 ++kept;
             }
         ids.resize(kept);
         positions.resize(kept);
         velocities.resize(kept);
         densities.resize(kept);
+        impulse[0].resize(kept);
+        impulse[1].resize(kept);
     }
 
     // Rust's `f as i64`: saturating, NaN to 0
@@ -996,7 +1014,7 @@ template <class R> class World {
         });
         std::vector<uint32_t> nid(n);
         std::vector<Vec> np(n), nv(n);
-        std::vector<R> nd(n);
+        std::vector<R> nd(n), nw0(n), nw1(n);
         std::vector<Key> keys(n);
         for (size_t i = 0; i < n; ++i) {
             uint32_t k = order[i].index;
@@ -1004,12 +1022,16 @@ template <class R> class World {
             np[i] = positions[k];
             nv[i] = velocities[k];
             nd[i] = densities[k];
+            nw0[i] = impulse[0][k];
+            nw1[i] = impulse[1][k];
             keys[i] = order[i].cell;
         }
         ids = std::move(nid);
         positions = std::move(np);
         velocities = std::move(nv);
         densities = std::move(nd);
+        impulse[0] = std::move(nw0);
+        impulse[1] = std::move(nw1);
         grid = Grid::build(keys);
 
         R reach = pow2(radius());
@@ -1286,6 +1308,8 @@ template <class R> class World {
             w.velocities.push_back(v);
         }
         w.densities.assign(count, R(st.rest_density));
+        w.impulse[0].assign(count, R(0));  // a loaded world starts cold
+        w.impulse[1].assign(count, R(0));
         if (!r.u32(w.next_id)) return SNAPSHOT;
         std::vector<uint32_t> seen = w.ids;
         std::sort(seen.begin(), seen.end());
@@ -1678,6 +1702,16 @@ template <class R> class World {
         R tolerance = which == 0 ? R(settings.divergence_tolerance) : R(settings.density_tolerance);
         uint32_t iterations = 0;
         std::vector<R> stiffness(n), errors(n);
+        std::vector<R>& applied = impulse[which];
+        if (settings.warm_start) {
+            // the stiffness that applies half the last solve's impulse at this dt, pushed once;
+            // the impulse restarts from it
+            for (size_t i = 0; i < n; ++i) {
+                stiffness[i] = (R(0.5f) * applied[i]) / dt;
+                applied[i] = stiffness[i] * dt;
+            }
+            push_apart(stiffness, dt);
+        }
         for (;;) {
 #pragma omp parallel for schedule(static) num_threads(nthreads())
             for (long long ii = 0; ii < (long long)n; ++ii) {
@@ -1714,6 +1748,8 @@ template <class R> class World {
             }
             if (settled || iterations >= settings.max_iterations) return iterations;
             push_apart(stiffness, dt);
+            if (settings.warm_start)
+                for (size_t i = 0; i < n; ++i) applied[i] = applied[i] + stiffness[i] * dt;
             iterations += 1;
         }
     }

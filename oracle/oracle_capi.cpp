@@ -43,6 +43,7 @@ Settings from_c(const slf_settings* s, int residual_sum) {
     o.min_iterations = s->min_iterations;
     o.max_iterations = s->max_iterations;
     o.residual_sum = residual_sum;
+    o.warm_start = s->warm_start;
     return o;
 }
 

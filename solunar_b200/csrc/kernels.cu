@@ -119,7 +119,8 @@ __global__ void k_rank_reorder(uint32_t n, const uint32_t* __restrict__ lin, con
                                const float* __restrict__ rho_in, const int4* __restrict__ cells_in,
                                uint32_t* __restrict__ ids_out, float4* __restrict__ pos_out,
                                float4* __restrict__ vel_out, float* __restrict__ rho_out,
-                               int4* __restrict__ cells_out, uint32_t skip_begin, uint32_t skip_end, Status* st,
+                               int4* __restrict__ cells_out, const float2* __restrict__ warm_in,
+                               float2* __restrict__ warm_out, uint32_t skip_begin, uint32_t skip_end, Status* st,
                                uint32_t* __restrict__ dest) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     // a job left undone (the fault injection of the dispatcher tests) places nothing; the count
@@ -140,6 +141,7 @@ __global__ void k_rank_reorder(uint32_t n, const uint32_t* __restrict__ lin, con
     vel_out[f] = vel_in[i];
     rho_out[f] = rho_in[i];
     if (cells_in) cells_out[f] = cells_in[i];
+    if (warm_in) warm_out[f] = warm_in[i];
 }
 
 // ---- exclusive scan of u32 in place, total written at data[m] ------------------------------
@@ -741,7 +743,7 @@ template <class Src>
 __device__ __forceinline__ void push_particle(const Params& p, const StepConsts* __restrict__ sc, const PairLists& fl,
                                               const PairLists& wl, uint32_t i, uint32_t row, const Src& src,
                                               const float4* __restrict__ pos, float4* __restrict__ vel,
-                                              const float4* __restrict__ walls) {
+                                              const float4* __restrict__ walls, float* __restrict__ applied) {
     const float dt = sc->dt;
     float4 a = pos[i];
     float own = a.w;
@@ -765,17 +767,19 @@ __device__ __forceinline__ void push_particle(const Params& p, const StepConsts*
     v.y = v.y + cy * dt;
     v.z = v.z + cz * dt;
     vel[i] = v;
+    // warm starts: the stiffness impulse this particle's solve has applied so far
+    if (applied) applied[2 * (size_t)i] += own * dt;
 }
 
 __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
                                                  float4* __restrict__ vel, const float4* __restrict__ walls,
-                                                 const Status* st) {
+                                                 const Status* st, float* __restrict__ applied) {
     if (__ldcg(&st->settled)) return;
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
-    push_particle(p, sc, fl, wl, i, row, FromGlobal{pos, nullptr}, pos, vel, walls);
+    push_particle(p, sc, fl, wl, i, row, FromGlobal{pos, nullptr}, pos, vel, walls, applied);
 }
 
 // viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
@@ -978,7 +982,8 @@ __global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const u
                           const float4* __restrict__ vel_in, const float* __restrict__ rho_in,
                           const int4* __restrict__ cells_in, uint32_t* __restrict__ ids_out,
                           float4* __restrict__ pos_out, float4* __restrict__ vel_out, float* __restrict__ rho_out,
-                          int4* __restrict__ cells_out) {
+                          int4* __restrict__ cells_out, const float2* __restrict__ warm_in,
+                          float2* __restrict__ warm_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !keep[i]) return;
     uint32_t f = dest[i];
@@ -987,6 +992,7 @@ __global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const u
     vel_out[f] = vel_in[i];
     rho_out[f] = rho_in[i];
     if (cells_in) cells_out[f] = cells_in[i];
+    if (warm_in) warm_out[f] = warm_in[i];
 }
 
 __global__ void k_set_consts(StepConsts c, StepConsts* out) { *out = c; }
@@ -1058,11 +1064,13 @@ void launch_scatter_members(uint32_t n, const uint32_t* lin, const uint32_t* slo
 void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start, const uint32_t* members,
                          const uint32_t* ids_in, const float4* pos_in, const float4* vel_in, const float* rho_in,
                          const int4* cells_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
-                         int4* cells_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
+                         int4* cells_out, const float2* warm_in, float2* warm_out, uint32_t skip_begin,
+                         uint32_t skip_end, Status* st, uint32_t* dest,
                          cudaStream_t s) {
     if (n)
         k_rank_reorder<<<blocks_for(n), kBlock, 0, s>>>(n, lin, start, members, ids_in, pos_in, vel_in, rho_in,
                                                         cells_in, ids_out, pos_out, vel_out, rho_out, cells_out,
+                                                        warm_in, warm_out,
                                                         skip_begin, skip_end, st, dest);
 }
 
@@ -1105,8 +1113,25 @@ void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLis
 }
 
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
-                 float4* vel, const float4* walls, const Status* st, cudaStream_t s) {
-    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st);
+                 float4* vel, const float4* walls, const Status* st, float* applied, cudaStream_t s) {
+    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied);
+}
+
+// Warm start of a solve: the stiffness that applies `share` of the impulse S the particle's last
+// solve of this kind applied (S = sum of kappa dt), at this substep's dt, into the position's
+// spare lane for one push; S restarts from that push's impulse.
+__global__ void k_warm_kappa(Params p, const StepConsts* __restrict__ sc, float share, float* __restrict__ applied,
+                             float4* __restrict__ pos) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const float dt = sc->dt;
+    float kappa = share * applied[2 * (size_t)i] / dt;
+    pos[i].w = kappa;
+    applied[2 * (size_t)i] = kappa * dt;
+}
+
+void launch_warm_kappa(const Params& p, const StepConsts* sc, float share, float* applied, float4* pos, cudaStream_t s) {
+    if (p.n) k_warm_kappa<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, share, applied, pos);
 }
 
 size_t walk_order_keys(int3 span) {
@@ -1164,10 +1189,10 @@ void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, 
 void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, const uint32_t* ids_in,
                     const float4* pos_in, const float4* vel_in, const float* rho_in, const int4* cells_in,
                     uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out, int4* cells_out,
-                    cudaStream_t s) {
+                    const float2* warm_in, float2* warm_out, cudaStream_t s) {
     if (n)
         k_compact<<<blocks_for(n), kBlock, 0, s>>>(n, keep, dest, ids_in, pos_in, vel_in, rho_in, cells_in, ids_out,
-                                                   pos_out, vel_out, rho_out, cells_out);
+                                                   pos_out, vel_out, rho_out, cells_out, warm_in, warm_out);
 }
 
 void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s) {

@@ -561,7 +561,8 @@ template <bool REL, class Src>
 __device__ __forceinline__ void push_particle_fast(const Params& p, const StepConsts* __restrict__ sc,
                                                    const IndexLists& fl, const IndexLists& wl, uint32_t i, uint32_t row,
                                                    const Src& src, const float4* __restrict__ pos,
-                                                   float4* __restrict__ vel, const float4* __restrict__ walls) {
+                                                   float4* __restrict__ vel, const float4* __restrict__ walls,
+                                                   float* __restrict__ applied) {
     const float mdt = p.mass * sc->dt;
     float4 a = pos[i];
     float own = a.w;
@@ -585,19 +586,20 @@ __device__ __forceinline__ void push_particle_fast(const Params& p, const StepCo
     v.y = fmaf(cy, mdt, v.y);
     v.z = fmaf(cz, mdt, v.z);
     vel[i] = v;
+    if (applied) applied[2 * (size_t)i] = fmaf(own, sc->dt, applied[2 * (size_t)i]);
 }
 
 template <bool REL>
 __global__ void __launch_bounds__(kBlock) k_push_fast(Params p, const StepConsts* __restrict__ sc, PairLists fpl,
                                                       PairLists wpl, const float4* __restrict__ pos,
                                                       float4* __restrict__ vel, const float4* __restrict__ walls,
-                                                      const Status* st) {
+                                                      const Status* st, float* __restrict__ applied) {
     if (__ldcg(&st->settled)) return;
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fpl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
-    push_particle_fast<REL>(p, sc, fl, wl, i, row, FromGlobalF{pos, nullptr}, pos, vel, walls);
+    push_particle_fast<REL>(p, sc, fl, wl, i, row, FromGlobalF{pos, nullptr}, pos, vel, walls, applied);
 }
 
 template <bool REL>
@@ -806,10 +808,11 @@ void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc
 }
 
 void launch_push_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                      const float4* pos, float4* vel, const float4* walls, const Status* st, cudaStream_t s) {
+                      const float4* pos, float4* vel, const float4* walls, const Status* st, float* applied,
+                      cudaStream_t s) {
     if (!p.n) return;
-    if (rel) k_push_fast<true><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st);
-    else k_push_fast<false><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st);
+    if (rel) k_push_fast<true><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied);
+    else k_push_fast<false><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied);
 }
 
 void launch_viscous_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,

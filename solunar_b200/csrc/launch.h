@@ -26,7 +26,8 @@ void launch_scatter_members(uint32_t n, const uint32_t* lin, const uint32_t* slo
 void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start, const uint32_t* members,
                          const uint32_t* ids_in, const float4* pos_in, const float4* vel_in, const float* rho_in,
                          const int4* cells_in, uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out,
-                         int4* cells_out, uint32_t skip_begin, uint32_t skip_end, Status* st, uint32_t* dest,
+                         int4* cells_out, const float2* warm_in, float2* warm_out, uint32_t skip_begin,
+                         uint32_t skip_end, Status* st, uint32_t* dest,
                          cudaStream_t s);
 
 // The list passes' walk order (PairLists::order) over the dense cell box `span` of a sort:
@@ -55,8 +56,11 @@ size_t rate_partial_bytes(uint32_t n);
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
                  void* partials, Status* st, SolveRec rec, cudaStream_t s);
+// applied (optional, stride 2): each particle's stiffness impulse sum, for warm starts
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
-                 float4* vel, const float4* walls, const Status* st, cudaStream_t s);
+                 float4* vel, const float4* walls, const Status* st, float* applied, cudaStream_t s);
+// warm start: pos.w = share * applied / dt, applied = that stiffness * dt
+void launch_warm_kappa(const Params& p, const StepConsts* sc, float share, float* applied, float4* pos, cudaStream_t s);
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                     const float4* vel, const float* rho, const float4* walls, float4* vel_out, cudaStream_t s);
 void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,
@@ -82,7 +86,7 @@ void launch_emit(uint32_t total, const uint32_t* taken_ex, int3 cnt, float3 low,
 void launch_compact(uint32_t n, const uint32_t* keep, const uint32_t* dest, const uint32_t* ids_in,
                     const float4* pos_in, const float4* vel_in, const float* rho_in, const int4* cells_in,
                     uint32_t* ids_out, float4* pos_out, float4* vel_out, float* rho_out, int4* cells_out,
-                    cudaStream_t s);
+                    const float2* warm_in, float2* warm_out, cudaStream_t s);
 
 void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s);
 
@@ -106,7 +110,8 @@ void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc
                       const PairLists& wl, float4* pos, const float4* vel, const float* rho, const float* alpha,
                       const float4* walls, void* partials, Status* st, SolveRec rec, cudaStream_t s);
 void launch_push_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                      const float4* pos, float4* vel, const float4* walls, const Status* st, cudaStream_t s);
+                      const float4* pos, float4* vel, const float4* walls, const Status* st, float* applied,
+                      cudaStream_t s);
 void launch_viscous_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                          const float4* pos, const float4* vel, const float* rho, const float4* walls,
                          float4* vel_out, cudaStream_t s);

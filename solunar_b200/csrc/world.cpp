@@ -307,6 +307,9 @@ struct World {
     DevBuf<int4> cell[3];  // cell-relative positions: the cell of each pos slot's offsets
     DevBuf<uint32_t> ids[2];
     DevBuf<float> rho[2];
+    // warm starts: per particle the stiffness impulse (sum of kappa dt) its last divergence (x)
+    // and density (y) solve applied; slotted with ids/rho, carried through sorts and compactions
+    DevBuf<float2> warm[2];
     DevBuf<float> press, scaled, alpha;
     DevBuf<uint32_t> lin, cslot, members, count, tiles, keep;
     // neighbour lists of the current substep (fluid and walls)
@@ -436,6 +439,7 @@ struct World {
                 b->release(stream);
             for (auto* b : {&rho[0], &rho[1], &press, &scaled, &alpha}) b->release(stream);
             for (auto* b : {&cell[0], &cell[1], &cell[2]}) b->release(stream);
+            for (auto* b : {&warm[0], &warm[1]}) b->release(stream);
             fent.release(stream);
             went.release(stream);
             partials.release(stream);
@@ -772,6 +776,7 @@ struct World {
         for (int i = 0; i < 2; ++i) {
             SLF_TRY(ids[i].ensure(m, i == cid ? n : 0, stream));
             SLF_TRY(rho[i].ensure(m, i == cid ? n : 0, stream));
+            if (warm_on()) SLF_TRY(warm[i].ensure(m, i == cid ? n : 0, stream));
         }
         if (rel()) {
             // absolute positions land in a free slot, then become offsets and cells
@@ -785,6 +790,7 @@ struct World {
         SLF_CUDA(cudaMemcpyAsync(vel[cpos].p + n, pend_vel.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
         SLF_CUDA(cudaMemcpyAsync(ids[cid].p + n, pend_ids.data(), k * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         SLF_CUDA(cudaMemsetAsync(rho[cid].p + n, 0, k * sizeof(float), stream));
+        if (warm_on()) SLF_CUDA(cudaMemsetAsync(warm[cid].p + n, 0, k * sizeof(float2), stream));
         SLF_CUDA(cudaStreamSynchronize(stream));  // the staging vectors are pageable and freed next
         pend_pos.clear();
         pend_vel.clear();
@@ -843,10 +849,14 @@ struct World {
             launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p, d_status,
                         rec, stream);
     }
-    void push_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v) {
-        if (fast()) launch_push_fast(rel(), p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
-        else launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, stream);
+    void push_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v,
+                   float* applied = nullptr) {
+        if (fast()) launch_push_fast(rel(), p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, applied, stream);
+        else launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, applied, stream);
     }
+    bool warm_on() const { return s.warm_start && s.solver == SLF_SOLVER_DFSPH; }
+    const float2* warm_in() const { return warm_on() ? warm[cid].p : nullptr; }
+    float2* warm_out() { return warm_on() ? warm[1 - cid].p : nullptr; }
     void advance_pass(const Params& p, int a, int b, float4* pre) {
         if (rel()) launch_advance_rel(p, d_consts, pos[a].p, cell[a].p, pos[b].p, cell[b].p, vel[b].p, d_status, pre,
                                       stream);
@@ -1186,8 +1196,7 @@ struct World {
         timed("hash_reorder", bytes_per_particle::reorder, [&] {
             launch_rank_reorder(uint32_t(n), lin.p, count.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p,
                                 rho[cid].p, cells_of(cpos), ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p,
-                                cells_of(to),
-                                job_lo, job_hi, d_status, sort_dest, stream);
+                                cells_of(to), warm_in(), warm_out(), job_lo, job_hi, d_status, sort_dest, stream);
         });
         // the walk order of this sort's lists (identity where its key space would not fit 32 bits)
         worder_valid = false;
@@ -1299,6 +1308,16 @@ struct World {
         const char* rate_name = which == 0 ? "rate_divergence" : "rate_density";
         const char* push_name = which == 0 ? "push_divergence" : "push_density";
         double rate_bytes = which == 0 ? bytes_per_particle::rate_divergence : bytes_per_particle::rate_density;
+        // warm start: one push at half the stiffness impulse the particle's last solve of this
+        // kind applied; the pushes then add theirs to it, for the next substep
+        float* applied = nullptr;
+        if (warm_on()) {
+            applied = reinterpret_cast<float*>(warm[nid].p) + which;
+            timed("warm_push", bytes_per_particle::push, [&] {
+                launch_warm_kappa(p, d_consts, 0.5f, applied, pos[a].p, stream);
+                push_pass(p, fl, wl, a, v);
+            });
+        }
         size_t first = prof.pending.size();
         std::vector<int> kinds;  // 0 rate, 1 push, in launch order, for the profile
         uint32_t batch = std::max<uint32_t>(expected_iterations[which], 1u);
@@ -1311,7 +1330,7 @@ struct World {
         rate();
         for (;;) {
             for (uint32_t b = 0; b < batch; ++b) {
-                timed(push_name, bytes_per_particle::push, [&] { push_pass(p, fl, wl, a, v); });
+                timed(push_name, bytes_per_particle::push, [&] { push_pass(p, fl, wl, a, v, applied); });
                 kinds.push_back(1);
                 rate();
             }
@@ -1443,6 +1462,7 @@ struct World {
     int32_t tape_begin(uint32_t every) {
         if (rel()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on absolute positions only");
         if (!terrains.empty()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint takes no terrain");
+        if (warm_on()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on cold-started solves only");
         SLF_TRY(flush());
         tape.on = true;
         tape.every = every;
@@ -1854,7 +1874,8 @@ struct World {
         int to = (cpos + 1) % 3;
         if (to == lists_pos) to = (cpos + 2) % 3;
         launch_compact(uint32_t(n), keep.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p, rho[cid].p,
-                       cells_of(cpos), ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, cells_of(to), stream);
+                       cells_of(cpos), ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p, cells_of(to), warm_in(),
+                       warm_out(), stream);
         SLF_CUDA(cudaStreamSynchronize(stream));
         removed = uint32_t(n - kept);
         n = kept;
@@ -1968,6 +1989,7 @@ struct World {
                 for (int i = 0; i < 2; ++i) {
                     SLF_TRY(ids[i].ensure(m, i == cid ? n : 0, stream));
                     SLF_TRY(rho[i].ensure(m, i == cid ? n : 0, stream));
+                    if (warm_on()) SLF_TRY(warm[i].ensure(m, i == cid ? n : 0, stream));
                 }
                 float4* out = pos[cpos].p + n;
                 if (rel()) {
@@ -1976,6 +1998,7 @@ struct World {
                 }
                 launch_emit(slots, etaken.p, cnt, low3, spacing, make_float3(f.velocity.x, f.velocity.y, f.velocity.z),
                             uint32_t(k), next_id, out, vel[cpos].p + n, ids[cid].p + n, rho[cid].p + n, stream);
+                if (warm_on()) SLF_CUDA(cudaMemsetAsync(warm[cid].p + n, 0, k * sizeof(float2), stream));
                 if (rel()) launch_to_relative(p, uint32_t(k), nullptr, estage.p, pos[cpos].p + n, cell[cpos].p + n, stream);
                 n = m;
                 next_id += uint32_t(k);
@@ -2424,7 +2447,6 @@ int32_t slf_create(const slf_settings* settings, slf_world** out) {
     SLF_NEED(out);
     *out = nullptr;
     if (!World::valid(*settings)) return fail(SLF_ERR_INVALID_SETTINGS, "invalid settings");
-    if (settings->warm_start) return fail(SLF_ERR_UNSUPPORTED, "only cold starts are built");
     if (settings->arithmetic != SLF_ARITHMETIC_EXACT && settings->arithmetic != SLF_ARITHMETIC_FAST)
         return fail(SLF_ERR_INVALID_SETTINGS, "unknown arithmetic");
     if (settings->positions != SLF_POSITIONS_ABSOLUTE && settings->positions != SLF_POSITIONS_CELL_RELATIVE)
@@ -2558,7 +2580,6 @@ int32_t slf_load_snapshot(const uint8_t* data, uint64_t size, const slf_settings
     slf_settings lib;
     slf_settings_default(&lib);
     if (library) lib = *library;
-    if (lib.warm_start) return fail(SLF_ERR_UNSUPPORTED, "only cold starts are built");
     if (lib.arithmetic != SLF_ARITHMETIC_EXACT && lib.arithmetic != SLF_ARITHMETIC_FAST)
         return fail(SLF_ERR_INVALID_SETTINGS, "unknown arithmetic");
     if (lib.positions != SLF_POSITIONS_ABSOLUTE && lib.positions != SLF_POSITIONS_CELL_RELATIVE)
