@@ -308,8 +308,15 @@ int32_t slf_profile_read(slf_world* world, slf_profile_entry* out, uint32_t capa
                          uint32_t* count);
 int32_t slf_profile_reset(slf_world* world);
 
-/* Kernel launches this process has issued through the library so far. */
+/* Kernels this process has run through the library so far (a solve run as a CUDA graph counts
+ * the kernels its loop ran). */
 int32_t slf_kernel_launches(uint64_t* out);
+
+/* on = 1 (the default): each DFSPH solve of a step without a tape or profile runs as one CUDA
+ * graph launch whose loop the device ends, and the host waits once a substep.  on = 0: the
+ * solves' launches are queued in batches with a host check between them.  Results are the
+ * same bit for bit; the profiler and recorded solves always take the batched launches. */
+int32_t slf_solver_graphs(slf_world* world, int32_t on);
 
 /* DFSPH solver iterations of the last substep: divergence and density (the per-solve split of
  * FluidReport::iterations, src/fluid/dfsph.rs:89,100). */

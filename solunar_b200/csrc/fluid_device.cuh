@@ -63,6 +63,9 @@ struct Status {
     uint32_t ticket;       // block counter of the last-block reduction
     uint32_t list_max;     // longest neighbour list the last density pass found
     uint32_t iterations;   // pushes of the running solve so far (dfsph.rs:236, 273)
+    uint32_t solved[2];    // pushes of the last divergence (0) and density (1) solve, set when it stops
+    uint32_t bodies;       // loop bodies a solve run as a CUDA graph has started
+    uint32_t overrun;      // such a solve passed max_iterations + 1 bodies and was stopped
 };
 
 // What a solver check records for the adjoint (both null: nothing): at slot it = the solve's

@@ -722,7 +722,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, 
                                                  const float* __restrict__ alpha, const float4* __restrict__ walls,
                                                  float* __restrict__ kappa_w, DD* __restrict__ partial,
                                                  uint32_t* __restrict__ partial_loaded, Status* st,
-                                                 SolveRec rec) {
+                                                 SolveRec rec, unsigned long long loop) {
     // a solve that already stopped leaves the rest of its batch of launches idle
     if (__ldcg(&st->settled)) return;
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
@@ -734,7 +734,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, 
     if (i < p.n)
         rate_particle<WHICH>(p, sc, fl, wl, i, row, FromGlobal{pos, vel}, pos, vel, rho, alpha, walls, kappa_w, rec, slot,
                              err, loaded);
-    residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
+    residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded, loop);
 }
 
 // push_apart (dfsph.rs:184-216) of particle i: the velocity change from each particle's
@@ -774,7 +774,8 @@ __device__ __forceinline__ void push_particle(const Params& p, const StepConsts*
 __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
                                                  float4* __restrict__ vel, const float4* __restrict__ walls,
-                                                 const Status* st, float* __restrict__ applied) {
+                                                 Status* st, float* __restrict__ applied, unsigned long long loop) {
+    loop_bound(p, st, loop);
     if (__ldcg(&st->settled)) return;
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
@@ -1018,6 +1019,7 @@ __global__ void k_unpack3(uint32_t n, const float* __restrict__ in, float4* __re
 static std::atomic<uint64_t> g_launches{0};
 uint64_t kernel_launches() { return g_launches.load(); }
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(int64_t k) { g_launches.fetch_add(uint64_t(k), std::memory_order_relaxed); }
 
 static inline uint32_t blocks_for(uint32_t n) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -1099,22 +1101,22 @@ size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (size
 
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 void* partials, Status* st, SolveRec rec, cudaStream_t s) {
+                 void* partials, Status* st, SolveRec rec, cudaStream_t s, unsigned long long loop) {
     if (!p.n) return;
     uint32_t nb = blocks_for(p.n);
     DD* part = static_cast<DD*>(partials);
     uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
     if (which == 0)
         k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
-                                        part, loaded, st, rec);
+                                        part, loaded, st, rec, loop);
     else
         k_rate<1><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
-                                        part, loaded, st, rec);
+                                        part, loaded, st, rec, loop);
 }
 
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
-                 float4* vel, const float4* walls, const Status* st, float* applied, cudaStream_t s) {
-    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied);
+                 float4* vel, const float4* walls, Status* st, float* applied, cudaStream_t s, unsigned long long loop) {
+    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied, loop);
 }
 
 // Warm start of a solve: the stiffness that applies `share` of the impulse S the particle's last

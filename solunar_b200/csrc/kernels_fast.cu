@@ -543,7 +543,7 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
                                                       const float4* __restrict__ walls, float* __restrict__ kappa,
                                                       DD* __restrict__ partial,
                                                       uint32_t* __restrict__ partial_loaded, Status* st,
-                                                      SolveRec rec) {
+                                                      SolveRec rec, unsigned long long loop) {
     if (__ldcg(&st->settled)) return;
     const uint32_t slot = rec.rate ? __ldcg(&st->iterations) : 0u;
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
@@ -554,7 +554,7 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
     if (i < p.n)
         rate_particle_fast<WHICH, REL>(p, sc, fl, wl, i, row, FromGlobalF{pos, vel}, pos, vel, rho, alpha, walls, kappa,
                                        rec, slot, err, loaded);
-    residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded);
+    residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded, loop);
 }
 
 template <bool REL, class Src>
@@ -593,7 +593,9 @@ template <bool REL>
 __global__ void __launch_bounds__(kBlock) k_push_fast(Params p, const StepConsts* __restrict__ sc, PairLists fpl,
                                                       PairLists wpl, const float4* __restrict__ pos,
                                                       float4* __restrict__ vel, const float4* __restrict__ walls,
-                                                      const Status* st, float* __restrict__ applied) {
+                                                      Status* st, float* __restrict__ applied,
+                                                      unsigned long long loop) {
+    loop_bound(p, st, loop);
     if (__ldcg(&st->settled)) return;
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
@@ -787,7 +789,8 @@ void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLi
 
 void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc, const PairLists& fl,
                       const PairLists& wl, float4* pos, const float4* vel, const float* rho, const float* alpha,
-                      const float4* walls, void* partials, Status* st, SolveRec rec, cudaStream_t s) {
+                      const float4* walls, void* partials, Status* st, SolveRec rec, cudaStream_t s,
+                      unsigned long long loop) {
     if (!p.n) return;
     uint32_t nb = fast_blocks(p.n);
     DD* part = static_cast<DD*>(partials);
@@ -795,24 +798,24 @@ void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc
     float* kw = reinterpret_cast<float*>(pos);
     if (which == 0 && rel)
         k_rate_fast<0, true><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
-                                                   rec);
+                                                   rec, loop);
     else if (which == 0)
         k_rate_fast<0, false><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
-                                                    rec);
+                                                    rec, loop);
     else if (rel)
         k_rate_fast<1, true><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
-                                                   rec);
+                                                   rec, loop);
     else
         k_rate_fast<1, false><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,
-                                                    rec);
+                                                    rec, loop);
 }
 
 void launch_push_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                      const float4* pos, float4* vel, const float4* walls, const Status* st, float* applied,
-                      cudaStream_t s) {
+                      const float4* pos, float4* vel, const float4* walls, Status* st, float* applied,
+                      cudaStream_t s, unsigned long long loop) {
     if (!p.n) return;
-    if (rel) k_push_fast<true><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied);
-    else k_push_fast<false><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied);
+    if (rel) k_push_fast<true><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied, loop);
+    else k_push_fast<false><<<fast_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied, loop);
 }
 
 void launch_viscous_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,

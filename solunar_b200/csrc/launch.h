@@ -52,13 +52,16 @@ size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
 // sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve
 // has settled, so a batch of iterations can be queued ahead of the check that ends it.
-// rec (optional): the check's rates and the velocities it read, recorded for the adjoint
+// rec (optional): the check's rates and the velocities it read, recorded for the adjoint.
+// loop (optional): the while-node handle of a solve captured as a CUDA graph; the check that
+// stops the solve ends that loop, and the push bounds it at max_iterations + 1 bodies.
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
-                 void* partials, Status* st, SolveRec rec, cudaStream_t s);
+                 void* partials, Status* st, SolveRec rec, cudaStream_t s, unsigned long long loop = 0);
 // applied (optional, stride 2): each particle's stiffness impulse sum, for warm starts
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
-                 float4* vel, const float4* walls, const Status* st, float* applied, cudaStream_t s);
+                 float4* vel, const float4* walls, Status* st, float* applied, cudaStream_t s,
+                 unsigned long long loop = 0);
 // warm start: pos.w = share * applied / dt, applied = that stiffness * dt
 void launch_warm_kappa(const Params& p, const StepConsts* sc, float share, float* applied, float4* pos, cudaStream_t s);
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
@@ -108,10 +111,11 @@ void launch_wcsph_force_fast(const Params& p, const StepConsts* sc, const PairLi
 // the stiffness goes into pos.w, as in launch_rate
 void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc, const PairLists& fl,
                       const PairLists& wl, float4* pos, const float4* vel, const float* rho, const float* alpha,
-                      const float4* walls, void* partials, Status* st, SolveRec rec, cudaStream_t s);
+                      const float4* walls, void* partials, Status* st, SolveRec rec, cudaStream_t s,
+                      unsigned long long loop = 0);
 void launch_push_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                      const float4* pos, float4* vel, const float4* walls, const Status* st, float* applied,
-                      cudaStream_t s);
+                      const float4* pos, float4* vel, const float4* walls, Status* st, float* applied,
+                      cudaStream_t s, unsigned long long loop = 0);
 void launch_viscous_fast(bool rel, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                          const float4* pos, const float4* vel, const float* rho, const float4* walls,
                          float4* vel_out, cudaStream_t s);
@@ -160,6 +164,8 @@ void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const
 // kernels launched through this library by the process so far
 uint64_t kernel_launches();
 void note_launch();
+// adds k (negative: takes back launches recorded into a graph, counted when it runs)
+void note_launches(int64_t k);
 
 // message slf_last_error() returns on this thread
 void set_last_error(const std::string& message);

@@ -52,13 +52,28 @@ __device__ __forceinline__ DD dd_add(DD a, DD b) {
     return DD{h, lo - (h - s)};
 }
 
+// The bound of a solve run as a CUDA graph, independent of the stopping check: one thread counts
+// the loop's bodies and ends the loop past max_iterations + 1 of them (the check stops a solve at
+// max_iterations pushes, so only a fault in it gets here).
+__device__ __forceinline__ void loop_bound(const Params& p, Status* st, unsigned long long loop) {
+    if (!loop || blockIdx.x != 0 || threadIdx.x != 0) return;
+    uint32_t bodies = atomicAdd(&st->bodies, 1u) + 1u;
+    if (bodies > p.max_iter + 1u) {
+        st->overrun = 1u;
+        cudaGraphSetConditional(loop, 0u);
+    }
+}
+
 // The error sum of one solver check (dfsph.rs:263-268): a block tree in double-double, block
 // partials in `partial`, and the last block to finish sums them in block order, takes the
 // average over the particles under load and writes the stop decision (dfsph.rs:268-271) into the
 // status.  Deterministic for a given launch shape.
+// `loop`: the while-node handle of a solve run as a CUDA graph (0 when launched on its own); the
+// check that stops the solve also ends the graph's loop.
 template <int WHICH>
 __device__ __forceinline__ void residual_finish(const Params& p, Status* st, DD* __restrict__ partial,
-                                                uint32_t* __restrict__ partial_loaded, double err, uint32_t loaded) {
+                                                uint32_t* __restrict__ partial_loaded, double err, uint32_t loaded,
+                                                unsigned long long loop) {
     // block sum: a fixed shuffle tree in double-double
     DD acc{err, 0.0};
 #pragma unroll
@@ -113,8 +128,13 @@ __device__ __forceinline__ void residual_finish(const Params& p, Status* st, DD*
         bool settled = iterations >= p.min_iter && average <= tol;
         st->average = average;
         st->loaded = cnt;
-        if (settled || iterations >= p.max_iter) st->settled = 1u;
-        else st->iterations = iterations + 1u;  // a push follows
+        if (settled || iterations >= p.max_iter) {
+            st->settled = 1u;
+            st->solved[WHICH] = iterations;
+            if (loop) cudaGraphSetConditional(loop, 0u);
+        } else {
+            st->iterations = iterations + 1u;  // a push follows
+        }
         st->ticket = 0;
     }
 }

@@ -455,6 +455,9 @@ struct World {
             dsites.release(stream);
             gslope.release(stream);
             cudaStreamSynchronize(stream);
+            drop_solve_graphs();
+            for (auto c : cap)
+                if (c) cudaStreamDestroy(c);
             if (d_status) cudaFree(d_status);
             if (d_consts) cudaFree(d_consts);
             if (h_status) cudaFreeHost(h_status);
@@ -840,19 +843,23 @@ struct World {
                                pos[b].p, vel[b].p, d_status, vel_pre, tdev, terrains.empty() ? nullptr : gslope.p,
                                stream);
     }
+    // cs, loop: the stream of a graph capture and the while-node handle of its solve loop
     void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid,
-                   SolveRec rec = SolveRec{nullptr, nullptr}) {
+                   SolveRec rec = SolveRec{nullptr, nullptr}, cudaStream_t cs = nullptr,
+                   unsigned long long loop = 0) {
+        cudaStream_t on = cs ? cs : stream;
         if (fast())
             launch_rate_fast(which, rel(), p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p,
-                             partials.p, d_status, rec, stream);
+                             partials.p, d_status, rec, on, loop);
         else
             launch_rate(which, p, d_consts, fl, wl, pos[a].p, v, rho[nid].p, alpha.p, dwalls.p, partials.p, d_status,
-                        rec, stream);
+                        rec, on, loop);
     }
     void push_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v,
-                   float* applied = nullptr) {
-        if (fast()) launch_push_fast(rel(), p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, applied, stream);
-        else launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, applied, stream);
+                   float* applied = nullptr, cudaStream_t cs = nullptr, unsigned long long loop = 0) {
+        cudaStream_t on = cs ? cs : stream;
+        if (fast()) launch_push_fast(rel(), p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, applied, on, loop);
+        else launch_push(p, d_consts, fl, wl, pos[a].p, v, dwalls.p, d_status, applied, on, loop);
     }
     bool warm_on() const { return s.warm_start && s.solver == SLF_SOLVER_DFSPH; }
     const float2* warm_in() const { return warm_on() ? warm[cid].p : nullptr; }
@@ -1303,6 +1310,8 @@ struct World {
                   SolveRec rec = SolveRec{nullptr, nullptr}) {
         iterations = 0;
         PairLists fl = fluid_lists(), wl = wall_lists();
+        // (a graph's loop body needs launches: no particles, no graph)
+        if (p.n && graphs_for(rec)) return solve_graph(which, p, a, v, nid, fl, wl);
         SLF_CUDA(cudaMemsetAsync(&d_status->settled, 0, 4, stream));
         SLF_CUDA(cudaMemsetAsync(&d_status->iterations, 0, 4, stream));
         const char* rate_name = which == 0 ? "rate_divergence" : "rate_density";
@@ -1354,6 +1363,165 @@ struct World {
         }
     }
 
+    // ---- solves as CUDA graphs ----------------------------------------------------------------
+    // A solve runs as one graph launch: its resets, the warm push, the first check, then a
+    // while node whose body is (push, check).  The check that stops the solve sets the node's
+    // condition to 0 on the device, so the host queues the whole substep and waits once, after
+    // the advance.  The push bounds the loop at max_iterations + 1 bodies by its own count.
+    // Graphs are cached by every value their launches take (slots, buffers, counts, constants),
+    // so a cached graph launches exactly what the eager path would.  The eager path stays for
+    // recorded solves (the adjoint) and for the profiler, which times each launch.
+    static constexpr uint32_t kGraphMaxIterations = 10000;
+    static constexpr size_t kGraphCache = 12;
+    struct SolveGraph {
+        std::vector<uint8_t> key;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t used = 0;
+        uint32_t pre = 0;  // kernels ahead of the loop
+    };
+    bool use_graphs = true;  // slf_solver_graphs
+    std::vector<SolveGraph> solve_graphs;
+    uint64_t graph_clock = 0;
+    cudaStream_t cap[2] = {nullptr, nullptr};
+    uint32_t graph_solves = 0;  // solves of the running substep that ran as graphs
+
+    bool graphs_for(const SolveRec& rec) const {
+        return use_graphs && !prof.on && !rec.rate && s.max_iterations <= kGraphMaxIterations;
+    }
+    void drop_solve_graphs() {
+        for (auto& g : solve_graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        solve_graphs.clear();
+    }
+    template <class T> static void key_add(std::vector<uint8_t>& k, const T& v) {
+        const uint8_t* b = reinterpret_cast<const uint8_t*>(&v);
+        k.insert(k.end(), b, b + sizeof(T));
+    }
+    static void key_lists(std::vector<uint8_t>& k, const PairLists& l) {
+        key_add(k, l.cap);
+        key_add(k, l.e);
+        key_add(k, l.count);
+        key_add(k, l.order);
+    }
+    std::vector<uint8_t> solve_key(int which, const Params& p, int a, float4* v, int nid, const PairLists& fl,
+                                   const PairLists& wl) {
+        static_assert(sizeof(Params) % 4 == 0, "Params holds 4-byte fields only");
+        std::vector<uint8_t> k;
+        key_add(k, which);
+        key_add(k, int32_t(fast()));
+        key_add(k, int32_t(rel()));
+        key_add(k, int32_t(warm_on()));
+        key_add(k, p);
+        key_lists(k, fl);
+        key_lists(k, wl);
+        for (const void* q : {(const void*)pos[a].p, (const void*)v, (const void*)rho[nid].p, (const void*)alpha.p,
+                              (const void*)dwalls.p, (const void*)partials.p, (const void*)d_status,
+                              (const void*)d_consts, (const void*)(warm_on() ? warm[nid].p : nullptr)})
+            key_add(k, q);
+        return k;
+    }
+
+    // records the solve's launches into a new graph on cap[0] (the loop body on cap[1])
+    int32_t capture_solve(int which, const Params& p, int a, float4* v, int nid, const PairLists& fl,
+                          const PairLists& wl, uint32_t& pre) {
+        cudaStream_t cs = cap[0];
+        SLF_CUDA(cudaMemsetAsync(&d_status->settled, 0, 4, cs));
+        SLF_CUDA(cudaMemsetAsync(&d_status->iterations, 0, 4, cs));
+        SLF_CUDA(cudaMemsetAsync(&d_status->bodies, 0, 4, cs));
+        SLF_CUDA(cudaMemsetAsync(&d_status->ticket, 0, 4, cs));
+        float* applied = nullptr;
+        if (warm_on()) {
+            applied = reinterpret_cast<float*>(warm[nid].p) + which;
+            launch_warm_kappa(p, d_consts, 0.5f, applied, pos[a].p, cs);
+            push_pass(p, fl, wl, a, v, nullptr, cs);
+            pre += 2;
+        }
+        cudaStreamCaptureStatus cst;
+        cudaGraph_t graph = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        SLF_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps));
+        cudaGraphConditionalHandle loop;
+        SLF_CUDA(cudaGraphConditionalHandleCreate(&loop, graph, 1u, cudaGraphCondAssignDefault));
+        rate_pass(which, p, fl, wl, a, v, nid, SolveRec{nullptr, nullptr}, cs, loop);
+        pre += 1;
+        SLF_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps));
+        // the node parameters are a union without a default constructor: zeroed raw storage
+        alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+        std::memset(raw, 0, sizeof raw);
+        cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = loop;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        SLF_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &np));
+        SLF_CUDA(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        SLF_CUDA(cudaStreamBeginCaptureToGraph(cap[1], body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        push_pass(p, fl, wl, a, v, applied, cap[1], loop);
+        rate_pass(which, p, fl, wl, a, v, nid, SolveRec{nullptr, nullptr}, cap[1], loop);
+        cudaGraph_t done = nullptr;
+        SLF_CUDA(cudaStreamEndCapture(cap[1], &done));
+        return SLF_OK;
+    }
+
+    int32_t solve_graph(int which, const Params& p, int a, float4* v, int nid, const PairLists& fl,
+                        const PairLists& wl) {
+        std::vector<uint8_t> key = solve_key(which, p, a, v, nid, fl, wl);
+        SolveGraph* hit = nullptr;
+        for (auto& g : solve_graphs)
+            if (g.key == key) hit = &g;
+        if (!hit) {
+            for (auto& c : cap)
+                if (!c) SLF_CUDA(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
+            SolveGraph g;
+            g.key = std::move(key);
+            uint64_t before = kernel_launches();
+            SLF_CUDA(cudaStreamBeginCapture(cap[0], cudaStreamCaptureModeThreadLocal));
+            int32_t st = capture_solve(which, p, a, v, nid, fl, wl, g.pre);
+            cudaGraph_t graph = nullptr;
+            cudaError_t ended = cudaStreamEndCapture(cap[0], &graph);
+            // launches recorded into the graph ran nothing yet; they count when it runs
+            note_launches(-int64_t(kernel_launches() - before));
+            if (st != SLF_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            SLF_CUDA(ended);
+            cudaError_t made = cudaGraphInstantiate(&g.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            SLF_CUDA(made);
+            if (solve_graphs.size() >= kGraphCache) {
+                auto old = std::min_element(solve_graphs.begin(), solve_graphs.end(),
+                                            [](const SolveGraph& x, const SolveGraph& y) { return x.used < y.used; });
+                cudaGraphExecDestroy(old->exec);
+                solve_graphs.erase(old);
+            }
+            solve_graphs.push_back(std::move(g));
+            hit = &solve_graphs.back();
+        }
+        hit->used = ++graph_clock;
+        SLF_CUDA(cudaGraphLaunch(hit->exec, stream));
+        note_launches(hit->pre);
+        graph_solves += 1;
+        return SLF_OK;
+    }
+
+    // After a substep whose solves ran as graphs (status read back): the solves' iteration
+    // counts, their loop kernels in the launch count, and the checks the eager path makes per
+    // solve (the lists' room, the stop flag).
+    int32_t finish_graph_solves(uint32_t& div_it, uint32_t& den_it) {
+        if (h_status->overrun) return fail(SLF_ERR_TIMEOUT, "solver loop passed max_iterations + 1 bodies");
+        SLF_TRY(lists_fit());
+        div_it = h_status->solved[0];
+        den_it = h_status->solved[1];
+        note_launches(2 * int64_t(div_it + den_it));
+        expected_iterations[0] = std::max<uint32_t>(div_it, 1u);
+        expected_iterations[1] = std::max<uint32_t>(den_it, 1u);
+        return SLF_OK;
+    }
+
     // The launches of a solve after its stopping check did nothing; their profile entries
     // go under "solver_idle" so the kernels' averages hold only launches that worked.
     void relabel_idle(size_t first, const std::vector<int>& kinds, uint32_t iterations) {
@@ -1392,6 +1560,7 @@ struct World {
         SLF_TRY(sort_into(a));
         int nid = 1 - cid;
         SLF_TRY(reset_status());
+        graph_solves = 0;
         launch_set_consts(consts(dt), d_consts, stream);
         PairLists fl = fluid_lists(), wl = wall_lists();
         timed("density_alpha", bytes_per_particle::density_dfsph,
@@ -1422,6 +1591,7 @@ struct World {
         }
         timed("advance", bytes_per_particle::advance, [&] { advance_pass(p, a, b, pre); });
         SLF_TRY(read_status());
+        if (graph_solves) SLF_TRY(finish_graph_solves(div_it, den_it));
         SLF_TRY(check_state());
         held = h_status->held;
         iterations = div_it + den_it;
@@ -2775,6 +2945,12 @@ int32_t slf_step_backward(slf_world* world, const float* dpositions, const float
         SLF_NEED(dvelocities);
     }
     return world->w.step_backward(dpositions, dvelocities, n, dpositions0, dvelocities0, out);
+}
+
+int32_t slf_solver_graphs(slf_world* world, int32_t on) {
+    SLF_WORLD(world);
+    world->w.use_graphs = on != 0;
+    return SLF_OK;
 }
 
 int32_t slf_profile_enable(slf_world* world, int32_t on) {

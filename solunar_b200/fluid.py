@@ -78,6 +78,7 @@ def load_library():
         "slf_write_state": [vp, fp, fp, ctypes.c_uint64],
         "slf_get_stream": [vp, ctypes.POINTER(vp)],
         "slf_profile_enable": [vp, ctypes.c_int32],
+        "slf_solver_graphs": [vp, ctypes.c_int32],
         "slf_profile_read": [vp, ctypes.POINTER(CProfileEntry), ctypes.c_uint32, u32p],
         "slf_profile_reset": [vp],
         "slf_kernel_launches": [u64p],
@@ -388,7 +389,13 @@ class FluidWorld:
         return s.value or 0
 
     def profile(self, on: bool = True):
+        """Times each kernel launch with CUDA events (solves then run launch by launch)."""
         _check(_lib.slf_profile_enable(self._h, 1 if on else 0))
+
+    def solver_graphs(self, on: bool = True):
+        """Runs each DFSPH solve as one CUDA graph whose loop the device ends (the default), or
+        as batches of launches with a host check between them; the results are identical."""
+        _check(_lib.slf_solver_graphs(self._h, 1 if on else 0))
 
     def profile_reset(self):
         _check(_lib.slf_profile_reset(self._h))
