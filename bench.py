@@ -381,8 +381,7 @@ def main():
         e0.record(stream)
         world.write_state_ptr(host_pos.data_ptr(), host_vel.data_ptr(), n)
         r = world.step(sc.dt)
-        world.read_positions_ptr(host_pos.data_ptr(), n)
-        world.read_velocities_ptr(host_vel.data_ptr(), n)
+        world.read_state_ptr(host_pos.data_ptr(), host_vel.data_ptr(), n)
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)

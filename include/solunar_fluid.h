@@ -209,6 +209,8 @@ int32_t slf_compute_densities(slf_world* world);
 int32_t slf_read_ids(const slf_world* world, uint32_t* out, uint64_t n);
 int32_t slf_read_positions(const slf_world* world, float* out, uint64_t n);
 int32_t slf_read_velocities(const slf_world* world, float* out, uint64_t n);
+/* Positions and velocities together (xyz triples each), with one wait for the device. */
+int32_t slf_read_state(const slf_world* world, float* positions, float* velocities, uint64_t n);
 int32_t slf_read_densities(const slf_world* world, float* out, uint64_t n);
 
 /* FluidWorld::neighbors_of (mod.rs:612-614) for every particle at once, as the lists the
@@ -227,7 +229,9 @@ int32_t slf_state_hash(const slf_world* world, uint64_t* out);
 
 /* Overwrites the positions and velocities of the current particles, in the current order (the
  * arrays FluidWorld::positions / velocities expose, mod.rs:397-403).  n must equal slf_len().
- * A host that owns the particle arrays uploads them with this before a step. */
+ * A host that owns the particle arrays uploads them with this before a step.  A non finite
+ * value (found on the device as the arrays unpack) returns SLF_ERR_NON_FINITE and leaves the
+ * world's state as it was. */
 int32_t slf_write_state(slf_world* world, const float* positions, const float* velocities,
                         uint64_t n);
 

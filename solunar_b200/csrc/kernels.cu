@@ -1008,10 +1008,13 @@ __global__ void k_pack3(uint32_t n, const float4* __restrict__ in, float* __rest
     out[3 * i + 2] = v.z;
 }
 
-__global__ void k_unpack3(uint32_t n, const float* __restrict__ in, float4* __restrict__ out) {
+// xyz triples into float4 slots; `bad` (optional) counts triples with a non finite component
+__global__ void k_unpack3(uint32_t n, const float* __restrict__ in, float4* __restrict__ out, uint32_t* bad) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    out[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0f);
+    float x = in[3 * i], y = in[3 * i + 1], z = in[3 * i + 2];
+    if (bad && !(isfinite(x) && isfinite(y) && isfinite(z))) atomicAdd(bad, 1u);
+    out[i] = make_float4(x, y, z, 0.0f);
 }
 
 // ---- launchers ------------------------------------------------------------------------------
@@ -1030,8 +1033,8 @@ void launch_pack3(uint32_t n, const float4* in, float* out, cudaStream_t s) {
     if (n) k_pack3<<<blocks_for(n), kBlock, 0, s>>>(n, in, out);
 }
 
-void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s) {
-    if (n) k_unpack3<<<blocks_for(n), kBlock, 0, s>>>(n, in, out);
+void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s, uint32_t* bad) {
+    if (n) k_unpack3<<<blocks_for(n), kBlock, 0, s>>>(n, in, out, bad);
 }
 
 void launch_state_stats(const Params& p, const float4* pos, const float4* vel, Status* st, cudaStream_t s) {

@@ -673,7 +673,7 @@ __global__ void k_advance_rel(Params p, const StepConsts* __restrict__ sc, const
 
 // absolute f32 positions -> offset in [0, r) and cell, cell = floor(x / r) as cell_of has it
 __global__ void k_to_relative(Params p, uint32_t n, const float* __restrict__ xyz, const float4* __restrict__ abs4,
-                              float4* __restrict__ pos, int4* __restrict__ cells) {
+                              float4* __restrict__ pos, int4* __restrict__ cells, uint32_t* bad) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float x, y, z;
@@ -687,6 +687,7 @@ __global__ void k_to_relative(Params p, uint32_t n, const float* __restrict__ xy
         y = q.y;
         z = q.z;
     }
+    if (bad && !(isfinite(x) && isfinite(y) && isfinite(z))) atomicAdd(bad, 1u);
     int3 c = cell_of(p, x, y, z);
     const double r = p.radius;
     float ox = float(double(x) - double(c.x) * r), oy = float(double(y) - double(c.y) * r),
@@ -836,8 +837,8 @@ void launch_advance_rel(const Params& p, const StepConsts* sc, const float4* pos
 }
 
 void launch_to_relative(const Params& p, uint32_t n, const float* xyz, const float4* abs4, float4* pos, int4* cells,
-                        cudaStream_t s) {
-    if (n) k_to_relative<<<fast_blocks(n), kBlock, 0, s>>>(p, n, xyz, abs4, pos, cells);
+                        cudaStream_t s, uint32_t* bad) {
+    if (n) k_to_relative<<<fast_blocks(n), kBlock, 0, s>>>(p, n, xyz, abs4, pos, cells, bad);
 }
 
 void launch_from_relative(const Params& p, uint32_t n, const float4* pos, const int4* cells, float* xyz,

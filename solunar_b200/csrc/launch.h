@@ -95,7 +95,8 @@ void launch_set_consts(const StepConsts& c, StepConsts* out, cudaStream_t s);
 
 // xyz triples <-> float4
 void launch_pack3(uint32_t n, const float4* in, float* out, cudaStream_t s);
-void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s);
+// bad (optional): incremented for each triple with a non finite component
+void launch_unpack3(uint32_t n, const float* in, float4* out, cudaStream_t s, uint32_t* bad = nullptr);
 
 // FAST arithmetic variants (kernels_fast.cu): same lists, order and sums, fused rounding; the
 // lists hold indexes only (with the cell step in their top bits) and each pass recomputes the
@@ -121,9 +122,10 @@ void launch_viscous_fast(bool rel, const Params& p, const StepConsts* sc, const 
                          float4* vel_out, cudaStream_t s);
 void launch_advance_rel(const Params& p, const StepConsts* sc, const float4* pos_in, const int4* cells_in,
                         float4* pos_out, int4* cells_out, float4* vel, Status* st, float4* vel_pre, cudaStream_t s);
-// absolute positions (xyz triples, or float4 when xyz is null) -> offsets and cells; and back
+// absolute positions (xyz triples, or float4 when xyz is null) -> offsets and cells; and back.
+// bad (optional): incremented for each position with a non finite component
 void launch_to_relative(const Params& p, uint32_t n, const float* xyz, const float4* abs4, float4* pos, int4* cells,
-                        cudaStream_t s);
+                        cudaStream_t s, uint32_t* bad = nullptr);
 void launch_from_relative(const Params& p, uint32_t n, const float4* pos, const int4* cells, float* xyz,
                           cudaStream_t s);
 void launch_state_stats_rel(const Params& p, const int4* cells, const float4* vel, Status* st, cudaStream_t s);

@@ -1311,7 +1311,7 @@ struct World {
         iterations = 0;
         PairLists fl = fluid_lists(), wl = wall_lists();
         // (a graph's loop body needs launches: no particles, no graph)
-        if (p.n && graphs_for(rec)) return solve_graph(which, p, a, v, nid, fl, wl);
+        if (p.n && graphs_for(rec)) return solve_graph(which, p, a, v, nid, fl, wl, rec, iterations);
         SLF_CUDA(cudaMemsetAsync(&d_status->settled, 0, 4, stream));
         SLF_CUDA(cudaMemsetAsync(&d_status->iterations, 0, 4, stream));
         const char* rate_name = which == 0 ? "rate_divergence" : "rate_density";
@@ -1370,7 +1370,8 @@ struct World {
     // the advance.  The push bounds the loop at max_iterations + 1 bodies by its own count.
     // Graphs are cached by every value their launches take (slots, buffers, counts, constants),
     // so a cached graph launches exactly what the eager path would.  The eager path stays for
-    // recorded solves (the adjoint) and for the profiler, which times each launch.
+    // the profiler, which times each launch.  A recorded solve (the adjoint's) runs as a graph too
+    // but is waited for at once, as its record is copied out by its iteration count.
     static constexpr uint32_t kGraphMaxIterations = 10000;
     static constexpr size_t kGraphCache = 12;
     struct SolveGraph {
@@ -1383,10 +1384,10 @@ struct World {
     std::vector<SolveGraph> solve_graphs;
     uint64_t graph_clock = 0;
     cudaStream_t cap[2] = {nullptr, nullptr};
-    uint32_t graph_solves = 0;  // solves of the running substep that ran as graphs
+    uint32_t graph_solves = 0;  // bit w: solve w of the running substep ran as a graph, not yet read
 
-    bool graphs_for(const SolveRec& rec) const {
-        return use_graphs && !prof.on && !rec.rate && s.max_iterations <= kGraphMaxIterations;
+    bool graphs_for(const SolveRec&) const {
+        return use_graphs && !prof.on && s.max_iterations <= kGraphMaxIterations;
     }
     void drop_solve_graphs() {
         for (auto& g : solve_graphs)
@@ -1404,7 +1405,7 @@ struct World {
         key_add(k, l.order);
     }
     std::vector<uint8_t> solve_key(int which, const Params& p, int a, float4* v, int nid, const PairLists& fl,
-                                   const PairLists& wl) {
+                                   const PairLists& wl, const SolveRec& rec) {
         static_assert(sizeof(Params) % 4 == 0, "Params holds 4-byte fields only");
         std::vector<uint8_t> k;
         key_add(k, which);
@@ -1416,14 +1417,15 @@ struct World {
         key_lists(k, wl);
         for (const void* q : {(const void*)pos[a].p, (const void*)v, (const void*)rho[nid].p, (const void*)alpha.p,
                               (const void*)dwalls.p, (const void*)partials.p, (const void*)d_status,
-                              (const void*)d_consts, (const void*)(warm_on() ? warm[nid].p : nullptr)})
+                              (const void*)d_consts, (const void*)(warm_on() ? warm[nid].p : nullptr),
+                              (const void*)rec.rate, (const void*)rec.vel})
             key_add(k, q);
         return k;
     }
 
     // records the solve's launches into a new graph on cap[0] (the loop body on cap[1])
     int32_t capture_solve(int which, const Params& p, int a, float4* v, int nid, const PairLists& fl,
-                          const PairLists& wl, uint32_t& pre) {
+                          const PairLists& wl, const SolveRec& rec, uint32_t& pre) {
         cudaStream_t cs = cap[0];
         SLF_CUDA(cudaMemsetAsync(&d_status->settled, 0, 4, cs));
         SLF_CUDA(cudaMemsetAsync(&d_status->iterations, 0, 4, cs));
@@ -1443,7 +1445,7 @@ struct World {
         SLF_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps));
         cudaGraphConditionalHandle loop;
         SLF_CUDA(cudaGraphConditionalHandleCreate(&loop, graph, 1u, cudaGraphCondAssignDefault));
-        rate_pass(which, p, fl, wl, a, v, nid, SolveRec{nullptr, nullptr}, cs, loop);
+        rate_pass(which, p, fl, wl, a, v, nid, rec, cs, loop);
         pre += 1;
         SLF_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps));
         // the node parameters are a union without a default constructor: zeroed raw storage
@@ -1460,15 +1462,15 @@ struct World {
         cudaGraph_t body = np.conditional.phGraph_out[0];
         SLF_CUDA(cudaStreamBeginCaptureToGraph(cap[1], body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         push_pass(p, fl, wl, a, v, applied, cap[1], loop);
-        rate_pass(which, p, fl, wl, a, v, nid, SolveRec{nullptr, nullptr}, cap[1], loop);
+        rate_pass(which, p, fl, wl, a, v, nid, rec, cap[1], loop);
         cudaGraph_t done = nullptr;
         SLF_CUDA(cudaStreamEndCapture(cap[1], &done));
         return SLF_OK;
     }
 
     int32_t solve_graph(int which, const Params& p, int a, float4* v, int nid, const PairLists& fl,
-                        const PairLists& wl) {
-        std::vector<uint8_t> key = solve_key(which, p, a, v, nid, fl, wl);
+                        const PairLists& wl, const SolveRec& rec, uint32_t& iterations) {
+        std::vector<uint8_t> key = solve_key(which, p, a, v, nid, fl, wl, rec);
         SolveGraph* hit = nullptr;
         for (auto& g : solve_graphs)
             if (g.key == key) hit = &g;
@@ -1479,7 +1481,7 @@ struct World {
             g.key = std::move(key);
             uint64_t before = kernel_launches();
             SLF_CUDA(cudaStreamBeginCapture(cap[0], cudaStreamCaptureModeThreadLocal));
-            int32_t st = capture_solve(which, p, a, v, nid, fl, wl, g.pre);
+            int32_t st = capture_solve(which, p, a, v, nid, fl, wl, rec, g.pre);
             cudaGraph_t graph = nullptr;
             cudaError_t ended = cudaStreamEndCapture(cap[0], &graph);
             // launches recorded into the graph ran nothing yet; they count when it runs
@@ -1504,21 +1506,29 @@ struct World {
         hit->used = ++graph_clock;
         SLF_CUDA(cudaGraphLaunch(hit->exec, stream));
         note_launches(hit->pre);
-        graph_solves += 1;
+        graph_solves |= 1u << which;
+        if (!rec.rate) return SLF_OK;
+        SLF_TRY(read_status());
+        uint32_t its[2] = {0, 0};
+        SLF_TRY(finish_graph_solves(its));
+        iterations = its[which];
         return SLF_OK;
     }
 
-    // After a substep whose solves ran as graphs (status read back): the solves' iteration
-    // counts, their loop kernels in the launch count, and the checks the eager path makes per
-    // solve (the lists' room, the stop flag).
-    int32_t finish_graph_solves(uint32_t& div_it, uint32_t& den_it) {
+    // After solves that ran as graphs (status read back): their iteration counts, their loop
+    // kernels in the launch count, and the checks the batched path makes per solve (the lists'
+    // room, the stop flag).  its[w] is set for each solve w that ran.
+    int32_t finish_graph_solves(uint32_t its[2]) {
+        uint32_t ran = graph_solves;
+        graph_solves = 0;
         if (h_status->overrun) return fail(SLF_ERR_TIMEOUT, "solver loop passed max_iterations + 1 bodies");
         SLF_TRY(lists_fit());
-        div_it = h_status->solved[0];
-        den_it = h_status->solved[1];
-        note_launches(2 * int64_t(div_it + den_it));
-        expected_iterations[0] = std::max<uint32_t>(div_it, 1u);
-        expected_iterations[1] = std::max<uint32_t>(den_it, 1u);
+        for (int w = 0; w < 2; ++w)
+            if (ran & (1u << w)) {
+                its[w] = h_status->solved[w];
+                note_launches(2 * int64_t(its[w]));
+                expected_iterations[w] = std::max<uint32_t>(its[w], 1u);
+            }
         return SLF_OK;
     }
 
@@ -1591,7 +1601,12 @@ struct World {
         }
         timed("advance", bytes_per_particle::advance, [&] { advance_pass(p, a, b, pre); });
         SLF_TRY(read_status());
-        if (graph_solves) SLF_TRY(finish_graph_solves(div_it, den_it));
+        if (graph_solves) {
+            uint32_t its[2] = {div_it, den_it};
+            SLF_TRY(finish_graph_solves(its));
+            div_it = its[0];
+            den_it = its[1];
+        }
         SLF_TRY(check_state());
         held = h_status->held;
         iterations = div_it + den_it;
@@ -2460,25 +2475,46 @@ struct World {
         return SLF_OK;
     }
 
+    // Uploads the caller's state into a free slot, checking it on the device as it unpacks and
+    // folding the box and speed the next step needs, then waits once: a state with a non finite
+    // value is refused and the committed one stays.
     int32_t write_state(const float* p, const float* v, uint64_t k) {
         SLF_TRY(flush());
         if (k != n) return fail(SLF_ERR_INVALID_ARGUMENT, "n must equal slf_len()");
-        for (uint64_t i = 0; i < k; ++i)
-            if (!finite3(p + 3 * i) || !finite3(v + 3 * i))
-                return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
-        if (rel()) {
-            SLF_TRY(stage.ensure(3 * k, 0, stream));
-            SLF_CUDA(cudaMemcpyAsync(stage.p, p, k * 12, cudaMemcpyHostToDevice, stream));
-            launch_to_relative(params(), uint32_t(k), stage.p, nullptr, pos[cpos].p, cell[cpos].p, stream);
-            SLF_TRY(sync());
-        } else {
-            SLF_TRY(write_vec(pos[cpos], p, k));
-        }
-        SLF_TRY(write_vec(vel[cpos], v, k));
-        SLF_TRY(sync());
+        if (!k) return SLF_OK;
+        int t = (cpos + 1) % 3;
+        SLF_TRY(stage.ensure(6 * k, 0, stream));
+        SLF_TRY(reset_status());
+        uint32_t* bad = &d_status->nonfinite;
+        SLF_CUDA(cudaMemcpyAsync(stage.p, p, k * 12, cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(stage.p + 3 * k, v, k * 12, cudaMemcpyHostToDevice, stream));
+        Params pr = params();
+        if (rel()) launch_to_relative(pr, uint32_t(k), stage.p, nullptr, pos[t].p, cell[t].p, stream, bad);
+        else launch_unpack3(uint32_t(k), stage.p, pos[t].p, stream, bad);
+        launch_unpack3(uint32_t(k), stage.p + 3 * k, vel[t].p, stream, bad);
+        if (rel()) launch_state_stats_rel(pr, cell[t].p, vel[t].p, d_status, stream);
+        else launch_state_stats(pr, pos[t].p, vel[t].p, d_status, stream);
+        SLF_TRY(read_status());
         lists_valid = false;
-        stats_fresh = false;
+        if (h_status->nonfinite) {
+            stats_fresh = false;
+            return fail(SLF_ERR_NON_FINITE, "non finite value in fluid particle");
+        }
+        cpos = t;
+        stats_fresh = true;
         return SLF_OK;
+    }
+
+    // positions and velocities into the caller's buffers with one wait
+    int32_t read_state(float* p, float* v, uint64_t k) {
+        if (!k) return SLF_OK;
+        SLF_TRY(stage.ensure(6 * k, 0, stream));
+        if (rel()) launch_from_relative(params(), uint32_t(k), pos[cpos].p, cell[cpos].p, stage.p, stream);
+        else launch_pack3(uint32_t(k), pos[cpos].p, stage.p, stream);
+        launch_pack3(uint32_t(k), vel[cpos].p, stage.p + 3 * k, stream);
+        SLF_CUDA(cudaMemcpyAsync(p, stage.p, k * 12, cudaMemcpyDeviceToHost, stream));
+        SLF_CUDA(cudaMemcpyAsync(v, stage.p + 3 * k, k * 12, cudaMemcpyDeviceToHost, stream));
+        return sync();
     }
 
     template <class T> int32_t read_plain(const DevBuf<T>& b, T* out, uint64_t k) {
@@ -2864,6 +2900,17 @@ int32_t slf_read_positions(const slf_world* world, float* out, uint64_t n) {
     if (n) SLF_NEED(out);
     World& w = const_cast<World&>(world->w);
     return w.read_positions(out, n);
+}
+
+int32_t slf_read_state(const slf_world* world, float* positions, float* velocities, uint64_t n) {
+    SLF_WORLD(world);
+    SLF_TRY(prep_read(world, n));
+    if (n) {
+        SLF_NEED(positions);
+        SLF_NEED(velocities);
+    }
+    World& w = const_cast<World&>(world->w);
+    return w.read_state(positions, velocities, n);
 }
 
 int32_t slf_read_velocities(const slf_world* world, float* out, uint64_t n) {

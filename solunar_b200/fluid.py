@@ -69,6 +69,7 @@ def load_library():
         "slf_read_ids": [vp, u32p, ctypes.c_uint64],
         "slf_read_positions": [vp, fp, ctypes.c_uint64],
         "slf_read_velocities": [vp, fp, ctypes.c_uint64],
+        "slf_read_state": [vp, fp, fp, ctypes.c_uint64],
         "slf_read_densities": [vp, fp, ctypes.c_uint64],
         "slf_neighbor_lists": [vp, u32p, ctypes.c_uint64, u32p, ctypes.c_uint64, u64p],
         "slf_wall_neighbor_lists": [vp, u32p, ctypes.c_uint64, u32p, ctypes.c_uint64, u64p],
@@ -382,6 +383,11 @@ class FluidWorld:
 
     def read_velocities_ptr(self, ptr: int, n: int):
         _check(_lib.slf_read_velocities(self._h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)), n))
+
+    def read_state_ptr(self, positions_ptr: int, velocities_ptr: int, n: int):
+        """Positions and velocities into raw host pointers (pinned buffers), one wait."""
+        fp = ctypes.POINTER(ctypes.c_float)
+        _check(_lib.slf_read_state(self._h, ctypes.cast(positions_ptr, fp), ctypes.cast(velocities_ptr, fp), n))
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

@@ -248,3 +248,15 @@ def test_wcsph_recorded_tape_gives_identical_gradients(gpu_lib, adjoint):
     dp, dv, pr = taped_gradients(w, STEPS, DT, 0, target)
     assert np.array_equal(dp, dp0) and np.array_equal(dv, dv0)
     same_params(pr, params)
+
+
+@pytest.mark.parametrize("every", [0, 2])
+def test_dfsph_gradients_do_not_depend_on_how_solves_launch(gpu_lib, dfsph_adjoint, every):
+    # the fixture's world ran its solves as CUDA graphs (the default); here they run in batches of
+    # launches with host checks between them, forward and recorded alike
+    pos, vel, target, dp0, dv0, params = dfsph_adjoint
+    w, _, _ = dfsph_run(gpu_lib.FluidWorld)
+    w.solver_graphs(False)
+    dp, dv, pr = taped_gradients(w, DFSPH_STEPS, DFSPH_DT, every, target)
+    assert np.array_equal(dp, dp0) and np.array_equal(dv, dv0)
+    same_params(pr, params)
