@@ -53,8 +53,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--profile-steps", type=int, default=8,
                     help="steps of the per-kernel CUDA-event pass behind the roofline")
-    ap.add_argument("--warm-steps", type=int, default=10,
-                    help="timed steps of the opt-in warm-started leg on its own world (0 skips it)")
+    ap.add_argument("--warm-steps", type=int, default=None,
+                    help="timed steps of the opt-in warm-started leg on its own world, after the same "
+                         "warm-up (default: --steps, the cold run's window; 0 skips it)")
     ap.add_argument("--no-graphs", action="store_true", help="queue the solves in host-checked batches")
     ap.add_argument("--adjoint-every", type=int, default=0,
                     help="tape checkpoint spacing of the forward+adjoint leg; 0 records every substep")
@@ -454,7 +455,8 @@ def main():
     # impulse) on its own world from the same initial state: the reference cold-starts, so this is
     # a variant beside the headline, not the headline
     warm = None
-    if args.warm_steps > 0 and sc.settings.solver.name == "DFSPH":
+    warm_steps = args.steps if args.warm_steps is None else args.warm_steps
+    if warm_steps > 0 and sc.settings.solver.name == "DFSPH":
         import dataclasses
 
         wsc = dataclasses.replace(sc, settings=dataclasses.replace(sc.settings, warm_start=True))
@@ -467,7 +469,7 @@ def main():
         barrier()
         w_ms = 0.0
         w_sub = w_its = 0
-        for _ in range(args.warm_steps):
+        for _ in range(warm_steps):
             flush.zero_()
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
@@ -481,7 +483,7 @@ def main():
             w_its += r.iterations
         ww.close()
         w_all, w_ms = reduce_timing(w_sub, w_ms, world_size, dev)
-        warm = {"value": w_all / (w_ms / 1e3), "unit": UNIT, "steps": args.warm_steps,
+        warm = {"value": w_all / (w_ms / 1e3), "unit": UNIT, "steps": warm_steps,
                 "after_steps": max(args.warmup, 3), "substeps": w_sub,
                 "solver_iterations_per_substep": w_its / max(w_sub, 1),
                 "setting": "warm_start=1: one push at half the stiffness impulse of the particle's last solve"}
