@@ -262,7 +262,9 @@ typedef struct slf_param_grads {
  * while recording.  WCSPH and DFSPH steps; UNSUPPORTED with cell-relative positions, terrain
  * or warm_start. */
 int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
-/* Stops recording and frees the tape. */
+/* Stops recording.  The tape's device buffers (substep records, checkpoints) stay with the world
+ * and are reused by the next tape, so the rounds of an optimisation loop record without
+ * allocating; slf_destroy frees them. */
 int32_t slf_tape_end(slf_world* world);
 /* Reverse pass over every step recorded since slf_tape_begin.  dpositions, dvelocities: dL/d of
  * the current positions and velocities (xyz triples, current order, n = slf_len()).  Writes

@@ -22,7 +22,7 @@ namespace slf {
 __device__ __forceinline__ uint32_t listed(const PairLists& l, bool packed, uint32_t i, uint32_t k) {
     size_t at = (size_t(i >> 5) * l.cap + k) * 32u + (i & 31u);
     // FAST entries carry the cell step in their top six bits (zero steps: absolute positions)
-    return packed ? l.e[at].x : (reinterpret_cast<const uint32_t*>(l.e)[at] & ((1u << 26) - 1u));
+    return packed ? SLF_LIST_LOAD(&l.e[at]).x : (SLF_LIST_LOAD(reinterpret_cast<const uint32_t*>(l.e) + at) & ((1u << 26) - 1u));
 }
 
 __device__ __forceinline__ uint32_t listed_count(const PairLists& l, uint32_t i) {
@@ -43,19 +43,40 @@ __device__ __forceinline__ void grad_factor(const Params& p, float d, float& g, 
 
 // Walks i's list four entries at a time: gather(j) for all four first, so their loads are in
 // flight together, then body(j, gathered) for each in list order (the sums keep their order).
-template <class G, class Gather, class Body>
+// PREFETCH: the next four entries are requested before the bodies run (past the end the last
+// entry is read again and not used); walks that gather several records a neighbour skip it, as
+// the registers it holds cost them occupancy.
+template <class G, bool PREFETCH = true, class Gather, class Body>
 __device__ __forceinline__ void walk4(const PairLists& l, bool packed, uint32_t i, Gather&& gather, Body&& body) {
     uint32_t n = listed_count(l, i);
+    if (n == 0) return;
+    uint32_t j[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) j[u] = listed(l, packed, i, u < (int)n ? u : n - 1);
     for (uint32_t k = 0; k < n; k += 4) {
-        uint32_t j[4];
         G g[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) j[u] = listed(l, packed, i, k + u < n ? k + u : n - 1);
-#pragma unroll
         for (int u = 0; u < 4; ++u) g[u] = gather(j[u]);
+        uint32_t next[4];
+        if (PREFETCH) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                uint32_t kk = k + 4 + u;
+                next[u] = listed(l, packed, i, kk < n ? kk : n - 1);
+            }
+        }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             if (k + u < n) body(j[u], g[u]);
+        if (!PREFETCH) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                uint32_t kk = k + 4 + u;
+                next[u] = listed(l, packed, i, kk < n ? kk : n - 1);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) j[u] = next[u];
     }
 }
 
@@ -395,7 +416,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
 
 // The velocity adjoint before the iteration: w plus the rate pass's transpose (a push on the
 // rate adjoint); and the positions' share of both passes, through grad W.
-__global__ void __launch_bounds__(kBlock) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+// four blocks a SM (64 registers)
+__global__ void __launch_bounds__(kBlock, 4) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                      PairLists wl, int packed, const float4* __restrict__ pos,
                                                      const float4* __restrict__ walls, const float4* __restrict__ kw,
                                                      const float4* __restrict__ vr, float4* __restrict__ wout,
@@ -408,7 +430,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_push(Params p, const StepConsts*
     float3 xi = f3(pos[i]), wi = f3(own_w), vi = f3(own_v);
     float ki = own_w.w, rbi = own_v.w;
     float3 vacc = make_float3(0, 0, 0), xacc = make_float3(0, 0, 0);
-    walk4<Three>(fl, packed != 0, row,
+    walk4<Three, false>(fl, packed != 0, row,
                  [&](uint32_t j) { return Three{__ldg(&pos[j]), __ldg(&kw[j]), __ldg(&vr[j])}; },
                  [&](uint32_t, const Three& q) {
                      float3 r = xi - f3(q.a);

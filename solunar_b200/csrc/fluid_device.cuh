@@ -179,6 +179,13 @@ struct GridDev {
 
 #ifdef __CUDACC__
 
+// Neighbour lists (a few hundred MB at a million particles, more than the L2) are written once
+// a substep and streamed once by each later pass: their loads are evict-first, so they do not
+// push the particle arrays the passes gather from out of the L2.
+#ifndef SLF_LIST_LOAD
+#define SLF_LIST_LOAD __ldcs
+#endif
+
 // ---- reference arithmetic (mod.rs:125-165, 526-533) ------------------------------------------
 
 __device__ __forceinline__ float pow3(float x) { return x * (x * x); }

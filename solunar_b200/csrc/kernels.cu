@@ -404,10 +404,15 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
 #define SLF_LIST_UNROLL 4
 #endif
 constexpr int kListUnroll = SLF_LIST_UNROLL;
-// resident blocks per SM the list-walking kernels are compiled for (caps their registers)
+// resident blocks per SM the list-walking kernels are compiled for (caps their registers); the
+// solver check runs best at four blocks (64 registers; 76 uncapped, three blocks)
 #ifndef SLF_PAIR_MIN_BLOCKS
 #define SLF_PAIR_MIN_BLOCKS 1
 #endif
+#ifndef SLF_RATE_MIN_BLOCKS
+#define SLF_RATE_MIN_BLOCKS 4
+#endif
+
 
 // Where a walk finds its neighbours (the global arrays, read through the L1).
 struct FromGlobal {
@@ -428,7 +433,7 @@ __device__ __forceinline__ void each_listed_from(const PairLists& l, uint32_t i,
     const uint2* __restrict__ base = l.e + l.at(i, 0);
     uint2 e[kListUnroll];
 #pragma unroll
-    for (int u = 0; u < kListUnroll; ++u) e[u] = __ldg(base + size_t(u < (int)n ? u : n - 1) * 32u);
+    for (int u = 0; u < kListUnroll; ++u) e[u] = SLF_LIST_LOAD(base + size_t(u < (int)n ? u : n - 1) * 32u);
     for (uint32_t k = 0; k < n; k += kListUnroll) {
         float4 q[kListUnroll];
 #pragma unroll
@@ -437,7 +442,7 @@ __device__ __forceinline__ void each_listed_from(const PairLists& l, uint32_t i,
 #pragma unroll
         for (int u = 0; u < kListUnroll; ++u) {
             uint32_t kk = k + kListUnroll + u;
-            next[u] = __ldg(base + size_t(kk < n ? kk : n - 1) * 32u);
+            next[u] = SLF_LIST_LOAD(base + size_t(kk < n ? kk : n - 1) * 32u);
         }
 #pragma unroll
         for (int u = 0; u < kListUnroll; ++u)
@@ -461,7 +466,7 @@ __device__ __forceinline__ void each_listed2_from(const PairLists& l, uint32_t i
     const uint2* __restrict__ base = l.e + l.at(i, 0);
     uint2 e[kListUnroll];
 #pragma unroll
-    for (int u = 0; u < kListUnroll; ++u) e[u] = __ldg(base + size_t(u < (int)n ? u : n - 1) * 32u);
+    for (int u = 0; u < kListUnroll; ++u) e[u] = SLF_LIST_LOAD(base + size_t(u < (int)n ? u : n - 1) * 32u);
     for (uint32_t k = 0; k < n; k += kListUnroll) {
         float4 q[kListUnroll], w[kListUnroll];
 #pragma unroll
@@ -470,7 +475,7 @@ __device__ __forceinline__ void each_listed2_from(const PairLists& l, uint32_t i
 #pragma unroll
         for (int u = 0; u < kListUnroll; ++u) {
             uint32_t kk = k + kListUnroll + u;
-            next[u] = __ldg(base + size_t(kk < n ? kk : n - 1) * 32u);
+            next[u] = SLF_LIST_LOAD(base + size_t(kk < n ? kk : n - 1) * 32u);
         }
 #pragma unroll
         for (int u = 0; u < kListUnroll; ++u)
@@ -716,7 +721,7 @@ __device__ __forceinline__ void rate_particle(const Params& p, const StepConsts*
 // One check of the solve, a particle a thread, and the average error of the particles under
 // load (dfsph.rs:263-268) in a last-block finish.
 template <int WHICH>
-__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_rate(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+__global__ void __launch_bounds__(kBlock, SLF_RATE_MIN_BLOCKS) k_rate(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
                                                  const float4* __restrict__ vel, const float* __restrict__ rho,
                                                  const float* __restrict__ alpha, const float4* __restrict__ walls,

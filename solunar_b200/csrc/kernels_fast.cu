@@ -82,24 +82,33 @@ struct FromGlobalF {
     }
 };
 
-// f(entry, q) for each listed neighbour, q its stored position; four entries and their
-// gathers ahead
+// f(entry, q) for each listed neighbour, q its stored position: four entries' gathers issued
+// together, and the next four entries requested before these are used (past the end of the
+// list the last entry is loaded again, a valid address, and not used)
 template <class Src, class F>
 __device__ __forceinline__ void each_index_from(const IndexLists& l, uint32_t i, const Src& src, F&& f) {
     uint32_t n = l.count[i];
     if (n > l.cap) n = l.cap;
     if (n == 0) return;
     const uint32_t* __restrict__ base = l.idx + l.at(i, 0);
+    uint32_t e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) e[u] = SLF_LIST_LOAD(base + size_t(u < (int)n ? u : n - 1) * 32u);
     for (uint32_t k = 0; k < n; k += 4) {
-        uint32_t e[4];
         float4 q[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) e[u] = __ldg(base + size_t(k + u < n ? k + u : n - 1) * 32u);
-#pragma unroll
         for (int u = 0; u < 4; ++u) src.get(e[u], q[u]);
+        uint32_t next[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            uint32_t kk = k + 4 + u;
+            next[u] = SLF_LIST_LOAD(base + size_t(kk < n ? kk : n - 1) * 32u);
+        }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             if (k + u < n) f(e[u], q[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) e[u] = next[u];
     }
 }
 
@@ -114,16 +123,24 @@ __device__ __forceinline__ void each_index2_from(const IndexLists& l, uint32_t i
     if (n > l.cap) n = l.cap;
     if (n == 0) return;
     const uint32_t* __restrict__ base = l.idx + l.at(i, 0);
+    uint32_t e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) e[u] = SLF_LIST_LOAD(base + size_t(u < (int)n ? u : n - 1) * 32u);
     for (uint32_t k = 0; k < n; k += 4) {
-        uint32_t e[4];
         float4 q[4], w[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) e[u] = __ldg(base + size_t(k + u < n ? k + u : n - 1) * 32u);
-#pragma unroll
         for (int u = 0; u < 4; ++u) src.get(e[u], q[u], w[u]);
+        uint32_t next[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            uint32_t kk = k + 4 + u;
+            next[u] = SLF_LIST_LOAD(base + size_t(kk < n ? kk : n - 1) * 32u);
+        }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             if (k + u < n) f(e[u], q[u], w[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) e[u] = next[u];
     }
 }
 

@@ -409,6 +409,30 @@ struct World {
         DevBuf<uint32_t> cids;
         std::vector<std::unique_ptr<SubRecord>> subs;  // every == 0: each substep's record
     } tape;
+    // Records of finished tapes and segments, kept with their device buffers for the next ones:
+    // the rounds of an optimisation loop then record without allocating (tens of GB at a
+    // million particles, whose first allocation costs far more than the steps).
+    std::vector<std::unique_ptr<SubRecord>> spare_records;
+    // scratch of slf_step_backward
+    struct BackScratch {
+        DevBuf<float4> spos, svel, xo, vo, xp, vp, ab, xb, vb, pre, gt, kw, vr;
+        DevBuf<uint32_t> sids, dest;
+        DevBuf<float> srho, rb, abar, zeros;
+        DevBuf<double> grads;
+        void release(cudaStream_t s) {
+            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt, &kw, &vr}) b->release(s);
+            for (auto* b : {&srho, &rb, &abar, &zeros}) b->release(s);
+            sids.release(s);
+            dest.release(s);
+            grads.release(s);
+        }
+    } back;
+    std::unique_ptr<SubRecord> new_record() {
+        if (spare_records.empty()) return std::make_unique<SubRecord>();
+        auto r = std::move(spare_records.back());
+        spare_records.pop_back();
+        return r;
+    }
     std::vector<float>* tape_step = nullptr;  // the step being recorded
     Profiler prof;
     DevBuf<float> stage;  // xyz triples for host copies
@@ -448,6 +472,11 @@ struct World {
             tape.cpos.release(stream);
             tape.cvel.release(stream);
             tape.cids.release(stream);
+            for (auto& r : tape.subs) r->release(stream);
+            for (auto& r : spare_records) r->release(stream);
+            back.release(stream);
+            rec_rate.release(stream);
+            rec_vel.release(stream);
             dwalls.release(stream);
             dwkeys.release(stream);
             dregions.release(stream);
@@ -1550,10 +1579,16 @@ struct World {
     DevBuf<float> rec_rate;
     DevBuf<float4> rec_vel;
 
+    // Records are sized for a quarter more iterations than any solve has recorded yet, so the
+    // records a later tape reuses seldom grow: a new device allocation in the middle of a taped
+    // run costs far more than the substep.
+    uint32_t record_room = 0;
     int32_t keep_record(uint32_t its, DevBuf<float>& rates, DevBuf<float4>& vels) {
         size_t m = size_t(its) * n;
-        SLF_TRY(rates.ensure(std::max<size_t>(m, 1), 0, stream));
-        SLF_TRY(vels.ensure(std::max<size_t>(m, 1), 0, stream));
+        if (its > record_room) record_room = its + its / 4 + 4;
+        size_t room = std::max<size_t>(size_t(record_room) * n, 1);
+        SLF_TRY(rates.ensure(room, 0, stream));
+        SLF_TRY(vels.ensure(room, 0, stream));
         if (m) {
             SLF_CUDA(cudaMemcpyAsync(rates.p, rec_rate.p, m * 4, cudaMemcpyDeviceToDevice, stream));
             SLF_CUDA(cudaMemcpyAsync(vels.p, rec_vel.p, m * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
@@ -1658,17 +1693,17 @@ struct World {
         return every ? checkpoint() : SLF_OK;
     }
 
-    // releases the recorded substeps from the keep-th on
+    // gives the recorded substeps from the keep-th on back to the spares
     void drop_records(size_t keep) {
         while (tape.subs.size() > keep) {
-            tape.subs.back()->release(stream);
+            spare_records.push_back(std::move(tape.subs.back()));
             tape.subs.pop_back();
         }
     }
 
     // a new substep record holding the committed state, for a tape with every == 0
     int32_t record_begin(float dt) {
-        auto sub = std::make_unique<SubRecord>();
+        auto sub = new_record();
         sub->dt = dt;
         SLF_TRY(sub->pos.ensure(n, 0, stream));
         SLF_TRY(sub->vel.ensure(n, 0, stream));
@@ -1678,16 +1713,12 @@ struct World {
         return SLF_OK;
     }
 
+    // the tape's buffers (records, checkpoints, solver scratch) stay for the next tape
     int32_t tape_end() {
         tape.on = false;
         tape.steps.clear();
         tape.ckpt_step.clear();
         drop_records(0);
-        rec_rate.release(stream);
-        rec_vel.release(stream);
-        tape.cpos.release(stream);
-        tape.cvel.release(stream);
-        tape.cids.release(stream);
         return sync();
     }
 
@@ -1764,21 +1795,15 @@ struct World {
             if (out) *out = pg;
             return SLF_OK;
         }
-        // the committed state, to put back at the end
-        DevBuf<float4> spos, svel, xo, vo, xp, vp, ab, xb, vb, pre, gt, kw, vr;
-        DevBuf<uint32_t> sids, dest;
-        DevBuf<float> srho, rb, abar, zeros;
-        DevBuf<double> grads;
-        DfsphRecord rec;
+        // the committed state, to put back at the end, and the pass's scratch (kept for the next
+        // call, like the tape's records)
+        BackScratch& B = back;
+        DevBuf<float4> &spos = B.spos, &svel = B.svel, &xo = B.xo, &vo = B.vo, &xp = B.xp, &vp = B.vp,
+                       &ab = B.ab, &xb = B.xb, &vb = B.vb, &pre = B.pre, &gt = B.gt, &kw = B.kw, &vr = B.vr;
+        DevBuf<uint32_t> &sids = B.sids, &dest = B.dest;
+        DevBuf<float> &srho = B.srho, &rb = B.rb, &abar = B.abar, &zeros = B.zeros;
+        DevBuf<double>& grads = B.grads;
         int32_t st = SLF_OK;
-        auto release = [&] {
-            for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt, &kw, &vr}) b->release(stream);
-            for (auto* b : {&srho, &rb, &abar, &zeros}) b->release(stream);
-            sids.release(stream);
-            dest.release(stream);
-            grads.release(stream);
-            rec.release(stream);
-        };
         auto run = [&]() -> int32_t {
             for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt, &kw, &vr})
                 SLF_TRY(b->ensure(n, 0, stream));
@@ -1885,7 +1910,7 @@ struct World {
             // substeps (states and solver records), then backward through them
             std::vector<std::unique_ptr<SubRecord>> segsubs;
             auto rel2 = [&] {
-                for (auto& r : segsubs) r->release(stream);
+                for (auto& r : segsubs) spare_records.push_back(std::move(r));
                 segsubs.clear();
             };
             auto segs = [&]() -> int32_t {
@@ -1895,7 +1920,7 @@ struct World {
                     if (b >= e) continue;
                     std::vector<float> dts;
                     for (size_t t = b; t < e; ++t) dts.insert(dts.end(), tape.steps[t].begin(), tape.steps[t].end());
-                    while (segsubs.size() < dts.size()) segsubs.push_back(std::make_unique<SubRecord>());
+                    while (segsubs.size() < dts.size()) segsubs.push_back(new_record());
                     SLF_TRY(load_state(tape.cpos.p + c * n, tape.cvel.p + c * n, tape.cids.p + c * n));
                     for (size_t q = 0; q < dts.size(); ++q) {
                         SubRecord& sub = *segsubs[q];
@@ -1931,7 +1956,6 @@ struct World {
             return sync();
         };
         st = run();
-        release();
         sync();
         if (st == SLF_OK && out) *out = pg;
         return st;
