@@ -87,6 +87,8 @@ def workload(sc) -> dict:
         "solver": sc.settings.solver.name,
         "arithmetic": sc.settings.arithmetic.name,
         "positions": sc.settings.positions.name,
+        "solver_tolerances": {"divergence": sc.settings.divergence_tolerance, "density": sc.settings.density_tolerance},
+        "warm_start": bool(sc.settings.warm_start),
         "l2": "flushed (256 MiB write) before every timed step",
     }
 

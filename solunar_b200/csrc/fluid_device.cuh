@@ -226,6 +226,27 @@ __device__ __forceinline__ int3 cell_of(const Params& p, float x, float y, float
                      __float2int_rz(floorf(__fdiv_rn(z, p.radius))));
 }
 
+// The candidates of one cell, points [b, e), two gathers in flight at a time; f(j, q) for each
+// point within reach, in array order.
+template <class F>
+__device__ __forceinline__ void each_in_cell(const Params& p, const float4* __restrict__ pts, uint32_t b,
+                                             uint32_t e, float ax, float ay, float az, F&& f) {
+    uint32_t j = b;
+#pragma unroll 1
+    for (; j + 1 < e; j += 2) {
+        float4 q0 = __ldg(&pts[j]), q1 = __ldg(&pts[j + 1]);
+        float ox = q0.x - ax, oy = q0.y - ay, oz = q0.z - az;
+        if (dot3(ox, oy, oz, ox, oy, oz) < p.reach) f(j, q0);
+        ox = q1.x - ax, oy = q1.y - ay, oz = q1.z - az;
+        if (dot3(ox, oy, oz, ox, oy, oz) < p.reach) f(j + 1, q1);
+    }
+    if (j < e) {
+        float4 q = __ldg(&pts[j]);
+        float ox = q.x - ax, oy = q.y - ay, oz = q.z - az;
+        if (dot3(ox, oy, oz, ox, oy, oz) < p.reach) f(j, q);
+    }
+}
+
 // Visit the points of `g` within reach of `at` in the reference's list order: the 27 cells
 // dz outer, dy, dx inner (mod.rs:250-261), each cell's points in array order, kept when
 // |p - at|^2 < reach strictly (mod.rs:264-277).
@@ -234,6 +255,31 @@ __device__ __forceinline__ void each_near(const Params& p, const GridDev& g, con
                                           int3 cell, float ax, float ay, float az, F&& f) {
     // the offsets below are single subtractions and the test uses dot3: exact under any flags
     if (g.mode == 0) return;
+    if (g.mode == 1) {
+        // dense table (under 2^31 cells): the cell's place in it once, in 64 bits as cells near
+        // the i32 limits overflow, each neighbour's index in 32 bits once it is known inside
+        const long long bx = (long long)cell.x - g.lx, by = (long long)cell.y - g.ly, bz = (long long)cell.z - g.lz;
+#pragma unroll 1
+        for (int dz = -1; dz <= 1; ++dz) {
+            long long z = bz + dz;
+            if (z < 0 || z >= g.sz) continue;
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                long long y = by + dy;
+                if (y < 0 || y >= g.sy) continue;
+                uint32_t yz = uint32_t(y) * uint32_t(g.sz) + uint32_t(z);
+#pragma unroll 1
+                for (int dx = -1; dx <= 1; ++dx) {
+                    long long x = bx + dx;
+                    if (x < 0 || x >= g.sx) continue;
+                    uint32_t c = uint32_t(x) * (uint32_t(g.sy) * uint32_t(g.sz)) + yz;
+                    uint32_t b = __ldg(&g.start[c]), e = __ldg(&g.start[c + 1]);
+                    if (e > b) each_in_cell(p, pts, b, e, ax, ay, az, f);
+                }
+            }
+        }
+        return;
+    }
 #pragma unroll 1
     for (int dz = -1; dz <= 1; ++dz) {
 #pragma unroll 1

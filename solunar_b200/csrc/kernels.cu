@@ -316,6 +316,35 @@ __device__ __forceinline__ float ground_damping(const TerrainDev& T, float dista
     return d0 + (d1 - d0) * part;
 }
 
+// The second half of a list-building walk: for each of row's first m listed neighbours, in list
+// order, q = pts[index] and the entry's factor becomes f(q).  Four entries and their points are
+// read ahead of their use (the entries were written by this thread just before: plain loads).
+template <class F>
+__device__ __forceinline__ void relist(const PairLists& l, uint32_t row, uint32_t m, const float4* __restrict__ pts,
+                                       F&& f) {
+    if (m == 0) return;
+    uint2* base = l.e + l.at(row, 0);
+    uint32_t j[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) j[u] = base[size_t(u < (int)m ? u : m - 1) * 32u].x;
+    for (uint32_t k = 0; k < m; k += 4) {
+        float4 q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) q[u] = __ldg(&pts[j[u]]);
+        uint32_t next[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            uint32_t kk = k + 4 + u;
+            next[u] = base[size_t(kk < m ? kk : m - 1) * 32u].x;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u < m) base[size_t(k + u) * 32u] = make_uint2(j[u], __float_as_uint(f(q[u])));
+#pragma unroll
+        for (int u = 0; u < 4; ++u) j[u] = next[u];
+    }
+}
+
 // ---- densities (mod.rs:621-675) and the substep's neighbour lists, with WCSPH pressure
 // (step.rs:147-172) or the DFSPH factors (dfsph.rs:108-163) --------------------------------
 
@@ -332,16 +361,29 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
     if (valid) {
         float4 a = pos[i];
         int3 cell = cell_of(p, a.x, a.y, a.z);
+        // The walk first only lists the neighbours (a tight loop over the ~216 candidates of 27
+        // cells, of which ~16 % are kept), then takes the sums over the list, in list order, so
+        // the arithmetic of the kept pairs runs without the candidates' divergence.  A list over
+        // its room is incomplete and the host runs the pass again with more room.
+        uint32_t nf = 0, nw = 0;
+        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4) {
+            if (nf < fl.cap) fl.e[fl.at(row, nf)].x = j;
+            ++nf;
+        });
+        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t j, float4) {
+            if (nw < wl.cap) wl.e[wl.at(row, nw)].x = j;
+            ++nw;
+        });
+        fl.count[row] = nf;
+        wl.count[row] = nw;
+        longest = nf > nw ? nf : nw;
         float sum = 0.0f, wsum = 0.0f;
         float sx = 0.0f, sy = 0.0f, sz = 0.0f, squares = 0.0f;
-        uint32_t nf = 0, nw = 0;
-        each_near(p, fg, pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+        relist(fl, row, nf < fl.cap ? nf : fl.cap, pos, [&](float4 q) {
             float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             sum += kernel_value(p, d);
             float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
-            if (nf < fl.cap) fl.e[fl.at(row, nf)] = make_uint2(j, __float_as_uint(g));
-            ++nf;
             if (SOLVER == 1) {
                 // gradient(at - other) (dfsph.rs:118), then factors (dfsph.rs:149-153)
                 float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
@@ -351,24 +393,21 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
                 sz = sz + pz;
                 squares += dot3(px, py, pz, px, py, pz);
             }
+            return g;
         });
-        each_near(p, wg, walls, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+        relist(wl, row, nw < wl.cap ? nw : wl.cap, walls, [&](float4 q) {
             float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             wsum += kernel_value(p, d);
             float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
-            if (nw < wl.cap) wl.e[wl.at(row, nw)] = make_uint2(j, __float_as_uint(g));
-            ++nw;
             if (SOLVER == 1) {
                 float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
                 sx = sx + (rx * g) * p.mass;
                 sy = sy + (ry * g) * p.mass;
                 sz = sz + (rz * g) * p.mass;
             }
+            return g;
         });
-        fl.count[row] = nf;
-        wl.count[row] = nw;
-        longest = nf > nw ? nf : nw;
         // mass (fluid + walls + movers, none here) + ground (mod.rs:657-663)
         float3 gslope;
         float ground = T.regions ? ground_near(T, a.x, a.y, a.z, gslope) : 0.0f;

@@ -157,6 +157,44 @@ template <class F>
 __device__ __forceinline__ void each_near_rel(const Params& p, const GridDev& g, const float4* __restrict__ pts,
                                               int3 cell, float4 a, F&& f) {
     if (g.mode == 0) return;
+    if (g.mode == 1) {
+        // dense table: as each_near's walk, the cell's place once, neighbours' indices in 32 bits
+        const long long bx = (long long)cell.x - g.lx, by = (long long)cell.y - g.ly, bz = (long long)cell.z - g.lz;
+#pragma unroll 1
+        for (int dz = -1; dz <= 1; ++dz) {
+            long long z = bz + dz;
+            if (z < 0 || z >= g.sz) continue;
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                long long y = by + dy;
+                if (y < 0 || y >= g.sy) continue;
+                uint32_t yz = uint32_t(y) * uint32_t(g.sz) + uint32_t(z);
+#pragma unroll 1
+                for (int dx = -1; dx <= 1; ++dx) {
+                    long long x = bx + dx;
+                    if (x < 0 || x >= g.sx) continue;
+                    uint32_t c = uint32_t(x) * (uint32_t(g.sy) * uint32_t(g.sz)) + yz;
+                    uint32_t b = __ldg(&g.start[c]), e = __ldg(&g.start[c + 1]);
+                    float sx = float(dx) * p.radius, sy = float(dy) * p.radius, sz = float(dz) * p.radius;
+                    uint32_t j = b;
+#pragma unroll 1
+                    for (; j + 1 < e; j += 2) {
+                        float4 q0 = __ldg(&pts[j]), q1 = __ldg(&pts[j + 1]);
+                        float rx = (a.x - q0.x) - sx, ry = (a.y - q0.y) - sy, rz = (a.z - q0.z) - sz;
+                        if (dot3(rx, ry, rz, rx, ry, rz) < p.reach) f(j, q0, dx, dy, dz, rx, ry, rz);
+                        rx = (a.x - q1.x) - sx, ry = (a.y - q1.y) - sy, rz = (a.z - q1.z) - sz;
+                        if (dot3(rx, ry, rz, rx, ry, rz) < p.reach) f(j + 1, q1, dx, dy, dz, rx, ry, rz);
+                    }
+                    if (j < e) {
+                        float4 q = __ldg(&pts[j]);
+                        float rx = (a.x - q.x) - sx, ry = (a.y - q.y) - sy, rz = (a.z - q.z) - sz;
+                        if (dot3(rx, ry, rz, rx, ry, rz) < p.reach) f(j, q, dx, dy, dz, rx, ry, rz);
+                    }
+                }
+            }
+        }
+        return;
+    }
 #pragma unroll 1
     for (int dz = -1; dz <= 1; ++dz) {
 #pragma unroll 1
