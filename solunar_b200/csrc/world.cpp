@@ -1586,9 +1586,10 @@ struct World {
     int32_t keep_record(uint32_t its, DevBuf<float>& rates, DevBuf<float4>& vels) {
         size_t m = size_t(its) * n;
         if (its > record_room) record_room = its + its / 4 + 4;
+        // a record that holds this solve keeps its buffers; one that does not grows to the room
         size_t room = std::max<size_t>(size_t(record_room) * n, 1);
-        SLF_TRY(rates.ensure(room, 0, stream));
-        SLF_TRY(vels.ensure(room, 0, stream));
+        if (rates.cap < std::max<size_t>(m, 1)) SLF_TRY(rates.ensure(room, 0, stream));
+        if (vels.cap < std::max<size_t>(m, 1)) SLF_TRY(vels.ensure(room, 0, stream));
         if (m) {
             SLF_CUDA(cudaMemcpyAsync(rates.p, rec_rate.p, m * 4, cudaMemcpyDeviceToDevice, stream));
             SLF_CUDA(cudaMemcpyAsync(vels.p, rec_vel.p, m * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
