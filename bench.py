@@ -443,6 +443,24 @@ def main():
         _, fwd_ms = reduce_timing(adj_substeps, fwd_ms, world_size, dev)
         bwd_ms = both_ms - fwd_ms
         finite = bool(np.isfinite(dv0).all() and np.isfinite(dp0).all())
+
+        # the backward's kernels: another round of up to 8 steps, its reverse pass profiled
+        # launch by launch (CUDA events)
+        pk_steps = min(k, 8)
+        world.tape_begin(every)
+        p_sub = 0
+        for _ in range(pk_steps):
+            p_sub += world.step(sc.dt).substeps
+        dv = loss_grad()
+        world.profile(True)
+        world.profile_reset()
+        world.step_backward(np.zeros_like(dv), dv)
+        bprof = world.profile_read()
+        world.profile(False)
+        world.tape_end()
+        backward_kernels = {name: {"launches": c, "us_per_launch": 1e3 * ms / max(c, 1),
+                                   "ms_per_substep": ms / max(p_sub, 1)}
+                            for name, (c, ms, _) in sorted(bprof.items(), key=lambda kv: -kv[1][1])}
         adjoint = {"value": adj_all / (both_ms / 1e3), "unit": UNIT,
                    "gradients_finite": finite,
                    "steps": k, "substeps": adj_substeps, "checkpoint_every": every,
@@ -450,6 +468,7 @@ def main():
                    "ratio_to_forward": (fwd_ms + bwd_ms) / fwd_ms,
                    "ratio_to_plain_substeps": value / (adj_all / (both_ms / 1e3)),
                    "loss": "kinetic energy of the water beyond x = 1 m after the steps",
+                   "backward_kernels": {"steps": pk_steps, "substeps": p_sub, "kernels": backward_kernels},
                    "grad_viscosity": grads["viscosity"], "grad_gravity": list(grads["gravity"]),
                    "grad_uniform_inflow": [float(x) for x in dv0.astype(np.float64).sum(axis=0)]}
 

@@ -30,6 +30,11 @@ __device__ __forceinline__ uint32_t listed_count(const PairLists& l, uint32_t i)
     return n < l.cap ? n : l.cap;
 }
 
+// 1/|r| from d2 = r.r through the reciprocal square root (a few ulp, as FAST arithmetic allows);
+// 0 below the smallest normal float, where the pair counts as coincident and adds nothing (the
+// hardware flushes such inputs, and 1/0 would turn the pair's zero terms into NaN)
+__device__ __forceinline__ float inv_length(float d2) { return d2 >= 1.17549435e-38f ? rsqrtf(d2) : 0.0f; }
+
 // gradient factor g(d) = slope(d) / d = grad_scale (1 - d/r)^3 and its derivative in d
 __device__ __forceinline__ void grad_factor(const Params& p, float d, float& g, float& gp) {
     float om = 1.0f - d * p.inv_radius;
@@ -377,20 +382,20 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
     walk4<Two>(fl, packed != 0, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&w[j])}; },
                [&](uint32_t, const Two& q) {
                    float3 r = xi - f3(q.a);
-                   float d = sqrtf(dotf(r, r));
-                   if (d <= 0.0f) return;
+                   float d2 = dotf(r, r), inv = inv_length(d2);
+                   if (inv == 0.0f) return;
                    float g, gp;
-                   grad_factor(p, d, g, gp);
+                   grad_factor(p, d2 * inv, g, gp);
                    acc += dotf(wi - f3(q.b), r) * g;
                });
     uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
         uint32_t j = listed(wl, packed != 0, row, k);
         float3 r = xi - f3(__ldg(&walls[j]));
-        float d = sqrtf(dotf(r, r));
-        if (d <= 0.0f) continue;
+        float d2 = dotf(r, r), inv = inv_length(d2);
+        if (inv == 0.0f) continue;
         float g, gp;
-        grad_factor(p, d, g, gp);
+        grad_factor(p, d2 * inv, g, gp);
         acc += dotf(wi, r) * g;
     }
     float kbar = -dt * m * acc;
@@ -434,27 +439,27 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_push(Params p, const StepCons
                  [&](uint32_t j) { return Three{__ldg(&pos[j]), __ldg(&kw[j]), __ldg(&vr[j])}; },
                  [&](uint32_t, const Three& q) {
                      float3 r = xi - f3(q.a);
-                     float d = sqrtf(dotf(r, r));
-                     if (d <= 0.0f) return;
+                     float d2 = dotf(r, r), inv = inv_length(d2);
+                     if (inv == 0.0f) return;
                      float g, gp;
-                     grad_factor(p, d, g, gp);
+                     grad_factor(p, d2 * inv, g, gp);
                      float rbj = q.c.w;
                      vacc = vacc + r * (g * m * (rbi + rbj));
                      // c . grad W(r) with c = -dt m (k_i + k_j)(w_i - w_j) + m (rb_i + rb_j)(v_i - v_j)
                      float3 c = (wi - f3(q.b)) * (-dt * m * (ki + q.b.w)) + (vi - f3(q.c)) * (m * (rbi + rbj));
-                     xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
+                     xacc = xacc + c * g + r * (dotf(c, r) * gp * inv);
                  });
     uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
         uint32_t j = listed(wl, packed != 0, row, k);
         float3 r = xi - f3(__ldg(&walls[j]));
-        float d = sqrtf(dotf(r, r));
-        if (d <= 0.0f) continue;
+        float d2 = dotf(r, r), inv = inv_length(d2);
+        if (inv == 0.0f) continue;
         float g, gp;
-        grad_factor(p, d, g, gp);
+        grad_factor(p, d2 * inv, g, gp);
         vacc = vacc + r * (g * m * rbi);
         float3 c = wi * (-dt * m * ki) + vi * (m * rbi);
-        xacc = xacc + c * g + r * (dotf(c, r) * gp / d);
+        xacc = xacc + c * g + r * (dotf(c, r) * gp * inv);
     }
     wout[i] = make_float4(wi.x + vacc.x, wi.y + vacc.y, wi.z + vacc.z, 0.0f);
     float4 x0 = xb[i];
@@ -580,15 +585,17 @@ void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float
 void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                           bool packed, const float4* pos, const float4* walls, const float4* w, const float* rate,
                           const float* alpha, const float* rho, const float4* vel, float4* kw, float4* vr,
-                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s) {
+                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s, int parts) {
     if (!p.n) return;
-    if (which == 1)
+    // parts: 1 the kappa pass, 2 the push, 3 both
+    if ((parts & 1) && which == 1)
         k_adj_kappa<1><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
                                                           rho, vel, kw, vr, abar, rb);
-    else
+    else if (parts & 1)
         k_adj_kappa<0><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
                                                           rho, vel, kw, vr, abar, rb);
-    k_adj_push<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, kw, vr, wout, xb);
+    if (parts & 2)
+        k_adj_push<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, kw, vr, wout, xb);
 }
 
 void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,

@@ -152,7 +152,7 @@ void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float
 void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                           bool packed, const float4* pos, const float4* walls, const float4* w, const float* rate,
                           const float* alpha, const float* rho, const float4* vel, float4* kw, float4* vr,
-                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s);
+                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s, int parts = 3);
 void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,
                           const float4* pos, const float4* vel, const float* rho, const float* zeros,
                           const float4* walls, float4* w, float4* ab, float4* xb, float* rb, double* grads,

@@ -1831,28 +1831,40 @@ struct World {
                 } else {
                     // advance, density solve, viscosity, divergence solve, factors, densities,
                     // sort: the substep's steps backwards
-                    launch_adj_advance_dfsph(p, d_consts, rec.pre.p, xo.p, vo.p, xb.p, vb.p, stream);
+                    timed("adj_advance", 0.0, [&] {
+                        launch_adj_advance_dfsph(p, d_consts, rec.pre.p, xo.p, vo.p, xb.p, vb.p, stream);
+                    });
                     SLF_CUDA(cudaMemsetAsync(rb.p, 0, n * 4, stream));
                     SLF_CUDA(cudaMemsetAsync(abar.p, 0, n * 4, stream));
                     for (uint32_t it = rec.den_n; it-- > 0;) {
-                        launch_adj_iteration(1, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
-                                             rec.den_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
-                                             rec.den_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p, vp.p, xb.p,
-                                             stream);
+                        for (int part = 1; part <= 2; ++part)
+                            timed(part == 1 ? "adj_kappa_density" : "adj_push_density", 0.0, [&] {
+                                launch_adj_iteration(1, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
+                                                     rec.den_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
+                                                     rec.den_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p,
+                                                     vp.p, xb.p, stream, part);
+                            });
                         std::swap(vb, vp);
                     }
-                    launch_adj_viscosity(p, d_consts, fl, wl, packed, pos[a].p, rec.va.p, rho[nid].p, zeros.p,
-                                         dwalls.p, vb.p, ab.p, xb.p, rb.p, grads.p, stream);
+                    timed("adj_viscosity", 0.0, [&] {
+                        launch_adj_viscosity(p, d_consts, fl, wl, packed, pos[a].p, rec.va.p, rho[nid].p, zeros.p,
+                                             dwalls.p, vb.p, ab.p, xb.p, rb.p, grads.p, stream);
+                    });
                     for (uint32_t it = rec.div_n; it-- > 0;) {
-                        launch_adj_iteration(0, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
-                                             rec.div_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
-                                             rec.div_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p, vp.p, xb.p,
-                                             stream);
+                        for (int part = 1; part <= 2; ++part)
+                            timed(part == 1 ? "adj_kappa_divergence" : "adj_push_divergence", 0.0, [&] {
+                                launch_adj_iteration(0, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
+                                                     rec.div_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
+                                                     rec.div_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p,
+                                                     vp.p, xb.p, stream, part);
+                            });
                         std::swap(vb, vp);
                     }
-                    launch_adj_factors_density(p, fl, wl, packed, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p, rb.p,
-                                               xb.p, stream);
-                    launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream);
+                    timed("adj_factors_density", 0.0, [&] {
+                        launch_adj_factors_density(p, fl, wl, packed, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p,
+                                                   rb.p, xb.p, stream);
+                    });
+                    timed("adj_unsort", 0.0, [&] { launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream); });
                 }
                 double g[kGradSlots];
                 SLF_CUDA(cudaMemcpyAsync(g, grads.p, sizeof(g), cudaMemcpyDeviceToHost, stream));
