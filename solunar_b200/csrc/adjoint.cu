@@ -147,6 +147,9 @@ __global__ void k_adj_advance(Params p, const StepConsts* __restrict__ sc, const
 }
 
 // ---- forces (step.rs:173-211), wall viscosity (step.rs:262-301), Tait pressure (step.rs:147-172)
+// PRESSURE = false: the DFSPH viscosity pass (dfsph.rs:90-99), the same pairs without pressure,
+// so the pressure records are neither gathered nor differentiated
+template <bool PRESSURE>
 __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                       PairLists wl, int packed, const float4* __restrict__ pos,
                                                       const float4* __restrict__ vel, const float* __restrict__ rho,
@@ -162,26 +165,26 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
     if (i < p.n) {
         const float nu = sc->viscosity, nuw = sc->wall_viscosity, m = p.mass;
         float3 xi = f3(pos[i]), vi = f3(vel[i]), ai = f3(ab[i]);
-        float rho_i = rho[i], p_i = press[i], s_i = scaled[i];
+        float rho_i = rho[i], p_i = PRESSURE ? press[i] : 0.0f, s_i = PRESSURE ? scaled[i] : 0.0f;
         float3 xbar = make_float3(0, 0, 0), vbar = make_float3(0, 0, 0);
         float sbar = 0.0f, pbar = 0.0f, rbar = 0.0f;
 
         // fluid pairs: L = (a_i-bar - a_j-bar) . T(r, u, S, R)
         walk4<FiveF>(fl, packed != 0, row,
                      [&](uint32_t j) {
-                         return FiveF{__ldg(&pos[j]), __ldg(&vel[j]), __ldg(&ab[j]), __ldg(&rho[j]), __ldg(&scaled[j])};
+                         return FiveF{__ldg(&pos[j]), __ldg(&vel[j]), __ldg(&ab[j]), __ldg(&rho[j]),
+                                      PRESSURE ? __ldg(&scaled[j]) : 0.0f};
                      },
                      [&](uint32_t, const FiveF& q) {
             float3 r = xi - f3(q.a);
-            float d2 = dotf(r, r);
-            if (d2 <= 0.0f) return;
-            float d = sqrtf(d2);
+            float d2 = dotf(r, r), inv = inv_length(d2);
+            if (inv == 0.0f) return;
             float g, gp;
-            grad_factor(p, d, g, gp);
+            grad_factor(p, d2 * inv, g, gp);
             float3 u = vi - f3(q.b);
             float3 w = ai - f3(q.c);
             float R = rho_i + q.d;
-            float S = s_i + q.e;
+            float S = PRESSURE ? s_i + q.e : 0.0f;
             float ur = dotf(u, r);
             bool act = ur < 0.0f;
             float t = act ? ur : 0.0f;
@@ -192,12 +195,12 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
             float dPi_dt = -2.0f * nu / den;
             float dPi_dd2 = -Pi / (d2 + p.soften);
             float c1 = -m * (S + Pi);
-            float3 dr = w * (c1 * g) + r * (c1 * G * gp / d + P * dPi_dd2 * 2.0f);
+            float3 dr = w * (c1 * g) + r * (c1 * G * gp * inv + P * dPi_dd2 * 2.0f);
             if (act) dr = dr + u * (P * dPi_dt);
             xbar = xbar + dr;
             if (act) vbar = vbar + r * (P * dPi_dt);
             rbar += P * (-Pi / R);
-            sbar += P;
+            if (PRESSURE) sbar += P;
             // viscosity enters a_i's own term: a_i-bar . dT/dnu
             nu_bar += (double)(2.0f * m * g * t * dotf(ai, r) / den);
         });
@@ -209,15 +212,17 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         for (uint32_t k = 0; k < nw; ++k) {
             uint32_t j = listed(wl, packed != 0, row, k);
             float3 r = xi - f3(__ldg(&walls[j]));
-            float d = sqrtf(dotf(r, r));
-            if (d <= 0.0f) continue;
+            float d2 = dotf(r, r), inv = inv_length(d2);
+            if (inv == 0.0f) continue;
             float g, gp;
-            grad_factor(p, d, g, gp);
-            float ar = dotf(ai, r);
-            float mb = -m * g * ar;
-            sbar += mb;
-            pbar += mb * p.inv_rest_sq;
-            xbar = xbar + (ai * g + r * (ar * gp / d)) * (-m * M);
+            grad_factor(p, d2 * inv, g, gp);
+            if (PRESSURE) {
+                float ar = dotf(ai, r);
+                float mb = -m * g * ar;
+                sbar += mb;
+                pbar += mb * p.inv_rest_sq;
+                xbar = xbar + (ai * g + r * (ar * gp * inv)) * (-m * M);
+            }
             A = A - r * g;
         }
 
@@ -273,14 +278,16 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         }
 
         // s = p / rho^2 and the Tait equation of state
-        float ptot = pbar + sbar / (rho_i * rho_i);
-        rbar += sbar * (-2.0f * p_i / (rho_i * rho_i * rho_i));
-        float raw = rho_i * p.inv_rest;
-        float ratio = fminf(raw, 1.1f);
-        float r2 = ratio * ratio, r3 = r2 * ratio, r6 = r3 * r3;
-        if (p_i > 0.0f) {
-            b_bar = (double)(ptot * (r6 * ratio - 1.0f));
-            if (raw < 1.1f) rbar += ptot * p.stiffness * 7.0f * r6 * p.inv_rest;
+        if (PRESSURE) {
+            float ptot = pbar + sbar / (rho_i * rho_i);
+            rbar += sbar * (-2.0f * p_i / (rho_i * rho_i * rho_i));
+            float raw = rho_i * p.inv_rest;
+            float ratio = fminf(raw, 1.1f);
+            float r2 = ratio * ratio, r3 = r2 * ratio, r6 = r3 * r3;
+            if (p_i > 0.0f) {
+                b_bar = (double)(ptot * (r6 * ratio - 1.0f));
+                if (raw < 1.1f) rbar += ptot * p.stiffness * 7.0f * r6 * p.inv_rest;
+            }
         }
         float4 x0 = xb[i], v0 = vb[i];
         xb[i] = make_float4(x0.x + xbar.x, x0.y + xbar.y, x0.z + xbar.z, 0.0f);
@@ -569,8 +576,8 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
     if (!p.n) return;
     uint32_t nb = adj_blocks(p.n);
     k_adj_advance<<<nb, kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, ab, xb, vb, grads);
-    k_adj_force<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, press, scaled, walls,
-                                                   ab, xb, vb, rb, grads, 0);
+    k_adj_force<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, press, scaled,
+                                                         walls, ab, xb, vb, rb, grads, 0);
     k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, rb, xb);
     k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp);
 }
@@ -604,8 +611,8 @@ void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists
                           cudaStream_t s) {
     if (!p.n) return;
     k_adj_scale<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, w, ab, grads);
-    k_adj_force<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, zeros, zeros, walls,
-                                                   ab, xb, w, rb, grads, 1);
+    k_adj_force<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, zeros, zeros,
+                                                          walls, ab, xb, w, rb, grads, 1);
 }
 
 void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, bool packed,
