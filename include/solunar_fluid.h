@@ -40,7 +40,8 @@ enum {
     SLF_ERR_CUDA = 7,                /* a CUDA call failed; see slf_last_error() */
     SLF_ERR_TIMEOUT = 8,             /* a bounded device loop gave up */
     SLF_ERR_INVALID_ARGUMENT = 9,    /* null pointer or wrong buffer size */
-    SLF_ERR_SNAPSHOT = 10            /* SnapshotError (src/snapshot/mod.rs:56-63); see slf_last_error() */
+    SLF_ERR_SNAPSHOT = 10,           /* SnapshotError (src/snapshot/mod.rs:56-63); see slf_last_error() */
+    SLF_ERR_INVALID_SHAPE = 11       /* PhysicsError::InvalidShape (src/error.rs:10) */
 };
 
 /* FluidSolver (src/fluid/mod.rs:43-53). */
@@ -160,9 +161,57 @@ int32_t slf_save_snapshot(slf_world* world, uint8_t* out, uint64_t capacity, uin
 /* FluidWorld::load_snapshot (save.rs:79-181): a new world from untrusted snapshot bytes
  * (versions 1-3).  The library's own settings fields (positions, arithmetic, solver limits,
  * device) come from `library`, or the defaults when it is NULL.  Bad bytes return
- * SLF_ERR_SNAPSHOT with the reference's message in slf_last_error(); coupled bodies in the
- * snapshot return SLF_ERR_UNSUPPORTED. */
+ * SLF_ERR_SNAPSHOT with the reference's message in slf_last_error().  Coupled bodies come back
+ * with their points and probes (couple.rs:58-75). */
 int32_t slf_load_snapshot(const uint8_t* data, uint64_t size, const slf_settings* library, slf_world** out);
+
+/* ---- coupled bodies (src/fluid/couple.rs, lift.rs) ---------------------------------------
+ * The caller owns the rigid bodies.  A body is named by the reference's BodyHandle::to_raw()
+ * pair (index, generation) as index << 32 | generation, which orders bodies as the reference
+ * does.  Each step the caller gives every coupled body's pose and gets back what the water did to
+ * it, to apply to its body as force and torque (impulse / dt) over the rigid step that follows. */
+enum { SLF_SHAPE_CUBOID = 0, SLF_SHAPE_SPHERE = 1, SLF_SHAPE_CAPSULE = 2 };
+
+/* SubstepPose (src/substep.rs) as FluidWorld::step_with_bodies reads it (couple.rs:418-426). */
+typedef struct slf_body_pose {
+    uint64_t body;
+    double position[3];          /* the rigid world's f64 position; the water uses it as f32 */
+    float rotation[4];           /* unit quaternion x, y, z, w */
+    float linear_velocity[3];
+    float angular_velocity[3];
+    int32_t dynamic;             /* 1: the body takes pushes (apply_force succeeds in the reference) */
+} slf_body_pose;
+
+/* What the water did to one coupled body over a step. */
+typedef struct slf_body_push {
+    uint64_t body;
+    float lift[3];               /* lift.rs: buoyancy, drag and wave damping, impulse over the step */
+    float lift_angular[3];       /* its angular impulse about the body's centre */
+    float damping[3];            /* couple.rs:375-416: the body points' damping, impulse */
+    float damping_angular[3];
+    int32_t lifted;              /* 1: the body is dynamic and the water lost the lift's momentum */
+} slf_body_push;
+
+/* FluidWorld::couple (couple.rs:165-200): shape SLF_SHAPE_CUBOID with dims = half extents,
+ * SPHERE with dims[0] = radius, CAPSULE with dims[0] = radius and dims[1] = half height.  A
+ * body coupled again takes the new shape.  SLF_ERR_INVALID_SHAPE for a bad shape or one too
+ * small to hold a point, SLF_ERR_FLUID_FULL past max_particles points. */
+int32_t slf_couple(slf_world* world, uint64_t body, int32_t shape, const float dims[3]);
+/* FluidWorld::uncouple (couple.rs:203-207): *removed = 0 for a body that was not coupled. */
+int32_t slf_uncouple(slf_world* world, uint64_t body, int32_t* removed);
+/* The coupled bodies in body order with their point and probe counts; *count receives how many
+ * there are, arrays (any may be NULL) hold at most `capacity`. */
+int32_t slf_coupled(const slf_world* world, uint64_t* bodies, uint32_t* points, uint32_t* probes,
+                    uint64_t capacity, uint64_t* count);
+/* FluidWorld::step_with_bodies (couple.rs:219-248) with the rigid world left to the caller: the
+ * coupled bodies stand where `poses` puts them (a coupled body without a pose is uncoupled, as
+ * the reference drops bodies gone from the world) and sweep on at their velocities through the
+ * substeps; `pushes` (room for `capacity`) receives one entry per coupled body, in body order,
+ * and *count how many.  A dynamic body's lift is taken out of the water it was read from.  WCSPH
+ * only (SLF_ERR_INVALID_SETTINGS for DFSPH with coupled bodies) and EXACT arithmetic only
+ * (SLF_ERR_UNSUPPORTED for FAST). */
+int32_t slf_step_with_bodies(slf_world* world, float dt, const slf_body_pose* poses, uint64_t npose,
+                             slf_report* out, slf_body_push* pushes, uint64_t capacity, uint64_t* count);
 
 /* The node lattice of a terrain region over [low, high] (terrain.rs:275-283): nodes[a] nodes along
  * axis a, spacing / 2 apart from `low`.  SLF_ERR_FLUID_FULL above 2^24 nodes. */

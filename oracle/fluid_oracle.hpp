@@ -42,6 +42,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -69,6 +70,7 @@ enum Status : int32_t {
     UNSUPPORTED = 6,
     INVALID_ARGUMENT = 9,
     SNAPSHOT = 10,  // SnapshotError (src/snapshot/mod.rs:56-63)
+    INVALID_SHAPE = 11,  // PhysicsError::InvalidShape (src/error.rs:10)
 };
 
 // ---- scalar helpers ---------------------------------------------------------------------
@@ -83,6 +85,25 @@ template <class R> inline R rmax(R a, R b) {
     if (std::isnan(a)) return b;
     if (std::isnan(b)) return a;
     return b > a ? b : a;
+}
+// Rust's `f as i32`: saturating, NaN to 0
+template <class R> inline int32_t as_i32(R v) {
+    if (std::isnan(v)) return 0;
+    if (v >= R(2147483647.0)) return INT32_MAX;
+    if (v <= R(-2147483648.0)) return INT32_MIN;
+    return int32_t(v);
+}
+// f32::total_cmp's order: -NaN < -inf < ... < -0 < +0 < ... < +inf < +NaN
+template <class R> inline bool total_less(R a, R b) {
+    using U = typename std::conditional<sizeof(R) == 4, int32_t, int64_t>::type;
+    using UU = typename std::make_unsigned<U>::type;
+    U x, y;
+    std::memcpy(&x, &a, sizeof(R));
+    std::memcpy(&y, &b, sizeof(R));
+    const int shift = int(8 * sizeof(R) - 1);
+    x ^= U(UU(x >> shift) >> 1);
+    y ^= U(UU(y >> shift) >> 1);
+    return x < y;
 }
 // `powi` lowered to binary exponentiation (mod.rs:136,145,154; step.rs:149,156).
 template <class R> inline R pow2(R x) { return x * x; }
@@ -134,6 +155,16 @@ template <class R> inline bool is_finite(V3<R> a) {
 template <class R> inline V3<R> vmin(V3<R> a, V3<R> b) { return {rmin(a.x, b.x), rmin(a.y, b.y), rmin(a.z, b.z)}; }
 template <class R> inline V3<R> vmax(V3<R> a, V3<R> b) { return {rmax(a.x, b.x), rmax(a.y, b.y), rmax(a.z, b.z)}; }
 template <class R> inline V3<R> clamp(V3<R> v, V3<R> lo, V3<R> hi) { return vmin(vmax(v, lo), hi); }
+template <class R> inline V3<R> cross(V3<R> a, V3<R> b) {
+    return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+// q * v for the unit quaternion (x, y, z, w): v (w^2 - |b|^2) + b 2 (v.b) + (b x v) 2 w, b = (x, y, z)
+template <class R> inline V3<R> rotate(const R q[4], V3<R> v) {
+    V3<R> b(q[0], q[1], q[2]);
+    R w = q[3];
+    R b2 = dot(b, b);
+    return v * (w * w - b2) + b * (dot(v, b) * R(2)) + cross(b, v) * (w * R(2));
+}
 template <class R> inline V3<R> normalize_or(V3<R> v, V3<R> fallback) {
     R len = length(v);
     if (std::isfinite(len) && len > R(0)) return v / len;
@@ -375,7 +406,7 @@ template <class R> class World {
     std::vector<R> impulse[2];
     uint32_t next_id = 0;
     Grid grid;
-    Lists neighbors, wall_neighbors;
+    Lists neighbors, wall_neighbors, mover_neighbors;
     Walls<R> walls;
     bool has_domain = false;
     Vec domain_low, domain_high;
@@ -403,6 +434,21 @@ template <class R> class World {
         std::vector<R> weights, fars, damping;
     } sites;
     std::vector<Vec> ground_slopes;  // mod.rs:320-322: empty without terrains
+    // coupled bodies (couple.rs:15-33), in body order, and their points for the running step
+    // (couple.rs:35-47)
+    struct Coupled {
+        uint64_t body;  // BodyHandle (index, generation) as index << 32 | generation
+        std::vector<Vec> points, probes;
+        R probe_spacing{0};
+        Vec center, velocity, moved;
+        Vec impulse, angular;  // what the water's damping did to the body this step
+    };
+    std::vector<Coupled> coupled;
+    struct Movers {
+        std::vector<Vec> start, positions, velocities;
+        std::vector<uint32_t> owners;
+        Grid grid;
+    } movers;
     // per-pair gradient caches of the last DFSPH substep (dfsph.rs:24-41)
     std::vector<Vec> grad_fluid, grad_walls;
     // solver iteration counts of the last DFSPH substep: divergence, density
@@ -681,6 +727,422 @@ template <class R> class World {
         return add_flow(low, high, true, velocity, id_out);
     }
     Status add_drain(Vec low, Vec high, uint32_t* id_out) { return add_flow(low, high, false, Vec(), id_out); }
+
+    // ---- coupled bodies (src/fluid/couple.rs, lift.rs) -------------------------------------
+
+    // A body's place and motion for a step (substep.rs SubstepPose, as couple.rs:418-426 reads
+    // it): position in f64 as the rigid world keeps it, rotation (x, y, z, w), velocities;
+    // `dynamic` when the body takes pushes (a fixed or kinematic one refuses them).
+    struct Pose {
+        uint64_t body;
+        double position[3];
+        float rotation[4];
+        float linear[3], angular[3];
+        int32_t dynamic;
+    };
+    // What the water did to a body over a step: lift.rs's lift (given back to the water when the
+    // body is dynamic) and the damping impulse of couple.rs:375-416.
+    struct Push {
+        uint64_t body;
+        Vec lift, lift_angular, damping, damping_angular;
+        int32_t lifted;
+    };
+    static constexpr size_t kMaxProbes = 4096;  // lift.rs:8
+
+    // couple.rs:453-511: lattice points `spacing` apart inside the shape (0 cuboid with half
+    // extents, 1 sphere with radius, 2 capsule with radius and half height), no deeper than
+    // `reach`, centred on it; FLUID_FULL past `limit` points
+    static Status shape_points(int kind, const float dims[3], R spacing, R reach, size_t limit, std::vector<Vec>& out) {
+        out.clear();
+        Vec half;
+        R a = R(dims[0]), b = R(dims[1]), c = R(dims[2]);
+        if (kind == 0) {
+            half = Vec(a, b, c);
+        } else if (kind == 1) {
+            half = Vec::splat(a);
+        } else if (kind == 2) {
+            if (!(b >= R(0))) return INVALID_SHAPE;  // a capsule's half height is not negative
+            half = Vec(a, b + a, a);
+        } else {
+            return INVALID_SHAPE;
+        }
+        if (!is_finite(half) || rmin(rmin(half.x, half.y), half.z) <= R(0)) return INVALID_SHAPE;
+        auto depth = [&](Vec at) -> R {
+            if (kind == 0) {
+                Vec room = half - Vec(std::fabs(at.x), std::fabs(at.y), std::fabs(at.z));
+                return rmin(rmin(room.x, room.y), room.z);
+            }
+            if (kind == 1) return a - length(at);
+            R y = rmin(rmax(at.y, -b), b);
+            return a - length(at - Vec(R(0), y, R(0)));
+        };
+        auto count = [&](R extent) -> int64_t {
+            R v = std::floor(R(2) * extent / spacing);
+            int64_t k = std::isnan(v) ? 0 : (v >= R(4096) ? 4096 : (v <= R(0) ? 0 : int64_t(v)));
+            return k;
+        };
+        int64_t cx = count(half.x), cy = count(half.y), cz = count(half.z);
+        if (cx * cy * cz > int64_t(std::min<size_t>(limit, size_t(INT64_MAX)))) return FLUID_FULL;
+        auto start = [&](int64_t cells) { return -(R(float(cells)) - R(1)) * spacing / R(2); };
+        Vec origin(start(cx), start(cy), start(cz));
+        for (int64_t y = 0; y < cy; ++y)
+            for (int64_t z = 0; z < cz; ++z)
+                for (int64_t x = 0; x < cx; ++x) {
+                    Vec at = origin + Vec(R(float(x)), R(float(y)), R(float(z))) * spacing;
+                    R inside = depth(at);
+                    if (inside >= R(0) && inside <= reach) out.push_back(at);
+                }
+        return OK;
+    }
+
+    size_t coupled_points() const {
+        size_t k = 0;
+        for (auto& c : coupled) k += c.points.size();
+        return k;
+    }
+
+    // couple.rs:165-200
+    Status couple(uint64_t body, int kind, const float dims[3]) {
+        std::vector<Vec> points, probes;
+        Status st = shape_points(kind, dims, R(settings.spacing), radius(), size_t(settings.max_particles), points);
+        if (st != OK) return st;
+        if (points.empty()) return INVALID_SHAPE;
+        uint64_t used = coupled_points();
+        uint64_t room = settings.max_particles > used ? settings.max_particles - used : 0;
+        if (points.size() > room) return FLUID_FULL;
+        // coarser probes for a big body, each standing for its share of the volume
+        R probe_spacing = R(settings.spacing);
+        for (;;) {
+            st = shape_points(kind, dims, probe_spacing, R(INFINITY), kMaxProbes, probes);
+            if (st == FLUID_FULL) {
+                probe_spacing = probe_spacing * R(1.25f);
+                continue;
+            }
+            if (st != OK) return st;
+            if (probes.empty()) {
+                probe_spacing = R(settings.spacing);
+                probes = points;
+            }
+            break;
+        }
+        uncouple(body);
+        Coupled c;
+        c.body = body;
+        c.points = std::move(points);
+        c.probes = std::move(probes);
+        c.probe_spacing = probe_spacing;
+        coupled.push_back(std::move(c));
+        std::stable_sort(coupled.begin(), coupled.end(),
+                         [](const Coupled& x, const Coupled& y) { return x.body < y.body; });
+        return OK;
+    }
+
+    // couple.rs:203-207
+    bool uncouple(uint64_t body) {
+        size_t before = coupled.size();
+        coupled.erase(std::remove_if(coupled.begin(), coupled.end(), [&](const Coupled& c) { return c.body == body; }),
+                      coupled.end());
+        return coupled.size() != before;
+    }
+
+    static const Pose* pose_of(const Pose* poses, size_t n, uint64_t body) {
+        for (size_t k = 0; k < n; ++k)
+            if (poses[k].body == body) return &poses[k];
+        return nullptr;
+    }
+    static Vec center_of(const Pose& p) {
+        // position.to_dvec3().as_vec3(): the f64 position rounded to f32
+        return Vec(R(float(p.position[0])), R(float(p.position[1])), R(float(p.position[2])));
+    }
+    static void quat_of(const Pose& p, R q[4]) {
+        for (int k = 0; k < 4; ++k) q[k] = R(p.rotation[k]);
+    }
+
+    // couple.rs:255-288: body points where the poses say, bodies without a pose uncoupled
+    void place_movers_at(const Pose* poses, size_t npose) {
+        coupled.erase(std::remove_if(coupled.begin(), coupled.end(),
+                                     [&](const Coupled& c) { return !pose_of(poses, npose, c.body); }),
+                      coupled.end());
+        Movers m;
+        for (size_t owner = 0; owner < coupled.size(); ++owner) {
+            Coupled& known = coupled[owner];
+            const Pose& state = *pose_of(poses, npose, known.body);
+            Vec center = center_of(state);
+            R q[4];
+            quat_of(state, q);
+            Vec lin(R(state.linear[0]), R(state.linear[1]), R(state.linear[2]));
+            Vec ang(R(state.angular[0]), R(state.angular[1]), R(state.angular[2]));
+            known.center = center;
+            known.velocity = lin;
+            known.impulse = known.angular = Vec();
+            for (const Vec& local : known.points) {
+                Vec arm = rotate(q, local);
+                m.start.push_back(center + arm);
+                m.velocities.push_back(lin + cross(ang, arm));
+                m.owners.push_back(uint32_t(owner));
+            }
+        }
+        m.positions = m.start;
+        movers = std::move(m);
+        carry_movers(R(0));
+    }
+
+    // couple.rs:291-322: points `elapsed` into the step, sorted by (cell, owner, place) again
+    void carry_movers(R elapsed) {
+        size_t k = movers.start.size();
+        struct MK {
+            Key cell;
+            uint32_t owner;
+            size_t index;
+        };
+        std::vector<MK> order(k);
+        for (size_t i = 0; i < k; ++i) {
+            Vec at = movers.start[i] + movers.velocities[i] * elapsed;
+            movers.positions[i] = at;
+            order[i] = MK{cell_of(at), movers.owners[i], i};
+        }
+        std::sort(order.begin(), order.end(), [](const MK& a, const MK& b) {
+            return std::tie(a.cell.x, a.cell.y, a.cell.z, a.owner, a.index) <
+                   std::tie(b.cell.x, b.cell.y, b.cell.z, b.owner, b.index);
+        });
+        Movers m;
+        std::vector<Key> keys(k);
+        for (size_t i = 0; i < k; ++i) {
+            size_t j = order[i].index;
+            m.start.push_back(movers.start[j]);
+            m.positions.push_back(movers.positions[j]);
+            m.velocities.push_back(movers.velocities[j]);
+            m.owners.push_back(movers.owners[j]);
+            keys[i] = order[i].cell;
+        }
+        m.grid = Grid::build(keys);
+        movers = std::move(m);
+        for (auto& known : coupled) known.moved = known.velocity * elapsed;
+    }
+
+    // couple.rs:325-366: the fastest coupled body that may meet the water within dt
+    R fastest_near_water(R dt, R slow) const {
+        size_t count = coupled.size();
+        std::vector<R> fastest_of(count, R(0));
+        std::vector<Vec> lows(count, Vec::splat(R(FLT_MAX))), highs(count, Vec::splat(R(-FLT_MAX)));
+        for (size_t i = 0; i < movers.positions.size(); ++i) {
+            size_t owner = movers.owners[i];
+            fastest_of[owner] = rmax(fastest_of[owner], length(movers.velocities[i]));
+            lows[owner] = vmin(lows[owner], movers.positions[i]);
+            highs[owner] = vmax(highs[owner], movers.positions[i]);
+        }
+        R water = fastest();
+        R r = radius();
+        R most = R(0);
+        for (size_t b = 0; b < count; ++b) {
+            R speed = fastest_of[b];
+            if (speed <= most) continue;
+            if (speed <= slow) {
+                most = speed;
+                continue;
+            }
+            Vec reach = Vec::splat(r + (speed + water) * dt);
+            Key lo = cell_of(lows[b] - reach), hi = cell_of(highs[b] + reach);
+            // before the first sort there is no grid to ask, any water counts
+            bool wet = grid.cells.empty() && !positions.empty();
+            for (size_t c = 0; !wet && c < grid.cells.size(); ++c) {
+                const Key& k = grid.cells[c].first;
+                wet = lo.x <= k.x && k.x <= hi.x && lo.y <= k.y && k.y <= hi.y && lo.z <= k.z && k.z <= hi.z;
+            }
+            if (wet) most = speed;
+        }
+        return most;
+    }
+
+    // couple.rs:375-416: pressure and damping between particle i and the body points near it;
+    // adds what the particle feels to `push` and, given `bodies`, the damping's opposite to them
+    void mover_push(size_t i, R mirrored, R damping, R settles, Vec& push, std::vector<std::pair<Vec, Vec>>* bodies) const {
+        uint32_t b = mover_neighbors.start.empty() ? 0 : mover_neighbors.start[i];
+        uint32_t e = mover_neighbors.start.empty() ? 0 : mover_neighbors.start[i + 1];
+        if (b == e) return;
+        Vec at = positions[i];
+        Vec velocity = velocities[i];
+        R density = densities[i];
+        R r = radius();
+        R soften = R(0.01f) * r * r;
+        for (uint32_t k = b; k < e; ++k) {
+            uint32_t point = mover_neighbors.items[k];
+            Vec offset = at - movers.positions[point];
+            Vec relative = velocity - movers.velocities[point];
+            R toward = dot(relative, offset);
+            R damp = toward < R(0) ? -damping * toward / (length_squared(offset) + soften) / density : R(0);
+            Vec gradient = kernel.gradient(offset) * mass;
+            push = push - gradient * (mirrored + damp);
+            if (toward * toward < settles * length_squared(offset)) continue;
+            if (!bodies) continue;
+            Vec force = gradient * (damp * mass);
+            uint32_t owner = movers.owners[point];
+            const Coupled& known = coupled[owner];
+            Vec arm = movers.positions[point] - (known.center + known.moved);
+            (*bodies)[owner].first = (*bodies)[owner].first + force;
+            (*bodies)[owner].second = (*bodies)[owner].second + cross(arm, force);
+        }
+    }
+
+    // lift.rs:24-158: what the water does to each coupled body over dt, read as one smooth field
+    struct Lift {
+        size_t owner;
+        Vec impulse, angular;
+        std::vector<uint32_t> near;
+    };
+    std::vector<Lift> lifts(R dt, const Pose* poses, size_t npose) const {
+        Vec g = gravity();
+        R grav = length(g);
+        Vec up = grav > R(0) ? (-g) / grav : Vec(R(0), R(1), R(0));
+        R r = radius();
+        R reach = R(3) * r;
+        R column = r;
+        std::vector<Lift> out;
+        for (size_t owner = 0; owner < coupled.size(); ++owner) {
+            const Coupled& known = coupled[owner];
+            const Pose* state = pose_of(poses, npose, known.body);
+            if (!state) continue;
+            Vec center = center_of(*state);
+            R q[4];
+            quat_of(*state, q);
+            Vec lin(R(state->linear[0]), R(state->linear[1]), R(state->linear[2]));
+            Vec ang(R(state->angular[0]), R(state->angular[1]), R(state->angular[2]));
+            std::vector<std::pair<Vec, Vec>> probes;
+            for (const Vec& local : known.probes) {
+                Vec arm = rotate(q, local);
+                probes.push_back({arm, lin + cross(ang, arm)});
+            }
+            Vec low = Vec::splat(R(FLT_MAX)), high = Vec::splat(R(-FLT_MAX));
+            for (auto& pr : probes) {
+                low = vmin(low, center + pr.first);
+                high = vmax(high, center + pr.first);
+            }
+            low = low - Vec::splat(reach);
+            high = high + Vec::splat(reach);
+            std::vector<uint32_t> near;
+            for (size_t i = 0; i < len(); ++i)
+                if (clamp(positions[i], low, high) == positions[i]) near.push_back(uint32_t(i));
+            if (near.empty()) continue;
+            // the level is the middle of the columns' tops
+            struct Top {
+                int32_t kx, kz;
+                R h;
+            };
+            std::vector<Top> tops;
+            for (uint32_t i : near) {
+                Vec at = positions[i];
+                tops.push_back(Top{as_i32(std::floor(at.x / column)), as_i32(std::floor(at.z / column)), dot(at, up)});
+            }
+            std::sort(tops.begin(), tops.end(), [](const Top& a, const Top& b) {
+                if (a.kx != b.kx) return a.kx < b.kx;
+                if (a.kz != b.kz) return a.kz < b.kz;
+                return total_less(b.h, a.h);
+            });
+            std::vector<R> heights;
+            for (size_t k = 0; k < tops.size(); ++k)
+                if (k == 0 || tops[k].kx != tops[k - 1].kx || tops[k].kz != tops[k - 1].kz) heights.push_back(tops[k].h);
+            std::sort(heights.begin(), heights.end(), [](R a, R b) { return total_less(a, b); });
+            size_t quarter = heights.size() / 4;
+            R sum = R(0);
+            for (size_t k = quarter; k < heights.size() - quarter; ++k) sum += heights[k];
+            R level = sum / R(float(heights.size() - 2 * quarter)) + R(settings.spacing) / R(2);
+            Vec flow;
+            uint32_t wet = 0;
+            for (uint32_t i : near)
+                if (dot(positions[i], up) <= level) {
+                    flow = flow + velocities[i];
+                    ++wet;
+                }
+            flow = flow / R(float(std::max<uint32_t>(wet, 1)));
+            R spacing = known.probe_spacing;
+            struct Under {
+                Vec arm, velocity;
+                R share;
+            };
+            std::vector<Under> under;
+            for (auto& pr : probes) {
+                R depth = level - dot(center + pr.first, up);
+                R share = rmin(rmax(depth / spacing + R(0.5f), R(0)), R(1));
+                if (share > R(0)) under.push_back(Under{pr.first, pr.second, share});
+            }
+            R wetted = R(0);
+            for (auto& u : under) wetted += u.share;
+            if (wetted <= R(0)) continue;
+            R volume = wetted * (spacing * spacing * spacing);
+            R density = R(settings.rest_density);
+            Vec middle;
+            for (auto& u : under) middle = middle + u.arm * u.share;
+            middle = middle / wetted;
+            Vec force, torque;
+            Vec buoyancy = up * (density * grav * volume);
+            force = force + buoyancy;
+            torque = torque + cross(middle, buoyancy);
+            R area = R(std::pow(volume, R(2.0f / 3.0f))) / wetted;
+            for (auto& u : under) {
+                Vec past = flow - u.velocity;
+                Vec drag = past * (R(0.5f) * R(1) * density * area * u.share * length(past));
+                force = force + drag;
+                torque = torque + cross(u.arm, drag);
+            }
+            size_t nline = 0;
+            for (auto& u : under) nline += u.share < R(1) ? 1 : 0;
+            R plane = R(float(nline)) * spacing * spacing;
+            R waves = density * plane * std::sqrt(grav * std::sqrt(plane));
+            R share = waves / R(float(std::max<size_t>(nline, 1)));
+            for (auto& u : under) {
+                if (!(u.share < R(1))) continue;
+                Vec calm = up * (share * dot(flow - u.velocity, up));
+                force = force + calm;
+                torque = torque + cross(u.arm, calm);
+            }
+            out.push_back(Lift{owner, force * dt, torque * dt, std::move(near)});
+        }
+        return out;
+    }
+
+    // lift.rs:160-166: the water read for a lift loses what the body got, shared by mass
+    void give_back(const Lift& lift) {
+        Vec change = lift.impulse / (mass * R(float(lift.near.size())));
+        for (uint32_t i : lift.near) velocities[i] = velocities[i] - change;
+    }
+
+    // couple.rs:219-248 with the rigid world's part left to the caller: the bodies stand where
+    // `poses` has them (a coupled body without a pose is uncoupled), and `pushes` receives, per
+    // coupled body in body order, the lift (given back to the water when the body is dynamic)
+    // and the damping impulse of the step, for the caller to apply as force and torque / dt
+    Status step_with_bodies(R dt, const Pose* poses, size_t npose, Report& report, std::vector<Push>& pushes) {
+        pushes.clear();
+        if (settings.solver != 0 && !coupled.empty()) return INVALID_SETTINGS;
+        place_movers_at(poses, npose);
+        Status st = step(dt, report);
+        movers = Movers{};
+        // the points are gone: so are the lists into them
+        if (!mover_neighbors.start.empty()) std::fill(mover_neighbors.start.begin(), mover_neighbors.start.end(), 0u);
+        mover_neighbors.items.clear();
+        if (st != OK) return st;
+        for (auto& known : coupled) {
+            Push p{};
+            p.body = known.body;
+            pushes.push_back(p);
+        }
+        if (dt > R(0)) {
+            for (const Lift& lift : lifts(dt, poses, npose)) {
+                Push& p = pushes[lift.owner];
+                p.lift = lift.impulse;
+                p.lift_angular = lift.angular;
+                if (pose_of(poses, npose, coupled[lift.owner].body)->dynamic) {
+                    give_back(lift);
+                    p.lifted = 1;
+                }
+            }
+            for (size_t b = 0; b < coupled.size(); ++b) {
+                pushes[b].damping = coupled[b].impulse;
+                pushes[b].damping_angular = coupled[b].angular;
+                coupled[b].impulse = coupled[b].angular = Vec();
+            }
+        }
+        return OK;
+    }
 
     // flow.rs:109-113
     bool remove_flow(uint32_t id) {
@@ -1035,17 +1497,18 @@ template <class R> class World {
         grid = Grid::build(keys);
 
         R reach = pow2(radius());
-        std::vector<uint32_t> fcount(n), wcount(n);
+        std::vector<uint32_t> fcount(n), wcount(n), mcount(n);
         // lists are formed per particle; joining them in particle order is the chunked join of
         // mod.rs:294-307 without the chunk boundaries, which do not change the result
-        std::vector<std::vector<uint32_t>> fparts, wparts;
+        std::vector<std::vector<uint32_t>> fparts, wparts, mparts;
         const size_t chunk = 512;
         size_t jobs = (n + chunk - 1) / chunk;
         fparts.resize(jobs);
         wparts.resize(jobs);
+        mparts.resize(jobs);
 #pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads())
         for (long long job = 0; job < (long long)jobs; ++job) {
-            std::vector<Range> af, aw;
+            std::vector<Range> af, aw, am;
             bool have = false;
             Key last{0, 0, 0};
             size_t b = size_t(job) * chunk, e = std::min(n, b + chunk);
@@ -1057,16 +1520,20 @@ template <class R> class World {
                     last = c;
                     grid.around(c, af);
                     walls.grid.around(c, aw);
+                    movers.grid.around(c, am);
                 }
-                size_t bf = fparts[job].size(), bw = wparts[job].size();
+                size_t bf = fparts[job].size(), bw = wparts[job].size(), bm = mparts[job].size();
                 near(positions, af, at, reach, fparts[job]);
                 near(walls.positions, aw, at, reach, wparts[job]);
+                near(movers.positions, am, at, reach, mparts[job]);
                 fcount[i] = uint32_t(fparts[job].size() - bf);
                 wcount[i] = uint32_t(wparts[job].size() - bw);
+                mcount[i] = uint32_t(mparts[job].size() - bm);
             }
         }
         join(fcount, fparts, neighbors);
         join(wcount, wparts, wall_neighbors);
+        join(mcount, mparts, mover_neighbors);
     }
 
     static void join(const std::vector<uint32_t>& counts, std::vector<std::vector<uint32_t>>& parts, Lists& out) {
@@ -1101,6 +1568,10 @@ template <class R> class World {
             R wsum = R(0);
             for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
                 wsum += kernel.value(length(walls.positions[wall_neighbors.items[k]] - at));
+            R msum = R(0);
+            if (!mover_neighbors.start.empty())
+                for (uint32_t k = mover_neighbors.start[i]; k < mover_neighbors.start[i + 1]; ++k)
+                    msum += kernel.value(length(movers.positions[mover_neighbors.items[k]] - at));
             // ground_near (mod.rs:657-663): each region holding the particle adds its ground
             R ground = R(0);
             Vec slope;
@@ -1111,7 +1582,7 @@ template <class R> class World {
                 ground = ground + density;
                 slope = slope + gradient;
             }
-            out[i] = mass * (sum + wsum + R(0)) + ground;
+            out[i] = mass * (sum + wsum + msum) + ground;
             if (!terrains.empty()) slopes[i] = slope;
         }
         densities = std::move(out);
@@ -1192,7 +1663,17 @@ template <class R> class World {
             if (f.emitter) o.v3(f.velocity);
         }
         o.u32(flow_next);
-        o.u32(0);  // coupled bodies
+        // Coupled::save (couple.rs:50-55)
+        o.u32(uint32_t(coupled.size()));
+        for (auto& c : coupled) {
+            o.u32(uint32_t(c.body >> 32));
+            o.u32(uint32_t(c.body & 0xffffffffu));
+            o.u32(uint32_t(c.points.size()));
+            for (auto& q : c.points) o.v3(q);
+            o.f32(float(c.probe_spacing));
+            o.u32(uint32_t(c.probes.size()));
+            for (auto& q : c.probes) o.v3(q);
+        }
         // TerrainField::save (terrain.rs:44-55)
         o.u32(uint32_t(terrains.size()));
         for (auto& t : terrains) {
@@ -1358,9 +1839,45 @@ template <class R> class World {
         if (!r.u32(w.flow_next)) return SNAPSHOT;
         for (auto& f : w.flows)
             if (f.id >= w.flow_next) return bad("invalid snapshot: fluid flow id");
-        size_t coupled, terrains;
-        if (!r.count(12, 1 << 16, coupled)) return SNAPSHOT;
-        if (coupled) return UNSUPPORTED;
+        size_t ncoupled, terrains;
+        if (!r.count(12, 1 << 16, ncoupled)) return SNAPSHOT;
+        // Coupled::load (couple.rs:58-75), load_points (couple.rs:435-451)
+        uint64_t room = st.max_particles;
+        auto points = [&](uint64_t max, std::vector<Vec>& out) -> Status {
+            size_t count;
+            if (!r.count(12, max, count)) return SNAPSHOT;
+            for (size_t k = 0; k < count; ++k) {
+                Vec q;
+                if (!r.v3(q)) return SNAPSHOT;
+                if (!is_finite(q)) return bad("invalid snapshot: fluid body point");
+                out.push_back(q);
+            }
+            if (out.empty()) return bad("invalid snapshot: fluid body");
+            return OK;
+        };
+        for (size_t k = 0; k < ncoupled; ++k) {
+            Coupled c;
+            uint32_t index, generation;
+            if (!(r.u32(index) && r.u32(generation))) return SNAPSHOT;
+            c.body = (uint64_t(index) << 32) | generation;
+            Status ps = points(room, c.points);
+            if (ps != OK) return ps;
+            if (version >= 3) {
+                float ps2;
+                if (!r.f32(ps2)) return SNAPSHOT;
+                if (!std::isfinite(ps2) || ps2 <= 0.0f) return bad("invalid snapshot: fluid body probes");
+                c.probe_spacing = R(ps2);
+                Status qs = points(kMaxProbes, c.probes);
+                if (qs != OK) return qs;
+            } else {
+                c.probe_spacing = R(st.spacing);
+                c.probes = c.points;
+            }
+            room -= c.points.size();
+            w.coupled.push_back(std::move(c));
+        }
+        for (size_t k = 1; k < w.coupled.size(); ++k)
+            if (w.coupled[k - 1].body >= w.coupled[k].body) return bad("invalid snapshot: fluid body order");
         if (!r.count(32, 1 << 16, terrains)) return SNAPSHOT;
         // TerrainField::load (terrain.rs:57-97)
         for (size_t k = 0; k < terrains; ++k) {
@@ -1431,15 +1948,20 @@ template <class R> class World {
         return OK;
     }
 
-    // step.rs:102-116 (no coupled bodies: the sound speed stays the configured one)
+    // step.rs:102-116: the sound speed of the step follows the fastest coupled body near water
     Status wcsph(R dt, Report& report) {
+        float configured = settings.sound_speed;
+        R mover = fastest_near_water(dt, R(configured) / R(4));
+        settings.sound_speed = float(rmax(R(configured), R(4) * mover));
         report.sound_speed = settings.sound_speed;
-        return wcsph_steps(dt, report);
+        Status st = wcsph_steps(dt, mover, report);
+        settings.sound_speed = configured;
+        return st;
     }
 
     // step.rs:118-142
-    Status wcsph_steps(R dt, Report& report) {
-        R fast = fastest();
+    Status wcsph_steps(R dt, R mover, Report& report) {
+        R fast = rmax(fastest(), mover);
         R largest = R(settings.courant) * radius() / (R(settings.sound_speed) + fast);
         R wanted = rmax(std::ceil(dt / largest), R(1));
         R cap = R(float(settings.max_substeps));
@@ -1448,6 +1970,7 @@ template <class R> class World {
         R small = dt / R(float(substeps));
         for (uint32_t i = 0; i < substeps; ++i) {
             uint32_t held = 0;
+            if (!coupled.empty()) carry_movers(small * R(float(i)));
             Status st = wcsph_substep(small, held);
             if (st != OK) return st;
             report.held_back += held;
@@ -1540,7 +2063,12 @@ template <class R> class World {
         R soften = R(0.01f) * r * r;
         R visc = viscosity(dt);
         Vec g = gravity();
+        // the body points' damping (step.rs:163-164) and the speed under which water settles
+        // against them (couple.rs:390)
+        R damping = rmin(R(1) * R(settings.sound_speed) * r, R(0.25f) * r * r / dt);
+        R settles = length(g) * R(settings.spacing);
         std::vector<Vec> pushes(n);
+        std::vector<R> mirrors(coupled.empty() ? 0 : n);
 #pragma omp parallel for schedule(static) num_threads(nthreads())
         for (long long ii = 0; ii < (long long)n; ++ii) {
             size_t i = size_t(ii);
@@ -1566,7 +2094,23 @@ template <class R> class World {
                 push = push - kernel.gradient(offset) * (mass * mirrored);
             }
             if (i < ground_slopes.size()) push = push - ground_slopes[i] * mirrored;
+            mover_push(i, mirrored, damping, settles, push, nullptr);
+            if (!mirrors.empty()) mirrors[i] = mirrored;
             pushes[i] = push + wall_viscous(i, dt) + g;
+        }
+        // what the body points took: summed per 512-particle chunk in particle order, the
+        // chunks' sums added in order (step.rs:173-221)
+        if (!coupled.empty()) {
+            for (size_t c0 = 0; c0 < n; c0 += 512) {
+                std::vector<std::pair<Vec, Vec>> felt(coupled.size());
+                Vec unused;
+                for (size_t i = c0; i < std::min(n, c0 + 512); ++i)
+                    mover_push(i, mirrors[i], damping, settles, unused, &felt);
+                for (size_t b = 0; b < coupled.size(); ++b) {
+                    coupled[b].impulse = coupled[b].impulse + felt[b].first * dt;
+                    coupled[b].angular = coupled[b].angular + felt[b].second * dt;
+                }
+            }
         }
         for (size_t i = 0; i < n; ++i) velocities[i] = velocities[i] + pushes[i] * dt;
         return advance(dt, held);

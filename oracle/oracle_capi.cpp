@@ -94,6 +94,45 @@ template <class R> int32_t read_lists(const Lists& l, uint32_t* start, uint64_t 
         }                                   \
     } while (0)
 
+template <class W>
+int32_t step_bodies(W& w, float dt, const slf_body_pose* poses, uint64_t npose, slf_report* out, slf_body_push* pushes,
+                    uint64_t cap, uint64_t* count) {
+    using Wd = typename std::decay<W>::type;
+    using R = decltype(w.mass);
+    std::vector<typename Wd::Pose> ps(npose);
+    for (uint64_t k = 0; k < npose; ++k) {
+        auto& q = ps[k];
+        q.body = poses[k].body;
+        for (int a = 0; a < 3; ++a) {
+            q.position[a] = poses[k].position[a];
+            q.linear[a] = poses[k].linear_velocity[a];
+            q.angular[a] = poses[k].angular_velocity[a];
+        }
+        for (int a = 0; a < 4; ++a) q.rotation[a] = poses[k].rotation[a];
+        q.dynamic = poses[k].dynamic;
+    }
+    Report r;
+    std::vector<typename Wd::Push> got;
+    int32_t st = w.step_with_bodies(R(dt), ps.data(), ps.size(), r, got);
+    to_report(r, out);
+    if (count) *count = got.size();
+    for (size_t k = 0; k < got.size() && k < cap && pushes; ++k) {
+        slf_body_push& o = pushes[k];
+        o.body = got[k].body;
+        auto put = [](float* d, const auto& v) {
+            d[0] = float(v.x);
+            d[1] = float(v.y);
+            d[2] = float(v.z);
+        };
+        put(o.lift, got[k].lift);
+        put(o.lift_angular, got[k].lift_angular);
+        put(o.damping, got[k].damping);
+        put(o.damping_angular, got[k].damping_angular);
+        o.lifted = got[k].lifted;
+    }
+    return st;
+}
+
 extern "C" {
 
 int32_t orc_create(const slf_settings* s, int32_t precision, int32_t residual_sum, void** out) {
@@ -312,6 +351,44 @@ int32_t orc_step(void* p, float dt, slf_report* out) {
     int32_t st = OK;
     ORC_DISPATCH(h, st = w.step(R(dt), r));
     to_report(r, out);
+    return st;
+}
+
+int32_t orc_couple(void* p, uint64_t body, int32_t shape, const float* dims) {
+    auto* h = static_cast<Handle*>(p);
+    if (!dims) return INVALID_ARGUMENT;
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = w.couple(body, shape, dims));
+    return st;
+}
+
+int32_t orc_uncouple(void* p, uint64_t body, int32_t* removed) {
+    auto* h = static_cast<Handle*>(p);
+    bool r = false;
+    ORC_DISPATCH(h, r = w.uncouple(body));
+    if (removed) *removed = r ? 1 : 0;
+    return OK;
+}
+
+int32_t orc_coupled(void* p, uint64_t* bodies, uint32_t* points, uint32_t* probes, uint64_t cap, uint64_t* count) {
+    auto* h = static_cast<Handle*>(p);
+    ORC_DISPATCH(h, {
+        if (count) *count = w.coupled.size();
+        for (size_t k = 0; k < w.coupled.size() && k < cap; ++k) {
+            if (bodies) bodies[k] = w.coupled[k].body;
+            if (points) points[k] = uint32_t(w.coupled[k].points.size());
+            if (probes) probes[k] = uint32_t(w.coupled[k].probes.size());
+        }
+    });
+    return OK;
+}
+
+int32_t orc_step_with_bodies(void* p, float dt, const slf_body_pose* poses, uint64_t npose, slf_report* out,
+                             slf_body_push* pushes, uint64_t cap, uint64_t* count) {
+    auto* h = static_cast<Handle*>(p);
+    if (npose && !poses) return INVALID_ARGUMENT;
+    int32_t st = OK;
+    ORC_DISPATCH(h, st = step_bodies(w, dt, poses, npose, out, pushes, cap, count));
     return st;
 }
 

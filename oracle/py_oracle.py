@@ -16,7 +16,8 @@ import subprocess
 
 import numpy as np
 
-from solunar_b200.abi import CReport, CSettings, FluidReport, FluidSettings, PhysicsError, vec3
+from solunar_b200.abi import (CBodyPose, CBodyPush, CReport, CSettings, FluidReport, FluidSettings, PhysicsError,
+                               step_with_bodies_call, vec3)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle_fluid.so")
@@ -66,6 +67,11 @@ def lib():
             "orc_wall_count": [vp, u64p],
             "orc_read_wall_positions": [vp, dp, ctypes.c_uint64],
             "orc_step": [vp, ctypes.c_float, ctypes.POINTER(CReport)],
+            "orc_couple": [vp, ctypes.c_uint64, ctypes.c_int32, f3],
+            "orc_uncouple": [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)],
+            "orc_coupled": [vp, u64p, u32p, u32p, ctypes.c_uint64, u64p],
+            "orc_step_with_bodies": [vp, ctypes.c_float, ctypes.POINTER(CBodyPose), ctypes.c_uint64,
+                                     ctypes.POINTER(CReport), ctypes.POINTER(CBodyPush), ctypes.c_uint64, u64p],
             "orc_update_neighbors": [vp],
             "orc_compute_densities": [vp],
             "orc_read_ids": [vp, u32p, ctypes.c_uint64],
@@ -262,6 +268,29 @@ class OracleWorld:
         r = CReport()
         _check(lib().orc_step(self._h, dt, ctypes.byref(r)))
         return FluidReport.from_c(r)
+
+    def couple(self, body: int, shape, dims):
+        """FluidWorld::couple (couple.rs:165-200)."""
+        d = list(dims) + [0.0] * (3 - len(dims))
+        _check(lib().orc_couple(self._h, body, int(shape), vec3(d)))
+
+    def uncouple(self, body: int) -> bool:
+        r = ctypes.c_int32()
+        _check(lib().orc_uncouple(self._h, body, ctypes.byref(r)))
+        return bool(r.value)
+
+    def coupled(self):
+        """[(body, points, probes)] in body order."""
+        n = ctypes.c_uint64()
+        _check(lib().orc_coupled(self._h, None, None, None, 0, ctypes.byref(n)))
+        k = n.value
+        b, p, q = (ctypes.c_uint64 * max(k, 1))(), (ctypes.c_uint32 * max(k, 1))(), (ctypes.c_uint32 * max(k, 1))()
+        _check(lib().orc_coupled(self._h, b, p, q, k, ctypes.byref(n)))
+        return [(int(b[i]), int(p[i]), int(q[i])) for i in range(k)]
+
+    def step_with_bodies(self, dt: float, poses):
+        """FluidWorld::step_with_bodies (couple.rs:219-248): (report, [BodyPush])."""
+        return step_with_bodies_call(lib().orc_step_with_bodies, self._h, dt, list(poses), _check)
 
     def update_neighbors(self):
         _check(lib().orc_update_neighbors(self._h))

@@ -21,6 +21,7 @@ STATUS_NAMES = {
     8: "Timeout",
     9: "InvalidArgument",
     10: "Snapshot",
+    11: "InvalidShape",
 }
 
 
@@ -208,6 +209,91 @@ class CParamGrads(ctypes.Structure):
         ("sound_speed", ctypes.c_double),
         ("gravity", ctypes.c_double * 3),
     ]
+
+
+class Shape(enum.IntEnum):
+    """Shapes a coupled body may have (src/shape.rs Cuboid, Sphere, Capsule)."""
+    CUBOID = 0   # dims: half extents
+    SPHERE = 1   # dims: (radius,)
+    CAPSULE = 2  # dims: (radius, half height)
+
+
+def body_handle(index: int, generation: int = 0) -> int:
+    """A BodyHandle's to_raw() pair as the library names bodies: index << 32 | generation."""
+    return (int(index) << 32) | int(generation)
+
+
+class CBodyPose(ctypes.Structure):
+    _fields_ = [
+        ("body", ctypes.c_uint64),
+        ("position", ctypes.c_double * 3),
+        ("rotation", ctypes.c_float * 4),
+        ("linear_velocity", ctypes.c_float * 3),
+        ("angular_velocity", ctypes.c_float * 3),
+        ("dynamic", ctypes.c_int32),
+    ]
+
+
+class CBodyPush(ctypes.Structure):
+    _fields_ = [
+        ("body", ctypes.c_uint64),
+        ("lift", ctypes.c_float * 3),
+        ("lift_angular", ctypes.c_float * 3),
+        ("damping", ctypes.c_float * 3),
+        ("damping_angular", ctypes.c_float * 3),
+        ("lifted", ctypes.c_int32),
+    ]
+
+
+@dataclasses.dataclass
+class BodyPose:
+    """Where a coupled body stands for a step and how it moves (src/substep.rs SubstepPose)."""
+    body: int
+    position: tuple
+    rotation: tuple = (0.0, 0.0, 0.0, 1.0)  # x, y, z, w
+    linear_velocity: tuple = (0.0, 0.0, 0.0)
+    angular_velocity: tuple = (0.0, 0.0, 0.0)
+    dynamic: bool = True
+
+    def to_c(self) -> CBodyPose:
+        c = CBodyPose()
+        c.body = int(self.body)
+        for a in range(3):
+            c.position[a] = float(self.position[a])
+            c.linear_velocity[a] = float(self.linear_velocity[a])
+            c.angular_velocity[a] = float(self.angular_velocity[a])
+        for a in range(4):
+            c.rotation[a] = float(self.rotation[a])
+        c.dynamic = 1 if self.dynamic else 0
+        return c
+
+
+@dataclasses.dataclass
+class BodyPush:
+    """What the water did to a coupled body over a step: impulses, to apply as force and
+    torque (impulse / dt) to a dynamic body over the rigid step that follows."""
+    body: int
+    lift: tuple
+    lift_angular: tuple
+    damping: tuple
+    damping_angular: tuple
+    lifted: bool
+
+    @classmethod
+    def from_c(cls, c: CBodyPush) -> "BodyPush":
+        return cls(int(c.body), tuple(c.lift), tuple(c.lift_angular), tuple(c.damping), tuple(c.damping_angular),
+                   bool(c.lifted))
+
+
+def step_with_bodies_call(fn, handle, dt, poses, check, capacity=64):
+    """Runs a C step_with_bodies entry point (library or restatement) and `check`s its status:
+    (report, pushes)."""
+    arr = (CBodyPose * max(len(poses), 1))(*[p.to_c() for p in poses])
+    out = (CBodyPush * capacity)()
+    count = ctypes.c_uint64()
+    r = CReport()
+    check(fn(handle, ctypes.c_float(dt), arr, len(poses), ctypes.byref(r), out, capacity, ctypes.byref(count)))
+    return FluidReport.from_c(r), [BodyPush.from_c(out[k]) for k in range(min(count.value, capacity))]
 
 
 def vec3(v) -> "ctypes.Array[ctypes.c_float]":

@@ -38,6 +38,7 @@ struct Params {
     float grad_scale;      // scale * (-20) / r^2: slope(d) / d = grad_scale * (1 - d / r)^3
     float inv_rest;        // 1 / rest_density
     float inv_rest_sq;     // 1 / rest_density^2
+    float settles;         // |gravity| spacing: the speed under which water settles on a body (couple.rs:390)
 };
 
 // Per-substep constants, in device memory so a captured substep reads the current ones.
@@ -46,6 +47,7 @@ struct StepConsts {
     float viscosity;       // viscosity(dt) (step.rs:254-259)
     float wall_viscosity;  // min(c r, 0.25 r^2 / dt) (step.rs:282-283)
     float dt_sq;           // dt * dt (dfsph.rs:246)
+    float mover_damping;   // min(1 c r, 0.25 r r / dt), the body points' damping (step.rs:163-164)
 };
 
 // Written by the kernels, read back by the host after each substep.
@@ -175,6 +177,16 @@ struct GridDev {
         return false;
     }
 #endif
+};
+
+// The points of the coupled bodies for the running substep (couple.rs:35-47), sorted by
+// (cell, owner, place) with their cell table: positions with the owner's index in w (as bits),
+// velocities.  count = 0: no bodies, every term is skipped.
+struct MoverDev {
+    uint32_t count;
+    GridDev grid;
+    const float4* pos;
+    const float4* vel;
 };
 
 #ifdef __CUDACC__

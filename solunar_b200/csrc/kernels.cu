@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
                                                     const float4* __restrict__ walls, PairLists fl, PairLists wl,
                                                     float* __restrict__ rho, float* __restrict__ press,
                                                     float* __restrict__ scaled, float* __restrict__ alpha, Status* st,
-                                                    TerrainDev T, float4* __restrict__ slope) {
+                                                    TerrainDev T, float4* __restrict__ slope, MoverDev M) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     bool valid = i < p.n;
@@ -408,10 +408,17 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
             }
             return g;
         });
-        // mass (fluid + walls + movers, none here) + ground (mod.rs:657-663)
+        // the coupled bodies' points, in their list order (mod.rs:648-656)
+        float msum = 0.0f;
+        if (M.count)
+            each_near(p, M.grid, M.pos, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+                float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
+                msum += kernel_value(p, sqrtf(dot3(ox, oy, oz, ox, oy, oz)));
+            });
+        // mass (fluid + walls + body points) + ground (mod.rs:657-663)
         float3 gslope;
         float ground = T.regions ? ground_near(T, a.x, a.y, a.z, gslope) : 0.0f;
-        float density = p.mass * (sum + wsum + 0.0f) + ground;
+        float density = p.mass * (sum + wsum + msum) + ground;
         rho[i] = density;
         if (slope) slope[i] = make_float4(gslope.x, gslope.y, gslope.z, 0.0f);
         if (SOLVER == 0) {
@@ -638,6 +645,81 @@ __device__ __forceinline__ void advance_one(const Params& p, float dt, float4& a
     a.z = nz;
 }
 
+// ---- coupled bodies' points (couple.rs:375-416) ---------------------------------------------
+
+// The body points within reach of a particle at `a` moving at `v`, in list order: for each,
+// f(j, gradient * mass (xyz), mirrored + damp, damp, toward) with the reference's arithmetic.
+template <class F>
+__device__ __forceinline__ void mover_pairs(const Params& p, const MoverDev& M, float damping, float4 a, float4 v,
+                                            float density, float mirrored, F&& f) {
+    int3 cell = cell_of(p, a.x, a.y, a.z);
+    each_near(p, M.grid, M.pos, cell, a.x, a.y, a.z, [&](uint32_t j, float4 q) {
+        float ox = a.x - q.x, oy = a.y - q.y, oz = a.z - q.z;  // at - point
+        float4 w = __ldg(&M.vel[j]);
+        float toward = dot3(v.x - w.x, v.y - w.y, v.z - w.z, ox, oy, oz);
+        float damp = toward < 0.0f ? -damping * toward / (dot3(ox, oy, oz, ox, oy, oz) + p.soften) / density : 0.0f;
+        float g = kernel_gradient_factor(p, ox, oy, oz);
+        f(j, (ox * g) * p.mass, (oy * g) * p.mass, (oz * g) * p.mass, mirrored + damp, damp, toward);
+    });
+}
+
+// What the body points took from the water this substep: one thread per (512-particle chunk,
+// body) walks the chunk's particles in order and sums, for the points of its body, the damping
+// force and its torque about the body's centre (couple.rs:401-414, step.rs:173-221).  Pairs
+// below the settling speed give nothing.  centre[b] = centre + moved; felt[c * bodies + b] =
+// (force, torque).
+__global__ void k_mover_felt(Params p, const StepConsts* __restrict__ sc, MoverDev M, const float4* __restrict__ pos,
+                             const float4* __restrict__ vel, const float* __restrict__ rho,
+                             const float* __restrict__ press, const float* __restrict__ scaled,
+                             const float4* __restrict__ centre, uint32_t bodies, float4* __restrict__ felt) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t chunks = (p.n + 511u) / 512u;
+    if (t >= chunks * bodies) return;
+    uint32_t c = t / bodies, b = t % bodies;
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f, tx = 0.0f, ty = 0.0f, tz = 0.0f;
+    float4 o = centre[b];
+    uint32_t end = min(p.n, (c + 1u) * 512u);
+    for (uint32_t i = c * 512u; i < end; ++i) {
+        float4 a = pos[i], v = vel[i];
+        float density = rho[i];
+        float mirrored = scaled[i] + press[i] / p.rest_sq;
+        mover_pairs(p, M, sc->mover_damping, a, v, density, mirrored,
+                    [&](uint32_t j, float gx, float gy, float gz, float, float damp, float toward) {
+                        float4 q = __ldg(&M.pos[j]);
+                        if (__float_as_uint(q.w) != b) return;
+                        float ox = a.x - q.x, oy = a.y - q.y, oz = a.z - q.z;
+                        if (toward * toward < p.settles * dot3(ox, oy, oz, ox, oy, oz)) return;
+                        float s = damp * p.mass;
+                        float ex = gx * s, ey = gy * s, ez = gz * s;
+                        float rx = q.x - o.x, ry = q.y - o.y, rz = q.z - o.z;
+                        fx = fx + ex;
+                        fy = fy + ey;
+                        fz = fz + ez;
+                        tx = tx + (ry * ez - ey * rz);
+                        ty = ty + (rz * ex - ez * rx);
+                        tz = tz + (rx * ey - ex * ry);
+                    });
+    }
+    felt[2 * size_t(t)] = make_float4(fx, fy, fz, 0.0f);
+    felt[2 * size_t(t) + 1] = make_float4(tx, ty, tz, 0.0f);
+}
+
+// Whether any cell of the box [lo, hi] (cell keys) holds fluid in the last sort's dense table
+// (couple.rs:350-357); *wet = 1 if so.
+__global__ void k_cells_wet(GridDev g, int3 lo, int3 hi, uint32_t* wet) {
+    long long nx = (long long)hi.x - lo.x + 1, ny = (long long)hi.y - lo.y + 1, nz = (long long)hi.z - lo.z + 1;
+    long long total = nx * ny * nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        long long x = lo.x + t / (ny * nz), y = lo.y + (t / nz) % ny, z = lo.z + t % nz;
+        uint32_t b, e;
+        if (g.range(x, y, z, b, e)) {
+            *wet = 1u;
+            return;
+        }
+    }
+}
+
 // ---- WCSPH: forces, velocity update and advance in one pass (step.rs:159-223, 305-339) -----
 
 __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
@@ -648,7 +730,7 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
                                                         const float4* __restrict__ walls, float4* __restrict__ pos_out,
                                                         float4* __restrict__ vel_out, Status* st,
                                                         float4* __restrict__ vel_pre, TerrainDev T,
-                                                        const float4* __restrict__ slope) {
+                                                        const float4* __restrict__ slope, MoverDev M) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     bool valid = i < p.n;
@@ -690,6 +772,13 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
             py = py - sl.y * mirrored;
             pz = pz - sl.z * mirrored;
         }
+        if (M.count)
+            mover_pairs(p, M, sc->mover_damping, a, v, density, mirrored,
+                        [&](uint32_t, float gx, float gy, float gz, float s, float, float) {
+                            px = px - gx * s;
+                            py = py - gy * s;
+                            pz = pz - gz * s;
+                        });
         float3 wv = wall_viscous(p, sc->wall_viscosity, wl, walls, row, a, v, density, T);
         float ax = (px + wv.x) + p.gravity.x, ay = (py + wv.y) + p.gravity.y, az = (pz + wv.z) + p.gravity.z;
         v.x = v.x + ax * dt;
@@ -1125,23 +1214,40 @@ void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start,
 
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
-                    Status* st, const TerrainDev& T, float4* slope, cudaStream_t s) {
+                    Status* st, const TerrainDev& T, float4* slope, cudaStream_t s, const MoverDev& M) {
     if (!p.n) return;
     if (p.solver == 0)
         k_density<0><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
-                                                        T, slope);
+                                                        T, slope, M);
     else
         k_density<1><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
-                                                        T, slope);
+                                                        T, slope, M);
 }
 
 void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                         const float4* pos, const float4* vel, const float* rho, const float* press,
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                        float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s) {
+                        float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s,
+                        const MoverDev& M) {
     if (p.n)
         k_wcsph_force<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled, walls, pos_out,
-                                                         vel_out, st, vel_pre, T, slope);
+                                                         vel_out, st, vel_pre, T, slope, M);
+}
+
+void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos, const float4* vel,
+                       const float* rho, const float* press, const float* scaled, const float4* centre,
+                       uint32_t bodies, float4* felt, cudaStream_t s) {
+    uint32_t threads = (p.n + 511u) / 512u * bodies;
+    if (threads) k_mover_felt<<<(threads + 63u) / 64u, 64, 0, s>>>(p, sc, M, pos, vel, rho, press, scaled, centre, bodies, felt);
+    note_launch();
+}
+
+void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStream_t s) {
+    long long total = ((long long)hi.x - lo.x + 1) * ((long long)hi.y - lo.y + 1) * ((long long)hi.z - lo.z + 1);
+    if (total <= 0) return;
+    long long blocks = std::min<long long>((total + kBlock - 1) / kBlock, 4096);
+    k_cells_wet<<<uint32_t(blocks), kBlock, 0, s>>>(g, lo, hi, wet);
+    note_launch();
 }
 
 size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (sizeof(DD) + sizeof(uint32_t)) + 64; }

@@ -41,13 +41,21 @@ void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32
 // T: terrain regions (regions = 0: none); slope (optional): each particle's ground density gradient
 void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const float4* walls,
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
-                    Status* st, const TerrainDev& T, float4* slope, cudaStream_t s);
+                    Status* st, const TerrainDev& T, float4* slope, cudaStream_t s, const MoverDev& M = MoverDev{});
 // vel_pre (optional): the velocity before the wall clamp, its w lane the bits of the components
 // the clamp zeroed (1 x, 2 y, 4 z), for the adjoint
 void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                         const float4* pos, const float4* vel, const float* rho, const float* press,
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
-                        float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s);
+                        float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s,
+                        const MoverDev& M = MoverDev{});
+// coupled bodies: per (512-particle chunk, body) the damping force and torque the body's points
+// took this substep (felt: chunks x bodies pairs of float4); and whether the last sort's table
+// holds fluid in the cell box [lo, hi] (*wet set to 1, left alone otherwise)
+void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos, const float4* vel,
+                       const float* rho, const float* press, const float* scaled, const float4* centre,
+                       uint32_t bodies, float4* felt, cudaStream_t s);
+void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
 // sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve

@@ -11,6 +11,7 @@
 // finished clean is committed by switching slot indexes.  A failed substep therefore leaves the
 // particles as the last finished substep put them (src/fluid/step.rs:55-57).
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -112,6 +113,34 @@ inline int32_t sat_i32(float v) {
 struct F3 {
     float x, y, z;
 };
+// f32 vector arithmetic of the coupled bodies' host-side steps, in the reference's order
+inline F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline F3 operator-(F3 a) { return {-a.x, -a.y, -a.z}; }
+inline F3 operator*(F3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline F3 operator/(F3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+inline bool operator==(F3 a, F3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+inline float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline float length(F3 a) { return std::sqrt(dot(a, a)); }
+inline F3 vmin(F3 a, F3 b) { return {rmin(a.x, b.x), rmin(a.y, b.y), rmin(a.z, b.z)}; }
+inline F3 vmax(F3 a, F3 b) { return {rmax(a.x, b.x), rmax(a.y, b.y), rmax(a.z, b.z)}; }
+// f32::total_cmp's order
+inline bool total_less(float a, float b) {
+    int32_t x, y;
+    std::memcpy(&x, &a, 4);
+    std::memcpy(&y, &b, 4);
+    x ^= int32_t(uint32_t(x >> 31) >> 1);
+    y ^= int32_t(uint32_t(y >> 31) >> 1);
+    return x < y;
+}
+inline F3 cross(F3 a, F3 b) { return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y}; }
+// q * v for the unit quaternion (x, y, z, w): v (w^2 - |b|^2) + b 2 (v.b) + (b x v) 2 w, b = (x, y, z)
+inline F3 rotate(const float q[4], F3 v) {
+    F3 b{q[0], q[1], q[2]};
+    float w = q[3];
+    float b2 = dot(b, b);
+    return v * (w * w - b2) + b * (dot(v, b) * 2.0f) + cross(b, v) * (w * 2.0f);
+}
 inline bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
 
 struct Key3 {
@@ -712,6 +741,8 @@ struct World {
         p.grad_scale = scale * -20.0f / (radius * radius);
         p.inv_rest = 1.0f / s.rest_density;
         p.inv_rest_sq = 1.0f / (s.rest_density * s.rest_density);
+        p.settles = std::sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] + s.gravity[2] * s.gravity[2]) *
+                    s.spacing;
         return p;
     }
 
@@ -723,6 +754,7 @@ struct World {
         float stable = radius * radius / dt;
         c.wall_viscosity = rmin(1.0f * s.sound_speed * radius, 0.25f * stable);
         c.dt_sq = dt * dt;
+        c.mover_damping = rmin(1.0f * s.sound_speed * radius, 0.25f * radius * radius / dt);
         return c;
     }
 
@@ -861,7 +893,7 @@ struct World {
                                 alpha.p, d_status, stream);
         else
             launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status,
-                           tdev, ground_slopes(), stream);
+                           tdev, ground_slopes(), stream, mover_dev());
     }
     void force_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
         if (fast())
@@ -870,7 +902,7 @@ struct World {
         else
             launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
                                pos[b].p, vel[b].p, d_status, vel_pre, tdev, terrains.empty() ? nullptr : gslope.p,
-                               stream);
+                               stream, mover_dev());
     }
     // cs, loop: the stream of a graph capture and the while-node handle of its solve loop
     void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid,
@@ -921,6 +953,477 @@ struct World {
         list_cap = (uint32_t(h_status->list_max) + h_status->list_max / 4 + 15u) & ~7u;
         SLF_TRY(ensure_work_buffers());
         return kRetry;
+    }
+
+    // ---- coupled bodies (src/fluid/couple.rs, lift.rs) -------------------------------------
+
+    // A body the water and the caller's rigid world share (couple.rs:15-33): its points, frozen
+    // water on its own lattice as deep under its surface as the kernel reaches, and its probes,
+    // a lattice through its volume for the lift, both in body axes about its centre.
+    struct Coupled {
+        uint64_t body;
+        std::vector<F3> points, probes;
+        float probe_spacing = 0.0f;
+        F3 center{0, 0, 0}, velocity{0, 0, 0}, moved{0, 0, 0};
+        F3 impulse{0, 0, 0}, angular{0, 0, 0};  // the damping's push this step
+    };
+    std::vector<Coupled> coupled;
+    static constexpr size_t kMaxProbes = 4096;  // lift.rs:8
+    // the body points of the running step (couple.rs:35-47), sorted, and their device copies
+    std::vector<F3> m_start, m_pos, m_vel;
+    std::vector<uint32_t> m_own;
+    DevBuf<float4> dmpos, dmvel, dcentre, dfelt;
+    DevBuf<uint32_t> dmstart, dwet;
+    DevBuf<int4> dmkeys;
+    GridDev mgrid{};
+    std::vector<float4> h_felt;
+
+    MoverDev mover_dev() const {
+        MoverDev M{};
+        if (m_pos.empty()) return M;
+        M.count = uint32_t(m_pos.size());
+        M.grid = mgrid;
+        M.pos = dmpos.p;
+        M.vel = dmvel.p;
+        return M;
+    }
+
+    // couple.rs:453-511: lattice points `spacing` apart inside the shape, no deeper than `reach`
+    static int32_t shape_points(int kind, const float dims[3], float spacing, float reach, uint64_t limit,
+                                std::vector<F3>& out) {
+        out.clear();
+        F3 half;
+        float a = dims[0], b = dims[1], c = dims[2];
+        if (kind == SLF_SHAPE_CUBOID) {
+            half = F3{a, b, c};
+        } else if (kind == SLF_SHAPE_SPHERE) {
+            half = F3{a, a, a};
+        } else if (kind == SLF_SHAPE_CAPSULE) {
+            if (!(b >= 0.0f)) return fail(SLF_ERR_INVALID_SHAPE, "invalid shape");
+            half = F3{a, b + a, a};
+        } else {
+            return fail(SLF_ERR_INVALID_SHAPE, "invalid shape");
+        }
+        bool finite = std::isfinite(half.x) && std::isfinite(half.y) && std::isfinite(half.z);
+        if (!finite || rmin(rmin(half.x, half.y), half.z) <= 0.0f) return fail(SLF_ERR_INVALID_SHAPE, "invalid shape");
+        auto depth = [&](F3 at) -> float {
+            if (kind == SLF_SHAPE_CUBOID) {
+                F3 room = half - F3{std::fabs(at.x), std::fabs(at.y), std::fabs(at.z)};
+                return rmin(rmin(room.x, room.y), room.z);
+            }
+            if (kind == SLF_SHAPE_SPHERE) return a - length(at);
+            float y = rmin(rmax(at.y, -b), b);
+            return a - length(at - F3{0.0f, y, 0.0f});
+        };
+        auto count = [&](float extent) -> int64_t {
+            float v = std::floor(2.0f * extent / spacing);
+            return std::isnan(v) ? 0 : (v >= 4096.0f ? 4096 : (v <= 0.0f ? 0 : int64_t(v)));
+        };
+        int64_t cx = count(half.x), cy = count(half.y), cz = count(half.z);
+        if (uint64_t(cx * cy * cz) > limit) return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
+        auto start = [&](int64_t cells) { return -(float(cells) - 1.0f) * spacing / 2.0f; };
+        F3 origin{start(cx), start(cy), start(cz)};
+        for (int64_t y = 0; y < cy; ++y)
+            for (int64_t z = 0; z < cz; ++z)
+                for (int64_t x = 0; x < cx; ++x) {
+                    F3 at = origin + F3{float(x), float(y), float(z)} * spacing;
+                    float inside = depth(at);
+                    if (inside >= 0.0f && inside <= reach) out.push_back(at);
+                }
+        return SLF_OK;
+    }
+
+    uint64_t coupled_points() const {
+        uint64_t k = 0;
+        for (auto& c : coupled) k += c.points.size();
+        return k;
+    }
+
+    // couple.rs:165-200
+    int32_t couple(uint64_t body, int32_t kind, const float dims[3]) {
+        std::vector<F3> points, probes;
+        SLF_TRY(shape_points(kind, dims, s.spacing, radius, s.max_particles, points));
+        if (points.empty()) return fail(SLF_ERR_INVALID_SHAPE, "invalid shape");
+        uint64_t used = coupled_points();
+        uint64_t room = s.max_particles > used ? s.max_particles - used : 0;
+        if (points.size() > room) return fail(SLF_ERR_FLUID_FULL, "fluid has no room for more particles");
+        // coarser probes for a big body, each standing for its share of the volume
+        float probe_spacing = s.spacing;
+        for (;;) {
+            int32_t st = shape_points(kind, dims, probe_spacing, INFINITY, kMaxProbes, probes);
+            if (st == SLF_ERR_FLUID_FULL) {
+                probe_spacing = probe_spacing * 1.25f;
+                continue;
+            }
+            SLF_TRY(st);
+            if (probes.empty()) {
+                probe_spacing = s.spacing;
+                probes = points;
+            }
+            break;
+        }
+        uncouple(body);
+        Coupled c;
+        c.body = body;
+        c.points = std::move(points);
+        c.probes = std::move(probes);
+        c.probe_spacing = probe_spacing;
+        coupled.push_back(std::move(c));
+        std::stable_sort(coupled.begin(), coupled.end(),
+                         [](const Coupled& x, const Coupled& y) { return x.body < y.body; });
+        return SLF_OK;
+    }
+
+    // couple.rs:203-207
+    bool uncouple(uint64_t body) {
+        size_t before = coupled.size();
+        coupled.erase(std::remove_if(coupled.begin(), coupled.end(), [&](const Coupled& c) { return c.body == body; }),
+                      coupled.end());
+        return coupled.size() != before;
+    }
+
+    static const slf_body_pose* pose_of(const slf_body_pose* poses, uint64_t n, uint64_t body) {
+        for (uint64_t k = 0; k < n; ++k)
+            if (poses[k].body == body) return &poses[k];
+        return nullptr;
+    }
+    // position.to_dvec3().as_vec3(): the f64 position rounded to f32
+    static F3 center_of(const slf_body_pose& p) {
+        return F3{float(p.position[0]), float(p.position[1]), float(p.position[2])};
+    }
+    static F3 f3v(const float* v) { return F3{v[0], v[1], v[2]}; }
+
+    // couple.rs:255-288: body points where the poses say; bodies without a pose are uncoupled
+    void place_movers_at(const slf_body_pose* poses, uint64_t npose) {
+        coupled.erase(std::remove_if(coupled.begin(), coupled.end(),
+                                     [&](const Coupled& c) { return !pose_of(poses, npose, c.body); }),
+                      coupled.end());
+        m_start.clear();
+        m_vel.clear();
+        m_own.clear();
+        for (size_t owner = 0; owner < coupled.size(); ++owner) {
+            Coupled& known = coupled[owner];
+            const slf_body_pose& state = *pose_of(poses, npose, known.body);
+            F3 center = center_of(state), lin = f3v(state.linear_velocity), ang = f3v(state.angular_velocity);
+            known.center = center;
+            known.velocity = lin;
+            known.impulse = known.angular = F3{0, 0, 0};
+            for (const F3& local : known.points) {
+                F3 arm = rotate(state.rotation, local);
+                m_start.push_back(center + arm);
+                m_vel.push_back(lin + cross(ang, arm));
+                m_own.push_back(uint32_t(owner));
+            }
+        }
+        m_pos = m_start;
+    }
+
+    // couple.rs:291-322: points `elapsed` into the step, sorted by (cell, owner, place), and their
+    // device copies and cell table
+    int32_t carry_movers(float elapsed) {
+        size_t k = m_start.size();
+        struct MK {
+            Key3 cell;
+            uint32_t owner;
+            size_t index;
+        };
+        std::vector<MK> order(k);
+        for (size_t i = 0; i < k; ++i) {
+            F3 at = m_start[i] + m_vel[i] * elapsed;
+            m_pos[i] = at;
+            order[i] = MK{cell_of(at), m_own[i], i};
+        }
+        std::sort(order.begin(), order.end(), [](const MK& a, const MK& b) {
+            return std::tie(a.cell.x, a.cell.y, a.cell.z, a.owner, a.index) <
+                   std::tie(b.cell.x, b.cell.y, b.cell.z, b.owner, b.index);
+        });
+        std::vector<F3> st(k), ps(k), vs(k);
+        std::vector<uint32_t> ow(k);
+        std::vector<Key3> keys(k);
+        for (size_t i = 0; i < k; ++i) {
+            size_t j = order[i].index;
+            st[i] = m_start[j];
+            ps[i] = m_pos[j];
+            vs[i] = m_vel[j];
+            ow[i] = m_own[j];
+            keys[i] = order[i].cell;
+        }
+        m_start = std::move(st);
+        m_pos = std::move(ps);
+        m_vel = std::move(vs);
+        m_own = std::move(ow);
+        for (auto& known : coupled) known.moved = known.velocity * elapsed;
+        if (!k) {
+            mgrid = GridDev{};
+            return SLF_OK;
+        }
+        std::vector<float4> hp(k), hv(k);
+        for (size_t i = 0; i < k; ++i) {
+            uint32_t bits = m_own[i];
+            float w;
+            std::memcpy(&w, &bits, 4);
+            hp[i] = make_float4(m_pos[i].x, m_pos[i].y, m_pos[i].z, w);
+            hv[i] = make_float4(m_vel[i].x, m_vel[i].y, m_vel[i].z, 0.0f);
+        }
+        SLF_TRY(dmpos.ensure(k, 0, stream));
+        SLF_TRY(dmvel.ensure(k, 0, stream));
+        SLF_CUDA(cudaMemcpyAsync(dmpos.p, hp.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        SLF_CUDA(cudaMemcpyAsync(dmvel.p, hv.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        SLF_TRY(grid_from_keys(keys, mgrid, dmstart, dmkeys));  // waits for the copies
+        return SLF_OK;
+    }
+
+    // couple.rs:325-366: the fastest coupled body that may meet the water within dt.  The water's
+    // cells are those of the last sort (the reference's grid).
+    int32_t fastest_near_water(float dt, float slow, float& most) {
+        most = 0.0f;
+        size_t count = coupled.size();
+        if (!count || m_pos.empty()) return SLF_OK;
+        std::vector<float> fastest_of(count, 0.0f);
+        std::vector<F3> lows(count, F3{FLT_MAX, FLT_MAX, FLT_MAX}), highs(count, F3{-FLT_MAX, -FLT_MAX, -FLT_MAX});
+        for (size_t i = 0; i < m_pos.size(); ++i) {
+            size_t owner = m_own[i];
+            fastest_of[owner] = rmax(fastest_of[owner], length(m_vel[i]));
+            lows[owner] = vmin(lows[owner], m_pos[i]);
+            highs[owner] = vmax(highs[owner], m_pos[i]);
+        }
+        float water = fastest();
+        for (size_t b = 0; b < count; ++b) {
+            float speed = fastest_of[b];
+            if (speed <= most) continue;
+            if (speed <= slow) {
+                most = speed;
+                continue;
+            }
+            float reach = radius + (speed + water) * dt;
+            Key3 lo = cell_of(lows[b] - F3{reach, reach, reach}), hi = cell_of(highs[b] + F3{reach, reach, reach});
+            // before the first sort there is no table to ask, any water counts
+            bool wet = fgrid.mode == 0 && n > 0;
+            if (!wet && fgrid.mode != 0) {
+                SLF_TRY(dwet.ensure(1, 0, stream));
+                SLF_CUDA(cudaMemsetAsync(dwet.p, 0, 4, stream));
+                launch_cells_wet(fgrid, make_int3(lo.x, lo.y, lo.z), make_int3(hi.x, hi.y, hi.z), dwet.p, stream);
+                uint32_t flag = 0;
+                SLF_CUDA(cudaMemcpyAsync(&flag, dwet.p, 4, cudaMemcpyDeviceToHost, stream));
+                SLF_TRY(sync());
+                wet = flag != 0;
+            }
+            if (wet) most = speed;
+        }
+        return SLF_OK;
+    }
+
+    // After a committed WCSPH substep of length dt: what each body's points took, per chunk of 512
+    // particles in particle order, added chunk by chunk (step.rs:173-221); the substep's
+    // inputs are slot a's positions and velocities and its densities and pressures
+    int32_t mover_felt(float dt, const Params& p, int a, int nid) {
+        if (coupled.empty() || m_pos.empty() || n == 0) return SLF_OK;
+        size_t bodies = coupled.size(), chunks = (n + 511) / 512;
+        std::vector<float4> centres(bodies);
+        for (size_t b = 0; b < bodies; ++b) {
+            F3 o = coupled[b].center + coupled[b].moved;
+            centres[b] = make_float4(o.x, o.y, o.z, 0.0f);
+        }
+        SLF_TRY(dcentre.ensure(bodies, 0, stream));
+        SLF_TRY(dfelt.ensure(2 * chunks * bodies, 0, stream));
+        SLF_CUDA(cudaMemcpyAsync(dcentre.p, centres.data(), bodies * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        launch_mover_felt(p, d_consts, mover_dev(), pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dcentre.p,
+                          uint32_t(bodies), dfelt.p, stream);
+        h_felt.resize(2 * chunks * bodies);
+        SLF_CUDA(cudaMemcpyAsync(h_felt.data(), dfelt.p, h_felt.size() * sizeof(float4), cudaMemcpyDeviceToHost,
+                                 stream));
+        SLF_TRY(sync());
+        for (size_t c = 0; c < chunks; ++c)
+            for (size_t b = 0; b < bodies; ++b) {
+                const float4& f = h_felt[2 * (c * bodies + b)];
+                const float4& t = h_felt[2 * (c * bodies + b) + 1];
+                coupled[b].impulse = coupled[b].impulse + F3{f.x, f.y, f.z} * dt;
+                coupled[b].angular = coupled[b].angular + F3{t.x, t.y, t.z} * dt;
+            }
+        return SLF_OK;
+    }
+
+    // lift.rs:24-158: what the water does to each coupled body over dt, read as one smooth field
+    // around it, from the committed positions and velocities (host copies in p, v)
+    struct Lift {
+        size_t owner;
+        F3 impulse, angular;
+        std::vector<uint32_t> near;
+    };
+    std::vector<Lift> lifts(float dt, const slf_body_pose* poses, uint64_t npose, const std::vector<F3>& P,
+                            const std::vector<F3>& V) const {
+        F3 g{s.gravity[0], s.gravity[1], s.gravity[2]};
+        float grav = length(g);
+        F3 up = grav > 0.0f ? (-g) / grav : F3{0.0f, 1.0f, 0.0f};
+        float reach = 3.0f * radius;
+        float column = radius;
+        std::vector<Lift> out;
+        for (size_t owner = 0; owner < coupled.size(); ++owner) {
+            const Coupled& known = coupled[owner];
+            const slf_body_pose* state = pose_of(poses, npose, known.body);
+            if (!state) continue;
+            F3 center = center_of(*state), lin = f3v(state->linear_velocity), ang = f3v(state->angular_velocity);
+            std::vector<std::pair<F3, F3>> probes;
+            for (const F3& local : known.probes) {
+                F3 arm = rotate(state->rotation, local);
+                probes.push_back({arm, lin + cross(ang, arm)});
+            }
+            F3 low{FLT_MAX, FLT_MAX, FLT_MAX}, high{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+            for (auto& pr : probes) {
+                low = vmin(low, center + pr.first);
+                high = vmax(high, center + pr.first);
+            }
+            low = low - F3{reach, reach, reach};
+            high = high + F3{reach, reach, reach};
+            std::vector<uint32_t> near;
+            for (size_t i = 0; i < P.size(); ++i)
+                if (vmin(vmax(P[i], low), high) == P[i]) near.push_back(uint32_t(i));
+            if (near.empty()) continue;
+            // the level is the middle of the columns' tops
+            struct Top {
+                int32_t kx, kz;
+                float h;
+            };
+            std::vector<Top> tops;
+            for (uint32_t i : near)
+                tops.push_back(Top{sat_i32(std::floor(P[i].x / column)), sat_i32(std::floor(P[i].z / column)),
+                                   dot(P[i], up)});
+            std::sort(tops.begin(), tops.end(), [](const Top& a, const Top& b) {
+                if (a.kx != b.kx) return a.kx < b.kx;
+                if (a.kz != b.kz) return a.kz < b.kz;
+                return total_less(b.h, a.h);
+            });
+            std::vector<float> heights;
+            for (size_t k = 0; k < tops.size(); ++k)
+                if (k == 0 || tops[k].kx != tops[k - 1].kx || tops[k].kz != tops[k - 1].kz) heights.push_back(tops[k].h);
+            std::sort(heights.begin(), heights.end(), total_less);
+            size_t quarter = heights.size() / 4;
+            float sum = 0.0f;
+            for (size_t k = quarter; k < heights.size() - quarter; ++k) sum += heights[k];
+            float level = sum / float(heights.size() - 2 * quarter) + s.spacing / 2.0f;
+            F3 flow{0, 0, 0};
+            uint32_t wet = 0;
+            for (uint32_t i : near)
+                if (dot(P[i], up) <= level) {
+                    flow = flow + V[i];
+                    ++wet;
+                }
+            flow = flow / float(std::max<uint32_t>(wet, 1));
+            float spacing = known.probe_spacing;
+            struct Under {
+                F3 arm, velocity;
+                float share;
+            };
+            std::vector<Under> under;
+            for (auto& pr : probes) {
+                float depth = level - dot(center + pr.first, up);
+                float share = rmin(rmax(depth / spacing + 0.5f, 0.0f), 1.0f);
+                if (share > 0.0f) under.push_back(Under{pr.first, pr.second, share});
+            }
+            float wetted = 0.0f;
+            for (auto& u : under) wetted += u.share;
+            if (wetted <= 0.0f) continue;
+            float volume = wetted * (spacing * spacing * spacing);
+            float density = s.rest_density;
+            F3 middle{0, 0, 0};
+            for (auto& u : under) middle = middle + u.arm * u.share;
+            middle = middle / wetted;
+            F3 force{0, 0, 0}, torque{0, 0, 0};
+            F3 buoyancy = up * (density * grav * volume);
+            force = force + buoyancy;
+            torque = torque + cross(middle, buoyancy);
+            float area = std::pow(volume, 2.0f / 3.0f) / wetted;
+            for (auto& u : under) {
+                F3 past = flow - u.velocity;
+                F3 drag = past * (0.5f * 1.0f * density * area * u.share * length(past));
+                force = force + drag;
+                torque = torque + cross(u.arm, drag);
+            }
+            size_t nline = 0;
+            for (auto& u : under) nline += u.share < 1.0f ? 1 : 0;
+            float plane = float(nline) * spacing * spacing;
+            float waves = density * plane * std::sqrt(grav * std::sqrt(plane));
+            float share = waves / float(std::max<size_t>(nline, 1));
+            for (auto& u : under) {
+                if (!(u.share < 1.0f)) continue;
+                F3 calm = up * (share * dot(flow - u.velocity, up));
+                force = force + calm;
+                torque = torque + cross(u.arm, calm);
+            }
+            out.push_back(Lift{owner, force * dt, torque * dt, std::move(near)});
+        }
+        return out;
+    }
+
+    // couple.rs:219-248 with the rigid world left to the caller
+    int32_t step_with_bodies(float dt, const slf_body_pose* poses, uint64_t npose, slf_report* out,
+                             std::vector<slf_body_push>& pushes) {
+        pushes.clear();
+        if (s.solver != SLF_SOLVER_WCSPH && !coupled.empty())
+            return fail(SLF_ERR_INVALID_SETTINGS, "the divergence free solver does not couple yet");
+        if (!coupled.empty() && fast()) return fail(SLF_ERR_UNSUPPORTED, "coupled bodies run with EXACT arithmetic only");
+        if (tape.on && !coupled.empty()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint takes no coupled bodies");
+        place_movers_at(poses, npose);
+        int32_t st = step(dt, out);
+        // the points are gone for the next step
+        m_start.clear();
+        m_pos.clear();
+        m_vel.clear();
+        m_own.clear();
+        mgrid = GridDev{};
+        SLF_TRY(st);
+        for (auto& known : coupled) {
+            slf_body_push p{};
+            p.body = known.body;
+            pushes.push_back(p);
+        }
+        if (!(dt > 0.0f) || coupled.empty()) return SLF_OK;
+        std::vector<F3> P, V;
+        if (n) {
+            std::vector<float> hp(3 * n), hv(3 * n);
+            SLF_TRY(read_state(hp.data(), hv.data(), n));
+            P.resize(n);
+            V.resize(n);
+            for (uint64_t i = 0; i < n; ++i) {
+                P[i] = F3{hp[3 * i], hp[3 * i + 1], hp[3 * i + 2]};
+                V[i] = F3{hv[3 * i], hv[3 * i + 1], hv[3 * i + 2]};
+            }
+        }
+        auto put = [](float* d, F3 v) {
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+        };
+        bool gave = false;
+        for (const Lift& lift : lifts(dt, poses, npose, P, V)) {
+            slf_body_push& p = pushes[lift.owner];
+            put(p.lift, lift.impulse);
+            put(p.lift_angular, lift.angular);
+            if (pose_of(poses, npose, coupled[lift.owner].body)->dynamic) {
+                // lift.rs:160-166: the water read for the lift loses what the body got
+                F3 change = lift.impulse / (mass * float(lift.near.size()));
+                for (uint32_t i : lift.near) V[i] = V[i] - change;
+                p.lifted = 1;
+                gave = true;
+            }
+        }
+        for (size_t b = 0; b < coupled.size(); ++b) {
+            put(pushes[b].damping, coupled[b].impulse);
+            put(pushes[b].damping_angular, coupled[b].angular);
+            coupled[b].impulse = coupled[b].angular = F3{0, 0, 0};
+        }
+        if (gave) {
+            std::vector<float> hv(3 * n);
+            for (uint64_t i = 0; i < n; ++i) {
+                hv[3 * i] = V[i].x;
+                hv[3 * i + 1] = V[i].y;
+                hv[3 * i + 2] = V[i].z;
+            }
+            SLF_TRY(write_vec(vel[cpos], hv.data(), n));
+            SLF_TRY(sync());
+            stats_fresh = false;
+        }
+        return SLF_OK;
     }
 
     // ---- walls (src/fluid/boundary.rs) -------------------------------------------------------
@@ -1074,6 +1577,69 @@ struct World {
         walls_dirty = true;
     }
 
+    // The cell table of points sorted by cell (keys in order, m = keys.size()): dense over their
+    // box while it holds at most 64 cells per occupied one plus 4096 (mod.rs:214-216), else the
+    // occupied cells for search; uploaded into dstart / dkeys, described by g.
+    int32_t grid_from_keys(const std::vector<Key3>& keys, GridDev& g, DevBuf<uint32_t>& dstart, DevBuf<int4>& dkeys) {
+        g = GridDev{};
+        size_t m = keys.size();
+        if (m == 0) return SLF_OK;
+        std::vector<Key3> cells;
+        std::vector<uint32_t> starts;
+        for (size_t i = 0; i < m; ++i)
+            if (i == 0 || !(keys[i] == keys[i - 1])) {
+                cells.push_back(keys[i]);
+                starts.push_back(uint32_t(i));
+            }
+        starts.push_back(uint32_t(m));
+        Key3 lo = cells[0], hi = cells[0];
+        for (auto& c : cells) {
+            lo = Key3{std::min(lo.x, c.x), std::min(lo.y, c.y), std::min(lo.z, c.z)};
+            hi = Key3{std::max(hi.x, c.x), std::max(hi.y, c.y), std::max(hi.z, c.z)};
+        }
+        int64_t sx = int64_t(hi.x) - lo.x + 1, sy = int64_t(hi.y) - lo.y + 1, sz = int64_t(hi.z) - lo.z + 1;
+        __int128 vol = (__int128)sx * sy * sz;
+        if (vol <= (__int128)64 * (__int128)cells.size() + 4096 && vol < (__int128)(1u << 30)) {
+            size_t volume = size_t(vol);
+            std::vector<uint32_t> start(volume + 1, 0);
+            // cells are in key order, which is the dense table's x-major order
+            size_t c = 0;
+            for (size_t at = 0; at < volume; ++at) {
+                start[at] = c < cells.size() ? starts[c] : uint32_t(m);
+                if (c < cells.size()) {
+                    const Key3& k = cells[c];
+                    size_t lin = size_t(((int64_t(k.x) - lo.x) * sy + (int64_t(k.y) - lo.y)) * sz + (int64_t(k.z) - lo.z));
+                    if (lin == at) ++c;
+                }
+            }
+            start[volume] = uint32_t(m);
+            SLF_TRY(dstart.ensure(volume + 1, 0, stream));
+            SLF_CUDA(cudaMemcpyAsync(dstart.p, start.data(), (volume + 1) * 4, cudaMemcpyHostToDevice, stream));
+            g.mode = 1;
+            g.lx = lo.x;
+            g.ly = lo.y;
+            g.lz = lo.z;
+            g.sx = int(sx);
+            g.sy = int(sy);
+            g.sz = int(sz);
+            g.start = dstart.p;
+            SLF_CUDA(cudaStreamSynchronize(stream));
+        } else {
+            std::vector<int4> k4(cells.size());
+            for (size_t i = 0; i < cells.size(); ++i) k4[i] = make_int4(cells[i].x, cells[i].y, cells[i].z, 0);
+            SLF_TRY(dkeys.ensure(cells.size(), 0, stream));
+            SLF_TRY(dstart.ensure(starts.size(), 0, stream));
+            SLF_CUDA(cudaMemcpyAsync(dkeys.p, k4.data(), k4.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
+            SLF_CUDA(cudaMemcpyAsync(dstart.p, starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, stream));
+            SLF_CUDA(cudaStreamSynchronize(stream));
+            g.mode = 2;
+            g.cells = uint32_t(cells.size());
+            g.keys = dkeys.p;
+            g.start = dstart.p;
+        }
+        return SLF_OK;
+    }
+
     // Uploads the walls and their cell table: dense over the walls' box while it holds at most 64
     // cells per occupied one plus 4096 (mod.rs:214-216), else the occupied cells for search.
     int32_t upload_walls() {
@@ -1097,61 +1663,9 @@ struct World {
                 w[i] = make_float4(wpos[i].x, wpos[i].y, wpos[i].z, 0.0f);
             }
         }
-        std::vector<Key3> cells;
-        std::vector<uint32_t> starts;
-        for (size_t i = 0; i < m; ++i)
-            if (i == 0 || !(keys[i] == keys[i - 1])) {
-                cells.push_back(keys[i]);
-                starts.push_back(uint32_t(i));
-            }
-        starts.push_back(uint32_t(m));
-        Key3 lo = cells[0], hi = cells[0];
-        for (auto& c : cells) {
-            lo = Key3{std::min(lo.x, c.x), std::min(lo.y, c.y), std::min(lo.z, c.z)};
-            hi = Key3{std::max(hi.x, c.x), std::max(hi.y, c.y), std::max(hi.z, c.z)};
-        }
-        int64_t sx = int64_t(hi.x) - lo.x + 1, sy = int64_t(hi.y) - lo.y + 1, sz = int64_t(hi.z) - lo.z + 1;
-        __int128 vol = (__int128)sx * sy * sz;
         SLF_TRY(dwalls.ensure(m, 0, stream));
         SLF_CUDA(cudaMemcpyAsync(dwalls.p, w.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream));
-        if (vol <= (__int128)64 * (__int128)cells.size() + 4096 && vol < (__int128)(1u << 30)) {
-            size_t volume = size_t(vol);
-            std::vector<uint32_t> start(volume + 1, 0);
-            // cells are in key order, which is the dense table's x-major order
-            size_t c = 0;
-            for (size_t at = 0; at < volume; ++at) {
-                start[at] = c < cells.size() ? starts[c] : uint32_t(m);
-                if (c < cells.size()) {
-                    const Key3& k = cells[c];
-                    size_t lin = size_t(((int64_t(k.x) - lo.x) * sy + (int64_t(k.y) - lo.y)) * sz + (int64_t(k.z) - lo.z));
-                    if (lin == at) ++c;
-                }
-            }
-            start[volume] = uint32_t(m);
-            SLF_TRY(dwstart.ensure(volume + 1, 0, stream));
-            SLF_CUDA(cudaMemcpyAsync(dwstart.p, start.data(), (volume + 1) * 4, cudaMemcpyHostToDevice, stream));
-            wgrid.mode = 1;
-            wgrid.lx = lo.x;
-            wgrid.ly = lo.y;
-            wgrid.lz = lo.z;
-            wgrid.sx = int(sx);
-            wgrid.sy = int(sy);
-            wgrid.sz = int(sz);
-            wgrid.start = dwstart.p;
-            SLF_CUDA(cudaStreamSynchronize(stream));
-        } else {
-            std::vector<int4> k4(cells.size());
-            for (size_t i = 0; i < cells.size(); ++i) k4[i] = make_int4(cells[i].x, cells[i].y, cells[i].z, 0);
-            SLF_TRY(dwkeys.ensure(cells.size(), 0, stream));
-            SLF_TRY(dwstart.ensure(starts.size(), 0, stream));
-            SLF_CUDA(cudaMemcpyAsync(dwkeys.p, k4.data(), k4.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
-            SLF_CUDA(cudaMemcpyAsync(dwstart.p, starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, stream));
-            SLF_CUDA(cudaStreamSynchronize(stream));
-            wgrid.mode = 2;
-            wgrid.cells = uint32_t(cells.size());
-            wgrid.keys = dwkeys.p;
-            wgrid.start = dwstart.p;
-        }
+        SLF_TRY(grid_from_keys(keys, wgrid, dwstart, dwkeys));
         walls_dirty = false;
         return SLF_OK;
     }
@@ -1320,6 +1834,7 @@ struct World {
         SLF_TRY(read_status());
         SLF_TRY(lists_fit());
         SLF_TRY(check_state());
+        SLF_TRY(mover_felt(dt, p, a, nid));
         held = h_status->held;
         cpos = b;
         cid = nid;
@@ -2002,9 +2517,18 @@ struct World {
             SLF_TRY(ensure_work_buffers());
             SLF_TRY(refresh_stats());
             if (s.solver == SLF_SOLVER_WCSPH) {
-                // wcsph (step.rs:102-142), no coupled bodies
+                // wcsph (step.rs:102-142): the step's sound speed follows the fastest coupled body
+                // near the water, its points sweep on through the substeps
+                float configured = s.sound_speed, mover = 0.0f;
+                SLF_TRY(fastest_near_water(dt, configured / 4.0f, mover));
+                struct Restore {
+                    float& to;
+                    float value;
+                    ~Restore() { to = value; }
+                } restore{s.sound_speed, configured};
+                s.sound_speed = rmax(configured, 4.0f * mover);
                 r.sound_speed = s.sound_speed;
-                float fast = fastest();
+                float fast = rmax(fastest(), mover);
                 float largest = s.courant * radius / (s.sound_speed + fast);
                 float wanted = rmax(std::ceil(dt / largest), 1.0f);
                 float cap = float(s.max_substeps);
@@ -2015,6 +2539,7 @@ struct World {
                     uint32_t held = 0;
                     if (tape_step) tape_step->push_back(small);
                     if (tape_step && tape.every == 0) SLF_TRY(record_begin(small));
+                    if (!coupled.empty()) SLF_TRY(carry_movers(small * float(i)));
                     int32_t st = wcsph_substep(small, held);
                     if (st == kRetry) st = wcsph_substep(small, held);
                     if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
@@ -2287,7 +2812,17 @@ struct World {
             }
         }
         w.u32(flow_next);
-        w.len(0);  // coupled bodies
+        // Coupled::save (couple.rs:50-55)
+        w.len(coupled.size());
+        for (const Coupled& c : coupled) {
+            w.u32(uint32_t(c.body >> 32));
+            w.u32(uint32_t(c.body & 0xffffffffu));
+            w.len(c.points.size());
+            for (const F3& q : c.points) w.vec3(q.x, q.y, q.z);
+            w.f32(c.probe_spacing);
+            w.len(c.probes.size());
+            for (const F3& q : c.probes) w.vec3(q.x, q.y, q.z);
+        }
         // TerrainField::save (terrain.rs:44-55)
         w.len(terrains.size());
         for (const TerrainHost& t : terrains) {
@@ -2419,9 +2954,44 @@ struct World {
         SLF_TRY(rd(r.u32(fnext)));
         for (auto& fl : lf)
             if (fl.id >= fnext) return bad("invalid snapshot: fluid flow id");
-        size_t coupled = 0, nterrain = 0;
-        SLF_TRY(rd(r.count(12, kMaxSnapshotParts, coupled)));
-        if (coupled) return fail(SLF_ERR_UNSUPPORTED, "coupled bodies are not on this path");
+        size_t ncoupled = 0, nterrain = 0;
+        SLF_TRY(rd(r.count(12, kMaxSnapshotParts, ncoupled)));
+        // Coupled::load (couple.rs:58-75), load_points (couple.rs:435-451)
+        std::vector<Coupled> lcoupled;
+        uint64_t room = st.max_particles;
+        auto points = [&](uint64_t max, std::vector<F3>& out) -> int32_t {
+            size_t count = 0;
+            SLF_TRY(rd(r.count(12, size_t(std::min<uint64_t>(max, SIZE_MAX)), count)));
+            for (size_t k = 0; k < count; ++k) {
+                F3 q;
+                SLF_TRY(rd(r.vec3(q)));
+                if (!finite3f(q)) return bad("invalid snapshot: fluid body point");
+                out.push_back(q);
+            }
+            if (out.empty()) return bad("invalid snapshot: fluid body");
+            return SLF_OK;
+        };
+        for (size_t k = 0; k < ncoupled; ++k) {
+            Coupled c;
+            uint32_t index = 0, generation = 0;
+            SLF_TRY(rd(r.u32(index) && r.u32(generation)));
+            c.body = (uint64_t(index) << 32) | generation;
+            SLF_TRY(points(room, c.points));
+            if (version >= 3) {
+                float ps = 0.0f;
+                SLF_TRY(rd(r.f32(ps)));
+                if (!std::isfinite(ps) || ps <= 0.0f) return bad("invalid snapshot: fluid body probes");
+                c.probe_spacing = ps;
+                SLF_TRY(points(kMaxProbes, c.probes));
+            } else {
+                c.probe_spacing = st.spacing;
+                c.probes = c.points;
+            }
+            room -= c.points.size();
+            lcoupled.push_back(std::move(c));
+        }
+        for (size_t k = 1; k < lcoupled.size(); ++k)
+            if (lcoupled[k - 1].body >= lcoupled[k].body) return bad("invalid snapshot: fluid body order");
         SLF_TRY(rd(r.count(32, kMaxSnapshotParts, nterrain)));
         // TerrainField::load (terrain.rs:57-97)
         std::vector<TerrainHost> lt(nterrain);
@@ -2477,6 +3047,7 @@ struct World {
         if (!lt.empty() && fast()) return fail(SLF_ERR_UNSUPPORTED, "terrain runs with EXACT arithmetic only");
         terrains = std::move(lt);
         terrain_dirty = true;
+        coupled = std::move(lcoupled);
         has_domain = dom;
         dlow = dl;
         dhigh = dh;
@@ -2878,6 +3449,43 @@ int32_t slf_remove_flow(slf_world* world, uint32_t flow, int32_t* removed) {
     bool r = world->w.remove_flow(flow);
     if (removed) *removed = r ? 1 : 0;
     return SLF_OK;
+}
+
+int32_t slf_couple(slf_world* world, uint64_t body, int32_t shape, const float dims[3]) {
+    SLF_WORLD(world);
+    SLF_NEED(dims);
+    return world->w.couple(body, shape, dims);
+}
+
+int32_t slf_uncouple(slf_world* world, uint64_t body, int32_t* removed) {
+    SLF_WORLD(world);
+    bool r = world->w.uncouple(body);
+    if (removed) *removed = r ? 1 : 0;
+    return SLF_OK;
+}
+
+int32_t slf_coupled(const slf_world* world, uint64_t* bodies, uint32_t* points, uint32_t* probes, uint64_t capacity,
+                    uint64_t* count) {
+    SLF_WORLD(world);
+    const auto& c = world->w.coupled;
+    if (count) *count = c.size();
+    for (size_t k = 0; k < c.size() && k < capacity; ++k) {
+        if (bodies) bodies[k] = c[k].body;
+        if (points) points[k] = uint32_t(c[k].points.size());
+        if (probes) probes[k] = uint32_t(c[k].probes.size());
+    }
+    return SLF_OK;
+}
+
+int32_t slf_step_with_bodies(slf_world* world, float dt, const slf_body_pose* poses, uint64_t npose, slf_report* out,
+                             slf_body_push* pushes, uint64_t capacity, uint64_t* count) {
+    SLF_WORLD(world);
+    if (npose) SLF_NEED(poses);
+    std::vector<slf_body_push> got;
+    int32_t st = world->w.step_with_bodies(dt, poses, npose, out, got);
+    if (count) *count = got.size();
+    for (size_t k = 0; k < got.size() && k < capacity && pushes; ++k) pushes[k] = got[k];
+    return st;
 }
 
 int32_t slf_wall_count(const slf_world* world, uint64_t* out) {

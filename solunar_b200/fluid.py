@@ -12,7 +12,8 @@ import os
 
 import numpy as np
 
-from .abi import CParamGrads, CProfileEntry, CReport, CSettings, FluidReport, FluidSettings, PhysicsError, vec3
+from .abi import (CBodyPose, CBodyPush, CParamGrads, CProfileEntry, CReport, CSettings, FluidReport, FluidSettings,
+                  PhysicsError, step_with_bodies_call, vec3)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_NAME = "libsolunar_fluid.so"
@@ -61,6 +62,11 @@ def load_library():
                               ctypes.POINTER(vp)],
         "slf_add_drain": [vp, fp, fp, u32p],
         "slf_remove_flow": [vp, ctypes.c_uint32, i32p],
+        "slf_couple": [vp, ctypes.c_uint64, ctypes.c_int32, fp],
+        "slf_uncouple": [vp, ctypes.c_uint64, i32p],
+        "slf_coupled": [vp, u64p, u32p, u32p, ctypes.c_uint64, u64p],
+        "slf_step_with_bodies": [vp, ctypes.c_float, ctypes.POINTER(CBodyPose), ctypes.c_uint64,
+                                 ctypes.POINTER(CReport), ctypes.POINTER(CBodyPush), ctypes.c_uint64, u64p],
         "slf_wall_count": [vp, u64p],
         "slf_read_wall_positions": [vp, fp, ctypes.c_uint64],
         "slf_step": [vp, ctypes.c_float, ctypes.POINTER(CReport)],
@@ -263,6 +269,31 @@ class FluidWorld:
         r = ctypes.c_int32()
         _check(_lib.slf_remove_flow(self._h, flow, ctypes.byref(r)))
         return bool(r.value)
+
+    def couple(self, body: int, shape, dims):
+        """FluidWorld::couple (couple.rs:165-200): body = index << 32 | generation, shape a
+        `Shape`, dims its half extents, (radius,) or (radius, half height)."""
+        d = list(dims) + [0.0] * (3 - len(dims))
+        _check(_lib.slf_couple(self._h, body, int(shape), vec3(d)))
+
+    def uncouple(self, body: int) -> bool:
+        r = ctypes.c_int32()
+        _check(_lib.slf_uncouple(self._h, body, ctypes.byref(r)))
+        return bool(r.value)
+
+    def coupled(self):
+        """[(body, points, probes)] in body order."""
+        n = ctypes.c_uint64()
+        _check(_lib.slf_coupled(self._h, None, None, None, 0, ctypes.byref(n)))
+        k = n.value
+        b, p, q = (ctypes.c_uint64 * max(k, 1))(), (ctypes.c_uint32 * max(k, 1))(), (ctypes.c_uint32 * max(k, 1))()
+        _check(_lib.slf_coupled(self._h, b, p, q, k, ctypes.byref(n)))
+        return [(int(b[i]), int(p[i]), int(q[i])) for i in range(k)]
+
+    def step_with_bodies(self, dt: float, poses):
+        """FluidWorld::step_with_bodies (couple.rs:219-248) with the bodies where `poses` (a
+        list of BodyPose) puts them: (report, [BodyPush])."""
+        return step_with_bodies_call(_lib.slf_step_with_bodies, self._h, dt, list(poses), _check)
 
     def wall_positions(self) -> np.ndarray:
         n = ctypes.c_uint64()
