@@ -668,10 +668,29 @@ __device__ __forceinline__ void mover_pairs(const Params& p, const MoverDev& M, 
 // force and its torque about the body's centre (couple.rs:401-414, step.rs:173-221).  Pairs
 // below the settling speed give nothing.  centre[b] = centre + moved; felt[c * bodies + b] =
 // (force, torque).
+// Which particles have a pair with a body point that passes the settling test (flag[i] = 1):
+// most have none, and the chunk walk below recomputes only those that do.
+__global__ void k_mover_flags(Params p, const StepConsts* __restrict__ sc, MoverDev M, const float4* __restrict__ pos,
+                              const float4* __restrict__ vel, const float* __restrict__ rho,
+                              uint8_t* __restrict__ flag) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float4 a = pos[i], v = vel[i];
+    uint8_t any = 0;
+    mover_pairs(p, M, sc->mover_damping, a, v, rho[i], 0.0f,
+                [&](uint32_t j, float, float, float, float, float, float toward) {
+                    float4 q = __ldg(&M.pos[j]);
+                    float ox = a.x - q.x, oy = a.y - q.y, oz = a.z - q.z;
+                    if (!(toward * toward < p.settles * dot3(ox, oy, oz, ox, oy, oz))) any = 1;
+                });
+    flag[i] = any;
+}
+
 __global__ void k_mover_felt(Params p, const StepConsts* __restrict__ sc, MoverDev M, const float4* __restrict__ pos,
                              const float4* __restrict__ vel, const float* __restrict__ rho,
                              const float* __restrict__ press, const float* __restrict__ scaled,
-                             const float4* __restrict__ centre, uint32_t bodies, float4* __restrict__ felt) {
+                             const float4* __restrict__ centre, uint32_t bodies, const uint8_t* __restrict__ flag,
+                             float4* __restrict__ felt) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t chunks = (p.n + 511u) / 512u;
     if (t >= chunks * bodies) return;
@@ -680,6 +699,7 @@ __global__ void k_mover_felt(Params p, const StepConsts* __restrict__ sc, MoverD
     float4 o = centre[b];
     uint32_t end = min(p.n, (c + 1u) * 512u);
     for (uint32_t i = c * 512u; i < end; ++i) {
+        if (!flag[i]) continue;
         float4 a = pos[i], v = vel[i];
         float density = rho[i];
         float mirrored = scaled[i] + press[i] / p.rest_sq;
@@ -1236,9 +1256,13 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
 
 void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos, const float4* vel,
                        const float* rho, const float* press, const float* scaled, const float4* centre,
-                       uint32_t bodies, float4* felt, cudaStream_t s) {
+                       uint32_t bodies, uint8_t* flag, float4* felt, cudaStream_t s) {
+    if (!p.n) return;
+    k_mover_flags<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, M, pos, vel, rho, flag);
     uint32_t threads = (p.n + 511u) / 512u * bodies;
-    if (threads) k_mover_felt<<<(threads + 63u) / 64u, 64, 0, s>>>(p, sc, M, pos, vel, rho, press, scaled, centre, bodies, felt);
+    if (threads)
+        k_mover_felt<<<(threads + 63u) / 64u, 64, 0, s>>>(p, sc, M, pos, vel, rho, press, scaled, centre, bodies, flag,
+                                                          felt);
     note_launch();
 }
 

@@ -54,7 +54,7 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
 // holds fluid in the cell box [lo, hi] (*wet set to 1, left alone otherwise)
 void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos, const float4* vel,
                        const float* rho, const float* press, const float* scaled, const float4* centre,
-                       uint32_t bodies, float4* felt, cudaStream_t s);
+                       uint32_t bodies, uint8_t* flag, float4* felt, cudaStream_t s);
 void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either

@@ -504,6 +504,11 @@ struct World {
             for (auto& r : tape.subs) r->release(stream);
             for (auto& r : spare_records) r->release(stream);
             back.release(stream);
+            for (auto* b : {&dmpos, &dmvel, &dcentre, &dfelt}) b->release(stream);
+            dmstart.release(stream);
+            dwet.release(stream);
+            dmflag.release(stream);
+            dmkeys.release(stream);
             rec_rate.release(stream);
             rec_vel.release(stream);
             dwalls.release(stream);
@@ -974,6 +979,7 @@ struct World {
     std::vector<uint32_t> m_own;
     DevBuf<float4> dmpos, dmvel, dcentre, dfelt;
     DevBuf<uint32_t> dmstart, dwet;
+    DevBuf<uint8_t> dmflag;
     DevBuf<int4> dmkeys;
     GridDev mgrid{};
     std::vector<float4> h_felt;
@@ -1226,9 +1232,10 @@ struct World {
         }
         SLF_TRY(dcentre.ensure(bodies, 0, stream));
         SLF_TRY(dfelt.ensure(2 * chunks * bodies, 0, stream));
+        SLF_TRY(dmflag.ensure(n, 0, stream));
         SLF_CUDA(cudaMemcpyAsync(dcentre.p, centres.data(), bodies * sizeof(float4), cudaMemcpyHostToDevice, stream));
         launch_mover_felt(p, d_consts, mover_dev(), pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dcentre.p,
-                          uint32_t(bodies), dfelt.p, stream);
+                          uint32_t(bodies), dmflag.p, dfelt.p, stream);
         h_felt.resize(2 * chunks * bodies);
         SLF_CUDA(cudaMemcpyAsync(h_felt.data(), dfelt.p, h_felt.size() * sizeof(float4), cudaMemcpyDeviceToHost,
                                  stream));
