@@ -429,6 +429,9 @@ def main():
         e1.record(stream)
         e1.synchronize()
         fwd_ms = e0.elapsed_time(e1)
+        # device memory in use with the tape held (the whole device: this process is its only user)
+        free_b, total_b = torch.cuda.mem_get_info(dev)
+        taped_gb = (total_b - free_b) / 1e9
         dv = loss_grad()
         torch.cuda.synchronize()
         e2 = torch.cuda.Event(enable_timing=True)
@@ -438,6 +441,8 @@ def main():
         e3.record(stream)
         e3.synchronize()
         bwd_ms = e2.elapsed_time(e3)
+        free_b, total_b = torch.cuda.mem_get_info(dev)
+        backward_gb = (total_b - free_b) / 1e9
         world.tape_end()
         adj_all, both_ms = reduce_timing(adj_substeps, fwd_ms + bwd_ms, world_size, dev)
         _, fwd_ms = reduce_timing(adj_substeps, fwd_ms, world_size, dev)
@@ -469,6 +474,8 @@ def main():
                    "ratio_to_plain_substeps": value / (adj_all / (both_ms / 1e3)),
                    "loss": "kinetic energy of the water beyond x = 1 m after the steps",
                    "backward_kernels": {"steps": pk_steps, "substeps": p_sub, "kernels": backward_kernels},
+                   "device_memory_gb": {"taped_forward": taped_gb, "after_backward": backward_gb,
+                                        "device_total": total_b / 1e9},
                    "grad_viscosity": grads["viscosity"], "grad_gravity": list(grads["gravity"]),
                    "grad_uniform_inflow": [float(x) for x in dv0.astype(np.float64).sum(axis=0)]}
 
