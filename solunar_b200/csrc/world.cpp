@@ -2588,11 +2588,18 @@ struct World {
                 }
             }
         }
+        // the last substep's status holds the committed state's fastest speed (its advance) and
+        // largest compression (its density pass): the report's maxima unless flows or the domain
+        // change the particles next
+        bool settled_report = n > 0 && r.substeps > 0 && flows.empty() && !has_domain && stats_fresh;
         // run_flows (step.rs:76-81), then keep_in_domain (mod.rs:451-486)
         SLF_TRY(run_flows(r.emitted, r.drained));
         SLF_TRY(keep_in_domain(r.lost));
         // max_speed and max_compression of what is left (step.rs:83-88)
-        if (n > 0) {
+        if (settled_report) {
+            std::memcpy(&r.max_speed, &h_status->vmax_bits, 4);
+            std::memcpy(&r.max_compression, &h_status->maxcomp_bits, 4);
+        } else if (n > 0) {
             SLF_TRY(reset_status());
             Params p = params();
             timed("stats", bytes_per_particle::stats, [&] {
