@@ -668,57 +668,61 @@ __device__ __forceinline__ void mover_pairs(const Params& p, const MoverDev& M, 
 // force and its torque about the body's centre (couple.rs:401-414, step.rs:173-221).  Pairs
 // below the settling speed give nothing.  centre[b] = centre + moved; felt[c * bodies + b] =
 // (force, torque).
-// Which particles have a pair with a body point that passes the settling test (flag[i] = 1):
-// most have none, and the chunk walk below recomputes only those that do.
-__global__ void k_mover_flags(Params p, const StepConsts* __restrict__ sc, MoverDev M, const float4* __restrict__ pos,
+// What the body points take (couple.rs:401-414) in three passes that keep the reference's order:
+// each particle counts its pairs above the settling speed, a scan places them, each particle
+// writes its pairs' force and torque about the owner's centre (in pair order) at its place, and
+// one thread per (512-particle chunk, body) adds its body's records over the chunk's range in
+// order (step.rs:173-221: chunk sums, in particle then pair order).
+template <bool WRITE>
+__global__ void k_mover_pairs(Params p, const StepConsts* __restrict__ sc, MoverDev M, const float4* __restrict__ pos,
                               const float4* __restrict__ vel, const float* __restrict__ rho,
-                              uint8_t* __restrict__ flag) {
+                              const float* __restrict__ press, const float* __restrict__ scaled,
+                              const float4* __restrict__ centre, uint32_t* __restrict__ count,
+                              const uint32_t* __restrict__ offset, float4* __restrict__ pair) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     float4 a = pos[i], v = vel[i];
-    uint8_t any = 0;
-    mover_pairs(p, M, sc->mover_damping, a, v, rho[i], 0.0f,
-                [&](uint32_t j, float, float, float, float, float, float toward) {
+    float density = rho[i];
+    float mirrored = scaled[i] + press[i] / p.rest_sq;
+    uint32_t k = WRITE ? offset[i] : 0u;
+    mover_pairs(p, M, sc->mover_damping, a, v, density, mirrored,
+                [&](uint32_t j, float gx, float gy, float gz, float, float damp, float toward) {
                     float4 q = __ldg(&M.pos[j]);
                     float ox = a.x - q.x, oy = a.y - q.y, oz = a.z - q.z;
-                    if (!(toward * toward < p.settles * dot3(ox, oy, oz, ox, oy, oz))) any = 1;
-                });
-    flag[i] = any;
-}
-
-__global__ void k_mover_felt(Params p, const StepConsts* __restrict__ sc, MoverDev M, const float4* __restrict__ pos,
-                             const float4* __restrict__ vel, const float* __restrict__ rho,
-                             const float* __restrict__ press, const float* __restrict__ scaled,
-                             const float4* __restrict__ centre, uint32_t bodies, const uint8_t* __restrict__ flag,
-                             float4* __restrict__ felt) {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t chunks = (p.n + 511u) / 512u;
-    if (t >= chunks * bodies) return;
-    uint32_t c = t / bodies, b = t % bodies;
-    float fx = 0.0f, fy = 0.0f, fz = 0.0f, tx = 0.0f, ty = 0.0f, tz = 0.0f;
-    float4 o = centre[b];
-    uint32_t end = min(p.n, (c + 1u) * 512u);
-    for (uint32_t i = c * 512u; i < end; ++i) {
-        if (!flag[i]) continue;
-        float4 a = pos[i], v = vel[i];
-        float density = rho[i];
-        float mirrored = scaled[i] + press[i] / p.rest_sq;
-        mover_pairs(p, M, sc->mover_damping, a, v, density, mirrored,
-                    [&](uint32_t j, float gx, float gy, float gz, float, float damp, float toward) {
-                        float4 q = __ldg(&M.pos[j]);
-                        if (__float_as_uint(q.w) != b) return;
-                        float ox = a.x - q.x, oy = a.y - q.y, oz = a.z - q.z;
-                        if (toward * toward < p.settles * dot3(ox, oy, oz, ox, oy, oz)) return;
+                    if (toward * toward < p.settles * dot3(ox, oy, oz, ox, oy, oz)) return;
+                    if (WRITE) {
+                        uint32_t b = __float_as_uint(q.w);
+                        float4 o = centre[b];
                         float s = damp * p.mass;
                         float ex = gx * s, ey = gy * s, ez = gz * s;
                         float rx = q.x - o.x, ry = q.y - o.y, rz = q.z - o.z;
-                        fx = fx + ex;
-                        fy = fy + ey;
-                        fz = fz + ez;
-                        tx = tx + (ry * ez - ey * rz);
-                        ty = ty + (rz * ex - ez * rx);
-                        tz = tz + (rx * ey - ex * ry);
-                    });
+                        pair[2 * size_t(k)] = make_float4(ex, ey, ez, q.w);
+                        pair[2 * size_t(k) + 1] =
+                            make_float4(ry * ez - ey * rz, rz * ex - ez * rx, rx * ey - ex * ry, 0.0f);
+                    }
+                    ++k;
+                });
+    if (!WRITE) count[i] = k;
+}
+
+__global__ void k_mover_felt(uint32_t n, uint32_t bodies, const uint32_t* __restrict__ offset,
+                             const float4* __restrict__ pair, float4* __restrict__ felt) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t chunks = (n + 511u) / 512u;
+    if (t >= chunks * bodies) return;
+    uint32_t c = t / bodies, b = t % bodies;
+    uint32_t from = offset[c * 512u], to = offset[min(n, (c + 1u) * 512u)];
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f, tx = 0.0f, ty = 0.0f, tz = 0.0f;
+    for (uint32_t k = from; k < to; ++k) {
+        float4 f = pair[2 * size_t(k)];
+        if (__float_as_uint(f.w) != b) continue;
+        float4 q = pair[2 * size_t(k) + 1];
+        fx = fx + f.x;
+        fy = fy + f.y;
+        fz = fz + f.z;
+        tx = tx + q.x;
+        ty = ty + q.y;
+        tz = tz + q.z;
     }
     felt[2 * size_t(t)] = make_float4(fx, fy, fz, 0.0f);
     felt[2 * size_t(t) + 1] = make_float4(tx, ty, tz, 0.0f);
@@ -1254,15 +1258,22 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
                                                          vel_out, st, vel_pre, T, slope, M);
 }
 
+void launch_mover_count(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos,
+                        const float4* vel, const float* rho, const float* press, const float* scaled,
+                        uint32_t* count, cudaStream_t s) {
+    if (p.n)
+        k_mover_pairs<false><<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, M, pos, vel, rho, press, scaled, nullptr, count,
+                                                                nullptr, nullptr);
+}
+
 void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos, const float4* vel,
                        const float* rho, const float* press, const float* scaled, const float4* centre,
-                       uint32_t bodies, uint8_t* flag, float4* felt, cudaStream_t s) {
+                       uint32_t bodies, const uint32_t* offset, float4* pair, float4* felt, cudaStream_t s) {
     if (!p.n) return;
-    k_mover_flags<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, M, pos, vel, rho, flag);
+    k_mover_pairs<true><<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, M, pos, vel, rho, press, scaled, centre, nullptr,
+                                                           offset, pair);
     uint32_t threads = (p.n + 511u) / 512u * bodies;
-    if (threads)
-        k_mover_felt<<<(threads + 63u) / 64u, 64, 0, s>>>(p, sc, M, pos, vel, rho, press, scaled, centre, bodies, flag,
-                                                          felt);
+    if (threads) k_mover_felt<<<(threads + 63u) / 64u, 64, 0, s>>>(p.n, bodies, offset, pair, felt);
     note_launch();
 }
 

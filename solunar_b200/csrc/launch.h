@@ -49,12 +49,16 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
                         float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s,
                         const MoverDev& M = MoverDev{});
-// coupled bodies: per (512-particle chunk, body) the damping force and torque the body's points
-// took this substep (felt: chunks x bodies pairs of float4); and whether the last sort's table
-// holds fluid in the cell box [lo, hi] (*wet set to 1, left alone otherwise)
+// coupled bodies: each particle's count of pairs whose damping a body takes (count[i]); then,
+// with their exclusive scan in `offset` (n + 1 entries), the pairs' force and torque records and
+// per (512-particle chunk, body) their sums in order (felt: chunks x bodies pairs of float4); and
+// whether the last sort's table holds fluid in the cell box [lo, hi] (*wet set to 1, else left)
+void launch_mover_count(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos,
+                        const float4* vel, const float* rho, const float* press, const float* scaled,
+                        uint32_t* count, cudaStream_t s);
 void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos, const float4* vel,
                        const float* rho, const float* press, const float* scaled, const float4* centre,
-                       uint32_t bodies, uint8_t* flag, float4* felt, cudaStream_t s);
+                       uint32_t bodies, const uint32_t* offset, float4* pair, float4* felt, cudaStream_t s);
 void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either

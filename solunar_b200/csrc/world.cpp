@@ -507,7 +507,9 @@ struct World {
             for (auto* b : {&dmpos, &dmvel, &dcentre, &dfelt}) b->release(stream);
             dmstart.release(stream);
             dwet.release(stream);
-            dmflag.release(stream);
+            dmcount.release(stream);
+            dmtiles.release(stream);
+            dmpair.release(stream);
             dmkeys.release(stream);
             rec_rate.release(stream);
             rec_vel.release(stream);
@@ -979,7 +981,8 @@ struct World {
     std::vector<uint32_t> m_own;
     DevBuf<float4> dmpos, dmvel, dcentre, dfelt;
     DevBuf<uint32_t> dmstart, dwet;
-    DevBuf<uint8_t> dmflag;
+    DevBuf<uint32_t> dmcount, dmtiles;
+    DevBuf<float4> dmpair;
     DevBuf<int4> dmkeys;
     GridDev mgrid{};
     std::vector<float4> h_felt;
@@ -1232,10 +1235,18 @@ struct World {
         }
         SLF_TRY(dcentre.ensure(bodies, 0, stream));
         SLF_TRY(dfelt.ensure(2 * chunks * bodies, 0, stream));
-        SLF_TRY(dmflag.ensure(n, 0, stream));
+        SLF_TRY(dmcount.ensure(n + 1, 0, stream));
+        SLF_TRY(dmtiles.ensure(scan_tiles(uint32_t(n)) + 1, 0, stream));
         SLF_CUDA(cudaMemcpyAsync(dcentre.p, centres.data(), bodies * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        launch_mover_count(p, d_consts, mover_dev(), pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dmcount.p,
+                           stream);
+        launch_exclusive_scan(dmcount.p, uint32_t(n), dmtiles.p, stream);
+        uint32_t total = 0;
+        SLF_CUDA(cudaMemcpyAsync(&total, dmcount.p + n, 4, cudaMemcpyDeviceToHost, stream));
+        SLF_TRY(sync());
+        SLF_TRY(dmpair.ensure(2 * size_t(std::max<uint32_t>(total, 1)), 0, stream));
         launch_mover_felt(p, d_consts, mover_dev(), pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dcentre.p,
-                          uint32_t(bodies), dmflag.p, dfelt.p, stream);
+                          uint32_t(bodies), dmcount.p, dmpair.p, dfelt.p, stream);
         h_felt.resize(2 * chunks * bodies);
         SLF_CUDA(cudaMemcpyAsync(h_felt.data(), dfelt.p, h_felt.size() * sizeof(float4), cudaMemcpyDeviceToHost,
                                  stream));
