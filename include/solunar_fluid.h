@@ -36,7 +36,8 @@ enum {
     SLF_ERR_OUT_OF_RANGE = 3,        /* PhysicsError::OutOfRange (src/error.rs:14) */
     SLF_ERR_FLUID_FULL = 4,          /* PhysicsError::FluidFull (src/error.rs:21) */
     SLF_ERR_DISPATCH_INCOMPLETE = 5, /* PhysicsError::DispatchIncomplete (src/error.rs:15) */
-    SLF_ERR_UNSUPPORTED = 6,         /* a feature off the fluid step (movers, terrain) */
+    SLF_ERR_UNSUPPORTED = 6,         /* a combination not built: FAST arithmetic with terrain or bodies,
+                                      * cell-relative positions or a tape with them, shallow water */
     SLF_ERR_CUDA = 7,                /* a CUDA call failed; see slf_last_error() */
     SLF_ERR_TIMEOUT = 8,             /* a bounded device loop gave up */
     SLF_ERR_INVALID_ARGUMENT = 9,    /* null pointer or wrong buffer size */
