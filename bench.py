@@ -6,9 +6,10 @@ Workload: the one-million-particle DFSPH dam break (100^3 particles at 0.01 m, s
 which takes as many DFSPH substeps as the flow needs.  A timed step is one such call; `value`
 is substeps per second over all ranks, device-timed with CUDA events on the world's stream,
 with the particle state resident in HBM and L2 flushed (a 256 MiB write) before each step.
-Each DFSPH solve runs as one CUDA graph whose loop the device ends; the per-kernel times of the
-roofline come from a second pass of the same steps with every launch timed by CUDA events (the
-profiler runs the solves launch by launch).
+Each DFSPH substep runs as one CUDA graph launch (sort, density, both solves with loops the
+device ends, viscosity, advance), recorded the second time its launches recur; the per-kernel
+times of the roofline come from a second pass of the same steps with every launch timed by CUDA
+events (the profiler runs the substep launch by launch).
 `e2e` is the same metric through the C ABI with host-owned state: each step uploads positions
 and velocities from pinned host memory, steps, and reads them back.
 
@@ -35,6 +36,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "1M-particle DFSPH substeps/s: plain vs fwd+adjoint, 0.1% density err, 1 B200"
 UNIT = "substeps/s"
+GRAPH_MODES = {0: "launch by launch, host-checked batches",
+               1: "one CUDA graph per solve, loop ended on the device",
+               2: "one CUDA graph per substep (sort, density, solves with device-ended loops, viscosity, advance)"}
 FLUSH_BYTES = 256 << 20
 
 
@@ -57,6 +61,8 @@ def parse():
                     help="timed steps of the opt-in warm-started leg on its own world, after the same "
                          "warm-up (default: --steps, the cold run's window; 0 skips it)")
     ap.add_argument("--no-graphs", action="store_true", help="queue the solves in host-checked batches")
+    ap.add_argument("--graph-mode", type=int, default=2, choices=(0, 1, 2),
+                    help="2 each substep one CUDA graph, 1 each solve one graph, 0 as --no-graphs")
     ap.add_argument("--adjoint-every", type=int, default=0,
                     help="tape checkpoint spacing of the forward+adjoint leg; 0 records every substep")
     ap.add_argument("--adjoint-steps", type=int, default=32,
@@ -269,6 +275,7 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world_size)
         return
+    graph_mode = 0 if args.no_graphs else args.graph_mode
 
     import torch
     import torch.distributed as dist
@@ -291,7 +298,7 @@ def main():
     sc = scene_of(args.scene, args.arithmetic, args.positions)
     sc.settings.device = local_rank
     world = fluid.FluidWorld(sc.settings)
-    world.solver_graphs(not args.no_graphs)
+    world.solver_graphs(graph_mode)
     sc.build(world)
     world.update_neighbors()
     stream = torch.cuda.ExternalStream(world.stream(), device=dev)
@@ -303,6 +310,7 @@ def main():
     clocks = Clocks(local_rank)
     clocks.start()
     launches0 = fluid.kernel_launches()
+    graphed0 = world.graph_substeps()
     barrier()
     times_ms = []
     substeps = iterations = 0
@@ -320,6 +328,7 @@ def main():
         iterations += r.iterations
     barrier()
     launches = fluid.kernel_launches() - launches0
+    graphed = world.graph_substeps() - graphed0
     clock_info = clocks.stop()
 
     all_substeps, total_ms = reduce_timing(substeps, sum(times_ms), world_size, dev)
@@ -489,7 +498,7 @@ def main():
 
         wsc = dataclasses.replace(sc, settings=dataclasses.replace(sc.settings, warm_start=True))
         ww = fluid.FluidWorld(wsc.settings)
-        ww.solver_graphs(not args.no_graphs)
+        ww.solver_graphs(graph_mode)
         wsc.build(ww)
         wstream = torch.cuda.ExternalStream(ww.stream(), device=dev)
         for _ in range(max(args.warmup, 3)):
@@ -529,8 +538,7 @@ def main():
                "config": dict(workload(sc), parallelism=f"replicas x{world_size}",
                               substeps=substeps, solver_iterations_per_substep=iterations / max(substeps, 1),
                               particle_substeps_per_s=value * sc.particles,
-                              solves="launch by launch, host-checked batches" if args.no_graphs
-                              else "one CUDA graph per solve, loop ended on the device"),
+                              solves=GRAPH_MODES[graph_mode], substeps_as_one_graph=graphed),
                "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "forward_adjoint": adjoint,
                "warm_start": warm,
                "clocks": clock_info, "gpu_launches": launches}

@@ -368,11 +368,18 @@ int32_t slf_profile_reset(slf_world* world);
  * the kernels its loop ran). */
 int32_t slf_kernel_launches(uint64_t* out);
 
-/* on = 1 (the default): each DFSPH solve of a step without a tape or profile runs as one CUDA
- * graph launch whose loop the device ends, and the host waits once a substep.  on = 0: the
- * solves' launches are queued in batches with a host check between them.  Results are the
- * same bit for bit; the profiler and recorded solves always take the batched launches. */
-int32_t slf_solver_graphs(slf_world* world, int32_t on);
+/* How a DFSPH step without a tape or profile launches its work.  mode = 2 (the default): each
+ * substep is one CUDA graph launch (sort, density, both solves with loops the device ends,
+ * viscosity, advance), recorded the second time the same launches recur and cached; substeps
+ * the cache does not hold yet run as in mode 1.  mode = 1: each solve is one graph launch, the
+ * rest is launched eagerly.  mode = 0: the solves' launches are queued in batches with a host
+ * check between them.  In every mode the host waits once a substep and the results are the same
+ * bit for bit; the profiler and recorded solves take the batched launches.  Other modes:
+ * SLF_ERR_INVALID_SETTINGS. */
+int32_t slf_solver_graphs(slf_world* world, int32_t mode);
+
+/* DFSPH substeps this world has run as one whole-substep graph launch (mode 2). */
+int32_t slf_graph_substeps(const slf_world* world, uint64_t* out);
 
 /* DFSPH solver iterations of the last substep: divergence and density (the per-solve split of
  * FluidReport::iterations, src/fluid/dfsph.rs:89,100). */
@@ -382,6 +389,11 @@ int32_t slf_last_iterations(const slf_world* world, uint32_t* divergence, uint32
  * (src/dispatch.rs:50-65): the next sort leaves the 512-particle job `job` undone, which the
  * completeness check reports as SLF_ERR_DISPATCH_INCOMPLETE with the particles untouched. */
 int32_t slf_debug_skip_job(slf_world* world, int64_t job);
+
+/* Test hook: sets the neighbour lists' room to `room` entries a particle (rounded down to a
+ * multiple of 8, at least 8), so that the next substep's lists outgrow it and the substep is run
+ * again with room for its longest list, from the committed state.  Invalidates the lists. */
+int32_t slf_debug_list_room(slf_world* world, uint32_t room);
 
 #ifdef __cplusplus
 }

@@ -392,6 +392,7 @@ struct World {
 
     Status* d_status = nullptr;
     Status* h_status = nullptr;
+    Status* h_reset = nullptr;  // pinned: the status a substep starts from (a graph copies it)
     StepConsts* d_consts = nullptr;
 
     int64_t skip_job = -1;  // testing: next sort leaves this 512-particle job undone
@@ -521,11 +522,13 @@ struct World {
             gslope.release(stream);
             cudaStreamSynchronize(stream);
             drop_solve_graphs();
+            drop_substep_graphs();
             for (auto c : cap)
                 if (c) cudaStreamDestroy(c);
             if (d_status) cudaFree(d_status);
             if (d_consts) cudaFree(d_consts);
             if (h_status) cudaFreeHost(h_status);
+            if (h_reset) cudaFreeHost(h_reset);
             cudaStreamDestroy(stream);
         }
     }
@@ -579,6 +582,8 @@ struct World {
         SLF_CUDA(cudaMalloc(&d_consts, sizeof(StepConsts)));
         SLF_CUDA(cudaMallocHost(&h_status, sizeof(Status)));
         std::memset(h_status, 0, sizeof(Status));
+        SLF_CUDA(cudaMallocHost(&h_reset, sizeof(Status)));
+        *h_reset = fresh_status();
         SLF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(Status), stream));
         build_ground_sites();
         return SLF_OK;
@@ -894,13 +899,16 @@ struct World {
     int4* cells_of(int slot) const { return rel() ? cell[slot].p : nullptr; }
 
     // the pair passes of the settings' arithmetic, over the positions of slot a
-    void density_pass(const Params& p, int a, const PairLists& fl, const PairLists& wl, float* rh) {
+    // (on: the stream of a graph capture; the world's stream when null)
+    void density_pass(const Params& p, int a, const PairLists& fl, const PairLists& wl, float* rh,
+                      cudaStream_t on = nullptr) {
+        if (!on) on = stream;
         if (fast())
             launch_density_fast(p, fgrid, wgrid, pos[a].p, cells_of(a), dwalls.p, fl, wl, rh, press.p, scaled.p,
-                                alpha.p, d_status, stream);
+                                alpha.p, d_status, on);
         else
             launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status,
-                           tdev, ground_slopes(), stream, mover_dev());
+                           tdev, ground_slopes(), on, mover_dev());
     }
     void force_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
         if (fast())
@@ -932,21 +940,24 @@ struct World {
     bool warm_on() const { return s.warm_start && s.solver == SLF_SOLVER_DFSPH; }
     const float2* warm_in() const { return warm_on() ? warm[cid].p : nullptr; }
     float2* warm_out() { return warm_on() ? warm[1 - cid].p : nullptr; }
-    void advance_pass(const Params& p, int a, int b, float4* pre) {
+    void advance_pass(const Params& p, int a, int b, float4* pre, cudaStream_t on = nullptr) {
+        if (!on) on = stream;
         if (rel()) launch_advance_rel(p, d_consts, pos[a].p, cell[a].p, pos[b].p, cell[b].p, vel[b].p, d_status, pre,
-                                      stream);
-        else launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, pre, stream);
+                                      on);
+        else launch_advance(p, d_consts, pos[a].p, pos[b].p, vel[b].p, d_status, pre, on);
     }
     void stats_pass(const Params& p) {
         if (rel()) launch_state_stats_rel(p, cell[cpos].p, vel[cpos].p, d_status, stream);
         else launch_state_stats(p, pos[cpos].p, vel[cpos].p, d_status, stream);
     }
-    void viscous_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
+    void viscous_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid,
+                      cudaStream_t on = nullptr) {
+        if (!on) on = stream;
         if (fast())
             launch_viscous_fast(rel(), p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p,
-                                stream);
+                                on);
         else
-            launch_viscous(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, stream);
+            launch_viscous(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, dwalls.p, vel[b].p, on);
     }
 
     const uint32_t* walk_order() const { return worder_valid ? worder.p : nullptr; }
@@ -955,10 +966,14 @@ struct World {
 
     // After a density pass: a list longer than its room leaves the substep to be run again.
     static constexpr int32_t kRetry = -1;
+    // The status then holds the failed substep's fields, so the committed state's box and speed
+    // are taken again for the rerun's sort.
     int32_t lists_fit() {
         if (h_status->list_max <= list_cap) return SLF_OK;
         list_cap = (uint32_t(h_status->list_max) + h_status->list_max / 4 + 15u) & ~7u;
         SLF_TRY(ensure_work_buffers());
+        stats_fresh = false;
+        SLF_TRY(refresh_stats());
         return kRetry;
     }
 
@@ -1702,11 +1717,14 @@ struct World {
     }
 
     // Clears the per-substep fields; the box starts empty.
-    int32_t reset_status() {
+    static Status fresh_status() {
         Status z{};
         z.cell_lo[0] = z.cell_lo[1] = z.cell_lo[2] = INT32_MAX;
         z.cell_hi[0] = z.cell_hi[1] = z.cell_hi[2] = INT32_MIN;
-        *h_status = z;
+        return z;
+    }
+    int32_t reset_status() {
+        *h_status = fresh_status();
         SLF_CUDA(cudaMemcpyAsync(d_status, h_status, sizeof(Status), cudaMemcpyHostToDevice, stream));
         return SLF_OK;
     }
@@ -1729,64 +1747,110 @@ struct World {
     // Sorts the committed state into slot `to` (pos/vel) and the other id slot, by (cell, id).
     // Needs the committed state's box in the status.  Commits nothing.
     int32_t sort_into(int to) {
-        Params p = params();
         if (n == 0) return SLF_OK;
-        int64_t lo[3], span[3];
-        __int128 vol = 1;
+        SortPlan sp;
+        SLF_TRY(plan_sort(sp, false));
+        enqueue_sort(to, sp, stream);
+        return SLF_OK;
+    }
+
+    // What a sort's launches take, fixed on the host before they are queued: the dense cell
+    // table's box, the particle range whose destinations are skipped, and whether the lists get a
+    // walk order.  Planning also sizes every buffer the sort and the pair passes write, so that
+    // the launches can be recorded into a graph (which allocates nothing).
+    struct SortPlan {
+        int3 lo{}, span{};
+        uint32_t volume = 0;
+        size_t keys = 0;  // walk-order keys; 0 when the lists keep the particle order
+        uint32_t job_lo = 0, job_hi = 0;
+    };
+    // stable: the table's box is the container's cells joined with the particles' (their own box
+    // when that is too large for the table).  Cells are ordered by (x, y, z) over any box that
+    // holds them, so the sort's order, and everything after it, is the same over either box.
+    int32_t plan_sort(SortPlan& sp, bool stable) {
+        int64_t lo[3], hi[3];
         for (int a = 0; a < 3; ++a) {
             lo[a] = h_status->cell_lo[a];
-            span[a] = int64_t(h_status->cell_hi[a]) - lo[a] + 1;
-            if (span[a] <= 0) return fail(SLF_ERR_CUDA, "empty cell box before a sort");
-            vol *= span[a];
+            hi[a] = h_status->cell_hi[a];
+            if (hi[a] < lo[a]) return fail(SLF_ERR_CUDA, "empty cell box before a sort");
         }
+        auto volume_of = [](const int64_t* l, const int64_t* h) {
+            __int128 v = 1;
+            for (int a = 0; a < 3; ++a) v *= __int128(h[a] - l[a] + 1);
+            return v;
+        };
         // a dense count table over the box; a scene spread too thin for it is not supported yet
-        if (vol > (__int128)64 * (__int128)n + (1 << 22) || vol >= (__int128)(1u << 31))
+        const __int128 limit = (__int128)64 * (__int128)n + (1 << 22);
+        auto fits = [&](__int128 v) { return v <= limit && v < (__int128)(1u << 31); };
+        if (stable && has_bounds) {
+            Key3 cl = cell_of(blow), ch = cell_of(bhigh);
+            int64_t wl[3] = {std::min<int64_t>(lo[0], cl.x), std::min<int64_t>(lo[1], cl.y),
+                             std::min<int64_t>(lo[2], cl.z)};
+            int64_t wh[3] = {std::max<int64_t>(hi[0], ch.x), std::max<int64_t>(hi[1], ch.y),
+                             std::max<int64_t>(hi[2], ch.z)};
+            if (fits(volume_of(wl, wh)))
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = wl[a];
+                    hi[a] = wh[a];
+                }
+        }
+        __int128 vol = volume_of(lo, hi);
+        if (!fits(vol))
             return fail(SLF_ERR_UNSUPPORTED, "particles spread over too many cells for the dense cell table");
-        uint32_t volume = uint32_t(vol);
-        SLF_TRY(ensure_work_buffers());
-        SLF_TRY(count.ensure(size_t(volume) + 1, 0, stream));
-        SLF_TRY(tiles.ensure(scan_tiles(volume) + 1, 0, stream));
-        SLF_CUDA(cudaMemsetAsync(count.p, 0, (size_t(volume) + 1) * 4, stream));
-        int3 lo3 = make_int3(int(lo[0]), int(lo[1]), int(lo[2]));
-        int3 sp3 = make_int3(int(span[0]), int(span[1]), int(span[2]));
-        timed("hash_count", bytes_per_particle::count_cells,
-              [&] { launch_count_cells(p, pos[cpos].p, cells_of(cpos), lo3, sp3, count.p, lin.p, cslot.p, stream); });
-        timed("hash_scan", bytes_per_particle::scan, [&] { launch_exclusive_scan(count.p, volume, tiles.p, stream); });
-        timed("hash_scatter", bytes_per_particle::scatter, [&] {
-            launch_scatter_members(uint32_t(n), lin.p, cslot.p, count.p, ids[cid].p, members.p, stream);
-        });
-        uint32_t job_lo = 0, job_hi = 0;
+        sp.volume = uint32_t(vol);
+        sp.lo = make_int3(int(lo[0]), int(lo[1]), int(lo[2]));
+        sp.span = make_int3(int(hi[0] - lo[0] + 1), int(hi[1] - lo[1] + 1), int(hi[2] - lo[2] + 1));
+        sp.job_lo = sp.job_hi = 0;
         if (skip_job >= 0) {
-            job_lo = uint32_t(skip_job) * 512u;
-            job_hi = job_lo + 512u;
+            sp.job_lo = uint32_t(skip_job) * 512u;
+            sp.job_hi = sp.job_lo + 512u;
             skip_job = -1;
         }
-        timed("hash_reorder", bytes_per_particle::reorder, [&] {
-            launch_rank_reorder(uint32_t(n), lin.p, count.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p,
-                                rho[cid].p, cells_of(cpos), ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p,
-                                cells_of(to), warm_in(), warm_out(), job_lo, job_hi, d_status, sort_dest, stream);
-        });
+        SLF_TRY(ensure_work_buffers());
+        SLF_TRY(count.ensure(size_t(sp.volume) + 1, 0, stream));
+        SLF_TRY(tiles.ensure(scan_tiles(sp.volume) + 1, 0, stream));
         // the walk order of this sort's lists (identity where its key space would not fit 32 bits)
-        worder_valid = false;
-        size_t keys = walk_order_keys(sp3);
+        size_t keys = walk_order_keys(sp.span);
+        sp.keys = 0;
         if (keys < (size_t(1) << 31)) {
             SLF_TRY(worder.ensure(n, 0, stream));
             SLF_TRY(wkeys.ensure(keys + 1, 0, stream));
             SLF_TRY(wsums.ensure(scan_tiles(uint32_t(keys)) + 1, 0, stream));
-            timed("walk_order", bytes_per_particle::walk_order,
-                  [&] { launch_walk_order(volume, sp3, count.p, wkeys.p, wsums.p, worder.p, stream); });
-            worder_valid = true;
+            sp.keys = keys;
         }
+        worder_valid = sp.keys != 0;
         fgrid = GridDev{};
         fgrid.mode = 1;
-        fgrid.lx = lo3.x;
-        fgrid.ly = lo3.y;
-        fgrid.lz = lo3.z;
-        fgrid.sx = sp3.x;
-        fgrid.sy = sp3.y;
-        fgrid.sz = sp3.z;
+        fgrid.lx = sp.lo.x;
+        fgrid.ly = sp.lo.y;
+        fgrid.lz = sp.lo.z;
+        fgrid.sx = sp.span.x;
+        fgrid.sy = sp.span.y;
+        fgrid.sz = sp.span.z;
         fgrid.start = count.p;
         return SLF_OK;
+    }
+
+    // the planned sort's launches on stream `on`
+    void enqueue_sort(int to, const SortPlan& sp, cudaStream_t on) {
+        Params p = params();
+        cudaMemsetAsync(count.p, 0, (size_t(sp.volume) + 1) * 4, on);
+        timed("hash_count", bytes_per_particle::count_cells, [&] {
+            launch_count_cells(p, pos[cpos].p, cells_of(cpos), sp.lo, sp.span, count.p, lin.p, cslot.p, on);
+        });
+        timed("hash_scan", bytes_per_particle::scan,
+              [&] { launch_exclusive_scan(count.p, sp.volume, tiles.p, on); });
+        timed("hash_scatter", bytes_per_particle::scatter, [&] {
+            launch_scatter_members(uint32_t(n), lin.p, cslot.p, count.p, ids[cid].p, members.p, on);
+        });
+        timed("hash_reorder", bytes_per_particle::reorder, [&] {
+            launch_rank_reorder(uint32_t(n), lin.p, count.p, members.p, ids[cid].p, pos[cpos].p, vel[cpos].p,
+                                rho[cid].p, cells_of(cpos), ids[1 - cid].p, pos[to].p, vel[to].p, rho[1 - cid].p,
+                                cells_of(to), warm_in(), warm_out(), sp.job_lo, sp.job_hi, d_status, sort_dest, on);
+        });
+        if (sp.keys)
+            timed("walk_order", bytes_per_particle::walk_order,
+                  [&] { launch_walk_order(sp.volume, sp.span, count.p, wkeys.p, wsums.p, worder.p, on); });
     }
 
     int32_t update_neighbors() {
@@ -1942,14 +2006,14 @@ struct World {
         uint64_t used = 0;
         uint32_t pre = 0;  // kernels ahead of the loop
     };
-    bool use_graphs = true;  // slf_solver_graphs
+    int32_t graph_mode = 2;  // slf_solver_graphs: 0 batched, 1 solves, 2 whole substeps
     std::vector<SolveGraph> solve_graphs;
     uint64_t graph_clock = 0;
     cudaStream_t cap[2] = {nullptr, nullptr};
     uint32_t graph_solves = 0;  // bit w: solve w of the running substep ran as a graph, not yet read
 
     bool graphs_for(const SolveRec&) const {
-        return use_graphs && !prof.on && s.max_iterations <= kGraphMaxIterations;
+        return graph_mode >= 1 && !prof.on && s.max_iterations <= kGraphMaxIterations;
     }
     void drop_solve_graphs() {
         for (auto& g : solve_graphs)
@@ -2077,6 +2141,147 @@ struct World {
         return SLF_OK;
     }
 
+    // ---- the whole DFSPH substep as one graph -------------------------------------------------
+    // In graph mode 2 a DFSPH substep without a tape or profile is one graph launch: the sort and
+    // its walk order, the status reset (a copy from pinned memory), the density pass, both solves
+    // with their device-ended loops, viscosity and the advance.  The substep's constants (dt and
+    // what follows from it) are read from device memory, written by one launch ahead of the
+    // graph, so a graph holds across substeps whose dt changes.  The cell table's box is the
+    // container's (plan_sort, stable), so slot rotation alone (3 position slots x 2 id slots)
+    // gives the 6 graphs of a steady run.  Graphs are cached by a key of every value their
+    // launches take and recorded the first time a key is met, until two graphs leave the cache
+    // having run once: from then on (a scene whose count changes every tick: flows, a domain) a
+    // key is recorded the second time it is met, and keys met once run the eager launches.
+    struct SubstepGraph {
+        std::vector<uint8_t> key;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t used = 0;
+        uint64_t runs = 0;
+        uint32_t outside = 0;  // kernels outside the solve loops
+    };
+    std::vector<SubstepGraph> substep_graphs;
+    std::vector<std::vector<uint8_t>> substep_seen;  // keys met once, oldest first
+    uint64_t graph_substeps = 0;                     // substeps run as one graph launch
+    uint32_t unused_graphs = 0;                      // graphs evicted after one run
+    static constexpr uint32_t kUnusedGraphs = 2;     // ... after which keys wait for a second sighting
+
+    bool whole_substeps() const {
+        return graph_mode >= 2 && !prof.on && s.max_iterations <= kGraphMaxIterations && skip_job < 0 &&
+               terrains.empty() && m_pos.empty() && n > 0;
+    }
+    void drop_substep_graphs() {
+        for (auto& g : substep_graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        substep_graphs.clear();
+        substep_seen.clear();
+        unused_graphs = 0;
+    }
+    std::vector<uint8_t> substep_key(const Params& p, int a, int b, int nid, const SortPlan& sp) {
+        static_assert(sizeof(GridDev) == 48, "GridDev has no padding");
+        std::vector<uint8_t> k;
+        key_add(k, int32_t(fast()));
+        key_add(k, int32_t(rel()));
+        key_add(k, int32_t(warm_on()));
+        key_add(k, p);
+        key_add(k, sp.lo);
+        key_add(k, sp.span);
+        key_add(k, sp.volume);
+        key_add(k, sp.keys);
+        key_add(k, sp.job_lo);
+        key_add(k, sp.job_hi);
+        key_add(k, fgrid);
+        key_add(k, wgrid);
+        key_lists(k, fluid_lists());
+        key_lists(k, wall_lists());
+        for (const void* q : std::initializer_list<const void*>{
+                 pos[cpos].p, vel[cpos].p, cells_of(cpos), ids[cid].p, ids[nid].p, rho[cid].p, rho[nid].p,
+                 pos[a].p, vel[a].p, cells_of(a), pos[b].p, vel[b].p, cells_of(b), warm_in(), warm_out(),
+                 sort_dest, count.p, tiles.p, lin.p, cslot.p, members.p, worder.p, wkeys.p, wsums.p, press.p,
+                 scaled.p, alpha.p, dwalls.p, partials.p, d_status, d_consts, vel_pre, h_reset})
+            key_add(k, q);
+        return k;
+    }
+
+    // records the substep's launches into g.exec (the solve loops' bodies on cap[1])
+    int32_t capture_substep(const Params& p, int a, int b, int nid, const SortPlan& sp, SubstepGraph& g) {
+        for (auto& c : cap)
+            if (!c) SLF_CUDA(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
+        cudaStream_t cs = cap[0];
+        uint64_t before = kernel_launches();
+        SLF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        auto record = [&]() -> int32_t {
+            enqueue_sort(a, sp, cs);
+            SLF_CUDA(cudaMemcpyAsync(d_status, h_reset, sizeof(Status), cudaMemcpyHostToDevice, cs));
+            PairLists fl = fluid_lists(), wl = wall_lists();
+            density_pass(p, a, fl, wl, rho[nid].p, cs);
+            uint32_t pre = 0;
+            SLF_TRY(capture_solve(0, p, a, vel[a].p, nid, fl, wl, SolveRec{nullptr, nullptr}, pre));
+            viscous_pass(p, fl, wl, a, b, nid, cs);
+            SLF_TRY(capture_solve(1, p, a, vel[b].p, nid, fl, wl, SolveRec{nullptr, nullptr}, pre));
+            advance_pass(p, a, b, vel_pre, cs);
+            return SLF_OK;
+        };
+        int32_t st = record();
+        cudaGraph_t graph = nullptr;
+        cudaError_t ended = cudaStreamEndCapture(cs, &graph);
+        // launches recorded into the graph ran nothing yet; they count when it runs
+        int64_t recorded = int64_t(kernel_launches() - before);
+        note_launches(-recorded);
+        if (st != SLF_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        SLF_CUDA(ended);
+        cudaError_t made = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        SLF_CUDA(made);
+        // each solve's loop body (a push and a check) counts per iteration when it runs
+        g.outside = uint32_t(recorded - 4);
+        return SLF_OK;
+    }
+
+    // Runs the planned substep as one graph launch when its graph is cached or recorded now;
+    // ran = false leaves the substep to the eager launches.
+    int32_t substep_graph(float dt, const Params& p, int a, int b, int nid, const SortPlan& sp, bool& ran) {
+        ran = false;
+        std::vector<uint8_t> key = substep_key(p, a, b, nid, sp);
+        SubstepGraph* hit = nullptr;
+        for (auto& g : substep_graphs)
+            if (g.key == key) hit = &g;
+        if (!hit) {
+            if (unused_graphs >= kUnusedGraphs) {
+                auto seen = std::find(substep_seen.begin(), substep_seen.end(), key);
+                if (seen == substep_seen.end()) {
+                    if (substep_seen.size() >= 2 * kGraphCache) substep_seen.erase(substep_seen.begin());
+                    substep_seen.push_back(std::move(key));
+                    return SLF_OK;
+                }
+                substep_seen.erase(seen);
+            }
+            SubstepGraph g;
+            g.key = std::move(key);
+            SLF_TRY(capture_substep(p, a, b, nid, sp, g));
+            if (substep_graphs.size() >= kGraphCache) {
+                auto old = std::min_element(substep_graphs.begin(), substep_graphs.end(),
+                                            [](const SubstepGraph& x, const SubstepGraph& y) { return x.used < y.used; });
+                if (old->runs <= 1) ++unused_graphs;
+                cudaGraphExecDestroy(old->exec);
+                substep_graphs.erase(old);
+            }
+            substep_graphs.push_back(std::move(g));
+            hit = &substep_graphs.back();
+        }
+        hit->used = ++graph_clock;
+        ++hit->runs;
+        launch_set_consts(consts(dt), d_consts, stream);
+        SLF_CUDA(cudaGraphLaunch(hit->exec, stream));
+        note_launches(hit->outside);
+        graph_solves = 3;
+        ++graph_substeps;
+        ran = true;
+        return SLF_OK;
+    }
+
     // After solves that ran as graphs (status read back): their iteration counts, their loop
     // kernels in the launch count, and the checks the batched path makes per solve (the lists'
     // room, the stop flag).  its[w] is set for each solve w that ran.
@@ -2136,39 +2341,46 @@ struct World {
     int32_t dfsph_substep(float dt, uint32_t& held, uint32_t& iterations, DfsphRecord* rec = nullptr) {
         Params p = params();
         int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
-        SLF_TRY(sort_into(a));
         int nid = 1 - cid;
-        SLF_TRY(reset_status());
-        graph_solves = 0;
-        launch_set_consts(consts(dt), d_consts, stream);
-        PairLists fl = fluid_lists(), wl = wall_lists();
-        timed("density_alpha", bytes_per_particle::density_dfsph,
-              [&] { density_pass(p, a, fl, wl, rho[nid].p); });
         uint32_t div_it = 0, den_it = 0;
-        SolveRec sr{nullptr, nullptr};
-        if (rec) {
-            size_t slots = (size_t(s.max_iterations) + 1) * n;
-            SLF_TRY(rec_rate.ensure(slots, 0, stream));
-            SLF_TRY(rec_vel.ensure(slots, 0, stream));
-            sr = SolveRec{rec_rate.p, rec_vel.p};
+        bool whole = !rec && whole_substeps();
+        SortPlan sp;
+        SLF_TRY(plan_sort(sp, whole));
+        if (whole) SLF_TRY(substep_graph(dt, p, a, b, nid, sp, whole));
+        if (!whole) {
+            enqueue_sort(a, sp, stream);
+            SLF_TRY(reset_status());
+            graph_solves = 0;
+            launch_set_consts(consts(dt), d_consts, stream);
+            PairLists fl = fluid_lists(), wl = wall_lists();
+            timed("density_alpha", bytes_per_particle::density_dfsph,
+                  [&] { density_pass(p, a, fl, wl, rho[nid].p); });
+            SolveRec sr{nullptr, nullptr};
+            if (rec) {
+                size_t slots = (size_t(s.max_iterations) + 1) * n;
+                SLF_TRY(rec_rate.ensure(slots, 0, stream));
+                SLF_TRY(rec_vel.ensure(slots, 0, stream));
+                sr = SolveRec{rec_rate.p, rec_vel.p};
+            }
+            SLF_TRY(solve(0, p, a, vel[a].p, nid, div_it, sr));
+            if (rec) {
+                SLF_TRY(keep_record(div_it, rec->div_rate, rec->div_vel));
+                rec->div_n = div_it;
+                SLF_TRY(rec->va.ensure(n, 0, stream));
+                SLF_CUDA(
+                    cudaMemcpyAsync(rec->va.p, vel[a].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+            }
+            timed("viscosity", bytes_per_particle::viscosity, [&] { viscous_pass(p, fl, wl, a, b, nid); });
+            SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it, sr));
+            float4* pre = vel_pre;
+            if (rec) {
+                SLF_TRY(keep_record(den_it, rec->den_rate, rec->den_vel));
+                rec->den_n = den_it;
+                SLF_TRY(rec->pre.ensure(n, 0, stream));
+                pre = rec->pre.p;
+            }
+            timed("advance", bytes_per_particle::advance, [&] { advance_pass(p, a, b, pre); });
         }
-        SLF_TRY(solve(0, p, a, vel[a].p, nid, div_it, sr));
-        if (rec) {
-            SLF_TRY(keep_record(div_it, rec->div_rate, rec->div_vel));
-            rec->div_n = div_it;
-            SLF_TRY(rec->va.ensure(n, 0, stream));
-            SLF_CUDA(cudaMemcpyAsync(rec->va.p, vel[a].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
-        }
-        timed("viscosity", bytes_per_particle::viscosity, [&] { viscous_pass(p, fl, wl, a, b, nid); });
-        SLF_TRY(solve(1, p, a, vel[b].p, nid, den_it, sr));
-        float4* pre = vel_pre;
-        if (rec) {
-            SLF_TRY(keep_record(den_it, rec->den_rate, rec->den_vel));
-            rec->den_n = den_it;
-            SLF_TRY(rec->pre.ensure(n, 0, stream));
-            pre = rec->pre.p;
-        }
-        timed("advance", bytes_per_particle::advance, [&] { advance_pass(p, a, b, pre); });
         SLF_TRY(read_status());
         if (graph_solves) {
             uint32_t its[2] = {div_it, den_it};
@@ -3666,7 +3878,8 @@ int32_t slf_step_backward(slf_world* world, const float* dpositions, const float
 
 int32_t slf_solver_graphs(slf_world* world, int32_t on) {
     SLF_WORLD(world);
-    world->w.use_graphs = on != 0;
+    if (on < 0 || on > 2) return fail(SLF_ERR_INVALID_SETTINGS, "graph mode is 0, 1 or 2");
+    world->w.graph_mode = on;
     return SLF_OK;
 }
 
@@ -3717,10 +3930,26 @@ int32_t slf_debug_skip_job(slf_world* world, int64_t job) {
     return SLF_OK;
 }
 
+int32_t slf_debug_list_room(slf_world* world, uint32_t room) {
+    SLF_WORLD(world);
+    World& w = world->w;
+    SLF_TRY(w.flush());
+    w.list_cap = std::max<uint32_t>(8u, room & ~7u);
+    w.lists_valid = false;
+    return w.n ? w.ensure_work_buffers() : SLF_OK;
+}
+
 int32_t slf_last_iterations(const slf_world* world, uint32_t* divergence, uint32_t* density) {
     SLF_WORLD(world);
     if (divergence) *divergence = world->w.last_iterations[0];
     if (density) *density = world->w.last_iterations[1];
+    return SLF_OK;
+}
+
+int32_t slf_graph_substeps(const slf_world* world, uint64_t* out) {
+    SLF_WORLD(world);
+    SLF_NEED(out);
+    *out = world->w.graph_substeps;
     return SLF_OK;
 }
 

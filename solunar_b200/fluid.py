@@ -82,10 +82,12 @@ def load_library():
         "slf_state_hash": [vp, u64p],
         "slf_last_iterations": [vp, u32p, u32p],
         "slf_debug_skip_job": [vp, ctypes.c_int64],
+        "slf_debug_list_room": [vp, ctypes.c_uint32],
         "slf_write_state": [vp, fp, fp, ctypes.c_uint64],
         "slf_get_stream": [vp, ctypes.POINTER(vp)],
         "slf_profile_enable": [vp, ctypes.c_int32],
         "slf_solver_graphs": [vp, ctypes.c_int32],
+        "slf_graph_substeps": [vp, ctypes.POINTER(ctypes.c_uint64)],
         "slf_profile_read": [vp, ctypes.POINTER(CProfileEntry), ctypes.c_uint32, u32p],
         "slf_profile_reset": [vp],
         "slf_kernel_launches": [u64p],
@@ -322,6 +324,10 @@ class FluidWorld:
     def debug_skip_job(self, job: int):
         _check(_lib.slf_debug_skip_job(self._h, job))
 
+    def debug_list_room(self, room: int):
+        """Test hook: shrinks the neighbour lists' room so the next substep outgrows it and runs again."""
+        _check(_lib.slf_debug_list_room(self._h, room))
+
     # ---- read-outs (mod.rs:393-408, 612, 678) ----
     def ids(self) -> np.ndarray:
         n = self.len()
@@ -429,10 +435,18 @@ class FluidWorld:
         """Times each kernel launch with CUDA events (solves then run launch by launch)."""
         _check(_lib.slf_profile_enable(self._h, 1 if on else 0))
 
-    def solver_graphs(self, on: bool = True):
-        """Runs each DFSPH solve as one CUDA graph whose loop the device ends (the default), or
-        as batches of launches with a host check between them; the results are identical."""
-        _check(_lib.slf_solver_graphs(self._h, 1 if on else 0))
+    def solver_graphs(self, mode=2):
+        """How DFSPH steps launch: 2 (the default, also True) each substep as one CUDA graph,
+        1 each solve as one graph whose loop the device ends, 0 (also False) solves as batches
+        of launches with a host check between them; the results are identical."""
+        mode = 2 if mode is True else 0 if mode is False else int(mode)
+        _check(_lib.slf_solver_graphs(self._h, mode))
+
+    def graph_substeps(self) -> int:
+        """DFSPH substeps this world ran as one whole-substep graph launch."""
+        out = ctypes.c_uint64(0)
+        _check(_lib.slf_graph_substeps(self._h, ctypes.byref(out)))
+        return out.value
 
     def profile_reset(self):
         _check(_lib.slf_profile_reset(self._h))
