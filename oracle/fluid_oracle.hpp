@@ -54,6 +54,8 @@
 #include <utility>
 #include <vector>
 
+#include "dual.hpp"
+
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -75,26 +77,38 @@ enum Status : int32_t {
 
 // ---- scalar helpers ---------------------------------------------------------------------
 
+// The standard functions on the restatement's scalar.  Called unqualified, so that a derivative
+// number type (dual.hpp) supplies its own by argument-dependent lookup; for float and double
+// they are the standard functions themselves.
+template <class R> inline R osqrt(R x) { return std::sqrt(x); }
+template <class R> inline R ofloor(R x) { return std::floor(x); }
+template <class R> inline R oceil(R x) { return std::ceil(x); }
+template <class R> inline R oround(R x) { return std::round(x); }
+template <class R> inline R ofabs(R x) { return std::fabs(x); }
+template <class R> inline bool oisnan(R x) { return std::isnan(x); }
+template <class R> inline bool oisfinite(R x) { return std::isfinite(x); }
+
 // Rust f32::min / f32::max: a NaN operand yields the other one.
 template <class R> inline R rmin(R a, R b) {
-    if (std::isnan(a)) return b;
-    if (std::isnan(b)) return a;
+    if (oisnan(a)) return b;
+    if (oisnan(b)) return a;
     return b < a ? b : a;
 }
 template <class R> inline R rmax(R a, R b) {
-    if (std::isnan(a)) return b;
-    if (std::isnan(b)) return a;
+    if (oisnan(a)) return b;
+    if (oisnan(b)) return a;
     return b > a ? b : a;
 }
 // Rust's `f as i32`: saturating, NaN to 0
 template <class R> inline int32_t as_i32(R v) {
-    if (std::isnan(v)) return 0;
+    if (oisnan(v)) return 0;
     if (v >= R(2147483647.0)) return INT32_MAX;
     if (v <= R(-2147483648.0)) return INT32_MIN;
     return int32_t(v);
 }
 // f32::total_cmp's order: -NaN < -inf < ... < -0 < +0 < ... < +inf < +NaN
 template <class R> inline bool total_less(R a, R b) {
+    static_assert(sizeof(R) == 4 || sizeof(R) == 8, "total_less: a float or a double");
     using U = typename std::conditional<sizeof(R) == 4, int32_t, int64_t>::type;
     using UU = typename std::make_unsigned<U>::type;
     U x, y;
@@ -113,13 +127,14 @@ template <class R> inline R pow7(R x) { R s = x * x; R q = s * s; return (x * s)
 
 // Rust `as i32` from a float: saturating, NaN to zero (mod.rs:529-531).
 template <class R> inline int32_t sat_i32(R v) {
-    if (std::isnan(v)) return 0;
+    if (oisnan(v)) return 0;
     if (v >= R(2147483647.0)) return std::numeric_limits<int32_t>::max();
     if (v <= R(-2147483648.0)) return std::numeric_limits<int32_t>::min();
     return static_cast<int32_t>(v);
 }
 
 template <class R> inline uint64_t bits_of(R v) {
+    static_assert(sizeof(R) == 4 || sizeof(R) == 8, "bits_of: a float or a double");
     if constexpr (std::is_same_v<R, float>) {
         uint32_t b;
         std::memcpy(&b, &v, 4);
@@ -148,9 +163,9 @@ template <class R> inline V3<R> operator*(V3<R> a, R s) { return {a.x * s, a.y *
 template <class R> inline V3<R> operator/(V3<R> a, R s) { return {a.x / s, a.y / s, a.z / s}; }
 template <class R> inline R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 template <class R> inline R length_squared(V3<R> a) { return dot(a, a); }
-template <class R> inline R length(V3<R> a) { return std::sqrt(length_squared(a)); }
+template <class R> inline R length(V3<R> a) { return osqrt(length_squared(a)); }
 template <class R> inline bool is_finite(V3<R> a) {
-    return std::isfinite(a.x) && std::isfinite(a.y) && std::isfinite(a.z);
+    return oisfinite(a.x) && oisfinite(a.y) && oisfinite(a.z);
 }
 template <class R> inline V3<R> vmin(V3<R> a, V3<R> b) { return {rmin(a.x, b.x), rmin(a.y, b.y), rmin(a.z, b.z)}; }
 template <class R> inline V3<R> vmax(V3<R> a, V3<R> b) { return {rmax(a.x, b.x), rmax(a.y, b.y), rmax(a.z, b.z)}; }
@@ -167,7 +182,7 @@ template <class R> inline V3<R> rotate(const R q[4], V3<R> v) {
 }
 template <class R> inline V3<R> normalize_or(V3<R> v, V3<R> fallback) {
     R len = length(v);
-    if (std::isfinite(len) && len > R(0)) return v / len;
+    if (oisfinite(len) && len > R(0)) return v / len;
     return fallback;
 }
 
@@ -199,11 +214,11 @@ struct Settings {
 
     // mod.rs:98-117
     bool valid() const {
-        auto positive = [](float v) { return std::isfinite(v) && v > 0.0f; };
+        auto positive = [](float v) { return oisfinite(v) && v > 0.0f; };
         bool support_ok = support >= 1.5f && support <= 4.0f;
         return positive(spacing) && positive(rest_density) && support_ok && max_particles > 0 &&
-               positive(sound_speed) && std::isfinite(viscosity) && viscosity >= 0.0f &&
-               std::isfinite(gravity[0]) && std::isfinite(gravity[1]) && std::isfinite(gravity[2]) &&
+               positive(sound_speed) && oisfinite(viscosity) && viscosity >= 0.0f &&
+               oisfinite(gravity[0]) && oisfinite(gravity[1]) && oisfinite(gravity[2]) &&
                courant > 0.0f && courant <= 1.0f && max_substeps > 0;
     }
 };
@@ -365,7 +380,7 @@ struct CompensatedSum {
     double sum = 0.0, carry = 0.0;
     void add(double v) {
         double t = sum + v;
-        if (std::fabs(sum) >= std::fabs(v)) carry += (sum - t) + v;
+        if (ofabs(sum) >= ofabs(v)) carry += (sum - t) + v;
         else carry += (v - t) + sum;
         sum = t;
     }
@@ -473,7 +488,7 @@ template <class R> class World {
         const R spacing = R(settings.spacing), r = radius();
         GroundSites g;
         g.spacing = spacing;
-        int reach = int(std::ceil(r / spacing));
+        int reach = int(oceil(r / spacing));
         for (int z = -reach; z <= reach; ++z)
             for (int y = -reach; y <= reach; ++y)
                 for (int x = -reach; x <= reach; ++x) {
@@ -499,7 +514,7 @@ template <class R> class World {
                     for (int b = -across_reach; b <= across_reach; ++b) {
                         R across = R(a * a + b * b) * spacing * spacing;
                         R squared = across + depth * depth;
-                        R far = std::sqrt(squared);
+                        R far = osqrt(squared);
                         if (far >= r || far <= R(0)) continue;
                         weight += mass * depth * depth * -kernel.slope(far) / (far * (squared + soften));
                     }
@@ -513,7 +528,7 @@ template <class R> class World {
     // GroundSites::damping (terrain.rs:241-249)
     R damping(R distance) const {
         R at = (rmax(distance, sites.low) - sites.low) / sites.step;
-        size_t below = size_t(std::floor(at));
+        size_t below = size_t(ofloor(at));
         if (below + 1 >= size_t(kMapSamples)) return R(0);
         R part = at - R(below);
         return sites.damping[below] + (sites.damping[below + 1] - sites.damping[below]) * part;
@@ -524,7 +539,7 @@ template <class R> class World {
         Vec local = (point - t.low) / t.step;
         auto inside = [](R v, size_t nodes) { return v >= R(0) && v <= R(nodes - 1); };
         if (!(inside(local.x, t.nx) && inside(local.y, t.ny) && inside(local.z, t.nz))) return false;
-        auto base = [](R v, size_t nodes) { return std::min(size_t(std::floor(v)), nodes - 2); };
+        auto base = [](R v, size_t nodes) { return std::min(size_t(ofloor(v)), nodes - 2); };
         size_t x = base(local.x, t.nx), y = base(local.y, t.ny), z = base(local.z, t.nz);
         R fx = local.x - R(x), fy = local.y - R(y), fz = local.z - R(z);
         auto corner = [&](size_t dx, size_t dy, size_t dz) {
@@ -605,7 +620,7 @@ template <class R> class World {
         if (!is_finite(low) || !is_finite(high)) return NON_FINITE;
         if (high.x <= low.x || high.y <= low.y || high.z <= low.z) return OUT_OF_RANGE;
         R step = R(settings.spacing) / R(2);
-        auto count = [&](R extent) { return size_t(rmin(std::ceil(extent / step), R(1e7))) + 1; };
+        auto count = [&](R extent) { return size_t(rmin(oceil(extent / step), R(1e7))) + 1; };
         Vec size = high - low;
         nodes[0] = count(size.x);
         nodes[1] = count(size.y);
@@ -638,12 +653,19 @@ template <class R> class World {
     static R radius_of(const Settings& s) { return R(s.spacing) * R(s.support); }
     R radius() const { return radius_of(settings); }
     size_t len() const { return ids.size(); }
-    Vec gravity() const { return Vec(R(settings.gravity[0]), R(settings.gravity[1]), R(settings.gravity[2])); }
+    Vec gravity() const { return Vec(param(settings.gravity[0], 2), param(settings.gravity[1], 3), param(settings.gravity[2], 4)); }
+    // A physics parameter as the step reads it: its value, and for a derivative run (R = Dual)
+    // the tangent seeded for it (0 viscosity, 1 sound speed, 2-4 gravity).
+    double param_tangent[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    R param(float v, int which) const {
+        if constexpr (std::is_same_v<R, Dual>) return R(double(v), param_tangent[which]);
+        else return R(v);
+    }
 
     // mod.rs:694-709
     static R rest_mass(const Settings& s) {
         Kernel<R> k(radius_of(s));
-        int reach = int(std::ceil(s.support));
+        int reach = int(oceil(s.support));
         R sum = R(0);
         for (int z = -reach; z <= reach; ++z)
             for (int y = -reach; y <= reach; ++y)
@@ -769,7 +791,7 @@ template <class R> class World {
         if (!is_finite(half) || rmin(rmin(half.x, half.y), half.z) <= R(0)) return INVALID_SHAPE;
         auto depth = [&](Vec at) -> R {
             if (kind == 0) {
-                Vec room = half - Vec(std::fabs(at.x), std::fabs(at.y), std::fabs(at.z));
+                Vec room = half - Vec(ofabs(at.x), ofabs(at.y), ofabs(at.z));
                 return rmin(rmin(room.x, room.y), room.z);
             }
             if (kind == 1) return a - length(at);
@@ -777,8 +799,8 @@ template <class R> class World {
             return a - length(at - Vec(R(0), y, R(0)));
         };
         auto count = [&](R extent) -> int64_t {
-            R v = std::floor(R(2) * extent / spacing);
-            int64_t k = std::isnan(v) ? 0 : (v >= R(4096) ? 4096 : (v <= R(0) ? 0 : int64_t(v)));
+            R v = ofloor(R(2) * extent / spacing);
+            int64_t k = oisnan(v) ? 0 : (v >= R(4096) ? 4096 : (v <= R(0) ? 0 : int64_t(v)));
             return k;
         };
         int64_t cx = count(half.x), cy = count(half.y), cz = count(half.z);
@@ -1031,7 +1053,7 @@ template <class R> class World {
             std::vector<Top> tops;
             for (uint32_t i : near) {
                 Vec at = positions[i];
-                tops.push_back(Top{as_i32(std::floor(at.x / column)), as_i32(std::floor(at.z / column)), dot(at, up)});
+                tops.push_back(Top{as_i32(ofloor(at.x / column)), as_i32(ofloor(at.z / column)), dot(at, up)});
             }
             std::sort(tops.begin(), tops.end(), [](const Top& a, const Top& b) {
                 if (a.kx != b.kx) return a.kx < b.kx;
@@ -1087,7 +1109,7 @@ template <class R> class World {
             size_t nline = 0;
             for (auto& u : under) nline += u.share < R(1) ? 1 : 0;
             R plane = R(float(nline)) * spacing * spacing;
-            R waves = density * plane * std::sqrt(grav * std::sqrt(plane));
+            R waves = density * plane * osqrt(grav * osqrt(plane));
             R share = waves / R(float(std::max<size_t>(nline, 1)));
             for (auto& u : under) {
                 if (!(u.share < R(1))) continue;
@@ -1175,7 +1197,7 @@ template <class R> class World {
 
     // Rust's `f as i64`: saturating, NaN to 0
     static int64_t as_i64(R v) {
-        if (std::isnan(v)) return 0;
+        if (oisnan(v)) return 0;
         if (v >= R(9.2233720368547758e18)) return INT64_MAX;
         if (v <= R(-9.2233720368547758e18)) return INT64_MIN;
         return int64_t(v);
@@ -1211,7 +1233,7 @@ template <class R> class World {
             if (!flow.emitter) continue;
             Vec size = flow.high - flow.low;
             auto count = [&](R extent) -> int64_t {
-                int64_t c = as_i64(std::floor(extent / spacing));
+                int64_t c = as_i64(ofloor(extent / spacing));
                 return std::min<int64_t>(std::max<int64_t>(c, 0), int64_t(1) << 12);
             };
             int64_t cx = count(size.x), cy = count(size.y), cz = count(size.z);
@@ -1225,7 +1247,7 @@ template <class R> class World {
                 Vec local = (at - flow.low) / spacing - Vec::splat(R(0.5));
                 // a slot index outside [-1, cells] reaches no slot; clamping keeps the loops finite
                 auto nearest = [](R v, int64_t cells) {
-                    int64_t c = as_i64(std::round(v));
+                    int64_t c = as_i64(oround(v));
                     return std::min<int64_t>(std::max<int64_t>(c, -2), cells + 1);
                 };
                 int64_t nx = nearest(local.x, cx), ny = nearest(local.y, cy), nz = nearest(local.z, cz);
@@ -1256,8 +1278,8 @@ template <class R> class World {
         if (high.x < low.x || high.y < low.y || high.z < low.z) return OUT_OF_RANGE;
         R spacing = R(settings.spacing);
         auto count = [&](R extent) -> uint64_t {
-            R c = rmin(std::floor(extent / spacing), R(4294967295.0));
-            if (std::isnan(c) || c <= R(0)) return 0;
+            R c = rmin(ofloor(extent / spacing), R(4294967295.0));
+            if (oisnan(c) || c <= R(0)) return 0;
             return uint64_t(c);
         };
         Vec size = high - low;
@@ -1292,7 +1314,7 @@ template <class R> class World {
     // boundary.rs:123-126 (f32::round rounds half away from zero)
     void cells_in(Vec extent, int64_t out[3]) const {
         auto count = [&](R length) -> int64_t {
-            R c = rmin(std::round(length / R(settings.spacing)), R(1e9));
+            R c = rmin(oround(length / R(settings.spacing)), R(1e9));
             return int64_t(c);
         };
         out[0] = count(extent.x);
@@ -1315,7 +1337,7 @@ template <class R> class World {
         if (st != OK) return st;
         int64_t cells[3];
         cells_in(high - low, cells);
-        int64_t layers = int64_t(std::ceil(settings.support));
+        int64_t layers = int64_t(oceil(settings.support));
         int64_t shell = (cells[0] + 2 * layers) * (cells[1] + 2 * layers) * (cells[2] + 2 * layers) -
                         cells[0] * cells[1] * cells[2];
         st = check_room(shell);
@@ -1419,7 +1441,7 @@ template <class R> class World {
 
     Key cell_of(Vec p) const {
         Vec c = p / radius();
-        return Key{sat_i32(std::floor(c.x)), sat_i32(std::floor(c.y)), sat_i32(std::floor(c.z))};
+        return Key{sat_i32(ofloor(c.x)), sat_i32(ofloor(c.y)), sat_i32(ofloor(c.z))};
     }
 
     // boundary.rs:155-178: by cell, owner, position bits, then index.
@@ -1865,7 +1887,7 @@ template <class R> class World {
             if (version >= 3) {
                 float ps2;
                 if (!r.f32(ps2)) return SNAPSHOT;
-                if (!std::isfinite(ps2) || ps2 <= 0.0f) return bad("invalid snapshot: fluid body probes");
+                if (!oisfinite(ps2) || ps2 <= 0.0f) return bad("invalid snapshot: fluid body probes");
                 c.probe_spacing = R(ps2);
                 Status qs = points(kMaxProbes, c.probes);
                 if (qs != OK) return qs;
@@ -1889,7 +1911,7 @@ template <class R> class World {
                   r.count(4, kMaxTerrainNodes, count)))
                 return SNAPSHOT;
             unsigned __int128 total = (unsigned __int128)nx * ny * nz;
-            if (!is_finite(t.low) || !std::isfinite(step) || step <= 0.0f || nx < 2 || ny < 2 || nz < 2 ||
+            if (!is_finite(t.low) || !oisfinite(step) || step <= 0.0f || nx < 2 || ny < 2 || nz < 2 ||
                 total != count)
                 return bad("invalid snapshot: fluid terrain");
             t.nx = nx;
@@ -1899,7 +1921,7 @@ template <class R> class World {
             for (size_t i = 0; i < count; ++i) {
                 float d;
                 if (!r.f32(d)) return SNAPSHOT;
-                if (!std::isfinite(d)) return bad("invalid snapshot: fluid terrain distance");
+                if (!oisfinite(d)) return bad("invalid snapshot: fluid terrain distance");
                 t.distances.push_back(R(d));
             }
             if (t.owner >= w.walls.next) return bad("invalid snapshot: fluid terrain owner");
@@ -1931,7 +1953,7 @@ template <class R> class World {
     // step.rs:58-90
     Status step(R dt, Report& report) {
         report = Report();
-        if (!std::isfinite(dt) || dt < R(0)) return NON_FINITE;
+        if (!oisfinite(dt) || dt < R(0)) return NON_FINITE;
         if (dt == R(0)) return OK;
         if (len() > 0) {
             Status st = settings.solver == 0 ? wcsph(dt, report) : dfsph(dt, report);
@@ -1963,7 +1985,7 @@ template <class R> class World {
     Status wcsph_steps(R dt, R mover, Report& report) {
         R fast = rmax(fastest(), mover);
         R largest = R(settings.courant) * radius() / (R(settings.sound_speed) + fast);
-        R wanted = rmax(std::ceil(dt / largest), R(1));
+        R wanted = rmax(oceil(dt / largest), R(1));
         R cap = R(float(settings.max_substeps));
         uint32_t substeps = uint32_t(rmin(wanted, cap));
         report.capped = wanted > cap;
@@ -1982,7 +2004,7 @@ template <class R> class World {
     // step.rs:254-259
     R viscosity(R dt) const {
         R r = radius();
-        return rmin(R(settings.viscosity) * R(settings.sound_speed) * r, R(0.05f) * r * r / dt);
+        return rmin(param(settings.viscosity, 0) * param(settings.sound_speed, 1) * r, R(0.05f) * r * r / dt);
     }
 
     // step.rs:262-301
@@ -1999,7 +2021,7 @@ template <class R> class World {
             away = away + (-kernel.gradient(at - walls.positions[wall_neighbors.items[k]]));
         Vec normal = normalize_or(away, Vec());
         Vec into = normal * rmin(dot(velocity, normal), R(0));
-        R wall_visc = rmin(R(1) * R(settings.sound_speed) * r, R(0.25f) * stable);
+        R wall_visc = rmin(R(1) * param(settings.sound_speed, 1) * r, R(0.25f) * stable);
         for (const Terrain& t : terrains) {
             R distance;
             Vec n;
@@ -2052,7 +2074,7 @@ template <class R> class World {
         if (st != OK) return st;
         size_t n = len();
         R rest = R(settings.rest_density);
-        R stiffness = rest * pow2(R(settings.sound_speed)) / R(7);
+        R stiffness = rest * pow2(param(settings.sound_speed, 1)) / R(7);
         std::vector<R> pressures(n), scaled(n);
         for (size_t i = 0; i < n; ++i) {
             R ratio = rmin(densities[i] / rest, R(1.1f));
@@ -2065,7 +2087,7 @@ template <class R> class World {
         Vec g = gravity();
         // the body points' damping (step.rs:163-164) and the speed under which water settles
         // against them (couple.rs:390)
-        R damping = rmin(R(1) * R(settings.sound_speed) * r, R(0.25f) * r * r / dt);
+        R damping = rmin(R(1) * param(settings.sound_speed, 1) * r, R(0.25f) * r * r / dt);
         R settles = length(g) * R(settings.spacing);
         std::vector<Vec> pushes(n);
         std::vector<R> mirrors(coupled.empty() ? 0 : n);
@@ -2082,7 +2104,7 @@ template <class R> class World {
                 Vec offset = at - positions[other];
                 R squared = length_squared(offset);
                 if (squared <= R(0)) continue;
-                R distance = std::sqrt(squared);
+                R distance = osqrt(squared);
                 Vec gradient = offset * (kernel.slope(distance) / distance);
                 R toward = rmin(dot(velocity - velocities[other], offset), R(0));
                 R damp = -visc * toward / (squared + soften) * R(2) / (density + densities[other]);
@@ -2155,7 +2177,7 @@ template <class R> class World {
         R left = dt;
         while (left > R(0)) {
             R small = courant * spacing / rmax(fastest(), R(1e-6f));
-            if (pull > R(0)) small = rmin(small, std::sqrt(R(2) * courant * spacing / pull));
+            if (pull > R(0)) small = rmin(small, osqrt(R(2) * courant * spacing / pull));
             if (report.substeps + 1 >= settings.max_substeps && small < left) {
                 report.capped = 1;
                 small = left;

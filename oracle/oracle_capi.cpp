@@ -79,6 +79,9 @@ template <class R> int32_t read_lists(const Lists& l, uint32_t* start, uint64_t 
 
 }  // namespace
 
+// the settings conversion, for the forward-mode runs of oracle_tangent.cpp
+Settings settings_from_c(const slf_settings* s, int residual_sum) { return from_c(s, residual_sum); }
+
 #define ORC_DISPATCH(h, ...)                \
     do {                                    \
         if ((h)->precision == 32) {         \
