@@ -3,7 +3,8 @@
 // CPU restatement of solunar's particle-fluid step, the checker for the CUDA library.  Only
 // tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it; the library never
 // links or calls it.  Templated on the arithmetic type: `float` is the parity oracle and the
-// timed CPU baseline, `double` is the precision oracle.
+// timed CPU baseline, `double` is the precision oracle, and `Dual` (dual.hpp) carries the exact
+// FP64 derivative along one direction for the adjoint's checks (oracle_tangent.cpp).
 //
 // It follows, function by function (paths relative to the reference project):
 //   src/fluid/mod.rs      Kernel :125-165, Grid :169-262, near :264-277, Lists :279-308,
