@@ -1,10 +1,17 @@
 // dual.hpp -- TEST INFRASTRUCTURE ONLY.
 //
-// Forward-mode derivative numbers for the CPU restatement: a double value and its derivative
-// along one direction of the inputs.  `World<Dual>` runs the restatement in FP64 and carries
-// with every quantity its derivative along that direction (the tangent), exactly, with no step
-// size.  Tests check the CUDA library's adjoint (step_backward, the transposed derivative) with
-// the identity <g, J d> = <J^T g, d>.  Branches (the pressure clamp, approach-only viscosity, wall
+// Forward-mode derivative numbers for the CPU restatement: a value and its derivative along one
+// direction of the inputs.  `World<DualOf<V>>` runs the restatement with values of type V and
+// carries with every quantity its derivative along that direction (the tangent), in double,
+// exactly, with no step size:
+//
+//   Dual   = DualOf<double>: the derivative of the FP64 method;
+//   Dual32 = DualOf<float>:  the derivative of the FP32 program itself.  Its values are the float
+//          restatement's bit for bit (every value operation is the float one), hence the CUDA
+//          library's in EXACT arithmetic, so it takes every branch the library's run takes.
+//
+// Tests check the CUDA library's adjoint (step_backward, the transposed derivative) with the
+// identity <g, J d> = <J^T g, d>.  Branches (the pressure clamp, approach-only viscosity, wall
 // clamps, solver stops) follow the value, as the adjoint follows the forward's branches; floor,
 // round and ceil have derivative zero; the square root of zero takes derivative zero (the only
 // zero lengths are a particle's offset to itself, whose derivative is zero too).
@@ -12,44 +19,63 @@
 
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
-struct Dual {
-    double v = 0.0, d = 0.0;
-    Dual() = default;
-    Dual(double x) : v(x) {}  // constants carry no derivative
-    Dual(double x, double dx) : v(x), d(dx) {}
-    explicit operator double() const { return v; }
+template <class V> struct DualOf {
+    V v = V(0);
+    double d = 0.0;
+    DualOf() = default;
+    DualOf(double x) : v(V(x)) {}  // constants carry no derivative
+    DualOf(double x, double dx) : v(V(x)), d(dx) {}
+    explicit operator double() const { return double(v); }
     explicit operator float() const { return float(v); }
     explicit operator int() const { return int(v); }
     explicit operator unsigned() const { return unsigned(v); }
     explicit operator long() const { return long(v); }
     explicit operator unsigned long() const { return (unsigned long)(v); }
     explicit operator long long() const { return (long long)(v); }
-    Dual& operator+=(Dual b) { d += b.d; v += b.v; return *this; }
-    Dual& operator-=(Dual b) { d -= b.d; v -= b.v; return *this; }
-    Dual& operator*=(Dual b) { d = d * b.v + v * b.d; v *= b.v; return *this; }
-    Dual& operator/=(Dual b) { *this = Dual(v / b.v, (d * b.v - v * b.d) / (b.v * b.v)); return *this; }
+
+    static DualOf of(V x, double dx) {
+        DualOf r;
+        r.v = x;
+        r.d = dx;
+        return r;
+    }
+    DualOf& operator+=(DualOf b) { return *this = *this + b; }
+    DualOf& operator-=(DualOf b) { return *this = *this - b; }
+    DualOf& operator*=(DualOf b) { return *this = *this * b; }
+    DualOf& operator/=(DualOf b) { return *this = *this / b; }
+
+    // hidden friends: found through the dual operand, the other one converts
+    friend DualOf operator+(DualOf a, DualOf b) { return of(a.v + b.v, a.d + b.d); }
+    friend DualOf operator-(DualOf a, DualOf b) { return of(a.v - b.v, a.d - b.d); }
+    friend DualOf operator-(DualOf a) { return of(-a.v, -a.d); }
+    friend DualOf operator*(DualOf a, DualOf b) { return of(a.v * b.v, a.d * double(b.v) + double(a.v) * b.d); }
+    friend DualOf operator/(DualOf a, DualOf b) {
+        double bv = double(b.v);
+        return of(a.v / b.v, (a.d * bv - double(a.v) * b.d) / (bv * bv));
+    }
+    friend bool operator<(DualOf a, DualOf b) { return a.v < b.v; }
+    friend bool operator>(DualOf a, DualOf b) { return a.v > b.v; }
+    friend bool operator<=(DualOf a, DualOf b) { return a.v <= b.v; }
+    friend bool operator>=(DualOf a, DualOf b) { return a.v >= b.v; }
+    friend bool operator==(DualOf a, DualOf b) { return a.v == b.v; }
+    friend bool operator!=(DualOf a, DualOf b) { return a.v != b.v; }
+
+    friend DualOf osqrt(DualOf x) {
+        V r = std::sqrt(x.v);
+        return of(r, r > V(0) ? x.d / (2.0 * double(r)) : 0.0);
+    }
+    friend DualOf ofloor(DualOf x) { return of(std::floor(x.v), 0.0); }
+    friend DualOf oceil(DualOf x) { return of(std::ceil(x.v), 0.0); }
+    friend DualOf oround(DualOf x) { return of(std::round(x.v), 0.0); }
+    friend DualOf ofabs(DualOf x) { return x.v < V(0) ? -x : x; }
+    friend bool oisnan(DualOf x) { return std::isnan(x.v); }
+    friend bool oisfinite(DualOf x) { return std::isfinite(x.v); }
 };
 
-inline Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
-inline Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
-inline Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
-inline Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
-inline Dual operator/(Dual a, Dual b) { return Dual(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)); }
-inline bool operator<(Dual a, Dual b) { return a.v < b.v; }
-inline bool operator>(Dual a, Dual b) { return a.v > b.v; }
-inline bool operator<=(Dual a, Dual b) { return a.v <= b.v; }
-inline bool operator>=(Dual a, Dual b) { return a.v >= b.v; }
-inline bool operator==(Dual a, Dual b) { return a.v == b.v; }
-inline bool operator!=(Dual a, Dual b) { return a.v != b.v; }
+using Dual = DualOf<double>;
+using Dual32 = DualOf<float>;
 
-inline Dual osqrt(Dual x) {
-    double r = std::sqrt(x.v);
-    return Dual(r, r > 0.0 ? x.d / (2.0 * r) : 0.0);
-}
-inline Dual ofloor(Dual x) { return Dual(std::floor(x.v)); }
-inline Dual oceil(Dual x) { return Dual(std::ceil(x.v)); }
-inline Dual oround(Dual x) { return Dual(std::round(x.v)); }
-inline Dual ofabs(Dual x) { return x.v < 0.0 ? -x : x; }
-inline bool oisnan(Dual x) { return std::isnan(x.v); }
-inline bool oisfinite(Dual x) { return std::isfinite(x.v); }
+template <class R> struct is_dual : std::false_type {};
+template <class V> struct is_dual<DualOf<V>> : std::true_type {};

@@ -3,8 +3,9 @@
 // CPU restatement of solunar's particle-fluid step, the checker for the CUDA library.  Only
 // tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it; the library never
 // links or calls it.  Templated on the arithmetic type: `float` is the parity oracle and the
-// timed CPU baseline, `double` is the precision oracle, and `Dual` (dual.hpp) carries the exact
-// FP64 derivative along one direction for the adjoint's checks (oracle_tangent.cpp).
+// timed CPU baseline, `double` is the precision oracle, and `DualOf<float | double>` (dual.hpp)
+// carries the exact derivative of the FP32 program or of the FP64 method along one direction for
+// the adjoint's checks (oracle_tangent.cpp).
 //
 // It follows, function by function (paths relative to the reference project):
 //   src/fluid/mod.rs      Kernel :125-165, Grid :169-262, near :264-277, Lists :279-308,
@@ -469,6 +470,11 @@ template <class R> class World {
     std::vector<Vec> grad_fluid, grad_walls;
     // solver iteration counts of the last DFSPH substep: divergence, density
     uint32_t last_iterations[2] = {0, 0};
+    // Iteration counts the next solves take regardless of their errors (divergence, density of
+    // each substep in turn): a derivative run then differentiates the same discrete steps as the
+    // run it checks.  Empty (the default): solves stop on their tolerances.
+    std::vector<uint32_t> forced_iterations;
+    size_t forced_next = 0;
     int threads = 0;  // 0: OpenMP default
 
     static Status create(const Settings& s, World& out) {
@@ -655,11 +661,11 @@ template <class R> class World {
     R radius() const { return radius_of(settings); }
     size_t len() const { return ids.size(); }
     Vec gravity() const { return Vec(param(settings.gravity[0], 2), param(settings.gravity[1], 3), param(settings.gravity[2], 4)); }
-    // A physics parameter as the step reads it: its value, and for a derivative run (R = Dual)
+    // A physics parameter as the step reads it: its value, and for a derivative run (R = DualOf)
     // the tangent seeded for it (0 viscosity, 1 sound speed, 2-4 gravity).
     double param_tangent[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     R param(float v, int which) const {
-        if constexpr (std::is_same_v<R, Dual>) return R(double(v), param_tangent[which]);
+        if constexpr (is_dual<R>::value) return R(double(v), param_tangent[which]);
         else return R(v);
     }
 
@@ -2313,7 +2319,12 @@ template <class R> class World {
                 double average = acc.value() / double(loaded);
                 settled = iterations >= settings.min_iterations && average <= double(tolerance);
             }
-            if (settled || iterations >= settings.max_iterations) return iterations;
+            // a derivative run held to another run's solves stops where that run stopped
+            if (forced_next < forced_iterations.size()) settled = iterations >= forced_iterations[forced_next];
+            if (settled || iterations >= settings.max_iterations) {
+                if (forced_next < forced_iterations.size()) ++forced_next;
+                return iterations;
+            }
             push_apart(stiffness, dt);
             if (settings.warm_start)
                 for (size_t i = 0; i < n; ++i) applied[i] = applied[i] + stiffness[i] * dt;

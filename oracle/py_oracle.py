@@ -82,8 +82,9 @@ def lib():
             "orc_wall_neighbor_lists": [vp, u32p, ctypes.c_uint64, u32p, ctypes.c_uint64, u64p],
             "orc_state_hash": [vp, u64p],
             "orc_last_iterations": [vp, u32p],
-            "orc_tangent_run": [ctypes.POINTER(CSettings), ctypes.c_int32, f3, f3, ctypes.c_uint64, f3, f3, dp, dp, dp,
-                                ctypes.c_uint32, ctypes.c_float, dp, dp, dp, dp, u32p],
+            "orc_tangent_run": [ctypes.POINTER(CSettings), ctypes.c_int32, ctypes.c_int32, f3, f3, ctypes.c_uint64, f3,
+                                f3, dp, dp, dp,
+                                ctypes.c_uint32, ctypes.c_float, u32p, ctypes.c_uint64, dp, dp, dp, dp, u32p],
             "orc_kernel_eval_f32": [ctypes.c_float, ctypes.c_uint64, f3, f3, f3, f3],
             "orc_grid_ranges": [ctypes.POINTER(ctypes.c_int32), ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32),
                                 ctypes.c_uint64, ctypes.c_int32, u32p, ctypes.POINTER(ctypes.c_int32)],
@@ -110,12 +111,17 @@ def _ptr(a: np.ndarray, ctype):
 
 
 def tangent_run(settings: FluidSettings, container, positions, velocities, dpositions, dvelocities,
-                dparams=(0.0, 0.0, 0.0, 0.0, 0.0), steps: int = 1, dt: float = 1e-3, residual_sum: int = 1):
-    """The restatement in forward-mode FP64 (oracle/dual.hpp): a world with one box container
+                dparams=(0.0, 0.0, 0.0, 0.0, 0.0), steps: int = 1, dt: float = 1e-3, residual_sum: int = 1,
+                forced_iterations=None, precision: int = 64):
+    """The restatement in forward-mode derivative numbers (oracle/dual.hpp): values of the FP64
+    method (precision 64) or of the float restatement bit for bit (32, the FP32 program the CUDA
+    library runs), derivatives in double.  A world with one box container
     `container` = (low, high), the particles added in row order (ids 0..n-1), `steps` calls of
     step(dt).  Each input carries a tangent: dpositions, dvelocities (n x 3) and dparams (viscosity,
-    sound speed, gravity x, y, z).  Returns (positions, velocities, their tangents, ids) of the
-    final state, rows in id order."""
+    sound speed, gravity x, y, z).  forced_iterations: the DFSPH solves' iteration counts
+    (divergence, density of each substep in turn) to take instead of stopping on the tolerances,
+    so that the run follows another run's discrete steps.  Returns (positions, velocities, their
+    tangents, ids) of the final state, rows in id order."""
     p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
     v = np.ascontiguousarray(velocities, dtype=np.float32).reshape(-1, 3)
     dp_ = np.ascontiguousarray(dpositions, dtype=np.float64).reshape(-1, 3)
@@ -129,9 +135,10 @@ def tangent_run(settings: FluidSettings, container, positions, velocities, dposi
     c = settings.to_c()
     f = ctypes.c_float
     d = ctypes.c_double
-    _check(lib().orc_tangent_run(ctypes.byref(c), residual_sum, _ptr(lo, f), _ptr(hi, f), n, _ptr(p, f), _ptr(v, f),
-                                 _ptr(dp_, d), _ptr(dv_, d), _ptr(dq, d), steps, dt, *(_ptr(o, d) for o in outs),
-                                 _ptr(ids, ctypes.c_uint32)))
+    forced = np.ascontiguousarray([] if forced_iterations is None else forced_iterations, dtype=np.uint32)
+    _check(lib().orc_tangent_run(ctypes.byref(c), precision, residual_sum, _ptr(lo, f), _ptr(hi, f), n, _ptr(p, f), _ptr(v, f),
+                                 _ptr(dp_, d), _ptr(dv_, d), _ptr(dq, d), steps, dt, _ptr(forced, ctypes.c_uint32),
+                                 len(forced), *(_ptr(o, d) for o in outs), _ptr(ids, ctypes.c_uint32)))
     order = np.argsort(ids)
     return tuple(o[order] for o in outs) + (ids[order],)
 

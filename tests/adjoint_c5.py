@@ -5,10 +5,18 @@ The bench's forward+adjoint workload (100^3 particles at 0.01 m in the 2 x 1 x 1
 Loss: the water's kinetic energy after the steps, sum of m |v|^2 / 2 (smooth, so differences do
 not jump where particles cross a boundary).  The adjoint's derivatives along a uniform change of
 the initial velocities (the inflow vector) and of gravity are compared with central differences of
-the same FP32 forward at two step sizes.  Every evaluation starts from the same state handed to a
+the same FP32 forward at two step sizes, and (--tangent 32) with the exact derivative of the FP32
+program itself along the same directions: the restatement in forward-mode derivative numbers
+whose values are the float restatement's, hence the library's, bit for bit, with derivatives in
+double (oracle/dual.hpp; about a minute a direction on the host cores at this size).  It takes
+every branch the library's run takes.  `--tangent 64` takes the FP64 method's derivative instead,
+which over this flowing, strongly non-linear horizon is a different number: the FP32 and FP64
+trajectories part.  The tangent is also held to the library's solver iteration counts (each
+substep's divergence and density solves).  Differences at eps 1e-2 cross the loss's kinks (solver
+stops, the < 20 neighbour rule, clamps), which is why they scatter.  Every evaluation starts from the same state handed to a
 new world, so the differences and the adjoint see the same particle order.
 
-    python tests/adjoint_c5.py [--steps 32] [--out FILE]
+    python tests/adjoint_c5.py [--steps 32] [--tangent 32|64] [--out FILE]
 """
 import argparse
 import dataclasses
@@ -48,6 +56,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=32)
     ap.add_argument("--warm", type=int, default=20)
+    ap.add_argument("--tangent", type=int, choices=(32, 64), default=None,
+                    help="add the column of the exact derivative of the FP32 program (32) or the FP64 method (64)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
 
@@ -62,19 +72,47 @@ def main():
     # the adjoint over the steps
     w = world_from(sc, sc.settings, pos, vel)
     w.tape_begin(0)
+    counts = []
     for _ in range(args.steps):
-        w.step(sc.dt)
+        r = w.step(sc.dt)
+        if r.substeps != 1:
+            raise SystemExit("a step took more than one substep: the solver counts would be incomplete")
+        counts += list(w.last_iterations())
     L = loss_of(w)
     dv = (w.particle_mass() * np.asarray(w.velocities(), dtype=np.float64)).astype(np.float32)
     _, dv0, params = w.step_backward(np.zeros_like(dv), dv)
     w.tape_end()
+    w_mass = w.particle_mass()
     w.close()
     inflow = dv0.astype(np.float64).sum(axis=0)
     gravity = np.array(params["gravity"])
 
+    def tangent(dvel, dparams):
+        """dL along the direction, from the FP64 restatement's exact derivative."""
+        from oracle import py_oracle
+
+        tank = ((0.0, 0.0, 0.0), sc.tank)
+        _, V, _, dV, _ = py_oracle.tangent_run(sc.settings, tank, pos, vel, np.zeros(pos.shape), dvel,
+                                               dparams=dparams, steps=args.steps, dt=sc.dt, forced_iterations=counts,
+                                               precision=args.tangent)
+        return w_mass * float(np.sum(V * dV))
+
+    head = "| derivative | adjoint | FD eps 1e-3 | rel | FD eps 1e-2 | rel |"
+    rule = "|---|---|---|---|---|---|"
+    if args.tangent:
+        head += f" FP{args.tangent} tangent | rel |"
+        rule += "---|---|"
     lines = [f"1M DFSPH dam, {args.steps} steps of {sc.dt} s from {args.warm} steps in; loss (kinetic energy) "
-             f"{L:.6e} J", "", "| derivative | adjoint | FD eps 1e-3 | rel | FD eps 1e-2 | rel |", "|---|---|---|---|---|---|"]
+             f"{L:.6e} J", "", head, rule]
     worst = []
+    exact = []
+
+    def tangent_cells(adj, dvel, dparams):
+        t = tangent(dvel, dparams)
+        rel = abs(adj - t) / max(abs(t), 1e-300)
+        exact.append(rel)
+        return [f"{t:.6e}", f"{rel:.2e}"]
+
     for k, axis in enumerate("xyz"):
         row = [f"d/d inflow {axis}", f"{inflow[k]:.6e}"]
         rels = []
@@ -87,6 +125,10 @@ def main():
             rels.append(rel)
             row += [f"{num:.6e}", f"{rel:.2e}"]
         worst.append(min(rels))
+        if args.tangent:
+            e = np.zeros(3)
+            e[k] = 1.0
+            row += tangent_cells(inflow[k], np.tile(e, (len(pos), 1)), np.zeros(5))
         lines.append("| " + " | ".join(row) + " |")
         print(lines[-1], flush=True)
     for k, axis in enumerate("xyz"):
@@ -103,9 +145,15 @@ def main():
             rels.append(rel)
             row += [f"{num:.6e}", f"{rel:.2e}"]
         worst.append(min(rels))
+        if args.tangent:
+            q = np.zeros(5)
+            q[2 + k] = 1.0
+            row += tangent_cells(gravity[k], np.zeros(pos.shape), q)
         lines.append("| " + " | ".join(row) + " |")
         print(lines[-1], flush=True)
     lines += ["", f"best-of-steps relative error: median {np.median(worst):.2e}, max {np.max(worst):.2e}"]
+    if exact:
+        lines += [f"against the FP{args.tangent} tangent: median {np.median(exact):.2e}, max {np.max(exact):.2e}"]
     text = "\n".join(lines) + "\n"
     print(text)
     if args.out:

@@ -269,14 +269,14 @@ def test_dfsph_gradients_do_not_depend_on_how_solves_launch(gpu_lib, dfsph_adjoi
 # of the tangent: relative error 1e-5 on the velocity directions and 1e-4 on the parameters
 # (measured on B200: at most 4.5e-7 and 2.0e-5) ----
 
-def tangent_projections(oracle_lib, settings, tank, pos, vel, target, steps, dt, directions, dparams):
-    """<g, dP> of the FP64 tangent for each velocity direction, then each parameter seed."""
+def tangent_projections(oracle_lib, settings, tank, pos, vel, target, steps, dt, directions, dparams, precision=64):
+    """<g, dP> of the tangent for each velocity direction, then each parameter seed."""
     n = len(pos)
     zero = np.zeros(pos.shape)
     out = []
     for d, dq in [(d, np.zeros(5)) for d in directions] + [(zero, q) for q in dparams]:
         P, _, dP, _, _ = oracle_lib.tangent_run(settings, ((0.0, 0.0, 0.0), tank), pos, vel, zero, d, dparams=dq,
-                                                steps=steps, dt=dt)
+                                                steps=steps, dt=dt, precision=precision)
         c = P.mean(axis=0)
         out.append(float(np.sum((2.0 * (c - target) / n) * dP)))
     return out
@@ -314,4 +314,29 @@ def test_dfsph_gradients_match_the_fp64_tangent(oracle_lib, dfsph_adjoint):
     ana += [params["viscosity"], params["gravity"][0]]
     rel = [abs(a - t) / abs(t) for a, t in zip(ana, tan)]
     print("DFSPH adjoint vs FP64 tangent, relative:", rel)
+    assert max(rel[:3]) <= 1e-5 and max(rel[3:]) <= 1e-4, (rel, ana, tan)
+
+
+# ---- against the FP32 program's own derivative: the restatement in derivative numbers whose
+# values are the float restatement's (and so the library's) bit for bit, derivatives in double; it
+# takes every branch the library's forward takes, so what remains is the adjoint's own FP32
+# arithmetic ----
+
+@pytest.mark.parametrize("solver", ["wcsph", "dfsph"])
+def test_gradients_match_the_fp32_programs_tangent(oracle_lib, adjoint, dfsph_adjoint, solver):
+    if solver == "wcsph":
+        sc, pos, vel, target, dp0, dv0, params = adjoint
+        settings, tank, steps, dt, which = sc.settings, sc.tank, STEPS, DT, [0, 1, 2]
+        names = [params["viscosity"], params["sound_speed"], params["gravity"][0]]
+    else:
+        pos, vel, target, dp0, dv0, params = dfsph_adjoint
+        settings, tank, steps, dt, which = dfsph_settings(), (0.5, 0.5, 0.5), DFSPH_STEPS, DFSPH_DT, [0, 2]
+        names = [params["viscosity"], params["gravity"][0]]
+    rng = np.random.default_rng(19)
+    directions = [rng.normal(size=vel.shape) for _ in range(3)]
+    tan = tangent_projections(oracle_lib, settings, tank, pos, vel, target, steps, dt, directions, seeds(which),
+                              precision=32)
+    ana = [float(np.sum(dv0.astype(np.float64) * d)) for d in directions] + names
+    rel = [abs(a - t) / abs(t) for a, t in zip(ana, tan)]
+    print(solver, "adjoint vs FP32 tangent, relative:", rel)
     assert max(rel[:3]) <= 1e-5 and max(rel[3:]) <= 1e-4, (rel, ana, tan)

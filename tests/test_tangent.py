@@ -83,3 +83,46 @@ def test_parameter_tangents_are_the_fp64_restatements_differences(oracle_lib, so
     (sp, hi), (sm, lo) = with_value(eps), with_value(-eps)
     num = (run64(oracle_lib, sp, steps, dt, pos, vel)[0] - run64(oracle_lib, sm, steps, dt, pos, vel)[0]) / (hi - lo)
     assert np.linalg.norm(num - dP) <= 1e-4 * np.linalg.norm(dP), (np.linalg.norm(num - dP), np.linalg.norm(dP))
+
+
+def test_a_run_held_to_its_own_solver_iterations_is_the_same_run(oracle_lib):
+    # forced iteration counts (the counts another run's solves took) change nothing when they are
+    # the counts this run takes anyway, and change the run when they are not
+    s, steps, dt, pos, vel = case(FluidSolver.DFSPH)
+    w = oracle_lib.OracleWorld(s, precision=64, residual_sum=1)
+    w.add_box_container(*TANK)
+    w.add_particles(pos, vel)
+    counts = []
+    for _ in range(steps):
+        r = w.step(dt)
+        assert r.substeps == 1
+        counts += list(w.last_iterations())
+    d = np.random.default_rng(7).normal(size=vel.shape)
+    free = oracle_lib.tangent_run(s, TANK, pos, vel, np.zeros_like(d), d, steps=steps, dt=dt)
+    held = oracle_lib.tangent_run(s, TANK, pos, vel, np.zeros_like(d), d, steps=steps, dt=dt, forced_iterations=counts)
+    for a, b in zip(free, held):
+        assert np.array_equal(a, b)
+    more = oracle_lib.tangent_run(s, TANK, pos, vel, np.zeros_like(d), d, steps=steps, dt=dt,
+                                  forced_iterations=[c + 1 for c in counts])
+    assert not np.array_equal(more[0], free[0])
+
+
+@pytest.mark.parametrize("solver", [FluidSolver.WCSPH, FluidSolver.DFSPH])
+def test_fp32_tangent_values_are_the_float_restatements_bit_for_bit(oracle_lib, solver):
+    # precision 32: every value operation is the float restatement's, so the run is the FP32
+    # program the CUDA library runs (and takes its branches); its derivative, in double, is close
+    # to the FP64 method's on this short run
+    s, steps, dt, pos, vel = case(solver)
+    d = np.random.default_rng(7).normal(size=vel.shape)
+    P, V, dP, dV, ids = oracle_lib.tangent_run(s, TANK, pos, vel, np.zeros_like(d), d, steps=steps, dt=dt,
+                                               precision=32)
+    w = oracle_lib.OracleWorld(s, precision=32, residual_sum=1)
+    w.add_box_container(*TANK)
+    w.add_particles(pos, vel)
+    for _ in range(steps):
+        w.step(dt)
+    order = np.argsort(w.ids())
+    assert np.array_equal(P.astype(np.float32), np.asarray(w.positions(), dtype=np.float32)[order])
+    assert np.array_equal(V.astype(np.float32), np.asarray(w.velocities(), dtype=np.float32)[order])
+    _, _, dP64, _, _ = oracle_lib.tangent_run(s, TANK, pos, vel, np.zeros_like(d), d, steps=steps, dt=dt)
+    assert np.linalg.norm(dP - dP64) <= 1e-3 * np.linalg.norm(dP64)
