@@ -4,9 +4,14 @@
 N(0, 0.1 m/s), 200 steps of 2e-4 s, tape checkpoint every 20 steps.  Loss: |centroid - (start
 centroid + 0.3 m along x)|^2.  The adjoint's derivative along 16 seeded directions of the initial
 velocities, and its viscosity derivative, are compared with central differences of the same FP32
-forward at several step sizes; the forward and the backward are timed with CUDA events.
+forward at several step sizes; the forward and the backward are timed with CUDA events.  With
+--tangent K the first K directions and the viscosity are also compared with the exact derivative
+of the FP32 program itself: the restatement in forward-mode derivative numbers whose values are the
+float restatement's, and so the library's, bit for bit (oracle/dual.hpp; about half a minute a
+direction on the host cores).  The particles start on the pressure clamp's kink, where the
+differences cannot converge; the tangent has no step size.
 
-    python tests/adjoint_c4.py [--directions 16] [--out FILE]
+    python tests/adjoint_c4.py [--directions 16] [--tangent K] [--out FILE]
 """
 import argparse
 import os
@@ -47,6 +52,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--directions", type=int, default=16)
     ap.add_argument("--every", type=int, default=20)
+    ap.add_argument("--tangent", type=int, default=0, help="directions also checked against the FP32 tangent")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     import torch
@@ -78,8 +84,24 @@ def main():
     lines = [f"loss {L:.6e}; forward {fwd_ms:.1f} ms, backward {bwd_ms:.1f} ms "
              f"(forward+adjoint {1 + bwd_ms / fwd_ms:.2f}x the taped forward), {sc.steps} steps, "
              f"checkpoint every {args.every}", ""]
-    lines.append("| direction | adjoint | FD eps 1e-3 | rel | FD eps 3e-3 | rel | FD eps 1e-2 | rel |")
-    lines.append("|---|---|---|---|---|---|---|---|")
+    tank = ((0.0, 0.0, 0.0), sc.tank)
+
+    def tangent(dvel, dparams):
+        """dL along the direction from the FP32 program's exact derivative."""
+        from oracle import py_oracle
+
+        P, _, dP, _, _ = py_oracle.tangent_run(sc.settings, tank, pos0, vel0, np.zeros(pos0.shape), dvel,
+                                               dparams=dparams, steps=sc.steps, dt=sc.dt, precision=32)
+        c = P.mean(axis=0)
+        return float(np.sum((2.0 * (c - target) / len(P)) * dP))
+
+    head = "| direction | adjoint | FD eps 1e-3 | rel | FD eps 3e-3 | rel | FD eps 1e-2 | rel |"
+    rule = "|---|---|---|---|---|---|---|---|"
+    if args.tangent:
+        head += " FP32 tangent | rel |"
+        rule += "---|---|"
+    lines += [head, rule]
+    exact = []
     rng = np.random.default_rng(11)
     worst = []
     for k in range(args.directions):
@@ -99,11 +121,19 @@ def main():
             rels.append(rel)
             row += [f"{num:.6e}", f"{rel:.2e}"]
         worst.append(min(rels))
+        if k < args.tangent:
+            t = tangent(d, np.zeros(5))
+            a = float(np.sum(dv0.astype(np.float64) * d))
+            exact.append(abs(a - t) / max(abs(t), 1e-300))
+            row += [f"{t:.6e}", f"{exact[-1]:.2e}"]
         lines.append("| " + " | ".join(row) + " |")
         print(lines[-1], flush=True)
     lines.append("")
     lines.append(f"best-of-steps relative error over the {args.directions} directions: median "
                  f"{np.median(worst):.2e}, max {np.max(worst):.2e}")
+    if exact:
+        lines.append(f"against the FP32 tangent over {len(exact)} directions: median {np.median(exact):.2e}, "
+                     f"max {np.max(exact):.2e}")
     s = sc.settings
     vrow = []
     for eps in (1e-4, 1e-3):
@@ -112,6 +142,9 @@ def main():
         dn = fluid.FluidSettings(**{**a, "viscosity": s.viscosity - eps})
         num = (forward_loss(up, sc, vel0, target) - forward_loss(dn, sc, vel0, target)) / (2 * eps)
         vrow.append(f"eps {eps:g}: FD {num:.6e}, rel {abs(params['viscosity'] - num) / max(abs(num), 1e-300):.2e}")
+    if args.tangent:
+        t = tangent(np.zeros(pos0.shape), np.array([1.0, 0.0, 0.0, 0.0, 0.0]))
+        vrow.append(f"FP32 tangent {t:.6e}, rel {abs(params['viscosity'] - t) / max(abs(t), 1e-300):.2e}")
     lines.append(f"viscosity: adjoint {params['viscosity']:.6e}; " + "; ".join(vrow))
     text = "\n".join(lines) + "\n"
     print(text)
