@@ -1750,8 +1750,7 @@ struct World {
         if (n == 0) return SLF_OK;
         SortPlan sp;
         SLF_TRY(plan_sort(sp, false));
-        enqueue_sort(to, sp, stream);
-        return SLF_OK;
+        return enqueue_sort(to, sp, stream);
     }
 
     // What a sort's launches take, fixed on the host before they are queued: the dense cell
@@ -1832,9 +1831,9 @@ struct World {
     }
 
     // the planned sort's launches on stream `on`
-    void enqueue_sort(int to, const SortPlan& sp, cudaStream_t on) {
+    int32_t enqueue_sort(int to, const SortPlan& sp, cudaStream_t on) {
         Params p = params();
-        cudaMemsetAsync(count.p, 0, (size_t(sp.volume) + 1) * 4, on);
+        SLF_CUDA(cudaMemsetAsync(count.p, 0, (size_t(sp.volume) + 1) * 4, on));
         timed("hash_count", bytes_per_particle::count_cells, [&] {
             launch_count_cells(p, pos[cpos].p, cells_of(cpos), sp.lo, sp.span, count.p, lin.p, cslot.p, on);
         });
@@ -1851,6 +1850,7 @@ struct World {
         if (sp.keys)
             timed("walk_order", bytes_per_particle::walk_order,
                   [&] { launch_walk_order(sp.volume, sp.span, count.p, wkeys.p, wsums.p, worder.p, on); });
+        return SLF_OK;
     }
 
     int32_t update_neighbors() {
@@ -2210,7 +2210,7 @@ struct World {
         uint64_t before = kernel_launches();
         SLF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
         auto record = [&]() -> int32_t {
-            enqueue_sort(a, sp, cs);
+            SLF_TRY(enqueue_sort(a, sp, cs));
             SLF_CUDA(cudaMemcpyAsync(d_status, h_reset, sizeof(Status), cudaMemcpyHostToDevice, cs));
             PairLists fl = fluid_lists(), wl = wall_lists();
             density_pass(p, a, fl, wl, rho[nid].p, cs);
@@ -2348,7 +2348,7 @@ struct World {
         SLF_TRY(plan_sort(sp, whole));
         if (whole) SLF_TRY(substep_graph(dt, p, a, b, nid, sp, whole));
         if (!whole) {
-            enqueue_sort(a, sp, stream);
+            SLF_TRY(enqueue_sort(a, sp, stream));
             SLF_TRY(reset_status());
             graph_solves = 0;
             launch_set_consts(consts(dt), d_consts, stream);
