@@ -366,6 +366,10 @@ def main():
     all_bytes = sum(v[2] for v in prof.values())
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / pk["hbm_gbs"], "peak_source": pk["source"], "traffic": traffic,
+                # the DRAM bytes the kernel moves (ncu, per launch; mostly neighbour lists) over its
+                # event-timed launch: how busy HBM is, beside the algorithmic fraction above
+                "traffic_gbs": traffic / (avg_ms / 1e3) / 1e9 if traffic else None,
+                "traffic_frac": traffic / (avg_ms / 1e3) / 1e9 / pk["hbm_gbs"] if traffic else None,
                 "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": avg_ms,
                 "share_of_kernel_time": ms / kernel_ms if kernel_ms else None,
                 "substep_algorithmic_gbs": (all_bytes / max(prof_substeps, 1)) * substeps / (sum(times_ms) / 1e3) / 1e9,
