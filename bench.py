@@ -7,7 +7,7 @@ which takes as many DFSPH substeps as the flow needs.  A timed step is one such 
 is substeps per second over all ranks, device-timed with CUDA events on the world's stream,
 with the particle state resident in HBM and L2 flushed (a 256 MiB write) before each step.
 Each DFSPH substep runs as one CUDA graph launch (sort, density, both solves with loops the
-device ends, viscosity, advance), recorded the second time its launches recur; the per-kernel
+device ends, viscosity, advance), recorded when its launches first occur; the per-kernel
 times of the roofline come from a second pass of the same steps with every launch timed by CUDA
 events (the profiler runs the substep launch by launch).
 `e2e` is the same metric through the C ABI with host-owned state: each step uploads positions

@@ -368,17 +368,19 @@ int32_t slf_profile_reset(slf_world* world);
  * the kernels its loop ran). */
 int32_t slf_kernel_launches(uint64_t* out);
 
-/* How a DFSPH step without a tape or profile launches its work.  mode = 2 (the default): each
- * substep is one CUDA graph launch (sort, density, both solves with loops the device ends,
- * viscosity, advance), recorded the second time the same launches recur and cached; substeps
- * the cache does not hold yet run as in mode 1.  mode = 1: each solve is one graph launch, the
+/* How a step without recorded solves or a profile launches its work.  mode = 2 (the default):
+ * each substep is one CUDA graph launch (sort and density; DFSPH: both solves with loops the
+ * device ends, viscosity, advance; WCSPH: the force and advance pass), recorded when its launches
+ * first occur and cached (once recorded graphs go unused, as when the particle count changes every
+ * tick, only launches that recur are recorded); substeps with terrain or coupled bodies, and those
+ * the cache does not hold, run as in mode 1.  mode = 1: each DFSPH solve is one graph launch, the
  * rest is launched eagerly.  mode = 0: the solves' launches are queued in batches with a host
  * check between them.  In every mode the host waits once a substep and the results are the same
  * bit for bit; the profiler and recorded solves take the batched launches.  Other modes:
  * SLF_ERR_INVALID_SETTINGS. */
 int32_t slf_solver_graphs(slf_world* world, int32_t mode);
 
-/* DFSPH substeps this world has run as one whole-substep graph launch (mode 2). */
+/* Substeps this world has run as one whole-substep graph launch (mode 2). */
 int32_t slf_graph_substeps(const slf_world* world, uint64_t* out);
 
 /* DFSPH solver iterations of the last substep: divergence and density (the per-solve split of

@@ -910,14 +910,16 @@ struct World {
             launch_density(p, fgrid, wgrid, pos[a].p, dwalls.p, fl, wl, rh, press.p, scaled.p, alpha.p, d_status,
                            tdev, ground_slopes(), on, mover_dev());
     }
-    void force_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid) {
+    void force_pass(const Params& p, const PairLists& fl, const PairLists& wl, int a, int b, int nid,
+                    cudaStream_t on = nullptr) {
+        if (!on) on = stream;
         if (fast())
             launch_wcsph_force_fast(p, d_consts, fl, wl, pos[a].p, cells_of(a), vel[a].p, rho[nid].p, press.p,
-                                    scaled.p, dwalls.p, pos[b].p, cells_of(b), vel[b].p, d_status, vel_pre, stream);
+                                    scaled.p, dwalls.p, pos[b].p, cells_of(b), vel[b].p, d_status, vel_pre, on);
         else
             launch_wcsph_force(p, d_consts, fl, wl, pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dwalls.p,
                                pos[b].p, vel[b].p, d_status, vel_pre, tdev, terrains.empty() ? nullptr : gslope.p,
-                               stream, mover_dev());
+                               on, mover_dev());
     }
     // cs, loop: the stream of a graph capture and the while-node handle of its solve loop
     void rate_pass(int which, const Params& p, const PairLists& fl, const PairLists& wl, int a, float4* v, int nid,
@@ -1905,14 +1907,21 @@ struct World {
     int32_t wcsph_substep(float dt, uint32_t& held) {
         Params p = params();
         int a = (cpos + 1) % 3, b = (cpos + 2) % 3;
-        SLF_TRY(sort_into(a));
         int nid = 1 - cid;
-        SLF_TRY(reset_status());
-        launch_set_consts(consts(dt), d_consts, stream);
-        PairLists fl = fluid_lists(), wl = wall_lists();
-        timed("density", bytes_per_particle::density_wcsph,
-              [&] { density_pass(p, a, fl, wl, rho[nid].p); });
-        timed("wcsph_force_advance", bytes_per_particle::wcsph_force, [&] { force_pass(p, fl, wl, a, b, nid); });
+        bool whole = whole_substeps();
+        SortPlan sp;
+        SLF_TRY(plan_sort(sp, whole));
+        if (whole) SLF_TRY(substep_graph(dt, p, a, b, nid, sp, whole));
+        if (!whole) {
+            SLF_TRY(enqueue_sort(a, sp, stream));
+            SLF_TRY(reset_status());
+            launch_set_consts(consts(dt), d_consts, stream);
+            PairLists fl = fluid_lists(), wl = wall_lists();
+            timed("density", bytes_per_particle::density_wcsph,
+                  [&] { density_pass(p, a, fl, wl, rho[nid].p); });
+            timed("wcsph_force_advance", bytes_per_particle::wcsph_force,
+                  [&] { force_pass(p, fl, wl, a, b, nid); });
+        }
         SLF_TRY(read_status());
         SLF_TRY(lists_fit());
         SLF_TRY(check_state());
@@ -2141,10 +2150,11 @@ struct World {
         return SLF_OK;
     }
 
-    // ---- the whole DFSPH substep as one graph -------------------------------------------------
-    // In graph mode 2 a DFSPH substep without a tape or profile is one graph launch: the sort and
-    // its walk order, the status reset (a copy from pinned memory), the density pass, both solves
-    // with their device-ended loops, viscosity and the advance.  The substep's constants (dt and
+    // ---- the whole substep as one graph ------------------------------------------------------
+    // In graph mode 2 a substep without a recorded solve or profile is one graph launch: the sort
+    // and its walk order, the status reset (a copy from pinned memory), the density pass, then for
+    // DFSPH both solves with their device-ended loops, viscosity and the advance, for WCSPH the
+    // force and advance pass.  The substep's constants (dt and
     // what follows from it) are read from device memory, written by one launch ahead of the
     // graph, so a graph holds across substeps whose dt changes.  The cell table's box is the
     // container's (plan_sort, stable), so slot rotation alone (3 position slots x 2 id slots)
@@ -2166,8 +2176,10 @@ struct World {
     static constexpr uint32_t kUnusedGraphs = 2;     // ... after which keys wait for a second sighting
 
     bool whole_substeps() const {
+        // (the adjoint's recomputed substeps, which redirect the sort and record velocities, launch
+        // eagerly)
         return graph_mode >= 2 && !prof.on && s.max_iterations <= kGraphMaxIterations && skip_job < 0 &&
-               terrains.empty() && m_pos.empty() && n > 0;
+               terrains.empty() && m_pos.empty() && n > 0 && !sort_dest && !vel_pre;
     }
     void drop_substep_graphs() {
         for (auto& g : substep_graphs)
@@ -2179,6 +2191,7 @@ struct World {
     std::vector<uint8_t> substep_key(const Params& p, int a, int b, int nid, const SortPlan& sp) {
         static_assert(sizeof(GridDev) == 48, "GridDev has no padding");
         std::vector<uint8_t> k;
+        key_add(k, int32_t(s.solver));
         key_add(k, int32_t(fast()));
         key_add(k, int32_t(rel()));
         key_add(k, int32_t(warm_on()));
@@ -2214,6 +2227,10 @@ struct World {
             SLF_CUDA(cudaMemcpyAsync(d_status, h_reset, sizeof(Status), cudaMemcpyHostToDevice, cs));
             PairLists fl = fluid_lists(), wl = wall_lists();
             density_pass(p, a, fl, wl, rho[nid].p, cs);
+            if (s.solver == SLF_SOLVER_WCSPH) {
+                force_pass(p, fl, wl, a, b, nid, cs);
+                return SLF_OK;
+            }
             uint32_t pre = 0;
             SLF_TRY(capture_solve(0, p, a, vel[a].p, nid, fl, wl, SolveRec{nullptr, nullptr}, pre));
             viscous_pass(p, fl, wl, a, b, nid, cs);
@@ -2235,8 +2252,8 @@ struct World {
         cudaError_t made = cudaGraphInstantiate(&g.exec, graph, 0);
         cudaGraphDestroy(graph);
         SLF_CUDA(made);
-        // each solve's loop body (a push and a check) counts per iteration when it runs
-        g.outside = uint32_t(recorded - 4);
+        // each DFSPH solve's loop body (a push and a check) counts per iteration when it runs
+        g.outside = uint32_t(recorded - (s.solver == SLF_SOLVER_DFSPH ? 4 : 0));
         return SLF_OK;
     }
 
@@ -2276,7 +2293,7 @@ struct World {
         launch_set_consts(consts(dt), d_consts, stream);
         SLF_CUDA(cudaGraphLaunch(hit->exec, stream));
         note_launches(hit->outside);
-        graph_solves = 3;
+        graph_solves = s.solver == SLF_SOLVER_DFSPH ? 3u : 0u;
         ++graph_substeps;
         ran = true;
         return SLF_OK;

@@ -436,14 +436,14 @@ class FluidWorld:
         _check(_lib.slf_profile_enable(self._h, 1 if on else 0))
 
     def solver_graphs(self, mode=2):
-        """How DFSPH steps launch: 2 (the default, also True) each substep as one CUDA graph,
+        """How steps launch: 2 (the default, also True) each substep as one CUDA graph,
         1 each solve as one graph whose loop the device ends, 0 (also False) solves as batches
         of launches with a host check between them; the results are identical."""
         mode = 2 if mode is True else 0 if mode is False else int(mode)
         _check(_lib.slf_solver_graphs(self._h, mode))
 
     def graph_substeps(self) -> int:
-        """DFSPH substeps this world ran as one whole-substep graph launch."""
+        """Substeps this world ran as one whole-substep graph launch."""
         out = ctypes.c_uint64(0)
         _check(_lib.slf_graph_substeps(self._h, ctypes.byref(out)))
         return out.value

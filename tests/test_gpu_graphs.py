@@ -160,3 +160,24 @@ def test_a_substep_whose_lists_outgrow_their_room_runs_again_as_the_restatement(
         a, b = g.step(1e-3), o.step(1e-3)
         assert (a.substeps, a.iterations, a.held_back) == (b.substeps, b.iterations, b.held_back), k
         assert g.state_hash() == o.state_hash(), k
+
+
+@pytest.mark.parametrize("arithmetic", [Arithmetic.EXACT, Arithmetic.FAST])
+def test_whole_wcsph_substeps_equal_eager_substeps_and_the_restatement(gpu_lib, oracle_lib, arithmetic):
+    # a WCSPH substep as one graph (sort, density, force and advance) against the same launches
+    # queued one by one, and (EXACT) against the restatement
+    s = FluidSettings(solver=FluidSolver.WCSPH, spacing=0.02, support=2.0, arithmetic=arithmetic)
+    g, e = pair(gpu_lib, s, dam_build())
+    subs = 0
+    for k in range(30):
+        a, b = g.step(1e-3), e.step(1e-3)
+        assert (a.substeps, a.held_back) == (b.substeps, b.held_back), k
+        subs += a.substeps
+    assert g.state_hash() == e.state_hash()
+    assert g.graph_substeps() == subs and e.graph_substeps() == 0
+    if arithmetic == Arithmetic.EXACT:
+        o = oracle_lib.OracleWorld(s)
+        dam_build()(o)
+        for _ in range(30):
+            o.step(1e-3)
+        assert g.state_hash() == o.state_hash()
