@@ -345,6 +345,61 @@ __device__ __forceinline__ void relist(const PairLists& l, uint32_t row, uint32_
     }
 }
 
+// One warp lists row `row`'s neighbours in grid g, in each_near's order: lanes 0-26 take the 27
+// cells' ranges (dz outer, dy, dx inner) and sum their lengths; then 32 consecutive candidates of
+// the cells laid end to end are tested at a time, a lane finding its cell by a binary search over
+// the sums, and the kept ones are written in order through a ballot.  The test is each_in_cell's,
+// so the list is the one-thread walk's entry for entry.  Returns the count (every lane).
+__device__ __forceinline__ uint32_t warp_list_near(const Params& p, const GridDev& g, const float4* __restrict__ pts,
+                                                   int3 cell, float ax, float ay, float az, const PairLists& l,
+                                                   uint32_t row, uint32_t lane) {
+    if (g.mode == 0) return 0u;
+    uint32_t b = 0, len = 0;
+    if (lane < 27u) {
+        int dz = int(lane / 9u) - 1, dy = int((lane / 3u) % 3u) - 1, dx = int(lane % 3u) - 1;
+        uint32_t e = 0;
+        if (g.range((long long)cell.x + dx, (long long)cell.y + dy, (long long)cell.z + dz, b, e) && e > b) len = e - b;
+    }
+    uint32_t incl = len;  // inclusive prefix sum of the lengths over the lanes
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t up = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= uint32_t(o)) incl += up;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t m = 0;
+    for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
+        uint32_t t = t0 + lane;
+        // the first cell whose inclusive sum exceeds t (cells 0-26; lanes past the end search too)
+        uint32_t lo = 0, hi = 26;
+#pragma unroll
+        for (int step = 0; step < 5; ++step) {
+            uint32_t mid = (lo + hi) >> 1;
+            uint32_t at = __shfl_sync(0xffffffffu, incl, mid);
+            if (t < at) hi = mid;
+            else lo = mid + 1u;
+        }
+        uint32_t k = lo < 26u ? lo : 26u;
+        uint32_t kb = __shfl_sync(0xffffffffu, b, k), kincl = __shfl_sync(0xffffffffu, incl, k),
+                 klen = __shfl_sync(0xffffffffu, len, k);
+        bool keep = false;
+        uint32_t j = 0;
+        if (t < total) {
+            j = kb + (t - (kincl - klen));
+            float4 q = __ldg(&pts[j]);
+            float ox = q.x - ax, oy = q.y - ay, oz = q.z - az;
+            keep = dot3(ox, oy, oz, ox, oy, oz) < p.reach;
+        }
+        uint32_t mask = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            uint32_t at = m + __popc(mask & ((1u << lane) - 1u));
+            if (at < l.cap) l.e[l.at(row, at)].x = j;
+        }
+        m += __popc(mask);
+    }
+    return m;
+}
+
 // ---- densities (mod.rs:621-675) and the substep's neighbour lists, with WCSPH pressure
 // (step.rs:147-172) or the DFSPH factors (dfsph.rs:108-163) --------------------------------
 
@@ -441,6 +496,124 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
     }
 }
 
+// The density pass for scenes too small to fill the GPU a thread a particle: a warp a row.  The
+// lists come from warp_list_near; each lane takes every 32nd listed neighbour's terms, and the
+// sums run in list order, one term after the other through shuffles, so every sum and factor is
+// k_density's bit for bit.  Body points and ground are taken by every lane alike.
+template <int SOLVER>
+__global__ void __launch_bounds__(kBlock) k_density_warp(Params p, GridDev fg, GridDev wg,
+                                                         const float4* __restrict__ pos, const float4* __restrict__ walls,
+                                                         PairLists fl, PairLists wl, float* __restrict__ rho,
+                                                         float* __restrict__ press, float* __restrict__ scaled,
+                                                         float* __restrict__ alpha, Status* st, TerrainDev T,
+                                                         float4* __restrict__ slope, MoverDev M) {
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+    uint32_t compressed = 0, longest = 0;
+    if (row < p.n) {  // whole warps
+        const uint32_t i = fl.particle(row);
+        const float4 a = pos[i];
+        const int3 cell = cell_of(p, a.x, a.y, a.z);
+        const uint32_t nf = warp_list_near(p, fg, pos, cell, a.x, a.y, a.z, fl, row, lane);
+        const uint32_t nw = warp_list_near(p, wg, walls, cell, a.x, a.y, a.z, wl, row, lane);
+        if (lane == 0) {
+            fl.count[row] = nf;
+            wl.count[row] = nw;
+        }
+        longest = nf > nw ? nf : nw;
+        __syncwarp();  // the entries other lanes wrote
+        float sum = 0.0f, wsum = 0.0f;
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f, squares = 0.0f;
+        const uint32_t mf = nf < fl.cap ? nf : fl.cap, mw = nw < wl.cap ? nw : wl.cap;
+        for (uint32_t k0 = 0; k0 < mf; k0 += 32u) {
+            const uint32_t k = k0 + lane;
+            float v = 0.0f, px = 0.0f, py = 0.0f, pz = 0.0f, sq = 0.0f;
+            if (k < mf) {
+                uint2* ent = fl.e + fl.at(row, k);
+                const uint32_t j = ent->x;
+                const float4 q = __ldg(&pos[j]);
+                float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
+                float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
+                v = kernel_value(p, d);
+                float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
+                if (SOLVER == 1) {
+                    float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+                    px = (rx * g) * p.mass, py = (ry * g) * p.mass, pz = (rz * g) * p.mass;
+                    sq = dot3(px, py, pz, px, py, pz);
+                }
+                *ent = make_uint2(j, __float_as_uint(g));
+            }
+            const uint32_t here = mf - k0 < 32u ? mf - k0 : 32u;
+            for (uint32_t t = 0; t < here; ++t) {
+                sum += __shfl_sync(0xffffffffu, v, t);
+                if (SOLVER == 1) {
+                    sx = sx + __shfl_sync(0xffffffffu, px, t);
+                    sy = sy + __shfl_sync(0xffffffffu, py, t);
+                    sz = sz + __shfl_sync(0xffffffffu, pz, t);
+                    squares += __shfl_sync(0xffffffffu, sq, t);
+                }
+            }
+        }
+        for (uint32_t k0 = 0; k0 < mw; k0 += 32u) {
+            const uint32_t k = k0 + lane;
+            float v = 0.0f, px = 0.0f, py = 0.0f, pz = 0.0f;
+            if (k < mw) {
+                uint2* ent = wl.e + wl.at(row, k);
+                const uint32_t j = ent->x;
+                const float4 q = __ldg(&walls[j]);
+                float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
+                float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
+                v = kernel_value(p, d);
+                float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
+                if (SOLVER == 1) {
+                    float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+                    px = (rx * g) * p.mass, py = (ry * g) * p.mass, pz = (rz * g) * p.mass;
+                }
+                *ent = make_uint2(j, __float_as_uint(g));
+            }
+            const uint32_t here = mw - k0 < 32u ? mw - k0 : 32u;
+            for (uint32_t t = 0; t < here; ++t) {
+                wsum += __shfl_sync(0xffffffffu, v, t);
+                if (SOLVER == 1) {
+                    sx = sx + __shfl_sync(0xffffffffu, px, t);
+                    sy = sy + __shfl_sync(0xffffffffu, py, t);
+                    sz = sz + __shfl_sync(0xffffffffu, pz, t);
+                }
+            }
+        }
+        // the coupled bodies' points, in their list order (mod.rs:648-656)
+        float msum = 0.0f;
+        if (M.count)
+            each_near(p, M.grid, M.pos, cell, a.x, a.y, a.z, [&](uint32_t, float4 q) {
+                float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
+                msum += kernel_value(p, sqrtf(dot3(ox, oy, oz, ox, oy, oz)));
+            });
+        float3 gslope;
+        float ground = T.regions ? ground_near(T, a.x, a.y, a.z, gslope) : 0.0f;
+        float density = p.mass * (sum + wsum + msum) + ground;
+        if (lane == 0) {
+            rho[i] = density;
+            if (slope) slope[i] = make_float4(gslope.x, gslope.y, gslope.z, 0.0f);
+            if (SOLVER == 0) {
+                float ratio = fminf(density / p.rest, 1.1f);
+                float pressure = fmaxf(p.stiffness * (pow7(ratio) - 1.0f), 0.0f);
+                press[i] = pressure;
+                scaled[i] = pressure / (density * density);
+            } else {
+                float total = dot3(sx, sy, sz, sx, sy, sz) + squares;
+                alpha[i] = total > 0.0f ? 1.0f / total : 0.0f;
+            }
+        }
+        float c = density / p.rest - 1.0f;
+        if (c > 0.0f) compressed = __float_as_uint(c);
+    }
+    compressed = block_reduce(compressed, MaxU(), 0u);
+    longest = block_reduce(longest, MaxU(), 0u);
+    if (threadIdx.x == 0) {
+        if (compressed) atomicMax(&st->maxcomp_bits, compressed);
+        if (longest) atomicMax(&st->list_max, longest);
+    }
+}
+
 // Walks particle i's list: f(j, g, q) for each neighbour in list order, q = pts[j].  Entries are
 // taken kListUnroll at a time, their gathers issued before any is used, and the next group's
 // entries are requested before this group is used; past the end of the list the last entry is
@@ -457,6 +630,10 @@ constexpr int kListUnroll = SLF_LIST_UNROLL;
 #endif
 #ifndef SLF_RATE_MIN_BLOCKS
 #define SLF_RATE_MIN_BLOCKS 4
+#endif
+// particle counts up to which the density pass runs a warp a particle (k_density_warp)
+#ifndef SLF_WARP_LIST_MAX
+#define SLF_WARP_LIST_MAX 131072u
 #endif
 
 
@@ -1240,6 +1417,16 @@ void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
                     Status* st, const TerrainDev& T, float4* slope, cudaStream_t s, const MoverDev& M) {
     if (!p.n) return;
+    if (p.n <= SLF_WARP_LIST_MAX) {
+        // a scene this small leaves most SMs idle a thread a particle: a warp a particle
+        if (p.solver == 0)
+            k_density_warp<0><<<blocks_for(p.n * 32u), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press,
+                                                                       scaled, alpha, st, T, slope, M);
+        else
+            k_density_warp<1><<<blocks_for(p.n * 32u), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press,
+                                                                       scaled, alpha, st, T, slope, M);
+        return;
+    }
     if (p.solver == 0)
         k_density<0><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
                                                         T, slope, M);
