@@ -923,6 +923,145 @@ __global__ void k_cells_wet(GridDev g, int3 lo, int3 hi, uint32_t* wet) {
 
 // ---- WCSPH: forces, velocity update and advance in one pass (step.rs:159-223, 305-339) -----
 
+// Subtracts, in list order, every lane's (tx, ty, tz) of this round from (px, py, pz): lane t's
+// term after lane t - 1's, as the one-thread walk subtracts them.  A lane without a term holds
+// +0, whose subtraction leaves any value as it was.
+__device__ __forceinline__ void take_in_order(float& px, float& py, float& pz, float tx, float ty, float tz,
+                                              uint32_t here) {
+    for (uint32_t t = 0; t < here; ++t) {
+        px = px - __shfl_sync(0xffffffffu, tx, t);
+        py = py - __shfl_sync(0xffffffffu, ty, t);
+        pz = pz - __shfl_sync(0xffffffffu, tz, t);
+    }
+}
+
+// The WCSPH force and advance pass for scenes too small to fill the GPU a thread a particle
+// (k_density_warp made the lists): a warp a row, the pair terms a lane a neighbour, subtracted in
+// list order, so every sum is k_wcsph_force's bit for bit; lane 0 advances the particle.  Without
+// terrain or coupled bodies (their terms stay with k_wcsph_force).
+__global__ void __launch_bounds__(kBlock) k_wcsph_force_warp(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                             PairLists wl, const float4* __restrict__ pos,
+                                                             const float4* __restrict__ vel,
+                                                             const float* __restrict__ rho,
+                                                             const float* __restrict__ press,
+                                                             const float* __restrict__ scaled,
+                                                             const float4* __restrict__ walls,
+                                                             float4* __restrict__ pos_out, float4* __restrict__ vel_out,
+                                                             Status* st, float4* __restrict__ vel_pre) {
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+    const bool valid = row < p.n;  // whole warps
+    int3 nc = make_int3(0, 0, 0);
+    float speed = 0.0f;
+    uint32_t held = 0, bad = 0;
+    if (valid) {
+        const uint32_t i = fl.particle(row);
+        const float dt = sc->dt;
+        const float visc = sc->viscosity;
+        float4 a = pos[i];
+        float4 v = vel[i];
+        const float density = rho[i];
+        const float own = scaled[i];
+        float px = 0.0f, py = 0.0f, pz = 0.0f;
+        const uint32_t nf = fl.count[row], nw = wl.count[row];
+        const uint32_t mf = nf < fl.cap ? nf : fl.cap, mw = nw < wl.cap ? nw : wl.cap;
+        for (uint32_t k0 = 0; k0 < mf; k0 += 32u) {
+            const uint32_t k = k0 + lane;
+            float tx = 0.0f, ty = 0.0f, tz = 0.0f;
+            if (k < mf) {
+                const uint2 en = SLF_LIST_LOAD(fl.e + fl.at(row, k));
+                const uint32_t j = en.x;
+                const float g = __uint_as_float(en.y);
+                const float4 q = __ldg(&pos[j]), w = __ldg(&vel[j]);
+                float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+                float squared = dot3(rx, ry, rz, rx, ry, rz);
+                if (squared > 0.0f) {
+                    float gx = rx * g, gy = ry * g, gz = rz * g;
+                    float toward = fminf(dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx, ry, rz), 0.0f);
+                    float damp = -visc * toward / (squared + p.soften) * 2.0f / (density + __ldg(&rho[j]));
+                    float s = p.mass * (own + __ldg(&scaled[j]) + damp);
+                    tx = gx * s, ty = gy * s, tz = gz * s;
+                }
+            }
+            take_in_order(px, py, pz, tx, ty, tz, mf - k0 < 32u ? mf - k0 : 32u);
+        }
+        const float mirrored = own + press[i] / p.rest_sq;
+        // the walls' pressure, then wall_viscous's two walks (its normal, then its damping)
+        float awx = 0.0f, awy = 0.0f, awz = 0.0f;
+        for (uint32_t k0 = 0; k0 < mw; k0 += 32u) {
+            const uint32_t k = k0 + lane;
+            float tx = 0.0f, ty = 0.0f, tz = 0.0f, nx = 0.0f, ny = 0.0f, nz = 0.0f;
+            if (k < mw) {
+                const uint2 en = SLF_LIST_LOAD(wl.e + wl.at(row, k));
+                const float g = __uint_as_float(en.y);
+                const float4 q = __ldg(&walls[en.x]);
+                float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+                float s = p.mass * mirrored;
+                tx = (rx * g) * s, ty = (ry * g) * s, tz = (rz * g) * s;
+                nx = -(rx * g), ny = -(ry * g), nz = -(rz * g);
+            }
+            const uint32_t here = mw - k0 < 32u ? mw - k0 : 32u;
+            take_in_order(px, py, pz, tx, ty, tz, here);
+            for (uint32_t t = 0; t < here; ++t) {
+                awx = awx + __shfl_sync(0xffffffffu, nx, t);
+                awy = awy + __shfl_sync(0xffffffffu, ny, t);
+                awz = awz + __shfl_sync(0xffffffffu, nz, t);
+            }
+        }
+        float wx = 0.0f, wy = 0.0f, wz = 0.0f;
+        if (nw != 0) {
+            // wall_viscous (step.rs:262-301): normalize_or(ZERO) dividing by the length
+            float len = sqrtf(dot3(awx, awy, awz, awx, awy, awz));
+            float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+            if (isfinite(len) && len > 0.0f) {
+                ux = awx / len;
+                uy = awy / len;
+                uz = awz / len;
+            }
+            float kk = fminf(dot3(v.x, v.y, v.z, ux, uy, uz), 0.0f);
+            float ix = ux * kk, iy = uy * kk, iz = uz * kk;
+            const float wall_visc = sc->wall_viscosity;
+            for (uint32_t k0 = 0; k0 < mw; k0 += 32u) {
+                const uint32_t k = k0 + lane;
+                float tx = 0.0f, ty = 0.0f, tz = 0.0f;
+                if (k < mw) {
+                    const uint2 en = SLF_LIST_LOAD(wl.e + wl.at(row, k));
+                    const float g = __uint_as_float(en.y);
+                    const float4 q = __ldg(&walls[en.x]);
+                    float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+                    float toward = dot3(ix, iy, iz, rx, ry, rz);
+                    if (toward < 0.0f) {
+                        float squeeze = toward / (dot3(rx, ry, rz, rx, ry, rz) + p.soften);
+                        float damp = -wall_visc * squeeze / density;
+                        float s = p.mass * damp;
+                        tx = (rx * g) * s, ty = (ry * g) * s, tz = (rz * g) * s;
+                    }
+                }
+                take_in_order(wx, wy, wz, tx, ty, tz, mw - k0 < 32u ? mw - k0 : 32u);
+            }
+        }
+        if (lane == 0) {
+            float ax = (px + wx) + p.gravity.x, ay = (py + wy) + p.gravity.y, az = (pz + wz) + p.gravity.z;
+            v.x = v.x + ax * dt;
+            v.y = v.y + ay * dt;
+            v.z = v.z + az * dt;
+            float4 pre = v;
+            advance_one(p, dt, a, v, held, bad, TerrainDev{});
+            if (vel_pre) {
+                // the velocity before the wall zeroed any component, and which ones it zeroed
+                uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
+                pre.w = __uint_as_float(flags);
+                vel_pre[i] = pre;
+            }
+            pos_out[i] = a;
+            vel_out[i] = v;
+            nc = cell_of(p, a.x, a.y, a.z);
+            speed = sqrtf(dot3(v.x, v.y, v.z, v.x, v.y, v.z));
+            if (!(speed == speed)) speed = 0.0f;
+        }
+    }
+    fold_advance_stats(st, valid && lane == 0, nc, speed, held, bad);
+}
+
 __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                         PairLists wl, const float4* __restrict__ pos,
                                                         const float4* __restrict__ vel, const float* __restrict__ rho,
@@ -1440,9 +1579,14 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
                         const float* scaled, const float4* walls, float4* pos_out, float4* vel_out, Status* st,
                         float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s,
                         const MoverDev& M) {
-    if (p.n)
-        k_wcsph_force<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled, walls, pos_out,
-                                                         vel_out, st, vel_pre, T, slope, M);
+    if (!p.n) return;
+    if (p.n <= SLF_WARP_LIST_MAX && T.regions == 0 && M.count == 0 && slope == nullptr) {
+        k_wcsph_force_warp<<<blocks_for(p.n * 32u), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled,
+                                                                    walls, pos_out, vel_out, st, vel_pre);
+        return;
+    }
+    k_wcsph_force<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled, walls, pos_out,
+                                                     vel_out, st, vel_pre, T, slope, M);
 }
 
 void launch_mover_count(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos,
