@@ -631,10 +631,7 @@ constexpr int kListUnroll = SLF_LIST_UNROLL;
 #ifndef SLF_RATE_MIN_BLOCKS
 #define SLF_RATE_MIN_BLOCKS 4
 #endif
-// particle counts up to which the density pass runs a warp a particle (k_density_warp)
-#ifndef SLF_WARP_LIST_MAX
-#define SLF_WARP_LIST_MAX 131072u
-#endif
+
 
 
 // Where a walk finds its neighbours (the global arrays, read through the L1).
@@ -1556,7 +1553,7 @@ void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
                     Status* st, const TerrainDev& T, float4* slope, cudaStream_t s, const MoverDev& M) {
     if (!p.n) return;
-    if (p.n <= SLF_WARP_LIST_MAX) {
+    if (p.n <= kWarpPassMax) {
         // a scene this small leaves most SMs idle a thread a particle: a warp a particle
         if (p.solver == 0)
             k_density_warp<0><<<blocks_for(p.n * 32u), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press,
@@ -1580,7 +1577,7 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
                         float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s,
                         const MoverDev& M) {
     if (!p.n) return;
-    if (p.n <= SLF_WARP_LIST_MAX && T.regions == 0 && M.count == 0 && slope == nullptr) {
+    if (p.n <= kWarpPassMax && T.regions == 0 && M.count == 0 && slope == nullptr) {
         k_wcsph_force_warp<<<blocks_for(p.n * 32u), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled,
                                                                     walls, pos_out, vel_out, st, vel_pre);
         return;

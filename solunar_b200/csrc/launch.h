@@ -34,6 +34,10 @@ void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start,
 // start is the sort's cell table (volume + 1), bcount holds walk_order_keys(span) + 1 words,
 // tile_sums scan_tiles(walk_order_keys(span)) + 1, order n.
 size_t walk_order_keys(int3 span);
+// Particle counts up to which the EXACT density pass, and the WCSPH force pass without terrain or
+// coupled bodies, run a warp a particle (k_density_warp, k_wcsph_force_warp): such scenes leave
+// most SMs idle a thread a particle.  Those passes need no walk order.
+constexpr uint32_t kWarpPassMax = 131072u;
 void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32_t* bcount, uint32_t* tile_sums,
                        uint32_t* order, cudaStream_t s);
 

@@ -1810,10 +1810,13 @@ struct World {
         SLF_TRY(ensure_work_buffers());
         SLF_TRY(count.ensure(size_t(sp.volume) + 1, 0, stream));
         SLF_TRY(tiles.ensure(scan_tiles(sp.volume) + 1, 0, stream));
-        // the walk order of this sort's lists (identity where its key space would not fit 32 bits)
+        // the walk order of this sort's lists (identity where its key space would not fit 32 bits,
+        // and where every pass over the lists runs a warp a particle)
         size_t keys = walk_order_keys(sp.span);
         sp.keys = 0;
-        if (keys < (size_t(1) << 31)) {
+        bool warp_passes = !fast() && s.solver == SLF_SOLVER_WCSPH && n <= kWarpPassMax && terrains.empty() &&
+                           m_pos.empty();
+        if (keys < (size_t(1) << 31) && !warp_passes) {
             SLF_TRY(worder.ensure(n, 0, stream));
             SLF_TRY(wkeys.ensure(keys + 1, 0, stream));
             SLF_TRY(wsums.ensure(scan_tiles(uint32_t(keys)) + 1, 0, stream));
