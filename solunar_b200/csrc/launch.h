@@ -35,9 +35,12 @@ void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start,
 // tile_sums scan_tiles(walk_order_keys(span)) + 1, order n.
 size_t walk_order_keys(int3 span);
 // Particle counts up to which the EXACT density pass, and the WCSPH force pass without terrain or
-// coupled bodies, run a warp a particle (k_density_warp, k_wcsph_force_warp): such scenes leave
-// most SMs idle a thread a particle.  Those passes need no walk order.
-constexpr uint32_t kWarpPassMax = 131072u;
+// coupled bodies, run a warp a particle (k_density_warp, k_wcsph_force_warp), which then needs no
+// walk order: below one 256-thread block per SM (148 on B200) a thread a particle leaves SMs idle
+// and each thread walks its candidates in one long chain of loads.  Measured: 8k particles at
+// support 4, density 392 -> 92 us and force 218 -> 67 us; 250k and 1M particles at support 2,
+// density 219 -> 547 us and 562 -> 2250 us, so larger scenes keep a thread a particle.
+constexpr uint32_t kWarpPassMax = 32768u;
 void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32_t* bcount, uint32_t* tile_sums,
                        uint32_t* order, cudaStream_t s);
 
