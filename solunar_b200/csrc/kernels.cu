@@ -1553,8 +1553,9 @@ void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
                     Status* st, const TerrainDev& T, float4* slope, cudaStream_t s, const MoverDev& M) {
     if (!p.n) return;
-    if (p.n <= kWarpPassMax) {
-        // a scene this small leaves most SMs idle a thread a particle: a warp a particle
+    if (p.n <= kWarpPassMax && T.regions == 0 && M.count == 0) {
+        // a scene this small leaves most SMs idle a thread a particle: a warp a particle (terrain
+        // and body points, which every lane would take alike, stay a thread a particle)
         if (p.solver == 0)
             k_density_warp<0><<<blocks_for(p.n * 32u), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press,
                                                                        scaled, alpha, st, T, slope, M);

@@ -34,7 +34,7 @@ void launch_rank_reorder(uint32_t n, const uint32_t* lin, const uint32_t* start,
 // start is the sort's cell table (volume + 1), bcount holds walk_order_keys(span) + 1 words,
 // tile_sums scan_tiles(walk_order_keys(span)) + 1, order n.
 size_t walk_order_keys(int3 span);
-// Particle counts up to which the EXACT density pass, and the WCSPH force pass without terrain or
+// Particle counts up to which the EXACT density pass and the WCSPH force pass, without terrain or
 // coupled bodies, run a warp a particle (k_density_warp, k_wcsph_force_warp), which then needs no
 // walk order: below one 256-thread block per SM (148 on B200) a thread a particle leaves SMs idle
 // and each thread walks its candidates in one long chain of loads.  Measured: 8k particles at
