@@ -1,14 +1,15 @@
 """The reference's own fluid tests, restated against both implementations.
 
-The reference stores no golden vectors for this path; its tests are properties.  Each test
+The reference stores no golden vectors for this path apart from the Martin & Moyce front table
+its dam-break test embeds (tests/golden/martin_moyce.json); its tests are properties.  Each test
 here restates one of them (src/fluid/mod.rs:742-973, src/fluid/step.rs:342-584) with the
 reference's thresholds.  Tests that take `backend` run against the CPU restatement (pinning the
 oracle) and, marked `gpu`, against the CUDA library; the rest probe parts only the restatement
 exposes (kernel samples, the cell table, thread counts).
 """
+import json
 import math
 import os
-import re
 
 import numpy as np
 import pytest
@@ -16,7 +17,6 @@ import pytest
 from solunar_b200.abi import FluidSettings, FluidSolver, PhysicsError
 from solunar_b200 import scenes
 
-from conftest import REFERENCE
 
 TICK = np.float32(1.0 / 60.0)
 
@@ -247,23 +247,17 @@ def test_a_column_collapses_but_never_outruns_the_ideal_front(backend):
 
 def martin_moyce_table():
     """The digitised Martin & Moyce (1952) front table embedded in the reference's own test
-    (src/fluid/step.rs:447-460), read from the reference's source at test time."""
-    path = os.path.join(REFERENCE, "src/fluid/step.rs")
-    if not os.path.exists(path):
-        return None
-    text = open(path).read()
-    block = text[text.index("const MARTIN_MOYCE"):]
-    block = block[: block.index("];")]
-    pairs = re.findall(r"\(([0-9.]+),\s*([0-9.]+)\)", block)
-    return [(float(a), float(b)) for a, b in pairs]
+    (src/fluid/step.rs:447-460), extracted into tests/golden/martin_moyce.json by
+    tests/golden/make_martin_moyce.py."""
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "martin_moyce.json")) as f:
+        return [(float(a), float(b)) for a, b in json.load(f)["pairs"]]
 
 
 @pytest.mark.slow
 def test_the_dam_break_front_follows_martin_and_moyce(backend):
     # src/fluid/step.rs:462-507
     table = martin_moyce_table()
-    if not table:
-        pytest.skip("reference sources not present")
+    assert len(table) == 10
     width = 0.3
     spacing = np.float32(0.3) / np.float32(18.0)
     w = backend(spacing=float(spacing))
@@ -368,3 +362,25 @@ def test_the_compensated_residual_stops_the_solves_where_the_reference_sum_does(
         assert a.iterations == b.iterations
         assert ref.last_iterations() == comp.last_iterations()
     assert ref.state_hash() == comp.state_hash()
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("name", ["dfsph_dam_250k", "dfsph_dam_250k_c2"])
+def test_the_compensated_residual_stops_where_the_reference_sum_does_at_250k(oracle_lib, name):
+    # The same check on the 250,000-particle dams, solve by solve, through the steps where the
+    # falling column drives the density solve to 10-15 iterations: the reference's f32 sum over
+    # a quarter of a million errors and the compensated FP64 sum stop at the same iteration.
+    # (tests/test_gpu_parity_at_scale.py makes the same comparison at one million particles.)
+    sc = getattr(scenes, name)()
+    ref = oracle_lib.OracleWorld(sc.settings, residual_sum=0)
+    comp = oracle_lib.OracleWorld(sc.settings, residual_sum=1)
+    sc.build(ref)
+    sc.build(comp)
+    counts = []
+    for _ in range(12):
+        ref.step(sc.dt)
+        comp.step(sc.dt)
+        assert ref.last_iterations() == comp.last_iterations()
+        counts.append(comp.last_iterations()[1])
+    assert ref.state_hash() == comp.state_hash()
+    assert max(counts) >= 4
