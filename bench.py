@@ -69,6 +69,8 @@ def parse():
                     help="steps of the forward+adjoint measurement (0 skips it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed CPU work in the baseline")
+    ap.add_argument("--no-density-error", action="store_true",
+                    help="skip the FP64 restatement run behind the density error of the timed steps")
     return ap.parse_args()
 
 
@@ -213,19 +215,53 @@ def cpu_baseline(sc, budget_s: float, state=None, threads: int = 0) -> dict:
         w.add_particles(state[0], state[1])
         where = "from the state the GPU's timed steps ended on"
     w.update_neighbors()
-    substeps = 0
+    substeps = iterations = 0
     t0 = time.perf_counter()
     steps = 0
     while True:
         r = w.step(sc.dt)
         substeps += r.substeps
+        iterations += r.iterations
         steps += 1
         if time.perf_counter() - t0 >= budget_s:
             break
     dt = time.perf_counter() - t0
     return {"value": substeps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "solver_iterations_per_substep": iterations / max(substeps, 1),
             "sample": f"{steps} steps ({substeps} substeps) of the {sc.particles}-particle scene {where}, "
-                      f"{dt:.1f} s on {cores} threads (C++ float restatement, OpenMP)"}
+                      f"{dt:.1f} s on {cores} threads (C++ float restatement, OpenMP, the reference's f32 "
+                      f"residual sum)"}
+
+
+def density_error(sc, steps: int, gpu_ids, gpu_rho, threads: int = 0) -> dict:
+    """Density error of the GPU run against the FP64 restatement of the same method: the double
+    oracle from the same initial state over the same steps (warm-up and timed), then
+    |rho - rho_64| / rho_0 particle by particle (matched by id)."""
+    import numpy as np
+
+    from oracle import py_oracle
+
+    py_oracle.build()
+    cores = threads or os.cpu_count()
+    w = py_oracle.OracleWorld(sc.settings, precision=64, residual_sum=1, threads=cores)
+    sc.build(w)
+    t0 = time.perf_counter()
+    its = subs = 0
+    for _ in range(steps):
+        r = w.step(sc.dt)
+        its += r.iterations
+        subs += r.substeps
+    ids = w.ids()
+    rho64 = np.empty(len(ids))
+    rho64[ids] = w.densities()
+    err = np.abs(np.asarray(gpu_rho, np.float64) - rho64[np.asarray(gpu_ids)]) / float(sc.settings.rest_density)
+    return {"max": float(err.max()), "mean": float(err.mean()),
+            "p99": float(np.quantile(err, 0.99)),
+            "within_0p1_percent": bool(err.max() <= 1e-3),
+            "fp64_solver_iterations_per_substep": its / max(subs, 1),
+            "against": f"FP64 restatement (double, compensated residual) from the same initial state over the "
+                       f"same {steps} steps (warm-up and timed), {time.perf_counter() - t0:.1f} s on {cores} "
+                       f"threads; |rho - rho_64| / rho_0 by particle id after the last timed step"}
 
 
 def run_reference(args, rank: int, world_size: int):
@@ -236,32 +272,49 @@ def run_reference(args, rank: int, world_size: int):
 
     py_oracle.build()
     cores = os.cpu_count()
-    w = py_oracle.OracleWorld(sc.settings, residual_sum=0, threads=cores)
-    sc.build(w)
-    w.update_neighbors()
-    budget = 150.0
-    t_start = time.perf_counter()
-    for _ in range(args.warmup):
-        w.step(sc.dt)
-        if time.perf_counter() - t_start > budget / 3:
-            break
-    substeps = 0
-    steps = 0
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        substeps += w.step(sc.dt).substeps
-        steps += 1
-        if time.perf_counter() - t0 > budget:
-            break
-    dt = time.perf_counter() - t0
+
+    def leg(residual_sum: int, budget: float):
+        """Warm-up then timed steps of the restatement: (steps, substeps, iterations, seconds)."""
+        w = py_oracle.OracleWorld(sc.settings, residual_sum=residual_sum, threads=cores)
+        sc.build(w)
+        w.update_neighbors()
+        t_start = time.perf_counter()
+        for _ in range(args.warmup):
+            w.step(sc.dt)
+            if time.perf_counter() - t_start > budget / 3:
+                break
+        substeps = iterations = steps = 0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            r = w.step(sc.dt)
+            substeps += r.substeps
+            iterations += r.iterations
+            steps += 1
+            if time.perf_counter() - t0 > budget:
+                break
+        return steps, substeps, iterations, time.perf_counter() - t0
+
+    # the reference's own stop test: the solver error summed in f32, sequentially (dfsph.rs:263-267)
+    steps, substeps, iterations, dt = leg(0, 150.0)
     value = substeps / dt
+    # beside it, the same steps with the compensated FP64 sum the CUDA library takes, so both
+    # arms' solver iterations can be compared step for step
+    c_steps, c_sub, c_its, c_dt = leg(1, 60.0)
     sample = (f"{steps} of {args.steps} timed steps ({substeps} substeps) of the {sc.particles}-particle scene, "
               f"{dt:.1f} s on {cores} threads (C++ float restatement of the reference, OpenMP; the Rust "
               f"reference has no toolchain here)")
     out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world_size,
            "steps": steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(steps, 1),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic", "config": workload(sc),
+           "data": "synthetic",
+           "config": dict(workload(sc), substeps=substeps,
+                          solver_iterations_per_substep=iterations / max(substeps, 1),
+                          solver_iterations_per_s=iterations / dt,
+                          residual_sum="f32 sequential (the reference's, dfsph.rs:263-267)"),
+           "compensated_residual_leg": {"value": c_sub / c_dt, "unit": UNIT, "steps": c_steps, "substeps": c_sub,
+                                        "solver_iterations_per_substep": c_its / max(c_sub, 1),
+                                        "solver_iterations_per_s": c_its / c_dt,
+                                        "residual_sum": "compensated FP64 (the CUDA library's)"},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -330,6 +383,8 @@ def main():
     launches = fluid.kernel_launches() - launches0
     graphed = world.graph_substeps() - graphed0
     clock_info = clocks.stop()
+    # the state the timed steps ended on, for the density error against the FP64 restatement
+    timed_end = (world.ids(), world.densities()) if rank == 0 and world_size == 1 else None
 
     all_substeps, total_ms = reduce_timing(substeps, sum(times_ms), world_size, dev)
     value = all_substeps / (total_ms / 1e3)
@@ -534,6 +589,9 @@ def main():
         state = (world.positions(), world.velocities())
         world.close()
         base = cpu_baseline(sc, args.cpu_budget, state)
+    dens_err = None
+    if timed_end is not None and not args.no_density_error:
+        dens_err = density_error(sc, max(args.warmup, 3) + args.steps, timed_end[0], timed_end[1])
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
@@ -541,8 +599,10 @@ def main():
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                "config": dict(workload(sc), parallelism=f"replicas x{world_size}",
                               substeps=substeps, solver_iterations_per_substep=iterations / max(substeps, 1),
+                              solver_iterations_per_s=iterations / (total_ms / 1e3),
                               particle_substeps_per_s=value * sc.particles,
                               solves=GRAPH_MODES[graph_mode], substeps_as_one_graph=graphed),
+               "density_error": dens_err,
                "roofline": roofline, "cpu_baseline": base, "e2e": e2e, "forward_adjoint": adjoint,
                "warm_start": warm,
                "clocks": clock_info, "gpu_launches": launches}
