@@ -337,7 +337,12 @@ int32_t slf_step_backward(slf_world* world, const float* dpositions, const float
  * cell size (the kernel radius, spacing * support).  order (device, n entries) receives, for
  * each place k of the (cell, id) order of update_neighbors (src/fluid/mod.rs:541-550), the
  * input index of the particle found there.  At most 262,144 particles whose bounding box spans
- * at most 1,048,576 cells: larger calls fail with SLF_ERR_OUT_OF_RANGE.  The call runs on
+ * at most 1,048,576 cells: larger calls fail with SLF_ERR_OUT_OF_RANGE, and so do particles whose
+ * cells saturate the i32 range (positions far beyond radius * 2^31).  Ids should be distinct, as
+ * a world's are; repeated ids still give a permutation, in no particular order among themselves.
+ * Ranking within a cell compares each particle with the cell's others, so a cell holding k
+ * particles costs k^2 work: a call whose particles crowd into a few cells (a radius far larger
+ * than their spacing) runs long, up to seconds at the particle limit.  The call runs on
  * `stream` (a cudaStream_t; NULL for the default stream) and waits for it before returning.
  * The first call on a device looks up the scratch array's address there, so make that first
  * call before any stream capture.  All calls share the one array and it keeps the last call's

@@ -61,6 +61,10 @@ __device__ __forceinline__ int3 na_cell(const float* pos, uint32_t i, float radi
 
 __global__ void k_na_bounds(const float* __restrict__ pos, uint32_t n, float radius, uint32_t* hdr) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // whether the warp holds a particle is its own flag: a particle's cell may itself saturate
+    // to INT_MAX or INT_MIN (a position of 1e30 at a small radius), so no cell value can
+    // stand for "none"
+    const bool any = __any_sync(0xffffffffu, i < n);
     int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
     if (i < n) {
         int3 c = na_cell(pos, i, radius);
@@ -76,7 +80,7 @@ __global__ void k_na_bounds(const float* __restrict__ pos, uint32_t n, float rad
             hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
         }
     }
-    if ((threadIdx.x & 31) == 0 && lo[0] != INT_MAX) {
+    if ((threadIdx.x & 31) == 0 && any) {
         int* h = reinterpret_cast<int*>(hdr);
         for (int a = 0; a < 3; ++a) {
             atomicMin(&h[kHdrLo + a], lo[a]);
@@ -91,7 +95,9 @@ __device__ __forceinline__ bool na_box(const uint32_t* hdr, int3& lo, int3& span
     long long sx = (long long)h[kHdrHi] - lo.x + 1, sy = (long long)h[kHdrHi + 1] - lo.y + 1,
               sz = (long long)h[kHdrHi + 2] - lo.z + 1;
     if (sx <= 0 || sy <= 0 || sz <= 0) return false;
-    if (sx * sy > (long long)kNoAllocMaxCells || sx * sy * sz > (long long)kNoAllocMaxCells) return false;
+    // each side is at most 2^32 cells: bounding them first keeps the products inside 64 bits
+    const long long cap = (long long)kNoAllocMaxCells;
+    if (sx > cap || sy > cap || sz > cap || sx * sy > cap || sx * sy * sz > cap) return false;
     span = make_int3(int(sx), int(sy), int(sz));
     return true;
 }
@@ -106,7 +112,15 @@ __global__ void k_na_count(const float* __restrict__ pos, uint32_t n, float radi
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int3 c = na_cell(pos, i, radius);
-    uint32_t l = uint32_t(((long long)(c.x - lo.x) * span.y + (c.y - lo.y)) * span.z + (c.z - lo.z));
+    // offsets in 64 bits (a cell minus the box's low corner can pass the i32 range), and every
+    // particle checked against the box before it touches the count table: a cell outside it
+    // fails the call instead of writing outside the scratch array
+    const long long x = (long long)c.x - lo.x, y = (long long)c.y - lo.y, z = (long long)c.z - lo.z;
+    if (x < 0 || x >= span.x || y < 0 || y >= span.y || z < 0 || z >= span.z) {
+        hdr[kHdrError] = 1;
+        return;
+    }
+    uint32_t l = uint32_t((x * span.y + y) * span.z + z);
     scratch[kOffLin + i] = l;
     scratch[kOffSlot + i] = atomicAdd(&scratch[kOffCount + l], 1u);
 }
@@ -119,7 +133,10 @@ __global__ void k_na_members(uint32_t n, const uint32_t* __restrict__ ids, uint3
     scratch[kOffMembers + scratch[kOffCount + l] + scratch[kOffSlot + i]] = ids[i];
 }
 
-// order[cell start + rank of the id in its cell] = i: the (cell, id) order of mod.rs:541-550
+// order[cell start + rank of the id in its cell] = i: the (cell, id) order of mod.rs:541-550.
+// A cell of k particles costs k comparisons a particle (k^2 for the cell).  Equal ids (a world's
+// ids are distinct; a caller's arrays need not be) are ranked by the slot each took in its cell,
+// so order is always a permutation, with repeated ids in no particular order among themselves.
 __global__ void k_na_order(uint32_t n, const uint32_t* __restrict__ ids, const uint32_t* __restrict__ scratch,
                            uint32_t* __restrict__ order) {
     if (scratch[kHdrError]) return;
@@ -127,8 +144,11 @@ __global__ void k_na_order(uint32_t n, const uint32_t* __restrict__ ids, const u
     if (i >= n) return;
     uint32_t l = scratch[kOffLin + i];
     uint32_t b = scratch[kOffCount + l], e = scratch[kOffCount + l + 1];
-    uint32_t id = ids[i], rank = 0;
-    for (uint32_t k = b; k < e; ++k) rank += scratch[kOffMembers + k] < id ? 1u : 0u;
+    uint32_t id = ids[i], own = b + scratch[kOffSlot + i], rank = 0;
+    for (uint32_t k = b; k < e; ++k) {
+        uint32_t m = scratch[kOffMembers + k];
+        rank += (m < id || (m == id && k < own)) ? 1u : 0u;
+    }
     order[b + rank] = i;
 }
 
