@@ -85,6 +85,62 @@ __device__ __forceinline__ void walk4(const PairLists& l, bool packed, uint32_t 
     }
 }
 
+// Walks row's gradient entries (PairLists::gv: the pair's kernel gradient and the neighbour's
+// index) four at a time: gather(j) for all four first, then body(G, gathered) in list order, the
+// next four entries requested before the bodies run.
+template <class Gather, class Body>
+__device__ __forceinline__ void walk_gradients(const PairLists& l, uint32_t row, Gather&& gather, Body&& body) {
+    uint32_t n = listed_count(l, row);
+    if (n == 0) return;
+    const float4* base = l.gv + l.at(row, 0);
+    float4 e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) e[u] = SLF_LIST_LOAD(base + size_t(u < (int)n ? u : n - 1) * 32u);
+    for (uint32_t k = 0; k < n; k += 4) {
+        float4 q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) q[u] = gather(__float_as_uint(e[u].w));
+        float4 next[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            uint32_t kk = k + 4 + u;
+            next[u] = SLF_LIST_LOAD(base + size_t(kk < n ? kk : n - 1) * 32u);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u < n) body(e[u], q[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) e[u] = next[u];
+    }
+}
+
+// Walks row's entries in both forms at once, U at a time: each pair's gradient G and index
+// (PairLists::gv) and its factor g = slope(d) / d (the {index, g} entry); gather(j) for all U
+// first, then body(G, g, gathered) in list order.
+template <class T, int U, class Gather, class Body>
+__device__ __forceinline__ void walk_gradients_g(const PairLists& l, uint32_t row, Gather&& gather, Body&& body) {
+    uint32_t n = listed_count(l, row);
+    if (n == 0) return;
+    const float4* gb = l.gv + l.at(row, 0);
+    const uint2* eb = l.e + l.at(row, 0);
+    for (uint32_t k = 0; k < n; k += U) {
+        float4 G[U];
+        float g[U];
+        T q[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            uint32_t kk = k + u < n ? k + u : n - 1;
+            G[u] = SLF_LIST_LOAD(gb + size_t(kk) * 32u);
+            g[u] = __uint_as_float(SLF_LIST_LOAD(eb + size_t(kk) * 32u).y);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) q[u] = gather(__float_as_uint(G[u].w));
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k + u < n) body(G[u], g[u], q[u]);
+    }
+}
+
 struct Two {
     float4 a, b;
 };
@@ -386,24 +442,33 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
     const float dt = sc->dt, m = p.mass;
     float3 xi = f3(pos[i]), wi = f3(w[i]);
     float acc = 0.0f;
-    walk4<Two>(fl, packed != 0, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&w[j])}; },
-               [&](uint32_t, const Two& q) {
-                   float3 r = xi - f3(q.a);
-                   float d2 = dotf(r, r), inv = inv_length(d2);
-                   if (inv == 0.0f) return;
-                   float g, gp;
-                   grad_factor(p, d2 * inv, g, gp);
-                   acc += dotf(wi - f3(q.b), r) * g;
-               });
-    uint32_t nw = listed_count(wl, row);
-    for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, row, k);
-        float3 r = xi - f3(__ldg(&walls[j]));
-        float d2 = dotf(r, r), inv = inv_length(d2);
-        if (inv == 0.0f) continue;
-        float g, gp;
-        grad_factor(p, d2 * inv, g, gp);
-        acc += dotf(wi, r) * g;
+    if (fl.gv && wl.gv) {
+        // the forward's kept gradients (EXACT DFSPH): rate(w) gathers only w of each neighbour
+        walk_gradients(fl, row, [&](uint32_t j) { return __ldg(&w[j]); },
+                       [&](float4 G, float4 wj) { acc += dotf(wi - f3(wj), f3(G)); });
+        uint32_t nw = listed_count(wl, row);
+        const float4* wg = wl.gv + wl.at(row, 0);
+        for (uint32_t k = 0; k < nw; ++k) acc += dotf(wi, f3(SLF_LIST_LOAD(wg + size_t(k) * 32u)));
+    } else {
+        walk4<Two>(fl, packed != 0, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&w[j])}; },
+                   [&](uint32_t, const Two& q) {
+                       float3 r = xi - f3(q.a);
+                       float d2 = dotf(r, r), inv = inv_length(d2);
+                       if (inv == 0.0f) return;
+                       float g, gp;
+                       grad_factor(p, d2 * inv, g, gp);
+                       acc += dotf(wi - f3(q.b), r) * g;
+                   });
+        uint32_t nw = listed_count(wl, row);
+        for (uint32_t k = 0; k < nw; ++k) {
+            uint32_t j = listed(wl, packed != 0, row, k);
+            float3 r = xi - f3(__ldg(&walls[j]));
+            float d2 = dotf(r, r), inv = inv_length(d2);
+            if (inv == 0.0f) continue;
+            float g, gp;
+            grad_factor(p, d2 * inv, g, gp);
+            acc += dotf(wi, r) * g;
+        }
     }
     float kbar = -dt * m * acc;
     float ri = rate[i], ai = alpha[i];
@@ -429,7 +494,15 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
 // The velocity adjoint before the iteration: w plus the rate pass's transpose (a push on the
 // rate adjoint); and the positions' share of both passes, through grad W.
 // four blocks a SM (64 registers)
-__global__ void __launch_bounds__(kBlock, 4) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+// GV: the forward kept each pair's gradient (EXACT DFSPH), read in place of the position gather.
+#ifndef SLF_ADJ_PUSH_GV_UNROLL
+#define SLF_ADJ_PUSH_GV_UNROLL 2
+#endif
+#ifndef SLF_ADJ_PUSH_GV_BLOCKS
+#define SLF_ADJ_PUSH_GV_BLOCKS 4
+#endif
+template <bool GV>
+__global__ void __launch_bounds__(kBlock, GV ? SLF_ADJ_PUSH_GV_BLOCKS : 4) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                      PairLists wl, int packed, const float4* __restrict__ pos,
                                                      const float4* __restrict__ walls, const float4* __restrict__ kw,
                                                      const float4* __restrict__ vr, float4* __restrict__ wout,
@@ -442,6 +515,44 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_push(Params p, const StepCons
     float3 xi = f3(pos[i]), wi = f3(own_w), vi = f3(own_v);
     float ki = own_w.w, rbi = own_v.w;
     float3 vacc = make_float3(0, 0, 0), xacc = make_float3(0, 0, 0);
+    if (GV) {
+        // the forward's kept gradients (EXACT DFSPH): r = G / g and |r| = |G| / |g| from the
+        // pair's entries, so only the two adjoint records of the neighbour are gathered
+        walk_gradients_g<Two, SLF_ADJ_PUSH_GV_UNROLL>(fl, row, [&](uint32_t j) { return Two{__ldg(&kw[j]), __ldg(&vr[j])}; },
+                              [&](float4 Gq, float g, const Two& q) {
+                                  if (g == 0.0f) return;  // coincident: the pair adds nothing
+                                  const float3 G = f3(Gq);
+                                  const float ig = 1.0f / g;
+                                  const float3 r = G * ig;
+                                  float d2 = dotf(r, r), inv = inv_length(d2);
+                                  if (inv == 0.0f) return;
+                                  float gd, gp;
+                                  grad_factor(p, d2 * inv, gd, gp);
+                                  float rbj = q.b.w;
+                                  vacc = vacc + G * (m * (rbi + rbj));
+                                  float3 c = (wi - f3(q.a)) * (-dt * m * (ki + q.a.w)) + (vi - f3(q.b)) * (m * (rbi + rbj));
+                                  xacc = xacc + c * g + r * (dotf(c, r) * gp * inv);
+                              });
+        uint32_t nw = listed_count(wl, row);
+        const float4* wgb = wl.gv + wl.at(row, 0);
+        for (uint32_t k = 0; k < nw; ++k) {
+            const float g = __uint_as_float(SLF_LIST_LOAD(wl.e + wl.at(row, k)).y);
+            if (g == 0.0f) continue;
+            const float3 G = f3(SLF_LIST_LOAD(wgb + size_t(k) * 32u));
+            const float3 r = G * (1.0f / g);
+            float d2 = dotf(r, r), inv = inv_length(d2);
+            if (inv == 0.0f) continue;
+            float gd, gp;
+            grad_factor(p, d2 * inv, gd, gp);
+            vacc = vacc + G * (m * rbi);
+            float3 c = wi * (-dt * m * ki) + vi * (m * rbi);
+            xacc = xacc + c * g + r * (dotf(c, r) * gp * inv);
+        }
+        wout[i] = make_float4(wi.x + vacc.x, wi.y + vacc.y, wi.z + vacc.z, 0.0f);
+        float4 x0 = xb[i];
+        xb[i] = make_float4(x0.x + xacc.x, x0.y + xacc.y, x0.z + xacc.z, 0.0f);
+        return;
+    }
     walk4<Three, false>(fl, packed != 0, row,
                  [&](uint32_t j) { return Three{__ldg(&pos[j]), __ldg(&kw[j]), __ldg(&vr[j])}; },
                  [&](uint32_t, const Three& q) {
@@ -602,7 +713,12 @@ void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, cons
         k_adj_kappa<0><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
                                                           rho, vel, kw, vr, abar, rb);
     if (parts & 2)
-        k_adj_push<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, kw, vr, wout, xb);
+        if (fl.gv && wl.gv)
+            k_adj_push<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, kw, vr, wout,
+                                                                xb);
+        else
+            k_adj_push<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, kw, vr, wout,
+                                                                 xb);
 }
 
 void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,

@@ -90,11 +90,18 @@ struct SolveRec {
 // order[s] (identity when order is null) and its list is row s.  The order visits the cells in 2 x 2-column bricks
 // (world.cpp builds it after each sort), so a block's 256 particles span about 2 x 2 x 8 cells and
 // their neighbourhoods overlap in the L1; particle arrays stay in the reference's sorted order.
+//
+// EXACT DFSPH also keeps each pair's whole gradient, as the reference's gradient cache does
+// (dfsph.rs:24-41): gv, at the same slots, holds {offset.x * g, offset.y * g, offset.z * g,
+// index bits} (walls: index 0).  The density pass writes it when gv is set; the solver check then
+// streams it and gathers only the neighbour's velocity, where from (index, g) it would gather the
+// position as well.  The products are the ones every pass forms, so the bits are the same.
 struct PairLists {
     uint32_t cap;          // slots per row
     uint2* e;              // entries {index, g bits}
     uint32_t* count;       // neighbours found per row; above cap the lists are incomplete
     const uint32_t* order; // particle of each row (null: row = particle)
+    float4* gv;            // gradient entries (null: not kept)
 
     __host__ __device__ static size_t slots_for(uint32_t n, uint32_t cap) {
         return size_t((n + 31u) / 32u) * cap * 32u;

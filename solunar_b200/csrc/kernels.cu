@@ -317,8 +317,10 @@ __device__ __forceinline__ float ground_damping(const TerrainDev& T, float dista
 }
 
 // The second half of a list-building walk: for each of row's first m listed neighbours, in list
-// order, q = pts[index] and the entry's factor becomes f(q).  Four entries and their points are
-// read ahead of their use (the entries were written by this thread just before: plain loads).
+// order, q = pts[index] and the entry's factor becomes f(q, index, k * 32), k the entry's place
+// in the list (k * 32: its offset from the row's first entry in the warp-tiled layout).  Four
+// entries and their points are read ahead of their use (the entries were written by this thread
+// just before: plain loads).
 template <class F>
 __device__ __forceinline__ void relist(const PairLists& l, uint32_t row, uint32_t m, const float4* __restrict__ pts,
                                        F&& f) {
@@ -339,7 +341,8 @@ __device__ __forceinline__ void relist(const PairLists& l, uint32_t row, uint32_
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            if (k + u < m) base[size_t(k + u) * 32u] = make_uint2(j[u], __float_as_uint(f(q[u])));
+            if (k + u < m)
+                base[size_t(k + u) * 32u] = make_uint2(j[u], __float_as_uint(f(q[u], j[u], (k + u) * 32u)));
 #pragma unroll
         for (int u = 0; u < 4; ++u) j[u] = next[u];
     }
@@ -434,7 +437,9 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
         longest = nf > nw ? nf : nw;
         float sum = 0.0f, wsum = 0.0f;
         float sx = 0.0f, sy = 0.0f, sz = 0.0f, squares = 0.0f;
-        relist(fl, row, nf < fl.cap ? nf : fl.cap, pos, [&](float4 q) {
+        float4* const fgv = fl.gv ? fl.gv + fl.at(row, 0) : nullptr;
+        float4* const wgv = wl.gv ? wl.gv + wl.at(row, 0) : nullptr;
+        relist(fl, row, nf < fl.cap ? nf : fl.cap, pos, [&](float4 q, uint32_t j, uint32_t at) {
             float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             sum += kernel_value(p, d);
@@ -442,7 +447,9 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
             if (SOLVER == 1) {
                 // gradient(at - other) (dfsph.rs:118), then factors (dfsph.rs:149-153)
                 float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-                float px = (rx * g) * p.mass, py = (ry * g) * p.mass, pz = (rz * g) * p.mass;
+                float gx = rx * g, gy = ry * g, gz = rz * g;
+                if (fgv) fgv[at] = make_float4(gx, gy, gz, __uint_as_float(j));
+                float px = gx * p.mass, py = gy * p.mass, pz = gz * p.mass;
                 sx = sx + px;
                 sy = sy + py;
                 sz = sz + pz;
@@ -450,16 +457,18 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
             }
             return g;
         });
-        relist(wl, row, nw < wl.cap ? nw : wl.cap, walls, [&](float4 q) {
+        relist(wl, row, nw < wl.cap ? nw : wl.cap, walls, [&](float4 q, uint32_t, uint32_t at) {
             float ox = q.x - a.x, oy = q.y - a.y, oz = q.z - a.z;
             float d = sqrtf(dot3(ox, oy, oz, ox, oy, oz));
             wsum += kernel_value(p, d);
             float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
             if (SOLVER == 1) {
                 float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-                sx = sx + (rx * g) * p.mass;
-                sy = sy + (ry * g) * p.mass;
-                sz = sz + (rz * g) * p.mass;
+                float gx = rx * g, gy = ry * g, gz = rz * g;
+                if (wgv) wgv[at] = make_float4(gx, gy, gz, 0.0f);
+                sx = sx + gx * p.mass;
+                sy = sy + gy * p.mass;
+                sz = sz + gz * p.mass;
             }
             return g;
         });
@@ -537,7 +546,9 @@ __global__ void __launch_bounds__(kBlock) k_density_warp(Params p, GridDev fg, G
                 float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
                 if (SOLVER == 1) {
                     float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-                    px = (rx * g) * p.mass, py = (ry * g) * p.mass, pz = (rz * g) * p.mass;
+                    float gx = rx * g, gy = ry * g, gz = rz * g;
+                    if (fl.gv) fl.gv[fl.at(row, k)] = make_float4(gx, gy, gz, __uint_as_float(j));
+                    px = gx * p.mass, py = gy * p.mass, pz = gz * p.mass;
                     sq = dot3(px, py, pz, px, py, pz);
                 }
                 *ent = make_uint2(j, __float_as_uint(g));
@@ -566,7 +577,9 @@ __global__ void __launch_bounds__(kBlock) k_density_warp(Params p, GridDev fg, G
                 float g = d <= 0.0f ? 0.0f : kernel_slope(p, d) / d;
                 if (SOLVER == 1) {
                     float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-                    px = (rx * g) * p.mass, py = (ry * g) * p.mass, pz = (rz * g) * p.mass;
+                    float gx = rx * g, gy = ry * g, gz = rz * g;
+                    if (wl.gv) wl.gv[wl.at(row, k)] = make_float4(gx, gy, gz, 0.0f);
+                    px = gx * p.mass, py = gy * p.mass, pz = gz * p.mass;
                 }
                 *ent = make_uint2(j, __float_as_uint(g));
             }
@@ -709,6 +722,49 @@ template <class F>
 __device__ __forceinline__ void each_listed2(const PairLists& l, uint32_t i, const float4* __restrict__ pts,
                                              const float4* __restrict__ more, F&& f) {
     each_listed2_from(l, i, FromGlobal{pts, more}, f);
+}
+
+// The solver check's walk over gradient entries (PairLists::gv): f(G, w) for each fluid neighbour
+// in list order, G the pair's kernel gradient and w = vel[index].  Entries stream evict-first,
+// kListUnroll at a time, the group's velocity gathers issued before any is used and the next
+// group's entries requested before this group is used; past the end of the list the last entry
+// is loaded again but not used.
+template <class F>
+__device__ __forceinline__ void each_gradient(const PairLists& l, uint32_t row, const float4* __restrict__ vel,
+                                              F&& f) {
+    uint32_t n = l.count[row];
+    if (n > l.cap) n = l.cap;
+    if (n == 0) return;
+    const float4* __restrict__ base = l.gv + l.at(row, 0);
+    float4 e[kListUnroll];
+#pragma unroll
+    for (int u = 0; u < kListUnroll; ++u) e[u] = SLF_LIST_LOAD(base + size_t(u < (int)n ? u : n - 1) * 32u);
+    for (uint32_t k = 0; k < n; k += kListUnroll) {
+        float4 w[kListUnroll];
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u) w[u] = __ldg(&vel[__float_as_uint(e[u].w)]);
+        float4 next[kListUnroll];
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u) {
+            uint32_t kk = k + kListUnroll + u;
+            next[u] = SLF_LIST_LOAD(base + size_t(kk < n ? kk : n - 1) * 32u);
+        }
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u)
+            if (k + u < n) f(e[u], w[u]);
+#pragma unroll
+        for (int u = 0; u < kListUnroll; ++u) e[u] = next[u];
+    }
+}
+
+// The same over wall gradient entries, which need no gather (walls do not move): f(G).
+template <class F>
+__device__ __forceinline__ void each_wall_gradient(const PairLists& l, uint32_t row, F&& f) {
+    uint32_t n = l.count[row];
+    if (n > l.cap) n = l.cap;
+    const float4* __restrict__ base = l.gv + l.at(row, 0);
+#pragma unroll 4
+    for (uint32_t k = 0; k < n; ++k) f(SLF_LIST_LOAD(base + size_t(k) * 32u));
 }
 
 // ---- wall viscosity (step.rs:262-301) -----------------------------------------------------
@@ -1153,14 +1209,22 @@ __device__ __forceinline__ void rate_particle(const Params& p, const StepConsts*
     float4 a = pos[i];
     float4 v = vel[i];
     float rate = 0.0f;
-    each_listed2_from(fl, row, src, [&](uint32_t, float g, float4 q, float4 w) {
-        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx * g, ry * g, rz * g);
-    });
-    each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
-        float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
-        rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
-    });
+    if (fl.gv && wl.gv) {
+        // the gradients the density pass kept: only the neighbours' velocities are gathered
+        each_gradient(fl, row, vel, [&](float4 G, float4 w) {
+            rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, G.x, G.y, G.z);
+        });
+        each_wall_gradient(wl, row, [&](float4 G) { rate += dot3(v.x, v.y, v.z, G.x, G.y, G.z); });
+    } else {
+        each_listed2_from(fl, row, src, [&](uint32_t, float g, float4 q, float4 w) {
+            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+            rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, rx * g, ry * g, rz * g);
+        });
+        each_listed(wl, row, walls, [&](uint32_t, float g, float4 q) {
+            float rx = a.x - q.x, ry = a.y - q.y, rz = a.z - q.z;
+            rate += dot3(v.x, v.y, v.z, rx * g, ry * g, rz * g);
+        });
+    }
     rate = rate * p.mass;
     if (rec.rate) {  // recorded for the adjoint
         size_t at = size_t(slot) * p.n + i;

@@ -24,6 +24,11 @@
 #include <cuda_runtime.h>
 
 #include "../../include/solunar_fluid.h"
+
+// EXACT DFSPH keeps each pair's gradient for the solver check (0: the check gathers positions)
+#ifndef SLF_KEEP_GRADIENTS
+#define SLF_KEEP_GRADIENTS 1
+#endif
 #include "launch.h"
 
 namespace slf {
@@ -343,6 +348,8 @@ struct World {
     DevBuf<uint32_t> lin, cslot, members, count, tiles, keep;
     // neighbour lists of the current substep (fluid and walls)
     DevBuf<uint2> fent, went;
+    // EXACT DFSPH: each pair's kernel gradient at the same slots (PairLists::gv), for the check
+    DevBuf<float4> fgv, wgv;
     DevBuf<uint32_t> fcnt, wcnt;
     uint32_t list_cap = 0;
     DevBuf<uint8_t> partials;
@@ -496,6 +503,8 @@ struct World {
             for (auto* b : {&warm[0], &warm[1]}) b->release(stream);
             fent.release(stream);
             went.release(stream);
+            fgv.release(stream);
+            wgv.release(stream);
             partials.release(stream);
             stage.release(stream);
             estage.release(stream);
@@ -884,6 +893,10 @@ struct World {
         size_t slots = PairLists::slots_for(uint32_t(n), list_cap);
         SLF_TRY(fent.ensure(slots, 0, stream));
         SLF_TRY(went.ensure(slots, 0, stream));
+        if (keeps_gradients()) {
+            SLF_TRY(fgv.ensure(slots, 0, stream));
+            SLF_TRY(wgv.ensure(slots, 0, stream));
+        }
         SLF_TRY(fcnt.ensure(n, 0, stream));
         SLF_TRY(wcnt.ensure(n, 0, stream));
         SLF_TRY(lin.ensure(n, 0, stream));
@@ -963,8 +976,15 @@ struct World {
     }
 
     const uint32_t* walk_order() const { return worder_valid ? worder.p : nullptr; }
-    PairLists fluid_lists() const { return PairLists{list_cap, fent.p, fcnt.p, walk_order()}; }
-    PairLists wall_lists() const { return PairLists{list_cap, went.p, wcnt.p, walk_order()}; }
+    // EXACT DFSPH keeps each pair's gradient for the solver check (16 bytes a slot, fluid and
+    // walls): the check then gathers a neighbour's velocity only, not its position too
+    bool keeps_gradients() const { return SLF_KEEP_GRADIENTS && !fast() && s.solver == SLF_SOLVER_DFSPH; }
+    PairLists fluid_lists() const {
+        return PairLists{list_cap, fent.p, fcnt.p, walk_order(), keeps_gradients() ? fgv.p : nullptr};
+    }
+    PairLists wall_lists() const {
+        return PairLists{list_cap, went.p, wcnt.p, walk_order(), keeps_gradients() ? wgv.p : nullptr};
+    }
 
     // After a density pass: a list longer than its room leaves the substep to be run again.
     static constexpr int32_t kRetry = -1;
@@ -2041,6 +2061,7 @@ struct World {
         key_add(k, l.e);
         key_add(k, l.count);
         key_add(k, l.order);
+        key_add(k, l.gv);
     }
     std::vector<uint8_t> solve_key(int which, const Params& p, int a, float4* v, int nid, const PairLists& fl,
                                    const PairLists& wl, const SolveRec& rec) {
