@@ -757,6 +757,71 @@ __device__ __forceinline__ void each_gradient(const PairLists& l, uint32_t row, 
     }
 }
 
+// The check's walk taking each slot in one of its two forms: slot k reads its kept gradient (16
+// bytes, then one gather: the neighbour's velocity) when bit k % 4 of GV_SLOTS is set, and its
+// {index, g} entry (8 bytes, then two gathers: position and velocity, G = (a - q) g as the
+// density pass formed it) when not.  The first form moves more list bytes, the second gathers
+// more: mixing them balances the pass's DRAM stream against its gathers.  f(G, w) in list order.
+#ifndef SLF_RATE_GV_SLOTS
+#define SLF_RATE_GV_SLOTS 0x7u
+#endif
+template <uint32_t GV_SLOTS, class F>
+__device__ __forceinline__ void each_gradient_mixed(const PairLists& l, uint32_t row, const float4* __restrict__ pos,
+                                                    const float4* __restrict__ vel, float4 a, F&& f) {
+    static_assert(kListUnroll == 4, "slot forms repeat every four slots");
+    uint32_t n = l.count[row];
+    if (n > l.cap) n = l.cap;
+    if (n == 0) return;
+    const float4* __restrict__ gb = l.gv + l.at(row, 0);
+    const uint2* __restrict__ eb = l.e + l.at(row, 0);
+    float4 eg[4];
+    uint2 ee[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        size_t kk = size_t(u < (int)n ? u : n - 1) * 32u;  // past the end: the last slot again, unused
+        if (GV_SLOTS >> u & 1u) eg[u] = SLF_LIST_LOAD(gb + kk);
+        else ee[u] = SLF_LIST_LOAD(eb + kk);
+    }
+    for (uint32_t k = 0; k < n; k += 4) {
+        float4 q[4], w[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (GV_SLOTS >> u & 1u) {
+                w[u] = __ldg(&vel[__float_as_uint(eg[u].w)]);
+            } else {
+                q[u] = __ldg(&pos[ee[u].x]);
+                w[u] = __ldg(&vel[ee[u].x]);
+            }
+        }
+        float4 ng[4];
+        uint2 ne[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            uint32_t kk = k + 4 + u;
+            size_t at = size_t(kk < n ? kk : n - 1) * 32u;
+            if (GV_SLOTS >> u & 1u) ng[u] = SLF_LIST_LOAD(gb + at);
+            else ne[u] = SLF_LIST_LOAD(eb + at);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (k + u < n) {
+                if (GV_SLOTS >> u & 1u) {
+                    f(eg[u], w[u]);
+                } else {
+                    const float g = __uint_as_float(ee[u].y);
+                    const float rx = a.x - q[u].x, ry = a.y - q[u].y, rz = a.z - q[u].z;
+                    f(make_float4(rx * g, ry * g, rz * g, 0.0f), w[u]);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (GV_SLOTS >> u & 1u) eg[u] = ng[u];
+            else ee[u] = ne[u];
+        }
+    }
+}
+
 // The same over wall gradient entries, which need no gather (walls do not move): f(G).
 template <class F>
 __device__ __forceinline__ void each_wall_gradient(const PairLists& l, uint32_t row, F&& f) {
@@ -1210,8 +1275,8 @@ __device__ __forceinline__ void rate_particle(const Params& p, const StepConsts*
     float4 v = vel[i];
     float rate = 0.0f;
     if (fl.gv && wl.gv) {
-        // the gradients the density pass kept: only the neighbours' velocities are gathered
-        each_gradient(fl, row, vel, [&](float4 G, float4 w) {
+        // the gradients the density pass kept, for the slots that read them
+        each_gradient_mixed<SLF_RATE_GV_SLOTS>(fl, row, pos, vel, a, [&](float4 G, float4 w) {
             rate += dot3(v.x - w.x, v.y - w.y, v.z - w.z, G.x, G.y, G.z);
         });
         each_wall_gradient(wl, row, [&](float4 G) { rate += dot3(v.x, v.y, v.z, G.x, G.y, G.z); });
