@@ -85,35 +85,6 @@ __device__ __forceinline__ void walk4(const PairLists& l, bool packed, uint32_t 
     }
 }
 
-// Walks row's gradient entries (PairLists::gv: the pair's kernel gradient and the neighbour's
-// index) four at a time: gather(j) for all four first, then body(G, gathered) in list order, the
-// next four entries requested before the bodies run.
-template <class Gather, class Body>
-__device__ __forceinline__ void walk_gradients(const PairLists& l, uint32_t row, Gather&& gather, Body&& body) {
-    uint32_t n = listed_count(l, row);
-    if (n == 0) return;
-    const float4* base = l.gv + l.at(row, 0);
-    float4 e[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) e[u] = SLF_LIST_LOAD(base + size_t(u < (int)n ? u : n - 1) * 32u);
-    for (uint32_t k = 0; k < n; k += 4) {
-        float4 q[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) q[u] = gather(__float_as_uint(e[u].w));
-        float4 next[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            uint32_t kk = k + 4 + u;
-            next[u] = SLF_LIST_LOAD(base + size_t(kk < n ? kk : n - 1) * 32u);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (k + u < n) body(e[u], q[u]);
-#pragma unroll
-        for (int u = 0; u < 4; ++u) e[u] = next[u];
-    }
-}
-
 // Walks row's entries in both forms at once, U at a time: each pair's gradient G and index
 // (PairLists::gv) and its factor g = slope(d) / d (the {index, g} entry); gather(j) for all U
 // first, then body(G, g, gathered) in list order.
@@ -173,6 +144,54 @@ __device__ __forceinline__ float dotf(float3 a, float3 b) { return a.x * b.x + a
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
 __device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+
+// The adjoint's stiffness pass takes each list slot in one of two forms, as the forward check
+// does: slot k uses the kept gradient G (PairLists::gv) when bit k % 4 of SLF_ADJ_KAPPA_GV_SLOTS
+// is set, and otherwise gathers the neighbour's position and forms G = (x_i - x_j) g from its
+// {index, g} entry.  The kept form streams more list bytes, the other gathers more; mixing them
+// balances the two.
+#ifndef SLF_ADJ_KAPPA_GV_SLOTS
+#define SLF_ADJ_KAPPA_GV_SLOTS 0x7u
+#endif
+__device__ __forceinline__ bool kept_form(uint32_t k) { return (SLF_ADJ_KAPPA_GV_SLOTS >> (k & 3u)) & 1u; }
+
+// body(G, gathered) for each of row's neighbours in list order, four at a time.
+template <class Gather, class Body>
+__device__ __forceinline__ void walk_gradients_mixed(const PairLists& l, uint32_t row, const float4* __restrict__ pos,
+                                                     float3 xi, Gather&& gather, Body&& body) {
+    uint32_t n = listed_count(l, row);
+    if (n == 0) return;
+    const float4* gb = l.gv + l.at(row, 0);
+    const uint2* eb = l.e + l.at(row, 0);
+    for (uint32_t k = 0; k < n; k += 4) {
+        float4 G[4], q[4];
+        uint32_t j[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t kk = k + u < n ? k + u : n - 1;
+            if (kept_form(k + u)) {
+                G[u] = SLF_LIST_LOAD(gb + size_t(kk) * 32u);
+                j[u] = __float_as_uint(G[u].w);
+            } else {
+                const uint2 e = SLF_LIST_LOAD(eb + size_t(kk) * 32u);
+                j[u] = e.x;
+                G[u].w = __uint_as_float(e.y);  // g until the position arrives
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            q[u] = gather(j[u]);
+            if (!kept_form(k + u)) {
+                const float4 xj = __ldg(&pos[j[u]]);
+                const float g = G[u].w;
+                G[u] = make_float4((xi.x - xj.x) * g, (xi.y - xj.y) * g, (xi.z - xj.z) * g, 0.0f);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u < n) body(G[u], q[u]);
+    }
+}
 
 // ---- advance and velocity update (step.rs:212-222, 305-339) ---------------------------------
 // y = x + v' dt is clamped per component; a clamped component passes no adjoint to y and zeroes
@@ -444,8 +463,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
     float acc = 0.0f;
     if (fl.gv && wl.gv) {
         // the forward's kept gradients (EXACT DFSPH): rate(w) gathers only w of each neighbour
-        walk_gradients(fl, row, [&](uint32_t j) { return __ldg(&w[j]); },
-                       [&](float4 G, float4 wj) { acc += dotf(wi - f3(wj), f3(G)); });
+        walk_gradients_mixed(fl, row, pos, xi, [&](uint32_t j) { return __ldg(&w[j]); },
+                             [&](float4 G, float4 wj) { acc += dotf(wi - f3(wj), f3(G)); });
         uint32_t nw = listed_count(wl, row);
         const float4* wg = wl.gv + wl.at(row, 0);
         for (uint32_t k = 0; k < nw; ++k) acc += dotf(wi, f3(SLF_LIST_LOAD(wg + size_t(k) * 32u)));
