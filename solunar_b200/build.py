@@ -25,7 +25,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["kernels.cu", "noalloc.cu"]
 # the FAST arithmetic variants: contraction on
 CUDA_FAST_SOURCES = ["kernels_fast.cu", "adjoint.cu"]
-HOST_SOURCES = ["world.cpp"]
+HOST_SOURCES = ["world_core.cpp", "world_walls.cpp", "world_bodies.cpp", "world_substep.cpp", "world_adjoint.cpp",
+                "world_flows.cpp", "world_snapshot.cpp", "capi.cpp"]
 
 
 def _nvcc() -> str:

@@ -88,7 +88,7 @@ struct SolveRec {
 // so a warp reading slot k of its 32 rows reads 256 contiguous bytes and each warp's lists are
 // one contiguous block.  Rows follow the walk order: thread s of a list pass walks particle
 // order[s] (identity when order is null) and its list is row s.  The order visits the cells in 2 x 2-column bricks
-// (world.cpp builds it after each sort), so a block's 256 particles span about 2 x 2 x 8 cells and
+// (the world builds it after each sort), so a block's 256 particles span about 2 x 2 x 8 cells and
 // their neighbourhoods overlap in the L1; particle arrays stay in the reference's sorted order.
 //
 // EXACT DFSPH also keeps each pair's whole gradient, as the reference's gradient cache does
