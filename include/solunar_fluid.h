@@ -37,7 +37,8 @@ enum {
     SLF_ERR_FLUID_FULL = 4,          /* PhysicsError::FluidFull (src/error.rs:21) */
     SLF_ERR_DISPATCH_INCOMPLETE = 5, /* PhysicsError::DispatchIncomplete (src/error.rs:15) */
     SLF_ERR_UNSUPPORTED = 6,         /* a combination not built: FAST arithmetic with terrain or bodies,
-                                      * cell-relative positions or a tape with them, shallow water */
+                                      * cell-relative positions with EXACT arithmetic, a tape with
+                                      * terrain, bodies or warm starts, shallow water */
     SLF_ERR_CUDA = 7,                /* a CUDA call failed; see slf_last_error() */
     SLF_ERR_TIMEOUT = 8,             /* a bounded device loop gave up */
     SLF_ERR_INVALID_ARGUMENT = 9,    /* null pointer or wrong buffer size */
@@ -309,8 +310,9 @@ typedef struct slf_param_grads {
  * every substep keeps the state before it and its solver record (the rates and velocities of each
  * DFSPH iteration), about 68 + 20 x iterations bytes per particle per substep; the backward pass
  * then redoes only each substep's sort and densities.  The number of particles must not change
- * while recording.  WCSPH and DFSPH steps; UNSUPPORTED with cell-relative positions, terrain
- * or warm_start. */
+ * while recording.  WCSPH and DFSPH steps, absolute or cell-relative positions (cell-relative
+ * checkpoints and records add the 16-byte cell of each particle); UNSUPPORTED with terrain,
+ * coupled bodies or warm_start. */
 int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
 /* Stops recording.  The tape's device buffers (substep records, checkpoints) stay with the world
  * and are reused by the next tape, so the rounds of an optimisation loop record without

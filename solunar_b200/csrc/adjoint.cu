@@ -18,11 +18,33 @@
 
 namespace slf {
 
-// Neighbour j in slot k: EXACT lists hold {index, g} pairs, FAST lists indexes only.
-__device__ __forceinline__ uint32_t listed(const PairLists& l, bool packed, uint32_t i, uint32_t k) {
+// How a world's lists hold a neighbour: EXACT lists {index, g} pairs; FAST lists the index in
+// the low 26 bits with the cell step to the neighbour in the top six (zero steps for absolute
+// positions); cell-relative positions are FAST lists whose steps matter.
+enum ListForm : int { kFormFast = 0, kFormExact = 1, kFormCellRelative = 2 };
+constexpr uint32_t kEntryIndexMask = (1u << 26) - 1u;
+
+// The entry in slot k: the index (EXACT), or index and step bits (FAST).
+__device__ __forceinline__ uint32_t listed_raw(const PairLists& l, int form, uint32_t i, uint32_t k) {
     size_t at = (size_t(i >> 5) * l.cap + k) * 32u + (i & 31u);
-    // FAST entries carry the cell step in their top six bits (zero steps: absolute positions)
-    return packed ? SLF_LIST_LOAD(&l.e[at]).x : (SLF_LIST_LOAD(reinterpret_cast<const uint32_t*>(l.e) + at) & ((1u << 26) - 1u));
+    return form == kFormExact ? SLF_LIST_LOAD(&l.e[at]).x : SLF_LIST_LOAD(reinterpret_cast<const uint32_t*>(l.e) + at);
+}
+__device__ __forceinline__ uint32_t entry_index(uint32_t e, int form) {
+    return form == kFormExact ? e : (e & kEntryIndexMask);
+}
+__device__ __forceinline__ uint32_t listed(const PairLists& l, int form, uint32_t i, uint32_t k) {
+    return entry_index(listed_raw(l, form, i, k), form);
+}
+
+// x_i - x_j from particle i's stored position xi and neighbour q's, given the entry e: with
+// cell-relative positions both are offsets from their cells and the entry's step (c_j - c_i)
+// restores the pair's offset as the forward pass forms it, (o_i - o_j) - step r.
+__device__ __forceinline__ float3 pair_off(const Params& p, int form, float3 xi, float4 q, uint32_t e) {
+    if (form != kFormCellRelative) return make_float3(xi.x - q.x, xi.y - q.y, xi.z - q.z);
+    float dx = float(int((e >> 26) & 3u) - 1), dy = float(int((e >> 28) & 3u) - 1),
+          dz = float(int((e >> 30) & 3u) - 1);
+    return make_float3(fmaf(-dx, p.radius, xi.x - q.x), fmaf(-dy, p.radius, xi.y - q.y),
+                       fmaf(-dz, p.radius, xi.z - q.z));
 }
 
 __device__ __forceinline__ uint32_t listed_count(const PairLists& l, uint32_t i) {
@@ -47,41 +69,42 @@ __device__ __forceinline__ void grad_factor(const Params& p, float d, float& g, 
 }
 
 // Walks i's list four entries at a time: gather(j) for all four first, so their loads are in
-// flight together, then body(j, gathered) for each in list order (the sums keep their order).
+// flight together, then body(j, gathered, e) for each in list order (the sums keep their order),
+// e the raw entry (its cell step for pair_off).
 // PREFETCH: the next four entries are requested before the bodies run (past the end the last
 // entry is read again and not used); walks that gather several records a neighbour skip it, as
 // the registers it holds cost them occupancy.
 template <class G, bool PREFETCH = true, class Gather, class Body>
-__device__ __forceinline__ void walk4(const PairLists& l, bool packed, uint32_t i, Gather&& gather, Body&& body) {
+__device__ __forceinline__ void walk4(const PairLists& l, int form, uint32_t i, Gather&& gather, Body&& body) {
     uint32_t n = listed_count(l, i);
     if (n == 0) return;
-    uint32_t j[4];
+    uint32_t e[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) j[u] = listed(l, packed, i, u < (int)n ? u : n - 1);
+    for (int u = 0; u < 4; ++u) e[u] = listed_raw(l, form, i, u < (int)n ? u : n - 1);
     for (uint32_t k = 0; k < n; k += 4) {
         G g[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) g[u] = gather(j[u]);
+        for (int u = 0; u < 4; ++u) g[u] = gather(entry_index(e[u], form));
         uint32_t next[4];
         if (PREFETCH) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 uint32_t kk = k + 4 + u;
-                next[u] = listed(l, packed, i, kk < n ? kk : n - 1);
+                next[u] = listed_raw(l, form, i, kk < n ? kk : n - 1);
             }
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            if (k + u < n) body(j[u], g[u]);
+            if (k + u < n) body(entry_index(e[u], form), g[u], e[u]);
         if (!PREFETCH) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 uint32_t kk = k + 4 + u;
-                next[u] = listed(l, packed, i, kk < n ? kk : n - 1);
+                next[u] = listed_raw(l, form, i, kk < n ? kk : n - 1);
             }
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) j[u] = next[u];
+        for (int u = 0; u < 4; ++u) e[u] = next[u];
     }
 }
 
@@ -226,7 +249,7 @@ __global__ void k_adj_advance(Params p, const StepConsts* __restrict__ sc, const
 // so the pressure records are neither gathered nor differentiated
 template <bool PRESSURE>
 __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
-                                                      PairLists wl, int packed, const float4* __restrict__ pos,
+                                                      PairLists wl, int form, const float4* __restrict__ pos,
                                                       const float4* __restrict__ vel, const float* __restrict__ rho,
                                                       const float* __restrict__ press,
                                                       const float* __restrict__ scaled,
@@ -245,13 +268,13 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         float sbar = 0.0f, pbar = 0.0f, rbar = 0.0f;
 
         // fluid pairs: L = (a_i-bar - a_j-bar) . T(r, u, S, R)
-        walk4<FiveF>(fl, packed != 0, row,
+        walk4<FiveF>(fl, form, row,
                      [&](uint32_t j) {
                          return FiveF{__ldg(&pos[j]), __ldg(&vel[j]), __ldg(&ab[j]), __ldg(&rho[j]),
                                       PRESSURE ? __ldg(&scaled[j]) : 0.0f};
                      },
-                     [&](uint32_t, const FiveF& q) {
-            float3 r = xi - f3(q.a);
+                     [&](uint32_t, const FiveF& q, uint32_t e) {
+            float3 r = pair_off(p, form, xi, q.a, e);
             float d2 = dotf(r, r), inv = inv_length(d2);
             if (inv == 0.0f) return;
             float g, gp;
@@ -285,8 +308,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         float M = s_i + p_i * p.inv_rest_sq;
         float3 A = make_float3(0, 0, 0);  // sum of -grad W over walls, for the wall normal
         for (uint32_t k = 0; k < nw; ++k) {
-            uint32_t j = listed(wl, packed != 0, row, k);
-            float3 r = xi - f3(__ldg(&walls[j]));
+            uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+            float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
             float d2 = dotf(r, r), inv = inv_length(d2);
             if (inv == 0.0f) continue;
             float g, gp;
@@ -311,8 +334,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
             float3 I = nrm * kk;
             float3 Ibar = make_float3(0, 0, 0);
             for (uint32_t k = 0; k < nw; ++k) {
-                uint32_t j = listed(wl, packed != 0, row, k);
-                float3 r = xi - f3(__ldg(&walls[j]));
+                uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+                float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
                 float tau = dotf(I, r);
                 if (!(tau < 0.0f)) continue;
                 float d2 = dotf(r, r);
@@ -342,8 +365,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
             float3 Abar = (nbar - nrm * dotf(nrm, nbar)) * (1.0f / alen);
             // A = sum -r g
             for (uint32_t k = 0; k < nw; ++k) {
-                uint32_t j = listed(wl, packed != 0, row, k);
-                float3 r = xi - f3(__ldg(&walls[j]));
+                uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+                float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
                 float d = sqrtf(dotf(r, r));
                 if (d <= 0.0f) continue;
                 float g, gp;
@@ -373,7 +396,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
 }
 
 // ---- densities (mod.rs:621-675): rho_i = m (sum_j W(r_ij) + sum_w W(r_iw)) ---------------------
-__global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, PairLists wl, int packed,
+__global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, PairLists wl, int form,
                                                         const float4* __restrict__ pos,
                                                         const float4* __restrict__ walls,
                                                         const float* __restrict__ rb, float4* __restrict__ xb) {
@@ -383,14 +406,14 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
     float3 xi = f3(pos[i]);
     float rbi = rb[i];
     float3 xbar = make_float3(0, 0, 0);
-    walk4<float4>(fl, packed != 0, row,
+    walk4<float4>(fl, form, row,
                   [&](uint32_t j) {
                       float4 q = __ldg(&pos[j]);
                       q.w = __ldg(&rb[j]);
                       return q;
                   },
-                  [&](uint32_t, float4 q) {
-                      float3 r = xi - f3(q);
+                  [&](uint32_t, float4 q, uint32_t e) {
+                      float3 r = pair_off(p, form, xi, q, e);
                       float d = sqrtf(dotf(r, r));
                       if (d <= 0.0f) return;
                       float g, gp;
@@ -399,8 +422,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
                   });
     uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, row, k);
-        float3 r = xi - f3(__ldg(&walls[j]));
+        uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+        float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) continue;
         float g, gp;
@@ -448,7 +471,7 @@ __global__ void k_adj_advance_dfsph(Params p, const StepConsts* __restrict__ sc,
 // gathers per neighbour (with the position).
 template <int WHICH>
 __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts* __restrict__ sc, PairLists fl,
-                                                      PairLists wl, int packed, const float4* __restrict__ pos,
+                                                      PairLists wl, int form, const float4* __restrict__ pos,
                                                       const float4* __restrict__ walls,
                                                       const float4* __restrict__ w, const float* __restrict__ rate,
                                                       const float* __restrict__ alpha, const float* __restrict__ rho,
@@ -469,9 +492,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
         const float4* wg = wl.gv + wl.at(row, 0);
         for (uint32_t k = 0; k < nw; ++k) acc += dotf(wi, f3(SLF_LIST_LOAD(wg + size_t(k) * 32u)));
     } else {
-        walk4<Two>(fl, packed != 0, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&w[j])}; },
-                   [&](uint32_t, const Two& q) {
-                       float3 r = xi - f3(q.a);
+        walk4<Two>(fl, form, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&w[j])}; },
+                   [&](uint32_t, const Two& q, uint32_t e) {
+                       float3 r = pair_off(p, form, xi, q.a, e);
                        float d2 = dotf(r, r), inv = inv_length(d2);
                        if (inv == 0.0f) return;
                        float g, gp;
@@ -480,8 +503,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
                    });
         uint32_t nw = listed_count(wl, row);
         for (uint32_t k = 0; k < nw; ++k) {
-            uint32_t j = listed(wl, packed != 0, row, k);
-            float3 r = xi - f3(__ldg(&walls[j]));
+            uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+            float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
             float d2 = dotf(r, r), inv = inv_length(d2);
             if (inv == 0.0f) continue;
             float g, gp;
@@ -522,7 +545,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
 #endif
 template <bool GV>
 __global__ void __launch_bounds__(kBlock, GV ? SLF_ADJ_PUSH_GV_BLOCKS : 4) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
-                                                     PairLists wl, int packed, const float4* __restrict__ pos,
+                                                     PairLists wl, int form, const float4* __restrict__ pos,
                                                      const float4* __restrict__ walls, const float4* __restrict__ kw,
                                                      const float4* __restrict__ vr, float4* __restrict__ wout,
                                                      float4* __restrict__ xb) {
@@ -572,10 +595,10 @@ __global__ void __launch_bounds__(kBlock, GV ? SLF_ADJ_PUSH_GV_BLOCKS : 4) k_adj
         xb[i] = make_float4(x0.x + xacc.x, x0.y + xacc.y, x0.z + xacc.z, 0.0f);
         return;
     }
-    walk4<Three, false>(fl, packed != 0, row,
+    walk4<Three, false>(fl, form, row,
                  [&](uint32_t j) { return Three{__ldg(&pos[j]), __ldg(&kw[j]), __ldg(&vr[j])}; },
-                 [&](uint32_t, const Three& q) {
-                     float3 r = xi - f3(q.a);
+                 [&](uint32_t, const Three& q, uint32_t e) {
+                     float3 r = pair_off(p, form, xi, q.a, e);
                      float d2 = dotf(r, r), inv = inv_length(d2);
                      if (inv == 0.0f) return;
                      float g, gp;
@@ -588,8 +611,8 @@ __global__ void __launch_bounds__(kBlock, GV ? SLF_ADJ_PUSH_GV_BLOCKS : 4) k_adj
                  });
     uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, row, k);
-        float3 r = xi - f3(__ldg(&walls[j]));
+        uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+        float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
         float d2 = dotf(r, r), inv = inv_length(d2);
         if (inv == 0.0f) continue;
         float g, gp;
@@ -621,7 +644,7 @@ __global__ void k_adj_scale(Params p, const StepConsts* __restrict__ sc, const f
 
 // factors (dfsph.rs:138-163): alpha = 1 / T, T = |G|^2 + sum_j |m grad W_ij|^2,
 // G = sum_j m grad W_ij + sum_w m grad W_iw.  First G and T-bar = -alpha-bar alpha^2 per particle.
-__global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists fl, PairLists wl, int packed,
+__global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists fl, PairLists wl, int form,
                                                            const float4* __restrict__ pos,
                                                            const float4* __restrict__ walls,
                                                            const float* __restrict__ alpha,
@@ -631,8 +654,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists f
     if (i >= p.n) return;
     float3 xi = f3(pos[i]);
     float3 G = make_float3(0, 0, 0);
-    walk4<float4>(fl, packed != 0, row, [&](uint32_t j) { return __ldg(&pos[j]); }, [&](uint32_t, float4 q) {
-        float3 r = xi - f3(q);
+    walk4<float4>(fl, form, row, [&](uint32_t j) { return __ldg(&pos[j]); }, [&](uint32_t, float4 q, uint32_t e) {
+        float3 r = pair_off(p, form, xi, q, e);
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) return;
         float g, gp;
@@ -641,8 +664,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists f
     });
     uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, row, k);
-        float3 r = xi - f3(__ldg(&walls[j]));
+        uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+        float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) continue;
         float g, gp;
@@ -653,7 +676,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha_prep(Params p, PairLists f
     gt[i] = make_float4(G.x, G.y, G.z, -abar[i] * a * a);
 }
 
-__global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, PairLists wl, int packed,
+__global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, PairLists wl, int form,
                                                       const float4* __restrict__ pos,
                                                       const float4* __restrict__ walls,
                                                       const float4* __restrict__ gt, float4* __restrict__ xb) {
@@ -666,9 +689,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, Pa
     float3 Gi = f3(own);
     float tbi = own.w;
     float3 xacc = make_float3(0, 0, 0);
-    walk4<Two>(fl, packed != 0, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&gt[j])}; },
-               [&](uint32_t, const Two& q) {
-                   float3 r = xi - f3(q.a);
+    walk4<Two>(fl, form, row, [&](uint32_t j) { return Two{__ldg(&pos[j]), __ldg(&gt[j])}; },
+               [&](uint32_t, const Two& q, uint32_t e) {
+                   float3 r = pair_off(p, form, xi, q.a, e);
                    float d = sqrtf(dotf(r, r));
                    if (d <= 0.0f) return;
                    float g, gp;
@@ -680,8 +703,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_alpha(Params p, PairLists fl, Pa
                });
     uint32_t nw = listed_count(wl, row);
     for (uint32_t k = 0; k < nw; ++k) {
-        uint32_t j = listed(wl, packed != 0, row, k);
-        float3 r = xi - f3(__ldg(&walls[j]));
+        uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+        float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
         float d = sqrtf(dotf(r, r));
         if (d <= 0.0f) continue;
         float g, gp;
@@ -699,16 +722,16 @@ static inline uint32_t adj_blocks(uint32_t n) {
 }
 
 void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                          bool packed, const float4* pos, const float4* vel, const float* rho, const float* press,
+                          int form, const float4* pos, const float4* vel, const float* rho, const float* press,
                           const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
                           const float4* xo, const float4* vo, float4* ab, float4* xb, float4* vb, float* rb,
                           float4* xp, float4* vp, double* grads, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = adj_blocks(p.n);
     k_adj_advance<<<nb, kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, ab, xb, vb, grads);
-    k_adj_force<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, press, scaled,
+    k_adj_force<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
                                                          walls, ab, xb, vb, rb, grads, 0);
-    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, rb, xb);
+    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb);
     k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp);
 }
 
@@ -720,43 +743,43 @@ void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float
 }
 
 void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                          bool packed, const float4* pos, const float4* walls, const float4* w, const float* rate,
+                          int form, const float4* pos, const float4* walls, const float4* w, const float* rate,
                           const float* alpha, const float* rho, const float4* vel, float4* kw, float4* vr,
                           float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s, int parts) {
     if (!p.n) return;
     // parts: 1 the kappa pass, 2 the push, 3 both
     if ((parts & 1) && which == 1)
-        k_adj_kappa<1><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
+        k_adj_kappa<1><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, rate, alpha,
                                                           rho, vel, kw, vr, abar, rb);
     else if (parts & 1)
-        k_adj_kappa<0><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, w, rate, alpha,
+        k_adj_kappa<0><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, rate, alpha,
                                                           rho, vel, kw, vr, abar, rb);
     if (parts & 2)
         if (fl.gv && wl.gv)
-            k_adj_push<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, kw, vr, wout,
+            k_adj_push<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, kw, vr, wout,
                                                                 xb);
         else
-            k_adj_push<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, walls, kw, vr, wout,
+            k_adj_push<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, kw, vr, wout,
                                                                  xb);
 }
 
-void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,
+void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, int form,
                           const float4* pos, const float4* vel, const float* rho, const float* zeros,
                           const float4* walls, float4* w, float4* ab, float4* xb, float* rb, double* grads,
                           cudaStream_t s) {
     if (!p.n) return;
     k_adj_scale<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, w, ab, grads);
-    k_adj_force<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, packed ? 1 : 0, pos, vel, rho, zeros, zeros,
+    k_adj_force<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, zeros, zeros,
                                                           walls, ab, xb, w, rb, grads, 1);
 }
 
-void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, bool packed,
+void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, int form,
                                 const float4* pos, const float4* walls, const float* alpha, const float* abar,
                                 float4* gt, const float* rb, float4* xb, cudaStream_t s) {
     if (!p.n) return;
-    k_adj_alpha_prep<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, alpha, abar, gt);
-    k_adj_alpha<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, gt, xb);
-    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, packed ? 1 : 0, pos, walls, rb, xb);
+    k_adj_alpha_prep<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, alpha, abar, gt);
+    k_adj_alpha<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, gt, xb);
+    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb);
 }
 
 void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const float4* vb, float4* xp, float4* vp,

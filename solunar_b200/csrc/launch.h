@@ -152,13 +152,17 @@ void launch_state_stats_rel(const Params& p, const int4* cells, const float4* ve
 void launch_list_rel(const Params& p, const GridDev& g, const float4* pos, const int4* cells, const float4* pts,
                      const uint32_t* start, uint32_t* out, cudaStream_t s);
 
+// `form` in the adjoint launchers: how the lists hold a neighbour, 1 EXACT {index, g} entries,
+// 0 FAST index entries (absolute positions), 2 FAST entries with cell steps (cell-relative
+// positions: pos then holds each particle's offset from its cell).
+//
 // The adjoint of one WCSPH substep (adjoint.cu).  Inputs are the recomputed forward of the
 // substep (sorted positions and velocities, lists, densities, pressures, the pre-clamp velocity,
 // the sort's destinations) and the adjoint of its output state xo, vo (sorted order); outputs
 // the adjoint of its input state xp, vp in the order before the sort, and adds the parameter
 // gradients (viscosity, wall viscosity, stiffness, gravity) to grads[kGradSlots].
 void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                          bool packed, const float4* pos, const float4* vel, const float* rho, const float* press,
+                          int form, const float4* pos, const float4* vel, const float* rho, const float* press,
                           const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
                           const float4* xo, const float4* vo, float4* ab, float4* xb, float4* vb, float* rb,
                           float4* xp, float4* vp, double* grads, cudaStream_t s);
@@ -169,14 +173,14 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
 void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float4* vel_pre, const float4* xo,
                               const float4* vo, float4* xb, float4* w, cudaStream_t s);
 void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
-                          bool packed, const float4* pos, const float4* walls, const float4* w, const float* rate,
+                          int form, const float4* pos, const float4* walls, const float4* w, const float* rate,
                           const float* alpha, const float* rho, const float4* vel, float4* kw, float4* vr,
                           float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s, int parts = 3);
-void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, bool packed,
+void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, int form,
                           const float4* pos, const float4* vel, const float* rho, const float* zeros,
                           const float4* walls, float4* w, float4* ab, float4* xb, float* rb, double* grads,
                           cudaStream_t s);
-void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, bool packed,
+void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, int form,
                                 const float4* pos, const float4* walls, const float* alpha, const float* abar,
                                 float4* gt, const float* rb, float4* xb, cudaStream_t s);
 void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const float4* vb, float4* xp, float4* vp,

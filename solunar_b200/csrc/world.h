@@ -426,11 +426,13 @@ struct World {
         float dt = 0.0f;
         DevBuf<float4> pos, vel;
         DevBuf<uint32_t> ids;
+        DevBuf<int4> cells;  // cell-relative positions: the cells of pos's offsets
         DfsphRecord rec;
         void release(cudaStream_t st) {
             pos.release(st);
             vel.release(st);
             ids.release(st);
+            cells.release(st);
             rec.release(st);
         }
     };
@@ -444,6 +446,7 @@ struct World {
         std::vector<size_t> ckpt_step;          // checkpoint c = the state before step ckpt_step[c]
         DevBuf<float4> cpos, cvel;              // [c][n]
         DevBuf<uint32_t> cids;
+        DevBuf<int4> ccells;                    // cell-relative positions: [c][n]
         std::vector<std::unique_ptr<SubRecord>> subs;  // every == 0: each substep's record
     } tape;
     // Records of finished tapes and segments, kept with their device buffers for the next ones:
@@ -454,9 +457,11 @@ struct World {
     struct BackScratch {
         DevBuf<float4> spos, svel, xo, vo, xp, vp, ab, xb, vb, pre, gt, kw, vr;
         DevBuf<uint32_t> sids, dest;
+        DevBuf<int4> scells;
         DevBuf<float> srho, rb, abar, zeros;
         DevBuf<double> grads;
         void release(cudaStream_t s) {
+            scells.release(s);
             for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt, &kw, &vr}) b->release(s);
             for (auto* b : {&srho, &rb, &abar, &zeros}) b->release(s);
             sids.release(s);
@@ -502,6 +507,7 @@ struct World {
             tape.cpos.release(stream);
             tape.cvel.release(stream);
             tape.cids.release(stream);
+            tape.ccells.release(stream);
             for (auto& r : tape.subs) r->release(stream);
             for (auto& r : spare_records) r->release(stream);
             back.release(stream);
@@ -927,9 +933,11 @@ struct World {
     // the committed state becomes checkpoint number ckpt_step.size()
     int32_t checkpoint();
 
-    int32_t save_state(float4* p, float4* v, uint32_t* id);
+    // the committed state (positions, velocities, ids and, for cell-relative positions, cells) to
+    // and from device buffers of n entries; c may be null for absolute positions
+    int32_t save_state(float4* p, float4* v, uint32_t* id, int4* c);
 
-    int32_t load_state(const float4* p, const float4* v, const uint32_t* id);
+    int32_t load_state(const float4* p, const float4* v, const uint32_t* id, const int4* c);
 
     int32_t substep_retrying(float dt);
 

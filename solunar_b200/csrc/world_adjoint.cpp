@@ -17,7 +17,6 @@ int32_t World::sync() {
 }
 
 int32_t World::tape_begin(uint32_t every) {
-    if (rel()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on absolute positions only");
     if (!terrains.empty()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint takes no terrain");
     if (warm_on()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on cold-started solves only");
     SLF_TRY(flush());
@@ -43,7 +42,8 @@ int32_t World::record_begin(float dt) {
     SLF_TRY(sub->pos.ensure(n, 0, stream));
     SLF_TRY(sub->vel.ensure(n, 0, stream));
     SLF_TRY(sub->ids.ensure(n, 0, stream));
-    SLF_TRY(save_state(sub->pos.p, sub->vel.p, sub->ids.p));
+    if (rel()) SLF_TRY(sub->cells.ensure(n, 0, stream));
+    SLF_TRY(save_state(sub->pos.p, sub->vel.p, sub->ids.p, sub->cells.p));
     tape.subs.push_back(std::move(sub));
     return SLF_OK;
 }
@@ -61,24 +61,28 @@ int32_t World::checkpoint() {
     SLF_TRY(tape.cpos.ensure((c + 1) * m, c * m, stream));
     SLF_TRY(tape.cvel.ensure((c + 1) * m, c * m, stream));
     SLF_TRY(tape.cids.ensure((c + 1) * m, c * m, stream));
-    SLF_TRY(save_state(tape.cpos.p + c * m, tape.cvel.p + c * m, tape.cids.p + c * m));
+    if (rel()) SLF_TRY(tape.ccells.ensure((c + 1) * m, c * m, stream));
+    SLF_TRY(save_state(tape.cpos.p + c * m, tape.cvel.p + c * m, tape.cids.p + c * m,
+                       rel() ? tape.ccells.p + c * m : nullptr));
     tape.ckpt_step.push_back(tape.steps.size());
     return SLF_OK;
 }
 
-int32_t World::save_state(float4* p, float4* v, uint32_t* id) {
+int32_t World::save_state(float4* p, float4* v, uint32_t* id, int4* c) {
     if (!n) return SLF_OK;
     SLF_CUDA(cudaMemcpyAsync(p, pos[cpos].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
     SLF_CUDA(cudaMemcpyAsync(v, vel[cpos].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
     SLF_CUDA(cudaMemcpyAsync(id, ids[cid].p, n * 4, cudaMemcpyDeviceToDevice, stream));
+    if (rel()) SLF_CUDA(cudaMemcpyAsync(c, cell[cpos].p, n * sizeof(int4), cudaMemcpyDeviceToDevice, stream));
     return SLF_OK;
 }
 
-int32_t World::load_state(const float4* p, const float4* v, const uint32_t* id) {
+int32_t World::load_state(const float4* p, const float4* v, const uint32_t* id, const int4* c) {
     if (n) {
         SLF_CUDA(cudaMemcpyAsync(pos[cpos].p, p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
         SLF_CUDA(cudaMemcpyAsync(vel[cpos].p, v, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
         SLF_CUDA(cudaMemcpyAsync(ids[cid].p, id, n * 4, cudaMemcpyDeviceToDevice, stream));
+        if (rel()) SLF_CUDA(cudaMemcpyAsync(cell[cpos].p, c, n * sizeof(int4), cudaMemcpyDeviceToDevice, stream));
     }
     stats_fresh = false;
     lists_valid = false;
@@ -130,6 +134,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
     DevBuf<float4> &spos = B.spos, &svel = B.svel, &xo = B.xo, &vo = B.vo, &xp = B.xp, &vp = B.vp,
                    &ab = B.ab, &xb = B.xb, &vb = B.vb, &pre = B.pre, &gt = B.gt, &kw = B.kw, &vr = B.vr;
     DevBuf<uint32_t> &sids = B.sids, &dest = B.dest;
+    DevBuf<int4>& scells = B.scells;
     DevBuf<float> &srho = B.srho, &rb = B.rb, &abar = B.abar, &zeros = B.zeros;
     DevBuf<double>& grads = B.grads;
     int32_t st = SLF_OK;
@@ -141,7 +146,8 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
         SLF_TRY(sids.ensure(n, 0, stream));
         SLF_TRY(dest.ensure(n, 0, stream));
         SLF_TRY(grads.ensure(kGradSlots, 0, stream));
-        SLF_TRY(save_state(spos.p, svel.p, sids.p));
+        if (rel()) SLF_TRY(scells.ensure(n, 0, stream));
+        SLF_TRY(save_state(spos.p, svel.p, sids.p, scells.p));
         SLF_CUDA(cudaMemcpyAsync(srho.p, rho[cid].p, n * 4, cudaMemcpyDeviceToDevice, stream));
         SLF_TRY(write_vec(xo, dpos, n));
         SLF_TRY(write_vec(vo, dvel, n));
@@ -151,9 +157,9 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
             Params p = params();
             SLF_CUDA(cudaMemsetAsync(grads.p, 0, kGradSlots * sizeof(double), stream));
             PairLists fl = fluid_lists(), wl = wall_lists();
-            bool packed = !fast();
+            const int form = !fast() ? 1 : (rel() ? 2 : 0);  // the lists' form (launch.h)
             if (s.solver == SLF_SOLVER_WCSPH) {
-                launch_adjoint_wcsph(p, d_consts, fl, wl, packed, pos[a].p, vel[a].p, rho[nid].p, press.p,
+                launch_adjoint_wcsph(p, d_consts, fl, wl, form, pos[a].p, vel[a].p, rho[nid].p, press.p,
                                      scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p, xb.p, vb.p, rb.p, xp.p,
                                      vp.p, grads.p, stream);
             } else {
@@ -167,7 +173,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                 for (uint32_t it = rec.den_n; it-- > 0;) {
                     for (int part = 1; part <= 2; ++part)
                         timed(part == 1 ? "adj_kappa_density" : "adj_push_density", 0.0, [&] {
-                            launch_adj_iteration(1, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
+                            launch_adj_iteration(1, p, d_consts, fl, wl, form, pos[a].p, dwalls.p, vb.p,
                                                  rec.den_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
                                                  rec.den_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p,
                                                  vp.p, xb.p, stream, part);
@@ -175,13 +181,13 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                     std::swap(vb, vp);
                 }
                 timed("adj_viscosity", 0.0, [&] {
-                    launch_adj_viscosity(p, d_consts, fl, wl, packed, pos[a].p, rec.va.p, rho[nid].p, zeros.p,
+                    launch_adj_viscosity(p, d_consts, fl, wl, form, pos[a].p, rec.va.p, rho[nid].p, zeros.p,
                                          dwalls.p, vb.p, ab.p, xb.p, rb.p, grads.p, stream);
                 });
                 for (uint32_t it = rec.div_n; it-- > 0;) {
                     for (int part = 1; part <= 2; ++part)
                         timed(part == 1 ? "adj_kappa_divergence" : "adj_push_divergence", 0.0, [&] {
-                            launch_adj_iteration(0, p, d_consts, fl, wl, packed, pos[a].p, dwalls.p, vb.p,
+                            launch_adj_iteration(0, p, d_consts, fl, wl, form, pos[a].p, dwalls.p, vb.p,
                                                  rec.div_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
                                                  rec.div_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p,
                                                  vp.p, xb.p, stream, part);
@@ -189,7 +195,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                     std::swap(vb, vp);
                 }
                 timed("adj_factors_density", 0.0, [&] {
-                    launch_adj_factors_density(p, fl, wl, packed, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p,
+                    launch_adj_factors_density(p, fl, wl, form, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p,
                                                rb.p, xb.p, stream);
                 });
                 timed("adj_unsort", 0.0, [&] { launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream); });
@@ -229,7 +235,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
         auto backward_through = [&](std::vector<std::unique_ptr<SubRecord>>& subs, size_t count) -> int32_t {
             for (size_t q = count; q-- > 0;) {
                 SubRecord& sub = *subs[q];
-                SLF_TRY(load_state(sub.pos.p, sub.vel.p, sub.ids.p));
+                SLF_TRY(load_state(sub.pos.p, sub.vel.p, sub.ids.p, sub.cells.p));
                 int a = 0, nid = 0;
                 if (s.solver == SLF_SOLVER_WCSPH) {
                     SLF_TRY(recompute(sub.dt, sub.rec, a, nid));
@@ -262,14 +268,16 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                 std::vector<float> dts;
                 for (size_t t = b; t < e; ++t) dts.insert(dts.end(), tape.steps[t].begin(), tape.steps[t].end());
                 while (segsubs.size() < dts.size()) segsubs.push_back(new_record());
-                SLF_TRY(load_state(tape.cpos.p + c * n, tape.cvel.p + c * n, tape.cids.p + c * n));
+                SLF_TRY(load_state(tape.cpos.p + c * n, tape.cvel.p + c * n, tape.cids.p + c * n,
+                                   rel() ? tape.ccells.p + c * n : nullptr));
                 for (size_t q = 0; q < dts.size(); ++q) {
                     SubRecord& sub = *segsubs[q];
                     sub.dt = dts[q];
                     SLF_TRY(sub.pos.ensure(n, 0, stream));
                     SLF_TRY(sub.vel.ensure(n, 0, stream));
                     SLF_TRY(sub.ids.ensure(n, 0, stream));
-                    SLF_TRY(save_state(sub.pos.p, sub.vel.p, sub.ids.p));
+                    if (rel()) SLF_TRY(sub.cells.ensure(n, 0, stream));
+                    SLF_TRY(save_state(sub.pos.p, sub.vel.p, sub.ids.p, sub.cells.p));
                     uint32_t held = 0, its = 0;
                     int32_t rs;
                     if (s.solver == SLF_SOLVER_WCSPH) {
@@ -292,7 +300,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
         if (dpos0) SLF_TRY(read_vec(xo, dpos0, n));
         if (dvel0) SLF_TRY(read_vec(vo, dvel0, n));
         // the state as it was
-        SLF_TRY(load_state(spos.p, svel.p, sids.p));
+        SLF_TRY(load_state(spos.p, svel.p, sids.p, scells.p));
         SLF_CUDA(cudaMemcpyAsync(rho[cid].p, srho.p, n * 4, cudaMemcpyDeviceToDevice, stream));
         return sync();
     };
