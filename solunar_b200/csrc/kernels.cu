@@ -1595,6 +1595,52 @@ __global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const u
     if (warm_in) warm_out[f] = warm_in[i];
 }
 
+// ---- the particles a coupled body's lift reads (lift.rs:29-60) -----------------------------------
+
+// keep[i] = 1 for a particle inside any of the boxes (low, high pairs, bounds inclusive, NaN
+// bounds ignored and NaN positions outside, as the host's clamp test min(max(p, low), high) == p)
+__global__ void k_in_boxes(uint32_t n, const float4* __restrict__ pos, const float3* __restrict__ boxes,
+                           uint32_t count, uint32_t* __restrict__ keep) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = pos[i];
+    uint32_t in = 0;
+    if (a.x == a.x && a.y == a.y && a.z == a.z) {
+        for (uint32_t b = 0; b < count && !in; ++b) {
+            const float3 lo = boxes[2 * b], hi = boxes[2 * b + 1];
+            in = !(lo.x > a.x) && !(a.x > hi.x) && !(lo.y > a.y) && !(a.y > hi.y) && !(lo.z > a.z) && !(a.z > hi.z);
+        }
+    }
+    keep[i] = in;
+}
+
+// the kept particles in index order: their index, position and velocity (xyz, 6 floats)
+__global__ void k_gather_kept(uint32_t n, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ at,
+                              const float4* __restrict__ pos, const float4* __restrict__ vel,
+                              uint32_t* __restrict__ index, float* __restrict__ pv) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !keep[i]) return;
+    const uint32_t k = at[i];
+    const float4 a = pos[i], v = vel[i];
+    index[k] = i;
+    float* o = pv + 6 * size_t(k);
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = a.z;
+    o[3] = v.x;
+    o[4] = v.y;
+    o[5] = v.z;
+}
+
+// vel[index[k]].xyz = v3[k]
+__global__ void k_scatter_velocities(uint32_t m, const uint32_t* __restrict__ index, const float* __restrict__ v3,
+                                     float4* __restrict__ vel) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const uint32_t i = index[k];
+    vel[i] = make_float4(v3[3 * size_t(k)], v3[3 * size_t(k) + 1], v3[3 * size_t(k) + 2], 0.0f);
+}
+
 __global__ void k_set_consts(StepConsts c, StepConsts* out) { *out = c; }
 
 // xyz triples <-> float4, so host copies move 12 bytes a particle
@@ -1827,6 +1873,19 @@ void launch_emit(uint32_t total, const uint32_t* taken_ex, int3 cnt, float3 low,
     if (total && room)
         k_emit<<<blocks_for(total), kBlock, 0, s>>>(total, taken_ex, cnt, low, spacing, velocity, room, first_id, pos_out,
                                                     vel_out, ids_out, rho_out);
+}
+
+void launch_in_boxes(uint32_t n, const float4* pos, const float3* boxes, uint32_t count, uint32_t* keep, cudaStream_t s) {
+    if (n) k_in_boxes<<<blocks_for(n), kBlock, 0, s>>>(n, pos, boxes, count, keep);
+}
+
+void launch_gather_kept(uint32_t n, const uint32_t* keep, const uint32_t* at, const float4* pos, const float4* vel,
+                        uint32_t* index, float* pv, cudaStream_t s) {
+    if (n) k_gather_kept<<<blocks_for(n), kBlock, 0, s>>>(n, keep, at, pos, vel, index, pv);
+}
+
+void launch_scatter_velocities(uint32_t m, const uint32_t* index, const float* v3, float4* vel, cudaStream_t s) {
+    if (m) k_scatter_velocities<<<blocks_for(m), kBlock, 0, s>>>(m, index, v3, vel);
 }
 
 void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, float3 low, float3 high, int drain,

@@ -96,6 +96,13 @@ void launch_list_fill(const Params& p, const GridDev& g, const float4* pos, cons
 
 // domain
 // keep flags: the domain's inside (drain = 0) or a drain box's outside (drain = 1)
+// the particles inside any of `count` boxes (boxes: low, high pairs): keep flags, then (after an
+// exclusive scan of them into `at`) their index, position and velocity in index order; and the
+// velocities of listed particles written back
+void launch_in_boxes(uint32_t n, const float4* pos, const float3* boxes, uint32_t count, uint32_t* keep, cudaStream_t s);
+void launch_gather_kept(uint32_t n, const uint32_t* keep, const uint32_t* at, const float4* pos, const float4* vel,
+                        uint32_t* index, float* pv, cudaStream_t s);
+void launch_scatter_velocities(uint32_t m, const uint32_t* index, const float* v3, float4* vel, cudaStream_t s);
 void launch_domain_flags(const Params& p, const float4* pos, const int4* cells, float3 low, float3 high, int drain,
                          uint32_t* keep, cudaStream_t s);
 // emitters: mark the taken lattice slots (taken cleared, total + 1 words), then, after an

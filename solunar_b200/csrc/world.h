@@ -501,6 +501,9 @@ struct World {
             went.release(stream);
             fgv.release(stream);
             wgv.release(stream);
+            for (auto* b : {&lkeep, &lat, &lidx, &ltiles}) b->release(stream);
+            lpv.release(stream);
+            lboxes.release(stream);
             partials.release(stream);
             stage.release(stream);
             estage.release(stream);
@@ -707,10 +710,24 @@ struct World {
     struct Lift {
         size_t owner;
         F3 impulse, angular;
-        std::vector<uint32_t> near;
+        std::vector<uint32_t> near;  // the particles read, as places in the lift's P and V
     };
+    // The region a body's lift reads (lift.rs:40-52): its probes placed by the pose (arm from the
+    // centre, velocity), and their box grown by three kernel radii.
+    void lift_region(const Coupled& known, const slf_body_pose& state, std::vector<std::pair<F3, F3>>& probes,
+                     F3& low, F3& high) const;
+    // P, V: the particles inside the bodies' regions (read_lift_water), in index order.
     std::vector<Lift> lifts(float dt, const slf_body_pose* poses, uint64_t npose, const std::vector<F3>& P,
                             const std::vector<F3>& V) const;
+    // The particles inside any of the boxes, selected and compacted on the device in index order,
+    // read back with their indexes: the lift reads these and not the whole state.
+    DevBuf<uint32_t> lkeep, lat, lidx, ltiles;
+    DevBuf<float> lpv;
+    DevBuf<float3> lboxes;
+    int32_t read_lift_water(const std::vector<float3>& boxes, std::vector<uint32_t>& index, std::vector<F3>& P,
+                            std::vector<F3>& V);
+    // the velocities of the particles read_lift_water read last, written back in the same order
+    int32_t write_lift_velocities(const std::vector<F3>& V);
 
     // couple.rs:219-248 with the rigid world left to the caller
     int32_t step_with_bodies(float dt, const slf_body_pose* poses, uint64_t npose, slf_report* out,

@@ -261,31 +261,90 @@ int32_t World::mover_felt(float dt, const Params& p, int a, int nid) {
     return SLF_OK;
 }
 
+void World::lift_region(const Coupled& known, const slf_body_pose& state, std::vector<std::pair<F3, F3>>& probes,
+                        F3& low, F3& high) const {
+    float reach = 3.0f * radius;
+    F3 center = center_of(state), lin = f3v(state.linear_velocity), ang = f3v(state.angular_velocity);
+    probes.clear();
+    for (const F3& local : known.probes) {
+        F3 arm = rotate(state.rotation, local);
+        probes.push_back({arm, lin + cross(ang, arm)});
+    }
+    low = F3{FLT_MAX, FLT_MAX, FLT_MAX};
+    high = F3{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (auto& pr : probes) {
+        low = vmin(low, center + pr.first);
+        high = vmax(high, center + pr.first);
+    }
+    low = low - F3{reach, reach, reach};
+    high = high + F3{reach, reach, reach};
+}
+
+int32_t World::read_lift_water(const std::vector<float3>& boxes, std::vector<uint32_t>& index, std::vector<F3>& P,
+                               std::vector<F3>& V) {
+    index.clear();
+    P.clear();
+    V.clear();
+    if (!n || boxes.empty()) return SLF_OK;
+    const uint32_t m = uint32_t(n);
+    SLF_TRY(lboxes.ensure(boxes.size(), 0, stream));
+    SLF_TRY(lkeep.ensure(m, 0, stream));
+    SLF_TRY(lat.ensure(size_t(m) + 1, 0, stream));
+    SLF_TRY(ltiles.ensure(scan_tiles(m) + 1, 0, stream));
+    SLF_CUDA(cudaMemcpyAsync(lboxes.p, boxes.data(), boxes.size() * sizeof(float3), cudaMemcpyHostToDevice, stream));
+    launch_in_boxes(m, pos[cpos].p, lboxes.p, uint32_t(boxes.size() / 2), lkeep.p, stream);
+    SLF_CUDA(cudaMemcpyAsync(lat.p, lkeep.p, size_t(m) * 4, cudaMemcpyDeviceToDevice, stream));
+    launch_exclusive_scan(lat.p, m, ltiles.p, stream);
+    uint32_t kept = 0;
+    SLF_CUDA(cudaMemcpyAsync(&kept, lat.p + m, 4, cudaMemcpyDeviceToHost, stream));
+    SLF_TRY(sync());
+    if (!kept) return SLF_OK;
+    SLF_TRY(lidx.ensure(kept, 0, stream));
+    SLF_TRY(lpv.ensure(size_t(6) * kept, 0, stream));
+    launch_gather_kept(m, lkeep.p, lat.p, pos[cpos].p, vel[cpos].p, lidx.p, lpv.p, stream);
+    index.resize(kept);
+    std::vector<float> pv(size_t(6) * kept);
+    SLF_CUDA(cudaMemcpyAsync(index.data(), lidx.p, size_t(kept) * 4, cudaMemcpyDeviceToHost, stream));
+    SLF_CUDA(cudaMemcpyAsync(pv.data(), lpv.p, pv.size() * 4, cudaMemcpyDeviceToHost, stream));
+    SLF_TRY(sync());
+    P.resize(kept);
+    V.resize(kept);
+    for (uint32_t k = 0; k < kept; ++k) {
+        const float* o = pv.data() + 6 * size_t(k);
+        P[k] = F3{o[0], o[1], o[2]};
+        V[k] = F3{o[3], o[4], o[5]};
+    }
+    return SLF_OK;
+}
+
+int32_t World::write_lift_velocities(const std::vector<F3>& V) {
+    if (V.empty()) return SLF_OK;
+    std::vector<float> v3(3 * V.size());
+    for (size_t k = 0; k < V.size(); ++k) {
+        v3[3 * k] = V[k].x;
+        v3[3 * k + 1] = V[k].y;
+        v3[3 * k + 2] = V[k].z;
+    }
+    SLF_CUDA(cudaMemcpyAsync(lpv.p, v3.data(), v3.size() * 4, cudaMemcpyHostToDevice, stream));
+    launch_scatter_velocities(uint32_t(V.size()), lidx.p, lpv.p, vel[cpos].p, stream);
+    return sync();
+}
+
 auto World::lifts(float dt, const slf_body_pose* poses, uint64_t npose, const std::vector<F3>& P,
                   const std::vector<F3>& V) const -> std::vector<Lift> {
     F3 g{s.gravity[0], s.gravity[1], s.gravity[2]};
     float grav = length(g);
     F3 up = grav > 0.0f ? (-g) / grav : F3{0.0f, 1.0f, 0.0f};
-    float reach = 3.0f * radius;
     float column = radius;
     std::vector<Lift> out;
+    std::vector<std::pair<F3, F3>> probes;
     for (size_t owner = 0; owner < coupled.size(); ++owner) {
         const Coupled& known = coupled[owner];
         const slf_body_pose* state = pose_of(poses, npose, known.body);
         if (!state) continue;
-        F3 center = center_of(*state), lin = f3v(state->linear_velocity), ang = f3v(state->angular_velocity);
-        std::vector<std::pair<F3, F3>> probes;
-        for (const F3& local : known.probes) {
-            F3 arm = rotate(state->rotation, local);
-            probes.push_back({arm, lin + cross(ang, arm)});
-        }
-        F3 low{FLT_MAX, FLT_MAX, FLT_MAX}, high{-FLT_MAX, -FLT_MAX, -FLT_MAX};
-        for (auto& pr : probes) {
-            low = vmin(low, center + pr.first);
-            high = vmax(high, center + pr.first);
-        }
-        low = low - F3{reach, reach, reach};
-        high = high + F3{reach, reach, reach};
+        F3 center = center_of(*state);
+        F3 low, high;
+        lift_region(known, *state, probes, low, high);
         std::vector<uint32_t> near;
         for (size_t i = 0; i < P.size(); ++i)
             if (vmin(vmax(P[i], low), high) == P[i]) near.push_back(uint32_t(i));
@@ -388,17 +447,20 @@ int32_t World::step_with_bodies(float dt, const slf_body_pose* poses, uint64_t n
         pushes.push_back(p);
     }
     if (!(dt > 0.0f) || coupled.empty()) return SLF_OK;
-    std::vector<F3> P, V;
-    if (n) {
-        std::vector<float> hp(3 * n), hv(3 * n);
-        SLF_TRY(read_state(hp.data(), hv.data(), n));
-        P.resize(n);
-        V.resize(n);
-        for (uint64_t i = 0; i < n; ++i) {
-            P[i] = F3{hp[3 * i], hp[3 * i + 1], hp[3 * i + 2]};
-            V[i] = F3{hv[3 * i], hv[3 * i + 1], hv[3 * i + 2]};
-        }
+    // the water the lifts read: the particles inside the bodies' regions, in index order
+    std::vector<float3> boxes;
+    std::vector<std::pair<F3, F3>> probes;
+    for (const Coupled& known : coupled) {
+        const slf_body_pose* state = pose_of(poses, npose, known.body);
+        if (!state) continue;
+        F3 low, high;
+        lift_region(known, *state, probes, low, high);
+        boxes.push_back(make_float3(low.x, low.y, low.z));
+        boxes.push_back(make_float3(high.x, high.y, high.z));
     }
+    std::vector<uint32_t> index;
+    std::vector<F3> P, V;
+    SLF_TRY(read_lift_water(boxes, index, P, V));
     auto put = [](float* d, F3 v) {
         d[0] = v.x;
         d[1] = v.y;
@@ -423,14 +485,7 @@ int32_t World::step_with_bodies(float dt, const slf_body_pose* poses, uint64_t n
         coupled[b].impulse = coupled[b].angular = F3{0, 0, 0};
     }
     if (gave) {
-        std::vector<float> hv(3 * n);
-        for (uint64_t i = 0; i < n; ++i) {
-            hv[3 * i] = V[i].x;
-            hv[3 * i + 1] = V[i].y;
-            hv[3 * i + 2] = V[i].z;
-        }
-        SLF_TRY(write_vec(vel[cpos], hv.data(), n));
-        SLF_TRY(sync());
+        SLF_TRY(write_lift_velocities(V));
         stats_fresh = false;
     }
     return SLF_OK;
