@@ -1595,6 +1595,54 @@ __global__ void k_compact(uint32_t n, const uint32_t* __restrict__ keep, const u
     if (warm_in) warm_out[f] = warm_in[i];
 }
 
+// ---- carrying the body points through a step (couple.rs:291-318) -----------------------------
+
+// The points at `elapsed` (start + velocity * elapsed, owner bits in start.w) and their place in
+// the dense table of box (low, span): lin[i], and slot[i] among the cell's points counted so far.
+__global__ void k_mover_cells(Params p, uint32_t k, const float4* __restrict__ start, const float4* __restrict__ vel,
+                              float elapsed, int3 low, int3 span, uint32_t* __restrict__ lin,
+                              uint32_t* __restrict__ slot, uint32_t* __restrict__ count) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const float4 s0 = start[i], v = vel[i];
+    const float x = s0.x + v.x * elapsed, y = s0.y + v.y * elapsed, z = s0.z + v.z * elapsed;
+    const int3 c = cell_of(p, x, y, z);
+    const uint32_t l = uint32_t(((long long)(c.x - low.x) * span.y + (c.y - low.y)) * span.z + (c.z - low.z));
+    lin[i] = l;
+    slot[i] = atomicAdd(&count[l], 1u);
+}
+
+// The points sorted by (cell, owner, place in the current order), as the host sort of
+// couple.rs:291-318 orders them: a point's place in its cell is the number of the cell's points
+// with a smaller (owner, current place).  Writes the sorted starts, velocities and positions at
+// `elapsed` (owner bits in w).
+__global__ void k_mover_order(uint32_t k, const uint32_t* __restrict__ lin, const uint32_t* __restrict__ slot,
+                              const uint32_t* __restrict__ table, uint32_t* __restrict__ members,
+                              const float4* __restrict__ start, const float4* __restrict__ vel, float elapsed,
+                              float4* __restrict__ start_out, float4* __restrict__ vel_out,
+                              float4* __restrict__ pos_out, int phase) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const uint32_t l = lin[i], b = table[l];
+    if (phase == 0) {  // the cell's members, in any order
+        members[b + slot[i]] = i;
+        return;
+    }
+    const uint32_t e = table[l + 1];
+    const uint32_t own = __float_as_uint(start[i].w);
+    uint32_t rank = 0;
+    for (uint32_t q = b; q < e; ++q) {
+        const uint32_t m = members[q];
+        const uint32_t om = __float_as_uint(__ldg(&start[m].w));
+        rank += (om < own || (om == own && m < i)) ? 1u : 0u;
+    }
+    const uint32_t d = b + rank;
+    const float4 s0 = start[i], v = vel[i];
+    start_out[d] = s0;
+    vel_out[d] = v;
+    pos_out[d] = make_float4(s0.x + v.x * elapsed, s0.y + v.y * elapsed, s0.z + v.z * elapsed, s0.w);
+}
+
 // ---- the particles a coupled body's lift reads (lift.rs:29-60) -----------------------------------
 
 // keep[i] = 1 for a particle inside any of the boxes (low, high pairs, bounds inclusive, NaN
@@ -1781,6 +1829,45 @@ void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M,
     note_launch();
 }
 
+// What each body took this substep, folded into its step's impulse as the host folds it
+// (step.rs:173-221): chunk by chunk in order, impulse + force * dt, angular + torque * dt.  A block
+// a body: its threads bring the chunks' records into shared memory 256 at a time and one thread
+// adds them in order.
+__global__ void k_mover_fold(uint32_t chunks, uint32_t bodies, const float4* __restrict__ felt, float dt,
+                             float4* __restrict__ impulse) {
+    __shared__ float4 force[kBlock], torque[kBlock];
+    const uint32_t b = blockIdx.x, t = threadIdx.x;
+    float4 imp = impulse[2 * size_t(b)], ang = impulse[2 * size_t(b) + 1];
+    for (uint32_t base = 0; base < chunks; base += kBlock) {
+        const uint32_t c = base + t;
+        if (c < chunks) {
+            force[t] = felt[2 * (size_t(c) * bodies + b)];
+            torque[t] = felt[2 * (size_t(c) * bodies + b) + 1];
+        }
+        __syncthreads();
+        if (t == 0) {
+            const uint32_t here = chunks - base < uint32_t(kBlock) ? chunks - base : uint32_t(kBlock);
+#pragma unroll 8
+            for (uint32_t j = 0; j < here; ++j) {
+                const float4 f = force[j], q = torque[j];
+                imp = make_float4(imp.x + f.x * dt, imp.y + f.y * dt, imp.z + f.z * dt, 0.0f);
+                ang = make_float4(ang.x + q.x * dt, ang.y + q.y * dt, ang.z + q.z * dt, 0.0f);
+            }
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        impulse[2 * size_t(b)] = imp;
+        impulse[2 * size_t(b) + 1] = ang;
+    }
+}
+
+void launch_mover_fold(uint32_t n, uint32_t bodies, const float4* felt, float dt, float4* impulse, cudaStream_t s) {
+    if (!n || !bodies) return;
+    k_mover_fold<<<bodies, kBlock, 0, s>>>((n + 511u) / 512u, bodies, felt, dt, impulse);
+    note_launch();
+}
+
 void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStream_t s) {
     long long total = ((long long)hi.x - lo.x + 1) * ((long long)hi.y - lo.y + 1) * ((long long)hi.z - lo.z + 1);
     if (total <= 0) return;
@@ -1873,6 +1960,20 @@ void launch_emit(uint32_t total, const uint32_t* taken_ex, int3 cnt, float3 low,
     if (total && room)
         k_emit<<<blocks_for(total), kBlock, 0, s>>>(total, taken_ex, cnt, low, spacing, velocity, room, first_id, pos_out,
                                                     vel_out, ids_out, rho_out);
+}
+
+void launch_carry_movers(const Params& p, uint32_t k, const float4* start, const float4* vel, float elapsed, int3 low,
+                         int3 span, uint32_t volume, uint32_t* lin, uint32_t* slot, uint32_t* table, uint32_t* tiles,
+                         uint32_t* members, float4* start_out, float4* vel_out, float4* pos_out, cudaStream_t s) {
+    if (!k) return;
+    cudaMemsetAsync(table, 0, (size_t(volume) + 1) * 4, s);
+    k_mover_cells<<<blocks_for(k), kBlock, 0, s>>>(p, k, start, vel, elapsed, low, span, lin, slot, table);
+    launch_exclusive_scan(table, volume, tiles, s);
+    k_mover_order<<<blocks_for(k), kBlock, 0, s>>>(k, lin, slot, table, members, start, vel, elapsed, start_out,
+                                                   vel_out, pos_out, 0);
+    k_mover_order<<<blocks_for(k), kBlock, 0, s>>>(k, lin, slot, table, members, start, vel, elapsed, start_out,
+                                                   vel_out, pos_out, 1);
+    g_launches.fetch_add(3, std::memory_order_relaxed);
 }
 
 void launch_in_boxes(uint32_t n, const float4* pos, const float3* boxes, uint32_t count, uint32_t* keep, cudaStream_t s) {

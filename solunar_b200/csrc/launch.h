@@ -66,6 +66,9 @@ void launch_mover_count(const Params& p, const StepConsts* sc, const MoverDev& M
 void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M, const float4* pos, const float4* vel,
                        const float* rho, const float* press, const float* scaled, const float4* centre,
                        uint32_t bodies, const uint32_t* offset, float4* pair, float4* felt, cudaStream_t s);
+// the bodies' felt records of a substep (launch_mover_felt) added into impulse[2 b] (force x dt)
+// and impulse[2 b + 1] (torque x dt), chunk by chunk in order
+void launch_mover_fold(uint32_t n, uint32_t bodies, const float4* felt, float dt, float4* impulse, cudaStream_t s);
 void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
@@ -96,6 +99,14 @@ void launch_list_fill(const Params& p, const GridDev& g, const float4* pos, cons
 
 // domain
 // keep flags: the domain's inside (drain = 0) or a drain box's outside (drain = 1)
+// The k body points at `elapsed` sorted by (cell, owner, current place) into the *_out arrays,
+// with the dense cell table of box (low, span) in table (volume + 1 entries, the last the total):
+// lin, slot, members hold k entries, tiles scan_tiles(volume) + 1.  Every point's cell must lie
+// in the box.
+void launch_carry_movers(const Params& p, uint32_t k, const float4* start, const float4* vel, float elapsed, int3 low,
+                         int3 span, uint32_t volume, uint32_t* lin, uint32_t* slot, uint32_t* table, uint32_t* tiles,
+                         uint32_t* members, float4* start_out, float4* vel_out, float4* pos_out, cudaStream_t s);
+
 // the particles inside any of `count` boxes (boxes: low, high pairs): keep flags, then (after an
 // exclusive scan of them into `at`) their index, position and velocity in index order; and the
 // velocities of listed particles written back

@@ -502,6 +502,8 @@ struct World {
             fgv.release(stream);
             wgv.release(stream);
             for (auto* b : {&lkeep, &lat, &lidx, &ltiles}) b->release(stream);
+            for (auto* b : {&dmcur_start, &dmcur_vel, &dmnext_start, &dmnext_vel, &dimpulse}) b->release(stream);
+            for (auto* b : {&dmlin, &dmslot, &dmmembers, &dmtable, &dmtable_tiles}) b->release(stream);
             lpv.release(stream);
             lboxes.release(stream);
             partials.release(stream);
@@ -662,11 +664,20 @@ struct World {
     std::vector<uint32_t> m_own;
     DevBuf<float4> dmpos, dmvel, dcentre, dfelt;
     DevBuf<uint32_t> dmstart, dwet;
+    // Carrying the points on the device (a step whose points stay within a dense cell box of
+    // modest volume): the step's box, the points in their current order (starts with the owner
+    // bits in w, velocities), the next order, and the sort's scratch; the table is the grid's.
+    // the damping impulse and its torque each body took so far this step ([2 b], [2 b + 1])
+    DevBuf<float4> dimpulse;
+    bool mdevice = false;
+    int3 mlow{}, mspan{};
+    uint32_t mvolume = 0;
+    DevBuf<float4> dmcur_start, dmcur_vel, dmnext_start, dmnext_vel;
+    DevBuf<uint32_t> dmlin, dmslot, dmmembers, dmtable, dmtable_tiles;
     DevBuf<uint32_t> dmcount, dmtiles;
     DevBuf<float4> dmpair;
     DevBuf<int4> dmkeys;
     GridDev mgrid{};
-    std::vector<float4> h_felt;
 
     MoverDev mover_dev() const;
 
@@ -694,7 +705,11 @@ struct World {
 
     // couple.rs:291-322: points `elapsed` into the step, sorted by (cell, owner, place), and their
     // device copies and cell table
-    int32_t carry_movers(float elapsed);
+    // the points at `elapsed` of the step's substeps, `last` the elapsed time of its last one
+    int32_t carry_movers(float elapsed, float last);
+    // at the step's first substep: the cell box the points reach over the step (their cells at
+    // its first and last substeps: each moves on a line), and whether the device carries them
+    int32_t plan_movers(float last);
 
     // couple.rs:325-366: the fastest coupled body that may meet the water within dt.  The water's
     // cells are those of the last sort (the reference's grid).

@@ -357,7 +357,7 @@ int32_t World::step_untaped(float dt, slf_report* out) {
                 uint32_t held = 0;
                 if (tape_step) tape_step->push_back(small);
                 if (tape_step && tape.every == 0) SLF_TRY(record_begin(small));
-                if (!coupled.empty()) SLF_TRY(carry_movers(small * float(i)));
+                if (!coupled.empty()) SLF_TRY(carry_movers(small * float(i), small * float(substeps - 1)));
                 int32_t st = wcsph_substep(small, held);
                 if (st == kRetry) st = wcsph_substep(small, held);
                 if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");

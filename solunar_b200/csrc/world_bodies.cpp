@@ -9,7 +9,7 @@ MoverDev World::mover_dev() const {
     M.count = uint32_t(m_pos.size());
     M.grid = mgrid;
     M.pos = dmpos.p;
-    M.vel = dmvel.p;
+    M.vel = mdevice ? dmcur_vel.p : dmvel.p;
     return M;
 }
 
@@ -134,8 +134,68 @@ void World::place_movers_at(const slf_body_pose* poses, uint64_t npose) {
     m_pos = m_start;
 }
 
-int32_t World::carry_movers(float elapsed) {
+int32_t World::plan_movers(float last) {
     size_t k = m_start.size();
+    mdevice = false;
+    if (!k) return SLF_OK;
+    Key3 lo = cell_of(m_start[0]), hi = lo;
+    for (size_t i = 0; i < k; ++i)
+        for (float e : {0.0f, last}) {
+            Key3 c = cell_of(m_start[i] + m_vel[i] * e);
+            lo = Key3{std::min(lo.x, c.x), std::min(lo.y, c.y), std::min(lo.z, c.z)};
+            hi = Key3{std::max(hi.x, c.x), std::max(hi.y, c.y), std::max(hi.z, c.z)};
+        }
+    // one cell more on every side, and well inside the i32 range
+    const int64_t lim = int64_t(1) << 30;
+    for (int64_t v : {int64_t(lo.x), int64_t(lo.y), int64_t(lo.z), int64_t(hi.x), int64_t(hi.y), int64_t(hi.z)})
+        if (v <= -lim || v >= lim) return SLF_OK;
+    int64_t sx = int64_t(hi.x) - lo.x + 3, sy = int64_t(hi.y) - lo.y + 3, sz = int64_t(hi.z) - lo.z + 3;
+    int64_t volume = sx * sy * sz;
+    if (volume > int64_t(64) * int64_t(k) + 4096 || volume >= (int64_t(1) << 24)) return SLF_OK;
+    mlow = make_int3(lo.x - 1, lo.y - 1, lo.z - 1);
+    mspan = make_int3(int(sx), int(sy), int(sz));
+    mvolume = uint32_t(volume);
+    std::vector<float4> hs(k), hv(k);
+    for (size_t i = 0; i < k; ++i) {
+        uint32_t bits = m_own[i];
+        float w;
+        std::memcpy(&w, &bits, 4);
+        hs[i] = make_float4(m_start[i].x, m_start[i].y, m_start[i].z, w);
+        hv[i] = make_float4(m_vel[i].x, m_vel[i].y, m_vel[i].z, 0.0f);
+    }
+    for (auto* b : {&dmcur_start, &dmcur_vel, &dmnext_start, &dmnext_vel, &dmpos}) SLF_TRY(b->ensure(k, 0, stream));
+    for (auto* b : {&dmlin, &dmslot, &dmmembers}) SLF_TRY(b->ensure(k, 0, stream));
+    SLF_TRY(dmtable.ensure(size_t(mvolume) + 1, 0, stream));
+    SLF_TRY(dmtable_tiles.ensure(scan_tiles(mvolume) + 1, 0, stream));
+    SLF_CUDA(cudaMemcpyAsync(dmcur_start.p, hs.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
+    SLF_CUDA(cudaMemcpyAsync(dmcur_vel.p, hv.data(), k * sizeof(float4), cudaMemcpyHostToDevice, stream));
+    SLF_CUDA(cudaStreamSynchronize(stream));  // the staging vectors are pageable and freed next
+    mdevice = true;
+    return SLF_OK;
+}
+
+int32_t World::carry_movers(float elapsed, float last) {
+    if (elapsed == 0.0f) SLF_TRY(plan_movers(last));
+    size_t k = m_start.size();
+    if (k && mdevice) {
+        for (auto& known : coupled) known.moved = known.velocity * elapsed;
+        launch_carry_movers(params(), uint32_t(k), dmcur_start.p, dmcur_vel.p, elapsed, mlow, mspan, mvolume, dmlin.p,
+                            dmslot.p, dmtable.p, dmtable_tiles.p, dmmembers.p, dmnext_start.p, dmnext_vel.p, dmpos.p,
+                            stream);
+        std::swap(dmcur_start, dmnext_start);
+        std::swap(dmcur_vel, dmnext_vel);
+        // the sorted velocities: dmcur_vel now; the grid: the dense table over the step's box
+        mgrid = GridDev{};
+        mgrid.mode = 1;
+        mgrid.lx = mlow.x;
+        mgrid.ly = mlow.y;
+        mgrid.lz = mlow.z;
+        mgrid.sx = mspan.x;
+        mgrid.sy = mspan.y;
+        mgrid.sz = mspan.z;
+        mgrid.start = dmtable.p;
+        return SLF_OK;
+    }
     struct MK {
         Key3 cell;
         uint32_t owner;
@@ -247,17 +307,8 @@ int32_t World::mover_felt(float dt, const Params& p, int a, int nid) {
     SLF_TRY(dmpair.ensure(2 * size_t(std::max<uint32_t>(total, 1)), 0, stream));
     launch_mover_felt(p, d_consts, mover_dev(), pos[a].p, vel[a].p, rho[nid].p, press.p, scaled.p, dcentre.p,
                       uint32_t(bodies), dmcount.p, dmpair.p, dfelt.p, stream);
-    h_felt.resize(2 * chunks * bodies);
-    SLF_CUDA(cudaMemcpyAsync(h_felt.data(), dfelt.p, h_felt.size() * sizeof(float4), cudaMemcpyDeviceToHost,
-                             stream));
-    SLF_TRY(sync());
-    for (size_t c = 0; c < chunks; ++c)
-        for (size_t b = 0; b < bodies; ++b) {
-            const float4& f = h_felt[2 * (c * bodies + b)];
-            const float4& t = h_felt[2 * (c * bodies + b) + 1];
-            coupled[b].impulse = coupled[b].impulse + F3{f.x, f.y, f.z} * dt;
-            coupled[b].angular = coupled[b].angular + F3{t.x, t.y, t.z} * dt;
-        }
+    // folded on the device into the step's impulses, read once when the step ends
+    launch_mover_fold(uint32_t(n), uint32_t(bodies), dfelt.p, dt, dimpulse.p, stream);
     return SLF_OK;
 }
 
@@ -433,7 +484,20 @@ int32_t World::step_with_bodies(float dt, const slf_body_pose* poses, uint64_t n
     if (!coupled.empty() && fast()) return fail(SLF_ERR_UNSUPPORTED, "coupled bodies run with EXACT arithmetic only");
     if (tape.on && !coupled.empty()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint takes no coupled bodies");
     place_movers_at(poses, npose);
+    if (!coupled.empty()) {
+        SLF_TRY(dimpulse.ensure(2 * coupled.size(), 0, stream));
+        SLF_CUDA(cudaMemsetAsync(dimpulse.p, 0, 2 * coupled.size() * sizeof(float4), stream));
+    }
     int32_t st = step(dt, out);
+    if (st == SLF_OK && !coupled.empty()) {  // the damping the bodies took, as the substeps folded it
+        std::vector<float4> imp(2 * coupled.size());
+        SLF_CUDA(cudaMemcpyAsync(imp.data(), dimpulse.p, imp.size() * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+        SLF_TRY(sync());
+        for (size_t b = 0; b < coupled.size(); ++b) {
+            coupled[b].impulse = F3{imp[2 * b].x, imp[2 * b].y, imp[2 * b].z};
+            coupled[b].angular = F3{imp[2 * b + 1].x, imp[2 * b + 1].y, imp[2 * b + 1].z};
+        }
+    }
     // the points are gone for the next step
     m_start.clear();
     m_pos.clear();
