@@ -644,6 +644,9 @@ constexpr int kListUnroll = SLF_LIST_UNROLL;
 #ifndef SLF_RATE_MIN_BLOCKS
 #define SLF_RATE_MIN_BLOCKS 4
 #endif
+#ifndef SLF_PUSH_MIN_BLOCKS
+#define SLF_PUSH_MIN_BLOCKS SLF_PAIR_MIN_BLOCKS
+#endif
 
 
 
@@ -1370,7 +1373,7 @@ __device__ __forceinline__ void push_particle(const Params& p, const StepConsts*
     if (applied) applied[2 * (size_t)i] += own * dt;
 }
 
-__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+__global__ void __launch_bounds__(kBlock, SLF_PUSH_MIN_BLOCKS) k_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                  PairLists wl, const float4* __restrict__ pos,
                                                  float4* __restrict__ vel, const float4* __restrict__ walls,
                                                  Status* st, float* __restrict__ applied, unsigned long long loop) {
