@@ -644,8 +644,10 @@ constexpr int kListUnroll = SLF_LIST_UNROLL;
 #ifndef SLF_RATE_MIN_BLOCKS
 #define SLF_RATE_MIN_BLOCKS 4
 #endif
+// the push at five blocks a SM (48 registers; 56 uncapped at four blocks: 72.2 -> 70.5 us at 1M;
+// six blocks spill)
 #ifndef SLF_PUSH_MIN_BLOCKS
-#define SLF_PUSH_MIN_BLOCKS SLF_PAIR_MIN_BLOCKS
+#define SLF_PUSH_MIN_BLOCKS 5
 #endif
 
 
