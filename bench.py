@@ -64,7 +64,8 @@ def parse():
     ap.add_argument("--graph-mode", type=int, default=2, choices=(0, 1, 2),
                     help="2 each substep one CUDA graph, 1 each solve one graph, 0 as --no-graphs")
     ap.add_argument("--adjoint-every", type=int, default=0,
-                    help="tape checkpoint spacing of the forward+adjoint leg; 0 records every substep")
+                    help="tape checkpoint spacing of the forward+adjoint leg, in substeps; 0 records every "
+                         "substep")
     ap.add_argument("--adjoint-steps", type=int, default=32,
                     help="steps of the forward+adjoint measurement (0 skips it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -469,7 +470,7 @@ def main():
            "d2h_bytes_per_step": 24 * n}
 
     # forward + adjoint (step_backward) on the same world: a taped forward of K steps (each
-    # substep's solver record kept, or checkpoints every --adjoint-every steps), then the reverse
+    # substep's solver record kept, or checkpoints every --adjoint-every substeps), then the reverse
     # pass, for a loss of the kinetic energy of the water beyond x = 1 m (gradients with respect
     # to every initial velocity and the settings)
     adjoint = None

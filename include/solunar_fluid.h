@@ -303,10 +303,10 @@ typedef struct slf_param_grads {
 } slf_param_grads;
 
 /* Starts recording the steps that follow for slf_step_backward.  checkpoint_every = k > 0: the
- * current state is the first checkpoint and the state after every k-th step is kept too (segment
- * checkpointing, 36 bytes per particle per checkpoint: the backward pass runs each segment
- * forward again from its checkpoint, recording its substeps, which holds one segment's records
- * at a time).  checkpoint_every = 0:
+ * current state is the first checkpoint and the state before every k-th substep is kept too
+ * (segment checkpointing, 36 bytes per particle per checkpoint: the backward pass runs each
+ * segment of k substeps forward again from its checkpoint, recording them, which holds one
+ * segment's records at a time, however many substeps the flow makes a step take).  checkpoint_every = 0:
  * every substep keeps the state before it and its solver record (the rates and velocities of each
  * DFSPH iteration), about 68 + 20 x iterations bytes per particle per substep; the backward pass
  * then redoes only each substep's sort and densities.  The number of particles must not change

@@ -443,7 +443,8 @@ struct World {
         uint32_t every = 1;
         uint64_t n = 0;
         std::vector<std::vector<float>> steps;  // substep lengths of each recorded step
-        std::vector<size_t> ckpt_step;          // checkpoint c = the state before step ckpt_step[c]
+        size_t count = 0;                       // substeps recorded so far
+        std::vector<size_t> ckpt_sub;           // checkpoint c = the state before substep ckpt_sub[c]
         DevBuf<float4> cpos, cvel;              // [c][n]
         DevBuf<uint32_t> cids;
         DevBuf<int4> ccells;                    // cell-relative positions: [c][n]
@@ -962,7 +963,9 @@ struct World {
     // the tape's buffers (records, checkpoints, solver scratch) stay for the next tape
     int32_t tape_end();
 
-    // the committed state becomes checkpoint number ckpt_step.size()
+    // the committed state becomes checkpoint number ckpt_sub.size(), before substep tape.count
+    // a substep of a recorded step: the checkpoint due before it (every k-th substep), then its length
+    int32_t tape_substep(float dt);
     int32_t checkpoint();
 
     // the committed state (positions, velocities, ids and, for cell-relative positions, cells) to

@@ -24,7 +24,8 @@ int32_t World::tape_begin(uint32_t every) {
     tape.every = every;
     tape.n = n;
     tape.steps.clear();
-    tape.ckpt_step.clear();
+    tape.count = 0;
+    tape.ckpt_sub.clear();
     drop_records(0);
     return every ? checkpoint() : SLF_OK;
 }
@@ -51,20 +52,29 @@ int32_t World::record_begin(float dt) {
 int32_t World::tape_end() {
     tape.on = false;
     tape.steps.clear();
-    tape.ckpt_step.clear();
+    tape.count = 0;
+    tape.ckpt_sub.clear();
     drop_records(0);
     return sync();
 }
 
 int32_t World::checkpoint() {
-    size_t c = tape.ckpt_step.size(), m = n;
+    size_t c = tape.ckpt_sub.size(), m = n;
     SLF_TRY(tape.cpos.ensure((c + 1) * m, c * m, stream));
     SLF_TRY(tape.cvel.ensure((c + 1) * m, c * m, stream));
     SLF_TRY(tape.cids.ensure((c + 1) * m, c * m, stream));
     if (rel()) SLF_TRY(tape.ccells.ensure((c + 1) * m, c * m, stream));
     SLF_TRY(save_state(tape.cpos.p + c * m, tape.cvel.p + c * m, tape.cids.p + c * m,
                        rel() ? tape.ccells.p + c * m : nullptr));
-    tape.ckpt_step.push_back(tape.steps.size());
+    tape.ckpt_sub.push_back(tape.count);
+    return SLF_OK;
+}
+
+int32_t World::tape_substep(float dt) {
+    if (!tape_step) return SLF_OK;
+    if (tape.every && tape.count > 0 && tape.count % tape.every == 0) SLF_TRY(checkpoint());
+    tape_step->push_back(dt);
+    ++tape.count;
     return SLF_OK;
 }
 
@@ -261,12 +271,13 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
             segsubs.clear();
         };
         auto segs = [&]() -> int32_t {
-            for (size_t c = tape.ckpt_step.size(); c-- > 0;) {
-                size_t b = tape.ckpt_step[c];
-                size_t e = c + 1 < tape.ckpt_step.size() ? tape.ckpt_step[c + 1] : tape.steps.size();
+            std::vector<float> all;  // every recorded substep's length, in order
+            for (const auto& st : tape.steps) all.insert(all.end(), st.begin(), st.end());
+            for (size_t c = tape.ckpt_sub.size(); c-- > 0;) {
+                size_t b = tape.ckpt_sub[c];
+                size_t e = c + 1 < tape.ckpt_sub.size() ? tape.ckpt_sub[c + 1] : all.size();
                 if (b >= e) continue;
-                std::vector<float> dts;
-                for (size_t t = b; t < e; ++t) dts.insert(dts.end(), tape.steps[t].begin(), tape.steps[t].end());
+                std::vector<float> dts(all.begin() + b, all.begin() + e);
                 while (segsubs.size() < dts.size()) segsubs.push_back(new_record());
                 SLF_TRY(load_state(tape.cpos.p + c * n, tape.cvel.p + c * n, tape.cids.p + c * n,
                                    rel() ? tape.ccells.p + c * n : nullptr));
@@ -355,7 +366,7 @@ int32_t World::step_untaped(float dt, slf_report* out) {
             float small = dt / float(substeps);
             for (uint32_t i = 0; i < substeps; ++i) {
                 uint32_t held = 0;
-                if (tape_step) tape_step->push_back(small);
+                SLF_TRY(tape_substep(small));
                 if (tape_step && tape.every == 0) SLF_TRY(record_begin(small));
                 if (!coupled.empty()) SLF_TRY(carry_movers(small * float(i), small * float(substeps - 1)));
                 int32_t st = wcsph_substep(small, held);
@@ -382,7 +393,7 @@ int32_t World::step_untaped(float dt, slf_report* out) {
                 }
                 small = rmin(small, left);
                 uint32_t held = 0, its = 0;
-                if (tape_step) tape_step->push_back(small);
+                SLF_TRY(tape_substep(small));
                 DfsphRecord* rec = nullptr;
                 if (tape_step && tape.every == 0) {
                     SLF_TRY(record_begin(small));

@@ -449,15 +449,16 @@ int32_t World::step(float dt, slf_report* out) {
         return fail(SLF_ERR_UNSUPPORTED, "the particles changed while a tape was recording");
     tape.steps.emplace_back();
     tape_step = &tape.steps.back();
-    size_t recorded = tape.subs.size();
+    size_t recorded = tape.subs.size(), checkpoints = tape.ckpt_sub.size();
     int32_t st = step_untaped(dt, out);
     tape_step = nullptr;
-    if (st != SLF_OK) {
+    if (st != SLF_OK) {  // the failed step's substeps and checkpoints are forgotten
+        tape.count -= tape.steps.back().size();
         tape.steps.pop_back();
+        tape.ckpt_sub.resize(checkpoints);
         drop_records(recorded);
         return st;
     }
-    if (tape.every && tape.steps.size() % tape.every == 0) SLF_TRY(checkpoint());
     return SLF_OK;
 }
 

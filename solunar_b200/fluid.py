@@ -382,8 +382,9 @@ class FluidWorld:
 
     # ---- the adjoint ----
     def tape_begin(self, checkpoint_every: int = 1):
-        """Records the steps that follow for step_backward: checkpoints every k-th state, or with
-        k = 0 keeps every substep's state and solver record (no forward recomputation)."""
+        """Records the steps that follow for step_backward: keeps the state before every k-th
+        substep as a checkpoint, or with k = 0 keeps every substep's state and solver record (no
+        forward recomputation)."""
         _check(_lib.slf_tape_begin(self._h, checkpoint_every))
 
     def tape_end(self):
