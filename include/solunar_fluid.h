@@ -38,7 +38,8 @@ enum {
     SLF_ERR_DISPATCH_INCOMPLETE = 5, /* PhysicsError::DispatchIncomplete (src/error.rs:15) */
     SLF_ERR_UNSUPPORTED = 6,         /* a combination not built: FAST arithmetic with terrain or bodies,
                                       * cell-relative positions with EXACT arithmetic, a tape with
-                                      * terrain, bodies or warm starts, shallow water */
+                                      * bodies or warm starts, terrain added while a tape records,
+                                      * shallow water */
     SLF_ERR_CUDA = 7,                /* a CUDA call failed; see slf_last_error() */
     SLF_ERR_TIMEOUT = 8,             /* a bounded device loop gave up */
     SLF_ERR_INVALID_ARGUMENT = 9,    /* null pointer or wrong buffer size */
@@ -306,13 +307,15 @@ typedef struct slf_param_grads {
  * current state is the first checkpoint and the state before every k-th substep is kept too
  * (segment checkpointing, 36 bytes per particle per checkpoint: the backward pass runs each
  * segment of k substeps forward again from its checkpoint, recording them, which holds one
- * segment's records at a time, however many substeps the flow makes a step take).  checkpoint_every = 0:
+ * segment's records at a time, however many substeps the flow makes a step take).
+ * checkpoint_every = 0:
  * every substep keeps the state before it and its solver record (the rates and velocities of each
  * DFSPH iteration), about 68 + 20 x iterations bytes per particle per substep; the backward pass
  * then redoes only each substep's sort and densities.  The number of particles must not change
  * while recording.  WCSPH and DFSPH steps, absolute or cell-relative positions (cell-relative
- * checkpoints and records add the 16-byte cell of each particle); UNSUPPORTED with terrain,
- * coupled bodies or warm_start. */
+ * checkpoints and records add the 16-byte cell of each particle), WCSPH worlds with terrain
+ * (the ground's density, push and damping and terrain contact are differentiated; terrain added
+ * while recording is UNSUPPORTED); UNSUPPORTED with coupled bodies or warm_start. */
 int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
 /* Stops recording.  The tape's device buffers (substep records, checkpoints) stay with the world
  * and are reused by the next tape, so the rounds of an optimisation loop record without

@@ -216,19 +216,149 @@ __device__ __forceinline__ void walk_gradients_mixed(const PairLists& l, uint32_
     }
 }
 
+// ---- terrain (terrain.rs) ------------------------------------------------------------------
+// The trilinear distance is linear along each axis inside a cell: its second derivatives are
+// zero on the diagonal and hxy, hxz, hyz off it.  hess_times(c, step, b) = H b.
+__device__ __forceinline__ float3 hess_times(const TerrainCell& c, float step, float3 b) {
+    float g00 = c.b00 - c.a00, g10 = c.b10 - c.a10, g01 = c.b01 - c.a01, g11 = c.b11 - c.a11;
+    float v00 = c.a00 + g00 * c.fx, v10 = c.a10 + g10 * c.fx, v01 = c.a01 + g01 * c.fx, v11 = c.a11 + g11 * c.fx;
+    float hxy = (g10 - g00) + ((g11 - g01) - (g10 - g00)) * c.fz;
+    float hxz = (g01 + (g11 - g01) * c.fy) - (g00 + (g10 - g00) * c.fy);
+    float hyz = (v11 - v01) - (v10 - v00);
+    float s2 = 1.0f / (step * step);
+    return make_float3((hxy * b.y + hxz * b.z) * s2, (hxy * b.x + hyz * b.z) * s2, (hxz * b.x + hyz * b.y) * s2);
+}
+
+// The adjoint of n = normalize_or(Y)(c): c-bar from n-bar (zero where the forward fell back to Y).
+__device__ __forceinline__ float3 unit_adjoint(float3 c, float3 n, float3 nbar) {
+    float len = sqrtf(c.x * c.x + c.y * c.y + c.z * c.z);
+    if (!(isfinite(len) && len > 0.0f)) return make_float3(0.0f, 0.0f, 0.0f);
+    return (nbar - n * dotf(n, nbar)) * (1.0f / len);
+}
+
+// The ground's slope at particle x (ground_near, terrain.rs:144-171, 305-310) is the sum over the
+// sites whose solid share lies strictly inside (0, 1) of -change(x + o) w / spacing; returns
+// (d slope / d x)^T b, the sites and their shares taken as the forward took them.
+__device__ __forceinline__ float3 ground_slope_adjoint(const TerrainDev& T, float3 x, float3 b) {
+    float3 out = make_float3(0.0f, 0.0f, 0.0f);
+    const float half = __fdiv_rn(T.spacing, 2.0f);
+    for (uint32_t r = 0; r < T.regions; ++r) {
+        const TerrainRegion& t = T.region[r];
+        float distance;
+        float3 change;
+        if (!terrain_read(T, t, x.x, x.y, x.z, distance, change)) continue;
+        if (!(distance < T.reach)) continue;
+        const float open = __fsub_rn(distance, half);
+        for (uint32_t k = 0; k < T.sites; ++k) {
+            if (__ldg(&T.far[k]) <= open) continue;
+            const float4 o = __ldg(&T.site[k]);
+            TerrainCell c;
+            if (!terrain_cell(T, t, __fadd_rn(x.x, o.x), __fadd_rn(x.y, o.y), __fadd_rn(x.z, o.z), c)) continue;
+            float there;
+            float3 toward;
+            terrain_values(c, t.step, there, toward);
+            const float v = __fsub_rn(0.5f, __fdiv_rn(there, T.spacing));
+            if (!(v > 0.0f && v < 1.0f)) continue;
+            out = out - hess_times(c, t.step, b) * (o.w / T.spacing);
+        }
+    }
+    return out;
+}
+
+// The ground's damping in the wall viscosity (step.rs:281-296): for each region holding x with
+// v . n < 0, a -= n nu_w (v . n) weight(d) / rho.  Adds its adjoint for a-bar ai.
+__device__ __forceinline__ void ground_damping_adjoint(const TerrainDev& T, float nuw, float3 x, float3 v, float rho,
+                                                       float3 ai, float3& xbar, float3& vbar, float& rbar,
+                                                       double& nuw_bar) {
+    for (uint32_t r = 0; r < T.regions; ++r) {
+        const TerrainRegion& t = T.region[r];
+        TerrainCell c;
+        if (!terrain_cell(T, t, x.x, x.y, x.z, c)) continue;
+        float d;
+        float3 ch;
+        terrain_values(c, t.step, d, ch);
+        const float3 n = normalize_or_up(ch);
+        const float into = dot3(v.x, v.y, v.z, n.x, n.y, n.z);
+        if (!(into < 0.0f)) continue;
+        float wslope;
+        const float weight = ground_damping(T, d, &wslope);
+        const float cc = nuw * into * weight / rho;
+        const float cbar = -dotf(ai, n);  // L = -cc (a-bar . n)
+        const float intobar = cbar * nuw * weight / rho;
+        rbar += -cbar * cc / rho;
+        nuw_bar += (double)(cbar * into * weight / rho);
+        vbar = vbar + n * intobar;
+        const float3 nbar = ai * (-cc) + v * intobar;
+        const float dbar = cbar * nuw * into / rho * wslope;
+        xbar = xbar + ch * dbar + hess_times(c, t.step, unit_adjoint(ch, n, nbar));
+    }
+}
+
+// terrain_contact (terrain.rs:314-333) backwards: (ybar, vbar) after every region's contact ->
+// before the first, the state before it (y0, v0) as the forward had it.  Each region's own state
+// is found by running the regions before it again.
+__device__ __forceinline__ void contact_adjoint(const TerrainDev& T, float rest, float3 y0, float4 v0, float3& ybar,
+                                                float3& vbar) {
+    for (uint32_t r = T.regions; r-- > 0;) {
+        float3 y = y0;
+        float4 v = v0;
+        bool under = false;
+        for (uint32_t q = 0; q < r; ++q) contact_region(T, T.region[q], rest, y.x, y.y, y.z, v, under);
+        const TerrainRegion& t = T.region[r];
+        TerrainCell c;
+        if (!terrain_cell(T, t, y.x, y.y, y.z, c)) continue;
+        float d;
+        float3 ch;
+        terrain_values(c, t.step, d, ch);
+        if (!(d < rest)) continue;
+        const float3 n = normalize_or_up(ch);
+        const float into = dot3(v.x, v.y, v.z, n.x, n.y, n.z);
+        // y' = y + n (rest - d); v' = v - n (v . n) when v . n < 0
+        float3 nbar = ybar * (rest - d);
+        const float dbar = -dotf(n, ybar);
+        if (into < 0.0f) {
+            const float nv = dotf(n, vbar);
+            nbar = nbar - (vbar * into + f3(v) * nv);
+            vbar = vbar - n * nv;
+        }
+        ybar = ybar + ch * dbar + hess_times(c, t.step, unit_adjoint(ch, n, nbar));
+    }
+}
+
 // ---- advance and velocity update (step.rs:212-222, 305-339) ---------------------------------
 // y = x + v' dt is clamped per component; a clamped component passes no adjoint to y and zeroes
 // v'.  v' = v + a dt.  Gravity's gradient is the sum of a-bar.
+// Terrain contact, after the clamp, goes back first (contact_adjoint): pos holds the substep's
+// sorted positions, from which the forward's position before contact is formed again.
 __global__ void k_adj_advance(Params p, const StepConsts* __restrict__ sc, const float4* __restrict__ vel_pre,
                               const float4* __restrict__ xo, const float4* __restrict__ vo,
                               float4* __restrict__ ab, float4* __restrict__ xb, float4* __restrict__ vb,
-                              double* __restrict__ grads) {
+                              double* __restrict__ grads, const float4* __restrict__ pos, TerrainDev T) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double gx = 0.0, gy = 0.0, gz = 0.0;
     if (i < p.n) {
         const float dt = sc->dt;
-        uint32_t flags = __float_as_uint(vel_pre[i].w);
+        const float4 pre = vel_pre[i];
+        uint32_t flags = __float_as_uint(pre.w);
         float4 x = xo[i], v = vo[i];
+        if (T.regions) {
+            // advance_one's position and velocity before contact: x + v' dt, clamped
+            const float4 a = pos[i];
+            float3 y = make_float3(__fadd_rn(a.x, __fmul_rn(pre.x, dt)), __fadd_rn(a.y, __fmul_rn(pre.y, dt)),
+                                   __fadd_rn(a.z, __fmul_rn(pre.z, dt)));
+            float4 w = make_float4(pre.x, pre.y, pre.z, 0.0f);
+            if (p.has_bounds) {
+                y = make_float3(fminf(fmaxf(y.x, p.low_in.x), p.high_in.x), fminf(fmaxf(y.y, p.low_in.y), p.high_in.y),
+                                fminf(fmaxf(y.z, p.low_in.z), p.high_in.z));
+                if (flags & 1u) w.x = 0.0f;
+                if (flags & 2u) w.y = 0.0f;
+                if (flags & 4u) w.z = 0.0f;
+            }
+            float3 ybar = f3(x), wbar = f3(v);
+            contact_adjoint(T, __fdiv_rn(p.spacing, 2.0f), y, w, ybar, wbar);
+            x = make_float4(ybar.x, ybar.y, ybar.z, 0.0f);
+            v = make_float4(wbar.x, wbar.y, wbar.z, 0.0f);
+        }
         float yx = flags & 1u ? 0.0f : x.x, yy = flags & 2u ? 0.0f : x.y, yz = flags & 4u ? 0.0f : x.z;
         float wx = (flags & 1u ? 0.0f : v.x) + yx * dt;
         float wy = (flags & 2u ? 0.0f : v.y) + yy * dt;
@@ -247,7 +377,8 @@ __global__ void k_adj_advance(Params p, const StepConsts* __restrict__ sc, const
 // ---- forces (step.rs:173-211), wall viscosity (step.rs:262-301), Tait pressure (step.rs:147-172)
 // PRESSURE = false: the DFSPH viscosity pass (dfsph.rs:90-99), the same pairs without pressure,
 // so the pressure records are neither gathered nor differentiated
-template <bool PRESSURE>
+// TERRAIN: the ground's terms as well (WCSPH worlds with terrain regions)
+template <bool PRESSURE, bool TERRAIN = false>
 __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                       PairLists wl, int form, const float4* __restrict__ pos,
                                                       const float4* __restrict__ vel, const float* __restrict__ rho,
@@ -256,7 +387,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
                                                       const float4* __restrict__ walls,
                                                       const float4* __restrict__ ab, float4* __restrict__ xb,
                                                       float4* __restrict__ vb, float* __restrict__ rb,
-                                                      double* __restrict__ grads, int add_rho) {
+                                                      double* __restrict__ grads, int add_rho, TerrainDev T,
+                                                      const float4* __restrict__ slope) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     double nu_bar = 0.0, nuw_bar = 0.0, b_bar = 0.0;
@@ -375,6 +507,19 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
             }
         }
 
+        // terrain (WCSPH): the ground's push with the particle's own pressure (step.rs:203-205),
+        // a -= slope M, and its damping in the wall viscosity
+        if (PRESSURE && TERRAIN) {
+            if (slope) {
+                const float3 sl = f3(slope[i]);
+                const float as = dotf(ai, sl);
+                sbar -= as;
+                pbar -= as * p.inv_rest_sq;
+                xbar = xbar + ground_slope_adjoint(T, xi, ai * (-M));
+            }
+            ground_damping_adjoint(T, nuw, xi, vi, rho_i, ai, xbar, vbar, rbar, nuw_bar);
+        }
+
         // s = p / rho^2 and the Tait equation of state
         if (PRESSURE) {
             float ptot = pbar + sbar / (rho_i * rho_i);
@@ -396,10 +541,13 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
 }
 
 // ---- densities (mod.rs:621-675): rho_i = m (sum_j W(r_ij) + sum_w W(r_iw)) ---------------------
+// slope (optional): the ground's density gradient of each particle, from the density pass (the
+// ground's part of rho, whose derivative it is)
 __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, PairLists wl, int form,
                                                         const float4* __restrict__ pos,
                                                         const float4* __restrict__ walls,
-                                                        const float* __restrict__ rb, float4* __restrict__ xb) {
+                                                        const float* __restrict__ rb, float4* __restrict__ xb,
+                                                        const float4* __restrict__ slope) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
@@ -430,6 +578,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
         grad_factor(p, d, g, gp);
         xbar = xbar + r * (g * p.mass * rbi);
     }
+    if (slope) xbar = xbar + f3(slope[i]) * rbi;
     float4 x0 = xb[i];
     xb[i] = make_float4(x0.x + xbar.x, x0.y + xbar.y, x0.z + xbar.z, 0.0f);
 }
@@ -725,13 +874,18 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
                           int form, const float4* pos, const float4* vel, const float* rho, const float* press,
                           const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
                           const float4* xo, const float4* vo, float4* ab, float4* xb, float4* vb, float* rb,
-                          float4* xp, float4* vp, double* grads, cudaStream_t s) {
+                          float4* xp, float4* vp, double* grads, const TerrainDev& T, const float4* slope,
+                          cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = adj_blocks(p.n);
-    k_adj_advance<<<nb, kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, ab, xb, vb, grads);
-    k_adj_force<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
-                                                         walls, ab, xb, vb, rb, grads, 0);
-    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb);
+    k_adj_advance<<<nb, kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, ab, xb, vb, grads, pos, T);
+    if (T.regions)
+        k_adj_force<true, true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
+                                                                   walls, ab, xb, vb, rb, grads, 0, T, slope);
+    else
+        k_adj_force<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
+                                                             walls, ab, xb, vb, rb, grads, 0, T, slope);
+    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, T.regions ? slope : nullptr);
     k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp);
 }
 
@@ -770,7 +924,7 @@ void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists
     if (!p.n) return;
     k_adj_scale<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, w, ab, grads);
     k_adj_force<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, zeros, zeros,
-                                                          walls, ab, xb, w, rb, grads, 1);
+                                                          walls, ab, xb, w, rb, grads, 1, TerrainDev{}, nullptr);
 }
 
 void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, int form,
@@ -779,7 +933,7 @@ void launch_adj_factors_density(const Params& p, const PairLists& fl, const Pair
     if (!p.n) return;
     k_adj_alpha_prep<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, alpha, abar, gt);
     k_adj_alpha<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, gt, xb);
-    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb);
+    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, nullptr);
 }
 
 void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const float4* vb, float4* xp, float4* vp,

@@ -245,6 +245,114 @@ __device__ __forceinline__ int3 cell_of(const Params& p, float x, float y, float
                      __float2int_rz(floorf(__fdiv_rn(z, p.radius))));
 }
 
+// ---- terrain fields (src/fluid/terrain.rs) ---------------------------------------------------
+// Every operation is rounded on its own through the intrinsics, so the EXACT forward and the
+// adjoint (compiled with contraction on) sample the same bits and take the same branches.
+
+__device__ __forceinline__ float lerp_rn(float a, float b, float u) { return __fadd_rn(a, __fmul_rn(__fsub_rn(b, a), u)); }
+
+// The corners of the field cell holding a point, and the point's place in it.
+struct TerrainCell {
+    float a00, b00, a10, b10, a01, b01, a11, b11;  // a: x low, b: x high; digits: y, z
+    float fx, fy, fz;
+};
+
+// The cell of TerrainField::read (terrain.rs:100-136); false outside the region.
+__device__ __forceinline__ bool terrain_cell(const TerrainDev& T, const TerrainRegion& t, float px, float py,
+                                             float pz, TerrainCell& c) {
+    float lx = __fdiv_rn(__fsub_rn(px, t.lx), t.step), ly = __fdiv_rn(__fsub_rn(py, t.ly), t.step),
+          lz = __fdiv_rn(__fsub_rn(pz, t.lz), t.step);
+    if (!(lx >= 0.0f && lx <= float(t.nx - 1) && ly >= 0.0f && ly <= float(t.ny - 1) && lz >= 0.0f &&
+          lz <= float(t.nz - 1)))
+        return false;
+    uint32_t x = min(uint32_t(floorf(lx)), t.nx - 2), y = min(uint32_t(floorf(ly)), t.ny - 2),
+             z = min(uint32_t(floorf(lz)), t.nz - 2);
+    c.fx = __fsub_rn(lx, float(x));
+    c.fy = __fsub_rn(ly, float(y));
+    c.fz = __fsub_rn(lz, float(z));
+    const float* d = T.dist + t.offset;
+    auto corner = [&](uint32_t dx, uint32_t dy, uint32_t dz) {
+        return __ldg(&d[(size_t(y + dy) * t.nz + (z + dz)) * t.nx + (x + dx)]);
+    };
+    c.a00 = corner(0, 0, 0), c.b00 = corner(1, 0, 0), c.a10 = corner(0, 1, 0), c.b10 = corner(1, 1, 0);
+    c.a01 = corner(0, 0, 1), c.b01 = corner(1, 0, 1), c.a11 = corner(0, 1, 1), c.b11 = corner(1, 1, 1);
+    return true;
+}
+
+// The trilinear distance in a cell and its change per axis (terrain.rs:100-136).
+__device__ __forceinline__ void terrain_values(const TerrainCell& c, float step, float& value, float3& change) {
+    float v00 = lerp_rn(c.a00, c.b00, c.fx), g00 = __fsub_rn(c.b00, c.a00);
+    float v10 = lerp_rn(c.a10, c.b10, c.fx), g10 = __fsub_rn(c.b10, c.a10);
+    float v01 = lerp_rn(c.a01, c.b01, c.fx), g01 = __fsub_rn(c.b01, c.a01);
+    float v11 = lerp_rn(c.a11, c.b11, c.fx), g11 = __fsub_rn(c.b11, c.a11);
+    float v0 = lerp_rn(v00, v10, c.fy), v1 = lerp_rn(v01, v11, c.fy);
+    value = lerp_rn(v0, v1, c.fz);
+    change = make_float3(__fdiv_rn(lerp_rn(lerp_rn(g00, g10, c.fy), lerp_rn(g01, g11, c.fy), c.fz), step),
+                         __fdiv_rn(lerp_rn(__fsub_rn(v10, v00), __fsub_rn(v11, v01), c.fz), step),
+                         __fdiv_rn(__fsub_rn(v1, v0), step));
+}
+
+// TerrainField::read (terrain.rs:100-136): the trilinear distance at a point and its change per
+// axis; false outside the region.
+__device__ __forceinline__ bool terrain_read(const TerrainDev& T, const TerrainRegion& t, float px, float py,
+                                             float pz, float& value, float3& change) {
+    TerrainCell c;
+    if (!terrain_cell(T, t, px, py, pz, c)) return false;
+    terrain_values(c, t.step, value, change);
+    return true;
+}
+
+// normalize_or(Y) dividing by the length
+__device__ __forceinline__ float3 normalize_or_up(float3 c) {
+    float len = __fsqrt_rn(dot3(c.x, c.y, c.z, c.x, c.y, c.z));
+    if (isfinite(len) && len > 0.0f) return make_float3(__fdiv_rn(c.x, len), __fdiv_rn(c.y, len), __fdiv_rn(c.z, len));
+    return make_float3(0.0f, 1.0f, 0.0f);
+}
+
+// TerrainField::sample (terrain.rs:139-142)
+__device__ __forceinline__ bool terrain_sample(const TerrainDev& T, const TerrainRegion& t, float px, float py,
+                                               float pz, float& distance, float3& normal) {
+    float3 change;
+    if (!terrain_read(T, t, px, py, pz, distance, change)) return false;
+    normal = normalize_or_up(change);
+    return true;
+}
+
+// One region of terrain_contact (terrain.rs:314-333): a particle at (x, y, z) nearer the
+// region's surface than `rest` goes back there and its velocity into the surface is removed.
+// Returns whether it was nearer; under: whether it was beneath the surface.
+__device__ __forceinline__ bool contact_region(const TerrainDev& T, const TerrainRegion& t, float rest, float& x,
+                                               float& y, float& z, float4& v, bool& under) {
+    float distance;
+    float3 gn;
+    if (!terrain_sample(T, t, x, y, z, distance, gn)) return false;
+    if (!(distance < rest)) return false;
+    under = under || distance < 0.0f;
+    float lift = __fsub_rn(rest, distance);
+    x = __fadd_rn(x, __fmul_rn(gn.x, lift));
+    y = __fadd_rn(y, __fmul_rn(gn.y, lift));
+    z = __fadd_rn(z, __fmul_rn(gn.z, lift));
+    float into = dot3(v.x, v.y, v.z, gn.x, gn.y, gn.z);
+    if (into < 0.0f) {
+        v.x = __fsub_rn(v.x, __fmul_rn(gn.x, into));
+        v.y = __fsub_rn(v.y, __fmul_rn(gn.y, into));
+        v.z = __fsub_rn(v.z, __fmul_rn(gn.z, into));
+    }
+    return true;
+}
+
+// GroundSites::damping (terrain.rs:241-249); slope (optional): its derivative in the distance
+__device__ __forceinline__ float ground_damping(const TerrainDev& T, float distance, float* slope = nullptr) {
+    float at = __fdiv_rn(__fsub_rn(fmaxf(distance, T.low), T.low), T.step);
+    uint32_t below = uint32_t(floorf(at));
+    if (slope) *slope = 0.0f;
+    if (below + 1 >= uint32_t(kGroundSamples)) return 0.0f;
+    float part = __fsub_rn(at, float(below));
+    float d0 = __ldg(&T.damping[below]), d1 = __ldg(&T.damping[below + 1]);
+    if (slope && distance > T.low) *slope = (d1 - d0) / T.step;
+    return __fadd_rn(d0, __fmul_rn(__fsub_rn(d1, d0), part));
+}
+
 // The candidates of one cell, points [b, e), two gathers in flight at a time; f(j, q) for each
 // point within reach, in array order.
 template <class F>

@@ -223,52 +223,7 @@ __global__ void k_scan_add(uint32_t* data, uint32_t m, const uint32_t* __restric
     if (blockIdx.x == 0 && threadIdx.x == 0) data[m] = tile_sums[gridDim.x];
 }
 
-// ---- terrain (src/fluid/terrain.rs) ------------------------------------------------------------
-
-// TerrainField::read (terrain.rs:100-136): the trilinear distance at a point and its change per
-// axis; false outside the region.
-__device__ __forceinline__ bool terrain_read(const TerrainDev& T, const TerrainRegion& t, float px, float py,
-                                             float pz, float& value, float3& change) {
-    float lx = (px - t.lx) / t.step, ly = (py - t.ly) / t.step, lz = (pz - t.lz) / t.step;
-    if (!(lx >= 0.0f && lx <= float(t.nx - 1) && ly >= 0.0f && ly <= float(t.ny - 1) && lz >= 0.0f &&
-          lz <= float(t.nz - 1)))
-        return false;
-    uint32_t x = min(uint32_t(floorf(lx)), t.nx - 2), y = min(uint32_t(floorf(ly)), t.ny - 2),
-             z = min(uint32_t(floorf(lz)), t.nz - 2);
-    float fx = lx - float(x), fy = ly - float(y), fz = lz - float(z);
-    const float* d = T.dist + t.offset;
-    auto corner = [&](uint32_t dx, uint32_t dy, uint32_t dz) {
-        return __ldg(&d[(size_t(y + dy) * t.nz + (z + dz)) * t.nx + (x + dx)]);
-    };
-    auto lerp = [](float a, float b, float u) { return a + (b - a) * u; };
-    float a00 = corner(0, 0, 0), b00 = corner(1, 0, 0), a10 = corner(0, 1, 0), b10 = corner(1, 1, 0);
-    float a01 = corner(0, 0, 1), b01 = corner(1, 0, 1), a11 = corner(0, 1, 1), b11 = corner(1, 1, 1);
-    float v00 = lerp(a00, b00, fx), g00 = b00 - a00;
-    float v10 = lerp(a10, b10, fx), g10 = b10 - a10;
-    float v01 = lerp(a01, b01, fx), g01 = b01 - a01;
-    float v11 = lerp(a11, b11, fx), g11 = b11 - a11;
-    float v0 = lerp(v00, v10, fy), v1 = lerp(v01, v11, fy);
-    value = lerp(v0, v1, fz);
-    change = make_float3(lerp(lerp(g00, g10, fy), lerp(g01, g11, fy), fz) / t.step,
-                         lerp(v10 - v00, v11 - v01, fz) / t.step, (v1 - v0) / t.step);
-    return true;
-}
-
-// normalize_or(Y) dividing by the length
-__device__ __forceinline__ float3 normalize_or_up(float3 c) {
-    float len = sqrtf(dot3(c.x, c.y, c.z, c.x, c.y, c.z));
-    if (isfinite(len) && len > 0.0f) return make_float3(c.x / len, c.y / len, c.z / len);
-    return make_float3(0.0f, 1.0f, 0.0f);
-}
-
-// TerrainField::sample (terrain.rs:139-142)
-__device__ __forceinline__ bool terrain_sample(const TerrainDev& T, const TerrainRegion& t, float px, float py,
-                                               float pz, float& distance, float3& normal) {
-    float3 change;
-    if (!terrain_read(T, t, px, py, pz, distance, change)) return false;
-    normal = normalize_or_up(change);
-    return true;
-}
+// ---- terrain (src/fluid/terrain.rs): the field's sampling is in fluid_device.cuh ---------------
 
 // ground_near (mod.rs:657-663, terrain.rs:144-171, 305-310): the density the terrain regions
 // holding the particle add, and the sum of their density gradients
@@ -304,16 +259,6 @@ __device__ __forceinline__ float ground_near(const TerrainDev& T, float px, floa
         slope = make_float3(slope.x + gx, slope.y + gy, slope.z + gz);
     }
     return ground;
-}
-
-// GroundSites::damping (terrain.rs:241-249)
-__device__ __forceinline__ float ground_damping(const TerrainDev& T, float distance) {
-    float at = (fmaxf(distance, T.low) - T.low) / T.step;
-    uint32_t below = uint32_t(floorf(at));
-    if (below + 1 >= uint32_t(kGroundSamples)) return 0.0f;
-    float part = at - float(below);
-    float d0 = __ldg(&T.damping[below]), d1 = __ldg(&T.damping[below + 1]);
-    return d0 + (d1 - d0) * part;
 }
 
 // The second half of a list-building walk: for each of row's first m listed neighbours, in list
@@ -892,34 +837,19 @@ __device__ __forceinline__ float3 wall_viscous(const Params& p, float wall_visc,
 
 // ---- advance (step.rs:305-339) --------------------------------------------------------------
 
-// terrain_contact (terrain.rs:314-333): a particle nearer a surface than `rest` goes back there,
-// its velocity into the surface removed; true when it got under a surface.
+// terrain_contact (terrain.rs:314-333): each region in turn; true when the particle got under a
+// surface.
 __device__ __forceinline__ bool terrain_contact(const TerrainDev& T, float rest, float& nx, float& ny, float& nz,
                                                 float4& v) {
     bool under = false;
-    for (uint32_t r = 0; r < T.regions; ++r) {
-        float distance;
-        float3 gn;
-        if (!terrain_sample(T, T.region[r], nx, ny, nz, distance, gn)) continue;
-        if (distance < rest) {
-            under = under || distance < 0.0f;
-            float lift = rest - distance;
-            nx = nx + gn.x * lift;
-            ny = ny + gn.y * lift;
-            nz = nz + gn.z * lift;
-            float into = dot3(v.x, v.y, v.z, gn.x, gn.y, gn.z);
-            if (into < 0.0f) {
-                v.x = v.x - gn.x * into;
-                v.y = v.y - gn.y * into;
-                v.z = v.z - gn.z * into;
-            }
-        }
-    }
+    for (uint32_t r = 0; r < T.regions; ++r) contact_region(T, T.region[r], rest, nx, ny, nz, v, under);
     return under;
 }
 
+// zeroed (optional): the components the container's clamp held (bits x, y, z), whose position
+// and velocity it set; terrain contact, after it, is not counted
 __device__ __forceinline__ void advance_one(const Params& p, float dt, float4& a, float4& v, uint32_t& held,
-                                            uint32_t& bad, const TerrainDev& T) {
+                                            uint32_t& bad, const TerrainDev& T, uint32_t* zeroed = nullptr) {
     float nx = a.x + v.x * dt, ny = a.y + v.y * dt, nz = a.z + v.z * dt;
     if (p.has_bounds) {
         float ix = fminf(fmaxf(nx, p.low_in.x), p.high_in.x);
@@ -930,6 +860,7 @@ __device__ __forceinline__ void advance_one(const Params& p, float dt, float4& a
             float cy = fminf(fmaxf(ny, p.low.y), p.high.y);
             float cz = fminf(fmaxf(nz, p.low.z), p.high.z);
             if (cx != nx || cy != ny || cz != nz) held += 1;
+            if (zeroed) *zeroed = (ix != nx ? 1u : 0u) | (iy != ny ? 2u : 0u) | (iz != nz ? 4u : 0u);
             if (ix != nx) v.x = 0.0f;
             if (iy != ny) v.y = 0.0f;
             if (iz != nz) v.z = 0.0f;
@@ -1168,10 +1099,10 @@ __global__ void __launch_bounds__(kBlock) k_wcsph_force_warp(Params p, const Ste
             v.y = v.y + ay * dt;
             v.z = v.z + az * dt;
             float4 pre = v;
-            advance_one(p, dt, a, v, held, bad, TerrainDev{});
+            uint32_t flags = 0;
+            advance_one(p, dt, a, v, held, bad, TerrainDev{}, &flags);
             if (vel_pre) {
                 // the velocity before the wall zeroed any component, and which ones it zeroed
-                uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
                 pre.w = __uint_as_float(flags);
                 vel_pre[i] = pre;
             }
@@ -1248,10 +1179,10 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_wcsph_force(Par
         v.y = v.y + ay * dt;
         v.z = v.z + az * dt;
         float4 pre = v;
-        advance_one(p, dt, a, v, held, bad, T);
+        uint32_t flags = 0;
+        advance_one(p, dt, a, v, held, bad, T, &flags);
         if (vel_pre) {
             // the velocity before the wall zeroed any component, and which ones it zeroed
-            uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
             pre.w = __uint_as_float(flags);
             vel_pre[i] = pre;
         }
@@ -1435,9 +1366,9 @@ __global__ void k_advance(Params p, const StepConsts* __restrict__ sc, const flo
         float4 a = pos_in[i];
         float4 v = vel[i];
         float4 pre = v;
-        advance_one(p, sc->dt, a, v, held, bad, TerrainDev{});
+        uint32_t flags = 0;
+        advance_one(p, sc->dt, a, v, held, bad, TerrainDev{}, &flags);
         if (vel_pre) {
-            uint32_t flags = (v.x != pre.x ? 1u : 0u) | (v.y != pre.y ? 2u : 0u) | (v.z != pre.z ? 4u : 0u);
             pre.w = __uint_as_float(flags);
             vel_pre[i] = pre;
         }

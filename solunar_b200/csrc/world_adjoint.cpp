@@ -17,7 +17,6 @@ int32_t World::sync() {
 }
 
 int32_t World::tape_begin(uint32_t every) {
-    if (!terrains.empty()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint takes no terrain");
     if (warm_on()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on cold-started solves only");
     SLF_TRY(flush());
     tape.on = true;
@@ -171,7 +170,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
             if (s.solver == SLF_SOLVER_WCSPH) {
                 launch_adjoint_wcsph(p, d_consts, fl, wl, form, pos[a].p, vel[a].p, rho[nid].p, press.p,
                                      scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p, xb.p, vb.p, rb.p, xp.p,
-                                     vp.p, grads.p, stream);
+                                     vp.p, grads.p, tdev, terrains.empty() ? nullptr : gslope.p, stream);
             } else {
                 // advance, density solve, viscosity, divergence solve, factors, densities,
                 // sort: the substep's steps backwards

@@ -163,6 +163,7 @@ int32_t World::terrain_nodes(const float* low, const float* high, uint64_t nodes
 
 int32_t World::add_terrain(const float* low, const float* high, const float* distances, uint64_t count, uint32_t* out) {
     if (fast()) return fail(SLF_ERR_UNSUPPORTED, "terrain runs with EXACT arithmetic only");
+    if (tape.on) return fail(SLF_ERR_UNSUPPORTED, "terrain is added before a tape begins, not while it records");
     uint64_t nodes[3];
     SLF_TRY(terrain_nodes(low, high, nodes));
     if (count != nodes[0] * nodes[1] * nodes[2])
