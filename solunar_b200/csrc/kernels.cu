@@ -1405,13 +1405,24 @@ __global__ void k_list_fill(Params p, GridDev g, const float4* __restrict__ pos,
 }
 
 // ---- the walk order of the list passes (PairLists::order) -------------------------------------
-// Cells taken in 2 x 2-column bricks: key = ((x / 2, y / 2), z, x % 2, y % 2) over the dense box,
-// so 256 consecutive rows cover about 2 x 2 x 8 cells instead of a 1 x 1 x 32 column.
+// Cells taken in 2 x 2-column bricks, so 256 consecutive rows cover about 2 x 2 x 8 cells instead
+// of a 1 x 1 x 32 column.  SLF_WALK_ZQUAD 0: key = ((x / 2, y / 2), z, x % 2, y % 2); 1: the
+// brick's z split in quads, key = ((x / 2, y / 2), z / 4, x % 2, y % 2, z % 4), so a warp's 32
+// rows are (about) four consecutive cells of one column, whose neighbours lie in consecutive
+// cells of the same neighbouring columns: a warp's gathers touch fewer cache lines.
+#ifndef SLF_WALK_ZQUAD
+#define SLF_WALK_ZQUAD 1
+#endif
+
+__host__ __device__ __forceinline__ uint32_t walk_quads(int z) { return SLF_WALK_ZQUAD ? (uint32_t(z) + 3u) / 4u : uint32_t(z); }
 
 __device__ __forceinline__ uint32_t brick_key(uint32_t lin, int3 span) {
     uint32_t z = lin % (uint32_t)span.z, xy = lin / (uint32_t)span.z;
     uint32_t y = xy % (uint32_t)span.y, x = xy / (uint32_t)span.y;
     uint32_t by = ((uint32_t)span.y + 1u) / 2u;
+    if (SLF_WALK_ZQUAD)
+        return ((((x >> 1) * by + (y >> 1)) * walk_quads(span.z) + (z >> 2)) * 4u + (x & 1u) * 2u + (y & 1u)) * 4u +
+               (z & 3u);
     return (((x >> 1) * by + (y >> 1)) * (uint32_t)span.z + z) * 4u + (x & 1u) * 2u + (y & 1u);
 }
 
@@ -1852,7 +1863,7 @@ void launch_warm_kappa(const Params& p, const StepConsts* sc, float share, float
 }
 
 size_t walk_order_keys(int3 span) {
-    return size_t((span.x + 1) / 2) * size_t((span.y + 1) / 2) * size_t(span.z) * 4u;
+    return size_t((span.x + 1) / 2) * size_t((span.y + 1) / 2) * size_t(walk_quads(span.z)) * (SLF_WALK_ZQUAD ? 16u : 4u);
 }
 
 void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32_t* bcount, uint32_t* tile_sums,
