@@ -540,6 +540,204 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
     add_grads3(grads, kGradViscosity, kGradWallViscosity, kGradStiffness, nu_bar, nuw_bar, b_bar);
 }
 
+// ---- the same two adjoints a warp a row, for scenes too small to fill the GPU a thread a row ----
+// Each lane takes every 32nd entry of the row's lists; partial sums meet in butterfly sums, which
+// leave every lane with the same bits (each level adds x + y on one lane and y + x on its partner),
+// so the lanes agree on the wall normal they all form.  Run to run the sums are deterministic.
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float3 warp_sum3(float3 v) { return make_float3(warp_sum(v.x), warp_sum(v.y), warp_sum(v.z)); }
+
+constexpr uint32_t kAdjWarpMax = 262144u;  // rows a warp each up to this many particles
+
+// k_adj_force (WCSPH forces, wall viscosity, Tait pressure) a warp a row; no terrain.
+__global__ void __launch_bounds__(kBlock) k_adj_force_warp(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                           PairLists wl, int form, const float4* __restrict__ pos,
+                                                           const float4* __restrict__ vel, const float* __restrict__ rho,
+                                                           const float* __restrict__ press,
+                                                           const float* __restrict__ scaled,
+                                                           const float4* __restrict__ walls,
+                                                           const float4* __restrict__ ab, float4* __restrict__ xb,
+                                                           float4* __restrict__ vb, float* __restrict__ rb,
+                                                           double* __restrict__ grads) {
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+    double nu_bar = 0.0, nuw_bar = 0.0, b_bar = 0.0;
+    if (row < p.n) {
+        const uint32_t i = fl.particle(row);
+        const float nu = sc->viscosity, nuw = sc->wall_viscosity, m = p.mass;
+        const float3 xi = f3(pos[i]), vi = f3(vel[i]), ai = f3(ab[i]);
+        const float rho_i = rho[i], p_i = press[i], s_i = scaled[i];
+        float3 xbar = make_float3(0, 0, 0), vbar = make_float3(0, 0, 0);
+        float sbar = 0.0f, pbar = 0.0f, rbar = 0.0f;
+
+        // fluid pairs: L = (a_i-bar - a_j-bar) . T(r, u, S, R)
+        const uint32_t nf = listed_count(fl, row);
+        for (uint32_t k = lane; k < nf; k += 32u) {
+            const uint32_t e = listed_raw(fl, form, row, k), j = entry_index(e, form);
+            const float4 qa = __ldg(&pos[j]), qv = __ldg(&vel[j]), qb = __ldg(&ab[j]);
+            const float qr = __ldg(&rho[j]), qs = __ldg(&scaled[j]);
+            float3 r = pair_off(p, form, xi, qa, e);
+            float d2 = dotf(r, r), inv = inv_length(d2);
+            if (inv == 0.0f) continue;
+            float g, gp;
+            grad_factor(p, d2 * inv, g, gp);
+            float3 u = vi - f3(qv);
+            float3 w = ai - f3(qb);
+            float R = rho_i + qr;
+            float S = s_i + qs;
+            float ur = dotf(u, r);
+            bool act = ur < 0.0f;
+            float t = act ? ur : 0.0f;
+            float den = (d2 + p.soften) * R;
+            float Pi = -nu * t * 2.0f / den;
+            float G = dotf(w, r);
+            float P = -m * g * G;
+            float dPi_dt = -2.0f * nu / den;
+            float dPi_dd2 = -Pi / (d2 + p.soften);
+            float c1 = -m * (S + Pi);
+            float3 dr = w * (c1 * g) + r * (c1 * G * gp * inv + P * dPi_dd2 * 2.0f);
+            if (act) dr = dr + u * (P * dPi_dt);
+            xbar = xbar + dr;
+            if (act) vbar = vbar + r * (P * dPi_dt);
+            rbar += P * (-Pi / R);
+            sbar += P;
+            nu_bar += (double)(2.0f * m * g * t * dotf(ai, r) / den);
+        }
+
+        // walls: pressure mirrored onto the wall, and the wall normal's sum
+        const uint32_t nw = listed_count(wl, row);
+        const float M = s_i + p_i * p.inv_rest_sq;
+        float3 A = make_float3(0, 0, 0);
+        for (uint32_t k = lane; k < nw; k += 32u) {
+            const uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+            float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
+            float d2 = dotf(r, r), inv = inv_length(d2);
+            if (inv == 0.0f) continue;
+            float g, gp;
+            grad_factor(p, d2 * inv, g, gp);
+            float ar = dotf(ai, r);
+            float mb = -m * g * ar;
+            sbar += mb;
+            pbar += mb * p.inv_rest_sq;
+            xbar = xbar + (ai * g + r * (ar * gp * inv)) * (-m * M);
+            A = A - r * g;
+        }
+        A = warp_sum3(A);
+
+        // wall viscosity (every lane holds the same A, so the same normal and branch)
+        float alen = sqrtf(dotf(A, A));
+        if (nw > 0 && alen > 0.0f && isfinite(alen)) {
+            float3 nrm = A * (1.0f / alen);
+            float vn = dotf(vi, nrm);
+            float kk = fminf(vn, 0.0f);
+            float3 I = nrm * kk;
+            float3 Ibar = make_float3(0, 0, 0);
+            for (uint32_t k = lane; k < nw; k += 32u) {
+                const uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+                float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
+                float tau = dotf(I, r);
+                if (!(tau < 0.0f)) continue;
+                float d2 = dotf(r, r);
+                float d = sqrtf(d2);
+                float g, gp;
+                grad_factor(p, d, g, gp);
+                float e2 = d2 + p.soften;
+                float D = -nuw * tau / (e2 * rho_i);
+                float ar = dotf(ai, r);
+                float h = -m * g * ar;
+                float tb = h * (-nuw / (e2 * rho_i));
+                rbar += -D * h / rho_i;
+                nuw_bar += (double)(-tau / (e2 * rho_i) * h);
+                float3 dh = (ai * g + r * (ar * gp / d)) * (-m);
+                xbar = xbar + dh * D + r * (h * (-D / e2) * 2.0f) + I * tb;
+                Ibar = Ibar + r * tb;
+            }
+            Ibar = warp_sum3(Ibar);
+            float3 nbar = Ibar * kk;
+            if (vn < 0.0f) {
+                float kbar = dotf(Ibar, nrm);
+                if (lane == 0) vbar = vbar + nrm * kbar;
+                nbar = nbar + vi * kbar;
+            }
+            float3 Abar = (nbar - nrm * dotf(nrm, nbar)) * (1.0f / alen);
+            for (uint32_t k = lane; k < nw; k += 32u) {
+                const uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+                float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
+                float d = sqrtf(dotf(r, r));
+                if (d <= 0.0f) continue;
+                float g, gp;
+                grad_factor(p, d, g, gp);
+                xbar = xbar - (Abar * g + r * (dotf(Abar, r) * gp / d));
+            }
+        }
+
+        xbar = warp_sum3(xbar);
+        vbar = warp_sum3(vbar);
+        sbar = warp_sum(sbar);
+        pbar = warp_sum(pbar);
+        rbar = warp_sum(rbar);
+        if (lane == 0) {
+            // s = p / rho^2 and the Tait equation of state
+            float ptot = pbar + sbar / (rho_i * rho_i);
+            rbar += sbar * (-2.0f * p_i / (rho_i * rho_i * rho_i));
+            float raw = rho_i * p.inv_rest;
+            float ratio = fminf(raw, 1.1f);
+            float r2 = ratio * ratio, r3 = r2 * ratio, r6 = r3 * r3;
+            if (p_i > 0.0f) {
+                b_bar = (double)(ptot * (r6 * ratio - 1.0f));
+                if (raw < 1.1f) rbar += ptot * p.stiffness * 7.0f * r6 * p.inv_rest;
+            }
+            float4 x0 = xb[i], v0 = vb[i];
+            xb[i] = make_float4(x0.x + xbar.x, x0.y + xbar.y, x0.z + xbar.z, 0.0f);
+            vb[i] = make_float4(v0.x + vbar.x, v0.y + vbar.y, v0.z + vbar.z, 0.0f);
+            rb[i] = rbar;
+        }
+    }
+    add_grads3(grads, kGradViscosity, kGradWallViscosity, kGradStiffness, nu_bar, nuw_bar, b_bar);
+}
+
+// k_adj_density a warp a row.
+__global__ void __launch_bounds__(kBlock) k_adj_density_warp(Params p, PairLists fl, PairLists wl, int form,
+                                                             const float4* __restrict__ pos,
+                                                             const float4* __restrict__ walls,
+                                                             const float* __restrict__ rb, float4* __restrict__ xb) {
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+    if (row >= p.n) return;
+    const uint32_t i = fl.particle(row);
+    const float3 xi = f3(pos[i]);
+    const float rbi = rb[i];
+    float3 xbar = make_float3(0, 0, 0);
+    const uint32_t nf = listed_count(fl, row);
+    for (uint32_t k = lane; k < nf; k += 32u) {
+        const uint32_t e = listed_raw(fl, form, row, k), j = entry_index(e, form);
+        const float4 q = __ldg(&pos[j]);
+        float3 r = pair_off(p, form, xi, q, e);
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        xbar = xbar + r * (g * p.mass * (rbi + __ldg(&rb[j])));
+    }
+    const uint32_t nw = listed_count(wl, row);
+    for (uint32_t k = lane; k < nw; k += 32u) {
+        const uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
+        float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
+        float d = sqrtf(dotf(r, r));
+        if (d <= 0.0f) continue;
+        float g, gp;
+        grad_factor(p, d, g, gp);
+        xbar = xbar + r * (g * p.mass * rbi);
+    }
+    xbar = warp_sum3(xbar);
+    if (lane == 0) {
+        float4 x0 = xb[i];
+        xb[i] = make_float4(x0.x + xbar.x, x0.y + xbar.y, x0.z + xbar.z, 0.0f);
+    }
+}
+
 // ---- densities (mod.rs:621-675): rho_i = m (sum_j W(r_ij) + sum_w W(r_iw)) ---------------------
 // slope (optional): the ground's density gradient of each particle, from the density pass (the
 // ground's part of rho, whose derivative it is)
@@ -879,13 +1077,20 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
     if (!p.n) return;
     uint32_t nb = adj_blocks(p.n);
     k_adj_advance<<<nb, kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, ab, xb, vb, grads, pos, T);
-    if (T.regions)
+    if (T.regions) {
         k_adj_force<true, true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
                                                                    walls, ab, xb, vb, rb, grads, 0, T, slope);
-    else
+        k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, slope);
+    } else if (p.n <= kAdjWarpMax) {
+        // few rows: a warp each, so that the GPU fills
+        k_adj_force_warp<<<adj_blocks(p.n * 32u), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
+                                                                  walls, ab, xb, vb, rb, grads);
+        k_adj_density_warp<<<adj_blocks(p.n * 32u), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb);
+    } else {
         k_adj_force<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
                                                              walls, ab, xb, vb, rb, grads, 0, T, slope);
-    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, T.regions ? slope : nullptr);
+        k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, nullptr);
+    }
     k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp);
 }
 

@@ -428,14 +428,36 @@ struct World {
         DevBuf<uint32_t> ids;
         DevBuf<int4> cells;  // cell-relative positions: the cells of pos's offsets
         DfsphRecord rec;
+        // A WCSPH substep that a checkpoint segment ran again keeps what its adjoint reads (the
+        // sorted state, densities and pressures, the sort's destinations, the pre-clamp
+        // velocities, the ground slopes, the walk order and both neighbour lists, which change
+        // places with the world's), so the segment's reverse sweep runs no substep a third time.
+        bool kept = false;
+        bool ordered = false;  // the lists walk rows in `order`
+        uint32_t cap = 0;      // the lists' room a row
+        DevBuf<float4> spos, svel, pre, slope;
+        DevBuf<int4> scells;
+        DevBuf<float> rho, press, scaled;
+        DevBuf<uint32_t> dest, order, fcnt, wcnt;
+        DevBuf<uint2> fent, went;
         void release(cudaStream_t st) {
             pos.release(st);
             vel.release(st);
             ids.release(st);
             cells.release(st);
             rec.release(st);
+            for (auto* b : {&spos, &svel, &pre, &slope}) b->release(st);
+            scells.release(st);
+            for (auto* b : {&rho, &press, &scaled}) b->release(st);
+            for (auto* b : {&dest, &order, &fcnt, &wcnt}) b->release(st);
+            fent.release(st);
+            went.release(st);
+            kept = false;
         }
     };
+    // After a WCSPH substep of a segment's replay (its sort writing `sub.dest`, its advance
+    // `sub.pre`): the substep's forward into `sub` (SubRecord::kept).
+    int32_t keep_wcsph_substep(SubRecord& sub);
 
     // ---- the tape of slf_tape_begin: checkpoints and the substep lengths of each step ----
     struct Tape {

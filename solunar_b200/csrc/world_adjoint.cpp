@@ -7,7 +7,37 @@ auto World::new_record() -> std::unique_ptr<SubRecord> {
     if (spare_records.empty()) return std::make_unique<SubRecord>();
     auto r = std::move(spare_records.back());
     spare_records.pop_back();
+    r->kept = false;
     return r;
+}
+
+int32_t World::keep_wcsph_substep(SubRecord& sub) {
+    // the committed substep's sorted slots, as recompute names them
+    const int a = (cpos + 2) % 3, nid = cid;
+    auto copy = [&](auto& to, const auto* from, size_t count) -> int32_t {
+        SLF_TRY(to.ensure(count, 0, stream));
+        SLF_CUDA(cudaMemcpyAsync(to.p, from, count * sizeof(*from), cudaMemcpyDeviceToDevice, stream));
+        return SLF_OK;
+    };
+    SLF_TRY(copy(sub.spos, pos[a].p, n));
+    SLF_TRY(copy(sub.svel, vel[a].p, n));
+    SLF_TRY(copy(sub.rho, rho[nid].p, n));
+    SLF_TRY(copy(sub.press, press.p, n));
+    SLF_TRY(copy(sub.scaled, scaled.p, n));
+    if (rel()) SLF_TRY(copy(sub.scells, cell[a].p, n));
+    sub.ordered = walk_order() != nullptr;
+    if (sub.ordered) SLF_TRY(copy(sub.order, worder.p, n));
+    if (!terrains.empty()) SLF_TRY(copy(sub.slope, gslope.p, n));
+    // the lists change places: the record takes this substep's, the world gets buffers to fill
+    sub.cap = list_cap;
+    std::swap(fent, sub.fent);
+    std::swap(went, sub.went);
+    std::swap(fcnt, sub.fcnt);
+    std::swap(wcnt, sub.wcnt);
+    lists_valid = false;
+    SLF_TRY(ensure_work_buffers());
+    sub.kept = true;
+    return SLF_OK;
 }
 
 int32_t World::sync() {
@@ -162,15 +192,30 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
         SLF_TRY(write_vec(vo, dvel, n));
         // the adjoint of the substep whose forward state sits in slots a (sorted positions)
         // and nid (densities), its constants in d_consts: (xo, vo) after it -> (xp, vp) before
-        auto adjoint_substep = [&](float dt, int a, int nid, const DfsphRecord& rec) -> int32_t {
+        // (kept: a WCSPH substep's forward as a segment's replay kept it, in place of the world's)
+        auto adjoint_substep = [&](float dt, int a, int nid, const DfsphRecord& rec,
+                                   const SubRecord* kept = nullptr) -> int32_t {
             Params p = params();
             SLF_CUDA(cudaMemsetAsync(grads.p, 0, kGradSlots * sizeof(double), stream));
             PairLists fl = fluid_lists(), wl = wall_lists();
             const int form = !fast() ? 1 : (rel() ? 2 : 0);  // the lists' form (launch.h)
-            if (s.solver == SLF_SOLVER_WCSPH) {
-                launch_adjoint_wcsph(p, d_consts, fl, wl, form, pos[a].p, vel[a].p, rho[nid].p, press.p,
-                                     scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p, xb.p, vb.p, rb.p, xp.p,
-                                     vp.p, grads.p, tdev, terrains.empty() ? nullptr : gslope.p, stream);
+            if (s.solver == SLF_SOLVER_WCSPH && kept) {
+                launch_set_consts(consts(dt), d_consts, stream);
+                const uint32_t* order = kept->ordered ? kept->order.p : nullptr;
+                PairLists kf{kept->cap, kept->fent.p, kept->fcnt.p, order, nullptr};
+                PairLists kw_{kept->cap, kept->went.p, kept->wcnt.p, order, nullptr};
+                timed("adj_wcsph", 0.0, [&] {
+                    launch_adjoint_wcsph(p, d_consts, kf, kw_, form, kept->spos.p, kept->svel.p, kept->rho.p,
+                                         kept->press.p, kept->scaled.p, dwalls.p, kept->pre.p, kept->dest.p, xo.p,
+                                         vo.p, ab.p, xb.p, vb.p, rb.p, xp.p, vp.p, grads.p, tdev,
+                                         terrains.empty() ? nullptr : kept->slope.p, stream);
+                });
+            } else if (s.solver == SLF_SOLVER_WCSPH) {
+                timed("adj_wcsph", 0.0, [&] {
+                    launch_adjoint_wcsph(p, d_consts, fl, wl, form, pos[a].p, vel[a].p, rho[nid].p, press.p,
+                                         scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p, xb.p, vb.p, rb.p, xp.p,
+                                         vp.p, grads.p, tdev, terrains.empty() ? nullptr : gslope.p, stream);
+                });
             } else {
                 // advance, density solve, viscosity, divergence solve, factors, densities,
                 // sort: the substep's steps backwards
@@ -244,6 +289,10 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
         auto backward_through = [&](std::vector<std::unique_ptr<SubRecord>>& subs, size_t count) -> int32_t {
             for (size_t q = count; q-- > 0;) {
                 SubRecord& sub = *subs[q];
+                if (sub.kept) {  // nothing to run again: its forward is in the record
+                    SLF_TRY(adjoint_substep(sub.dt, 0, 0, sub.rec, &sub));
+                    continue;
+                }
                 SLF_TRY(load_state(sub.pos.p, sub.vel.p, sub.ids.p, sub.cells.p));
                 int a = 0, nid = 0;
                 if (s.solver == SLF_SOLVER_WCSPH) {
@@ -291,8 +340,16 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                     uint32_t held = 0, its = 0;
                     int32_t rs;
                     if (s.solver == SLF_SOLVER_WCSPH) {
+                        // the sort's destinations and the pre-clamp velocities go into the record
+                        SLF_TRY(sub.dest.ensure(n, 0, stream));
+                        SLF_TRY(sub.pre.ensure(n, 0, stream));
+                        sort_dest = sub.dest.p;
+                        vel_pre = sub.pre.p;
                         rs = wcsph_substep(dts[q], held);
                         if (rs == kRetry) rs = wcsph_substep(dts[q], held);
+                        sort_dest = nullptr;
+                        vel_pre = nullptr;
+                        if (rs == SLF_OK) rs = keep_wcsph_substep(sub);
                     } else {
                         rs = dfsph_substep(dts[q], held, its, &sub.rec);
                         if (rs == kRetry) rs = dfsph_substep(dts[q], held, its, &sub.rec);

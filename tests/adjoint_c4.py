@@ -11,7 +11,7 @@ float restatement's, and so the library's, bit for bit (oracle/dual.hpp; about h
 direction on the host cores).  The particles start on the pressure clamp's kink, where the
 differences cannot converge; the tangent has no step size.
 
-    python tests/adjoint_c4.py [--directions 16] [--tangent K] [--out FILE]
+    python tests/adjoint_c4.py [--directions 16] [--tangent K] [--repeat R] [--out FILE]
 """
 import argparse
 import os
@@ -54,6 +54,11 @@ def main():
     ap.add_argument("--every", type=int, default=20)
     ap.add_argument("--tangent", type=int, default=0, help="directions also checked against the FP32 tangent")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--repeat", type=int, default=1,
+                    help="tapes timed on the same world, each from the initial state (the later ones reuse the "
+                         "tape's device buffers)")
+    ap.add_argument("--profile", action="store_true",
+                    help="one more tape whose backward is timed kernel by kernel (CUDA events)")
     args = ap.parse_args()
     import torch
 
@@ -63,27 +68,52 @@ def main():
 
     w, _ = run(sc.settings, sc, vel0)
     stream = torch.cuda.ExternalStream(w.stream())
-    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    w.tape_begin(args.every)
-    e[0].record(stream)
-    for _ in range(sc.steps):
-        w.step(sc.dt)
-    e[1].record(stream)
-    e[1].synchronize()
-    L, c = loss_of(w, target)
-    n = w.len()
-    dpos = np.tile(2.0 * (c - target) / n, (n, 1)).astype(np.float32)
-    e[2].record(stream)
-    dp0, dv0, params = w.step_backward(dpos, np.zeros_like(dpos))
-    e[3].record(stream)
-    e[3].synchronize()
-    fwd_ms, bwd_ms = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
-    w.tape_end()
+    lines = []
+    for r in range(max(1, args.repeat)):
+        if r:  # the initial state again, in the world's current order
+            ids = w.ids()
+            w.write_state(pos0[ids], vel0[ids])
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        w.tape_begin(args.every)
+        e[0].record(stream)
+        for _ in range(sc.steps):
+            w.step(sc.dt)
+        e[1].record(stream)
+        e[1].synchronize()
+        L, c = loss_of(w, target)
+        n = w.len()
+        dpos = np.tile(2.0 * (c - target) / n, (n, 1)).astype(np.float32)
+        e[2].record(stream)
+        dp0, dv0, params = w.step_backward(dpos, np.zeros_like(dpos))
+        e[3].record(stream)
+        e[3].synchronize()
+        fwd_ms, bwd_ms = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+        w.tape_end()
+        lines.append(f"tape {r}: loss {L:.6e}; forward {fwd_ms:.1f} ms, backward {bwd_ms:.1f} ms "
+                     f"(forward+adjoint {1 + bwd_ms / fwd_ms:.2f}x the taped forward), {sc.steps} steps, "
+                     f"checkpoint every {args.every}")
+        print(lines[-1], flush=True)
+    if args.profile:
+        ids = w.ids()
+        w.write_state(pos0[ids], vel0[ids])
+        w.tape_begin(args.every)
+        for _ in range(sc.steps):
+            w.step(sc.dt)
+        L, c = loss_of(w, target)
+        dpos = np.tile(2.0 * (c - target) / w.len(), (w.len(), 1)).astype(np.float32)
+        w.profile(True)
+        w.profile_reset()
+        w.step_backward(dpos, np.zeros_like(dpos))
+        prof = w.profile_read()
+        w.profile(False)
+        w.tape_end()
+        total = sum(v[1] for v in prof.values())
+        lines.append(f"backward kernel by kernel (CUDA events, launch by launch): {total:.1f} ms in all")
+        for name, (k, ms, _) in sorted(prof.items(), key=lambda kv: -kv[1][1]):
+            lines.append(f"  {name}: {k} launches, {ms:.1f} ms, {1e3 * ms / max(k, 1):.1f} us each")
+        print("\n".join(lines[-len(prof) - 1:]), flush=True)
     w.close()
-
-    lines = [f"loss {L:.6e}; forward {fwd_ms:.1f} ms, backward {bwd_ms:.1f} ms "
-             f"(forward+adjoint {1 + bwd_ms / fwd_ms:.2f}x the taped forward), {sc.steps} steps, "
-             f"checkpoint every {args.every}", ""]
+    lines.append("")
     tank = ((0.0, 0.0, 0.0), sc.tank)
 
     def tangent(dvel, dparams):
@@ -129,8 +159,9 @@ def main():
         lines.append("| " + " | ".join(row) + " |")
         print(lines[-1], flush=True)
     lines.append("")
-    lines.append(f"best-of-steps relative error over the {args.directions} directions: median "
-                 f"{np.median(worst):.2e}, max {np.max(worst):.2e}")
+    if worst:
+        lines.append(f"best-of-steps relative error over the {args.directions} directions: median "
+                     f"{np.median(worst):.2e}, max {np.max(worst):.2e}")
     if exact:
         lines.append(f"against the FP32 tangent over {len(exact)} directions: median {np.median(exact):.2e}, "
                      f"max {np.max(exact):.2e}")
