@@ -307,7 +307,9 @@ typedef struct slf_param_grads {
  * current state is the first checkpoint and the state before every k-th substep is kept too
  * (segment checkpointing, 36 bytes per particle per checkpoint: the backward pass runs each
  * segment of k substeps forward again from its checkpoint, recording them, which holds one
- * segment's records at a time, however many substeps the flow makes a step take).
+ * segment's records at a time, however many substeps the flow makes a step take; a WCSPH segment's
+ * records keep each substep's neighbour lists too, about 16 bytes per particle per list slot, and
+ * this call reserves them).
  * checkpoint_every = 0:
  * every substep keeps the state before it and its solver record (the rates and velocities of each
  * DFSPH iteration), about 68 + 20 x iterations bytes per particle per substep; the backward pass

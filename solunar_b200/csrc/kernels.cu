@@ -1723,7 +1723,7 @@ void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const
                     const PairLists& fl, const PairLists& wl, float* rho, float* press, float* scaled, float* alpha,
                     Status* st, const TerrainDev& T, float4* slope, cudaStream_t s, const MoverDev& M) {
     if (!p.n) return;
-    if (p.n <= kWarpPassMax && T.regions == 0 && M.count == 0) {
+    if (warp_rows(p.n, p.radius, p.spacing) && T.regions == 0 && M.count == 0) {
         // a scene this small leaves most SMs idle a thread a particle: a warp a particle (terrain
         // and body points, which every lane would take alike, stay a thread a particle)
         if (p.solver == 0)
@@ -1748,7 +1748,7 @@ void launch_wcsph_force(const Params& p, const StepConsts* sc, const PairLists& 
                         float4* vel_pre, const TerrainDev& T, const float4* slope, cudaStream_t s,
                         const MoverDev& M) {
     if (!p.n) return;
-    if (p.n <= kWarpPassMax && T.regions == 0 && M.count == 0 && slope == nullptr) {
+    if (warp_rows(p.n, p.radius, p.spacing) && T.regions == 0 && M.count == 0 && slope == nullptr) {
         k_wcsph_force_warp<<<blocks_for(p.n * 32u), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, press, scaled,
                                                                     walls, pos_out, vel_out, st, vel_pre);
         return;

@@ -41,6 +41,15 @@ size_t walk_order_keys(int3 span);
 // support 4, density 392 -> 92 us and force 218 -> 67 us; 250k and 1M particles at support 2,
 // density 219 -> 547 us and 562 -> 2250 us, so larger scenes keep a thread a particle.
 constexpr uint32_t kWarpPassMax = 32768u;
+// Scenes at support 3 and more (hundreds of neighbours, thousands of candidates a particle) may
+// keep the warp passes up to this many particles.  Off: on the 64k-particle scene at support 4
+// the density pass gained (592 -> 548 us) but the force pass lost more (239 -> 358 us).
+#ifndef SLF_WARP_PASS_WIDE_MAX
+#define SLF_WARP_PASS_WIDE_MAX 0u
+#endif
+inline bool warp_rows(uint32_t n, float radius, float spacing) {
+    return n <= kWarpPassMax || (n <= SLF_WARP_PASS_WIDE_MAX && radius >= 3.0f * spacing);
+}
 void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32_t* bcount, uint32_t* tile_sums,
                        uint32_t* order, cudaStream_t s);
 

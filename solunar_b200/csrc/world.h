@@ -458,6 +458,9 @@ struct World {
     // After a WCSPH substep of a segment's replay (its sort writing `sub.dest`, its advance
     // `sub.pre`): the substep's forward into `sub` (SubRecord::kept).
     int32_t keep_wcsph_substep(SubRecord& sub);
+    // The device buffers a WCSPH checkpoint segment's records take, at the current size and list
+    // room, so that the backward allocates nothing (slf_tape_begin reserves a segment of them).
+    int32_t reserve_kept(SubRecord& sub);
 
     // ---- the tape of slf_tape_begin: checkpoints and the substep lengths of each step ----
     struct Tape {

@@ -11,6 +11,21 @@ auto World::new_record() -> std::unique_ptr<SubRecord> {
     return r;
 }
 
+int32_t World::reserve_kept(SubRecord& sub) {
+    for (auto* b : {&sub.pos, &sub.vel, &sub.spos, &sub.svel, &sub.pre}) SLF_TRY(b->ensure(n, 0, stream));
+    for (auto* b : {&sub.rho, &sub.press, &sub.scaled}) SLF_TRY(b->ensure(n, 0, stream));
+    for (auto* b : {&sub.ids, &sub.dest, &sub.order, &sub.fcnt, &sub.wcnt}) SLF_TRY(b->ensure(n, 0, stream));
+    if (rel()) {
+        SLF_TRY(sub.cells.ensure(n, 0, stream));
+        SLF_TRY(sub.scells.ensure(n, 0, stream));
+    }
+    if (!terrains.empty()) SLF_TRY(sub.slope.ensure(n, 0, stream));
+    const size_t slots = PairLists::slots_for(uint32_t(n), list_cap);
+    SLF_TRY(sub.fent.ensure(slots, 0, stream));
+    SLF_TRY(sub.went.ensure(slots, 0, stream));
+    return SLF_OK;
+}
+
 int32_t World::keep_wcsph_substep(SubRecord& sub) {
     // the committed substep's sorted slots, as recompute names them
     const int a = (cpos + 2) % 3, nid = cid;
@@ -56,6 +71,12 @@ int32_t World::tape_begin(uint32_t every) {
     tape.count = 0;
     tape.ckpt_sub.clear();
     drop_records(0);
+    if (every && s.solver == SLF_SOLVER_WCSPH && n) {
+        // the records of one checkpoint segment, each with room for its substep's forward
+        while (spare_records.size() < every) spare_records.push_back(std::make_unique<SubRecord>());
+        for (size_t k = spare_records.size() - every; k < spare_records.size(); ++k)
+            SLF_TRY(reserve_kept(*spare_records[k]));
+    }
     return every ? checkpoint() : SLF_OK;
 }
 

@@ -481,8 +481,8 @@ int32_t World::plan_sort(SortPlan& sp, bool stable) {
     // and where every pass over the lists runs a warp a particle)
     size_t keys = walk_order_keys(sp.span);
     sp.keys = 0;
-    bool warp_passes = !fast() && s.solver == SLF_SOLVER_WCSPH && n <= kWarpPassMax && terrains.empty() &&
-                       m_pos.empty();
+    bool warp_passes = !fast() && s.solver == SLF_SOLVER_WCSPH && warp_rows(uint32_t(n), radius, s.spacing) &&
+                       terrains.empty() && m_pos.empty();
     if (keys < (size_t(1) << 31) && !warp_passes) {
         SLF_TRY(worder.ensure(n, 0, stream));
         SLF_TRY(wkeys.ensure(keys + 1, 0, stream));
