@@ -294,6 +294,39 @@ __device__ __forceinline__ void ground_damping_adjoint(const TerrainDev& T, floa
     }
 }
 
+// The body points' push (couple.rs:375-416, mover_pairs): for each point within reach of x,
+// a -= G (M + D) with G = m o g(|o|), o = x - point, and the damping D = -k tau / ((|o|^2 + eps)
+// rho) where tau = (v - u) . o < 0 (u: the point's velocity).  Adds the adjoint for a-bar ai into
+// x-bar, v-bar, rho-bar, M-bar (the mirrored pressure) and k-bar; the points' motion is given.
+__device__ __forceinline__ void mover_adjoint(const Params& p, const MoverDev& B, float k, float3 xi, float3 vi,
+                                              float rho, float mirrored, float3 ai, float3& xbar, float3& vbar,
+                                              float& rbar, float& mbar, double& kbar) {
+    const int3 cell = cell_of(p, xi.x, xi.y, xi.z);
+    each_near(p, B.grid, B.pos, cell, xi.x, xi.y, xi.z, [&](uint32_t j, float4 q) {
+        const float3 o = make_float3(xi.x - q.x, xi.y - q.y, xi.z - q.z);
+        const float d2 = dotf(o, o), inv = inv_length(d2);
+        if (inv == 0.0f) return;  // coincident: no gradient, and tau = 0 takes no damping
+        float g, gp;
+        grad_factor(p, d2 * inv, g, gp);
+        const float3 u = vi - f3(__ldg(&B.vel[j]));
+        const float tau = dotf(u, o);
+        const bool act = tau < 0.0f;
+        const float e2 = d2 + p.soften;
+        const float D = act ? -k * tau / (e2 * rho) : 0.0f;
+        const float A = dotf(ai, o);
+        const float h = -p.mass * g * A;  // dL/dM = dL/dD
+        mbar += h;
+        xbar = xbar + (ai * g + o * (A * gp * inv)) * (-p.mass * (mirrored + D));
+        if (act) {
+            const float dtau = -k / (e2 * rho);  // dD/dtau
+            xbar = xbar + u * (h * dtau) + o * (h * (-D / e2) * 2.0f);
+            vbar = vbar + o * (h * dtau);
+            rbar += h * (-D / rho);
+            kbar += (double)(h * (-tau / (e2 * rho)));
+        }
+    });
+}
+
 // terrain_contact (terrain.rs:314-333) backwards: (ybar, vbar) after every region's contact ->
 // before the first, the state before it (y0, v0) as the forward had it.  Each region's own state
 // is found by running the regions before it again.
@@ -377,7 +410,8 @@ __global__ void k_adj_advance(Params p, const StepConsts* __restrict__ sc, const
 // ---- forces (step.rs:173-211), wall viscosity (step.rs:262-301), Tait pressure (step.rs:147-172)
 // PRESSURE = false: the DFSPH viscosity pass (dfsph.rs:90-99), the same pairs without pressure,
 // so the pressure records are neither gathered nor differentiated
-// TERRAIN: the ground's terms as well (WCSPH worlds with terrain regions)
+// TERRAIN: the ground's terms and the body points' as well (WCSPH worlds with terrain regions or
+// coupled bodies)
 template <bool PRESSURE, bool TERRAIN = false>
 __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                       PairLists wl, int form, const float4* __restrict__ pos,
@@ -388,7 +422,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
                                                       const float4* __restrict__ ab, float4* __restrict__ xb,
                                                       float4* __restrict__ vb, float* __restrict__ rb,
                                                       double* __restrict__ grads, int add_rho, TerrainDev T,
-                                                      const float4* __restrict__ slope) {
+                                                      const float4* __restrict__ slope, MoverDev bodies) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     double nu_bar = 0.0, nuw_bar = 0.0, b_bar = 0.0;
@@ -518,6 +552,14 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
                 xbar = xbar + ground_slope_adjoint(T, xi, ai * (-M));
             }
             ground_damping_adjoint(T, nuw, xi, vi, rho_i, ai, xbar, vbar, rbar, nuw_bar);
+            if (bodies.count) {
+                // the mover damping has the wall viscosity's form (couple.rs:375-416): its gradient
+                // joins that slot
+                float mbar = 0.0f;
+                mover_adjoint(p, bodies, sc->mover_damping, xi, vi, rho_i, M, ai, xbar, vbar, rbar, mbar, nuw_bar);
+                sbar += mbar;
+                pbar += mbar * p.inv_rest_sq;
+            }
         }
 
         // s = p / rho^2 and the Tait equation of state
@@ -745,7 +787,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
                                                         const float4* __restrict__ pos,
                                                         const float4* __restrict__ walls,
                                                         const float* __restrict__ rb, float4* __restrict__ xb,
-                                                        const float4* __restrict__ slope) {
+                                                        const float4* __restrict__ slope, MoverDev bodies) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
     if (i >= p.n) return;
@@ -777,6 +819,17 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
         xbar = xbar + r * (g * p.mass * rbi);
     }
     if (slope) xbar = xbar + f3(slope[i]) * rbi;
+    if (bodies.count) {  // the body points' kernel sum (mod.rs:648-656)
+        const int3 cell = cell_of(p, xi.x, xi.y, xi.z);
+        each_near(p, bodies.grid, bodies.pos, cell, xi.x, xi.y, xi.z, [&](uint32_t, float4 q) {
+            const float3 o = make_float3(xi.x - q.x, xi.y - q.y, xi.z - q.z);
+            const float d = sqrtf(dotf(o, o));
+            if (d <= 0.0f) return;
+            float g, gp;
+            grad_factor(p, d, g, gp);
+            xbar = xbar + o * (g * p.mass * rbi);
+        });
+    }
     float4 x0 = xb[i];
     xb[i] = make_float4(x0.x + xbar.x, x0.y + xbar.y, x0.z + xbar.z, 0.0f);
 }
@@ -1073,14 +1126,15 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
                           const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
                           const float4* xo, const float4* vo, float4* ab, float4* xb, float4* vb, float* rb,
                           float4* xp, float4* vp, double* grads, const TerrainDev& T, const float4* slope,
-                          cudaStream_t s) {
+                          const MoverDev& bodies, cudaStream_t s) {
     if (!p.n) return;
     uint32_t nb = adj_blocks(p.n);
     k_adj_advance<<<nb, kBlock, 0, s>>>(p, sc, vel_pre, xo, vo, ab, xb, vb, grads, pos, T);
-    if (T.regions) {
+    if (T.regions || bodies.count) {
         k_adj_force<true, true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
-                                                                   walls, ab, xb, vb, rb, grads, 0, T, slope);
-        k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, slope);
+                                                                   walls, ab, xb, vb, rb, grads, 0, T, slope, bodies);
+        k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, T.regions ? slope : nullptr,
+                                                         bodies);
     } else if (p.n <= kAdjWarpMax) {
         // few rows: a warp each, so that the GPU fills
         k_adj_force_warp<<<adj_blocks(p.n * 32u), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
@@ -1088,8 +1142,8 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
         k_adj_density_warp<<<adj_blocks(p.n * 32u), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb);
     } else {
         k_adj_force<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, press, scaled,
-                                                             walls, ab, xb, vb, rb, grads, 0, T, slope);
-        k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, nullptr);
+                                                             walls, ab, xb, vb, rb, grads, 0, T, slope, MoverDev{});
+        k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, nullptr, MoverDev{});
     }
     k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp);
 }
@@ -1129,7 +1183,8 @@ void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists
     if (!p.n) return;
     k_adj_scale<<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, w, ab, grads);
     k_adj_force<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, vel, rho, zeros, zeros,
-                                                          walls, ab, xb, w, rb, grads, 1, TerrainDev{}, nullptr);
+                                                          walls, ab, xb, w, rb, grads, 1, TerrainDev{}, nullptr,
+                                                          MoverDev{});
 }
 
 void launch_adj_factors_density(const Params& p, const PairLists& fl, const PairLists& wl, int form,
@@ -1138,7 +1193,7 @@ void launch_adj_factors_density(const Params& p, const PairLists& fl, const Pair
     if (!p.n) return;
     k_adj_alpha_prep<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, alpha, abar, gt);
     k_adj_alpha<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, gt, xb);
-    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, nullptr);
+    k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, nullptr, MoverDev{});
 }
 
 void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const float4* vb, float4* xp, float4* vp,

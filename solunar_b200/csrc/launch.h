@@ -188,13 +188,14 @@ void launch_list_rel(const Params& p, const GridDev& g, const float4* pos, const
 // the sort's destinations) and the adjoint of its output state xo, vo (sorted order); outputs
 // the adjoint of its input state xp, vp in the order before the sort, and adds the parameter
 // gradients (viscosity, wall viscosity, stiffness, gravity) to grads[kGradSlots].  T and slope:
-// the terrain regions and the density pass's ground slopes (T.regions = 0: no terrain).
+// the terrain regions and the density pass's ground slopes (T.regions = 0: no terrain); bodies:
+// the coupled bodies' points the substep met (count 0: none).
 void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                           int form, const float4* pos, const float4* vel, const float* rho, const float* press,
                           const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
                           const float4* xo, const float4* vo, float4* ab, float4* xb, float4* vb, float* rb,
                           float4* xp, float4* vp, double* grads, const TerrainDev& T, const float4* slope,
-                          cudaStream_t s);
+                          const MoverDev& bodies, cudaStream_t s);
 
 // The adjoint of a DFSPH substep, in pieces the host strings together (adjoint.cu): the advance;
 // one solver iteration (kappa, then the velocity adjoint before its push); the viscosity; the

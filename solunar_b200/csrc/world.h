@@ -440,6 +440,16 @@ struct World {
         DevBuf<float> rho, press, scaled;
         DevBuf<uint32_t> dest, order, fcnt, wcnt;
         DevBuf<uint2> fent, went;
+        // With coupled bodies (tapes that record every substep): the body points the substep
+        // met, with their cell table, and the sound speed the step ran at, `raised` when a fast
+        // body set it above the settings' (the settings' then take no derivative from it).
+        uint32_t mcount = 0;
+        GridDev mgrid{};
+        DevBuf<float4> mpos, mvel;
+        DevBuf<uint32_t> mstart;
+        DevBuf<int4> mkeys;
+        float sound = 0.0f;
+        bool raised = false;
         void release(cudaStream_t st) {
             pos.release(st);
             vel.release(st);
@@ -452,6 +462,10 @@ struct World {
             for (auto* b : {&dest, &order, &fcnt, &wcnt}) b->release(st);
             fent.release(st);
             went.release(st);
+            for (auto* b : {&mpos, &mvel}) b->release(st);
+            mstart.release(st);
+            mkeys.release(st);
+            mcount = 0;
             kept = false;
         }
     };
@@ -1013,7 +1027,8 @@ struct World {
     // The substep's sensitivities to its derived constants, taken back to the settings:
     // nu = min(viscosity c r, 0.05 r^2 / dt) (step.rs:254-259), nu_w = min(c r, 0.25 r^2 / dt)
     // (step.rs:282-283), B = rest c^2 / 7 (step.rs:149); the branch the substep took decides.
-    void accumulate_param_grads(float dt, const double* g, slf_param_grads& pg) const;
+    void accumulate_param_grads(float dt, const double* g, slf_param_grads& pg, float sound = 0.0f,
+                                bool raised = false) const;
 
     int32_t step_untaped(float dt, slf_report* out);
 

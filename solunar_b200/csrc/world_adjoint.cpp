@@ -43,6 +43,24 @@ int32_t World::keep_wcsph_substep(SubRecord& sub) {
     sub.ordered = walk_order() != nullptr;
     if (sub.ordered) SLF_TRY(copy(sub.order, worder.p, n));
     if (!terrains.empty()) SLF_TRY(copy(sub.slope, gslope.p, n));
+    // the body points this substep met, and their cell table
+    const MoverDev M = mover_dev();
+    sub.mcount = M.count;
+    if (M.count) {
+        SLF_TRY(copy(sub.mpos, M.pos, M.count));
+        SLF_TRY(copy(sub.mvel, M.vel, M.count));
+        sub.mgrid = M.grid;
+        if (M.grid.mode == 1) {
+            size_t cells = size_t(M.grid.sx) * size_t(M.grid.sy) * size_t(M.grid.sz);
+            SLF_TRY(copy(sub.mstart, M.grid.start, cells + 1));
+            sub.mgrid.start = sub.mstart.p;
+        } else if (M.grid.mode == 2) {
+            SLF_TRY(copy(sub.mstart, M.grid.start, size_t(M.grid.cells) + 1));
+            SLF_TRY(copy(sub.mkeys, M.grid.keys, M.grid.cells));
+            sub.mgrid.start = sub.mstart.p;
+            sub.mgrid.keys = sub.mkeys.p;
+        }
+    }
     // the lists change places: the record takes this substep's, the world gets buffers to fill
     sub.cap = list_cap;
     std::swap(fent, sub.fent);
@@ -221,21 +239,37 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
             PairLists fl = fluid_lists(), wl = wall_lists();
             const int form = !fast() ? 1 : (rel() ? 2 : 0);  // the lists' form (launch.h)
             if (s.solver == SLF_SOLVER_WCSPH && kept) {
-                launch_set_consts(consts(dt), d_consts, stream);
+                // the stiffness and constants at the sound speed the step ran at (a fast body may
+                // have raised it)
+                {
+                    const float configured = s.sound_speed;
+                    if (kept->sound > 0.0f) s.sound_speed = kept->sound;
+                    p = params();
+                    launch_set_consts(consts(dt), d_consts, stream);
+                    s.sound_speed = configured;
+                }
                 const uint32_t* order = kept->ordered ? kept->order.p : nullptr;
                 PairLists kf{kept->cap, kept->fent.p, kept->fcnt.p, order, nullptr};
                 PairLists kw_{kept->cap, kept->went.p, kept->wcnt.p, order, nullptr};
+                MoverDev km{};
+                if (kept->mcount) {
+                    km.count = kept->mcount;
+                    km.grid = kept->mgrid;
+                    km.pos = kept->mpos.p;
+                    km.vel = kept->mvel.p;
+                }
                 timed("adj_wcsph", 0.0, [&] {
                     launch_adjoint_wcsph(p, d_consts, kf, kw_, form, kept->spos.p, kept->svel.p, kept->rho.p,
                                          kept->press.p, kept->scaled.p, dwalls.p, kept->pre.p, kept->dest.p, xo.p,
                                          vo.p, ab.p, xb.p, vb.p, rb.p, xp.p, vp.p, grads.p, tdev,
-                                         terrains.empty() ? nullptr : kept->slope.p, stream);
+                                         terrains.empty() ? nullptr : kept->slope.p, km, stream);
                 });
             } else if (s.solver == SLF_SOLVER_WCSPH) {
                 timed("adj_wcsph", 0.0, [&] {
                     launch_adjoint_wcsph(p, d_consts, fl, wl, form, pos[a].p, vel[a].p, rho[nid].p, press.p,
                                          scaled.p, dwalls.p, pre.p, dest.p, xo.p, vo.p, ab.p, xb.p, vb.p, rb.p, xp.p,
-                                         vp.p, grads.p, tdev, terrains.empty() ? nullptr : gslope.p, stream);
+                                         vp.p, grads.p, tdev, terrains.empty() ? nullptr : gslope.p, MoverDev{},
+                                         stream);
                 });
             } else {
                 // advance, density solve, viscosity, divergence solve, factors, densities,
@@ -278,7 +312,8 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
             double g[kGradSlots];
             SLF_CUDA(cudaMemcpyAsync(g, grads.p, sizeof(g), cudaMemcpyDeviceToHost, stream));
             SLF_TRY(sync());
-            accumulate_param_grads(dt, g, pg);
+            if (kept) accumulate_param_grads(dt, g, pg, kept->sound, kept->raised);
+            else accumulate_param_grads(dt, g, pg);
             std::swap(xo, xp);
             std::swap(vo, vp);
             return SLF_OK;
@@ -398,16 +433,19 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
     return st;
 }
 
-void World::accumulate_param_grads(float dt, const double* g, slf_param_grads& pg) const {
-    double r = radius, c = s.sound_speed, visc = s.viscosity;
+void World::accumulate_param_grads(float dt, const double* g, slf_param_grads& pg, float sound, bool raised) const {
+    // sound: the speed the substep ran at; raised: a fast body set it, so the settings' sound
+    // speed did not reach the substep
+    double r = radius, c = sound > 0.0f ? sound : s.sound_speed, visc = s.viscosity;
+    double dc = raised ? 0.0 : 1.0;
     bool nu_free = double(s.viscosity) * c * r < 0.05 * r * r / dt;
     bool nuw_free = c * r < 0.25 * r * r / dt;
     if (nu_free) {
         pg.viscosity += g[kGradViscosity] * c * r;
-        pg.sound_speed += g[kGradViscosity] * visc * r;
+        pg.sound_speed += dc * g[kGradViscosity] * visc * r;
     }
-    if (nuw_free) pg.sound_speed += g[kGradWallViscosity] * r;
-    pg.sound_speed += g[kGradStiffness] * 2.0 * double(s.rest_density) * c / 7.0;
+    if (nuw_free) pg.sound_speed += dc * g[kGradWallViscosity] * r;
+    pg.sound_speed += dc * g[kGradStiffness] * 2.0 * double(s.rest_density) * c / 7.0;
     for (int a = 0; a < 3; ++a) pg.gravity[a] += g[kGradGravity + a];
 }
 
@@ -446,9 +484,25 @@ int32_t World::step_untaped(float dt, slf_report* out) {
                 SLF_TRY(tape_substep(small));
                 if (tape_step && tape.every == 0) SLF_TRY(record_begin(small));
                 if (!coupled.empty()) SLF_TRY(carry_movers(small * float(i), small * float(substeps - 1)));
+                // with coupled bodies a recording tape keeps each substep's forward as it runs:
+                // the body points' order follows their history, so the backward cannot run it again
+                SubRecord* keep = tape_step && tape.every == 0 && !coupled.empty() ? tape.subs.back().get() : nullptr;
+                if (keep) {
+                    SLF_TRY(keep->dest.ensure(n, 0, stream));
+                    SLF_TRY(keep->pre.ensure(n, 0, stream));
+                    sort_dest = keep->dest.p;
+                    vel_pre = keep->pre.p;
+                }
                 int32_t st = wcsph_substep(small, held);
                 if (st == kRetry) st = wcsph_substep(small, held);
                 if (st == kRetry) st = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
+                if (keep) {
+                    sort_dest = nullptr;
+                    vel_pre = nullptr;
+                    if (st == SLF_OK) st = keep_wcsph_substep(*keep);
+                    keep->sound = s.sound_speed;
+                    keep->raised = s.sound_speed != configured;
+                }
                 SLF_TRY(st);
                 r.held_back += held;
             }

@@ -482,7 +482,17 @@ int32_t World::step_with_bodies(float dt, const slf_body_pose* poses, uint64_t n
     if (s.solver != SLF_SOLVER_WCSPH && !coupled.empty())
         return fail(SLF_ERR_INVALID_SETTINGS, "the divergence free solver does not couple yet");
     if (!coupled.empty() && fast()) return fail(SLF_ERR_UNSUPPORTED, "coupled bodies run with EXACT arithmetic only");
-    if (tape.on && !coupled.empty()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint takes no coupled bodies");
+    if (tape.on && !coupled.empty()) {
+        // the adjoint takes bodies on the paths the caller gives, substep by substep as recorded
+        if (tape.every != 0)
+            return fail(SLF_ERR_UNSUPPORTED, "a tape with coupled bodies records every substep (checkpoint_every 0)");
+        for (const Coupled& known : coupled) {
+            const slf_body_pose* state = pose_of(poses, npose, known.body);
+            if (state && state->dynamic)
+                return fail(SLF_ERR_UNSUPPORTED,
+                            "the adjoint takes no dynamic body: its lift gives momentum back to the water");
+        }
+    }
     place_movers_at(poses, npose);
     if (!coupled.empty()) {
         SLF_TRY(dimpulse.ensure(2 * coupled.size(), 0, stream));
