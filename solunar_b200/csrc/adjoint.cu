@@ -449,7 +449,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
             float3 w = ai - f3(q.c);
             float R = rho_i + q.d;
             float S = PRESSURE ? s_i + q.e : 0.0f;
-            float ur = dotf(u, r);
+            // EXACT lists: the forward's own dot product decides whether the pair approaches
+            float ur = form == kFormExact ? dot3(u.x, u.y, u.z, r.x, r.y, r.z) : dotf(u, r);
             bool act = ur < 0.0f;
             float t = act ? ur : 0.0f;
             float den = (d2 + p.soften) * R;
@@ -473,9 +474,17 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
         uint32_t nw = listed_count(wl, row);
         float M = s_i + p_i * p.inv_rest_sq;
         float3 A = make_float3(0, 0, 0);  // sum of -grad W over walls, for the wall normal
+        // EXACT lists: the same sum as the forward forms it (the entries' g, each operation on its
+        // own), so that the normal's branches below are the forward's
+        float3 Ae = make_float3(0, 0, 0);
         for (uint32_t k = 0; k < nw; ++k) {
             uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
             float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
+            if (form == kFormExact) {
+                const float ge = __uint_as_float(SLF_LIST_LOAD(&wl.e[wl.at(row, k)]).y);
+                Ae = make_float3(__fadd_rn(Ae.x, -__fmul_rn(r.x, ge)), __fadd_rn(Ae.y, -__fmul_rn(r.y, ge)),
+                                 __fadd_rn(Ae.z, -__fmul_rn(r.z, ge)));
+            }
             float d2 = dotf(r, r), inv = inv_length(d2);
             if (inv == 0.0f) continue;
             float g, gp;
@@ -492,17 +501,20 @@ __global__ void __launch_bounds__(kBlock) k_adj_force(Params p, const StepConsts
 
         // wall viscosity (step.rs:262-301): n = A / |A|, I = n min(v.n, 0), and per wall with
         // tau = I.r < 0: D = -nu_w tau / ((|r|^2 + eps) rho), push -= r g m D
-        float alen = sqrtf(dotf(A, A));
+        const bool exact = form == kFormExact;
+        float alen = exact ? __fsqrt_rn(dot3(Ae.x, Ae.y, Ae.z, Ae.x, Ae.y, Ae.z)) : sqrtf(dotf(A, A));
         if (nw > 0 && alen > 0.0f && isfinite(alen)) {
-            float3 nrm = A * (1.0f / alen);
-            float vn = dotf(vi, nrm);
+            // EXACT lists: normal, v.n and each tau as the forward rounds them (wall_viscous)
+            float3 nrm = exact ? make_float3(__fdiv_rn(Ae.x, alen), __fdiv_rn(Ae.y, alen), __fdiv_rn(Ae.z, alen))
+                               : A * (1.0f / alen);
+            float vn = exact ? dot3(vi.x, vi.y, vi.z, nrm.x, nrm.y, nrm.z) : dotf(vi, nrm);
             float kk = fminf(vn, 0.0f);
-            float3 I = nrm * kk;
+            float3 I = exact ? make_float3(__fmul_rn(nrm.x, kk), __fmul_rn(nrm.y, kk), __fmul_rn(nrm.z, kk)) : nrm * kk;
             float3 Ibar = make_float3(0, 0, 0);
             for (uint32_t k = 0; k < nw; ++k) {
                 uint32_t e = listed_raw(wl, form, row, k), j = entry_index(e, form);
                 float3 r = pair_off(p, form, xi, __ldg(&walls[j]), e);
-                float tau = dotf(I, r);
+                float tau = exact ? dot3(I.x, I.y, I.z, r.x, r.y, r.z) : dotf(I, r);
                 if (!(tau < 0.0f)) continue;
                 float d2 = dotf(r, r);
                 float d = sqrtf(d2);
@@ -630,7 +642,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_force_warp(Params p, const StepC
             float3 w = ai - f3(qb);
             float R = rho_i + qr;
             float S = s_i + qs;
-            float ur = dotf(u, r);
+            // EXACT lists: the forward's own dot product decides whether the pair approaches
+            float ur = form == kFormExact ? dot3(u.x, u.y, u.z, r.x, r.y, r.z) : dotf(u, r);
             bool act = ur < 0.0f;
             float t = act ? ur : 0.0f;
             float den = (d2 + p.soften) * R;
@@ -916,7 +929,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
     float ri = rate[i], ai = alpha[i];
     float phi, dphi, dphi_rho = 0.0f;
     if (WHICH == 1) {
-        float over = rho[i] + dt * ri - p.rest;
+        // the forward's rounding, each operation on its own (no contraction): particles at rest
+        // density sit within an ulp of the clamp, and the branch must be the forward's
+        float over = __fsub_rn(__fadd_rn(rho[i], __fmul_rn(dt, ri)), p.rest);
         bool on = over > 0.0f;
         phi = on ? over / sc->dt_sq : 0.0f;
         dphi = on ? 1.0f / dt : 0.0f;
