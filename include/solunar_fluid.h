@@ -303,24 +303,26 @@ typedef struct slf_param_grads {
     double gravity[3];   /* dL / d settings.gravity */
 } slf_param_grads;
 
-/* Starts recording the steps that follow for slf_step_backward.  checkpoint_every = k > 0: the
- * current state is the first checkpoint and the state before every k-th substep is kept too
- * (segment checkpointing, 36 bytes per particle per checkpoint: the backward pass runs each
- * segment of k substeps forward again from its checkpoint, recording them, which holds one
- * segment's records at a time, however many substeps the flow makes a step take; a WCSPH segment's
- * records keep each substep's neighbour lists too, about 16 bytes per particle per list slot, and
- * this call reserves them).
- * checkpoint_every = 0:
- * every substep keeps the state before it and its solver record (the rates and velocities of each
- * DFSPH iteration), about 68 + 20 x iterations bytes per particle per substep; the backward pass
- * then redoes only each substep's sort and densities.  The number of particles must not change
- * while recording.  WCSPH and DFSPH steps, absolute or cell-relative positions (cell-relative
- * checkpoints and records add the 16-byte cell of each particle), WCSPH worlds with terrain
- * (the ground's density, push and damping and terrain contact are differentiated; terrain added
- * while recording is UNSUPPORTED), WCSPH worlds with coupled bodies on the caller's paths
- * (checkpoint_every 0 only: each substep's forward is kept as it runs, since the body points'
- * order follows their history; dynamic bodies, whose lift gives momentum back to the water, are
- * UNSUPPORTED); UNSUPPORTED with warm_start. */
+/* Starts recording the steps that follow for slf_step_backward.  The number of particles must not
+ * change while recording.
+ *
+ * checkpoint_every = k > 0 (segment checkpointing): the current state is the first checkpoint and
+ * the state before every k-th substep is kept too, 36 bytes per particle each.  The backward pass
+ * runs each segment of k substeps forward again from its checkpoint, recording it, so it holds one
+ * segment's records at a time however many substeps the flow makes a step take.  A WCSPH
+ * segment's records also keep each substep's neighbour lists (about 16 bytes per particle per list
+ * slot), which this call reserves.
+ *
+ * checkpoint_every = 0: every substep keeps the state before it and its solver record (the rates
+ * and velocities of each DFSPH iteration), about 68 + 20 x iterations bytes per particle per
+ * substep; the backward pass redoes only each substep's sort and densities.
+ *
+ * Taken: WCSPH and DFSPH, absolute or cell-relative positions (cell-relative checkpoints and
+ * records add the 16-byte cell of each particle); WCSPH with terrain (its density, push, damping
+ * and contact; terrain added while recording is UNSUPPORTED); WCSPH with coupled bodies on the
+ * caller's paths, checkpoint_every 0 only (each substep's forward is kept as it runs, since the
+ * body points' order follows their history).  UNSUPPORTED: warm_start, dynamic bodies (whose lift
+ * gives momentum back to the water), bodies with checkpoints. */
 int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
 /* Stops recording.  The tape's device buffers (substep records, checkpoints) stay with the world
  * and are reused by the next tape, so the rounds of an optimisation loop record without
