@@ -311,7 +311,8 @@ typedef struct slf_param_grads {
  * runs each segment of k substeps forward again from its checkpoint, recording it, so it holds one
  * segment's records at a time however many substeps the flow makes a step take.  A WCSPH
  * segment's records also keep each substep's neighbour lists (about 16 bytes per particle per list
- * slot), which this call reserves.
+ * slot), which this call reserves when a segment's worth fits in half the device's free memory;
+ * otherwise the backward runs each of the segment's substeps once more before its adjoint.
  *
  * checkpoint_every = 0: every substep keeps the state before it and its solver record (the rates
  * and velocities of each DFSPH iteration), about 68 + 20 x iterations bytes per particle per

@@ -488,6 +488,7 @@ struct World {
         DevBuf<uint32_t> cids;
         DevBuf<int4> ccells;                    // cell-relative positions: [c][n]
         std::vector<std::unique_ptr<SubRecord>> subs;  // every == 0: each substep's record
+        bool keep_segments = false;  // WCSPH checkpoint segments keep each substep's forward
     } tape;
     // Records of finished tapes and segments, kept with their device buffers for the next ones:
     // the rounds of an optimisation loop then record without allocating (tens of GB at a

@@ -89,11 +89,20 @@ int32_t World::tape_begin(uint32_t every) {
     tape.count = 0;
     tape.ckpt_sub.clear();
     drop_records(0);
+    tape.keep_segments = false;
     if (every && s.solver == SLF_SOLVER_WCSPH && n) {
-        // the records of one checkpoint segment, each with room for its substep's forward
-        while (spare_records.size() < every) spare_records.push_back(std::make_unique<SubRecord>());
-        for (size_t k = spare_records.size() - every; k < spare_records.size(); ++k)
-            SLF_TRY(reserve_kept(*spare_records[k]));
+        // the records of one checkpoint segment, each with room for its substep's forward, when
+        // a segment's worth fits in half the device's free memory (else the backward runs each
+        // substep again before its adjoint)
+        const size_t per = 2 * PairLists::slots_for(uint32_t(n), list_cap) * sizeof(uint2) + size_t(n) * 160;
+        size_t free = 0, total = 0;
+        SLF_CUDA(cudaMemGetInfo(&free, &total));
+        tape.keep_segments = size_t(every) * per <= free / 2;
+        if (tape.keep_segments) {
+            while (spare_records.size() < every) spare_records.push_back(std::make_unique<SubRecord>());
+            for (size_t k = spare_records.size() - every; k < spare_records.size(); ++k)
+                SLF_TRY(reserve_kept(*spare_records[k]));
+        }
     }
     return every ? checkpoint() : SLF_OK;
 }
@@ -395,7 +404,10 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                     SLF_TRY(save_state(sub.pos.p, sub.vel.p, sub.ids.p, sub.cells.p));
                     uint32_t held = 0, its = 0;
                     int32_t rs;
-                    if (s.solver == SLF_SOLVER_WCSPH) {
+                    if (s.solver == SLF_SOLVER_WCSPH && !tape.keep_segments) {
+                        rs = wcsph_substep(dts[q], held);
+                        if (rs == kRetry) rs = wcsph_substep(dts[q], held);
+                    } else if (s.solver == SLF_SOLVER_WCSPH) {
                         // the sort's destinations and the pre-clamp velocities go into the record
                         SLF_TRY(sub.dest.ensure(n, 0, stream));
                         SLF_TRY(sub.pre.ensure(n, 0, stream));
