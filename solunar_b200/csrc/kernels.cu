@@ -1260,16 +1260,21 @@ __global__ void __launch_bounds__(kBlock, SLF_RATE_MIN_BLOCKS) k_rate(Params p, 
                                                  SolveRec rec, unsigned long long loop) {
     // a solve that already stopped leaves the rest of its batch of launches idle
     if (__ldcg(&st->settled)) return;
-    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
-    double err = 0.0;
+    DD acc{0.0, 0.0};
     uint32_t loaded = 0;
     // every block reads the count before the last block advances it
     const uint32_t slot = rec.rate ? __ldcg(&st->iterations) : 0u;
-    if (i < p.n)
+    // rows of the walk order, a grid's width apart (one each when the grid covers them all)
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x) {
+        const uint32_t i = fl.particle(row);
+        double err = 0.0;
+        uint32_t one = 0;
         rate_particle<WHICH>(p, sc, fl, wl, i, row, FromGlobal{pos, vel}, pos, vel, rho, alpha, walls, kappa_w, rec, slot,
-                             err, loaded);
-    residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded, loop);
+                             err, one);
+        acc = dd_add(acc, DD{err, 0.0});
+        loaded += one;
+    }
+    residual_finish<WHICH>(p, st, partial, partial_loaded, acc, loaded, loop);
 }
 
 // push_apart (dfsph.rs:184-216) of particle i: the velocity change from each particle's
@@ -1312,10 +1317,8 @@ __global__ void __launch_bounds__(kBlock, SLF_PUSH_MIN_BLOCKS) k_push(Params p, 
                                                  Status* st, float* __restrict__ applied, unsigned long long loop) {
     loop_bound(p, st, loop);
     if (__ldcg(&st->settled)) return;
-    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
-    if (i >= p.n) return;
-    push_particle(p, sc, fl, wl, i, row, FromGlobal{pos, nullptr}, pos, vel, walls, applied);
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x)
+        push_particle(p, sc, fl, wl, fl.particle(row), row, FromGlobal{pos, nullptr}, pos, vel, walls, applied);
 }
 
 // viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
@@ -1825,13 +1828,41 @@ void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStr
 
 size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (sizeof(DD) + sizeof(uint32_t)) + 64; }
 
+// The solver passes' grid: with SLF_SOLVER_RESIDENT, no more blocks than the SMs hold at once
+// (each block then strides over rows), so no launch ends on a partial wave.
+#ifndef SLF_SOLVER_RESIDENT
+#define SLF_SOLVER_RESIDENT 1
+#endif
+// resident blocks of k_rate<0>, k_rate<1>, k_push on the device (prepare_solver_grids; 0: not
+// known yet, the grid then covers every row)
+static std::atomic<uint32_t> g_resident[3] = {0, 0, 0};
+
+void prepare_solver_grids() {
+    if (!SLF_SOLVER_RESIDENT || g_resident[2].load()) return;
+    int dev = 0, sms = 0, per[3] = {0, 0, 0};
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_rate<0>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_rate<1>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_push, kBlock, 0);
+    for (int k = 0; k < 3; ++k) g_resident[k].store(uint32_t(std::max(per[k], 0) * std::max(sms, 0)));
+}
+
+static uint32_t solver_blocks(uint32_t n, int kernel) {
+    uint32_t nb = blocks_for(n);
+    uint32_t resident = g_resident[kernel].load();
+    return resident && resident < nb ? resident : nb;
+}
+
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
                  void* partials, Status* st, SolveRec rec, cudaStream_t s, unsigned long long loop) {
     if (!p.n) return;
-    uint32_t nb = blocks_for(p.n);
+    // the partials' room is for one block a 256 rows; the grid takes at most that many
+    uint32_t nb = solver_blocks(p.n, which == 0 ? 0 : 1);
     DD* part = static_cast<DD*>(partials);
-    uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
+    uint32_t* loaded = reinterpret_cast<uint32_t*>(part + (p.n + kBlock - 1) / kBlock);
     if (which == 0)
         k_rate<0><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, reinterpret_cast<float*>(pos),
                                         part, loaded, st, rec, loop);
@@ -1842,7 +1873,7 @@ void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLis
 
 void launch_push(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                  float4* vel, const float4* walls, Status* st, float* applied, cudaStream_t s, unsigned long long loop) {
-    if (p.n) k_push<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied, loop);
+    if (p.n) k_push<<<solver_blocks(p.n, 2), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, walls, st, applied, loop);
 }
 
 // Warm start of a solve: the stiffness that applies `share` of the impulse S the particle's last

@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
     if (i < p.n)
         rate_particle_fast<WHICH, REL>(p, sc, fl, wl, i, row, FromGlobalF{pos, vel}, pos, vel, rho, alpha, walls, kappa,
                                        rec, slot, err, loaded);
-    residual_finish<WHICH>(p, st, partial, partial_loaded, err, loaded, loop);
+    residual_finish<WHICH>(p, st, partial, partial_loaded, DD{err, 0.0}, loaded, loop);
 }
 
 template <bool REL, class Src>

@@ -80,6 +80,9 @@ void launch_mover_felt(const Params& p, const StepConsts* sc, const MoverDev& M,
 void launch_mover_fold(uint32_t n, uint32_t bodies, const float4* felt, float dt, float4* impulse, cudaStream_t s);
 void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStream_t s);
 size_t rate_partial_bytes(uint32_t n);
+// Looks up, once per process, how many blocks of the solver passes the device holds at once (not
+// during a stream capture): their grids take no more, each block striding over rows.
+void prepare_solver_grids();
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
 // sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve
 // has settled, so a batch of iterations can be queued ahead of the check that ends it.

@@ -72,10 +72,9 @@ __device__ __forceinline__ void loop_bound(const Params& p, Status* st, unsigned
 // check that stops the solve also ends the graph's loop.
 template <int WHICH>
 __device__ __forceinline__ void residual_finish(const Params& p, Status* st, DD* __restrict__ partial,
-                                                uint32_t* __restrict__ partial_loaded, double err, uint32_t loaded,
+                                                uint32_t* __restrict__ partial_loaded, DD acc, uint32_t loaded,
                                                 unsigned long long loop) {
-    // block sum: a fixed shuffle tree in double-double
-    DD acc{err, 0.0};
+    // block sum: a fixed shuffle tree in double-double (acc: this thread's rows' errors)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         DD other{__shfl_xor_sync(0xffffffffu, acc.hi, o), __shfl_xor_sync(0xffffffffu, acc.lo, o)};
