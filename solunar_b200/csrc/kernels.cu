@@ -351,17 +351,17 @@ __device__ __forceinline__ uint32_t warp_list_near(const Params& p, const GridDe
 // ---- densities (mod.rs:621-675) and the substep's neighbour lists, with WCSPH pressure
 // (step.rs:147-172) or the DFSPH factors (dfsph.rs:108-163) --------------------------------
 
+// four blocks a SM (64 registers), as the pass compiled before it strode over rows
 template <int SOLVER>
-__global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDev wg, const float4* __restrict__ pos,
+__global__ void __launch_bounds__(kBlock, 4) k_density(Params p, GridDev fg, GridDev wg, const float4* __restrict__ pos,
                                                     const float4* __restrict__ walls, PairLists fl, PairLists wl,
                                                     float* __restrict__ rho, float* __restrict__ press,
                                                     float* __restrict__ scaled, float* __restrict__ alpha, Status* st,
                                                     TerrainDev T, float4* __restrict__ slope, MoverDev M) {
-    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
-    bool valid = i < p.n;
     uint32_t compressed = 0, longest = 0;
-    if (valid) {
+    // rows of the walk order, a grid's width apart (one each when the grid covers them all)
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x) {
+        const uint32_t i = fl.particle(row);
         float4 a = pos[i];
         int3 cell = cell_of(p, a.x, a.y, a.z);
         // The walk first only lists the neighbours (a tight loop over the ~216 candidates of 27
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
         });
         fl.count[row] = nf;
         wl.count[row] = nw;
-        longest = nf > nw ? nf : nw;
+        longest = max(longest, nf > nw ? nf : nw);
         float sum = 0.0f, wsum = 0.0f;
         float sx = 0.0f, sy = 0.0f, sz = 0.0f, squares = 0.0f;
         float4* const fgv = fl.gv ? fl.gv + fl.at(row, 0) : nullptr;
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params p, GridDev fg, GridDe
             alpha[i] = total > 0.0f ? 1.0f / total : 0.0f;
         }
         float c = density / p.rest - 1.0f;
-        if (c > 0.0f) compressed = __float_as_uint(c);
+        if (c > 0.0f) compressed = max(compressed, __float_as_uint(c));
     }
     compressed = block_reduce(compressed, MaxU(), 0u);
     longest = block_reduce(longest, MaxU(), 0u);
@@ -1321,15 +1321,12 @@ __global__ void __launch_bounds__(kBlock, SLF_PUSH_MIN_BLOCKS) k_push(Params p, 
         push_particle(p, sc, fl, wl, fl.particle(row), row, FromGlobal{pos, nullptr}, pos, vel, walls, applied);
 }
 
-// viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
-// because neighbours read the old velocities.
-__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params p, const StepConsts* __restrict__ sc, PairLists fl,
-                                                    PairLists wl, const float4* __restrict__ pos,
-                                                    const float4* __restrict__ vel, const float* __restrict__ rho,
-                                                    const float4* __restrict__ walls, float4* __restrict__ vel_out) {
-    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
-    if (i >= p.n) return;
+// viscous (step.rs:229-251) + gravity of particle i (row `row` of the walk order)
+__device__ __forceinline__ void viscous_particle(const Params& p, const StepConsts* __restrict__ sc,
+                                                 const PairLists& fl, const PairLists& wl, uint32_t i, uint32_t row,
+                                                 const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                 const float* __restrict__ rho, const float4* __restrict__ walls,
+                                                 float4* __restrict__ vel_out) {
     const float dt = sc->dt;
     const float visc = sc->viscosity;
     float4 a = pos[i];
@@ -1355,6 +1352,16 @@ __global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params 
     v.y = v.y + ay * dt;
     v.z = v.z + az * dt;
     vel_out[i] = v;
+}
+
+// viscous (step.rs:229-251) + gravity, velocity update (dfsph.rs:90-99); writes a new buffer
+// because neighbours read the old velocities.
+__global__ void __launch_bounds__(kBlock, SLF_PAIR_MIN_BLOCKS) k_viscous(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                    PairLists wl, const float4* __restrict__ pos,
+                                                    const float4* __restrict__ vel, const float* __restrict__ rho,
+                                                    const float4* __restrict__ walls, float4* __restrict__ vel_out) {
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x)
+        viscous_particle(p, sc, fl, wl, fl.particle(row), row, pos, vel, rho, walls, vel_out);
 }
 
 __global__ void k_advance(Params p, const StepConsts* __restrict__ sc, const float4* __restrict__ pos_in,
@@ -1672,6 +1679,37 @@ static inline uint32_t blocks_for(uint32_t n) {
     return (n + kBlock - 1) / kBlock;
 }
 
+// The list passes' grids (the solves' check and push, the density pass, the viscosity): with
+// SLF_SOLVER_RESIDENT, no more blocks than the SMs hold at once (each block then strides over
+// rows), so no launch ends on a partial wave and the check's residual sums fewer block partials.
+#ifndef SLF_SOLVER_RESIDENT
+#define SLF_SOLVER_RESIDENT 1
+#endif
+// resident blocks of k_rate<0>, k_rate<1>, k_push, k_density<0>, k_density<1>, k_viscous on the
+// device (prepare_solver_grids; 0: not known yet, the grid then covers every row)
+static std::atomic<uint32_t> g_resident[6] = {0, 0, 0, 0, 0, 0};
+
+void prepare_solver_grids() {
+    if (!SLF_SOLVER_RESIDENT || g_resident[2].load()) return;
+    int dev = 0, sms = 0, per[6] = {0, 0, 0, 0, 0, 0};
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_rate<0>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_rate<1>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_push, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[3], k_density<0>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[4], k_density<1>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[5], k_viscous, kBlock, 0);
+    for (int k = 0; k < 6; ++k) g_resident[k].store(uint32_t(std::max(per[k], 0) * std::max(sms, 0)));
+}
+
+static uint32_t solver_blocks(uint32_t n, int kernel) {
+    uint32_t nb = blocks_for(n);
+    uint32_t resident = g_resident[kernel].load();
+    return resident && resident < nb ? resident : nb;
+}
+
 void launch_pack3(uint32_t n, const float4* in, float* out, cudaStream_t s) {
     if (n) k_pack3<<<blocks_for(n), kBlock, 0, s>>>(n, in, out);
 }
@@ -1738,10 +1776,10 @@ void launch_density(const Params& p, const GridDev& fg, const GridDev& wg, const
         return;
     }
     if (p.solver == 0)
-        k_density<0><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
+        k_density<0><<<solver_blocks(p.n, 3), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
                                                         T, slope, M);
     else
-        k_density<1><<<blocks_for(p.n), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
+        k_density<1><<<solver_blocks(p.n, 4), kBlock, 0, s>>>(p, fg, wg, pos, walls, fl, wl, rho, press, scaled, alpha, st,
                                                         T, slope, M);
 }
 
@@ -1828,32 +1866,6 @@ void launch_cells_wet(const GridDev& g, int3 lo, int3 hi, uint32_t* wet, cudaStr
 
 size_t rate_partial_bytes(uint32_t n) { return (n + kBlock - 1) / kBlock * (sizeof(DD) + sizeof(uint32_t)) + 64; }
 
-// The solver passes' grid: with SLF_SOLVER_RESIDENT, no more blocks than the SMs hold at once
-// (each block then strides over rows), so no launch ends on a partial wave.
-#ifndef SLF_SOLVER_RESIDENT
-#define SLF_SOLVER_RESIDENT 1
-#endif
-// resident blocks of k_rate<0>, k_rate<1>, k_push on the device (prepare_solver_grids; 0: not
-// known yet, the grid then covers every row)
-static std::atomic<uint32_t> g_resident[3] = {0, 0, 0};
-
-void prepare_solver_grids() {
-    if (!SLF_SOLVER_RESIDENT || g_resident[2].load()) return;
-    int dev = 0, sms = 0, per[3] = {0, 0, 0};
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-        return;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_rate<0>, kBlock, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_rate<1>, kBlock, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_push, kBlock, 0);
-    for (int k = 0; k < 3; ++k) g_resident[k].store(uint32_t(std::max(per[k], 0) * std::max(sms, 0)));
-}
-
-static uint32_t solver_blocks(uint32_t n, int kernel) {
-    uint32_t nb = blocks_for(n);
-    uint32_t resident = g_resident[kernel].load();
-    return resident && resident < nb ? resident : nb;
-}
 
 void launch_rate(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                  float4* pos, const float4* vel, const float* rho, const float* alpha, const float4* walls,
@@ -1909,7 +1921,7 @@ void launch_walk_order(uint32_t volume, int3 span, const uint32_t* start, uint32
 
 void launch_viscous(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, const float4* pos,
                     const float4* vel, const float* rho, const float4* walls, float4* vel_out, cudaStream_t s) {
-    if (p.n) k_viscous<<<blocks_for(p.n), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, walls, vel_out);
+    if (p.n) k_viscous<<<solver_blocks(p.n, 5), kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, walls, vel_out);
 }
 
 void launch_advance(const Params& p, const StepConsts* sc, const float4* pos_in, float4* pos_out, float4* vel,
