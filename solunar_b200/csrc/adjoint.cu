@@ -10,6 +10,7 @@
 // with no atomics and no second list.  Neighbour lists are the forward's, fixed for the substep;
 // non-smooth points take the branch the forward took.  Particle-level adjoints are FP32; the
 // parameter gradients are summed in FP64.
+#include <atomic>
 #include <cmath>
 
 #include "fluid_device.cuh"
@@ -883,17 +884,15 @@ __global__ void k_adj_advance_dfsph(Params p, const StepConsts* __restrict__ sc,
 // Writes kw = (w, kappa) and vr = (v, rate-bar) per particle: the three records k_adj_push
 // gathers per neighbour (with the position).
 template <int WHICH>
-__global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+__device__ __forceinline__ void adj_kappa_row(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                       PairLists wl, int form, const float4* __restrict__ pos,
                                                       const float4* __restrict__ walls,
                                                       const float4* __restrict__ w, const float* __restrict__ rate,
                                                       const float* __restrict__ alpha, const float* __restrict__ rho,
                                                       const float4* __restrict__ vel, float4* __restrict__ kw,
                                                       float4* __restrict__ vr, float* __restrict__ abar,
-                                                      float* __restrict__ rb) {
-    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
-    if (i >= p.n) return;
+                                                      float* __restrict__ rb, uint32_t row) {
+    const uint32_t i = fl.particle(row);  // row of the walk order, its particle
     const float dt = sc->dt, m = p.mass;
     float3 xi = f3(pos[i]), wi = f3(w[i]);
     float acc = 0.0f;
@@ -948,6 +947,20 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
     if (WHICH == 1) rb[i] += kbar * ai * dphi_rho;
 }
 
+template <int WHICH>
+__global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                      PairLists wl, int form, const float4* __restrict__ pos,
+                                                      const float4* __restrict__ walls,
+                                                      const float4* __restrict__ w, const float* __restrict__ rate,
+                                                      const float* __restrict__ alpha, const float* __restrict__ rho,
+                                                      const float4* __restrict__ vel, float4* __restrict__ kw,
+                                                      float4* __restrict__ vr, float* __restrict__ abar,
+                                                      float* __restrict__ rb) {
+    // rows a grid's width apart (one each when the grid covers them all)
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x)
+        adj_kappa_row<WHICH>(p, sc, fl, wl, form, pos, walls, w, rate, alpha, rho, vel, kw, vr, abar, rb, row);
+}
+
 // The velocity adjoint before the iteration: w plus the rate pass's transpose (a push on the
 // rate adjoint); and the positions' share of both passes, through grad W.
 // four blocks a SM (64 registers)
@@ -959,14 +972,12 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
 #define SLF_ADJ_PUSH_GV_BLOCKS 4
 #endif
 template <bool GV>
-__global__ void __launch_bounds__(kBlock, GV ? SLF_ADJ_PUSH_GV_BLOCKS : 4) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+__device__ __forceinline__ void adj_push_row(Params p, const StepConsts* __restrict__ sc, PairLists fl,
                                                      PairLists wl, int form, const float4* __restrict__ pos,
                                                      const float4* __restrict__ walls, const float4* __restrict__ kw,
                                                      const float4* __restrict__ vr, float4* __restrict__ wout,
-                                                     float4* __restrict__ xb) {
-    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t i = row < p.n ? fl.particle(row) : row;  // row of the walk order, its particle
-    if (i >= p.n) return;
+                                                     float4* __restrict__ xb, uint32_t row) {
+    const uint32_t i = fl.particle(row);  // row of the walk order, its particle
     const float dt = sc->dt, m = p.mass;
     float4 own_w = kw[i], own_v = vr[i];
     float3 xi = f3(pos[i]), wi = f3(own_w), vi = f3(own_v);
@@ -1039,6 +1050,16 @@ __global__ void __launch_bounds__(kBlock, GV ? SLF_ADJ_PUSH_GV_BLOCKS : 4) k_adj
     wout[i] = make_float4(wi.x + vacc.x, wi.y + vacc.y, wi.z + vacc.z, 0.0f);
     float4 x0 = xb[i];
     xb[i] = make_float4(x0.x + xacc.x, x0.y + xacc.y, x0.z + xacc.z, 0.0f);
+}
+
+template <bool GV>
+__global__ void __launch_bounds__(kBlock, GV ? SLF_ADJ_PUSH_GV_BLOCKS : 4) k_adj_push(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                     PairLists wl, int form, const float4* __restrict__ pos,
+                                                     const float4* __restrict__ walls, const float4* __restrict__ kw,
+                                                     const float4* __restrict__ vr, float4* __restrict__ wout,
+                                                     float4* __restrict__ xb) {
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x)
+        adj_push_row<GV>(p, sc, fl, wl, form, pos, walls, kw, vr, wout, xb, row);
 }
 
 // viscosity + gravity (dfsph.rs:90-99): a-bar = dt w, gravity-bar = sum a-bar
@@ -1136,6 +1157,27 @@ static inline uint32_t adj_blocks(uint32_t n) {
     return (n + kBlock - 1) / kBlock;
 }
 
+// The adjoint's stiffness passes on grids no larger than the SMs hold at once, each block striding
+// over rows (k_adj_kappa<0>, <1>; 0: not looked up yet): 127 -> 123 us at 1M.  The adjoint push
+// keeps a block a 256 rows (on the resident grid: 205 -> 218 us).
+static std::atomic<uint32_t> g_adj_resident[2] = {0, 0};
+
+void prepare_adjoint_grids() {
+    if (g_adj_resident[1].load()) return;
+    int dev = 0, sms = 0, per[2] = {0, 0};
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_adj_kappa<0>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_adj_kappa<1>, kBlock, 0);
+    for (int k = 0; k < 2; ++k) g_adj_resident[k].store(uint32_t(std::max(per[k], 0) * std::max(sms, 0)));
+}
+
+static inline uint32_t adj_iteration_blocks(uint32_t n, int kernel) {
+    uint32_t nb = adj_blocks(n), resident = g_adj_resident[kernel].load();
+    return resident && resident < nb ? resident : nb;
+}
+
 void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                           int form, const float4* pos, const float4* vel, const float* rho, const float* press,
                           const float* scaled, const float4* walls, const float4* vel_pre, const uint32_t* dest,
@@ -1177,10 +1219,10 @@ void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, cons
     if (!p.n) return;
     // parts: 1 the kappa pass, 2 the push, 3 both
     if ((parts & 1) && which == 1)
-        k_adj_kappa<1><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, rate, alpha,
+        k_adj_kappa<1><<<adj_iteration_blocks(p.n, 1), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, rate, alpha,
                                                           rho, vel, kw, vr, abar, rb);
     else if (parts & 1)
-        k_adj_kappa<0><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, rate, alpha,
+        k_adj_kappa<0><<<adj_iteration_blocks(p.n, 0), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, rate, alpha,
                                                           rho, vel, kw, vr, abar, rb);
     if (parts & 2)
         if (fl.gv && wl.gv)

@@ -210,6 +210,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
     if (!tape.on || tape.steps.empty()) return fail(SLF_ERR_OUT_OF_RANGE, "no steps recorded");
     SLF_TRY(flush());
     if (k != n || n != tape.n) return fail(SLF_ERR_INVALID_ARGUMENT, "n must equal slf_len()");
+    prepare_adjoint_grids();
     slf_param_grads pg{};
     if (n == 0) {
         if (out) *out = pg;
