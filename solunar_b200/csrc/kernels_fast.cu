@@ -17,6 +17,8 @@
 #include <cfloat>
 #include <climits>
 
+#include <atomic>
+
 #include "fluid_device.cuh"
 #include "launch.h"
 #include "reduce.cuh"
@@ -602,14 +604,18 @@ __global__ void __launch_bounds__(kBlock) k_rate_fast(Params p, const StepConsts
     if (__ldcg(&st->settled)) return;
     const uint32_t slot = rec.rate ? __ldcg(&st->iterations) : 0u;
     IndexLists fl = index_lists(fpl), wl = index_lists(wpl);
-    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t i = row < p.n ? fpl.particle(row) : row;  // row of the walk order, its particle
-    double err = 0.0;
+    DD acc{0.0, 0.0};
     uint32_t loaded = 0;
-    if (i < p.n)
-        rate_particle_fast<WHICH, REL>(p, sc, fl, wl, i, row, FromGlobalF{pos, vel}, pos, vel, rho, alpha, walls, kappa,
-                                       rec, slot, err, loaded);
-    residual_finish<WHICH>(p, st, partial, partial_loaded, DD{err, 0.0}, loaded, loop);
+    // rows of the walk order, a grid's width apart (one each when the grid covers them all)
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x) {
+        double err = 0.0;
+        uint32_t one = 0;
+        rate_particle_fast<WHICH, REL>(p, sc, fl, wl, fpl.particle(row), row, FromGlobalF{pos, vel}, pos, vel, rho,
+                                       alpha, walls, kappa, rec, slot, err, one);
+        acc = dd_add(acc, DD{err, 0.0});
+        loaded += one;
+    }
+    residual_finish<WHICH>(p, st, partial, partial_loaded, acc, loaded, loop);
 }
 
 template <bool REL, class Src>
@@ -807,6 +813,23 @@ static inline uint32_t fast_blocks(uint32_t n) {
     return (n + kBlock - 1) / kBlock;
 }
 
+// The FAST check on grids no larger than the SMs hold at once (as the EXACT one: its last block
+// then sums fewer partials); k_rate_fast<which, rel> at [which * 2 + rel], 0 until looked up.
+static std::atomic<uint32_t> g_fast_resident[4] = {0, 0, 0, 0};
+
+void prepare_fast_grids() {
+    if (g_fast_resident[3].load()) return;
+    int dev = 0, sms = 0, per[4] = {0, 0, 0, 0};
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_rate_fast<0, false>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_rate_fast<0, true>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_rate_fast<1, false>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[3], k_rate_fast<1, true>, kBlock, 0);
+    for (int k = 0; k < 4; ++k) g_fast_resident[k].store(uint32_t(std::max(per[k], 0) * std::max(sms, 0)));
+}
+
 void launch_density_fast(const Params& p, const GridDev& fg, const GridDev& wg, const float4* pos, const int4* cells,
                          const float4* walls, const PairLists& fl, const PairLists& wl, float* rho, float* press,
                          float* scaled, float* alpha, Status* st, cudaStream_t s) {
@@ -849,8 +872,10 @@ void launch_rate_fast(int which, bool rel, const Params& p, const StepConsts* sc
                       unsigned long long loop) {
     if (!p.n) return;
     uint32_t nb = fast_blocks(p.n);
+    const uint32_t resident = g_fast_resident[which * 2 + (rel ? 1 : 0)].load();
     DD* part = static_cast<DD*>(partials);
-    uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);
+    uint32_t* loaded = reinterpret_cast<uint32_t*>(part + nb);  // the partials' room: a block a 256 rows
+    if (resident && resident < nb) nb = resident;
     float* kw = reinterpret_cast<float*>(pos);
     if (which == 0 && rel)
         k_rate_fast<0, true><<<nb, kBlock, 0, s>>>(p, sc, fl, wl, pos, vel, rho, alpha, walls, kw, part, loaded, st,

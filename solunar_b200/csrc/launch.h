@@ -83,8 +83,9 @@ size_t rate_partial_bytes(uint32_t n);
 // Looks up, once per process, how many blocks of the solver passes the device holds at once (not
 // during a stream capture): their grids take no more, each block striding over rows.
 void prepare_solver_grids();
-// The same for the adjoint's stiffness passes (adjoint.cu).
+// The same for the adjoint's stiffness passes (adjoint.cu) and the FAST check (kernels_fast.cu).
 void prepare_adjoint_grids();
+void prepare_fast_grids();
 // One solver check: writes each particle's stiffness into the w lane of its position, and either
 // sets st->settled or advances st->iterations.  Both it and the push do nothing once the solve
 // has settled, so a batch of iterations can be queued ahead of the check that ends it.

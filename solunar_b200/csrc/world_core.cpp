@@ -322,6 +322,7 @@ int32_t World::flush() {
 
 int32_t World::ensure_work_buffers() {
     prepare_solver_grids();
+    if (fast()) prepare_fast_grids();
     SLF_TRY(press.ensure(n, 0, stream));
     SLF_TRY(scaled.ensure(n, 0, stream));
     SLF_TRY(alpha.ensure(n, 0, stream));
