@@ -38,8 +38,8 @@ enum {
     SLF_ERR_DISPATCH_INCOMPLETE = 5, /* PhysicsError::DispatchIncomplete (src/error.rs:15) */
     SLF_ERR_UNSUPPORTED = 6,         /* a combination not built: FAST arithmetic with terrain or bodies,
                                       * cell-relative positions with EXACT arithmetic, a tape with
-                                      * warm starts, with dynamic bodies or with bodies and
-                                      * checkpoints, terrain added while a tape records, shallow water */
+                                      * dynamic bodies or with bodies and checkpoints, terrain
+                                      * added while a tape records, shallow water */
     SLF_ERR_CUDA = 7,                /* a CUDA call failed; see slf_last_error() */
     SLF_ERR_TIMEOUT = 8,             /* a bounded device loop gave up */
     SLF_ERR_INVALID_ARGUMENT = 9,    /* null pointer or wrong buffer size */
@@ -322,8 +322,10 @@ typedef struct slf_param_grads {
  * records add the 16-byte cell of each particle); WCSPH with terrain (its density, push, damping
  * and contact; terrain added while recording is UNSUPPORTED); WCSPH with coupled bodies on the
  * caller's paths, checkpoint_every 0 only (each substep's forward is kept as it runs, since the
- * body points' order follows their history).  UNSUPPORTED: warm_start, dynamic bodies (whose lift
- * gives momentum back to the water), bodies with checkpoints. */
+ * body points' order follows their history); DFSPH with warm_start (checkpoints and records keep
+ * each particle's two impulses, 8 bytes, and the backward pass carries their adjoint from substep
+ * to substep).  UNSUPPORTED: dynamic bodies (whose lift gives momentum back to the water), bodies
+ * with checkpoints. */
 int32_t slf_tape_begin(slf_world* world, uint32_t checkpoint_every);
 /* Stops recording.  The tape's device buffers (substep records, checkpoints) stay with the world
  * and are reused by the next tape, so the rounds of an optimisation loop record without

@@ -849,13 +849,16 @@ __global__ void __launch_bounds__(kBlock) k_adj_density(Params p, PairLists fl, 
 }
 
 // ---- the sort (mod.rs:541-566): back to the order before it ------------------------------------
+// (ib, ip: the warm starts' impulse adjoint, when the solves start warm)
 __global__ void k_adj_unsort(uint32_t n, const uint32_t* __restrict__ dest, const float4* __restrict__ xb,
-                             const float4* __restrict__ vb, float4* __restrict__ xp, float4* __restrict__ vp) {
+                             const float4* __restrict__ vb, float4* __restrict__ xp, float4* __restrict__ vp,
+                             const float2* __restrict__ ib, float2* __restrict__ ip) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t f = dest[i];
     xp[i] = xb[f];
     vp[i] = vb[f];
+    if (ib) ip[i] = ib[f];
 }
 
 // ---- DFSPH (dfsph.rs:79-275) --------------------------------------------------------------------
@@ -879,22 +882,11 @@ __global__ void k_adj_advance_dfsph(Params p, const StepConsts* __restrict__ sc,
                        (flags & 4u ? 0.0f : v.z) + yz * dt, 0.0f);
 }
 
-// One iteration's stiffness, back from the velocity adjoint w after its push: kappa-bar = -dt
-// rate(w); then through kappa = phi(rate) alpha (dfsph.rs:241-259).
-// Writes kw = (w, kappa) and vr = (v, rate-bar) per particle: the three records k_adj_push
-// gathers per neighbour (with the position).
-template <int WHICH>
-__device__ __forceinline__ void adj_kappa_row(Params p, const StepConsts* __restrict__ sc, PairLists fl,
-                                                      PairLists wl, int form, const float4* __restrict__ pos,
-                                                      const float4* __restrict__ walls,
-                                                      const float4* __restrict__ w, const float* __restrict__ rate,
-                                                      const float* __restrict__ alpha, const float* __restrict__ rho,
-                                                      const float4* __restrict__ vel, float4* __restrict__ kw,
-                                                      float4* __restrict__ vr, float* __restrict__ abar,
-                                                      float* __restrict__ rb, uint32_t row) {
-    const uint32_t i = fl.particle(row);  // row of the walk order, its particle
-    const float dt = sc->dt, m = p.mass;
-    float3 xi = f3(pos[i]), wi = f3(w[i]);
+// density_rate (dfsph.rs:166-181) of the velocity adjoint w at row's particle i, without its mass:
+// sum_j (w_i - w_j) . grad W_ij + sum_walls w_i . grad W_iw, over the substep's lists.
+__device__ __forceinline__ float adjoint_rate(const Params& p, const PairLists& fl, const PairLists& wl, int form,
+                                              const float4* __restrict__ pos, const float4* __restrict__ walls,
+                                              const float4* __restrict__ w, uint32_t row, float3 xi, float3 wi) {
     float acc = 0.0f;
     if (fl.gv && wl.gv) {
         // the forward's kept gradients (EXACT DFSPH): rate(w) gathers only w of each neighbour
@@ -924,7 +916,29 @@ __device__ __forceinline__ void adj_kappa_row(Params p, const StepConsts* __rest
             acc += dotf(wi, r) * g;
         }
     }
-    float kbar = -dt * m * acc;
+    return acc;
+}
+
+// One iteration's stiffness, back from the velocity adjoint w after its push: kappa-bar = -dt
+// rate(w); then through kappa = phi(rate) alpha (dfsph.rs:241-259).
+// Writes kw = (w, kappa) and vr = (v, rate-bar) per particle: the three records k_adj_push
+// gathers per neighbour (with the position).
+template <int WHICH>
+__device__ __forceinline__ void adj_kappa_row(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                      PairLists wl, int form, const float4* __restrict__ pos,
+                                                      const float4* __restrict__ walls,
+                                                      const float4* __restrict__ w, const float* __restrict__ rate,
+                                                      const float* __restrict__ alpha, const float* __restrict__ rho,
+                                                      const float4* __restrict__ vel, float4* __restrict__ kw,
+                                                      float4* __restrict__ vr, float* __restrict__ abar,
+                                                      float* __restrict__ rb, const float2* __restrict__ appbar,
+                                                      uint32_t row) {
+    const uint32_t i = fl.particle(row);  // row of the walk order, its particle
+    const float dt = sc->dt, m = p.mass;
+    float3 xi = f3(pos[i]), wi = f3(w[i]);
+    float kbar = -dt * m * adjoint_rate(p, fl, wl, form, pos, walls, w, row, xi, wi);
+    // warm starts: the impulse the solve leaves sums each push's kappa dt (applied-bar of WHICH)
+    if (appbar) kbar += dt * (WHICH == 1 ? appbar[i].y : appbar[i].x);
     float ri = rate[i], ai = alpha[i];
     float phi, dphi, dphi_rho = 0.0f;
     if (WHICH == 1) {
@@ -955,10 +969,38 @@ __global__ void __launch_bounds__(kBlock) k_adj_kappa(Params p, const StepConsts
                                                       const float* __restrict__ alpha, const float* __restrict__ rho,
                                                       const float4* __restrict__ vel, float4* __restrict__ kw,
                                                       float4* __restrict__ vr, float* __restrict__ abar,
-                                                      float* __restrict__ rb) {
+                                                      float* __restrict__ rb, const float2* __restrict__ appbar) {
     // rows a grid's width apart (one each when the grid covers them all)
     for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < p.n; row += gridDim.x * blockDim.x)
-        adj_kappa_row<WHICH>(p, sc, fl, wl, form, pos, walls, w, rate, alpha, rho, vel, kw, vr, abar, rb, row);
+        adj_kappa_row<WHICH>(p, sc, fl, wl, form, pos, walls, w, rate, alpha, rho, vel, kw, vr, abar, rb, appbar,
+                             row);
+}
+
+// The warm push of a solve (dfsph.rs's cold start replaced by one push at kappa_w = share applied /
+// dt before the first check): kappa_w-bar from the velocity adjoint w after it, as the stiffness
+// pass forms kappa-bar, plus dt applied-bar (the solve's impulse starts at kappa_w dt); the records
+// k_adj_push then reads (rate-bar and velocities zero: the push moves only positions' adjoint), and
+// applied-bar before the solve, kappa_w-bar share / dt, into component WHICH of appbar_out.
+template <int WHICH>
+__global__ void __launch_bounds__(kBlock) k_adj_warm(Params p, const StepConsts* __restrict__ sc, PairLists fl,
+                                                     PairLists wl, int form, const float4* __restrict__ pos,
+                                                     const float4* __restrict__ walls, const float4* __restrict__ w,
+                                                     const float2* __restrict__ applied,
+                                                     const float2* __restrict__ appbar, float share,
+                                                     float4* __restrict__ kw, float4* __restrict__ vr,
+                                                     float2* __restrict__ appbar_out) {
+    const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= p.n) return;
+    const uint32_t i = fl.particle(row);
+    const float dt = sc->dt, m = p.mass;
+    const float3 xi = f3(pos[i]), wi = f3(w[i]);
+    float kbar = -dt * m * adjoint_rate(p, fl, wl, form, pos, walls, w, row, xi, wi);
+    kbar += dt * (WHICH == 1 ? appbar[i].y : appbar[i].x);
+    // the forward's kappa_w, rounded as k_warm_kappa rounds it
+    const float kappa = __fdiv_rn(__fmul_rn(share, WHICH == 1 ? applied[i].y : applied[i].x), dt);
+    kw[i] = make_float4(wi.x, wi.y, wi.z, kappa);
+    vr[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    reinterpret_cast<float*>(appbar_out)[2 * size_t(i) + WHICH] = kbar * share / dt;
 }
 
 // The velocity adjoint before the iteration: w plus the rate pass's transpose (a push on the
@@ -1202,7 +1244,7 @@ void launch_adjoint_wcsph(const Params& p, const StepConsts* sc, const PairLists
                                                              walls, ab, xb, vb, rb, grads, 0, T, slope, MoverDev{});
         k_adj_density<<<adj_blocks(p.n), kBlock, 0, s>>>(p, fl, wl, form, pos, walls, rb, xb, nullptr, MoverDev{});
     }
-    k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp);
+    k_adj_unsort<<<adj_blocks(p.n), kBlock, 0, s>>>(p.n, dest, xb, vb, xp, vp, nullptr, nullptr);
 }
 
 
@@ -1215,15 +1257,16 @@ void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float
 void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                           int form, const float4* pos, const float4* walls, const float4* w, const float* rate,
                           const float* alpha, const float* rho, const float4* vel, float4* kw, float4* vr,
-                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s, int parts) {
+                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s, int parts,
+                          const float2* appbar) {
     if (!p.n) return;
     // parts: 1 the kappa pass, 2 the push, 3 both
     if ((parts & 1) && which == 1)
         k_adj_kappa<1><<<adj_iteration_blocks(p.n, 1), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, rate, alpha,
-                                                          rho, vel, kw, vr, abar, rb);
+                                                          rho, vel, kw, vr, abar, rb, appbar);
     else if (parts & 1)
         k_adj_kappa<0><<<adj_iteration_blocks(p.n, 0), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, rate, alpha,
-                                                          rho, vel, kw, vr, abar, rb);
+                                                          rho, vel, kw, vr, abar, rb, appbar);
     if (parts & 2)
         if (fl.gv && wl.gv)
             k_adj_push<true><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, kw, vr, wout,
@@ -1231,6 +1274,21 @@ void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, cons
         else
             k_adj_push<false><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, kw, vr, wout,
                                                                  xb);
+}
+
+void launch_adj_warm(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                     int form, const float4* pos, const float4* walls, const float4* w, const float2* applied,
+                     const float2* appbar, float share, float4* kw, float4* vr, float2* appbar_out, float4* wout,
+                     float4* xb, cudaStream_t s) {
+    if (!p.n) return;
+    if (which == 1)
+        k_adj_warm<1><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, applied, appbar, share,
+                                                         kw, vr, appbar_out);
+    else
+        k_adj_warm<0><<<adj_blocks(p.n), kBlock, 0, s>>>(p, sc, fl, wl, form, pos, walls, w, applied, appbar, share,
+                                                         kw, vr, appbar_out);
+    launch_adj_iteration(which, p, sc, fl, wl, form, pos, walls, w, nullptr, nullptr, nullptr, nullptr, kw, vr,
+                         nullptr, nullptr, wout, xb, s, 2);
 }
 
 void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, int form,
@@ -1254,8 +1312,8 @@ void launch_adj_factors_density(const Params& p, const PairLists& fl, const Pair
 }
 
 void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const float4* vb, float4* xp, float4* vp,
-                       cudaStream_t s) {
-    if (n) k_adj_unsort<<<adj_blocks(n), kBlock, 0, s>>>(n, dest, xb, vb, xp, vp);
+                       cudaStream_t s, const float2* ib, float2* ip) {
+    if (n) k_adj_unsort<<<adj_blocks(n), kBlock, 0, s>>>(n, dest, xb, vb, xp, vp, ib, ip);
 }
 
 }  // namespace slf

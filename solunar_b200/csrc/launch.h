@@ -211,7 +211,16 @@ void launch_adj_advance_dfsph(const Params& p, const StepConsts* sc, const float
 void launch_adj_iteration(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
                           int form, const float4* pos, const float4* walls, const float4* w, const float* rate,
                           const float* alpha, const float* rho, const float4* vel, float4* kw, float4* vr,
-                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s, int parts = 3);
+                          float* abar, float* rb, float4* wout, float4* xb, cudaStream_t s, int parts = 3,
+                          const float2* appbar = nullptr);
+// warm starts: the adjoint of a solve's warm push (kappa_w = share applied / dt, applied the
+// impulse of the particle's last solve of this kind, sorted): its kappa_w-bar from w, the push's
+// position adjoint into xb, w through to wout, and applied-bar before the solve into component
+// `which` of appbar_out (appbar: the adjoint of the impulse the solve leaves)
+void launch_adj_warm(int which, const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl,
+                     int form, const float4* pos, const float4* walls, const float4* w, const float2* applied,
+                     const float2* appbar, float share, float4* kw, float4* vr, float2* appbar_out, float4* wout,
+                     float4* xb, cudaStream_t s);
 void launch_adj_viscosity(const Params& p, const StepConsts* sc, const PairLists& fl, const PairLists& wl, int form,
                           const float4* pos, const float4* vel, const float* rho, const float* zeros,
                           const float4* walls, float4* w, float4* ab, float4* xb, float* rb, double* grads,
@@ -220,7 +229,7 @@ void launch_adj_factors_density(const Params& p, const PairLists& fl, const Pair
                                 const float4* pos, const float4* walls, const float* alpha, const float* abar,
                                 float4* gt, const float* rb, float4* xb, cudaStream_t s);
 void launch_adj_unsort(uint32_t n, const uint32_t* dest, const float4* xb, const float4* vb, float4* xp, float4* vp,
-                       cudaStream_t s);
+                       cudaStream_t s, const float2* ib = nullptr, float2* ip = nullptr);
 
 // kernels launched through this library by the process so far
 uint64_t kernel_launches();

@@ -427,6 +427,7 @@ struct World {
         DevBuf<float4> pos, vel;
         DevBuf<uint32_t> ids;
         DevBuf<int4> cells;  // cell-relative positions: the cells of pos's offsets
+        DevBuf<float2> warm;  // warm starts: each particle's impulses before the substep
         DfsphRecord rec;
         // A WCSPH substep that a checkpoint segment ran again keeps what its adjoint reads (the
         // sorted state, densities and pressures, the sort's destinations, the pre-clamp
@@ -455,6 +456,7 @@ struct World {
             vel.release(st);
             ids.release(st);
             cells.release(st);
+            warm.release(st);
             rec.release(st);
             for (auto* b : {&spos, &svel, &pre, &slope}) b->release(st);
             scells.release(st);
@@ -487,6 +489,7 @@ struct World {
         DevBuf<float4> cpos, cvel;              // [c][n]
         DevBuf<uint32_t> cids;
         DevBuf<int4> ccells;                    // cell-relative positions: [c][n]
+        DevBuf<float2> cwarm;                   // warm starts: [c][n]
         std::vector<std::unique_ptr<SubRecord>> subs;  // every == 0: each substep's record
         bool keep_segments = false;  // WCSPH checkpoint segments keep each substep's forward
     } tape;
@@ -501,8 +504,12 @@ struct World {
         DevBuf<int4> scells;
         DevBuf<float> srho, rb, abar, zeros;
         DevBuf<double> grads;
+        // warm starts: the world's impulses, put back at the end; the adjoint of the impulses
+        // each particle's solves leave (after the substep; before it)
+        DevBuf<float2> swarm, appbar, appbar_out;
         void release(cudaStream_t s) {
             scells.release(s);
+            for (auto* b : {&swarm, &appbar, &appbar_out}) b->release(s);
             for (auto* b : {&spos, &svel, &xo, &vo, &xp, &vp, &ab, &xb, &vb, &pre, &gt, &kw, &vr}) b->release(s);
             for (auto* b : {&srho, &rb, &abar, &zeros}) b->release(s);
             sids.release(s);
@@ -1010,9 +1017,11 @@ struct World {
 
     // the committed state (positions, velocities, ids and, for cell-relative positions, cells) to
     // and from device buffers of n entries; c may be null for absolute positions
-    int32_t save_state(float4* p, float4* v, uint32_t* id, int4* c);
+    // (w: warm starts' impulses of each particle, copied when warm starts are on)
+    int32_t save_state(float4* p, float4* v, uint32_t* id, int4* c, float2* w = nullptr);
 
-    int32_t load_state(const float4* p, const float4* v, const uint32_t* id, const int4* c);
+    int32_t load_state(const float4* p, const float4* v, const uint32_t* id, const int4* c,
+                       const float2* w = nullptr);
 
     int32_t substep_retrying(float dt);
 

@@ -80,7 +80,6 @@ int32_t World::sync() {
 }
 
 int32_t World::tape_begin(uint32_t every) {
-    if (warm_on()) return fail(SLF_ERR_UNSUPPORTED, "the adjoint runs on cold-started solves only");
     SLF_TRY(flush());
     tape.on = true;
     tape.every = every;
@@ -121,7 +120,8 @@ int32_t World::record_begin(float dt) {
     SLF_TRY(sub->vel.ensure(n, 0, stream));
     SLF_TRY(sub->ids.ensure(n, 0, stream));
     if (rel()) SLF_TRY(sub->cells.ensure(n, 0, stream));
-    SLF_TRY(save_state(sub->pos.p, sub->vel.p, sub->ids.p, sub->cells.p));
+    if (warm_on()) SLF_TRY(sub->warm.ensure(n, 0, stream));
+    SLF_TRY(save_state(sub->pos.p, sub->vel.p, sub->ids.p, sub->cells.p, sub->warm.p));
     tape.subs.push_back(std::move(sub));
     return SLF_OK;
 }
@@ -141,8 +141,9 @@ int32_t World::checkpoint() {
     SLF_TRY(tape.cvel.ensure((c + 1) * m, c * m, stream));
     SLF_TRY(tape.cids.ensure((c + 1) * m, c * m, stream));
     if (rel()) SLF_TRY(tape.ccells.ensure((c + 1) * m, c * m, stream));
+    if (warm_on()) SLF_TRY(tape.cwarm.ensure((c + 1) * m, c * m, stream));
     SLF_TRY(save_state(tape.cpos.p + c * m, tape.cvel.p + c * m, tape.cids.p + c * m,
-                       rel() ? tape.ccells.p + c * m : nullptr));
+                       rel() ? tape.ccells.p + c * m : nullptr, warm_on() ? tape.cwarm.p + c * m : nullptr));
     tape.ckpt_sub.push_back(tape.count);
     return SLF_OK;
 }
@@ -155,8 +156,10 @@ int32_t World::tape_substep(float dt) {
     return SLF_OK;
 }
 
-int32_t World::save_state(float4* p, float4* v, uint32_t* id, int4* c) {
+int32_t World::save_state(float4* p, float4* v, uint32_t* id, int4* c, float2* w) {
     if (!n) return SLF_OK;
+    if (w && warm_on())
+        SLF_CUDA(cudaMemcpyAsync(w, warm[cid].p, n * sizeof(float2), cudaMemcpyDeviceToDevice, stream));
     SLF_CUDA(cudaMemcpyAsync(p, pos[cpos].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
     SLF_CUDA(cudaMemcpyAsync(v, vel[cpos].p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
     SLF_CUDA(cudaMemcpyAsync(id, ids[cid].p, n * 4, cudaMemcpyDeviceToDevice, stream));
@@ -164,7 +167,9 @@ int32_t World::save_state(float4* p, float4* v, uint32_t* id, int4* c) {
     return SLF_OK;
 }
 
-int32_t World::load_state(const float4* p, const float4* v, const uint32_t* id, const int4* c) {
+int32_t World::load_state(const float4* p, const float4* v, const uint32_t* id, const int4* c, const float2* w) {
+    if (n && w && warm_on())
+        SLF_CUDA(cudaMemcpyAsync(warm[cid].p, w, n * sizeof(float2), cudaMemcpyDeviceToDevice, stream));
     if (n) {
         SLF_CUDA(cudaMemcpyAsync(pos[cpos].p, p, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
         SLF_CUDA(cudaMemcpyAsync(vel[cpos].p, v, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
@@ -235,7 +240,12 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
         SLF_TRY(dest.ensure(n, 0, stream));
         SLF_TRY(grads.ensure(kGradSlots, 0, stream));
         if (rel()) SLF_TRY(scells.ensure(n, 0, stream));
-        SLF_TRY(save_state(spos.p, svel.p, sids.p, scells.p));
+        if (warm_on()) {
+            for (auto* b : {&B.swarm, &B.appbar, &B.appbar_out}) SLF_TRY(b->ensure(n, 0, stream));
+            // the impulses the last substep's solves leave reach no output
+            SLF_CUDA(cudaMemsetAsync(B.appbar.p, 0, n * sizeof(float2), stream));
+        }
+        SLF_TRY(save_state(spos.p, svel.p, sids.p, scells.p, B.swarm.p));
         SLF_CUDA(cudaMemcpyAsync(srho.p, rho[cid].p, n * 4, cudaMemcpyDeviceToDevice, stream));
         SLF_TRY(write_vec(xo, dpos, n));
         SLF_TRY(write_vec(vo, dvel, n));
@@ -289,16 +299,31 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                 });
                 SLF_CUDA(cudaMemsetAsync(rb.p, 0, n * 4, stream));
                 SLF_CUDA(cudaMemsetAsync(abar.p, 0, n * 4, stream));
+                // warm starts: the impulses before the substep (the replayed sort left them in
+                // slot nid, sorted) and their adjoint after it
+                const float2* applied = warm_on() ? warm[nid].p : nullptr;
+                const float2* apb = warm_on() ? B.appbar.p : nullptr;
+                // each solve's warm push ran before its first check: its adjoint after the
+                // last iteration's (share: the forward's half of the last impulse)
+                auto warm_push = [&](int which) {
+                    if (!applied) return;
+                    timed(which == 1 ? "adj_warm_density" : "adj_warm_divergence", 0.0, [&] {
+                        launch_adj_warm(which, p, d_consts, fl, wl, form, pos[a].p, dwalls.p, vb.p, applied, apb,
+                                        0.5f, kw.p, vr.p, B.appbar_out.p, vp.p, xb.p, stream);
+                    });
+                    std::swap(vb, vp);
+                };
                 for (uint32_t it = rec.den_n; it-- > 0;) {
                     for (int part = 1; part <= 2; ++part)
                         timed(part == 1 ? "adj_kappa_density" : "adj_push_density", 0.0, [&] {
                             launch_adj_iteration(1, p, d_consts, fl, wl, form, pos[a].p, dwalls.p, vb.p,
                                                  rec.den_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
                                                  rec.den_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p,
-                                                 vp.p, xb.p, stream, part);
+                                                 vp.p, xb.p, stream, part, apb);
                         });
                     std::swap(vb, vp);
                 }
+                warm_push(1);
                 timed("adj_viscosity", 0.0, [&] {
                     launch_adj_viscosity(p, d_consts, fl, wl, form, pos[a].p, rec.va.p, rho[nid].p, zeros.p,
                                          dwalls.p, vb.p, ab.p, xb.p, rb.p, grads.p, stream);
@@ -309,15 +334,19 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                             launch_adj_iteration(0, p, d_consts, fl, wl, form, pos[a].p, dwalls.p, vb.p,
                                                  rec.div_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
                                                  rec.div_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p,
-                                                 vp.p, xb.p, stream, part);
+                                                 vp.p, xb.p, stream, part, apb);
                         });
                     std::swap(vb, vp);
                 }
+                warm_push(0);
                 timed("adj_factors_density", 0.0, [&] {
                     launch_adj_factors_density(p, fl, wl, form, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p,
                                                rb.p, xb.p, stream);
                 });
-                timed("adj_unsort", 0.0, [&] { launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream); });
+                timed("adj_unsort", 0.0, [&] {
+                    launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream,
+                                      warm_on() ? B.appbar_out.p : nullptr, B.appbar.p);
+                });
             }
             double g[kGradSlots];
             SLF_CUDA(cudaMemcpyAsync(g, grads.p, sizeof(g), cudaMemcpyDeviceToHost, stream));
@@ -359,7 +388,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                     SLF_TRY(adjoint_substep(sub.dt, 0, 0, sub.rec, &sub));
                     continue;
                 }
-                SLF_TRY(load_state(sub.pos.p, sub.vel.p, sub.ids.p, sub.cells.p));
+                SLF_TRY(load_state(sub.pos.p, sub.vel.p, sub.ids.p, sub.cells.p, sub.warm.p));
                 int a = 0, nid = 0;
                 if (s.solver == SLF_SOLVER_WCSPH) {
                     SLF_TRY(recompute(sub.dt, sub.rec, a, nid));
@@ -394,7 +423,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                 std::vector<float> dts(all.begin() + b, all.begin() + e);
                 while (segsubs.size() < dts.size()) segsubs.push_back(new_record());
                 SLF_TRY(load_state(tape.cpos.p + c * n, tape.cvel.p + c * n, tape.cids.p + c * n,
-                                   rel() ? tape.ccells.p + c * n : nullptr));
+                                   rel() ? tape.ccells.p + c * n : nullptr, warm_on() ? tape.cwarm.p + c * n : nullptr));
                 for (size_t q = 0; q < dts.size(); ++q) {
                     SubRecord& sub = *segsubs[q];
                     sub.dt = dts[q];
@@ -402,7 +431,8 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                     SLF_TRY(sub.vel.ensure(n, 0, stream));
                     SLF_TRY(sub.ids.ensure(n, 0, stream));
                     if (rel()) SLF_TRY(sub.cells.ensure(n, 0, stream));
-                    SLF_TRY(save_state(sub.pos.p, sub.vel.p, sub.ids.p, sub.cells.p));
+                    if (warm_on()) SLF_TRY(sub.warm.ensure(n, 0, stream));
+                    SLF_TRY(save_state(sub.pos.p, sub.vel.p, sub.ids.p, sub.cells.p, sub.warm.p));
                     uint32_t held = 0, its = 0;
                     int32_t rs;
                     if (s.solver == SLF_SOLVER_WCSPH && !tape.keep_segments) {
@@ -436,7 +466,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
         if (dpos0) SLF_TRY(read_vec(xo, dpos0, n));
         if (dvel0) SLF_TRY(read_vec(vo, dvel0, n));
         // the state as it was
-        SLF_TRY(load_state(spos.p, svel.p, sids.p, scells.p));
+        SLF_TRY(load_state(spos.p, svel.p, sids.p, scells.p, B.swarm.p));
         SLF_CUDA(cudaMemcpyAsync(rho[cid].p, srho.p, n * 4, cudaMemcpyDeviceToDevice, stream));
         return sync();
     };

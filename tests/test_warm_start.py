@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from solunar_b200 import scenes
-from solunar_b200.abi import Arithmetic, FluidSettings, FluidSolver, PhysicsError
+from solunar_b200.abi import Arithmetic, FluidSettings, FluidSolver
 
 TICK = np.float32(1.0 / 60.0)
 
@@ -110,11 +110,17 @@ def test_a_loaded_snapshot_starts_cold(backend):
 
 
 @pytest.mark.gpu
-def test_warm_start_takes_no_tape(gpu_lib):
-    w = dam(lambda s: gpu_lib.FluidWorld(s), True, counts=(4, 4, 4))
-    with pytest.raises(PhysicsError) as e:
-        w.tape_begin(0)
-    assert e.value.kind == "Unsupported"
+def test_a_warm_taped_forward_is_the_untaped_one(gpu_lib):
+    # a tape records the impulses with the state (the adjoint is tests/test_gpu_adjoint_warm.py)
+    taped = dam(lambda s: gpu_lib.FluidWorld(s), True, counts=(4, 4, 4))
+    plain = dam(lambda s: gpu_lib.FluidWorld(s), True, counts=(4, 4, 4))
+    for every in (0, 2):
+        taped.tape_begin(every)
+        for _ in range(3):
+            taped.step(1e-3)
+            plain.step(1e-3)
+        taped.tape_end()
+        assert taped.state_hash() == plain.state_hash()
 
 
 @pytest.mark.gpu
