@@ -473,54 +473,64 @@ def main():
     # substep's solver record kept, or checkpoints every --adjoint-every substeps), then the reverse
     # pass, for a loss of the kinetic energy of the water beyond x = 1 m (gradients with respect
     # to every initial velocity and the settings)
-    adjoint = None
-    if args.adjoint_steps > 0 and args.positions == "absolute":
-        import numpy as np
+    import numpy as np
 
-        k = args.adjoint_steps
-        every = max(0, args.adjoint_every)
+    def loss_grad(w):
+        pos_now, vel_now = w.positions(), w.velocities()
+        m = w.particle_mass()
+        return np.where((pos_now[:, 0] > 1.0)[:, None], m * vel_now, 0.0).astype(np.float32)
 
-        def loss_grad():
-            pos_now, vel_now = world.positions(), world.velocities()
-            m = world.particle_mass()
-            return np.where((pos_now[:, 0] > 1.0)[:, None], m * vel_now, 0.0).astype(np.float32)
-
-        # one untimed round first (one segment long), as the rounds of an optimisation loop follow
-        # one another: the tape's memory is then in the allocator's pool
-        world.tape_begin(every)
+    def taped_round(w, wstream, k, every):
+        """A taped forward of k steps on world w and its reverse pass, each timed with CUDA events on
+        the world's stream, after one untimed round (one segment long), as the rounds of an
+        optimisation loop follow one another: the tape's memory is then in the allocator's pool."""
+        torch.cuda.synchronize()
+        free_b, total_b = torch.cuda.mem_get_info(dev)
+        before_gb = (total_b - free_b) / 1e9
+        w.tape_begin(every)
         for _ in range(k if every == 0 else min(k, every)):
-            world.step(sc.dt)
-        dv = loss_grad()
-        world.step_backward(np.zeros_like(dv), dv)
-        world.tape_end()
+            w.step(sc.dt)
+        dv = loss_grad(w)
+        w.step_backward(np.zeros_like(dv), dv)
+        w.tape_end()
         barrier()
-        world.tape_begin(every)
+        w.tape_begin(every)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        adj_substeps = 0
+        e0.record(wstream)
+        substeps = 0
         for _ in range(k):
-            adj_substeps += world.step(sc.dt).substeps
-        e1.record(stream)
+            substeps += w.step(sc.dt).substeps
+        e1.record(wstream)
         e1.synchronize()
         fwd_ms = e0.elapsed_time(e1)
         # device memory in use with the tape held (the whole device: this process is its only user)
         free_b, total_b = torch.cuda.mem_get_info(dev)
         taped_gb = (total_b - free_b) / 1e9
-        dv = loss_grad()
+        dv = loss_grad(w)
         torch.cuda.synchronize()
         e2 = torch.cuda.Event(enable_timing=True)
         e3 = torch.cuda.Event(enable_timing=True)
-        e2.record(stream)
-        dp0, dv0, grads = world.step_backward(np.zeros_like(dv), dv)
-        e3.record(stream)
+        e2.record(wstream)
+        dp0, dv0, grads = w.step_backward(np.zeros_like(dv), dv)
+        e3.record(wstream)
         e3.synchronize()
         bwd_ms = e2.elapsed_time(e3)
         free_b, total_b = torch.cuda.mem_get_info(dev)
-        backward_gb = (total_b - free_b) / 1e9
-        world.tape_end()
-        adj_all, both_ms = reduce_timing(adj_substeps, fwd_ms + bwd_ms, world_size, dev)
-        _, fwd_ms = reduce_timing(adj_substeps, fwd_ms, world_size, dev)
+        w.tape_end()
+        return {"substeps": substeps, "fwd_ms": fwd_ms, "bwd_ms": bwd_ms, "taped_gb": taped_gb, "before_gb": before_gb,
+                "backward_gb": (total_b - free_b) / 1e9, "total_gb": total_b / 1e9,
+                "dp0": dp0, "dv0": dv0, "grads": grads}
+
+    adjoint = None
+    if args.adjoint_steps > 0 and args.positions == "absolute":
+        k = args.adjoint_steps
+        every = max(0, args.adjoint_every)
+        tr = taped_round(world, stream, k, every)
+        adj_substeps, dp0, dv0, grads = tr["substeps"], tr["dp0"], tr["dv0"], tr["grads"]
+        taped_gb, backward_gb, total_b = tr["taped_gb"], tr["backward_gb"], tr["total_gb"] * 1e9
+        adj_all, both_ms = reduce_timing(adj_substeps, tr["fwd_ms"] + tr["bwd_ms"], world_size, dev)
+        _, fwd_ms = reduce_timing(adj_substeps, tr["fwd_ms"], world_size, dev)
         bwd_ms = both_ms - fwd_ms
         finite = bool(np.isfinite(dv0).all() and np.isfinite(dp0).all())
 
@@ -531,7 +541,7 @@ def main():
         p_sub = 0
         for _ in range(pk_steps):
             p_sub += world.step(sc.dt).substeps
-        dv = loss_grad()
+        dv = loss_grad(world)
         world.profile(True)
         world.profile_reset()
         world.step_backward(np.zeros_like(dv), dv)
@@ -584,12 +594,33 @@ def main():
             w_ms += e0.elapsed_time(e1)
             w_sub += r.substeps
             w_its += r.iterations
+        # forward + adjoint of the warm-started world, as the cold leg's, from where its timed
+        # steps ended (the impulses are taped with the state)
+        wtr = None
+        if args.adjoint_steps > 0 and args.positions == "absolute":
+            wtr = taped_round(ww, wstream, args.adjoint_steps, max(0, args.adjoint_every))
         ww.close()
         w_all, w_ms = reduce_timing(w_sub, w_ms, world_size, dev)
         warm = {"value": w_all / (w_ms / 1e3), "unit": UNIT, "steps": warm_steps,
                 "after_steps": max(args.warmup, 3), "substeps": w_sub,
                 "solver_iterations_per_substep": w_its / max(w_sub, 1),
                 "setting": "warm_start=1: one push at half the stiffness impulse of the particle's last solve"}
+        if wtr is not None:
+            a_all, a_ms = reduce_timing(wtr["substeps"], wtr["fwd_ms"] + wtr["bwd_ms"], world_size, dev)
+            _, a_fwd = reduce_timing(wtr["substeps"], wtr["fwd_ms"], world_size, dev)
+            a_value = a_all / (a_ms / 1e3)
+            warm["forward_adjoint"] = {
+                "value": a_value, "unit": UNIT,
+                "gradients_finite": bool(np.isfinite(wtr["dv0"]).all() and np.isfinite(wtr["dp0"]).all()),
+                "steps": args.adjoint_steps, "substeps": wtr["substeps"],
+                "checkpoint_every": max(0, args.adjoint_every),
+                "forward_ms": a_fwd, "backward_ms": a_ms - a_fwd, "ratio_to_forward": a_ms / a_fwd,
+                "ratio_to_plain_substeps": warm["value"] / a_value,
+                "device_memory_gb": {"taped_forward": wtr["taped_gb"], "after_backward": wtr["backward_gb"],
+                                     "before_tape": wtr["before_gb"],
+                                     "note": "the whole device, the cold world and its tape's records included"},
+                "grad_gravity": list(wtr["grads"]["gravity"]),
+                "grad_uniform_inflow": [float(x) for x in wtr["dv0"].astype(np.float64).sum(axis=0)]}
 
     base = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
