@@ -16,7 +16,7 @@ substep's divergence and density solves).  Differences at eps 1e-2 cross the los
 stops, the < 20 neighbour rule, clamps), which is why they scatter.  Every evaluation starts from the same state handed to a
 new world, so the differences and the adjoint see the same particle order.
 
-    python tests/adjoint_c5.py [--steps 32] [--tangent 32|64] [--out FILE]
+    python tests/adjoint_c5.py [--steps 32] [--tangent 32|64] [--warm-start] [--out FILE]
 """
 import argparse
 import dataclasses
@@ -58,10 +58,14 @@ def main():
     ap.add_argument("--warm", type=int, default=20)
     ap.add_argument("--tangent", type=int, choices=(32, 64), default=None,
                     help="add the column of the exact derivative of the FP32 program (32) or the FP64 method (64)")
+    ap.add_argument("--warm-start", action="store_true",
+                    help="warm-started solves (each run starts with no impulses: a world made from a state)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
 
     sc = scenes.dfsph_dam_1m()
+    if args.warm_start:
+        sc = dataclasses.replace(sc, settings=dataclasses.replace(sc.settings, warm_start=True))
     w = fluid.FluidWorld(sc.settings)
     sc.build(w)
     for _ in range(args.warm):
@@ -105,7 +109,8 @@ def main():
     # the inflow derivative sums a million per-particle terms: how much of their size cancels (an
     # FP32 error in each term grows by this factor in the sum)
     spread = np.abs(dv0.astype(np.float64)).sum(axis=0) / np.maximum(np.abs(inflow), 1e-300)
-    lines = [f"1M DFSPH dam, {args.steps} steps of {sc.dt} s from {args.warm} steps in; loss (kinetic energy) "
+    lines = [f"1M DFSPH dam{' (warm-started solves)' if args.warm_start else ''}, {args.steps} steps of "
+             f"{sc.dt} s from {args.warm} steps in; loss (kinetic energy) "
              f"{L:.6e} J", f"sum |dL/dv0| / |sum dL/dv0| per axis: {spread[0]:.3g}, {spread[1]:.3g}, {spread[2]:.3g}",
              "", head, rule]
     worst = []
