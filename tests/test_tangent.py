@@ -42,9 +42,12 @@ def run64(oracle_lib, s, steps, dt, pos, vel):
     return np.asarray(w.positions())[order], np.asarray(w.velocities())[order]
 
 
-@pytest.mark.parametrize("solver", [FluidSolver.WCSPH, FluidSolver.DFSPH])
-def test_tangent_values_are_the_fp64_restatements_and_tangents_its_differences(oracle_lib, solver):
+@pytest.mark.parametrize("solver,warm", [(FluidSolver.WCSPH, False), (FluidSolver.DFSPH, False),
+                                         (FluidSolver.DFSPH, True)])
+def test_tangent_values_are_the_fp64_restatements_and_tangents_its_differences(oracle_lib, solver, warm):
+    # warm: warm-started solves, whose impulses carry derivatives from substep to substep
     s, steps, dt, pos, vel = case(solver)
+    s = dataclasses.replace(s, warm_start=warm)
     d = np.random.default_rng(7).normal(size=vel.shape)
     P, V, dP, dV, ids = oracle_lib.tangent_run(s, TANK, pos, vel, np.zeros_like(d), d, steps=steps, dt=dt)
     assert np.array_equal(ids, np.arange(len(pos)))
