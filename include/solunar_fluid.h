@@ -307,16 +307,18 @@ typedef struct slf_param_grads {
  * change while recording.
  *
  * checkpoint_every = k > 0 (segment checkpointing): the current state is the first checkpoint and
- * the state before every k-th substep is kept too, 36 bytes per particle each.  The backward pass
- * runs each segment of k substeps forward again from its checkpoint, recording it, so it holds one
- * segment's records at a time however many substeps the flow makes a step take.  A WCSPH
+ * the state before every k-th substep is kept too, 36 bytes per particle each (44 with warm
+ * starts: the two solver impulses).  The backward pass runs each segment of k substeps forward
+ * again from its checkpoint, recording it, so it holds one segment's records at a time however
+ * many substeps the flow makes a step take.  A WCSPH
  * segment's records also keep each substep's neighbour lists (about 16 bytes per particle per list
  * slot), which this call reserves when a segment's worth fits in half the device's free memory;
  * otherwise the backward runs each of the segment's substeps once more before its adjoint.
  *
  * checkpoint_every = 0: every substep keeps the state before it and its solver record (the rates
  * and velocities of each DFSPH iteration), about 68 + 20 x iterations bytes per particle per
- * substep; the backward pass redoes only each substep's sort and densities.
+ * substep (8 more with warm starts); the backward pass redoes only each substep's sort and
+ * densities.
  *
  * Taken: WCSPH and DFSPH, absolute or cell-relative positions (cell-relative checkpoints and
  * records add the 16-byte cell of each particle); WCSPH with terrain (its density, push, damping
