@@ -68,6 +68,8 @@ def parse():
                          "substep")
     ap.add_argument("--adjoint-steps", type=int, default=32,
                     help="steps of the forward+adjoint measurement (0 skips it)")
+    ap.add_argument("--warm-adjoint-steps", type=int, default=None,
+                    help="steps of the warm-started world's forward+adjoint (default: --adjoint-steps; 0 skips it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed CPU work in the baseline")
     ap.add_argument("--no-density-error", action="store_true",
@@ -597,8 +599,9 @@ def main():
         # forward + adjoint of the warm-started world, as the cold leg's, from where its timed
         # steps ended (the impulses are taped with the state)
         wtr = None
-        if args.adjoint_steps > 0 and args.positions == "absolute":
-            wtr = taped_round(ww, wstream, args.adjoint_steps, max(0, args.adjoint_every))
+        w_adj_steps = args.adjoint_steps if args.warm_adjoint_steps is None else args.warm_adjoint_steps
+        if w_adj_steps > 0 and args.positions == "absolute":
+            wtr = taped_round(ww, wstream, w_adj_steps, max(0, args.adjoint_every))
         ww.close()
         w_all, w_ms = reduce_timing(w_sub, w_ms, world_size, dev)
         warm = {"value": w_all / (w_ms / 1e3), "unit": UNIT, "steps": warm_steps,
@@ -612,7 +615,7 @@ def main():
             warm["forward_adjoint"] = {
                 "value": a_value, "unit": UNIT,
                 "gradients_finite": bool(np.isfinite(wtr["dv0"]).all() and np.isfinite(wtr["dp0"]).all()),
-                "steps": args.adjoint_steps, "substeps": wtr["substeps"],
+                "steps": w_adj_steps, "substeps": wtr["substeps"],
                 "checkpoint_every": max(0, args.adjoint_every),
                 "forward_ms": a_fwd, "backward_ms": a_ms - a_fwd, "ratio_to_forward": a_ms / a_fwd,
                 "ratio_to_plain_substeps": warm["value"] / a_value,

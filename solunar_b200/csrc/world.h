@@ -413,11 +413,13 @@ struct World {
     struct DfsphRecord {
         DevBuf<float4> div_vel, den_vel, va, pre;
         DevBuf<float> div_rate, den_rate;
+        DevBuf<float2> warm;  // warm starts: the impulses the solves started from, sorted
         uint32_t div_n = 0, den_n = 0;
         void release(cudaStream_t st) {
             for (auto* b : {&div_vel, &den_vel, &va, &pre}) b->release(st);
             div_rate.release(st);
             den_rate.release(st);
+            warm.release(st);
         }
     };
     // A substep recorded as it ran (tapes that checkpoint every substep's record): the state
@@ -429,18 +431,22 @@ struct World {
         DevBuf<int4> cells;  // cell-relative positions: the cells of pos's offsets
         DevBuf<float2> warm;  // warm starts: each particle's impulses before the substep
         DfsphRecord rec;
-        // A WCSPH substep that a checkpoint segment ran again keeps what its adjoint reads (the
-        // sorted state, densities and pressures, the sort's destinations, the pre-clamp
-        // velocities, the ground slopes, the walk order and both neighbour lists, which change
-        // places with the world's), so the segment's reverse sweep runs no substep a third time.
+        // A substep that a checkpoint segment ran again keeps what its adjoint reads, so the
+        // segment's reverse sweep runs no substep a third time: WCSPH the sorted state, densities
+        // and pressures, the sort's destinations, the pre-clamp velocities, the ground slopes,
+        // the walk order and both neighbour lists (which change places with the world's); DFSPH
+        // the sorted positions, densities and factors, the sort's destinations, the walk order
+        // and both lists with their kept gradients (written there by the substep's own density
+        // pass), beside its solver record.
         bool kept = false;
         bool ordered = false;  // the lists walk rows in `order`
         uint32_t cap = 0;      // the lists' room a row
         DevBuf<float4> spos, svel, pre, slope;
         DevBuf<int4> scells;
-        DevBuf<float> rho, press, scaled;
+        DevBuf<float> rho, press, scaled, alpha;
         DevBuf<uint32_t> dest, order, fcnt, wcnt;
         DevBuf<uint2> fent, went;
+        DevBuf<float4> fgv, wgv;
         // With coupled bodies (tapes that record every substep): the body points the substep
         // met, with their cell table, and the sound speed the step ran at, `raised` when a fast
         // body set it above the settings' (the settings' then take no derivative from it).
@@ -460,10 +466,12 @@ struct World {
             rec.release(st);
             for (auto* b : {&spos, &svel, &pre, &slope}) b->release(st);
             scells.release(st);
-            for (auto* b : {&rho, &press, &scaled}) b->release(st);
+            for (auto* b : {&rho, &press, &scaled, &alpha}) b->release(st);
             for (auto* b : {&dest, &order, &fcnt, &wcnt}) b->release(st);
             fent.release(st);
             went.release(st);
+            fgv.release(st);
+            wgv.release(st);
             for (auto* b : {&mpos, &mvel}) b->release(st);
             mstart.release(st);
             mkeys.release(st);
@@ -474,8 +482,14 @@ struct World {
     // After a WCSPH substep of a segment's replay (its sort writing `sub.dest`, its advance
     // `sub.pre`): the substep's forward into `sub` (SubRecord::kept).
     int32_t keep_wcsph_substep(SubRecord& sub);
-    // The device buffers a WCSPH checkpoint segment's records take, at the current size and list
-    // room, so that the backward allocates nothing (slf_tape_begin reserves a segment of them).
+    // A DFSPH substep of a segment's replay into `sub`: its lists and counts change places with
+    // the world's for the substep (the density pass writes them into the record, so the solves'
+    // graphs see the same buffers each time the record comes round), its sort writes `sub.dest`;
+    // then the sorted positions, densities, factors and walk order are copied.
+    int32_t kept_dfsph_substep(float dt, SubRecord& sub);
+    void swap_lists(SubRecord& sub);
+    // The device buffers a checkpoint segment's records take, at the current size and list room,
+    // so that the backward allocates nothing (slf_tape_begin reserves a segment of them).
     int32_t reserve_kept(SubRecord& sub);
 
     // ---- the tape of slf_tape_begin: checkpoints and the substep lengths of each step ----
@@ -902,6 +916,10 @@ struct World {
     // but is waited for at once, as its record is copied out by its iteration count.
     static constexpr uint32_t kGraphMaxIterations = 10000;
     static constexpr size_t kGraphCache = 12;
+    // Solve graphs: a checkpoint segment's replay keeps each DFSPH substep's lists in that
+    // substep's record, so a segment of k substeps brings k list sets, each solved twice in up
+    // to six slot arrangements (12 k graphs); room for a 22-substep segment's 264.
+    static constexpr size_t kSolveGraphCache = 300;
     struct SolveGraph {
         std::vector<uint8_t> key;
         cudaGraphExec_t exec = nullptr;

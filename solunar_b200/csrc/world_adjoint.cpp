@@ -12,6 +12,21 @@ auto World::new_record() -> std::unique_ptr<SubRecord> {
 }
 
 int32_t World::reserve_kept(SubRecord& sub) {
+    const size_t slots = PairLists::slots_for(uint32_t(n), list_cap);
+    if (s.solver == SLF_SOLVER_DFSPH) {
+        for (auto* b : {&sub.pos, &sub.vel, &sub.spos}) SLF_TRY(b->ensure(n, 0, stream));
+        for (auto* b : {&sub.rho, &sub.alpha}) SLF_TRY(b->ensure(n, 0, stream));
+        for (auto* b : {&sub.ids, &sub.dest, &sub.order, &sub.fcnt, &sub.wcnt}) SLF_TRY(b->ensure(n, 0, stream));
+        if (rel()) SLF_TRY(sub.cells.ensure(n, 0, stream));
+        if (warm_on()) SLF_TRY(sub.warm.ensure(n, 0, stream));
+        SLF_TRY(sub.fent.ensure(slots, 0, stream));
+        SLF_TRY(sub.went.ensure(slots, 0, stream));
+        if (keeps_gradients()) {
+            SLF_TRY(sub.fgv.ensure(slots, 0, stream));
+            SLF_TRY(sub.wgv.ensure(slots, 0, stream));
+        }
+        return SLF_OK;
+    }
     for (auto* b : {&sub.pos, &sub.vel, &sub.spos, &sub.svel, &sub.pre}) SLF_TRY(b->ensure(n, 0, stream));
     for (auto* b : {&sub.rho, &sub.press, &sub.scaled}) SLF_TRY(b->ensure(n, 0, stream));
     for (auto* b : {&sub.ids, &sub.dest, &sub.order, &sub.fcnt, &sub.wcnt}) SLF_TRY(b->ensure(n, 0, stream));
@@ -20,7 +35,6 @@ int32_t World::reserve_kept(SubRecord& sub) {
         SLF_TRY(sub.scells.ensure(n, 0, stream));
     }
     if (!terrains.empty()) SLF_TRY(sub.slope.ensure(n, 0, stream));
-    const size_t slots = PairLists::slots_for(uint32_t(n), list_cap);
     SLF_TRY(sub.fent.ensure(slots, 0, stream));
     SLF_TRY(sub.went.ensure(slots, 0, stream));
     return SLF_OK;
@@ -79,6 +93,47 @@ int32_t World::sync() {
     return SLF_OK;
 }
 
+void World::swap_lists(SubRecord& sub) {
+    std::swap(fent, sub.fent);
+    std::swap(went, sub.went);
+    std::swap(fcnt, sub.fcnt);
+    std::swap(wcnt, sub.wcnt);
+    std::swap(fgv, sub.fgv);
+    std::swap(wgv, sub.wgv);
+}
+
+int32_t World::kept_dfsph_substep(float dt, SubRecord& sub) {
+    SLF_TRY(sub.dest.ensure(n, 0, stream));
+    swap_lists(sub);
+    sort_dest = sub.dest.p;
+    uint32_t held = 0, its = 0;
+    int32_t rs = dfsph_substep(dt, held, its, &sub.rec);
+    if (rs == kRetry) rs = dfsph_substep(dt, held, its, &sub.rec);
+    if (rs == kRetry) rs = fail(SLF_ERR_CUDA, "neighbour lists outgrew their room twice");
+    sort_dest = nullptr;
+    // the record keeps the lists the substep wrote; the world's own buffers come back, to be
+    // refilled by the next substep (a list room grown in the substep grows them too)
+    sub.cap = list_cap;
+    swap_lists(sub);
+    lists_valid = false;
+    SLF_TRY(rs);
+    SLF_TRY(ensure_work_buffers());
+    // the committed substep's sorted slots, as recompute names them
+    const int a = (cpos + 2) % 3, nid = cid;
+    auto copy = [&](auto& to, const auto* from, size_t count) -> int32_t {
+        SLF_TRY(to.ensure(count, 0, stream));
+        SLF_CUDA(cudaMemcpyAsync(to.p, from, count * sizeof(*from), cudaMemcpyDeviceToDevice, stream));
+        return SLF_OK;
+    };
+    SLF_TRY(copy(sub.spos, pos[a].p, n));
+    SLF_TRY(copy(sub.rho, rho[nid].p, n));
+    SLF_TRY(copy(sub.alpha, alpha.p, n));
+    sub.ordered = walk_order() != nullptr;
+    if (sub.ordered) SLF_TRY(copy(sub.order, worder.p, n));
+    sub.kept = true;
+    return SLF_OK;
+}
+
 int32_t World::tape_begin(uint32_t every) {
     SLF_TRY(flush());
     tape.on = true;
@@ -89,11 +144,13 @@ int32_t World::tape_begin(uint32_t every) {
     tape.ckpt_sub.clear();
     drop_records(0);
     tape.keep_segments = false;
-    if (every && s.solver == SLF_SOLVER_WCSPH && n) {
+    if (every && n) {
         // the records of one checkpoint segment, each with room for its substep's forward, when
         // a segment's worth fits in half the device's free memory (else the backward runs each
-        // substep again before its adjoint)
-        const size_t per = 2 * PairLists::slots_for(uint32_t(n), list_cap) * sizeof(uint2) + size_t(n) * 160;
+        // substep again before its adjoint: WCSPH whole, DFSPH its sort and density pass)
+        const size_t slots = PairLists::slots_for(uint32_t(n), list_cap);
+        const size_t entry = sizeof(uint2) + (keeps_gradients() ? sizeof(float4) : 0);
+        const size_t per = 2 * slots * entry + size_t(n) * (s.solver == SLF_SOLVER_DFSPH ? 112 : 160);
         size_t free = 0, total = 0;
         SLF_CUDA(cudaMemGetInfo(&free, &total));
         tape.keep_segments = size_t(every) * per <= free / 2;
@@ -292,6 +349,26 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                                          stream);
                 });
             } else {
+                // the substep's sorted positions, densities, factors, sort destinations, lists
+                // and starting impulses: the world's after the replay of its sort and densities,
+                // or those a segment's replay kept
+                const float4* spx = pos[a].p;
+                const float *srh = rho[nid].p, *sal = alpha.p;
+                const uint32_t* sdest = dest.p;
+                const float2* applied = warm_on() ? warm[nid].p : nullptr;
+                if (kept) {
+                    spx = kept->spos.p;
+                    srh = kept->rho.p;
+                    sal = kept->alpha.p;
+                    sdest = kept->dest.p;
+                    if (applied) applied = kept->rec.warm.p;
+                    const uint32_t* order = kept->ordered ? kept->order.p : nullptr;
+                    fl = PairLists{kept->cap, kept->fent.p, kept->fcnt.p, order,
+                                   keeps_gradients() ? kept->fgv.p : nullptr};
+                    wl = PairLists{kept->cap, kept->went.p, kept->wcnt.p, order,
+                                   keeps_gradients() ? kept->wgv.p : nullptr};
+                    launch_set_consts(consts(dt), d_consts, stream);
+                }
                 // advance, density solve, viscosity, divergence solve, factors, densities,
                 // sort: the substep's steps backwards
                 timed("adj_advance", 0.0, [&] {
@@ -299,16 +376,14 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                 });
                 SLF_CUDA(cudaMemsetAsync(rb.p, 0, n * 4, stream));
                 SLF_CUDA(cudaMemsetAsync(abar.p, 0, n * 4, stream));
-                // warm starts: the impulses before the substep (the replayed sort left them in
-                // slot nid, sorted) and their adjoint after it
-                const float2* applied = warm_on() ? warm[nid].p : nullptr;
+                // warm starts: the adjoint of the impulses after the substep
                 const float2* apb = warm_on() ? B.appbar.p : nullptr;
                 // each solve's warm push ran before its first check: its adjoint after the
                 // last iteration's (share: the forward's half of the last impulse)
                 auto warm_push = [&](int which) {
                     if (!applied) return;
                     timed(which == 1 ? "adj_warm_density" : "adj_warm_divergence", 0.0, [&] {
-                        launch_adj_warm(which, p, d_consts, fl, wl, form, pos[a].p, dwalls.p, vb.p, applied, apb,
+                        launch_adj_warm(which, p, d_consts, fl, wl, form, spx, dwalls.p, vb.p, applied, apb,
                                         0.5f, kw.p, vr.p, B.appbar_out.p, vp.p, xb.p, stream);
                     });
                     std::swap(vb, vp);
@@ -316,8 +391,8 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                 for (uint32_t it = rec.den_n; it-- > 0;) {
                     for (int part = 1; part <= 2; ++part)
                         timed(part == 1 ? "adj_kappa_density" : "adj_push_density", 0.0, [&] {
-                            launch_adj_iteration(1, p, d_consts, fl, wl, form, pos[a].p, dwalls.p, vb.p,
-                                                 rec.den_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
+                            launch_adj_iteration(1, p, d_consts, fl, wl, form, spx, dwalls.p, vb.p,
+                                                 rec.den_rate.p + size_t(it) * n, sal, srh,
                                                  rec.den_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p,
                                                  vp.p, xb.p, stream, part, apb);
                         });
@@ -325,14 +400,14 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                 }
                 warm_push(1);
                 timed("adj_viscosity", 0.0, [&] {
-                    launch_adj_viscosity(p, d_consts, fl, wl, form, pos[a].p, rec.va.p, rho[nid].p, zeros.p,
+                    launch_adj_viscosity(p, d_consts, fl, wl, form, spx, rec.va.p, srh, zeros.p,
                                          dwalls.p, vb.p, ab.p, xb.p, rb.p, grads.p, stream);
                 });
                 for (uint32_t it = rec.div_n; it-- > 0;) {
                     for (int part = 1; part <= 2; ++part)
                         timed(part == 1 ? "adj_kappa_divergence" : "adj_push_divergence", 0.0, [&] {
-                            launch_adj_iteration(0, p, d_consts, fl, wl, form, pos[a].p, dwalls.p, vb.p,
-                                                 rec.div_rate.p + size_t(it) * n, alpha.p, rho[nid].p,
+                            launch_adj_iteration(0, p, d_consts, fl, wl, form, spx, dwalls.p, vb.p,
+                                                 rec.div_rate.p + size_t(it) * n, sal, srh,
                                                  rec.div_vel.p + size_t(it) * n, kw.p, vr.p, abar.p, rb.p,
                                                  vp.p, xb.p, stream, part, apb);
                         });
@@ -340,11 +415,11 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                 }
                 warm_push(0);
                 timed("adj_factors_density", 0.0, [&] {
-                    launch_adj_factors_density(p, fl, wl, form, pos[a].p, dwalls.p, alpha.p, abar.p, gt.p,
+                    launch_adj_factors_density(p, fl, wl, form, spx, dwalls.p, sal, abar.p, gt.p,
                                                rb.p, xb.p, stream);
                 });
                 timed("adj_unsort", 0.0, [&] {
-                    launch_adj_unsort(uint32_t(n), dest.p, xb.p, vb.p, xp.p, vp.p, stream,
+                    launch_adj_unsort(uint32_t(n), sdest, xb.p, vb.p, xp.p, vp.p, stream,
                                       warm_on() ? B.appbar_out.p : nullptr, B.appbar.p);
                 });
             }
@@ -449,6 +524,8 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                         sort_dest = nullptr;
                         vel_pre = nullptr;
                         if (rs == SLF_OK) rs = keep_wcsph_substep(sub);
+                    } else if (tape.keep_segments) {
+                        rs = kept_dfsph_substep(dts[q], sub);
                     } else {
                         rs = dfsph_substep(dts[q], held, its, &sub.rec);
                         if (rs == kRetry) rs = dfsph_substep(dts[q], held, its, &sub.rec);

@@ -194,7 +194,7 @@ int32_t World::solve_graph(int which, const Params& p, int a, float4* v, int nid
         cudaError_t made = cudaGraphInstantiate(&g.exec, graph, 0);
         cudaGraphDestroy(graph);
         SLF_CUDA(made);
-        if (solve_graphs.size() >= kGraphCache) {
+        if (solve_graphs.size() >= kSolveGraphCache) {
             auto old = std::min_element(solve_graphs.begin(), solve_graphs.end(),
                                         [](const SolveGraph& x, const SolveGraph& y) { return x.used < y.used; });
             cudaGraphExecDestroy(old->exec);
@@ -389,6 +389,10 @@ int32_t World::dfsph_substep(float dt, uint32_t& held, uint32_t& iterations, Dfs
     if (whole) SLF_TRY(substep_graph(dt, p, a, b, nid, sp, whole));
     if (!whole) {
         SLF_TRY(enqueue_sort(a, sp, stream));
+        if (rec && warm_on()) {  // the impulses the solves start from, which they overwrite
+            SLF_TRY(rec->warm.ensure(n, 0, stream));
+            SLF_CUDA(cudaMemcpyAsync(rec->warm.p, warm[nid].p, n * sizeof(float2), cudaMemcpyDeviceToDevice, stream));
+        }
         SLF_TRY(reset_status());
         graph_solves = 0;
         launch_set_consts(consts(dt), d_consts, stream);
