@@ -488,8 +488,8 @@ struct World {
     // then the sorted positions, densities, factors and walk order are copied.
     int32_t kept_dfsph_substep(float dt, SubRecord& sub);
     void swap_lists(SubRecord& sub);
-    // The device buffers a checkpoint segment's records take, at the current size and list room,
-    // so that the backward allocates nothing (slf_tape_begin reserves a segment of them).
+    // The device buffers a WCSPH checkpoint segment's records take, at the current size and list
+    // room, so that the backward allocates nothing (slf_tape_begin reserves a segment of them).
     int32_t reserve_kept(SubRecord& sub);
 
     // ---- the tape of slf_tape_begin: checkpoints and the substep lengths of each step ----
@@ -920,6 +920,11 @@ struct World {
     // substep's record, so a segment of k substeps brings k list sets, each solved twice in up
     // to six slot arrangements (12 k graphs); room for a 22-substep segment's 264.
     static constexpr size_t kSolveGraphCache = 300;
+    // A DFSPH segment kept in its records (kept_dfsph_substep) saves each substep's third sort
+    // and density pass, but its solves meet new graph keys until every record has come round in
+    // every slot arrangement: with graphs the backward keeps segments only on tapes of at least
+    // this many (C5's 251 gain 0.8 ms a substep; 4 segments of 8 substeps lost 130 ms).
+    static constexpr size_t kKeepMinSegments = 32;
     struct SolveGraph {
         std::vector<uint8_t> key;
         cudaGraphExec_t exec = nullptr;

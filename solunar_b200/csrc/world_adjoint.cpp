@@ -13,20 +13,6 @@ auto World::new_record() -> std::unique_ptr<SubRecord> {
 
 int32_t World::reserve_kept(SubRecord& sub) {
     const size_t slots = PairLists::slots_for(uint32_t(n), list_cap);
-    if (s.solver == SLF_SOLVER_DFSPH) {
-        for (auto* b : {&sub.pos, &sub.vel, &sub.spos}) SLF_TRY(b->ensure(n, 0, stream));
-        for (auto* b : {&sub.rho, &sub.alpha}) SLF_TRY(b->ensure(n, 0, stream));
-        for (auto* b : {&sub.ids, &sub.dest, &sub.order, &sub.fcnt, &sub.wcnt}) SLF_TRY(b->ensure(n, 0, stream));
-        if (rel()) SLF_TRY(sub.cells.ensure(n, 0, stream));
-        if (warm_on()) SLF_TRY(sub.warm.ensure(n, 0, stream));
-        SLF_TRY(sub.fent.ensure(slots, 0, stream));
-        SLF_TRY(sub.went.ensure(slots, 0, stream));
-        if (keeps_gradients()) {
-            SLF_TRY(sub.fgv.ensure(slots, 0, stream));
-            SLF_TRY(sub.wgv.ensure(slots, 0, stream));
-        }
-        return SLF_OK;
-    }
     for (auto* b : {&sub.pos, &sub.vel, &sub.spos, &sub.svel, &sub.pre}) SLF_TRY(b->ensure(n, 0, stream));
     for (auto* b : {&sub.rho, &sub.press, &sub.scaled}) SLF_TRY(b->ensure(n, 0, stream));
     for (auto* b : {&sub.ids, &sub.dest, &sub.order, &sub.fcnt, &sub.wcnt}) SLF_TRY(b->ensure(n, 0, stream));
@@ -154,7 +140,9 @@ int32_t World::tape_begin(uint32_t every) {
         size_t free = 0, total = 0;
         SLF_CUDA(cudaMemGetInfo(&free, &total));
         tape.keep_segments = size_t(every) * per <= free / 2;
-        if (tape.keep_segments) {
+        // (a DFSPH segment's records take their buffers when a backward first keeps one: a
+        // short tape replays its segments, and holds none)
+        if (tape.keep_segments && s.solver == SLF_SOLVER_WCSPH) {
             while (spare_records.size() < every) spare_records.push_back(std::make_unique<SubRecord>());
             for (size_t k = spare_records.size() - every; k < spare_records.size(); ++k)
                 SLF_TRY(reserve_kept(*spare_records[k]));
@@ -489,6 +477,8 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
             segsubs.clear();
         };
         auto segs = [&]() -> int32_t {
+            const bool keep_dfsph = tape.keep_segments && (!graphs_for(SolveRec{nullptr, nullptr}) ||
+                                                           tape.ckpt_sub.size() >= kKeepMinSegments);
             std::vector<float> all;  // every recorded substep's length, in order
             for (const auto& st : tape.steps) all.insert(all.end(), st.begin(), st.end());
             for (size_t c = tape.ckpt_sub.size(); c-- > 0;) {
@@ -524,7 +514,7 @@ int32_t World::step_backward(const float* dpos, const float* dvel, uint64_t k, f
                         sort_dest = nullptr;
                         vel_pre = nullptr;
                         if (rs == SLF_OK) rs = keep_wcsph_substep(sub);
-                    } else if (tape.keep_segments) {
+                    } else if (keep_dfsph) {
                         rs = kept_dfsph_substep(dts[q], sub);
                     } else {
                         rs = dfsph_substep(dts[q], held, its, &sub.rec);

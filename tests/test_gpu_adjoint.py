@@ -242,6 +242,24 @@ def test_dfsph_tape_modes_give_identical_gradients(gpu_lib, dfsph_adjoint, every
     same_params(pr, params)
 
 
+@pytest.mark.parametrize("warm", [False, True])
+def test_dfsph_kept_segments_give_identical_gradients(gpu_lib, warm):
+    # 40 checkpoints, one a substep: enough segments that the backward keeps each segment's
+    # substeps in their records with the solves as graphs, against a tape that recorded every
+    # substep as it ran (the same records, the lists from the world's replay of each substep)
+    steps = 40
+    target = np.array([0.4, 0.1, 0.1])
+    out = []
+    for every in (0, 1):
+        w, _, _ = dfsph_run(gpu_lib.FluidWorld, settings=dfsph_settings(warm_start=warm))
+        out.append(taped_gradients(w, steps, DFSPH_DT, every, target))
+        w.close()
+    (dp0, dv0, p0), (dp1, dv1, p1) = out
+    assert np.isfinite(dv0).all() and np.abs(dv0).max() > 0
+    assert np.array_equal(dp1, dp0) and np.array_equal(dv1, dv0)
+    same_params(p1, p0)
+
+
 def test_wcsph_recorded_tape_gives_identical_gradients(gpu_lib, adjoint):
     sc, pos, vel, target, dp0, dv0, params = adjoint
     w, _, _ = run(gpu_lib.FluidWorld, sc)
