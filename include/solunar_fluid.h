@@ -310,10 +310,13 @@ typedef struct slf_param_grads {
  * the state before every k-th substep is kept too, 36 bytes per particle each (44 with warm
  * starts: the two solver impulses).  The backward pass runs each segment of k substeps forward
  * again from its checkpoint, recording it, so it holds one segment's records at a time however
- * many substeps the flow makes a step take.  A WCSPH
- * segment's records also keep each substep's neighbour lists (about 16 bytes per particle per list
- * slot), which this call reserves when a segment's worth fits in half the device's free memory;
- * otherwise the backward runs each of the segment's substeps once more before its adjoint.
+ * many substeps the flow makes a step take.  When a segment's worth fits in half the device's
+ * free memory, its records also keep each substep's neighbour lists, so the backward does not run
+ * the substep a third time: WCSPH about 16 bytes per particle per list slot, reserved by this
+ * call; DFSPH 48 with the EXACT kept gradients (about 3.2 GB a substep at a million particles),
+ * taken by the first backward that keeps, which it does on tapes of at least 32 segments or
+ * with solve graphs off (slf_solver_graphs 0).  Otherwise the backward runs each of the
+ * segment's substeps (DFSPH: its sort and densities) once more before its adjoint.
  *
  * checkpoint_every = 0: every substep keeps the state before it and its solver record (the rates
  * and velocities of each DFSPH iteration), about 68 + 20 x iterations bytes per particle per
