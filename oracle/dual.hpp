@@ -8,7 +8,10 @@
 //   Dual   = DualOf<double>: the derivative of the FP64 method;
 //   Dual32 = DualOf<float>:  the derivative of the FP32 program itself.  Its values are the float
 //          restatement's bit for bit (every value operation is the float one), hence the CUDA
-//          library's in EXACT arithmetic, so it takes every branch the library's run takes.
+//          library's in EXACT arithmetic, so it takes every branch the library's run takes;
+//   DualOf<float, float>:    the same values with each derivative operation rounded to float, as a
+//          single-precision derivative code carries it (how far that drifts from Dual32 measures
+//          the conditioning an FP32 adjoint meets).
 //
 // Tests check the CUDA library's adjoint (step_backward, the transposed derivative) with the
 // identity <g, J d> = <J^T g, d>.  Branches (the pressure clamp, approach-only viscosity, wall
@@ -21,12 +24,12 @@
 #include <cstdint>
 #include <type_traits>
 
-template <class V> struct DualOf {
+template <class V, class D = double> struct DualOf {
     V v = V(0);
-    double d = 0.0;
+    D d = D(0);
     DualOf() = default;
     DualOf(double x) : v(V(x)) {}  // constants carry no derivative
-    DualOf(double x, double dx) : v(V(x)), d(dx) {}
+    DualOf(double x, double dx) : v(V(x)), d(D(dx)) {}
     explicit operator double() const { return double(v); }
     explicit operator float() const { return float(v); }
     explicit operator int() const { return int(v); }
@@ -35,7 +38,7 @@ template <class V> struct DualOf {
     explicit operator unsigned long() const { return (unsigned long)(v); }
     explicit operator long long() const { return (long long)(v); }
 
-    static DualOf of(V x, double dx) {
+    static DualOf of(V x, D dx) {
         DualOf r;
         r.v = x;
         r.d = dx;
@@ -50,10 +53,10 @@ template <class V> struct DualOf {
     friend DualOf operator+(DualOf a, DualOf b) { return of(a.v + b.v, a.d + b.d); }
     friend DualOf operator-(DualOf a, DualOf b) { return of(a.v - b.v, a.d - b.d); }
     friend DualOf operator-(DualOf a) { return of(-a.v, -a.d); }
-    friend DualOf operator*(DualOf a, DualOf b) { return of(a.v * b.v, a.d * double(b.v) + double(a.v) * b.d); }
+    friend DualOf operator*(DualOf a, DualOf b) { return of(a.v * b.v, a.d * D(b.v) + D(a.v) * b.d); }
     friend DualOf operator/(DualOf a, DualOf b) {
-        double bv = double(b.v);
-        return of(a.v / b.v, (a.d * bv - double(a.v) * b.d) / (bv * bv));
+        D bv = D(b.v);
+        return of(a.v / b.v, (a.d * bv - D(a.v) * b.d) / (bv * bv));
     }
     friend bool operator<(DualOf a, DualOf b) { return a.v < b.v; }
     friend bool operator>(DualOf a, DualOf b) { return a.v > b.v; }
@@ -64,11 +67,11 @@ template <class V> struct DualOf {
 
     friend DualOf osqrt(DualOf x) {
         V r = std::sqrt(x.v);
-        return of(r, r > V(0) ? x.d / (2.0 * double(r)) : 0.0);
+        return of(r, r > V(0) ? x.d / (D(2) * D(r)) : D(0));
     }
-    friend DualOf ofloor(DualOf x) { return of(std::floor(x.v), 0.0); }
-    friend DualOf oceil(DualOf x) { return of(std::ceil(x.v), 0.0); }
-    friend DualOf oround(DualOf x) { return of(std::round(x.v), 0.0); }
+    friend DualOf ofloor(DualOf x) { return of(std::floor(x.v), D(0)); }
+    friend DualOf oceil(DualOf x) { return of(std::ceil(x.v), D(0)); }
+    friend DualOf oround(DualOf x) { return of(std::round(x.v), D(0)); }
     friend DualOf ofabs(DualOf x) { return x.v < V(0) ? -x : x; }
     friend bool oisnan(DualOf x) { return std::isnan(x.v); }
     friend bool oisfinite(DualOf x) { return std::isfinite(x.v); }
@@ -78,4 +81,4 @@ using Dual = DualOf<double>;
 using Dual32 = DualOf<float>;
 
 template <class R> struct is_dual : std::false_type {};
-template <class V> struct is_dual<DualOf<V>> : std::true_type {};
+template <class V, class D> struct is_dual<DualOf<V, D>> : std::true_type {};

@@ -14,8 +14,10 @@
 #include "fluid_oracle.hpp"
 
 // f32::total_cmp's order and the bit pattern of the value (the walls' sort key, boundary.rs:155-178)
-template <class V> inline bool total_less(DualOf<V> a, DualOf<V> b) { return oracle::total_less(a.v, b.v); }
-template <class V> inline uint64_t bits_of(DualOf<V> a) { return oracle::bits_of(a.v); }
+template <class V, class D> inline bool total_less(DualOf<V, D> a, DualOf<V, D> b) {
+    return oracle::total_less(a.v, b.v);
+}
+template <class V, class D> inline uint64_t bits_of(DualOf<V, D> a) { return oracle::bits_of(a.v); }
 
 using namespace oracle;
 
@@ -23,12 +25,12 @@ Settings settings_from_c(const slf_settings* s, int residual_sum);  // oracle_ca
 
 namespace {
 
-template <class V>
+template <class V, class D = double>
 int32_t tangent_run(const slf_settings* s, int32_t residual_sum, const float* low, const float* high, uint64_t n,
                     const float* pos, const float* vel, const double* dpos, const double* dvel, const double* dparams,
                     uint32_t steps, float dt, const uint32_t* forced, uint64_t nforced, double* out_pos,
                     double* out_vel, double* out_dpos, double* out_dvel, uint32_t* out_ids) {
-    using R = DualOf<V>;
+    using R = DualOf<V, D>;
     using Vec = V3<R>;
     World<R> w;
     Status st = World<R>::create(settings_from_c(s, residual_sum), w);
@@ -60,9 +62,9 @@ int32_t tangent_run(const slf_settings* s, int32_t residual_sum, const float* lo
         double* odp = out_dpos + 3 * i;
         double* odv = out_dvel + 3 * i;
         op[0] = double(p.x.v), op[1] = double(p.y.v), op[2] = double(p.z.v);
-        odp[0] = p.x.d, odp[1] = p.y.d, odp[2] = p.z.d;
+        odp[0] = double(p.x.d), odp[1] = double(p.y.d), odp[2] = double(p.z.d);
         ov[0] = double(v.x.v), ov[1] = double(v.y.v), ov[2] = double(v.z.v);
-        odv[0] = v.x.d, odv[1] = v.y.d, odv[2] = v.z.d;
+        odv[0] = double(v.x.d), odv[1] = double(v.y.d), odv[2] = double(v.z.d);
         out_ids[i] = w.ids[i];
     }
     return OK;
@@ -72,7 +74,8 @@ int32_t tangent_run(const slf_settings* s, int32_t residual_sum, const float* lo
 
 extern "C" {
 
-// precision: 32 (values of the float restatement, bit for bit) or 64 (the FP64 method).
+// precision: 32 (values of the float restatement, bit for bit), 64 (the FP64 method) or -32 (the
+// float restatement's values with every derivative operation rounded to float).
 // pos, vel, dpos, dvel: n x 3 in the order the particles are added (ids 0..n-1); dparams: the
 // tangents of viscosity, sound speed and gravity x, y, z.  forced (nforced counts, may be 0): the
 // iteration counts the DFSPH solves take, divergence and density of each substep in turn, so that
@@ -89,6 +92,9 @@ int32_t orc_tangent_run(const slf_settings* s, int32_t precision, int32_t residu
     if (precision == 32)
         return tangent_run<float>(s, residual_sum, low, high, n, pos, vel, dpos, dvel, dparams, steps, dt, forced,
                                   nforced, out_pos, out_vel, out_dpos, out_dvel, out_ids);
+    if (precision == -32)
+        return tangent_run<float, float>(s, residual_sum, low, high, n, pos, vel, dpos, dvel, dparams, steps, dt,
+                                         forced, nforced, out_pos, out_vel, out_dpos, out_dvel, out_ids);
     if (precision == 64)
         return tangent_run<double>(s, residual_sum, low, high, n, pos, vel, dpos, dvel, dparams, steps, dt, forced,
                                    nforced, out_pos, out_vel, out_dpos, out_dvel, out_ids);

@@ -115,7 +115,8 @@ def tangent_run(settings: FluidSettings, container, positions, velocities, dposi
                 forced_iterations=None, precision: int = 64):
     """The restatement in forward-mode derivative numbers (oracle/dual.hpp): values of the FP64
     method (precision 64) or of the float restatement bit for bit (32, the FP32 program the CUDA
-    library runs), derivatives in double.  A world with one box container
+    library runs), derivatives in double; -32: the float restatement's values with every
+    derivative operation rounded to float.  A world with one box container
     `container` = (low, high), the particles added in row order (ids 0..n-1), `steps` calls of
     step(dt).  Each input carries a tangent: dpositions, dvelocities (n x 3) and dparams (viscosity,
     sound speed, gravity x, y, z).  forced_iterations: the DFSPH solves' iteration counts
