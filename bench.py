@@ -12,6 +12,10 @@ times of the roofline come from a second pass of the same steps with every launc
 events (the profiler runs the substep launch by launch).
 `e2e` is the same metric through the C ABI with host-owned state: each step uploads positions
 and velocities from pinned host memory, steps, and reads them back.
+`forward_adjoint` tapes `--adjoint-steps` steps (every substep recorded, or a checkpoint every
+`--adjoint-every` substeps) and runs step_backward; `warm_start` repeats the plain steps and,
+with `--warm-adjoint-steps` (default: the same count), the forward+adjoint with warm-started
+solves on a world of its own.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
