@@ -129,3 +129,16 @@ def test_fp32_tangent_values_are_the_float_restatements_bit_for_bit(oracle_lib, 
     assert np.array_equal(V.astype(np.float32), np.asarray(w.velocities(), dtype=np.float32)[order])
     _, _, dP64, _, _ = oracle_lib.tangent_run(s, TANK, pos, vel, np.zeros_like(d), d, steps=steps, dt=dt)
     assert np.linalg.norm(dP - dP64) <= 1e-3 * np.linalg.norm(dP64)
+
+
+def test_float_derivatives_stay_near_the_exact_ones_on_a_short_run(oracle_lib):
+    # precision -32: the float restatement's values, each derivative operation rounded to float
+    # (tests/tangent_conditioning.py measures the same on the 1M dam)
+    s, steps, dt, pos, vel = case(FluidSolver.DFSPH)
+    d = np.random.default_rng(11).normal(size=vel.shape)
+    zero = np.zeros_like(d)
+    P32, V32, dP32, dV32, _ = oracle_lib.tangent_run(s, TANK, pos, vel, zero, d, steps=steps, dt=dt, precision=32)
+    Pf, Vf, dPf, dVf, _ = oracle_lib.tangent_run(s, TANK, pos, vel, zero, d, steps=steps, dt=dt, precision=-32)
+    assert np.array_equal(P32, Pf) and np.array_equal(V32, Vf)
+    assert np.linalg.norm(dVf - dV32) <= 1e-5 * np.linalg.norm(dV32)
+    assert np.linalg.norm(dPf - dP32) <= 1e-5 * np.linalg.norm(dP32)
