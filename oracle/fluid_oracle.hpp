@@ -475,6 +475,20 @@ template <class R> class World {
     // run it checks.  Empty (the default): solves stop on their tolerances.
     std::vector<uint32_t> forced_iterations;
     size_t forced_next = 0;
+    // A derivative run only: quantities held constant (their derivative dropped), to measure
+    // what each path of the DFSPH substep contributes to a tangent.  Bits: 1 fluid pair
+    // gradients, 2 wall pair gradients, 4 factors, 8 densities, 16 viscosity and gravity's
+    // velocity change, 32 solver stiffnesses.
+    uint32_t hold = 0;
+    template <class T> T constant_if(T x, uint32_t bit) const {
+        if constexpr (is_dual<R>::value) {
+            if (hold & bit) {
+                if constexpr (std::is_same<T, Vec>::value) return Vec(R(double(x.x)), R(double(x.y)), R(double(x.z)));
+                else return R::of(x.v, 0.0);
+            }
+        }
+        return x;
+    }
     int threads = 0;  // 0: OpenMP default
 
     static Status create(const Settings& s, World& out) {
@@ -2211,9 +2225,9 @@ template <class R> class World {
             size_t i = size_t(ii);
             Vec at = positions[i];
             for (uint32_t k = neighbors.start[i]; k < neighbors.start[i + 1]; ++k)
-                grad_fluid[k] = kernel.gradient(at - positions[neighbors.items[k]]);
+                grad_fluid[k] = constant_if(kernel.gradient(at - positions[neighbors.items[k]]), 1);
             for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
-                grad_walls[k] = kernel.gradient(at - walls.positions[wall_neighbors.items[k]]);
+                grad_walls[k] = constant_if(kernel.gradient(at - walls.positions[wall_neighbors.items[k]]), 2);
         }
     }
 
@@ -2234,7 +2248,7 @@ template <class R> class World {
             for (uint32_t k = wall_neighbors.start[i]; k < wall_neighbors.start[i + 1]; ++k)
                 sum = sum + grad_walls[k] * mass;
             R total = length_squared(sum) + squares;
-            out[i] = total > R(0) ? R(1) / total : R(0);
+            out[i] = constant_if(total > R(0) ? R(1) / total : R(0), 4);
         }
         return out;
     }
@@ -2301,7 +2315,7 @@ template <class R> class World {
                     target = r / dt;
                     error = dt * r / rest;
                 }
-                stiffness[i] = target * alpha[i];
+                stiffness[i] = constant_if(target * alpha[i], 32);
                 errors[i] = error;
             }
             size_t loaded = 0;
@@ -2337,6 +2351,8 @@ template <class R> class World {
         update_neighbors();
         Status st = compute_densities();
         if (st != OK) return st;
+        if (hold & 8)
+            for (auto& d : densities) d = constant_if(d, 8);
         gradients();
         std::vector<R> alpha = factors();
         last_iterations[0] = solve(0, dt, alpha);
@@ -2345,7 +2361,7 @@ template <class R> class World {
         Vec g = gravity();
         std::vector<Vec> pushes(n);
 #pragma omp parallel for schedule(static) num_threads(nthreads())
-        for (long long ii = 0; ii < (long long)n; ++ii) pushes[size_t(ii)] = viscous(size_t(ii), dt) + g;
+        for (long long ii = 0; ii < (long long)n; ++ii) pushes[size_t(ii)] = constant_if(viscous(size_t(ii), dt) + g, 16);
         for (size_t i = 0; i < n; ++i) velocities[i] = velocities[i] + pushes[i] * dt;
         last_iterations[1] = solve(1, dt, alpha);
         iterations += last_iterations[1];

@@ -25,6 +25,8 @@ Settings settings_from_c(const slf_settings* s, int residual_sum);  // oracle_ca
 
 namespace {
 
+uint32_t g_hold = 0;  // World::hold of the next runs (orc_tangent_hold)
+
 template <class V, class D = double>
 int32_t tangent_run(const slf_settings* s, int32_t residual_sum, const float* low, const float* high, uint64_t n,
                     const float* pos, const float* vel, const double* dpos, const double* dvel, const double* dparams,
@@ -37,6 +39,7 @@ int32_t tangent_run(const slf_settings* s, int32_t residual_sum, const float* lo
     if (st != OK) return st;
     for (int k = 0; k < 5; ++k) w.param_tangent[k] = dparams[k];
     w.forced_iterations.assign(forced, forced + nforced);
+    w.hold = g_hold;
     st = w.add_box_container(Vec(R(low[0]), R(low[1]), R(low[2])), Vec(R(high[0]), R(high[1]), R(high[2])), nullptr);
     if (st != OK) return st;
     for (uint64_t i = 0; i < n; ++i) {
@@ -73,6 +76,9 @@ int32_t tangent_run(const slf_settings* s, int32_t residual_sum, const float* lo
 }  // namespace
 
 extern "C" {
+
+// The quantities the next tangent runs hold constant (World::hold bits; 0: none).
+void orc_tangent_hold(uint32_t mask) { g_hold = mask; }
 
 // precision: 32 (values of the float restatement, bit for bit), 64 (the FP64 method) or -32 (the
 // float restatement's values with every derivative operation rounded to float).

@@ -93,6 +93,8 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = ctypes.c_int32
+        L.orc_tangent_hold.argtypes = [ctypes.c_uint32]
+        L.orc_tangent_hold.restype = None
         L.orc_snapshot_message.argtypes = []
         L.orc_snapshot_message.restype = ctypes.c_char_p
         L.orc_destroy.argtypes = [vp]
@@ -110,9 +112,15 @@ def _ptr(a: np.ndarray, ctype):
     return a.ctypes.data_as(ctypes.POINTER(ctype))
 
 
+# DFSPH quantities a tangent run can hold constant (their derivative dropped), for measuring what
+# each path of the substep contributes (World::hold in oracle/fluid_oracle.hpp)
+TANGENT_HOLD = {"fluid_gradients": 1, "wall_gradients": 2, "factors": 4, "densities": 8, "viscosity": 16,
+                "stiffness": 32}
+
+
 def tangent_run(settings: FluidSettings, container, positions, velocities, dpositions, dvelocities,
                 dparams=(0.0, 0.0, 0.0, 0.0, 0.0), steps: int = 1, dt: float = 1e-3, residual_sum: int = 1,
-                forced_iterations=None, precision: int = 64):
+                forced_iterations=None, precision: int = 64, hold=()):
     """The restatement in forward-mode derivative numbers (oracle/dual.hpp): values of the FP64
     method (precision 64) or of the float restatement bit for bit (32, the FP32 program the CUDA
     library runs), derivatives in double; -32: the float restatement's values with every
@@ -121,8 +129,9 @@ def tangent_run(settings: FluidSettings, container, positions, velocities, dposi
     step(dt).  Each input carries a tangent: dpositions, dvelocities (n x 3) and dparams (viscosity,
     sound speed, gravity x, y, z).  forced_iterations: the DFSPH solves' iteration counts
     (divergence, density of each substep in turn) to take instead of stopping on the tolerances,
-    so that the run follows another run's discrete steps.  Returns (positions, velocities, their
-    tangents, ids) of the final state, rows in id order."""
+    so that the run follows another run's discrete steps.  hold: names of TANGENT_HOLD whose
+    derivative the run drops.  Returns (positions, velocities, their tangents, ids) of the final
+    state, rows in id order."""
     p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
     v = np.ascontiguousarray(velocities, dtype=np.float32).reshape(-1, 3)
     dp_ = np.ascontiguousarray(dpositions, dtype=np.float64).reshape(-1, 3)
@@ -137,6 +146,10 @@ def tangent_run(settings: FluidSettings, container, positions, velocities, dposi
     f = ctypes.c_float
     d = ctypes.c_double
     forced = np.ascontiguousarray([] if forced_iterations is None else forced_iterations, dtype=np.uint32)
+    mask = 0
+    for name in hold:
+        mask |= TANGENT_HOLD[name]
+    lib().orc_tangent_hold(ctypes.c_uint32(mask))
     _check(lib().orc_tangent_run(ctypes.byref(c), precision, residual_sum, _ptr(lo, f), _ptr(hi, f), n, _ptr(p, f), _ptr(v, f),
                                  _ptr(dp_, d), _ptr(dv_, d), _ptr(dq, d), steps, dt, _ptr(forced, ctypes.c_uint32),
                                  len(forced), *(_ptr(o, d) for o in outs), _ptr(ids, ctypes.c_uint32)))

@@ -10,7 +10,13 @@ the exact derivative of the FP32 program) and once with every derivative operati
 float (precision -32, oracle/dual.hpp). The relative difference of dL/d(inflow) between the two,
 L the water's kinetic energy, is printed per horizon.
 
+With --hold, the tangent (derivatives in double) runs once with nothing held and once with
+each named quantity held constant (its derivative dropped: py_oracle.TANGENT_HOLD), and the
+table gives what each path contributes to dL/d(inflow).  --order sorted takes the state in the
+world's own order after the warm-up (the library's, bit for bit), as tests/adjoint_c5.py does.
+
     python tests/tangent_conditioning.py [--steps 8 16] [--axis 0] [--counts 100 100 100]
+    python tests/tangent_conditioning.py --steps 16 --order sorted --hold each
 """
 import argparse
 import os
@@ -32,6 +38,10 @@ def main():
     ap.add_argument("--warm", type=int, default=20, help="steps into the dam break before the tangent")
     ap.add_argument("--axis", type=int, default=0)
     ap.add_argument("--counts", type=int, nargs=3, default=None, help="block counts (default: the 1M scene's)")
+    ap.add_argument("--order", choices=("ids", "sorted"), default="ids",
+                    help="the state's rows after the warm-up: by particle id, or in the world's order")
+    ap.add_argument("--hold", nargs="*", default=None,
+                    help="quantities to hold constant one at a time ('each': all of py_oracle.TANGENT_HOLD)")
     args = ap.parse_args()
 
     py_oracle.build()
@@ -45,7 +55,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.warm):
         w.step(sc.dt)
-    order = np.argsort(w.ids())
+    order = np.argsort(w.ids()) if args.order == "ids" else np.arange(w.len())
     pos = np.asarray(w.positions(), dtype=np.float32)[order]
     vel = np.asarray(w.velocities(), dtype=np.float32)[order]
     mass = w.particle_mass()
@@ -54,6 +64,24 @@ def main():
     direction = np.zeros(pos.shape)
     direction[:, args.axis] = 1.0
     tank = ((0.0, 0.0, 0.0), sc.tank)
+    if args.hold is not None:
+        names = list(py_oracle.TANGENT_HOLD) if args.hold in (["each"], []) else args.hold
+        print("| steps | held constant | dL/d inflow | change |")
+        print("|---|---|---|---|")
+        for steps in args.steps:
+            full = None
+            for name in [None] + names:
+                t0 = time.perf_counter()
+                _, V, _, dV, _ = py_oracle.tangent_run(sc.settings, tank, pos, vel, np.zeros(pos.shape), direction,
+                                                       steps=steps, dt=sc.dt, precision=32,
+                                                       hold=() if name is None else (name,))
+                value = mass * float(np.sum(V * dV))
+                if name is None:
+                    full = value
+                change = "" if name is None else f"{value - full:+.6e}"
+                print(f"| {steps} | {name or 'nothing'} | {value:.9e} | {change} |", flush=True)
+                print(f"  ({time.perf_counter() - t0:.1f} s)", file=sys.stderr, flush=True)
+        return
     print("| steps | dL/d inflow, derivatives in double | in float | relative difference |")
     print("|---|---|---|---|")
     for steps in args.steps:
