@@ -478,7 +478,7 @@ template <class R> class World {
     // A derivative run only: quantities held constant (their derivative dropped), to measure
     // what each path of the DFSPH substep contributes to a tangent.  Bits: 1 fluid pair
     // gradients, 2 wall pair gradients, 4 factors, 8 densities, 16 viscosity and gravity's
-    // velocity change, 32 solver stiffnesses.
+    // velocity change, 32 solver stiffnesses, 64 the fluid pairs' viscosity, 128 the walls'.
     uint32_t hold = 0;
     template <class T> T constant_if(T x, uint32_t bit) const {
         if constexpr (is_dual<R>::value) {
@@ -2085,7 +2085,7 @@ template <class R> class World {
                 push = push - kernel.gradient(offset) * (mass * damp);
             }
         }
-        return push + wall_viscous(index, dt);
+        return constant_if(push, 64) + constant_if(wall_viscous(index, dt), 128);
     }
 
     // step.rs:144-224

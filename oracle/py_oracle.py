@@ -115,7 +115,7 @@ def _ptr(a: np.ndarray, ctype):
 # DFSPH quantities a tangent run can hold constant (their derivative dropped), for measuring what
 # each path of the substep contributes (World::hold in oracle/fluid_oracle.hpp)
 TANGENT_HOLD = {"fluid_gradients": 1, "wall_gradients": 2, "factors": 4, "densities": 8, "viscosity": 16,
-                "stiffness": 32}
+                "stiffness": 32, "fluid_viscosity": 64, "wall_viscosity": 128}
 
 
 def tangent_run(settings: FluidSettings, container, positions, velocities, dpositions, dvelocities,
